@@ -1,0 +1,66 @@
+// Device-side types and helpers shared by the factorization and solve kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hsg {
+
+// One front (supernode) as the kernels see it.
+struct SnDev {
+  std::int32_t first;     // first pivot position (global index of its first column)
+  std::int32_t k;         // fully-summed columns
+  std::int32_t m;         // rows of the front
+  std::int32_t parent;    // -1: root
+  std::int64_t panel_off; // m x k panel, ld m, in the factor storage
+  std::int64_t cb_off;    // (m-k)^2 contribution block, ld m-k, in the CB arena (-1: none)
+  std::int64_t rows_off;  // its rows in the row array
+  std::int64_t rmap_off;  // its CB rows' positions in the parent's rows
+  std::int64_t vec_off;   // contribution vector (m-k entries per rhs) in the solve arena
+  std::int64_t scratch_off;  // pivoting scratch of the panel kernel (doubles)
+};
+
+// Counters written by the factorization kernels (integers: sums are order independent).
+struct FactorCounters {
+  unsigned long long neg;
+  unsigned long long zero;
+  unsigned long long pos;
+  unsigned long long two_by_two;
+  unsigned long long failed;     // columns that could not be pivoted in their front
+  unsigned long long forced;     // pivots accepted without the threshold test (roots)
+  unsigned long long amax_bits;  // max |entry| of the scaled matrix (double bits)
+  unsigned long long pad;
+};
+
+struct FactorParams {
+  double u;              // threshold of pivot acceptance
+  double null_tol;       // relative null-pivot tolerance (0: detection off)
+  const FactorCounters* cnt;  // amax lives in cnt->amax_bits
+  std::int32_t failed_cap;
+};
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ double null_threshold(const FactorParams& p) {
+  return p.null_tol > 0.0 ? p.null_tol * __longlong_as_double(static_cast<long long>(p.cnt->amax_bits)) : -1.0;
+}
+
+// atomic max of a non-negative double stored as its bit pattern (order independent)
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* slot, double v) {
+  atomicMax(slot, static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+#endif  // __CUDACC__
+
+}  // namespace hsg

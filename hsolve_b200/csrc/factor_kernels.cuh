@@ -1,0 +1,37 @@
+// Launchers of the factorization kernels (factor_kernels.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace hsg {
+
+constexpr int kSmallMax = 64;          // fronts up to this order are factorized in shared memory
+constexpr int kNB = 32;                // panel width of the a-posteriori pivoting kernel
+constexpr int kTile = 64;              // trailing-update tile (rows = cols)
+constexpr int kAppThreads = 256;
+constexpr int kColsPerThread = kTile * kTile / kAppThreads;  // 16
+constexpr int kExtendAddCols = 8;      // contribution-block columns per extend-add CTA
+
+void launch_fill(double* x, std::int64_t n, double v, cudaStream_t s);
+void launch_zero_u64(unsigned long long* x, std::int64_t n, cudaStream_t s);
+void launch_scale_rowmax(std::int64_t nnz, const std::int32_t* row, const std::int32_t* col, const double* a,
+                         const double* b, double alpha, double beta, const double* d, unsigned long long* r,
+                         cudaStream_t s);
+void launch_scale_update(std::int64_t n, double* d, unsigned long long* r, cudaStream_t s);
+void launch_scatter(std::int64_t nnz, const std::int32_t* row, const std::int32_t* col, const double* a,
+                    const double* b, double alpha, double beta, const double* d, const std::int64_t* dest,
+                    double* panels, FactorCounters* cnt, cudaStream_t s);
+void launch_zero_cb(const std::int32_t* list, int nlist, int chunks, const SnDev* sn, double* cb, cudaStream_t s);
+void launch_extend_add(const int2* items, int nitems, const SnDev* sn, const std::int32_t* rmap, double* panels,
+                       double* cb, cudaStream_t s);
+void launch_front_small(int maxm, const std::int32_t* list, int nlist, const SnDev* sn, double* panels, double* cb,
+                        signed char* piv, std::int32_t* pidx, const FactorParams& prm, FactorCounters* cnt,
+                        std::int32_t* failed, cudaStream_t s);
+void launch_front_app(const std::int32_t* list, int nlist, const SnDev* sn, double* panels, double* cb,
+                      double* scratch, signed char* piv, std::int32_t* pidx, const FactorParams& prm,
+                      FactorCounters* cnt, std::int32_t* failed, cudaStream_t s);
+
+}  // namespace hsg

@@ -1,0 +1,359 @@
+// GpuFactor: analysis, numeric factorization driver and solves on the device (see gpu_factor.hpp).
+#include "gpu_factor.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <numeric>
+
+#include "factor_kernels.cuh"
+#include "solve_kernels.cuh"
+
+namespace hsg {
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) HSG_THROW(HSG_INTERNAL, "CUDA error in " << what << ": " << cudaGetErrorString(e));
+}
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Union of the upper patterns of A and B (B == null: identity), diagonal always present.
+void merge_upper(std::int64_t n, const std::int64_t* arp, const std::int32_t* aci, const double* av,
+                 const std::int64_t* brp, const std::int32_t* bci, const double* bv, std::vector<std::int64_t>& rp,
+                 std::vector<std::int32_t>& ci, std::vector<double>& a, std::vector<double>& b) {
+  rp.assign(n + 1, 0);
+  ci.clear();
+  a.clear();
+  b.clear();
+  std::vector<std::pair<std::int32_t, std::pair<double, double>>> row;
+  for (std::int64_t i = 0; i < n; ++i) {
+    row.clear();
+    row.push_back({static_cast<std::int32_t>(i), {0.0, 0.0}});
+    for (std::int64_t p = arp[i]; p < arp[i + 1]; ++p) {
+      HSG_REQUIRE(aci[p] >= i && aci[p] < n, HSG_INVALID_INPUT, "A: entry (" << i << ", " << aci[p] << ") outside the upper triangle");
+      HSG_REQUIRE(std::isfinite(av[p]), HSG_INVALID_INPUT, "A: non-finite entry");
+      row.push_back({aci[p], {av[p], 0.0}});
+    }
+    if (brp) {
+      for (std::int64_t p = brp[i]; p < brp[i + 1]; ++p) {
+        HSG_REQUIRE(bci[p] >= i && bci[p] < n, HSG_INVALID_INPUT, "B: entry (" << i << ", " << bci[p] << ") outside the upper triangle");
+        HSG_REQUIRE(std::isfinite(bv[p]), HSG_INVALID_INPUT, "B: non-finite entry");
+        row.push_back({bci[p], {0.0, bv[p]}});
+      }
+    } else {
+      row.push_back({static_cast<std::int32_t>(i), {0.0, 1.0}});
+    }
+    std::sort(row.begin(), row.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+    for (std::size_t q = 0; q < row.size();) {
+      std::size_t e = q;
+      double sa = 0.0, sb = 0.0;
+      while (e < row.size() && row[e].first == row[q].first) { sa += row[e].second.first; sb += row[e].second.second; ++e; }
+      ci.push_back(row[q].first);
+      a.push_back(sa);
+      b.push_back(sb);
+      q = e;
+    }
+    rp[i + 1] = static_cast<std::int64_t>(ci.size());
+  }
+}
+
+}  // namespace
+
+GpuFactor::GpuFactor(const hsg_options_t& opt) : opt_(opt) {
+  int count = 0;
+  cuda_check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+  HSG_REQUIRE(opt_.device >= 0 && opt_.device < count, HSG_INVALID_INPUT, "no CUDA device " << opt_.device);
+  HSG_REQUIRE(opt_.precision == 0, HSG_UNSUPPORTED, "only double-precision factors are built into this handle type");
+  HSG_REQUIRE(opt_.pivot_threshold > 0.0 && opt_.pivot_threshold <= 0.5, HSG_INVALID_INPUT, "pivot threshold outside (0, 0.5]");
+  HSG_REQUIRE(opt_.null_pivot_tol > 0.0 && opt_.null_pivot_tol < 1.0, HSG_INVALID_INPUT, "null_pivot_tol outside (0, 1)");
+  DeviceGuard g(opt_.device);
+  cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+}
+
+GpuFactor::~GpuFactor() {
+  DeviceGuard g(opt_.device);
+  if (stream_) {
+    cudaStreamSynchronize(stream_);
+    cudaStreamDestroy(stream_);
+  }
+}
+
+void GpuFactor::analyze(std::int64_t n, const std::int64_t* a_rp, const std::int32_t* a_ci, const double* a_v,
+                        const std::int64_t* b_rp, const std::int32_t* b_ci, const double* b_v,
+                        const std::int32_t* order) {
+  HSG_REQUIRE(n > 0 && a_rp && a_ci && a_v, HSG_INVALID_INPUT, "analyze: empty pencil or null pointer");
+  HSG_REQUIRE(n < (std::int64_t(1) << 31) - 1, HSG_UNSUPPORTED, "order above the 32-bit index range");
+  HSG_REQUIRE(!b_rp || (b_ci && b_v), HSG_INVALID_INPUT, "analyze: incomplete B");
+  DeviceGuard g(opt_.device);
+  analysed_ = false;
+  factored_ = false;
+  std::vector<double> av, bv;
+  merge_upper(n, a_rp, a_ci, a_v, b_rp, b_ci, b_v, rp_, ci_, av, bv);
+  n_ = n;
+  nnz_ = rp_[n];
+  std::vector<std::int32_t> perm;
+  if (order) {
+    perm.assign(n, -1);
+    for (std::int64_t v = 0; v < n; ++v) {
+      const std::int64_t p = static_cast<std::int64_t>(order[v]) - 1;
+      HSG_REQUIRE(p >= 0 && p < n && perm[p] < 0, HSG_INVALID_INPUT, "pivot order is not a permutation of 1..n");
+      perm[p] = static_cast<std::int32_t>(v);
+    }
+  }
+  SymbolicOptions so;
+  so.ordering.seed = opt_.ordering_seed;
+  sym_ = analyze_pattern(n, rp_.data(), ci_.data(), order ? perm.data() : nullptr, so);
+  row_.resize(nnz_);
+  for (std::int64_t i = 0; i < n; ++i)
+    for (std::int64_t p = rp_[i]; p < rp_[i + 1]; ++p) row_[p] = static_cast<std::int32_t>(i);
+  d_row_.upload(row_, stream_);
+  d_col_.upload(ci_, stream_);
+  d_a_.upload(av, stream_);
+  d_b_.upload(bv, stream_);
+  d_scale_.alloc(n);
+  d_r_.alloc(n);
+  d_cnt_.alloc(1);
+  d_failed_.alloc(static_cast<std::size_t>(n));
+  d_piv_.alloc(n);
+  d_pidx_.alloc(n);
+  build_plan();
+  cuda_check(cudaStreamSynchronize(stream_), "analyze");
+  inertia_ = hsg_inertia_t{-1, -1, -1, 0, 0, 0, 0, 0};
+  analysed_ = true;
+}
+
+void GpuFactor::build_plan() {
+  const Symbolic& S = sym_;
+  const std::int32_t ns = S.ns;
+  std::vector<SnDev> sn(ns);
+  std::int64_t vec = 0;
+  for (std::int32_t s = 0; s < ns; ++s) {
+    SnDev& d = sn[s];
+    d.first = S.first[s];
+    d.k = S.k_of(s);
+    d.m = S.m_of(s);
+    d.parent = S.parent[s];
+    d.panel_off = S.panel_off[s];
+    d.cb_off = d.m > d.k ? S.cb_off[s] : -1;
+    d.rows_off = S.rowptr[s];
+    d.rmap_off = S.rmap_off[s];
+    d.vec_off = vec;
+    vec += d.m - d.k;
+    d.scratch_off = 0;
+  }
+  vec_total_ = vec;
+  std::vector<std::int32_t> lists;
+  std::vector<int2> items;
+  levels_.assign(S.nlevels, LevelPlan{});
+  std::int64_t scratch_max = 0;
+  for (std::int32_t l = 0; l < S.nlevels; ++l) {
+    LevelPlan& L = levels_[l];
+    std::vector<std::int32_t> zero, s32, s64, app, all;
+    std::int64_t maxcb = 0, scratch = 0;
+    int maxm = 0;
+    for (std::int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+      const std::int32_t s = S.level_sn[q];
+      const int m = sn[s].m, k = sn[s].k;
+      all.push_back(s);
+      maxm = std::max(maxm, m);
+      if (m > k) { zero.push_back(s); maxcb = std::max<std::int64_t>(maxcb, static_cast<std::int64_t>(m - k) * (m - k)); }
+      if (m <= 32) s32.push_back(s);
+      else if (m <= kSmallMax) s64.push_back(s);
+      else {
+        app.push_back(s);
+        sn[s].scratch_off = scratch;
+        scratch += static_cast<std::int64_t>(m) * kNB;
+      }
+    }
+    scratch_max = std::max(scratch_max, scratch);
+    auto put = [&](const std::vector<std::int32_t>& v, std::int64_t& off, int& cnt) {
+      off = static_cast<std::int64_t>(lists.size());
+      cnt = static_cast<int>(v.size());
+      lists.insert(lists.end(), v.begin(), v.end());
+    };
+    put(zero, L.zero_off, L.zero_n);
+    put(s32, L.s32_off, L.s32_n);
+    put(s64, L.s64_off, L.s64_n);
+    put(app, L.app_off, L.app_n);
+    put(all, L.all_off, L.all_n);
+    L.maxm = maxm;
+    L.zero_chunks = static_cast<int>(std::max<std::int64_t>(1, std::min<std::int64_t>(64, (maxcb + 4095) / 4096)));
+    // extend-add items by child rank
+    int maxrank = 0;
+    for (std::int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+      const std::int32_t s = S.level_sn[q];
+      maxrank = std::max(maxrank, S.child_ptr[s + 1] - S.child_ptr[s]);
+    }
+    for (int r = 0; r < maxrank; ++r) {
+      const std::int64_t off = static_cast<std::int64_t>(items.size());
+      for (std::int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+        const std::int32_t s = S.level_sn[q];
+        if (S.child_ptr[s] + r >= S.child_ptr[s + 1]) continue;
+        const std::int32_t c = S.children[S.child_ptr[s] + r];
+        const int mc = sn[c].m - sn[c].k;
+        for (int b0 = 0; b0 < mc; b0 += kExtendAddCols) items.push_back(make_int2(c, b0));
+      }
+      const int cnt = static_cast<int>(items.size() - off);
+      if (cnt) L.ea.push_back({off, cnt});
+    }
+  }
+  std::vector<std::int32_t> rows(S.rows.begin(), S.rows.end());
+  d_sn_.upload(sn, stream_);
+  d_lists_.upload(lists, stream_);
+  d_items_.upload(items, stream_);
+  d_rmap_.upload(S.rmap, stream_);
+  d_rows_.upload(rows, stream_);
+  d_child_ptr_.upload(S.child_ptr, stream_);
+  d_children_.upload(S.children, stream_);
+  d_iperm_.upload(S.iperm, stream_);
+  d_dest_.upload(S.dest, stream_);
+  d_panels_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, S.factor_entries)));
+  d_cb_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, S.cb_arena)));
+  d_scratch_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, scratch_max)));
+}
+
+void GpuFactor::run_numeric(double alpha, double beta, bool detection) {
+  cudaStream_t s = stream_;
+  cuda_check(cudaMemsetAsync(d_cnt_.p, 0, sizeof(FactorCounters), s), "memset counters");
+  launch_fill(d_scale_.p, n_, 1.0, s);
+  if (opt_.scaling) {
+    cuda_check(cudaMemsetAsync(d_r_.p, 0, n_ * sizeof(unsigned long long), s), "memset r");
+    for (int it = 0; it < 10; ++it) {
+      launch_scale_rowmax(nnz_, d_row_.p, d_col_.p, d_a_.p, d_b_.p, alpha, beta, d_scale_.p, d_r_.p, s);
+      launch_scale_update(n_, d_scale_.p, d_r_.p, s);
+    }
+  }
+  cuda_check(cudaMemsetAsync(d_panels_.p, 0, sym_.factor_entries * sizeof(double), s), "memset panels");
+  launch_scatter(nnz_, d_row_.p, d_col_.p, d_a_.p, d_b_.p, alpha, beta, d_scale_.p, d_dest_.p, d_panels_.p, d_cnt_.p, s);
+  FactorParams prm;
+  prm.u = opt_.pivot_threshold;
+  prm.null_tol = detection ? opt_.null_pivot_tol : 0.0;
+  prm.cnt = d_cnt_.p;
+  prm.failed_cap = static_cast<std::int32_t>(n_);
+  const std::int32_t* lists = d_lists_.p;
+  for (const LevelPlan& L : levels_) {
+    launch_zero_cb(lists + L.zero_off, L.zero_n, L.zero_chunks, d_sn_.p, d_cb_.p, s);
+    for (const auto& ea : L.ea) launch_extend_add(d_items_.p + ea.first, ea.second, d_sn_.p, d_rmap_.p, d_panels_.p, d_cb_.p, s);
+    launch_front_small(32, lists + L.s32_off, L.s32_n, d_sn_.p, d_panels_.p, d_cb_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
+    launch_front_small(kSmallMax, lists + L.s64_off, L.s64_n, d_sn_.p, d_panels_.p, d_cb_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
+    launch_front_app(lists + L.app_off, L.app_n, d_sn_.p, d_panels_.p, d_cb_.p, d_scratch_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
+  }
+  cuda_check(cudaGetLastError(), "factorization launch");
+}
+
+hsg_inertia_t GpuFactor::factorize(double alpha, double beta, bool detection) {
+  HSG_REQUIRE(analysed_, HSG_INTERNAL, "factorize before analyze");
+  HSG_REQUIRE(std::isfinite(alpha) && std::isfinite(beta), HSG_INVALID_INPUT, "non-finite alpha / beta");
+  DeviceGuard g(opt_.device);
+  factored_ = false;
+  const auto t0 = std::chrono::steady_clock::now();
+  FactorCounters c{};
+  int replans = 0;
+  std::int64_t delayed = 0;
+  for (;;) {
+    run_numeric(alpha, beta, detection);
+    cuda_check(cudaMemcpyAsync(&c, d_cnt_.p, sizeof(c), cudaMemcpyDeviceToHost, stream_), "counters");
+    cuda_check(cudaStreamSynchronize(stream_), "factorization");
+    if (c.failed == 0) break;
+    HSG_REQUIRE(replans < 16, HSG_FACTORIZATION_FAILED, "delayed pivots could not be placed after " << replans << " re-plans");
+    const std::int64_t nf = std::min<std::int64_t>(static_cast<std::int64_t>(c.failed), n_);
+    std::vector<std::int32_t> failed(nf);
+    cuda_check(cudaMemcpy(failed.data(), d_failed_.p, nf * sizeof(std::int32_t), cudaMemcpyDeviceToHost), "failed list");
+    const std::int64_t moved = move_delayed(sym_, rp_.data(), ci_.data(), failed);
+    HSG_REQUIRE(moved > 0, HSG_FACTORIZATION_FAILED, "pivots failed in root fronts");
+    delayed += moved;
+    ++replans;
+    build_plan();
+  }
+  inertia_.neg = static_cast<std::int64_t>(c.neg);
+  inertia_.zero = static_cast<std::int64_t>(c.zero);
+  inertia_.pos = n_ - inertia_.neg - inertia_.zero;
+  inertia_.null_pivots = static_cast<std::int64_t>(c.zero);
+  inertia_.two_by_two = static_cast<std::int64_t>(c.two_by_two);
+  inertia_.delayed_pivots = sym_.delayed_moves;
+  inertia_.replans = replans;
+  inertia_.valid = c.zero == 0 ? 1 : 0;
+  factored_ = inertia_.valid != 0;
+  last_factor_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  (void)delayed;
+  return inertia_;
+}
+
+void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_device) {
+  HSG_REQUIRE(factored_, HSG_INTERNAL, "solve without a valid factorization");
+  HSG_REQUIRE(nrhs >= 0 && ldb >= n_, HSG_INVALID_INPUT, "solve: nrhs < 0 or ldb < n");
+  if (nrhs == 0) return;
+  HSG_REQUIRE(b, HSG_INVALID_INPUT, "solve: null right-hand side");
+  DeviceGuard g(opt_.device);
+  const auto t0 = std::chrono::steady_clock::now();
+  cudaStream_t s = stream_;
+  const int nr = static_cast<int>(nrhs);
+  d_xwork_.alloc(static_cast<std::size_t>(n_) * nr);
+  d_vec_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, vec_total_)) * nr);
+  double* db = b;
+  std::int64_t ld = ldb;
+  if (!on_device) {
+    d_btmp_.alloc(static_cast<std::size_t>(n_) * nr);
+    cuda_check(cudaMemcpy2DAsync(d_btmp_.p, n_ * sizeof(double), b, ldb * sizeof(double), n_ * sizeof(double), nr,
+                                 cudaMemcpyHostToDevice, s), "H2D rhs");
+    db = d_btmp_.p;
+    ld = n_;
+  }
+  launch_gather_scale(n_, nr, db, ld, d_scale_.p, d_iperm_.p, d_xwork_.p, s);
+  const std::int32_t* lists = d_lists_.p;
+  for (const LevelPlan& L : levels_)
+    launch_solve_fwd(lists + L.all_off, L.all_n, L.maxm, d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p,
+                     d_panels_.p, d_piv_.p, d_pidx_.p, d_xwork_.p, n_, d_vec_.p, nr, s);
+  launch_solve_diag(sym_.ns, d_sn_.p, d_panels_.p, d_piv_.p, d_pidx_.p, d_xwork_.p, n_, nr, s);
+  for (auto it = levels_.rbegin(); it != levels_.rend(); ++it)
+    launch_solve_bwd(lists + it->all_off, it->all_n, it->maxm, d_sn_.p, d_rows_.p, d_panels_.p, d_piv_.p, d_pidx_.p,
+                     d_xwork_.p, n_, nr, s);
+  launch_scatter_scale(n_, nr, db, ld, d_scale_.p, d_iperm_.p, d_xwork_.p, s);
+  cuda_check(cudaGetLastError(), "solve launch");
+  if (!on_device) {
+    cuda_check(cudaMemcpy2DAsync(b, ldb * sizeof(double), d_btmp_.p, n_ * sizeof(double), n_ * sizeof(double), nr,
+                                 cudaMemcpyDeviceToHost, s), "D2H rhs");
+  }
+  cuda_check(cudaStreamSynchronize(s), "solve");
+  last_solve_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void GpuFactor::release() {
+  factored_ = false;
+  inertia_.valid = 0;
+}
+
+hsg_estimate_t GpuFactor::estimate() const {
+  HSG_REQUIRE(analysed_, HSG_INTERNAL, "estimate before analyze");
+  hsg_estimate_t e{};
+  e.factor_entries = sym_.factor_entries;
+  e.nnz_l = sym_.nnz_l;
+  e.flops = sym_.flops;
+  e.device_mb = 8.0 * static_cast<double>(sym_.factor_entries + sym_.cb_arena + 4 * nnz_ + 4 * n_) / 1e6;
+  e.supernodes = sym_.ns;
+  e.levels = sym_.nlevels;
+  e.max_front = sym_.max_front;
+  e.ordering_s = sym_.ordering_seconds;
+  e.analyze_s = sym_.ordering_seconds + sym_.symbolic_seconds;
+  return e;
+}
+
+void GpuFactor::pivot_order(std::int32_t* out) const {
+  HSG_REQUIRE(analysed_, HSG_INTERNAL, "pivot_order before analyze");
+  for (std::int64_t p = 0; p < n_; ++p) out[sym_.perm[p]] = static_cast<std::int32_t>(p + 1);
+}
+
+}  // namespace hsg

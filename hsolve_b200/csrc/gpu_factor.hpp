@@ -1,0 +1,111 @@
+// GPU sparse LDL^T object behind the C ABI: the B200 replacement of hsolve's MumpsFactorization
+// (src/factor/mumps_factorization.{hpp,cpp}; contract hs::SparseFactorization<T>,
+// include/hsolve/factor.hpp:341-443).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "common.hpp"
+#include "device.cuh"
+#include "hsg.h"
+#include "symbolic.hpp"
+
+namespace hsg {
+
+void cuda_check(cudaError_t e, const char* what);
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  std::size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(std::size_t count) {
+    if (count <= n && p) return;
+    release();
+    if (count == 0) return;
+    const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      HSG_THROW(HSG_OUT_OF_MEMORY_BUDGET, "cudaMalloc of " << count * sizeof(T) << " bytes failed: " << cudaGetErrorString(e));
+    }
+    n = count;
+  }
+  void upload(const std::vector<T>& h, cudaStream_t s) {
+    alloc(h.size());
+    if (!h.empty()) cuda_check(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
+  }
+};
+
+class GpuFactor {
+ public:
+  explicit GpuFactor(const hsg_options_t& opt);
+  ~GpuFactor();
+
+  void analyze(std::int64_t n, const std::int64_t* a_rp, const std::int32_t* a_ci, const double* a_v,
+               const std::int64_t* b_rp, const std::int32_t* b_ci, const double* b_v, const std::int32_t* order);
+  hsg_inertia_t factorize(double alpha, double beta, bool detection);
+  void solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_device);
+  void release();
+  hsg_estimate_t estimate() const;
+  const hsg_inertia_t& inertia() const { return inertia_; }
+  std::int64_t order() const { return n_; }
+  void pivot_order(std::int32_t* out) const;
+  void set_detection(bool on) { detection_ = on; }
+  bool detection() const { return detection_; }
+  bool analysed() const { return analysed_; }
+  cudaStream_t stream() const { return stream_; }
+  int device() const { return opt_.device; }
+  // Device copies of the pencil (upper CSR of the union pattern), for SpMV users.
+  const Symbolic& symbolic() const { return sym_; }
+  double last_factor_seconds() const { return last_factor_s_; }
+  double last_solve_seconds() const { return last_solve_s_; }
+
+ private:
+  struct LevelPlan {
+    std::int64_t zero_off = 0; int zero_n = 0; int zero_chunks = 1;
+    std::int64_t s32_off = 0; int s32_n = 0;
+    std::int64_t s64_off = 0; int s64_n = 0;
+    std::int64_t app_off = 0; int app_n = 0;
+    std::int64_t all_off = 0; int all_n = 0; int maxm = 0;
+    std::vector<std::pair<std::int64_t, int>> ea;  // (offset into items, count) per child rank
+  };
+  void build_plan();
+  void run_numeric(double alpha, double beta, bool detection);
+
+  hsg_options_t opt_;
+  cudaStream_t stream_ = nullptr;
+  bool analysed_ = false;
+  bool factored_ = false;
+  bool detection_ = true;
+  std::int64_t n_ = 0, nnz_ = 0;
+  std::vector<std::int64_t> rp_;
+  std::vector<std::int32_t> ci_, row_;
+  Symbolic sym_;
+  std::vector<LevelPlan> levels_;
+  hsg_inertia_t inertia_{};
+  double last_factor_s_ = 0.0, last_solve_s_ = 0.0;
+  std::int64_t vec_total_ = 0;
+
+  DevBuf<std::int32_t> d_row_, d_col_, d_rmap_, d_rows_, d_child_ptr_, d_children_, d_iperm_, d_lists_, d_pidx_,
+      d_failed_;
+  DevBuf<double> d_a_, d_b_, d_scale_, d_panels_, d_cb_, d_scratch_, d_vec_, d_xwork_, d_btmp_;
+  DevBuf<std::int64_t> d_dest_;
+  DevBuf<unsigned long long> d_r_;
+  DevBuf<SnDev> d_sn_;
+  DevBuf<int2> d_items_;
+  DevBuf<signed char> d_piv_;
+  DevBuf<FactorCounters> d_cnt_;
+};
+
+}  // namespace hsg

@@ -1,0 +1,30 @@
+// Launchers of the solve kernels (solve_kernels.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace hsg {
+
+constexpr std::size_t kSolveSmemMax = 200 * 1024;  // dynamic shared memory of a solve CTA
+
+// right-hand sides carried together by one solve CTA of fronts up to maxm rows
+int solve_rhs_chunk(int maxm, int nrhs);
+
+void launch_gather_scale(std::int64_t n, int nrhs, const double* b, std::int64_t ldb, const double* d,
+                         const std::int32_t* iperm, double* x, cudaStream_t s);
+void launch_scatter_scale(std::int64_t n, int nrhs, double* b, std::int64_t ldb, const double* d,
+                          const std::int32_t* iperm, const double* x, cudaStream_t s);
+void launch_solve_fwd(const std::int32_t* list, int nlist, int maxm, const SnDev* sn, const std::int32_t* child_ptr,
+                      const std::int32_t* children, const std::int32_t* rmap, const double* panels,
+                      const signed char* piv, const std::int32_t* pidx, double* x, std::int64_t n, double* vec,
+                      int nrhs, cudaStream_t s);
+void launch_solve_diag(int ns, const SnDev* sn, const double* panels, const signed char* piv,
+                       const std::int32_t* pidx, double* x, std::int64_t n, int nrhs, cudaStream_t s);
+void launch_solve_bwd(const std::int32_t* list, int nlist, int maxm, const SnDev* sn, const std::int32_t* rows,
+                      const double* panels, const signed char* piv, const std::int32_t* pidx, double* x,
+                      std::int64_t n, int nrhs, cudaStream_t s);
+
+}  // namespace hsg

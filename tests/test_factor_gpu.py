@@ -1,0 +1,147 @@
+"""GPU parity of the sparse LDL^T through the C ABI (hsolve tests/cpp/test_factor.cpp semantics):
+exact Sylvester counts at mid-gap shifts, counts equal to the CPU oracle's and to dense counts,
+singular shifts flagged, multi-RHS solves backward stable (<= 1e-12)."""
+import numpy as np
+import pytest
+import scipy.linalg as sla
+import scipy.sparse as sp
+
+from hsolve_b200 import Factorization
+from hsolve_b200.gen import yee
+from oracle import yee_exact
+from oracle.ldlt import OracleLDLT
+from tests.helpers import laplacian_1d, laplacian_2d, random_spd, random_symmetric, saddle_point
+
+pytestmark = pytest.mark.gpu
+
+
+def backward_error(k, x, b):
+    kn = abs(k).sum(axis=0).max()  # ||K||_1 >= ||K||_2
+    r = k @ x - b
+    return max(np.linalg.norm(r[:, j]) / (kn * np.linalg.norm(x[:, j])) for j in range(x.shape[1]))
+
+
+def test_laplacian_1d_exact_inertia():
+    n = 600
+    a = laplacian_1d(n)
+    w = yee_exact.laplacian_1d_spectrum(n)
+    f = Factorization()
+    f.analyze(a, None, 1.0, -2.0)
+    for s in yee_exact.mid_gap_shifts(w, 9, 1e-9):
+        assert f.factorize(1.0, -s), s
+        inr = f.inertia()
+        assert inr.valid and inr.neg == yee_exact.count_below(w, s) and inr.zero == 0 and inr.pos == n - inr.neg
+
+
+def test_laplacian_2d_exact_inertia_and_solve():
+    nx, ny = 60, 45
+    a = laplacian_2d(nx, ny)
+    n = a.shape[0]
+    w = yee_exact.laplacian_2d_spectrum(nx, ny)
+    f = Factorization()
+    f.analyze(a, None, 1.0, -4.0)
+    rng = np.random.default_rng(0)
+    for s in yee_exact.mid_gap_shifts(w, 12, 1e-7):
+        assert f.factorize(1.0, -s)
+        inr = f.inertia()
+        assert inr.neg == yee_exact.count_below(w, s) and inr.zero == 0
+        b = rng.standard_normal((n, 4))
+        x = f.solve(b)
+        assert backward_error(a - s * sp.identity(n), x, b) < 1e-12
+
+
+@pytest.mark.parametrize("cells", [(8, 7, 6), (12, 12, 12)])
+def test_yee_exact_inertia_matches_oracle(cells):
+    box = yee.Box(cells)
+    a, _ = yee.pencil(box)
+    n = a.shape[0]
+    w = yee_exact.exact_spectrum(cells)
+    f = Factorization()
+    f.analyze(a, None, 1.0, -25.0)
+    o = OracleLDLT(a)
+    rng = np.random.default_rng(3)
+    shifts = yee_exact.mid_gap_shifts(w[w > 1.0], 8, 1e-6) + [25.0, -3.0]
+    for s in shifts:
+        assert f.factorize(1.0, -s), s
+        inr = f.inertia()
+        k = (a - s * sp.identity(n)).tocsr()
+        ok, (oneg, ozero, opos), _ = o.factorize(k)
+        assert ok
+        assert inr.neg == yee_exact.count_below(w, s) == oneg, (s, inr)
+        assert inr.zero == ozero == 0
+        b = rng.standard_normal((n, 3))
+        assert backward_error(k, f.solve(b), b) < 1e-12
+
+
+def test_generalized_yee_box():
+    box = yee.Box((7, 6, 5), (1.0, 0.7, 0.45))
+    a, b = yee.pencil(box, "generalized")
+    w = yee_exact.exact_spectrum(box.cells, box.lengths)
+    f = Factorization()
+    f.analyze(a, b, 1.0, -30.0)
+    for s in yee_exact.mid_gap_shifts(w[w > 1.0], 6, 1e-6):
+        assert f.factorize(1.0, -s)
+        assert f.inertia().neg == yee_exact.count_below(w, s)
+
+
+def test_random_pencils_dense_counts():
+    for seed in range(3):
+        a = random_symmetric(300, 0.03, seed)
+        b = random_spd(300, 0.02, seed + 100)
+        w = sla.eigh(a.toarray(), b.toarray(), eigvals_only=True)
+        f = Factorization()
+        f.analyze(a, b, 1.0, 0.0)
+        for s in yee_exact.mid_gap_shifts(w, 8, 1e-6):
+            assert f.factorize(1.0, -s)
+            assert f.inertia().neg == yee_exact.count_below(w, s), (seed, s)
+        # B definiteness test as the driver does it: inertia of 0*A + 1*B
+        inr = f.count(0.0, 1.0)
+        assert inr.valid and inr.neg == 0 and inr.zero == 0 and inr.pos == 300
+
+
+def test_saddle_point_needs_pivoting():
+    k = saddle_point(400, 150, 5)
+    n = k.shape[0]
+    w = np.linalg.eigvalsh(k.toarray())
+    order = np.empty(n, dtype=np.int32)
+    # multipliers first (1-based pivot positions): forces 2x2 pivots / delays
+    seq = np.concatenate((np.arange(400, n), np.arange(400)))
+    order[seq] = np.arange(1, n + 1)
+    f = Factorization()
+    f.analyze(k, None, 1.0, 0.0, pivot_order=order)
+    assert f.factorize(1.0, 0.0)
+    inr = f.inertia()
+    assert inr.neg == int((w < 0).sum()) and inr.pos == int((w > 0).sum())
+    assert inr.two_by_two + inr.delayed_pivots > 0
+    b = np.random.default_rng(2).standard_normal((n, 2))
+    assert backward_error(k, f.solve(b), b) < 1e-12
+
+
+def test_singular_shift_flagged(golden):
+    z = np.load(golden / "near_singular.npz")
+    a = sp.csr_matrix((z["data"], z["indices"], z["indptr"]))
+    w = z["eigenvalues"]
+    import json
+    sigma = json.loads((golden / "examples.json").read_text())["near-singular-shift"]["config"]["target"]["sigma"]
+    f = Factorization()
+    f.analyze(a, None, 1.0, -sigma)
+    assert not f.factorize(1.0, -sigma)
+    inr = f.inertia()
+    assert not inr.valid and inr.null_pivots >= 1
+    with pytest.raises(Exception):
+        f.solve(np.ones(a.shape[0]))
+    s = yee_exact.mid_gap_shifts(w, 3, 1e-6)[1]
+    assert f.factorize(1.0, -s)
+    assert f.inertia().neg == yee_exact.count_below(w, s)
+
+
+def test_count_releases_factors():
+    a = laplacian_2d(30, 20)
+    f = Factorization()
+    f.analyze(a, None, 1.0, -1.0)
+    inr = f.count(1.0, -1.0)
+    assert inr.valid
+    with pytest.raises(Exception):
+        f.solve(np.ones(a.shape[0]))
+    assert f.factorize(1.0, -1.0)
+    f.solve(np.ones(a.shape[0]))
