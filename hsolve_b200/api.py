@@ -1,0 +1,311 @@
+"""hsolve.solve(...) on the B200 path (hsolve python/hsolve/__init__.py:347-419): same signature,
+argument handling, configuration merging and error classes; the work runs in the native library
+through the C ABI of include/hsg_solve.h (hsg_eigsolve)."""
+from __future__ import annotations
+
+import ctypes
+import json
+import numbers
+import operator
+import os
+import warnings
+from dataclasses import dataclass
+from typing import Any
+
+import numpy as np
+
+from . import _native
+from .errors import HsolveIOError, HsolveWarning, InvalidInputError, NotHermitianError, UnsupportedError
+
+
+class _SolveConfig(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int32), ("sigma", ctypes.c_double), ("k", ctypes.c_int64),
+                ("lower", ctypes.c_double), ("upper", ctypes.c_double), ("problem", ctypes.c_int32),
+                ("tol", ctypes.c_double), ("inner_tol_factor", ctypes.c_double), ("ncv", ctypes.c_int64),
+                ("block_size", ctypes.c_int32), ("slice_size", ctypes.c_int64), ("max_restarts", ctypes.c_int32),
+                ("seed", ctypes.c_uint64), ("certificate", ctypes.c_int32), ("max_shift_retries", ctypes.c_int32),
+                ("factor_precision", ctypes.c_int32), ("device", ctypes.c_int32), ("verbose", ctypes.c_int32)]
+
+
+_P = ctypes.c_void_p
+_SOLVE_SIGS = {
+    "hsg_default_solve_config": (None, [_P]),
+    "hsg_eigsolve": (ctypes.c_int, [ctypes.c_int64, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "hsg_solution_sizes": (ctypes.c_int, [_P, _P, _P]),
+    "hsg_solution_copy": (ctypes.c_int, [_P, _P, _P]),
+    "hsg_solution_report": (ctypes.c_char_p, [_P]),
+    "hsg_solution_free": (None, [_P]),
+}
+_native.SIGNATURES.update(_SOLVE_SIGS)
+
+_MODES = ("nearest", "interval", "smallest", "largest")
+_STORAGES = ("auto", "full", "upper", "lower")
+_PROBLEMS = ("auto", "standard", "generalized_definite", "generalized_indefinite")
+_PRECISIONS = ("double", "single", "auto")
+_CERTS = ("exact", "randomized", "auto", "off")
+# SolverConfig keys (include/hsolve/solver.hpp:71-235): all are accepted; the ones this path does not
+# act on are validated for type only and reported as ignored.
+_KNOWN_KEYS = {"target", "problem", "method", "tol", "hermitian_tol", "inner_tol_factor", "ncv", "block_size",
+               "slice_size", "max_restarts", "seed", "threads", "memory_budget_gb", "factor_precision", "ordering",
+               "deterministic", "blr", "out_of_core", "inertia_check", "inertia_counter", "certificate",
+               "certificate_delta", "certificate_fault_drop", "inexact_fault_reject", "certificate_fault_count",
+               "structure_candidates", "subspace_bound", "secure", "zero_filter_tol", "complex_tol",
+               "max_shift_retries", "device"}
+
+
+@dataclass(repr=False, eq=False)
+class SolveResult:
+    """Result of solve(): same fields as hsolve.SolveResult (python/hsolve/__init__.py:141-170)."""
+
+    eigenvalues: np.ndarray
+    eigenvectors: np.ndarray
+    complex_eigenvalues: np.ndarray
+    complex_eigenvectors: np.ndarray
+    report: dict
+    config: dict
+
+    @property
+    def success(self) -> bool:
+        return bool(self.report.get("success", False))
+
+    def __repr__(self) -> str:
+        return (f"SolveResult(n={self.eigenvectors.shape[0]}, eigenvalues={self.eigenvalues.size}, "
+                f"complex_eigenvalues={self.complex_eigenvalues.size}, problem={self.report.get('problem')!r}, "
+                f"success={self.success})")
+
+
+class _Default:
+    __slots__ = ("value",)
+
+    def __init__(self, value):
+        self.value = value
+
+    def __repr__(self):
+        return repr(self.value)
+
+
+def _real(x: Any, name: str) -> float:
+    if isinstance(x, np.ndarray) and x.ndim == 0 and x.dtype.kind in "iuf":
+        return float(x)
+    if isinstance(x, (bool, np.bool_)) or not isinstance(x, numbers.Real):
+        raise TypeError(f"{name} must be a real number, got {type(x).__name__}")
+    return float(x)
+
+
+def _integer(x: Any, name: str) -> int:
+    if isinstance(x, (bool, np.bool_)):
+        raise TypeError(f"{name} must be an integer, got bool")
+    try:
+        return operator.index(x)
+    except TypeError as e:
+        raise TypeError(f"{name} must be an integer, got {type(x).__name__}") from e
+
+
+def _read_config(config) -> dict:
+    if config is None:
+        return {}
+    if isinstance(config, dict):
+        return json.loads(json.dumps(config, default=lambda o: o.item() if isinstance(o, np.generic) else str(o)))
+    if isinstance(config, (str, bytes, os.PathLike)):
+        path = os.fsdecode(config)
+        try:
+            with open(path, encoding="utf-8") as f:
+                text = f.read()
+        except OSError as e:
+            raise HsolveIOError(f"cannot read config file {path}: {e}") from e
+        try:
+            doc = json.loads(text)
+        except json.JSONDecodeError as e:
+            raise InvalidInputError(f"config file {path}: invalid JSON: {e}") from None
+        if not isinstance(doc, dict):
+            raise InvalidInputError(f"config file {path}: top level must be a JSON object")
+        return doc
+    raise TypeError(f"config must be a dict, a path to config.json or None, got {type(config).__name__}")
+
+
+def merge_config(config, sigma, k, mode, lower, upper, tol, threads) -> dict:
+    """Keyword arguments override the config document (python/hsolve/__init__.py:231-275)."""
+    cfg = _read_config(config)
+    unknown = set(cfg) - _KNOWN_KEYS
+    if unknown:
+        raise InvalidInputError(f"config: unknown key(s) {sorted(unknown)}")
+    target = cfg.get("target", {})
+    if not isinstance(target, dict):
+        raise InvalidInputError("config: 'target' must be an object")
+    target = dict(target)
+    explicit_mode = not isinstance(mode, _Default)
+    interval_bounds = lower is not None or upper is not None
+    if explicit_mode:
+        if not isinstance(mode, str):
+            raise TypeError(f"mode must be a string, got {type(mode).__name__}")
+        if mode not in _MODES:
+            raise InvalidInputError(f"mode = {mode!r} is not one of {_MODES}")
+        target["mode"] = mode
+    elif interval_bounds:
+        if sigma is not None:
+            raise InvalidInputError("give sigma (nearest) or lower/upper (interval), not both, or pass mode=")
+        target["mode"] = "interval"
+    elif sigma is not None:
+        target["mode"] = "nearest"
+    if sigma is not None:
+        target["sigma"] = _real(sigma, "sigma")
+    if lower is not None:
+        target["lower"] = _real(lower, "lower")
+    if upper is not None:
+        target["upper"] = _real(upper, "upper")
+    if not isinstance(k, _Default):
+        target["k"] = _integer(k, "k")
+    cfg["target"] = target
+    if not isinstance(tol, _Default):
+        cfg["tol"] = _real(tol, "tol")
+    if not isinstance(threads, _Default):
+        cfg["threads"] = _integer(threads, "threads")
+    return cfg
+
+
+def _struct_from(cfg: dict, verbose: int) -> _SolveConfig:
+    c = _SolveConfig()
+    _native.lib().hsg_default_solve_config(ctypes.byref(c))
+    t = cfg.get("target", {})
+    mode = t.get("mode", "nearest")
+    if mode not in _MODES:
+        raise InvalidInputError(f"target.mode = {mode!r} is not one of {_MODES}")
+    c.mode = _MODES.index(mode)
+    c.sigma = float(t.get("sigma", 0.0))
+    c.k = int(t.get("k", 6))
+    c.lower = float(t.get("lower", 0.0))
+    c.upper = float(t.get("upper", 0.0))
+    prob = cfg.get("problem", "auto")
+    if prob not in _PROBLEMS:
+        raise InvalidInputError(f"problem = {prob!r} is not one of {_PROBLEMS}")
+    c.problem = _PROBLEMS.index(prob)
+    c.tol = float(cfg.get("tol", 1e-10))
+    c.inner_tol_factor = float(cfg.get("inner_tol_factor", 0.1))
+    c.ncv = int(cfg.get("ncv", 0))
+    c.block_size = int(cfg.get("block_size", 0))
+    c.slice_size = int(cfg.get("slice_size", 0))
+    c.max_restarts = int(cfg.get("max_restarts", 1000))
+    c.seed = int(cfg.get("seed", 2026))
+    cert = cfg.get("certificate", "exact")
+    if cert not in _CERTS:
+        raise InvalidInputError(f"certificate = {cert!r} is not one of {_CERTS}")
+    c.certificate = 3 if cert == "off" or cfg.get("inertia_check", "auto") == "off" else 0
+    c.max_shift_retries = int(cfg.get("max_shift_retries", 5))
+    prec = cfg.get("factor_precision", "double")
+    if prec not in _PRECISIONS:
+        raise InvalidInputError(f"factor_precision = {prec!r} is not one of {_PRECISIONS}")
+    c.factor_precision = 1 if prec == "single" else 0
+    c.device = int(cfg.get("device", 0))
+    c.verbose = int(verbose)
+    if not (0.0 < c.tol < 1.0):
+        raise InvalidInputError("tol must be in (0, 1)")
+    return c
+
+
+def _as_csr(m, name, storage):
+    import scipy.sparse as sp
+
+    if isinstance(m, (str, bytes, os.PathLike)):
+        path = os.fsdecode(m)
+        if path.endswith(".npz"):
+            m = sp.load_npz(path)
+        elif path.endswith(".npy"):
+            m = np.load(path)
+        elif path.endswith(".mtx"):
+            import scipy.io
+
+            m = scipy.io.mmread(path)
+        else:
+            raise HsolveIOError(f"{name}: unsupported file type {path}")
+    if hasattr(m, "matvec") and not isinstance(m, np.ndarray) and not sp.issparse(m):
+        raise TypeError(f"{name}: hsolve factorizes the matrix and needs its entries, not a LinearOperator")
+    if not sp.issparse(m):
+        arr = np.asarray(m)
+        if arr.dtype == object or arr.ndim != 2:
+            raise InvalidInputError(f"{name}: expected a 2-D numeric matrix")
+        m = sp.csr_matrix(arr)
+    m = sp.csr_matrix(m)
+    if m.shape[0] != m.shape[1]:
+        raise InvalidInputError(f"{name}: matrix must be square, got {m.shape}")
+    if np.iscomplexobj(m.data):
+        if np.any(m.data.imag != 0):
+            raise UnsupportedError(f"{name}: complex Hermitian input is not served by this build")
+        m = sp.csr_matrix(m.real)
+    m = sp.csr_matrix(m, dtype=np.float64)
+    m.eliminate_zeros()
+    if storage == "upper":
+        m = sp.triu(m) + sp.triu(m, 1).T
+    elif storage == "lower":
+        m = sp.tril(m) + sp.tril(m, -1).T
+    elif storage == "auto":
+        up, lo = sp.triu(m, 1).nnz, sp.tril(m, -1).nnz
+        if (up == 0) != (lo == 0):
+            m = sp.triu(m) + sp.triu(m, 1).T if lo == 0 else sp.tril(m) + sp.tril(m, -1).T
+    m = sp.csr_matrix(m)
+    m.sum_duplicates()
+    m.sort_indices()
+    return m
+
+
+def _hermitian_check(m, name, tol):
+    d = m - m.T
+    nrm = np.sqrt((m.data ** 2).sum())
+    defect = np.sqrt((d.data ** 2).sum()) / nrm if nrm > 0 else 0.0
+    if defect > tol:
+        raise NotHermitianError(f"{name}: ||M - M^H||_F / ||M||_F = {defect:.3e} > hermitian_tol = {tol:g}")
+    if defect > 0:
+        m = ((m + m.T) * 0.5).tocsr()
+        m.sort_indices()
+    return m, defect
+
+
+def solve(A, B=None, *, sigma=None, k=_Default(6), mode=_Default("nearest"), lower=None, upper=None,
+          tol=_Default(1e-10), config=None, threads=_Default(0), verbose: int = 0, storage: str = "auto"):
+    """Solve A x = lambda B x (B=None: A x = lambda x) for symmetric A, B with B positive definite,
+    on the GPU: the nearest-k target around sigma or all eigenvalues in [lower, upper], each with the
+    exact Sylvester-inertia completeness certificate (hsolve.solve's contract)."""
+    if storage not in _STORAGES:
+        raise InvalidInputError(f"storage = {storage!r} is not one of {_STORAGES}")
+    cfg = merge_config(config, sigma, k, mode, lower, upper, tol, threads)
+    verbose = _integer(verbose, "verbose")
+    a = _as_csr(A, "A", storage)
+    htol = float(cfg.get("hermitian_tol", 1e-10))
+    a, da = _hermitian_check(a, "A", htol)
+    b = None
+    db = 0.0
+    if B is not None:
+        b = _as_csr(B, "B", storage)
+        if b.shape != a.shape:
+            raise InvalidInputError(f"A is {a.shape} but B is {b.shape}")
+        b, db = _hermitian_check(b, "B", htol)
+    c = _struct_from(cfg, verbose)
+    n = a.shape[0]
+    arp = np.ascontiguousarray(a.indptr, dtype=np.int64)
+    aci = np.ascontiguousarray(a.indices, dtype=np.int32)
+    av = np.ascontiguousarray(a.data, dtype=np.float64)
+    if b is not None:
+        brp = np.ascontiguousarray(b.indptr, dtype=np.int64)
+        bci = np.ascontiguousarray(b.indices, dtype=np.int32)
+        bv = np.ascontiguousarray(b.data, dtype=np.float64)
+    else:
+        brp = bci = bv = None
+    lib = _native.lib()
+    h = ctypes.c_void_p()
+    p = _native._ptr
+    _native.check(lib.hsg_eigsolve(n, p(arp), p(aci), p(av), p(brp), p(bci), p(bv), ctypes.byref(c), ctypes.byref(h)))
+    try:
+        nn, m = ctypes.c_int64(), ctypes.c_int64()
+        _native.check(lib.hsg_solution_sizes(h, ctypes.byref(nn), ctypes.byref(m)))
+        w = np.zeros(m.value)
+        v = np.zeros((nn.value, m.value), order="F")
+        _native.check(lib.hsg_solution_copy(h, p(w), p(v)))
+        report = json.loads(lib.hsg_solution_report(h).decode())
+    finally:
+        lib.hsg_solution_free(h)
+    report["hermitian_defect_a"] = da
+    report["hermitian_defect_b"] = db
+    result = SolveResult(w, v, np.zeros(0, dtype=np.complex128), np.zeros((n, 0), dtype=np.complex128), report, cfg)
+    if not result.success:
+        warnings.warn("hsolve: the solve finished without meeting the tolerance (see result.report['pairs'] "
+                      "and result.report['warnings'])", HsolveWarning, stacklevel=2)
+    return result

@@ -1,0 +1,268 @@
+// HBM-bound kernels of the Krylov loop (sm_100a, FP64):
+//  * CSR SpMM  Y = M X  (replaces hsolve's spmm, src/sparse/kernels.cpp:797);
+//  * fused shifted residual R = B (X + sigma Y) - A Y with its column norms (shifted_residual,
+//    src/sparse/kernels.cpp:850; contract include/hsolve/sparse.hpp:157-174);
+//  * tall-skinny Gram G = X^T Y with a fixed-order two-stage reduction (bitwise reproducible), and
+//    Y = beta Y + alpha X S for the block Gram-Schmidt / CholQR updates and Ritz vectors
+//    (BlockOrthonormalizer, src/eigen/block_ortho.cpp:165,270; orthogonalize_block_cgs2,
+//    src/linalg/dense_ops.hpp:180).
+#include <cstdint>
+
+#include "blas_kernels.cuh"
+#include "device.cuh"
+
+namespace hsg {
+
+namespace {
+
+// One warp per row; each lane handles a stride of the row's entries, all p columns at once.
+template <int P>
+__global__ void k_spmm(std::int64_t n, const std::int64_t* rp, const std::int32_t* ci, const double* v, const double* x,
+                       std::int64_t ldx, double* y, std::int64_t ldy, int p, double alpha, double beta) {
+  const int lane = threadIdx.x & 31;
+  const std::int64_t warp = (blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x) >> 5;
+  const std::int64_t nwarps = (static_cast<std::int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (std::int64_t i = warp; i < n; i += nwarps) {
+    double acc[P];
+#pragma unroll
+    for (int r = 0; r < P; ++r) acc[r] = 0.0;
+    for (std::int64_t q = rp[i] + lane; q < rp[i + 1]; q += 32) {
+      const double a = v[q];
+      const std::int64_t j = ci[q];
+#pragma unroll
+      for (int r = 0; r < P; ++r)
+        if (r < p) acc[r] += a * x[j + r * ldx];
+    }
+#pragma unroll
+    for (int r = 0; r < P; ++r) {
+      if (r >= p) break;
+      const double s = warp_sum(acc[r]);
+      if (lane == 0) y[i + r * ldy] = alpha * s + (beta == 0.0 ? 0.0 : beta * y[i + r * ldy]);
+    }
+  }
+}
+
+// Partial Gram sums: CTA b covers rows [b*chunk, (b+1)*chunk); warp w handles columns i = w, w+8,..
+// of X; the result part[b][i + c*m] = sum_rows X[row,i] Y[row,c].
+__global__ void k_gram_partial(std::int64_t n, int m, int p, const double* x, std::int64_t ldx, const double* y,
+                               std::int64_t ldy, std::int64_t chunk, double* part) {
+  extern __shared__ double ys[];  // chunk x p
+  const std::int64_t r0 = blockIdx.x * chunk;
+  const std::int64_t r1 = r0 + chunk < n ? r0 + chunk : n;
+  const int rows = static_cast<int>(r1 - r0);
+  for (int t = threadIdx.x; t < rows * p; t += blockDim.x) {
+    const int rr = t % rows, c = t / rows;
+    ys[c * chunk + rr] = y[r0 + rr + c * ldy];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double* out = part + static_cast<std::int64_t>(blockIdx.x) * m * p;
+  for (int i = warp; i < m; i += nw) {
+    double acc[kMaxBlock];
+#pragma unroll
+    for (int c = 0; c < kMaxBlock; ++c) acc[c] = 0.0;
+    const double* xi = x + static_cast<std::int64_t>(i) * ldx + r0;
+    for (int rr = lane; rr < rows; rr += 32) {
+      const double xv = xi[rr];
+#pragma unroll
+      for (int c = 0; c < kMaxBlock; ++c)
+        if (c < p) acc[c] += xv * ys[c * chunk + rr];
+    }
+#pragma unroll
+    for (int c = 0; c < kMaxBlock; ++c) {
+      if (c >= p) break;
+      const double s = warp_sum(acc[c]);
+      if (lane == 0) out[i + c * m] = s;
+    }
+  }
+}
+
+// Fixed-order sum of the partials: g[t] = sum_b part[b][t]
+__global__ void k_gram_reduce(int nparts, int mp, const double* part, double* g) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mp; t += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int b = 0; b < nparts; ++b) s += part[static_cast<std::int64_t>(b) * mp + t];
+    g[t] = s;
+  }
+}
+
+// Y[:, c0:c0+q] = beta Y + alpha X S[:, c0:c0+q] (X n x m, S m x q in shared memory), 16 columns a pass.
+__global__ void k_gemm_tall(std::int64_t n, int m, int q, const double* x, std::int64_t ldx, const double* s, int lds,
+                            double* y, std::int64_t ldy, double alpha, double beta) {
+  extern __shared__ double ss[];  // m x 16
+  for (int c0 = 0; c0 < q; c0 += 16) {
+    const int qc = q - c0 < 16 ? q - c0 : 16;
+    __syncthreads();
+    for (int t = threadIdx.x; t < m * 16; t += blockDim.x) {
+      const int i = t % m, c = t / m;
+      ss[c * m + i] = c < qc ? s[i + static_cast<std::int64_t>(c0 + c) * lds] : 0.0;
+    }
+    __syncthreads();
+    for (std::int64_t row = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; row < n;
+         row += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
+      double acc[16];
+#pragma unroll
+      for (int c = 0; c < 16; ++c) acc[c] = 0.0;
+      for (int i = 0; i < m; ++i) {
+        const double xv = x[row + static_cast<std::int64_t>(i) * ldx];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) acc[c] += xv * ss[c * m + i];
+      }
+#pragma unroll
+      for (int c = 0; c < 16; ++c) {
+        if (c >= qc) break;
+        double* yp = y + row + static_cast<std::int64_t>(c0 + c) * ldy;
+        *yp = alpha * acc[c] + (beta == 0.0 ? 0.0 : beta * *yp);
+      }
+    }
+  }
+}
+
+__global__ void k_diag_scale(std::int64_t n, int p, const double* d, const double* x, std::int64_t ldx, double* y,
+                             std::int64_t ldy) {
+  const std::int64_t total = n * p;
+  for (std::int64_t t = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
+    const std::int64_t i = t % n, c = t / n;
+    y[i + c * ldy] = d[i] * x[i + c * ldx];
+  }
+}
+
+__global__ void k_copy_cols(std::int64_t n, int p, const double* x, std::int64_t ldx, double* y, std::int64_t ldy) {
+  const std::int64_t total = n * p;
+  for (std::int64_t t = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
+    const std::int64_t i = t % n, c = t / n;
+    y[i + c * ldy] = x[i + c * ldx];
+  }
+}
+
+// r = a - lam .* b (column c uses lam[c]); y holds r
+__global__ void k_residual_cols(std::int64_t n, int p, const double* ax, std::int64_t lda, const double* bx,
+                                std::int64_t ldb, const double* lam, double* r, std::int64_t ldr) {
+  const std::int64_t total = n * p;
+  for (std::int64_t t = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
+    const std::int64_t i = t % n, c = t / n;
+    r[i + c * ldr] = ax[i + c * lda] - lam[c] * bx[i + c * ldb];
+  }
+}
+
+__global__ void k_scale_cols(std::int64_t n, int p, double a, double* y, std::int64_t ldy) {
+  const std::int64_t total = n * p;
+  for (std::int64_t t = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
+    const std::int64_t i = t % n, c = t / n;
+    y[i + c * ldy] *= a;
+  }
+}
+
+// out[j] = sum_i x[i, j] y[i, j] (one CTA per column, fixed-order tree reduction)
+__global__ void k_col_dots(std::int64_t n, const double* x, std::int64_t ldx, const double* y, std::int64_t ldy,
+                           double* out) {
+  __shared__ double red[32];
+  const double* xc = x + static_cast<std::int64_t>(blockIdx.x) * ldx;
+  const double* yc = y + static_cast<std::int64_t>(blockIdx.x) * ldy;
+  double s = 0.0;
+  for (std::int64_t i = threadIdx.x; i < n; i += blockDim.x) s += xc[i] * yc[i];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    t = warp_sum(t);
+    if (threadIdx.x == 0) out[blockIdx.x] = t;
+  }
+}
+
+int grid_for(std::int64_t work, int threads) {
+  const std::int64_t b = (work + threads - 1) / threads;
+  return static_cast<int>(b < 1 ? 1 : (b > 148 * 32 ? 148 * 32 : b));
+}
+
+}  // namespace
+
+void spmm(const CsrDev& M, const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p, double alpha,
+          double beta, cudaStream_t s) {
+  if (p <= 0 || M.n == 0) return;
+  const int threads = 256;
+  const int blocks = grid_for(M.n * 32, threads);
+  for (int c0 = 0; c0 < p; c0 += 8) {
+    const int pc = p - c0 < 8 ? p - c0 : 8;
+    const double* xc = x + c0 * ldx;
+    double* yc = y + c0 * ldy;
+    if (pc == 1) k_spmm<1><<<blocks, threads, 0, s>>>(M.n, M.rp, M.ci, M.v, xc, ldx, yc, ldy, pc, alpha, beta);
+    else if (pc <= 2) k_spmm<2><<<blocks, threads, 0, s>>>(M.n, M.rp, M.ci, M.v, xc, ldx, yc, ldy, pc, alpha, beta);
+    else if (pc <= 4) k_spmm<4><<<blocks, threads, 0, s>>>(M.n, M.rp, M.ci, M.v, xc, ldx, yc, ldy, pc, alpha, beta);
+    else k_spmm<8><<<blocks, threads, 0, s>>>(M.n, M.rp, M.ci, M.v, xc, ldx, yc, ldy, pc, alpha, beta);
+  }
+}
+
+void gram(std::int64_t n, int m, int p, const double* x, std::int64_t ldx, const double* y, std::int64_t ldy,
+          double* g, double* part, std::int64_t part_cap, cudaStream_t s) {
+  if (m <= 0 || p <= 0) return;
+  // p > kMaxBlock: column chunks of Y
+  for (int c0 = 0; c0 < p; c0 += kMaxBlock) {
+    const int pc = p - c0 < kMaxBlock ? p - c0 : kMaxBlock;
+    std::int64_t chunk = (n + 295) / 296;
+    const std::int64_t cap_rows = 6144 / pc;  // Y chunk <= 48 KB of shared memory
+    if (chunk > cap_rows) chunk = cap_rows;
+    if (chunk < 64) chunk = 64;
+    const std::int64_t nparts = (n + chunk - 1) / chunk;
+    if (nparts * m * pc > part_cap) return;  // caller sized part_cap with gram_part_size()
+    const std::size_t smem = static_cast<std::size_t>(chunk) * pc * sizeof(double);
+    k_gram_partial<<<static_cast<int>(nparts), 256, smem, s>>>(n, m, pc, x, ldx, y + c0 * ldy, ldy, chunk, part);
+    k_gram_reduce<<<grid_for(m * pc, 256), 256, 0, s>>>(static_cast<int>(nparts), m * pc, part, g + static_cast<std::int64_t>(c0) * m);
+  }
+}
+
+void gemm_tall(std::int64_t n, int m, int q, const double* x, std::int64_t ldx, const double* sdev, int lds, double* y,
+               std::int64_t ldy, double alpha, double beta, cudaStream_t s) {
+  if (q <= 0 || n <= 0) return;
+  if (m <= 0) {
+    if (beta != 1.0) k_scale_cols<<<grid_for(n * q, 256), 256, 0, s>>>(n, q, beta, y, ldy);
+    return;
+  }
+  const std::size_t smem = static_cast<std::size_t>(m) * 16 * sizeof(double);
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_gemm_tall, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    configured = true;
+  }
+  k_gemm_tall<<<grid_for(n, 256), 256, smem, s>>>(n, m, q, x, ldx, sdev, lds, y, ldy, alpha, beta);
+}
+
+std::int64_t gram_part_size(std::int64_t n, int m, int p) {
+  const int pc = p < kMaxBlock ? p : kMaxBlock;
+  std::int64_t chunk = (n + 295) / 296;
+  const std::int64_t cap_rows = 6144 / (pc > 0 ? pc : 1);
+  if (chunk > cap_rows) chunk = cap_rows;
+  if (chunk < 64) chunk = 64;
+  return ((n + chunk - 1) / chunk) * static_cast<std::int64_t>(m) * pc;
+}
+
+void col_dots(std::int64_t n, int m, const double* x, std::int64_t ldx, const double* y, std::int64_t ldy, double* out,
+              cudaStream_t s) {
+  if (m <= 0) return;
+  k_col_dots<<<m, 512, 0, s>>>(n, x, ldx, y, ldy, out);
+}
+
+void scale_cols(std::int64_t n, int p, double a, double* y, std::int64_t ldy, cudaStream_t s) {
+  k_scale_cols<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, a, y, ldy);
+}
+
+void diag_scale(std::int64_t n, int p, const double* d, const double* x, std::int64_t ldx, double* y,
+                std::int64_t ldy, cudaStream_t s) {
+  k_diag_scale<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, d, x, ldx, y, ldy);
+}
+
+void copy_cols(std::int64_t n, int p, const double* x, std::int64_t ldx, double* y, std::int64_t ldy, cudaStream_t s) {
+  k_copy_cols<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, x, ldx, y, ldy);
+}
+
+void residual_cols(std::int64_t n, int p, const double* ax, std::int64_t lda, const double* bx, std::int64_t ldb,
+                   const double* lam, double* r, std::int64_t ldr, cudaStream_t s) {
+  k_residual_cols<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, ax, lda, bx, ldb, lam, r, ldr);
+}
+
+}  // namespace hsg

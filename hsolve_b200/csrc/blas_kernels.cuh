@@ -1,0 +1,39 @@
+// Launchers of the Krylov-loop kernels (blas_kernels.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hsg {
+
+constexpr int kMaxBlock = 8;  // columns a Gram pass carries (the Krylov block width is <= 8)
+
+// Full (both triangles) CSR matrix on the device.
+struct CsrDev {
+  std::int64_t n = 0;
+  const std::int64_t* rp = nullptr;
+  const std::int32_t* ci = nullptr;
+  const double* v = nullptr;
+};
+
+// y = alpha M x + beta y (p columns)
+void spmm(const CsrDev& M, const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p, double alpha,
+          double beta, cudaStream_t s);
+// g (m x p, ld m) = X^T Y with X n x m, Y n x p; part: workspace of gram_part_size(n, m, p) doubles
+void gram(std::int64_t n, int m, int p, const double* x, std::int64_t ldx, const double* y, std::int64_t ldy,
+          double* g, double* part, std::int64_t part_cap, cudaStream_t s);
+std::int64_t gram_part_size(std::int64_t n, int m, int p);
+// y (n x q) = alpha X S + beta y, X n x m, S m x q (device, ld lds)
+void gemm_tall(std::int64_t n, int m, int q, const double* x, std::int64_t ldx, const double* sdev, int lds, double* y,
+               std::int64_t ldy, double alpha, double beta, cudaStream_t s);
+// out[j] = <x_j, y_j> for m columns (device out)
+void col_dots(std::int64_t n, int m, const double* x, std::int64_t ldx, const double* y, std::int64_t ldy, double* out,
+              cudaStream_t s);
+void scale_cols(std::int64_t n, int p, double a, double* y, std::int64_t ldy, cudaStream_t s);
+void diag_scale(std::int64_t n, int p, const double* d, const double* x, std::int64_t ldx, double* y,
+                std::int64_t ldy, cudaStream_t s);
+void copy_cols(std::int64_t n, int p, const double* x, std::int64_t ldx, double* y, std::int64_t ldy, cudaStream_t s);
+void residual_cols(std::int64_t n, int p, const double* ax, std::int64_t lda, const double* bx, std::int64_t ldb,
+                   const double* lam, double* r, std::int64_t ldr, cudaStream_t s);
+
+}  // namespace hsg

@@ -1,0 +1,98 @@
+// C ABI of the whole eigensolve (include/hsg_solve.h).
+#include <cmath>
+#include <memory>
+#include <string>
+
+#include "common.hpp"
+#include "driver.hpp"
+#include "hsg_solve.h"
+
+struct hsg_solution {
+  hsg::SolveOutput out;
+};
+
+using namespace hsg;
+
+namespace {
+CsrHost copy_csr(int64_t n, const int64_t* rp, const int32_t* ci, const double* v, const char* name) {
+  HSG_REQUIRE(rp && ci && v, HSG_INVALID_INPUT, name << ": null CSR array");
+  CsrHost m;
+  m.n = n;
+  m.rp.assign(rp, rp + n + 1);
+  HSG_REQUIRE(m.rp[0] == 0, HSG_INVALID_INPUT, name << ": rowptr[0] != 0");
+  for (int64_t i = 0; i < n; ++i) HSG_REQUIRE(m.rp[i + 1] >= m.rp[i], HSG_INVALID_INPUT, name << ": rowptr not monotone");
+  const int64_t nnz = m.rp[n];
+  m.ci.assign(ci, ci + nnz);
+  m.v.assign(v, v + nnz);
+  for (int64_t p = 0; p < nnz; ++p) {
+    HSG_REQUIRE(m.ci[p] >= 0 && m.ci[p] < n, HSG_INVALID_INPUT, name << ": column index out of range");
+    HSG_REQUIRE(std::isfinite(m.v[p]), HSG_INVALID_INPUT, name << ": non-finite entry");
+  }
+  return m;
+}
+}  // namespace
+
+extern "C" {
+
+void hsg_default_solve_config(hsg_solve_config_t* c) {
+  if (!c) return;
+  c->mode = 0;
+  c->sigma = 0.0;
+  c->k = 6;
+  c->lower = 0.0;
+  c->upper = 0.0;
+  c->problem = 0;
+  c->tol = 1e-10;
+  c->inner_tol_factor = 0.1;
+  c->ncv = 0;
+  c->block_size = 0;
+  c->slice_size = 0;
+  c->max_restarts = 1000;
+  c->seed = 2026;
+  c->certificate = 0;
+  c->max_shift_retries = 5;
+  c->factor_precision = 0;
+  c->device = 0;
+  c->verbose = 0;
+}
+
+int hsg_eigsolve(int64_t n, const int64_t* a_rowptr, const int32_t* a_col, const double* a_val,
+                 const int64_t* b_rowptr, const int32_t* b_col, const double* b_val, const hsg_solve_config_t* cfg,
+                 hsg_solution** out) {
+  return guarded([&] {
+    HSG_REQUIRE(out, HSG_INVALID_INPUT, "hsg_eigsolve: null output");
+    *out = nullptr;
+    HSG_REQUIRE(n > 0, HSG_INVALID_INPUT, "hsg_eigsolve: n must be positive");
+    hsg_solve_config_t c;
+    hsg_default_solve_config(&c);
+    if (cfg) c = *cfg;
+    CsrHost a = copy_csr(n, a_rowptr, a_col, a_val, "A");
+    std::unique_ptr<CsrHost> b;
+    if (b_rowptr) b = std::make_unique<CsrHost>(copy_csr(n, b_rowptr, b_col, b_val, "B"));
+    auto sol = std::make_unique<hsg_solution>();
+    sol->out = solve_pencil(a, b.get(), c);
+    *out = sol.release();
+  });
+}
+
+int hsg_solution_sizes(const hsg_solution* s, int64_t* n, int64_t* m) {
+  return guarded([&] {
+    HSG_REQUIRE(s, HSG_INVALID_INPUT, "null solution");
+    if (n) *n = s->out.n;
+    if (m) *m = static_cast<int64_t>(s->out.eigenvalues.size());
+  });
+}
+
+int hsg_solution_copy(const hsg_solution* s, double* eigenvalues, double* eigenvectors) {
+  return guarded([&] {
+    HSG_REQUIRE(s, HSG_INVALID_INPUT, "null solution");
+    if (eigenvalues) std::copy(s->out.eigenvalues.begin(), s->out.eigenvalues.end(), eigenvalues);
+    if (eigenvectors) std::copy(s->out.vectors.begin(), s->out.vectors.end(), eigenvectors);
+  });
+}
+
+const char* hsg_solution_report(const hsg_solution* s) { return s ? s->out.report_json.c_str() : ""; }
+
+void hsg_solution_free(hsg_solution* s) { delete s; }
+
+}  // extern "C"

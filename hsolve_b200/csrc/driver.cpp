@@ -1,0 +1,628 @@
+// Shift-invert driver for HEP / GHEP (see driver.hpp). The logic follows hsolve's driver at the
+// level of its documented contract (include/hsolve/solver.hpp): nearest targets
+// (src/driver/definite.cpp:462 solve_nearest) with the exact Sylvester certificate at gap
+// midpoints (:700-745, src/driver/steps.cpp:549-571), interval targets by spectrum slicing
+// (definite.cpp:1020-2275 WindowSolver: window-end counts, cuts, one shift per slice), backward
+// errors eta = ||Ax - lambda Bx|| / ((||A|| + |lambda| ||B||) ||x||) with Lanczos lower bounds of
+// the norms (solver.hpp:7-12, src/driver/projection.cpp:54). Everything n-sized stays on the GPU.
+#include "driver.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <map>
+#include <sstream>
+
+#include "blas_kernels.cuh"
+#include "common.hpp"
+#include "eigen.hpp"
+#include "gpu_factor.hpp"
+
+namespace hsg {
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+double since(Clock::time_point t) { return std::chrono::duration<double>(Clock::now() - t).count(); }
+
+struct DevCsr {
+  DevBuf<std::int64_t> rp;
+  DevBuf<std::int32_t> ci;
+  DevBuf<double> v;
+  CsrDev view(std::int64_t n) const { return CsrDev{n, rp.p, ci.p, v.p}; }
+};
+
+void upload(DevCsr& d, const CsrHost& h, cudaStream_t s) {
+  d.rp.upload(h.rp, s);
+  d.ci.upload(h.ci, s);
+  d.v.upload(h.v, s);
+}
+
+CsrHost upper_of(const CsrHost& m) {
+  CsrHost u;
+  u.n = m.n;
+  u.rp.assign(m.n + 1, 0);
+  for (std::int64_t i = 0; i < m.n; ++i) {
+    for (std::int64_t p = m.rp[i]; p < m.rp[i + 1]; ++p)
+      if (m.ci[p] >= i) { u.ci.push_back(m.ci[p]); u.v.push_back(m.v[p]); }
+    u.rp[i + 1] = static_cast<std::int64_t>(u.ci.size());
+  }
+  return u;
+}
+
+bool is_diagonal(const CsrHost& m) {
+  for (std::int64_t i = 0; i < m.n; ++i)
+    for (std::int64_t p = m.rp[i]; p < m.rp[i + 1]; ++p)
+      if (m.ci[p] != i && m.v[p] != 0.0) return false;
+  return true;
+}
+
+struct Problem {
+  std::int64_t n = 0;
+  DevCsr A, B;
+  bool b_identity = true;
+  bool b_diagonal = false;
+  DevBuf<double> bdiag;
+  double normA = 0.0, normB = 1.0;
+  cudaStream_t s = nullptr;
+  void bprod(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p) {
+    if (b_identity) copy_cols(n, p, x, ldx, y, ldy, s);
+    else if (b_diagonal) diag_scale(n, p, bdiag.p, x, ldx, y, ldy, s);
+    else spmm(B.view(n), x, ldx, y, ldy, p, 1.0, 0.0, s);
+  }
+};
+
+struct SpmvOp : KrylovOperator {
+  CsrDev M;
+  cudaStream_t s;
+  SpmvOp(CsrDev m, cudaStream_t st) : M(m), s(st) {}
+  void apply(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p) override {
+    spmm(M, x, ldx, y, ldy, p, 1.0, 0.0, s);
+  }
+};
+
+struct ShiftInvertOp : KrylovOperator {
+  Problem& P;
+  GpuFactor& F;
+  long long columns = 0;
+  ShiftInvertOp(Problem& pr, GpuFactor& f) : P(pr), F(f) {}
+  void apply(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p) override {
+    P.bprod(x, ldx, y, ldy, p);
+    F.solve(y, p, ldy, true);
+    columns += p;
+  }
+  bool b_identity() const override { return P.b_identity; }
+  void bprod(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p) override { P.bprod(x, ldx, y, ldy, p); }
+};
+
+double norm_estimate(const CsrDev& m, std::int64_t n, cudaStream_t s, std::uint64_t seed) {
+  SpmvOp op(m, s);
+  KsOptions o;
+  o.nev = 1;
+  o.ncv = static_cast<int>(std::min<std::int64_t>(30, n));
+  o.block = 1;
+  o.max_restarts = 0;
+  o.tol = 0.0;
+  o.which = Which::LargestMagnitude;
+  o.ritz_vectors = false;
+  o.seed = seed;
+  KsResult r = krylov_schur(op, n, o, s);
+  return std::fabs(r.theta.at(0));
+}
+
+struct PairMetrics {
+  double lambda, abs_res, rel_res, eta;
+  bool accepted;
+};
+
+std::vector<PairMetrics> pair_metrics(Problem& P, const double* X, int m, const std::vector<double>& lam, double tol) {
+  std::vector<PairMetrics> out(m);
+  if (m == 0) return out;
+  const std::int64_t n = P.n;
+  cudaStream_t s = P.s;
+  DevBuf<double> AX, BX, R, lamd, dots;
+  AX.alloc(static_cast<std::size_t>(n) * m);
+  BX.alloc(static_cast<std::size_t>(n) * m);
+  R.alloc(static_cast<std::size_t>(n) * m);
+  lamd.upload(lam, s);
+  dots.alloc(3 * static_cast<std::size_t>(m));
+  spmm(P.A.view(n), X, n, AX.p, n, m, 1.0, 0.0, s);
+  P.bprod(X, n, BX.p, n, m);
+  residual_cols(n, m, AX.p, n, BX.p, n, lamd.p, R.p, n, s);
+  col_dots(n, m, R.p, n, R.p, n, dots.p, s);
+  col_dots(n, m, X, n, X, n, dots.p + m, s);
+  col_dots(n, m, BX.p, n, BX.p, n, dots.p + 2 * m, s);
+  std::vector<double> h(3 * static_cast<std::size_t>(m));
+  cuda_check(cudaMemcpyAsync(h.data(), dots.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s), "dots");
+  cuda_check(cudaStreamSynchronize(s), "pair metrics");
+  for (int j = 0; j < m; ++j) {
+    const double r = std::sqrt(h[j]), x = std::sqrt(h[m + j]), bx = std::sqrt(h[2 * m + j]);
+    PairMetrics& q = out[j];
+    q.lambda = lam[j];
+    q.abs_res = r;
+    q.rel_res = lam[j] != 0.0 ? r / (std::fabs(lam[j]) * bx) : r / bx;
+    q.eta = r / ((P.normA + std::fabs(lam[j]) * P.normB) * x);
+    q.accepted = q.eta <= tol;
+  }
+  return out;
+}
+
+// --------------------------------------------------------------------------- JSON writing
+struct Json {
+  std::ostringstream os;
+  bool first = true;
+  std::vector<bool> stack;
+  void sep() { if (!first) os << ","; first = false; }
+  void key(const char* k) { sep(); os << "\"" << k << "\":"; first = true; }
+  static std::string num(double v) {
+    if (std::isnan(v)) return "null";
+    if (std::isinf(v)) return v > 0 ? "1e308" : "-1e308";
+    char b[40];
+    std::snprintf(b, sizeof b, "%.17g", v);
+    return b;
+  }
+  void val(double v) { sep(); os << num(v); }
+  void val(long long v) { sep(); os << v; }
+  void val(int v) { sep(); os << v; }
+  void val(bool v) { sep(); os << (v ? "true" : "false"); }
+  void val(const std::string& v) {
+    sep();
+    os << "\"";
+    for (char c : v) { if (c == '"' || c == '\\') os << '\\'; os << c; }
+    os << "\"";
+  }
+  void open(char c) { sep(); os << c; first = true; }
+  void close(char c) { os << c; first = false; }
+  template <class T> void kv(const char* k, const T& v) { key(k); val(v); }
+};
+
+struct Certificate {
+  bool performed = false;
+  double lower = 0.0, upper = 0.0;
+  long long count_inertia = -1, count_found = -1, endpoint_moves = 0;
+  bool passed = false;
+  std::string note, method = "none";
+};
+
+struct SliceRec {
+  double lower, upper, sigma;
+  long long count_inertia, count_found, nev, reruns, restarts, op_applies;
+  bool passed;
+};
+
+struct Timers { double setup = 0, factor = 0, iterate = 0, verify = 0, cert = 0; };
+
+// Inertia count nu_-(A - s B) with endpoint moves on singular shifts (steps.cpp:549-571 behaviour):
+// returns the count and the (possibly moved) shift.
+long long count_below(GpuFactor& F, double& s, double scale, double direction, long long& moves, Timers& tm) {
+  const auto t0 = Clock::now();
+  for (int t = 0; t < 8; ++t) {
+    hsg_inertia_t in = F.factorize(1.0, -s, true);
+    if (in.valid) { tm.cert += since(t0); return in.neg; }
+    s += direction * 1e-7 * (scale + std::fabs(s)) * (t + 1);
+    ++moves;
+  }
+  tm.cert += since(t0);
+  HSG_THROW(HSG_SINGULAR, "inertia count: singular at every moved endpoint near " << s);
+}
+
+bool factorize_at(GpuFactor& F, double& sigma, double scale, int retries, int& used_retries, Timers& tm) {
+  const auto t0 = Clock::now();
+  for (int t = 0; t <= retries; ++t) {
+    hsg_inertia_t in = F.factorize(1.0, -sigma, true);
+    if (in.valid) { tm.factor += since(t0); return true; }
+    const double step = 1e-6 * (scale + std::fabs(sigma)) * (t + 1);
+    sigma += (t % 2 == 0 ? 1.0 : -2.0) * step;
+    ++used_retries;
+  }
+  tm.factor += since(t0);
+  return false;
+}
+
+struct NearestRun {
+  std::vector<double> lam;       // converged eigenvalues sorted by distance to sigma
+  std::vector<int> col;          // their column in X
+  DevBuf<double> X;
+  int restarts = 0, applies = 0;
+};
+
+NearestRun run_krylov(ShiftInvertOp& op, Problem& P, double sigma, int nev, const hsg_solve_config_t& cfg, int p,
+                      std::uint64_t seed, Timers& tm) {
+  const auto t0 = Clock::now();
+  KsOptions o;
+  o.nev = nev;
+  o.ncv = static_cast<int>(cfg.ncv);
+  o.block = p;
+  o.tol = cfg.tol * cfg.inner_tol_factor;
+  o.max_restarts = cfg.max_restarts;
+  o.seed = seed;
+  o.which = Which::LargestMagnitude;
+  KsResult r = krylov_schur(op, P.n, o, P.s);
+  tm.iterate += since(t0);
+  NearestRun out;
+  out.restarts = r.restarts;
+  out.applies = r.applies;
+  std::vector<std::pair<double, int>> v;
+  for (std::size_t i = 0; i < r.theta.size(); ++i)
+    if (r.converged[i] && r.theta[i] != 0.0) v.push_back({sigma + 1.0 / r.theta[i], static_cast<int>(i)});
+  std::stable_sort(v.begin(), v.end(), [&](const auto& a, const auto& b) { return std::fabs(a.first - sigma) < std::fabs(b.first - sigma); });
+  for (auto& e : v) { out.lam.push_back(e.first); out.col.push_back(e.second); }
+  out.X = std::move(r.X);
+  return out;
+}
+
+int auto_block(int nev) { return nev >= 32 ? 8 : (nev >= 8 ? 4 : (nev >= 3 ? 2 : 1)); }
+
+}  // namespace
+
+SolveOutput solve_pencil(const CsrHost& a, const CsrHost* b, const hsg_solve_config_t& cfg) {
+  const auto t_start = Clock::now();
+  Timers tm;
+  const std::int64_t n = a.n;
+  HSG_REQUIRE(n > 0, HSG_INVALID_INPUT, "empty matrix");
+  HSG_REQUIRE(!b || b->n == n, HSG_INVALID_INPUT, "A and B differ in size");
+  HSG_REQUIRE(cfg.tol > 0.0 && cfg.tol < 1.0, HSG_INVALID_INPUT, "tol outside (0, 1)");
+  HSG_REQUIRE(cfg.mode == 0 || cfg.mode == 1, HSG_UNSUPPORTED, "only 'nearest' and 'interval' targets are served by this build");
+  HSG_REQUIRE(cfg.factor_precision == 0 || cfg.factor_precision == 1, HSG_INVALID_INPUT, "factor_precision");
+  hsg_options_t fo;
+  hsg_default_options(&fo);
+  fo.device = cfg.device;
+  GpuFactor F(fo);
+  Problem P;
+  P.n = n;
+  P.s = F.stream();
+  cuda_check(cudaSetDevice(cfg.device), "cudaSetDevice");
+  upload(P.A, a, P.s);
+  std::string problem = "HEP";
+  std::vector<std::string> warnings;
+  if (b) {
+    upload(P.B, *b, P.s);
+    P.b_identity = false;
+    P.b_diagonal = is_diagonal(*b);
+    problem = "GHEP";
+    if (P.b_diagonal) {
+      std::vector<double> d(n, 0.0);
+      for (std::int64_t i = 0; i < n; ++i)
+        for (std::int64_t q = b->rp[i]; q < b->rp[i + 1]; ++q)
+          if (b->ci[q] == i) d[i] += b->v[q];
+      double mx = 0.0, mn = std::numeric_limits<double>::infinity();
+      for (double x : d) { mx = std::max(mx, std::fabs(x)); mn = std::min(mn, x); }
+      HSG_REQUIRE(mn > 0.0, HSG_UNSUPPORTED, "B is indefinite (GHIEP): not served by this build");
+      P.bdiag.upload(d, P.s);
+      P.normB = mx;
+    }
+  }
+  // norm estimates (Lanczos lower bounds)
+  {
+    const auto t0 = Clock::now();
+    P.normA = norm_estimate(P.A.view(n), n, P.s, cfg.seed + 7);
+    if (b && !P.b_diagonal) P.normB = norm_estimate(P.B.view(n), n, P.s, cfg.seed + 11);
+    tm.setup += since(t0);
+  }
+  const double scale = P.normB > 0 ? P.normA / P.normB : P.normA;
+  // analysis on the pencil's upper pattern
+  {
+    const auto t0 = Clock::now();
+    const CsrHost au = upper_of(a);
+    CsrHost bu;
+    if (b) bu = upper_of(*b);
+    F.analyze(n, au.rp.data(), au.ci.data(), au.v.data(), b ? bu.rp.data() : nullptr, b ? bu.ci.data() : nullptr,
+              b ? bu.v.data() : nullptr, nullptr);
+    tm.factor += since(t0);
+  }
+  if (b && !P.b_diagonal) {
+    const auto t0 = Clock::now();
+    hsg_inertia_t in = F.factorize(0.0, 1.0, true);
+    tm.factor += since(t0);
+    HSG_REQUIRE(in.valid && in.neg == 0 && in.zero == 0, HSG_UNSUPPORTED, "B is not positive definite (GHIEP): not served by this build");
+  }
+  ShiftInvertOp op(P, F);
+  SolveOutput out;
+  out.n = n;
+  Certificate cert;
+  std::vector<SliceRec> slices;
+  std::vector<double> lam_out;
+  DevBuf<double> Xout;
+  int shift_retries = 0, restarts = 0, block_used = 0;
+  long long applies_before = 0;
+  double sigma_used = cfg.sigma;
+  const bool certify = cfg.certificate == 0;
+
+  if (cfg.mode == 0) {
+    // ---------------------------------------------------------------- nearest
+    const std::int64_t k = cfg.k;
+    HSG_REQUIRE(k >= 1 && k < n, HSG_INVALID_INPUT, "k must be in [1, n)");
+    double sigma = cfg.sigma;
+    HSG_REQUIRE(std::isfinite(sigma), HSG_INVALID_INPUT, "sigma must be finite");
+    if (!factorize_at(F, sigma, scale, cfg.max_shift_retries, shift_retries, tm))
+      HSG_THROW(HSG_SINGULAR, "A - sigma B is numerically singular at and near sigma = " << cfg.sigma);
+    sigma_used = sigma;
+    int nev = static_cast<int>(std::min<std::int64_t>(n - 1, k + std::max<std::int64_t>(4, (k + 1) / 2)));
+    const int p = cfg.block_size > 0 ? cfg.block_size : auto_block(nev);
+    block_used = p;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+      if (attempt > 0 && !factorize_at(F, sigma, scale, cfg.max_shift_retries, shift_retries, tm))
+        HSG_THROW(HSG_SINGULAR, "A - sigma B is numerically singular at the working shift");
+      NearestRun run = run_krylov(op, P, sigma, nev, cfg, p, cfg.seed + attempt, tm);
+      restarts += run.restarts;
+      const std::size_t M = run.lam.size();
+      if (static_cast<std::int64_t>(M) < k) {
+        nev = static_cast<int>(std::min<std::int64_t>(n - 1, 2 * nev));
+        warnings.push_back("fewer converged pairs than k; rerun with more");
+        continue;
+      }
+      // window: midpoint of the first distance gap at or after the k-th pair
+      std::vector<double> d(M);
+      for (std::size_t i = 0; i < M; ++i) d[i] = std::fabs(run.lam[i] - sigma);
+      long long q = -1;
+      for (std::size_t i = static_cast<std::size_t>(k) - 1; i + 1 < M; ++i) {
+        const double ctol = 1e-8 * (std::fabs(sigma) + d[i + 1] + scale * 1e-3);
+        if (d[i + 1] - d[i] > ctol) { q = static_cast<long long>(i) + 1; break; }
+      }
+      bool passed = !certify;
+      double R = 0.0, lo = 0.0, hi = 0.0;
+      long long cnt = -1, moves = 0;
+      if (certify) {
+        if (q < 0) {
+          nev = static_cast<int>(std::min<std::int64_t>(n - 1, nev + std::max<int>(4, nev / 2)));
+          continue;  // no gap among the converged pairs yet
+        }
+        R = 0.5 * (d[q - 1] + d[q]);
+        lo = sigma - R;
+        hi = sigma + R;
+        double lo_m = lo, hi_m = hi;
+        const long long nlo = count_below(F, lo_m, scale, -1.0, moves, tm);
+        const long long nhi = count_below(F, hi_m, scale, +1.0, moves, tm);
+        cnt = nhi - nlo;
+        lo = lo_m;
+        hi = hi_m;
+        long long found = 0;
+        for (std::size_t i = 0; i < M; ++i)
+          if (run.lam[i] >= lo && run.lam[i] < hi) ++found;
+        passed = cnt == found;
+        cert.performed = true;
+        cert.lower = lo;
+        cert.upper = hi;
+        cert.count_inertia = cnt;
+        cert.count_found = found;
+        cert.endpoint_moves += moves;
+        cert.passed = passed;
+        cert.method = "exact";
+        if (!passed) {
+          nev = static_cast<int>(std::min<std::int64_t>(n - 1, nev + (cnt - found) + 4));
+          warnings.push_back("certificate found missing eigenvalues; deflated rerun with larger nev");
+          continue;
+        }
+      }
+      // select the k nearest
+      std::vector<double> sel;
+      std::vector<double> S(static_cast<std::size_t>(run.X.n / n) * k, 0.0);
+      const int ncols = static_cast<int>(run.X.n / n);
+      for (std::int64_t j = 0; j < k; ++j) {
+        sel.push_back(run.lam[j]);
+        S[static_cast<std::size_t>(run.col[j]) + static_cast<std::size_t>(j) * ncols] = 1.0;
+      }
+      DevBuf<double> Sd;
+      Sd.upload(S, P.s);
+      Xout.alloc(static_cast<std::size_t>(n) * k);
+      gemm_tall(n, ncols, static_cast<int>(k), run.X.p, n, Sd.p, ncols, Xout.p, n, 1.0, 0.0, P.s);
+      lam_out = sel;
+      break;
+    }
+    HSG_REQUIRE(!lam_out.empty(), HSG_NOT_CONVERGED, "nearest target: no certified set of eigenpairs after reruns");
+  } else {
+    // ---------------------------------------------------------------- interval (slicing)
+    double lo = cfg.lower, hi = cfg.upper;
+    HSG_REQUIRE(std::isfinite(lo) && std::isfinite(hi) && lo < hi, HSG_INVALID_INPUT, "interval needs lower < upper");
+    long long moves = 0;
+    const long long nlo = count_below(F, lo, scale, -1.0, moves, tm);
+    const long long nhi = count_below(F, hi, scale, +1.0, moves, tm);
+    const long long N = nhi - nlo;
+    cert.performed = true;
+    cert.lower = lo;
+    cert.upper = hi;
+    cert.count_inertia = N;
+    cert.method = "exact";
+    cert.endpoint_moves = moves;
+    std::vector<double> cuts{lo, hi};
+    std::vector<long long> below{nlo, nhi};
+    const long long target = cfg.slice_size > 0 ? cfg.slice_size : 96;
+    // split slices with too many eigenvalues at their midpoint (one count per cut)
+    for (std::size_t i = 0; i + 1 < cuts.size();) {
+      const long long c = below[i + 1] - below[i];
+      if (c > target && cuts[i + 1] - cuts[i] > 1e-9 * (scale + std::fabs(cuts[i]))) {
+        double mid = 0.5 * (cuts[i] + cuts[i + 1]);
+        const long long nm = count_below(F, mid, scale, +1.0, cert.endpoint_moves, tm);
+        cuts.insert(cuts.begin() + static_cast<std::ptrdiff_t>(i) + 1, mid);
+        below.insert(below.begin() + static_cast<std::ptrdiff_t>(i) + 1, nm);
+        continue;
+      }
+      ++i;
+    }
+    std::vector<std::vector<double>> vals;
+    std::vector<DevBuf<double>> vecs;
+    long long found_total = 0;
+    bool all_pass = true;
+    for (std::size_t i = 0; i + 1 < cuts.size(); ++i) {
+      const long long c = below[i + 1] - below[i];
+      SliceRec rec{cuts[i], cuts[i + 1], 0.5 * (cuts[i] + cuts[i + 1]), c, 0, 0, 0, 0, 0, c == 0};
+      if (c == 0) { slices.push_back(rec); continue; }
+      double sigma = rec.sigma;
+      if (!factorize_at(F, sigma, scale, cfg.max_shift_retries, shift_retries, tm))
+        HSG_THROW(HSG_SINGULAR, "slice shift singular near " << rec.sigma);
+      rec.sigma = sigma;
+      int nev = static_cast<int>(std::min<std::int64_t>(n - 1, c + std::max<long long>(4, c / 4)));
+      const int p = cfg.block_size > 0 ? cfg.block_size : auto_block(nev);
+      block_used = std::max(block_used, p);
+      for (int attempt = 0; attempt < 4; ++attempt) {
+        if (attempt > 0 && !factorize_at(F, sigma, scale, cfg.max_shift_retries, shift_retries, tm))
+          HSG_THROW(HSG_SINGULAR, "slice shift singular");
+        const long long applies0 = op.columns;
+        NearestRun run = run_krylov(op, P, sigma, nev, cfg, p, cfg.seed + 17 * i + attempt, tm);
+        rec.restarts += run.restarts;
+        rec.op_applies += op.columns - applies0;
+        rec.nev = nev;
+        std::vector<int> inside;
+        for (std::size_t j = 0; j < run.lam.size(); ++j)
+          if (run.lam[j] >= cuts[i] && run.lam[j] < cuts[i + 1]) inside.push_back(static_cast<int>(j));
+        rec.count_found = static_cast<long long>(inside.size());
+        if (rec.count_found != c && attempt + 1 < 4) {
+          ++rec.reruns;
+          nev = static_cast<int>(std::min<std::int64_t>(n - 1, nev + std::max<long long>(4, c - rec.count_found + 4)));
+          continue;
+        }
+        rec.passed = rec.count_found == c;
+        const int ncols = static_cast<int>(run.X.n / n);
+        std::vector<double> S(static_cast<std::size_t>(ncols) * inside.size(), 0.0);
+        std::vector<double> lv;
+        for (std::size_t q = 0; q < inside.size(); ++q) {
+          S[static_cast<std::size_t>(run.col[inside[q]]) + q * ncols] = 1.0;
+          lv.push_back(run.lam[inside[q]]);
+        }
+        DevBuf<double> Sd, Xs;
+        Sd.upload(S, P.s);
+        Xs.alloc(static_cast<std::size_t>(n) * std::max<std::size_t>(1, inside.size()));
+        if (!inside.empty()) gemm_tall(n, ncols, static_cast<int>(inside.size()), run.X.p, n, Sd.p, ncols, Xs.p, n, 1.0, 0.0, P.s);
+        cuda_check(cudaStreamSynchronize(P.s), "slice vectors");
+        vals.push_back(lv);
+        vecs.push_back(std::move(Xs));
+        break;
+      }
+      found_total += rec.count_found;
+      all_pass = all_pass && rec.passed;
+      restarts += static_cast<int>(rec.restarts);
+      slices.push_back(rec);
+    }
+    cert.count_found = found_total;
+    cert.passed = all_pass && found_total == N;
+    // gather ascending
+    std::vector<std::pair<double, std::pair<int, int>>> all;
+    for (std::size_t s = 0; s < vals.size(); ++s)
+      for (std::size_t q = 0; q < vals[s].size(); ++q) all.push_back({vals[s][q], {static_cast<int>(s), static_cast<int>(q)}});
+    std::stable_sort(all.begin(), all.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+    Xout.alloc(static_cast<std::size_t>(n) * std::max<std::size_t>(1, all.size()));
+    for (std::size_t j = 0; j < all.size(); ++j) {
+      lam_out.push_back(all[j].first);
+      const auto& src = vecs[all[j].second.first];
+      copy_cols(n, 1, src.p + static_cast<std::int64_t>(all[j].second.second) * n, n, Xout.p + static_cast<std::int64_t>(j) * n, n, P.s);
+    }
+    sigma_used = slices.empty() ? 0.5 * (lo + hi) : slices.front().sigma;
+  }
+  (void)applies_before;
+  // verification
+  const auto t_ver = Clock::now();
+  const int m = static_cast<int>(lam_out.size());
+  std::vector<PairMetrics> pm = pair_metrics(P, Xout.p, m, lam_out, cfg.tol);
+  out.eigenvalues = lam_out;
+  out.vectors.resize(static_cast<std::size_t>(n) * m);
+  if (m > 0)
+    cuda_check(cudaMemcpyAsync(out.vectors.data(), Xout.p, out.vectors.size() * sizeof(double), cudaMemcpyDeviceToHost, P.s), "vectors");
+  cuda_check(cudaStreamSynchronize(P.s), "vectors");
+  tm.verify += since(t_ver);
+  bool all_ok = true;
+  for (const auto& q : pm) all_ok = all_ok && q.accepted;
+  const bool success = all_ok && (!cert.performed || cert.passed) && (cfg.mode != 1 || m == cert.count_inertia);
+  // report
+  const hsg_estimate_t est = F.estimate();
+  const hsg_inertia_t inr = F.inertia();
+  Json j;
+  j.open('{');
+  j.kv("n", static_cast<long long>(n));
+  j.kv("nnz_a", static_cast<long long>(a.rp[n]));
+  j.kv("nnz_b", static_cast<long long>(b ? b->rp[n] : 0));
+  j.kv("complex_scalars", false);
+  j.kv("problem", problem);
+  j.kv("norm2_a", P.normA);
+  j.kv("norm2_b", P.normB);
+  j.kv("scale", scale);
+  j.kv("method", std::string("shift_invert_lanczos"));
+  j.kv("candidate_source", std::string("iterative"));
+  j.kv("sigma_requested", cfg.mode == 0 ? cfg.sigma : 0.5 * (cfg.lower + cfg.upper));
+  j.kv("sigma_used", sigma_used);
+  j.kv("shift_retries", shift_retries);
+  j.kv("block_size", block_used);
+  j.kv("restarts", restarts);
+  j.kv("op_applies", static_cast<long long>(op.columns));
+  const double total = since(t_start);
+  j.kv("time_total_s", total);
+  j.kv("time_setup_s", tm.setup);
+  j.kv("time_factor_s", tm.factor);
+  j.kv("time_iterate_s", tm.iterate);
+  j.kv("time_verify_s", tm.verify);
+  j.kv("time_certificate_s", tm.cert);
+  j.key("factor_stats");
+  j.open('{');
+  j.kv("factor_entries", static_cast<long long>(est.factor_entries));
+  j.kv("nnz_l", static_cast<long long>(est.nnz_l));
+  j.kv("flops", est.flops);
+  j.kv("supernodes", est.supernodes);
+  j.kv("levels", est.levels);
+  j.kv("max_front", est.max_front);
+  j.kv("analyze_s", est.analyze_s);
+  j.kv("ordering_s", est.ordering_s);
+  j.kv("last_factorize_s", F.last_factor_seconds());
+  j.kv("delayed_pivots", static_cast<long long>(inr.delayed_pivots));
+  j.kv("two_by_two", static_cast<long long>(inr.two_by_two));
+  j.close('}');
+  j.key("precision");
+  j.open('{');
+  j.kv("requested", std::string(cfg.factor_precision == 1 ? "single" : "double"));
+  j.kv("used", std::string("double"));
+  j.close('}');
+  j.key("pairs");
+  j.open('[');
+  for (const auto& q : pm) {
+    j.open('{');
+    j.kv("lambda_re", q.lambda);
+    j.kv("lambda_im", 0.0);
+    j.kv("abs_residual", q.abs_res);
+    j.kv("rel_residual", q.rel_res);
+    j.kv("backward_error", q.eta);
+    j.kv("accepted", q.accepted);
+    j.close('}');
+  }
+  j.close(']');
+  j.key("certificate");
+  j.open('{');
+  j.kv("performed", cert.performed);
+  j.kv("lower", cert.lower);
+  j.kv("upper", cert.upper);
+  j.kv("count_inertia", cert.count_inertia);
+  j.kv("count_found", cert.count_found);
+  j.kv("endpoint_moves", cert.endpoint_moves);
+  j.kv("passed", cert.passed);
+  j.kv("note", cert.note);
+  j.kv("method", cert.method);
+  j.kv("rigorous", cert.performed && cert.passed);
+  j.kv("failure_probability", cert.performed && cert.passed ? 0.0 : 1.0);
+  j.close('}');
+  j.key("slices");
+  j.open('[');
+  for (const auto& r : slices) {
+    j.open('{');
+    j.kv("lower", r.lower);
+    j.kv("upper", r.upper);
+    j.kv("sigma", r.sigma);
+    j.kv("which", std::string("largest_magnitude"));
+    j.kv("count_inertia", r.count_inertia);
+    j.kv("count_found", r.count_found);
+    j.kv("nev", r.nev);
+    j.kv("reruns", r.reruns);
+    j.kv("restarts", r.restarts);
+    j.kv("op_applies", r.op_applies);
+    j.kv("passed", r.passed);
+    j.close('}');
+  }
+  j.close(']');
+  j.kv("success", success);
+  j.key("warnings");
+  j.open('[');
+  for (const auto& w : warnings) j.val(w);
+  j.close(']');
+  j.close('}');
+  out.report_json = j.os.str();
+  return out;
+}
+
+}  // namespace hsg

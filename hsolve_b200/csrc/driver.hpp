@@ -1,0 +1,29 @@
+// Top-level shift-invert driver: the device-resident equivalent of hs::solve for HEP / GHEP
+// (hsolve include/hsolve/solver.hpp:545-547; src/driver/solver.cpp:307-520, definite.cpp).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "hsg_solve.h"
+
+namespace hsg {
+
+struct CsrHost {
+  std::int64_t n = 0;
+  std::vector<std::int64_t> rp;
+  std::vector<std::int32_t> ci;
+  std::vector<double> v;
+};
+
+struct SolveOutput {
+  std::vector<double> eigenvalues;
+  std::vector<double> vectors;  // n x m, column-major
+  std::int64_t n = 0;
+  std::string report_json;
+};
+
+SolveOutput solve_pencil(const CsrHost& a, const CsrHost* b, const hsg_solve_config_t& cfg);
+
+}  // namespace hsg

@@ -1,0 +1,271 @@
+// Block Krylov-Schur (see eigen.hpp).
+#include "eigen.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <random>
+
+#include "blas_kernels.cuh"
+#include "dense_host.hpp"
+
+namespace hsg {
+
+namespace {
+
+struct Basis {
+  std::int64_t n;
+  int cols;
+  bool bid;
+  DevBuf<double> V, BV, tmp, tmpB, g, part, small;
+  std::int64_t part_cap = 0;
+  double* v(int j) { return V.p + static_cast<std::int64_t>(j) * n; }
+  double* bv(int j) { return bid ? v(j) : BV.p + static_cast<std::int64_t>(j) * n; }
+};
+
+void to_host(std::vector<double>& h, const double* d, std::size_t count, cudaStream_t s) {
+  h.resize(count);
+  cuda_check(cudaMemcpyAsync(h.data(), d, count * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H");
+  cuda_check(cudaStreamSynchronize(s), "sync");
+}
+
+void to_dev(double* d, const std::vector<double>& h, cudaStream_t s) {
+  cuda_check(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s), "H2D");
+}
+
+// Orthogonalize columns [j, j+p) of the basis against columns [0, j) (CGS2, B inner product),
+// returning the accumulated coefficients H (j x p) on the host.
+std::vector<double> orthogonalize(Basis& B, int j, int p, cudaStream_t s) {
+  std::vector<double> Htot(static_cast<std::size_t>(j) * p, 0.0), H;
+  if (j == 0) return Htot;
+  for (int pass = 0; pass < 2; ++pass) {
+    gram(B.n, j, p, B.bid ? B.v(0) : B.bv(0), B.n, B.v(j), B.n, B.g.p, B.part.p, B.part_cap, s);
+    gemm_tall(B.n, j, p, B.v(0), B.n, B.g.p, j, B.v(j), B.n, -1.0, 1.0, s);
+    to_host(H, B.g.p, static_cast<std::size_t>(j) * p, s);
+    for (std::size_t t = 0; t < H.size(); ++t) Htot[t] += H[t];
+  }
+  return Htot;
+}
+
+// B-orthonormalize columns [j, j+p) in place (CholQR2). Returns R (p x p, upper in the sense
+// W_old = W_new R, stored column-major) or an empty vector on breakdown.
+std::vector<double> normalize(Basis& B, KrylovOperator& op, int j, int p, cudaStream_t s) {
+  std::vector<double> Rtot(static_cast<std::size_t>(p) * p, 0.0);
+  for (int i = 0; i < p; ++i) Rtot[i + i * p] = 1.0;
+  std::vector<double> G, L;
+  for (int pass = 0; pass < 2; ++pass) {
+    if (!B.bid) op.bprod(B.v(j), B.n, B.bv(j), B.n, p);
+    gram(B.n, p, p, B.v(j), B.n, B.bv(j), B.n, B.g.p, B.part.p, B.part_cap, s);
+    to_host(G, B.g.p, static_cast<std::size_t>(p) * p, s);
+    for (int a = 0; a < p; ++a)
+      for (int b = 0; b < a; ++b) { const double m = 0.5 * (G[a + b * p] + G[b + a * p]); G[a + b * p] = m; G[b + a * p] = m; }
+    if (!cholesky(p, G, L, 1e-28)) return {};
+    // W = W L^{-T}  (W^T B W = L L^T -> (W L^{-T})^T B (W L^{-T}) = I)
+    std::vector<double> Linv = lower_inverse(p, L);
+    std::vector<double> LinvT(static_cast<std::size_t>(p) * p);
+    for (int a = 0; a < p; ++a)
+      for (int b = 0; b < p; ++b) LinvT[a + b * p] = Linv[b + a * p];
+    to_dev(B.small.p, LinvT, s);
+    gemm_tall(B.n, p, p, B.v(j), B.n, B.small.p, p, B.tmp.p, B.n, 1.0, 0.0, s);
+    copy_cols(B.n, p, B.tmp.p, B.n, B.v(j), B.n, s);
+    if (!B.bid) {
+      gemm_tall(B.n, p, p, B.bv(j), B.n, B.small.p, p, B.tmp.p, B.n, 1.0, 0.0, s);
+      copy_cols(B.n, p, B.tmp.p, B.n, B.bv(j), B.n, s);
+    }
+    // R_total = L^T R_total
+    std::vector<double> LT(static_cast<std::size_t>(p) * p);
+    for (int a = 0; a < p; ++a)
+      for (int b = 0; b < p; ++b) LT[a + b * p] = L[b + a * p];
+    Rtot = matmul(p, p, p, LT, Rtot);
+  }
+  return Rtot;
+}
+
+void random_block(Basis& B, int j, int p, std::mt19937_64& rng, cudaStream_t s) {
+  std::normal_distribution<double> nd;
+  std::vector<double> h(static_cast<std::size_t>(B.n) * p);
+  for (auto& x : h) x = nd(rng);
+  to_dev(B.v(j), h, s);
+  cuda_check(cudaStreamSynchronize(s), "random block");
+}
+
+// New block [j, j+p) made orthonormal to [0, j); breakdown columns replaced by random ones.
+// Returns R (coupling) of the original block; zero rows where random vectors were drawn.
+std::vector<double> ortho_block(Basis& B, KrylovOperator& op, int j, int p, std::vector<double>& H, std::mt19937_64& rng,
+                                cudaStream_t s) {
+  H = orthogonalize(B, j, p, s);
+  std::vector<double> R = normalize(B, op, j, p, s);
+  if (!R.empty()) return R;
+  // breakdown (invariant subspace): restart the block from random vectors, no coupling
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    random_block(B, j, p, rng, s);
+    std::vector<double> Hr = orthogonalize(B, j, p, s);
+    std::vector<double> Rr = normalize(B, op, j, p, s);
+    if (!Rr.empty()) return std::vector<double>(static_cast<std::size_t>(p) * p, 0.0);
+  }
+  HSG_THROW(HSG_NOT_CONVERGED, "Krylov basis: could not extend the basis (breakdown)");
+}
+
+}  // namespace
+
+KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, cudaStream_t s) {
+  const int p = std::max(1, std::min(opt.block, kMaxBlock));
+  const int nev = std::max(1, opt.nev);
+  int mmax = opt.ncv > 0 ? opt.ncv : std::max(2 * nev + 1, nev + 16) + 4 * p;
+  mmax = std::max(mmax, nev + 2 * p);
+  mmax = (mmax + p - 1) / p * p;
+  if (mmax > n) mmax = static_cast<int>(n / p * p);
+  HSG_REQUIRE(mmax >= p && nev <= mmax - p + p, HSG_INVALID_INPUT, "Krylov basis larger than the problem (n = " << n << ")");
+  Basis B;
+  B.n = n;
+  B.bid = op.b_identity();
+  B.cols = mmax + p;
+  B.V.alloc(static_cast<std::size_t>(n) * B.cols);
+  if (!B.bid) B.BV.alloc(static_cast<std::size_t>(n) * B.cols);
+  B.tmp.alloc(static_cast<std::size_t>(n) * std::max(p, mmax));
+  if (!B.bid) B.tmpB.alloc(static_cast<std::size_t>(n) * mmax);
+  B.g.alloc(static_cast<std::size_t>(B.cols) * std::max(p, mmax));
+  B.part_cap = gram_part_size(n, B.cols, p);
+  B.part.alloc(static_cast<std::size_t>(B.part_cap));
+  B.small.alloc(static_cast<std::size_t>(std::max(p * p, mmax * mmax)));
+  std::mt19937_64 rng(opt.seed);
+  KsResult res;
+  // starting block
+  random_block(B, 0, p, rng, s);
+  {
+    std::vector<double> H;
+    std::vector<double> R = ortho_block(B, op, 0, p, H, rng, s);
+    (void)R;
+  }
+  const int tdim = mmax + p;
+  std::vector<double> T(static_cast<std::size_t>(tdim) * tdim, 0.0);
+  auto Tm = [&](int i, int j) -> double& { return T[static_cast<std::size_t>(i) + static_cast<std::size_t>(j) * tdim]; };
+  int m = 0;
+  std::vector<double> S, w;
+  std::vector<int> order;
+  while (true) {
+    while (m + p <= mmax) {
+      const int j0 = m;
+      op.apply(B.v(j0), n, B.v(j0 + p), n, p);
+      res.applies += p;
+      res.block_steps += 1;
+      std::vector<double> H;
+      std::vector<double> R = ortho_block(B, op, j0 + p, p, H, rng, s);
+      const int jh = j0 + p;  // H is jh x p
+      for (int c = 0; c < p; ++c)
+        for (int i = 0; i < jh; ++i) {
+          Tm(i, j0 + c) = H[i + static_cast<std::size_t>(c) * jh];
+          Tm(j0 + c, i) = H[i + static_cast<std::size_t>(c) * jh];
+        }
+      for (int a = 0; a < p; ++a)
+        for (int b = 0; b < a; ++b) {
+          const double mm = 0.5 * (Tm(j0 + a, j0 + b) + Tm(j0 + b, j0 + a));
+          Tm(j0 + a, j0 + b) = mm;
+          Tm(j0 + b, j0 + a) = mm;
+        }
+      for (int c = 0; c < p; ++c)
+        for (int a = 0; a < p; ++a) {
+          Tm(jh + a, j0 + c) = R[a + c * p];
+          Tm(j0 + c, jh + a) = R[a + c * p];
+        }
+      m += p;
+    }
+    // Rayleigh-Ritz on T[0:m, 0:m]
+    S.assign(static_cast<std::size_t>(m) * m, 0.0);
+    for (int j = 0; j < m; ++j)
+      for (int i = 0; i < m; ++i) S[i + static_cast<std::size_t>(j) * m] = Tm(i, j);
+    sym_eig(m, S, w);
+    order.resize(m);
+    std::iota(order.begin(), order.end(), 0);
+    auto key = [&](int i) {
+      switch (opt.which) {
+        case Which::LargestMagnitude: return -std::fabs(w[i]);
+        case Which::LargestAlgebraic: return -w[i];
+        default: return w[i];
+      }
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key(a) < key(b); });
+    // residual norms ||T[m:m+p, 0:m] s_i||
+    std::vector<double> rn(m, 0.0);
+    for (int i = 0; i < m; ++i) {
+      double acc = 0.0;
+      for (int a = 0; a < p; ++a) {
+        double t = 0.0;
+        for (int q = 0; q < m; ++q) t += Tm(m + a, q) * S[q + static_cast<std::size_t>(i) * m];
+        acc += t * t;
+      }
+      rn[i] = std::sqrt(acc);
+    }
+    int nconv = 0;
+    for (int q = 0; q < nev && q < m; ++q) {
+      const int i = order[q];
+      if (rn[i] <= opt.tol * std::fabs(w[i])) ++nconv;
+    }
+    const bool done = nconv >= std::min(nev, m) || res.restarts >= opt.max_restarts;
+    if (done) {
+      const int take = std::min(nev, m);
+      res.theta.resize(take);
+      res.resid.resize(take);
+      res.converged.resize(take);
+      std::vector<double> Q(static_cast<std::size_t>(m) * take);
+      for (int q = 0; q < take; ++q) {
+        const int i = order[q];
+        res.theta[q] = w[i];
+        res.resid[q] = rn[i];
+        res.converged[q] = rn[i] <= opt.tol * std::fabs(w[i]);
+        std::copy(S.begin() + static_cast<std::ptrdiff_t>(i) * m, S.begin() + static_cast<std::ptrdiff_t>(i + 1) * m,
+                  Q.begin() + static_cast<std::ptrdiff_t>(q) * m);
+      }
+      res.nconv = nconv;
+      for (int q = take; q < m; ++q) {
+        res.other_theta.push_back(w[order[q]]);
+        res.other_resid.push_back(rn[order[q]]);
+      }
+      if (opt.ritz_vectors) {
+        res.X.alloc(static_cast<std::size_t>(n) * take);
+        B.small.alloc(Q.size());
+        to_dev(B.small.p, Q, s);
+        gemm_tall(n, m, take, B.v(0), n, B.small.p, m, res.X.p, n, 1.0, 0.0, s);
+        cuda_check(cudaStreamSynchronize(s), "ritz vectors");
+      }
+      return res;
+    }
+    // thick restart
+    const int keep = std::min(mmax - p, std::max(nev + p, (nev + mmax) / 2));
+    std::vector<double> Q(static_cast<std::size_t>(m) * keep);
+    std::vector<double> th(keep);
+    for (int q = 0; q < keep; ++q) {
+      const int i = order[q];
+      th[q] = w[i];
+      std::copy(S.begin() + static_cast<std::ptrdiff_t>(i) * m, S.begin() + static_cast<std::ptrdiff_t>(i + 1) * m,
+                Q.begin() + static_cast<std::ptrdiff_t>(q) * m);
+    }
+    B.small.alloc(Q.size());
+    to_dev(B.small.p, Q, s);
+    gemm_tall(n, m, keep, B.v(0), n, B.small.p, m, B.tmp.p, n, 1.0, 0.0, s);
+    if (!B.bid) gemm_tall(n, m, keep, B.bv(0), n, B.small.p, m, B.tmpB.p, n, 1.0, 0.0, s);
+    // residual block to [keep, keep+p), then the kept vectors to [0, keep)
+    copy_cols(n, p, B.v(m), n, B.v(keep), n, s);
+    copy_cols(n, keep, B.tmp.p, n, B.v(0), n, s);
+    if (!B.bid) {
+      copy_cols(n, p, B.bv(m), n, B.bv(keep), n, s);
+      copy_cols(n, keep, B.tmpB.p, n, B.bv(0), n, s);
+    }
+    // coupling b = T[m:m+p, 0:m] Q
+    std::vector<double> Tn(static_cast<std::size_t>(tdim) * tdim, 0.0);
+    auto Tnm = [&](int i, int j) -> double& { return Tn[static_cast<std::size_t>(i) + static_cast<std::size_t>(j) * tdim]; };
+    for (int q = 0; q < keep; ++q) Tnm(q, q) = th[q];
+    for (int a = 0; a < p; ++a)
+      for (int q = 0; q < keep; ++q) {
+        double t = 0.0;
+        for (int r = 0; r < m; ++r) t += Tm(m + a, r) * Q[r + static_cast<std::size_t>(q) * m];
+        Tnm(keep + a, q) = t;
+        Tnm(q, keep + a) = t;
+      }
+    T.swap(Tn);
+    m = keep;
+    res.restarts += 1;
+  }
+}
+
+}  // namespace hsg

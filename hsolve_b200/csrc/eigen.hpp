@@ -1,0 +1,58 @@
+// Block Krylov-Schur (thick-restart block Lanczos) with the basis resident on the GPU.
+//
+// Replaces hsolve's BlockThickRestartLanczos / lanczos_krylov_schur (src/eigen/block_lanczos.cpp:280-322,
+// include/hsolve/eigen.hpp:144-146) for a B-self-adjoint operator such as OP = (A - sigma B)^{-1} B:
+// full CGS2 re-orthogonalization in the B inner product and CholQR2 normalization of every new
+// block (BlockOrthonormalizer, src/eigen/block_ortho.cpp:165,270), Rayleigh-Ritz on the projected
+// matrix on the host, thick restart keeping the wanted Ritz vectors.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "gpu_factor.hpp"
+
+namespace hsg {
+
+struct KrylovOperator {
+  virtual ~KrylovOperator() = default;
+  // y = OP x (device, n x p)
+  virtual void apply(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p) = 0;
+  // y = B x for the inner product; B = I when b_identity()
+  virtual bool b_identity() const { return true; }
+  virtual void bprod(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p) {
+    (void)x; (void)ldx; (void)y; (void)ldy; (void)p;
+  }
+};
+
+enum class Which { LargestMagnitude, LargestAlgebraic, SmallestAlgebraic };
+
+struct KsOptions {
+  int nev = 6;
+  int ncv = 0;           // basis columns (0: automatic)
+  int block = 1;         // block width p
+  double tol = 1e-11;    // ||OP y - theta y||_B <= tol |theta|
+  int max_restarts = 1000;
+  std::uint64_t seed = 2026;
+  Which which = Which::LargestMagnitude;
+  bool ritz_vectors = true;
+};
+
+struct KsResult {
+  std::vector<double> theta;   // the nev wanted Ritz values (ordered by `which`)
+  std::vector<double> resid;   // their residual norms
+  std::vector<char> converged;
+  int nconv = 0;
+  int restarts = 0;
+  int applies = 0;             // operator applications (columns)
+  int block_steps = 0;
+  std::vector<double> other_theta;  // the remaining Ritz values of the last basis (gap placement)
+  std::vector<double> other_resid;
+  DevBuf<double> X;            // n x nev Ritz vectors (B-orthonormal), if requested
+};
+
+KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, cudaStream_t stream);
+
+}  // namespace hsg

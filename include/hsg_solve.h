@@ -1,0 +1,63 @@
+/* hsolve_b200 — C ABI of the whole shift-invert eigensolve (hs::solve, hsolve
+ * include/hsolve/solver.hpp:545-547), the call behind hsolve.solve(A, B, sigma, k | interval).
+ *
+ * A and B are given in full storage (both triangles) as CSR with int64 row pointers and int32
+ * columns (host pointers); B may be NULL (standard problem, B = I). The configuration mirrors the
+ * SolverConfig keys this path honours (solver.hpp:71-235); the report is the SolveReport JSON
+ * document (solver.hpp:457-516, docs/FORMATS.md section 3 in hsolve) with the keys this path fills.
+ */
+#ifndef HSG_SOLVE_H_
+#define HSG_SOLVE_H_
+
+#include <stdint.h>
+
+#include "hsg.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int32_t mode;               /* hs::TargetMode: 0 nearest, 1 interval, 2 smallest, 3 largest */
+  double sigma;               /* Target::sigma (nearest) */
+  int64_t k;                  /* Target::k */
+  double lower, upper;        /* Target::lower / upper (interval) */
+  int32_t problem;            /* hs::ProblemType: 0 auto, 1 standard, 2 generalized definite, 3 indefinite */
+  double tol;                 /* backward-error acceptance, default 1e-10 */
+  double inner_tol_factor;    /* Krylov tolerance = tol * inner_tol_factor, default 0.1 */
+  int64_t ncv;                /* Krylov basis columns, 0 = auto */
+  int32_t block_size;         /* Krylov block width p, 0 = auto */
+  int64_t slice_size;         /* eigenvalues per spectrum slice, 0 = auto */
+  int32_t max_restarts;       /* default 1000 */
+  uint64_t seed;              /* Krylov start vectors, default 2026 */
+  int32_t certificate;        /* hs::CertificateMode: 0 exact, 3 off */
+  int32_t max_shift_retries;  /* default 5 */
+  int32_t factor_precision;   /* hs::FactorPrecision: 0 double, 1 single (FP32 factors + FP64 refinement) */
+  int32_t device;             /* CUDA device */
+  int32_t verbose;
+} hsg_solve_config_t;
+
+typedef struct hsg_solution hsg_solution;
+
+/* The SolverConfig defaults (solver.hpp:71-235). */
+HSG_API void hsg_default_solve_config(hsg_solve_config_t* cfg);
+
+/* hs::solve<double>(A, B, cfg): eigenpairs ordered by the target; HSG_OK also when the run did
+ * not meet tol (report "success": false), an error status otherwise (hs::Error::Code + 1). */
+HSG_API int hsg_eigsolve(int64_t n, const int64_t* a_rowptr, const int32_t* a_col, const double* a_val,
+                         const int64_t* b_rowptr, const int32_t* b_col, const double* b_val,
+                         const hsg_solve_config_t* cfg, hsg_solution** out);
+
+/* Solution<double>::eigenvalues.size() and n. */
+HSG_API int hsg_solution_sizes(const hsg_solution* s, int64_t* n, int64_t* m);
+/* Copies eigenvalues (m) and eigenvectors (n x m column-major; NULL to skip). */
+HSG_API int hsg_solution_copy(const hsg_solution* s, double* eigenvalues, double* eigenvectors);
+/* SolveReport::to_json(). Valid until hsg_solution_free. */
+HSG_API const char* hsg_solution_report(const hsg_solution* s);
+HSG_API void hsg_solution_free(hsg_solution* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HSG_SOLVE_H_ */
