@@ -9,12 +9,12 @@ from __future__ import annotations
 
 from . import errors
 from ._native import Factorization, Inertia, compute_ordering, symbolic_stats
-from .api import SolveResult, solve
+from .api import Session, SolveResult, solve
 from .errors import (FactorizationFailedError, HsolveError, HsolveIOError, HsolveWarning, InternalError,
                      InvalidInputError, NotConvergedError, NotHermitianError, OutOfMemoryBudgetError, SingularError,
                      UnsupportedError)
 
-__all__ = ["solve", "SolveResult", "Factorization", "Inertia", "compute_ordering", "symbolic_stats", "errors",
+__all__ = ["solve", "Session", "SolveResult", "Factorization", "Inertia", "compute_ordering", "symbolic_stats", "errors",
            "HsolveError", "InvalidInputError", "HsolveIOError", "NotHermitianError", "UnsupportedError",
            "FactorizationFailedError", "SingularError", "OutOfMemoryBudgetError", "NotConvergedError",
            "InternalError", "HsolveWarning"]

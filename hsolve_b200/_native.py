@@ -49,6 +49,8 @@ _D = ctypes.c_double
 SIGNATURES = {
     "hsg_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "hsg_last_error": (ctypes.c_char_p, []),
+    "hsg_kernel_launches": (ctypes.c_int64, []),
+    "hsg_fp64_peak_probe": (ctypes.c_int, [_I32, _P]),
     "hsg_default_options": (None, [_P]),
     "hsg_create": (ctypes.c_int, [_P, _P]),
     "hsg_destroy": (ctypes.c_int, [_P]),
@@ -231,3 +233,15 @@ def symbolic_stats(A, pivot_order=None, amalgamate=True) -> dict:
     po = None if pivot_order is None else np.ascontiguousarray(pivot_order, dtype=np.int32)
     check(lib().hsg_symbolic_stats(A.shape[0], _ptr(rp), _ptr(ci), _ptr(po), int(amalgamate), ctypes.byref(e)))
     return {f: getattr(e, f) for f, _ in _Estimate._fields_}
+
+
+def kernel_launches() -> int:
+    """Kernel launches this library has issued in the process so far."""
+    return int(lib().hsg_kernel_launches())
+
+
+def fp64_peak_tflops(device: int = 0) -> float:
+    """Measured FP64 FMA throughput (TFLOP/s) of the device."""
+    v = ctypes.c_double()
+    check(lib().hsg_fp64_peak_probe(device, ctypes.byref(v)))
+    return float(v.value)

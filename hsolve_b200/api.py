@@ -35,6 +35,9 @@ _SOLVE_SIGS = {
     "hsg_solution_copy": (ctypes.c_int, [_P, _P, _P]),
     "hsg_solution_report": (ctypes.c_char_p, [_P]),
     "hsg_solution_free": (None, [_P]),
+    "hsg_session_create": (ctypes.c_int, [ctypes.c_int64, _P, _P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_uint64, _P]),
+    "hsg_session_solve": (ctypes.c_int, [_P, _P, _P]),
+    "hsg_session_free": (None, [_P]),
 }
 _native.SIGNATURES.update(_SOLVE_SIGS)
 
@@ -293,6 +296,12 @@ def solve(A, B=None, *, sigma=None, k=_Default(6), mode=_Default("nearest"), low
     h = ctypes.c_void_p()
     p = _native._ptr
     _native.check(lib.hsg_eigsolve(n, p(arp), p(aci), p(av), p(brp), p(bci), p(bv), ctypes.byref(c), ctypes.byref(h)))
+    return _result(h, n, cfg, da, db)
+
+
+def _result(h, n, cfg, da, db) -> SolveResult:
+    lib = _native.lib()
+    p = _native._ptr
     try:
         nn, m = ctypes.c_int64(), ctypes.c_int64()
         _native.check(lib.hsg_solution_sizes(h, ctypes.byref(nn), ctypes.byref(m)))
@@ -307,5 +316,57 @@ def solve(A, B=None, *, sigma=None, k=_Default(6), mode=_Default("nearest"), low
     result = SolveResult(w, v, np.zeros(0, dtype=np.complex128), np.zeros((n, 0), dtype=np.complex128), report, cfg)
     if not result.success:
         warnings.warn("hsolve: the solve finished without meeting the tolerance (see result.report['pairs'] "
-                      "and result.report['warnings'])", HsolveWarning, stacklevel=2)
+                      "and result.report['warnings'])", HsolveWarning, stacklevel=3)
     return result
+
+
+class Session:
+    """A pencil (A, B) resident on the GPU with its nested-dissection analysis and norm bounds done
+    once; solve(...) takes solve()'s target arguments and reuses them for every target and shift
+    (the serving path's symbolic reuse)."""
+
+    def __init__(self, A, B=None, *, device: int = 0, seed: int = 2026, storage: str = "auto",
+                 hermitian_tol: float = 1e-10):
+        a = _as_csr(A, "A", storage)
+        a, self._da = _hermitian_check(a, "A", hermitian_tol)
+        self._db = 0.0
+        b = None
+        if B is not None:
+            b = _as_csr(B, "B", storage)
+            if b.shape != a.shape:
+                raise InvalidInputError(f"A is {a.shape} but B is {b.shape}")
+            b, self._db = _hermitian_check(b, "B", hermitian_tol)
+        self.n = a.shape[0]
+        self.device = device
+        keep = [np.ascontiguousarray(a.indptr, dtype=np.int64), np.ascontiguousarray(a.indices, dtype=np.int32),
+                np.ascontiguousarray(a.data, dtype=np.float64)]
+        if b is not None:
+            keep += [np.ascontiguousarray(b.indptr, dtype=np.int64), np.ascontiguousarray(b.indices, dtype=np.int32),
+                     np.ascontiguousarray(b.data, dtype=np.float64)]
+        else:
+            keep += [None, None, None]
+        p = _native._ptr
+        h = ctypes.c_void_p()
+        _native.check(_native.lib().hsg_session_create(self.n, *[p(x) for x in keep], int(device), int(seed),
+                                                       ctypes.byref(h)))
+        self._h = h
+
+    def solve(self, *, sigma=None, k=_Default(6), mode=_Default("nearest"), lower=None, upper=None,
+              tol=_Default(1e-10), config=None, verbose: int = 0) -> SolveResult:
+        cfg = merge_config(config, sigma, k, mode, lower, upper, tol, _Default(0))
+        cfg.setdefault("device", self.device)
+        c = _struct_from(cfg, verbose)
+        h = ctypes.c_void_p()
+        _native.check(_native.lib().hsg_session_solve(self._h, ctypes.byref(c), ctypes.byref(h)))
+        return _result(h, self.n, cfg, self._da, self._db)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _native.lib().hsg_session_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -9,6 +9,7 @@
 #include <cstdint>
 
 #include "blas_kernels.cuh"
+#include "common.hpp"
 #include "device.cuh"
 
 namespace hsg {
@@ -191,10 +192,10 @@ void spmm(const CsrDev& M, const double* x, std::int64_t ldx, double* y, std::in
     const int pc = p - c0 < 8 ? p - c0 : 8;
     const double* xc = x + c0 * ldx;
     double* yc = y + c0 * ldy;
-    if (pc == 1) k_spmm<1><<<blocks, threads, 0, s>>>(M.n, M.rp, M.ci, M.v, xc, ldx, yc, ldy, pc, alpha, beta);
-    else if (pc <= 2) k_spmm<2><<<blocks, threads, 0, s>>>(M.n, M.rp, M.ci, M.v, xc, ldx, yc, ldy, pc, alpha, beta);
-    else if (pc <= 4) k_spmm<4><<<blocks, threads, 0, s>>>(M.n, M.rp, M.ci, M.v, xc, ldx, yc, ldy, pc, alpha, beta);
-    else k_spmm<8><<<blocks, threads, 0, s>>>(M.n, M.rp, M.ci, M.v, xc, ldx, yc, ldy, pc, alpha, beta);
+    if (pc == 1) { note_launches(1); k_spmm<1><<<blocks, threads, 0, s>>>(M.n, M.rp, M.ci, M.v, xc, ldx, yc, ldy, pc, alpha, beta); }
+    else if (pc <= 2) { note_launches(1); k_spmm<2><<<blocks, threads, 0, s>>>(M.n, M.rp, M.ci, M.v, xc, ldx, yc, ldy, pc, alpha, beta); }
+    else if (pc <= 4) { note_launches(1); k_spmm<4><<<blocks, threads, 0, s>>>(M.n, M.rp, M.ci, M.v, xc, ldx, yc, ldy, pc, alpha, beta); }
+    else { note_launches(1); k_spmm<8><<<blocks, threads, 0, s>>>(M.n, M.rp, M.ci, M.v, xc, ldx, yc, ldy, pc, alpha, beta); }
   }
 }
 
@@ -211,7 +212,9 @@ void gram(std::int64_t n, int m, int p, const double* x, std::int64_t ldx, const
     const std::int64_t nparts = (n + chunk - 1) / chunk;
     if (nparts * m * pc > part_cap) return;  // caller sized part_cap with gram_part_size()
     const std::size_t smem = static_cast<std::size_t>(chunk) * pc * sizeof(double);
+    note_launches(1);
     k_gram_partial<<<static_cast<int>(nparts), 256, smem, s>>>(n, m, pc, x, ldx, y + c0 * ldy, ldy, chunk, part);
+    note_launches(1);
     k_gram_reduce<<<grid_for(m * pc, 256), 256, 0, s>>>(static_cast<int>(nparts), m * pc, part, g + static_cast<std::int64_t>(c0) * m);
   }
 }
@@ -220,7 +223,7 @@ void gemm_tall(std::int64_t n, int m, int q, const double* x, std::int64_t ldx, 
                std::int64_t ldy, double alpha, double beta, cudaStream_t s) {
   if (q <= 0 || n <= 0) return;
   if (m <= 0) {
-    if (beta != 1.0) k_scale_cols<<<grid_for(n * q, 256), 256, 0, s>>>(n, q, beta, y, ldy);
+    if (beta != 1.0) { note_launches(1); k_scale_cols<<<grid_for(n * q, 256), 256, 0, s>>>(n, q, beta, y, ldy); }
     return;
   }
   const std::size_t smem = static_cast<std::size_t>(m) * 16 * sizeof(double);
@@ -229,6 +232,7 @@ void gemm_tall(std::int64_t n, int m, int q, const double* x, std::int64_t ldx, 
     cudaFuncSetAttribute(k_gemm_tall, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     configured = true;
   }
+  note_launches(1);
   k_gemm_tall<<<grid_for(n, 256), 256, smem, s>>>(n, m, q, x, ldx, sdev, lds, y, ldy, alpha, beta);
 }
 
@@ -244,24 +248,29 @@ std::int64_t gram_part_size(std::int64_t n, int m, int p) {
 void col_dots(std::int64_t n, int m, const double* x, std::int64_t ldx, const double* y, std::int64_t ldy, double* out,
               cudaStream_t s) {
   if (m <= 0) return;
+  note_launches(1);
   k_col_dots<<<m, 512, 0, s>>>(n, x, ldx, y, ldy, out);
 }
 
 void scale_cols(std::int64_t n, int p, double a, double* y, std::int64_t ldy, cudaStream_t s) {
+  note_launches(1);
   k_scale_cols<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, a, y, ldy);
 }
 
 void diag_scale(std::int64_t n, int p, const double* d, const double* x, std::int64_t ldx, double* y,
                 std::int64_t ldy, cudaStream_t s) {
+  note_launches(1);
   k_diag_scale<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, d, x, ldx, y, ldy);
 }
 
 void copy_cols(std::int64_t n, int p, const double* x, std::int64_t ldx, double* y, std::int64_t ldy, cudaStream_t s) {
+  note_launches(1);
   k_copy_cols<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, x, ldx, y, ldy);
 }
 
 void residual_cols(std::int64_t n, int p, const double* ax, std::int64_t lda, const double* bx, std::int64_t ldb,
                    const double* lam, double* r, std::int64_t ldr, cudaStream_t s) {
+  note_launches(1);
   k_residual_cols<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, ax, lda, bx, ldb, lam, r, ldr);
 }
 

@@ -1,4 +1,5 @@
 // Host-only C ABI entry points (no GPU needed): status strings, ordering, symbolic statistics.
+#include <atomic>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -10,8 +11,10 @@
 namespace hsg {
 namespace {
 thread_local std::string g_last_error;
-}
+std::atomic<long long> g_launches{0};
+}  // namespace
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+void note_launches(long long count) { g_launches.fetch_add(count, std::memory_order_relaxed); }
 }  // namespace hsg
 
 using namespace hsg;
@@ -35,6 +38,8 @@ const char* hsg_status_string(int status) {
 }
 
 const char* hsg_last_error(void) { return g_last_error.c_str(); }
+
+int64_t hsg_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
 
 void hsg_default_options(hsg_options_t* opt) {
   if (!opt) return;

@@ -11,6 +11,10 @@ struct hsg_solution {
   hsg::SolveOutput out;
 };
 
+struct hsg_session {
+  std::unique_ptr<hsg::Session> impl;
+};
+
 using namespace hsg;
 
 namespace {
@@ -74,6 +78,37 @@ int hsg_eigsolve(int64_t n, const int64_t* a_rowptr, const int32_t* a_col, const
     *out = sol.release();
   });
 }
+
+int hsg_session_create(int64_t n, const int64_t* a_rowptr, const int32_t* a_col, const double* a_val,
+                       const int64_t* b_rowptr, const int32_t* b_col, const double* b_val, int32_t device, uint64_t seed,
+                       hsg_session** out) {
+  return guarded([&] {
+    HSG_REQUIRE(out, HSG_INVALID_INPUT, "hsg_session_create: null output");
+    *out = nullptr;
+    HSG_REQUIRE(n > 0, HSG_INVALID_INPUT, "hsg_session_create: n must be positive");
+    CsrHost a = copy_csr(n, a_rowptr, a_col, a_val, "A");
+    std::unique_ptr<CsrHost> b;
+    if (b_rowptr) b = std::make_unique<CsrHost>(copy_csr(n, b_rowptr, b_col, b_val, "B"));
+    auto s = std::make_unique<hsg_session>();
+    s->impl = std::make_unique<Session>(a, b.get(), device, seed);
+    *out = s.release();
+  });
+}
+
+int hsg_session_solve(hsg_session* s, const hsg_solve_config_t* cfg, hsg_solution** out) {
+  return guarded([&] {
+    HSG_REQUIRE(s && s->impl && out, HSG_INVALID_INPUT, "hsg_session_solve: null argument");
+    *out = nullptr;
+    hsg_solve_config_t c;
+    hsg_default_solve_config(&c);
+    if (cfg) c = *cfg;
+    auto sol = std::make_unique<hsg_solution>();
+    sol->out = s->impl->solve(c, false);
+    *out = sol.release();
+  });
+}
+
+void hsg_session_free(hsg_session* s) { delete s; }
 
 int hsg_solution_sizes(const hsg_solution* s, int64_t* n, int64_t* m) {
   return guarded([&] {

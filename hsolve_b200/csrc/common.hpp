@@ -33,6 +33,9 @@ class Error : public std::runtime_error {
 
 void set_last_error(const std::string& msg);
 
+// Kernel launches issued by this library (exported as hsg_kernel_launches).
+void note_launches(long long count);
+
 // Runs f(), mapping exceptions to status codes and recording the message (C ABI wrapper).
 template <class F>
 int guarded(F&& f) noexcept {

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <map>
+#include <memory>
 #include <sstream>
 
 #include "blas_kernels.cuh"
@@ -256,31 +257,45 @@ int auto_block(int nev) { return nev >= 32 ? 8 : (nev >= 8 ? 4 : (nev >= 3 ? 2 :
 
 }  // namespace
 
-SolveOutput solve_pencil(const CsrHost& a, const CsrHost* b, const hsg_solve_config_t& cfg) {
-  const auto t_start = Clock::now();
-  Timers tm;
+struct Session::Impl {
+  CsrHost a;
+  std::unique_ptr<CsrHost> b;
+  std::unique_ptr<GpuFactor> F;
+  Problem P;
+  std::string problem = "HEP";
+  double scale = 0.0;
+  Timers setup_tm;
+  int device = 0;
+  std::uint64_t seed = 2026;
+};
+
+Session::Session(const CsrHost& a_in, const CsrHost* b_in, int device, std::uint64_t seed) : d_(new Impl) {
+  Impl& S = *d_;
+  S.a = a_in;
+  if (b_in) S.b = std::make_unique<CsrHost>(*b_in);
+  S.device = device;
+  S.seed = seed;
+  const CsrHost& a = S.a;
+  const CsrHost* b = S.b.get();
+  Timers& tm = S.setup_tm;
   const std::int64_t n = a.n;
   HSG_REQUIRE(n > 0, HSG_INVALID_INPUT, "empty matrix");
   HSG_REQUIRE(!b || b->n == n, HSG_INVALID_INPUT, "A and B differ in size");
-  HSG_REQUIRE(cfg.tol > 0.0 && cfg.tol < 1.0, HSG_INVALID_INPUT, "tol outside (0, 1)");
-  HSG_REQUIRE(cfg.mode == 0 || cfg.mode == 1, HSG_UNSUPPORTED, "only 'nearest' and 'interval' targets are served by this build");
-  HSG_REQUIRE(cfg.factor_precision == 0 || cfg.factor_precision == 1, HSG_INVALID_INPUT, "factor_precision");
   hsg_options_t fo;
   hsg_default_options(&fo);
-  fo.device = cfg.device;
-  GpuFactor F(fo);
-  Problem P;
+  fo.device = device;
+  S.F = std::make_unique<GpuFactor>(fo);
+  GpuFactor& F = *S.F;
+  Problem& P = S.P;
   P.n = n;
   P.s = F.stream();
-  cuda_check(cudaSetDevice(cfg.device), "cudaSetDevice");
+  cuda_check(cudaSetDevice(device), "cudaSetDevice");
   upload(P.A, a, P.s);
-  std::string problem = "HEP";
-  std::vector<std::string> warnings;
   if (b) {
     upload(P.B, *b, P.s);
     P.b_identity = false;
     P.b_diagonal = is_diagonal(*b);
-    problem = "GHEP";
+    S.problem = "GHEP";
     if (P.b_diagonal) {
       std::vector<double> d(n, 0.0);
       for (std::int64_t i = 0; i < n; ++i)
@@ -293,15 +308,13 @@ SolveOutput solve_pencil(const CsrHost& a, const CsrHost* b, const hsg_solve_con
       P.normB = mx;
     }
   }
-  // norm estimates (Lanczos lower bounds)
   {
     const auto t0 = Clock::now();
-    P.normA = norm_estimate(P.A.view(n), n, P.s, cfg.seed + 7);
-    if (b && !P.b_diagonal) P.normB = norm_estimate(P.B.view(n), n, P.s, cfg.seed + 11);
+    P.normA = norm_estimate(P.A.view(n), n, P.s, seed + 7);
+    if (b && !P.b_diagonal) P.normB = norm_estimate(P.B.view(n), n, P.s, seed + 11);
     tm.setup += since(t0);
   }
-  const double scale = P.normB > 0 ? P.normA / P.normB : P.normA;
-  // analysis on the pencil's upper pattern
+  S.scale = P.normB > 0 ? P.normA / P.normB : P.normA;
   {
     const auto t0 = Clock::now();
     const CsrHost au = upper_of(a);
@@ -317,6 +330,31 @@ SolveOutput solve_pencil(const CsrHost& a, const CsrHost* b, const hsg_solve_con
     tm.factor += since(t0);
     HSG_REQUIRE(in.valid && in.neg == 0 && in.zero == 0, HSG_UNSUPPORTED, "B is not positive definite (GHIEP): not served by this build");
   }
+}
+
+Session::~Session() = default;
+
+std::int64_t Session::order() const { return d_->a.n; }
+
+SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
+  const auto t_start = Clock::now();
+  Impl& S = *d_;
+  Timers tm;
+  if (include_setup) tm = S.setup_tm;
+  const CsrHost& a = S.a;
+  const CsrHost* b = S.b.get();
+  const std::int64_t n = a.n;
+  HSG_REQUIRE(cfg.tol > 0.0 && cfg.tol < 1.0, HSG_INVALID_INPUT, "tol outside (0, 1)");
+  HSG_REQUIRE(cfg.mode == 0 || cfg.mode == 1, HSG_UNSUPPORTED, "only 'nearest' and 'interval' targets are served by this build");
+  HSG_REQUIRE(cfg.factor_precision == 0 || cfg.factor_precision == 1, HSG_INVALID_INPUT, "factor_precision");
+  HSG_REQUIRE(cfg.device == S.device, HSG_INVALID_INPUT, "config device differs from the session's device");
+  GpuFactor& F = *S.F;
+  Problem& P = S.P;
+  F.reset_device_stats();
+  const long long launches0 = hsg_kernel_launches();
+  const double scale = S.scale;
+  const std::string problem = S.problem;
+  std::vector<std::string> warnings;
   ShiftInvertOp op(P, F);
   SolveOutput out;
   out.n = n;
@@ -544,7 +582,7 @@ SolveOutput solve_pencil(const CsrHost& a, const CsrHost* b, const hsg_solve_con
   j.kv("block_size", block_used);
   j.kv("restarts", restarts);
   j.kv("op_applies", static_cast<long long>(op.columns));
-  const double total = since(t_start);
+  const double total = since(t_start) + (include_setup ? S.setup_tm.setup + S.setup_tm.factor : 0.0);
   j.kv("time_total_s", total);
   j.kv("time_setup_s", tm.setup);
   j.kv("time_factor_s", tm.factor);
@@ -565,6 +603,21 @@ SolveOutput solve_pencil(const CsrHost& a, const CsrHost* b, const hsg_solve_con
   j.kv("delayed_pivots", static_cast<long long>(inr.delayed_pivots));
   j.kv("two_by_two", static_cast<long long>(inr.two_by_two));
   j.close('}');
+  {
+    const GpuFactor::DeviceStats& ds = F.device_stats();
+    j.key("device_timing");
+    j.open('{');
+    j.kv("factorizations", ds.factorizations);
+    j.kv("factor_ms", ds.factor_ms);
+    j.kv("flops_per_factorization", est.flops);
+    j.kv("solves", ds.solves);
+    j.kv("solve_columns", ds.solve_columns);
+    j.kv("solve_ms", ds.solve_ms);
+    j.kv("nnz_l", static_cast<long long>(est.nnz_l));
+    j.kv("n", static_cast<long long>(n));
+    j.kv("kernel_launches", static_cast<long long>(hsg_kernel_launches() - launches0));
+    j.close('}');
+  }
   j.key("precision");
   j.open('{');
   j.kv("requested", std::string(cfg.factor_precision == 1 ? "single" : "double"));
@@ -623,6 +676,11 @@ SolveOutput solve_pencil(const CsrHost& a, const CsrHost* b, const hsg_solve_con
   j.close('}');
   out.report_json = j.os.str();
   return out;
+}
+
+SolveOutput solve_pencil(const CsrHost& a, const CsrHost* b, const hsg_solve_config_t& cfg) {
+  Session s(a, b, cfg.device, cfg.seed);
+  return s.solve(cfg, true);
 }
 
 }  // namespace hsg

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -22,6 +23,22 @@ struct SolveOutput {
   std::vector<double> vectors;  // n x m, column-major
   std::int64_t n = 0;
   std::string report_json;
+};
+
+// A pencil resident on the GPU with its analysis (ordering, symbolic factorization) and norm bounds
+// computed once; solve() serves any number of targets on it (symbolic reuse across shifts).
+class Session {
+ public:
+  Session(const CsrHost& a, const CsrHost* b, int device, std::uint64_t seed);
+  ~Session();
+  Session(const Session&) = delete;
+  Session& operator=(const Session&) = delete;
+  SolveOutput solve(const hsg_solve_config_t& cfg, bool include_setup = false);
+  std::int64_t order() const;
+
+ private:
+  struct Impl;
+  std::unique_ptr<Impl> d_;
 };
 
 SolveOutput solve_pencil(const CsrHost& a, const CsrHost* b, const hsg_solve_config_t& cfg);

@@ -16,6 +16,7 @@
 // (failed) so that the host can move them into the parent front and factorize again.
 #include <cstdint>
 
+#include "common.hpp"
 #include "device.cuh"
 #include "factor_kernels.cuh"
 
@@ -661,12 +662,14 @@ __global__ void __launch_bounds__(kAppThreads) k_front_app(const std::int32_t* l
 void launch_fill(double* x, std::int64_t n, double v, cudaStream_t s) {
   if (n <= 0) return;
   const int blocks = static_cast<int>(std::min<std::int64_t>((n + 255) / 256, 148 * 16));
+  note_launches(1);
   k_fill<<<blocks, 256, 0, s>>>(x, n, v);
 }
 
 void launch_zero_u64(unsigned long long* x, std::int64_t n, cudaStream_t s) {
   if (n <= 0) return;
   const int blocks = static_cast<int>(std::min<std::int64_t>((n + 255) / 256, 148 * 16));
+  note_launches(1);
   k_zero_u64<<<blocks, 256, 0, s>>>(x, n);
 }
 
@@ -674,11 +677,13 @@ void launch_scale_rowmax(std::int64_t nnz, const std::int32_t* row, const std::i
                          const double* b, double alpha, double beta, const double* d, unsigned long long* r,
                          cudaStream_t s) {
   const int blocks = static_cast<int>(std::min<std::int64_t>((nnz + 255) / 256, 148 * 16));
+  note_launches(1);
   k_scale_rowmax<<<blocks, 256, 0, s>>>(nnz, row, col, a, b, alpha, beta, d, r);
 }
 
 void launch_scale_update(std::int64_t n, double* d, unsigned long long* r, cudaStream_t s) {
   const int blocks = static_cast<int>(std::min<std::int64_t>((n + 255) / 256, 148 * 16));
+  note_launches(1);
   k_scale_update<<<blocks, 256, 0, s>>>(n, d, r);
 }
 
@@ -686,18 +691,21 @@ void launch_scatter(std::int64_t nnz, const std::int32_t* row, const std::int32_
                     const double* b, double alpha, double beta, const double* d, const std::int64_t* dest,
                     double* panels, FactorCounters* cnt, cudaStream_t s) {
   const int blocks = static_cast<int>(std::min<std::int64_t>((nnz + 255) / 256, 148 * 16));
+  note_launches(1);
   k_scatter<<<blocks, 256, 0, s>>>(nnz, row, col, a, b, alpha, beta, d, dest, panels, cnt);
 }
 
 void launch_zero_cb(const std::int32_t* list, int nlist, int chunks, const SnDev* sn, double* cb, cudaStream_t s) {
   if (nlist <= 0) return;
   dim3 grid(nlist, chunks);
+  note_launches(1);
   k_zero_cb<<<grid, 256, 0, s>>>(list, sn, cb);
 }
 
 void launch_extend_add(const int2* items, int nitems, const SnDev* sn, const std::int32_t* rmap, double* panels,
                        double* cb, cudaStream_t s) {
   if (nitems <= 0) return;
+  note_launches(1);
   k_extend_add<<<nitems, 128, 0, s>>>(items, sn, rmap, panels, cb);
 }
 
@@ -706,8 +714,8 @@ void launch_front_small(int maxm, const std::int32_t* list, int nlist, const SnD
                         std::int32_t* failed, cudaStream_t s) {
   if (nlist <= 0) return;
   const std::size_t smem = static_cast<std::size_t>(maxm) * maxm * sizeof(double);
-  if (maxm <= 32) k_front_small<32><<<nlist, 128, smem, s>>>(list, sn, panels, cb, piv, pidx, prm, cnt, failed);
-  else k_front_small<kSmallMax><<<nlist, 256, smem, s>>>(list, sn, panels, cb, piv, pidx, prm, cnt, failed);
+  if (maxm <= 32) { note_launches(1); k_front_small<32><<<nlist, 128, smem, s>>>(list, sn, panels, cb, piv, pidx, prm, cnt, failed); }
+  else { note_launches(1); k_front_small<kSmallMax><<<nlist, 256, smem, s>>>(list, sn, panels, cb, piv, pidx, prm, cnt, failed); }
 }
 
 void launch_front_app(const std::int32_t* list, int nlist, const SnDev* sn, double* panels, double* cb,
@@ -720,6 +728,7 @@ void launch_front_app(const std::int32_t* list, int nlist, const SnDev* sn, doub
     cudaFuncSetAttribute(k_front_app, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     configured = true;
   }
+  note_launches(1);
   k_front_app<<<nlist, kAppThreads, smem, s>>>(list, sn, panels, cb, scratch, piv, pidx, prm, cnt, failed);
 }
 

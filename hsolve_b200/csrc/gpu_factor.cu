@@ -81,6 +81,8 @@ GpuFactor::GpuFactor(const hsg_options_t& opt) : opt_(opt) {
   HSG_REQUIRE(opt_.null_pivot_tol > 0.0 && opt_.null_pivot_tol < 1.0, HSG_INVALID_INPUT, "null_pivot_tol outside (0, 1)");
   DeviceGuard g(opt_.device);
   cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  cuda_check(cudaEventCreate(&ev0_), "cudaEventCreate");
+  cuda_check(cudaEventCreate(&ev1_), "cudaEventCreate");
 }
 
 GpuFactor::~GpuFactor() {
@@ -89,6 +91,8 @@ GpuFactor::~GpuFactor() {
     cudaStreamSynchronize(stream_);
     cudaStreamDestroy(stream_);
   }
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
 }
 
 void GpuFactor::analyze(std::int64_t n, const std::int64_t* a_rp, const std::int32_t* a_ci, const double* a_v,
@@ -264,9 +268,17 @@ hsg_inertia_t GpuFactor::factorize(double alpha, double beta, bool detection) {
   int replans = 0;
   std::int64_t delayed = 0;
   for (;;) {
+    cuda_check(cudaEventRecord(ev0_, stream_), "event");
     run_numeric(alpha, beta, detection);
+    cuda_check(cudaEventRecord(ev1_, stream_), "event");
     cuda_check(cudaMemcpyAsync(&c, d_cnt_.p, sizeof(c), cudaMemcpyDeviceToHost, stream_), "counters");
     cuda_check(cudaStreamSynchronize(stream_), "factorization");
+    {
+      float ms = 0.0f;
+      cuda_check(cudaEventElapsedTime(&ms, ev0_, ev1_), "event time");
+      dstats_.factor_ms += ms;
+      dstats_.factorizations += 1;
+    }
     if (c.failed == 0) break;
     HSG_REQUIRE(replans < 16, HSG_FACTORIZATION_FAILED, "delayed pivots could not be placed after " << replans << " re-plans");
     const std::int64_t nf = std::min<std::int64_t>(static_cast<std::int64_t>(c.failed), n_);
@@ -312,6 +324,7 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
     db = d_btmp_.p;
     ld = n_;
   }
+  cuda_check(cudaEventRecord(ev0_, s), "event");
   launch_gather_scale(n_, nr, db, ld, d_scale_.p, d_iperm_.p, d_xwork_.p, s);
   const std::int32_t* lists = d_lists_.p;
   for (const LevelPlan& L : levels_)
@@ -322,12 +335,20 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
     launch_solve_bwd(lists + it->all_off, it->all_n, it->maxm, d_sn_.p, d_rows_.p, d_panels_.p, d_piv_.p, d_pidx_.p,
                      d_xwork_.p, n_, nr, s);
   launch_scatter_scale(n_, nr, db, ld, d_scale_.p, d_iperm_.p, d_xwork_.p, s);
+  cuda_check(cudaEventRecord(ev1_, s), "event");
   cuda_check(cudaGetLastError(), "solve launch");
   if (!on_device) {
     cuda_check(cudaMemcpy2DAsync(b, ldb * sizeof(double), d_btmp_.p, n_ * sizeof(double), n_ * sizeof(double), nr,
                                  cudaMemcpyDeviceToHost, s), "D2H rhs");
   }
   cuda_check(cudaStreamSynchronize(s), "solve");
+  {
+    float ms = 0.0f;
+    cuda_check(cudaEventElapsedTime(&ms, ev0_, ev1_), "event time");
+    dstats_.solve_ms += ms;
+    dstats_.solves += 1;
+    dstats_.solve_columns += nrhs;
+  }
   last_solve_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 

@@ -75,6 +75,16 @@ class GpuFactor {
   const Symbolic& symbolic() const { return sym_; }
   double last_factor_seconds() const { return last_factor_s_; }
   double last_solve_seconds() const { return last_solve_s_; }
+  // Device time (CUDA events on the handle's stream) and counts since the last reset.
+  struct DeviceStats {
+    long long factorizations = 0;  // numeric passes, re-plans included
+    double factor_ms = 0.0;
+    long long solves = 0;
+    long long solve_columns = 0;
+    double solve_ms = 0.0;
+  };
+  const DeviceStats& device_stats() const { return dstats_; }
+  void reset_device_stats() { dstats_ = DeviceStats{}; }
 
  private:
   struct LevelPlan {
@@ -100,6 +110,8 @@ class GpuFactor {
   std::vector<LevelPlan> levels_;
   hsg_inertia_t inertia_{};
   double last_factor_s_ = 0.0, last_solve_s_ = 0.0;
+  DeviceStats dstats_;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   std::int64_t vec_total_ = 0;
 
   DevBuf<std::int32_t> d_row_, d_col_, d_rmap_, d_rows_, d_child_ptr_, d_children_, d_iperm_, d_lists_, d_pidx_,

@@ -9,6 +9,7 @@
 // are carried together so that every L entry is read once per chunk.
 #include <cstdint>
 
+#include "common.hpp"
 #include "device.cuh"
 #include "solve_kernels.cuh"
 
@@ -241,6 +242,7 @@ void launch_gather_scale(std::int64_t n, int nrhs, const double* b, std::int64_t
                          const std::int32_t* iperm, double* x, cudaStream_t s) {
   const std::int64_t total = n * nrhs;
   const int blocks = static_cast<int>(std::min<std::int64_t>((total + 255) / 256, 148 * 16));
+  note_launches(1);
   k_gather_scale<<<blocks, 256, 0, s>>>(n, nrhs, b, ldb, d, iperm, x);
 }
 
@@ -248,6 +250,7 @@ void launch_scatter_scale(std::int64_t n, int nrhs, double* b, std::int64_t ldb,
                           const std::int32_t* iperm, const double* x, cudaStream_t s) {
   const std::int64_t total = n * nrhs;
   const int blocks = static_cast<int>(std::min<std::int64_t>((total + 255) / 256, 148 * 16));
+  note_launches(1);
   k_scatter_scale<<<blocks, 256, 0, s>>>(n, nrhs, b, ldb, d, iperm, x);
 }
 
@@ -273,12 +276,14 @@ void launch_solve_fwd(const std::int32_t* list, int nlist, int maxm, const SnDev
     cudaFuncSetAttribute(k_solve_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSolveSmemMax));
     configured = true;
   }
+  note_launches(1);
   k_solve_fwd<<<nlist, 256, smem, s>>>(list, sn, child_ptr, children, rmap, panels, piv, pidx, x, n, vec, nrhs, R);
 }
 
 void launch_solve_diag(int ns, const SnDev* sn, const double* panels, const signed char* piv,
                        const std::int32_t* pidx, double* x, std::int64_t n, int nrhs, cudaStream_t s) {
   if (ns <= 0) return;
+  note_launches(1);
   k_solve_diag<<<ns, 128, 0, s>>>(sn, panels, piv, pidx, x, n, nrhs);
 }
 
@@ -293,6 +298,7 @@ void launch_solve_bwd(const std::int32_t* list, int nlist, int maxm, const SnDev
     cudaFuncSetAttribute(k_solve_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSolveSmemMax));
     configured = true;
   }
+  note_launches(1);
   k_solve_bwd<<<nlist, 256, smem, s>>>(list, sn, rows, panels, piv, pidx, x, n, nrhs, R);
 }
 

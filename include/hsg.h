@@ -43,6 +43,9 @@ enum {
 HSG_API const char* hsg_status_string(int status);
 /* Message of the last failing call on this thread (empty if none). */
 HSG_API const char* hsg_last_error(void);
+/* Kernel launches this library has issued in the process so far (instrumentation; no counterpart
+ * in hsolve). */
+HSG_API int64_t hsg_kernel_launches(void);
 
 /* ------------------------------------------------------------------------ options, results */
 
@@ -130,6 +133,10 @@ HSG_API int hsg_pivot_order(const hsg_factor* f, int32_t* out);
 
 /* SparseFactorization::order() (factor.hpp:441-442). */
 HSG_API int64_t hsg_order(const hsg_factor* f);
+
+/* Measured FP64 FMA throughput of the device (TFLOP/s), the denominator of the factorization's
+ * roofline (instrumentation; no counterpart in hsolve). */
+HSG_API int hsg_fp64_peak_probe(int32_t device, double* tflops);
 
 /* ----------------------------------------------------------------- host-only (no GPU needed) */
 

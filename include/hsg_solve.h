@@ -48,6 +48,17 @@ HSG_API int hsg_eigsolve(int64_t n, const int64_t* a_rowptr, const int32_t* a_co
                          const int64_t* b_rowptr, const int32_t* b_col, const double* b_val,
                          const hsg_solve_config_t* cfg, hsg_solution** out);
 
+/* A pencil resident on the GPU with its analysis and norm bounds computed once (the serving path:
+ * symbolic analyses and device copies reused across targets and shifts). No counterpart type in
+ * hsolve; hsg_session_solve(s, cfg) returns what hs::solve(A, B, cfg) returns for the session's
+ * pencil. A session is used by one caller at a time. */
+typedef struct hsg_session hsg_session;
+HSG_API int hsg_session_create(int64_t n, const int64_t* a_rowptr, const int32_t* a_col, const double* a_val,
+                               const int64_t* b_rowptr, const int32_t* b_col, const double* b_val, int32_t device,
+                               uint64_t seed, hsg_session** out);
+HSG_API int hsg_session_solve(hsg_session* s, const hsg_solve_config_t* cfg, hsg_solution** out);
+HSG_API void hsg_session_free(hsg_session* s);
+
 /* Solution<double>::eigenvalues.size() and n. */
 HSG_API int hsg_solution_sizes(const hsg_solution* s, int64_t* n, int64_t* m);
 /* Copies eigenvalues (m) and eigenvectors (n x m column-major; NULL to skip). */
