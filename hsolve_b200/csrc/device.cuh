@@ -18,6 +18,7 @@ struct SnDev {
   std::int64_t rmap_off;  // its CB rows' positions in the parent's rows
   std::int64_t vec_off;   // contribution vector (m-k entries per rhs) in the solve arena
   std::int64_t scratch_off;  // pivoting scratch of the panel kernel (doubles)
+  std::int64_t inv_off;      // inverse diagonal blocks (32 x 32 each) of the solve
 };
 
 // Counters written by the factorization kernels (integers: sums are order independent).

@@ -14,6 +14,7 @@
 // (|l| <= 1/u), rejected columns are restored from a backup and moved behind the candidates, and
 // the trailing matrix receives the rank-q update. Columns no candidate order can pivot are reported
 // (failed) so that the host can move them into the parent front and factorize again.
+#include <cooperative_groups.h>
 #include <cstdint>
 
 #include "common.hpp"
@@ -357,6 +358,11 @@ __global__ void __launch_bounds__(256) k_front_small(const std::int32_t* list, c
 }
 
 // ------------------------------------------------------------- larger fronts: a-posteriori pivoting
+//
+// One front is processed by nr CTAs (nr = 1 for the one-CTA-per-front kernel; nr >= 1 per front in the
+// cooperative kernel, where every step is separated by a grid-wide barrier). The pivoting state of a
+// front lives in its global scratch (AppCtrl + block + labels + column maxima + backup), written by
+// the front's rank-0 CTA and read by all its CTAs after the barrier.
 
 namespace {
 
@@ -370,10 +376,53 @@ struct FrontView {
   __device__ double& at(int i, int c) const { return col(c)[i]; }
 };
 
-struct AppShared {
-  int p, lim, prog, force, done, q, w, eb, stop;
-  int neg, pos, zero, two, forced;
+struct AppCtrl {
+  int p, lim, prog, force, stop, w, eb, q;
+  int neg, pos, zero, two, forced, finished, pad0, pad1;
 };
+
+struct AppFront {
+  FrontView f;
+  int first;
+  bool root;
+  AppCtrl* ctrl;
+  double* B;       // factored diagonal block, kNB x kNB col-major
+  double* Borig;   // the block before factorization
+  int* lab;        // block permutation
+  signed char* pv; // block pivot types
+  unsigned long long* cmax;
+  unsigned long long* rmax;
+  double* backup;  // kNB columns of m rows
+  std::int32_t* plab;
+  signed char* ppv;
+};
+
+__device__ AppFront make_front(const SnDev& d, double* panels, double* cb, double* scratch, signed char* piv_out,
+                               std::int32_t* pidx_out) {
+  AppFront F;
+  F.f = FrontView{panels + d.panel_off, d.cb_off >= 0 ? cb + d.cb_off : nullptr, d.m, d.k};
+  F.first = d.first;
+  F.root = d.parent < 0;
+  double* s = scratch + d.scratch_off;
+  F.ctrl = reinterpret_cast<AppCtrl*>(s);
+  s += kAppCtrlDoubles;
+  F.B = s;
+  s += kNB * kNB;
+  F.Borig = s;
+  s += kNB * kNB;
+  F.lab = reinterpret_cast<int*>(s);
+  s += kNB / 2;
+  F.pv = reinterpret_cast<signed char*>(s);
+  s += kNB / 8;
+  F.cmax = reinterpret_cast<unsigned long long*>(s);
+  s += kNB;
+  F.rmax = reinterpret_cast<unsigned long long*>(s);
+  s += kNB;
+  F.backup = s;
+  F.plab = pidx_out + d.first;
+  F.ppv = piv_out + d.first;
+  return F;
+}
 
 // symmetric swap of fully-summed positions a, b (< k) of the front in global memory
 __device__ void front_swap(const FrontView& f, int a, int b, std::int32_t* lab) {
@@ -391,17 +440,235 @@ __device__ void front_swap(const FrontView& f, int a, int b, std::int32_t* lab) 
   if (threadIdx.x == 0) { const std::int32_t t = lab[a]; lab[a] = lab[b]; lab[b] = t; }
 }
 
-// C(i, c) -= sum_{s<q} L(i, p+s) W(c, s) for from <= c <= i < m, W = L D (from the factored block B)
-__device__ void trailing_update(const FrontView& f, int p, int q, int from, const double* B, const signed char* pv,
-                                double* Ls, double* Ws) {
-  const int rows = f.m - from;
+// Init (all ranks split the label work; rank 0 the control block).
+__device__ void app_init(AppFront& F, int rank, int nr) {
+  const int k = F.f.k;
+  for (int t = rank * blockDim.x + threadIdx.x; t < k; t += nr * blockDim.x) { F.plab[t] = t; F.ppv[t] = -1; }
+  if (rank == 0 && threadIdx.x == 0) {
+    AppCtrl c{};
+    c.lim = k;
+    *F.ctrl = c;
+  }
+}
+
+// Rank 0: decide what the next panel is (stop = 1: front finished), and factorize its diagonal block
+// with block-restricted threshold Bunch-Kaufman; permute the L rows of the block; publish to scratch.
+__device__ void app_control_and_block(AppFront& F, const FactorParams& prm, double thr, double* Bs, double* tmp0,
+                                      double* tmp1, int* slab, signed char* spv, StepShared& bst, int* shared_stop,
+                                      FactorCounters* cnt, std::int32_t* failed, int* level_done) {
+  AppCtrl* c = F.ctrl;
+  const int k = F.f.k;
+  if (threadIdx.x == 0) {
+    int stop = 1;
+    if (!c->finished) {
+      while (true) {
+        if (c->p >= k) { stop = 1; break; }
+        if (c->p >= c->lim) {
+          if (c->prog) { c->lim = k; c->prog = 0; continue; }
+          if (F.root && !c->force) { c->force = 1; c->lim = k; continue; }
+          stop = 1;
+          break;
+        }
+        stop = 0;
+        c->w = min(kNB, c->lim - c->p);
+        break;
+      }
+    }
+    c->stop = stop;
+    *shared_stop = stop;
+    if (stop && !c->finished) {
+      c->finished = 1;
+      const int e = c->p;
+      if (c->neg) atomicAdd(&cnt->neg, static_cast<unsigned long long>(c->neg));
+      if (c->pos) atomicAdd(&cnt->pos, static_cast<unsigned long long>(c->pos));
+      if (c->zero) atomicAdd(&cnt->zero, static_cast<unsigned long long>(c->zero));
+      if (c->two) atomicAdd(&cnt->two_by_two, static_cast<unsigned long long>(c->two));
+      if (c->forced) atomicAdd(&cnt->forced, static_cast<unsigned long long>(c->forced));
+      if (e < k) {
+        const unsigned long long at = atomicAdd(&cnt->failed, static_cast<unsigned long long>(k - e));
+        for (int t = e; t < k; ++t)
+          if (at + (t - e) < static_cast<unsigned long long>(prm.failed_cap)) failed[at + (t - e)] = F.first + F.plab[t];
+      }
+      if (level_done) atomicAdd(level_done, 1);
+    }
+  }
+  __syncthreads();
+  if (*shared_stop) return;
+  const int p = c->p, w = c->w;
+  const bool force = c->force != 0;
+  for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
+    const int i = t % w, j = t / w;
+    if (i >= j) {
+      const double v = F.f.at(p + i, p + j);
+      Bs[i + j * kNB] = v;
+      F.Borig[i + j * kNB] = v;
+    }
+  }
+  for (int t = threadIdx.x; t < w; t += blockDim.x) slab[t] = t;
+  __syncthreads();
+  const int eb = dense_bk(Bs, kNB, w, w, force, prm.u, thr, slab, spv, tmp0, tmp1, bst);
+  // permute the L rows p..p+w-1 of the eliminated columns c < p
+  for (int c0 = 0; c0 < p; c0 += blockDim.x / kNB) {
+    const int cc = c0 + threadIdx.x / kNB, a = threadIdx.x % kNB;
+    double v = 0.0;
+    if (cc < p && a < w) v = F.f.at(p + slab[a], cc);
+    __syncthreads();
+    if (cc < p && a < w) F.f.at(p + a, cc) = v;
+    __syncthreads();
+  }
+  {
+    int old = 0;
+    if (threadIdx.x < w) old = F.plab[p + slab[threadIdx.x]];
+    __syncthreads();
+    if (threadIdx.x < w) F.plab[p + threadIdx.x] = old;
+  }
+  for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
+    const int i = t % w, j = t / w;
+    if (i >= j) F.f.at(p + i, p + j) = Bs[i + j * kNB];
+  }
+  for (int t = threadIdx.x; t < kNB * kNB; t += blockDim.x) F.B[t] = Bs[t];
+  for (int t = threadIdx.x; t < kNB; t += blockDim.x) {
+    F.lab[t] = slab[t];
+    F.pv[t] = spv[t];
+    F.cmax[t] = 0ull;
+    F.rmax[t] = 0ull;
+  }
+  if (threadIdx.x == 0) c->eb = eb;
+}
+
+// All ranks: rows [p+w, m) solved against the block (L21 = F21 P L11^-T D^-1), backup, column maxima.
+__device__ void app_rows(AppFront& F, int rank, int nr, double* Bs, int* slab, signed char* spv,
+                         unsigned long long* scm, unsigned long long* srm) {
+  const AppCtrl* c = F.ctrl;
+  const int p = c->p, w = c->w, eb = c->eb, m = F.f.m;
+  for (int t = threadIdx.x; t < kNB * kNB; t += blockDim.x) Bs[t] = F.B[t];
+  for (int t = threadIdx.x; t < kNB; t += blockDim.x) {
+    slab[t] = F.lab[t];
+    spv[t] = F.pv[t];
+    scm[t] = 0ull;
+    srm[t] = 0ull;
+  }
+  __syncthreads();
+  for (int i = p + w + rank * blockDim.x + threadIdx.x; i < m; i += nr * blockDim.x) {
+    double x[kNB], y[kNB];
+#pragma unroll
+    for (int t = 0; t < kNB; ++t) x[t] = t < w ? F.f.at(i, p + t) : 0.0;
+#pragma unroll
+    for (int t = 0; t < kNB; ++t)
+      if (t < w) F.backup[static_cast<std::int64_t>(t) * m + i] = x[t];
+    for (int t = 0; t < w; ++t) {
+      double v = x[slab[t]];
+      const int lim_s = t < eb ? t : eb;
+      for (int s = 0; s < lim_s; ++s) {
+        if (spv[s] == 2 && s + 1 == t) continue;
+        v -= y[s] * Bs[t + s * kNB];
+      }
+      y[t] = v;
+    }
+    for (int t = 0; t < w; ++t) {
+      double out;
+      if (t < eb) {
+        const signed char ty = spv[t];
+        if (ty == 0) out = 0.0;
+        else if (ty == 1) out = y[t] / Bs[t + t * kNB];
+        else if (ty == 2) {
+          const double a = Bs[t + t * kNB], b = Bs[t + 1 + t * kNB], cc = Bs[t + 1 + (t + 1) * kNB];
+          out = (cc * y[t] - b * y[t + 1]) / (a * cc - b * b);
+        } else {
+          const double a = Bs[t - 1 + (t - 1) * kNB], b = Bs[t + (t - 1) * kNB], cc = Bs[t + t * kNB];
+          out = (-b * y[t - 1] + a * y[t]) / (a * cc - b * b);
+        }
+        atomic_max_nonneg(&scm[t], fabs(out));
+        atomic_max_nonneg(&srm[t], fabs(y[t]));
+      } else {
+        out = y[t];
+      }
+      F.f.at(i, p + t) = out;
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < w; t += blockDim.x) {
+    if (scm[t]) atomicMax(&F.cmax[t], scm[t]);
+    if (srm[t]) atomicMax(&F.rmax[t], srm[t]);
+  }
+}
+
+// All ranks: the accepted prefix q (identical in every CTA); rank 0 books the inertia.
+__device__ int app_accept(AppFront& F, int rank, bool force, double thr, double inv_u, int* sq) {
+  const AppCtrl* c = F.ctrl;
+  const int eb = c->eb;
+  if (threadIdx.x == 0) {
+    int q = 0;
+    while (q < eb) {
+      const signed char ty = F.pv[q];
+      const double cm = __longlong_as_double(static_cast<long long>(F.cmax[q]));
+      if (ty == 0) {
+        if (!force && __longlong_as_double(static_cast<long long>(F.rmax[q])) > thr) break;
+        q += 1;
+      } else if (ty == 1) {
+        if (!force && cm > inv_u) break;
+        q += 1;
+      } else {
+        const double cm2 = __longlong_as_double(static_cast<long long>(F.cmax[q + 1]));
+        if (!force && fmax(cm, cm2) > inv_u) break;
+        q += 2;
+      }
+    }
+    *sq = q;
+  }
+  __syncthreads();
+  const int q = *sq;
+  if (rank == 0) {
+    for (int t = threadIdx.x; t < q; t += blockDim.x) F.ppv[c->p + t] = F.pv[t];
+    if (threadIdx.x == 0) {
+      AppCtrl* cw = F.ctrl;
+      cw->q = q;
+      for (int t = 0; t < q; ++t) {
+        const signed char ty = F.pv[t];
+        if (ty == 0) cw->zero++;
+        else if (ty == 1) { if (F.B[t + t * kNB] < 0) cw->neg++; else cw->pos++; }
+        else if (ty == 2) {
+          const double a = F.B[t + t * kNB], b = F.B[t + 1 + t * kNB], cc = F.B[t + 1 + (t + 1) * kNB];
+          const double det = a * cc - b * b;
+          if (det < 0) { cw->neg++; cw->pos++; } else if (a + cc < 0) cw->neg += 2; else cw->pos += 2;
+          cw->two++;
+        }
+      }
+      if (force) cw->forced += q;
+    }
+  }
+  return q;
+}
+
+// All ranks: restore the rejected block columns [q, w) from the backup / original block.
+__device__ void app_restore(AppFront& F, int rank, int nr, int q) {
+  const AppCtrl* c = F.ctrl;
+  const int p = c->p, w = c->w, m = F.f.m;
+  for (int i = p + w + rank * blockDim.x + threadIdx.x; i < m; i += nr * blockDim.x)
+    for (int t = q; t < w; ++t) F.f.at(i, p + t) = F.backup[static_cast<std::int64_t>(F.lab[t]) * m + i];
+  if (rank == 0) {
+    for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
+      const int a = t % w, b = t / w;
+      if (b >= q && a >= b) {
+        const int la = F.lab[a], lb = F.lab[b];
+        F.f.at(p + a, p + b) = la >= lb ? F.Borig[la + lb * kNB] : F.Borig[lb + la * kNB];
+      }
+    }
+  }
+}
+
+// All ranks: C(i, c) -= sum_{s<q} L(i, p+s) W(c, s), from <= c <= i < m, W = L D; 64 x 64 tiles
+// of the lower triangle dealt round-robin to the ranks; 4 x 4 outputs per thread.
+__device__ void app_update(AppFront& F, int rank, int nr, int q, double* Ls, double* Ws, const double* Bs,
+                           const signed char* spv) {
+  const AppCtrl* c = F.ctrl;
+  const int p = c->p, from = p + q, m = F.f.m;
+  const int rows = m - from;
   if (rows <= 0 || q <= 0) return;
   const int nt = (rows + kTile - 1) / kTile;
   const int ntiles = nt * (nt + 1) / 2;
-  const int tr = threadIdx.x % kTile;        // row within tile
-  const int cg = threadIdx.x / kTile;        // column group (kTile / kColsPerThread groups)
-  for (int tile = 0; tile < ntiles; ++tile) {
-    // tile -> (ti, tj), ti >= tj
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  for (int tile = rank; tile < ntiles; tile += nr) {
     int ti = static_cast<int>((sqrt(8.0 * tile + 1.0) - 1.0) * 0.5);
     while ((ti + 1) * (ti + 2) / 2 <= tile) ++ti;
     while (ti * (ti + 1) / 2 > tile) --ti;
@@ -410,250 +677,156 @@ __device__ void trailing_update(const FrontView& f, int p, int q, int from, cons
     __syncthreads();
     for (int t = threadIdx.x; t < q * kTile; t += blockDim.x) {
       const int s = t / kTile, r = t % kTile;
-      const int i = i0 + r, c = j0 + r;
-      Ls[s * kTile + r] = i < f.m ? f.at(i, p + s) : 0.0;
-      double w = 0.0;
-      if (c < f.m) {
-        const signed char ty = pv[s];
-        if (ty == 1) w = f.at(c, p + s) * B[s * kNB + s];
-        else if (ty == 2) w = f.at(c, p + s) * B[s * kNB + s] + f.at(c, p + s + 1) * B[s * kNB + s + 1];
-        else if (ty == 3) w = f.at(c, p + s - 1) * B[(s - 1) * kNB + s] + f.at(c, p + s) * B[s * kNB + s];
+      const int i = i0 + r, cc = j0 + r;
+      Ls[s * kTile + r] = i < m ? F.f.at(i, p + s) : 0.0;
+      double wv = 0.0;
+      if (cc < m) {
+        const signed char tyv = spv[s];
+        if (tyv == 1) wv = F.f.at(cc, p + s) * Bs[s * kNB + s];
+        else if (tyv == 2) wv = F.f.at(cc, p + s) * Bs[s * kNB + s] + F.f.at(cc, p + s + 1) * Bs[s * kNB + s + 1];
+        else if (tyv == 3) wv = F.f.at(cc, p + s - 1) * Bs[(s - 1) * kNB + s] + F.f.at(cc, p + s) * Bs[s * kNB + s];
       }
-      Ws[s * kTile + r] = w;
+      Ws[s * kTile + r] = wv;
     }
     __syncthreads();
-    double acc[kColsPerThread];
+    double acc[4][4];
 #pragma unroll
-    for (int b = 0; b < kColsPerThread; ++b) acc[b] = 0.0;
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
     for (int s = 0; s < q; ++s) {
-      const double l = Ls[s * kTile + tr];
-      const double* wr = Ws + s * kTile + cg * kColsPerThread;
+      double l[4], wv[4];
 #pragma unroll
-      for (int b = 0; b < kColsPerThread; ++b) acc[b] = fma(l, wr[b], acc[b]);
+      for (int a = 0; a < 4; ++a) l[a] = Ls[s * kTile + tx + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) wv[b] = Ws[s * kTile + ty + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(l[a], wv[b], acc[a][b]);
     }
-    const int i = i0 + tr;
-    if (i < f.m) {
 #pragma unroll
-      for (int b = 0; b < kColsPerThread; ++b) {
-        const int c = j0 + cg * kColsPerThread + b;
-        if (c <= i) f.at(i, c) -= acc[b];
+    for (int b = 0; b < 4; ++b) {
+      const int cc = j0 + ty + 16 * b;
+      if (cc >= m) continue;
+      double* colp = F.f.col(cc);
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int i = i0 + tx + 16 * a;
+        if (i < m && cc <= i) colp[i] -= acc[a][b];
       }
     }
+  }
+}
+
+// Rank 0: advance past the accepted pivots; move rejected columns behind the candidates.
+__device__ void app_advance(AppFront& F, int q) {
+  AppCtrl* c = F.ctrl;
+  const int p = c->p, w = c->w;
+  const int np = p + q, r = w - q;
+  const int lim = c->lim;
+  if (r > 0 && np + r < lim) {
+    for (int t = 0; t < r; ++t) {
+      front_swap(F.f, np + t, lim - r + t, F.plab);
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    c->p = np;
+    if (q > 0) { c->prog = 1; c->force = 0; }
+    if (r > 0) c->lim = np + r < lim ? lim - r : np;
   }
   __syncthreads();
 }
 
+struct AppSmem {
+  double Bs[kNB * kNB];
+  double tmp0[kNB], tmp1[kNB];
+  int slab[kNB];
+  signed char spv[kNB];
+  unsigned long long scm[kNB], srm[kNB];
+  StepShared bst;
+  int stop, q;
+};
+
 }  // namespace
 
+// One CTA per front (nr = 1), fronts listed in `list`.
 __global__ void __launch_bounds__(kAppThreads) k_front_app(const std::int32_t* list, const SnDev* sn, double* panels,
                                                            double* cb, double* scratch, signed char* piv_out,
                                                            std::int32_t* pidx_out, FactorParams prm,
                                                            FactorCounters* cnt, std::int32_t* failed) {
-  __shared__ double B[kNB * kNB];      // factored diagonal block (col-major, ld kNB)
-  __shared__ double Borig[kNB * kNB];  // the block before factorization
-  __shared__ double tmp0[kNB], tmp1[kNB];
-  extern __shared__ double app_dyn[];  // trailing-update tiles: Ls, Ws (kNB x kTile each)
+  extern __shared__ double app_dyn[];
   double* Ls = app_dyn;
   double* Ws = app_dyn + kNB * kTile;
-  __shared__ int lab[kNB];
-  __shared__ signed char pv[kNB];
-  __shared__ unsigned long long cmax[kNB], rmax[kNB];
-  __shared__ StepShared bst;
-  __shared__ AppShared st;
+  __shared__ AppSmem sm;
   const SnDev d = sn[list[blockIdx.x]];
-  const int m = d.m, k = d.k;
-  FrontView f{panels + d.panel_off, d.cb_off >= 0 ? cb + d.cb_off : nullptr, m, k};
-  double* backup = scratch + d.scratch_off;  // kNB columns of m rows
-  std::int32_t* plab = pidx_out + d.first;
-  signed char* ppv = piv_out + d.first;
-  const bool root = d.parent < 0;
+  AppFront F = make_front(d, panels, cb, scratch, piv_out, pidx_out);
   const double thr = null_threshold(prm);
   const double inv_u = 1.0 / prm.u;
-  for (int t = threadIdx.x; t < k; t += blockDim.x) { plab[t] = t; ppv[t] = -1; }
-  if (threadIdx.x == 0) {
-    st.p = 0; st.lim = k; st.prog = 0; st.force = 0; st.done = 0;
-    st.neg = st.pos = st.zero = st.two = st.forced = 0;
-  }
+  app_init(F, 0, 1);
   __syncthreads();
   while (true) {
-    if (threadIdx.x == 0) {
-      st.stop = 0;
-      if (st.p >= k) st.stop = 1;
-      else if (st.p >= st.lim) {
-        if (st.prog) { st.lim = k; st.prog = 0; st.stop = 2; }
-        else if (root && !st.force) { st.force = 1; st.lim = k; st.stop = 2; }
-        else st.stop = 1;
-      }
-      st.w = min(kNB, st.lim - st.p);
-    }
+    app_control_and_block(F, prm, thr, sm.Bs, sm.tmp0, sm.tmp1, sm.slab, sm.spv, sm.bst, &sm.stop, cnt, failed, nullptr);
     __syncthreads();
-    if (st.stop == 1) break;
-    if (st.stop == 2) continue;
-    const int p = st.p, w = st.w;
-    const bool force = st.force != 0;
-    // ---- step A: factorize the diagonal block with block-restricted threshold pivoting
-    for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
-      const int i = t % w, j = t / w;
-      if (i >= j) {
-        const double v = f.at(p + i, p + j);
-        B[i + j * kNB] = v;
-        Borig[i + j * kNB] = v;
-      }
-    }
-    for (int t = threadIdx.x; t < w; t += blockDim.x) lab[t] = t;
+    if (sm.stop) break;
+    app_rows(F, 0, 1, sm.Bs, sm.slab, sm.spv, sm.scm, sm.srm);
     __syncthreads();
-    const int eb = dense_bk(B, kNB, w, w, force, prm.u, thr, lab, pv, tmp0, tmp1, bst);
-    // block-restricted force accepts everything the block can pivot
-    for (int t = threadIdx.x; t < kNB; t += blockDim.x) { cmax[t] = 0ull; rmax[t] = 0ull; }
-    // permute the L rows p..p+w-1 of the eliminated columns c < p, and the labels
+    const bool force = F.ctrl->force != 0;
+    const int q = app_accept(F, 0, force, thr, inv_u, &sm.q);
     __syncthreads();
-    for (int c0 = 0; c0 < p; c0 += blockDim.x / kNB) {
-      const int c = c0 + threadIdx.x / kNB, a = threadIdx.x % kNB;
-      double v = 0.0;
-      if (c < p && a < w) v = f.at(p + lab[a], c);
-      __syncthreads();
-      if (c < p && a < w) f.at(p + a, c) = v;
-      __syncthreads();
-    }
-    {
-      int old = 0;
-      if (threadIdx.x < w) old = plab[p + lab[threadIdx.x]];
-      __syncthreads();
-      if (threadIdx.x < w) plab[p + threadIdx.x] = old;
-    }
-    for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
-      const int i = t % w, j = t / w;
-      if (i >= j) f.at(p + i, p + j) = B[i + j * kNB];
-    }
+    if (q < F.ctrl->w) app_restore(F, 0, 1, q);
     __syncthreads();
-    // ---- step B: rows below the block: L21 = F21 P L11^-T D^-1, column maxima, backup
-    for (int i = p + w + threadIdx.x; i < m; i += blockDim.x) {
-      double x[kNB], y[kNB];
-#pragma unroll
-      for (int t = 0; t < kNB; ++t) x[t] = t < w ? f.at(i, p + t) : 0.0;
-#pragma unroll
-      for (int t = 0; t < kNB; ++t)
-        if (t < w) backup[static_cast<std::int64_t>(t) * m + i] = x[t];
-#pragma unroll
-      for (int t = 0; t < kNB; ++t) {
-        if (t >= w) break;
-        double v = x[lab[t]];
-        const int lim_s = t < eb ? t : eb;
-        for (int s = 0; s < lim_s; ++s) {
-          if (pv[s] == 2 && s + 1 == t) continue;  // inside a 2x2 block: no L entry
-          v -= y[s] * B[t + s * kNB];
-        }
-        y[t] = v;
-      }
-      for (int t = 0; t < w; ++t) {
-        double out;
-        if (t < eb) {
-          const signed char ty = pv[t];
-          if (ty == 0) out = 0.0;
-          else if (ty == 1) out = y[t] / B[t + t * kNB];
-          else if (ty == 2) {
-            const double a = B[t + t * kNB], b = B[t + 1 + t * kNB], c = B[t + 1 + (t + 1) * kNB];
-            const double det = a * c - b * b;
-            out = (c * y[t] - b * y[t + 1]) / det;
-          } else {
-            const double a = B[t - 1 + (t - 1) * kNB], b = B[t + (t - 1) * kNB], c = B[t + t * kNB];
-            const double det = a * c - b * b;
-            out = (-b * y[t - 1] + a * y[t]) / det;
-          }
-          atomic_max_nonneg(&cmax[t], fabs(out));
-          atomic_max_nonneg(&rmax[t], fabs(y[t]));
-        } else {
-          out = y[t];
-        }
-        f.at(i, p + t) = out;
-      }
-    }
+    app_update(F, 0, 1, q, Ls, Ws, sm.Bs, sm.spv);
     __syncthreads();
-    // ---- step C: accepted prefix
-    if (threadIdx.x == 0) {
-      int q = 0;
-      while (q < eb) {
-        const signed char ty = pv[q];
-        const double cm = __longlong_as_double(static_cast<long long>(cmax[q]));
-        if (ty == 0) {
-          if (!force && __longlong_as_double(static_cast<long long>(rmax[q])) > thr) break;
-          q += 1;
-        } else if (ty == 1) {
-          if (!force && cm > inv_u) break;
-          q += 1;
-        } else {
-          const double cm2 = __longlong_as_double(static_cast<long long>(cmax[q + 1]));
-          if (!force && fmax(cm, cm2) > inv_u) break;
-          q += 2;
-        }
-      }
-      st.q = q;
-      st.eb = eb;
-      // inertia of the accepted pivots
-      for (int t = 0; t < q; ++t) {
-        const signed char ty = pv[t];
-        if (ty == 0) st.zero++;
-        else if (ty == 1) { if (B[t + t * kNB] < 0) st.neg++; else st.pos++; }
-        else if (ty == 2) {
-          const double a = B[t + t * kNB], b = B[t + 1 + t * kNB], c = B[t + 1 + (t + 1) * kNB];
-          const double det = a * c - b * b;
-          if (det < 0) { st.neg++; st.pos++; } else if (a + c < 0) st.neg += 2; else st.pos += 2;
-          st.two++;
-        }
-      }
-      if (force) st.forced += q;
-    }
-    __syncthreads();
-    const int q = st.q;
-    for (int t = threadIdx.x; t < q; t += blockDim.x) ppv[p + t] = pv[t];
-    if (q < w) {
-      // restore rejected columns [q, w) (in block order) from the backup / original block
-      for (int i = p + w + threadIdx.x; i < m; i += blockDim.x)
-        for (int t = q; t < w; ++t) f.at(i, p + t) = backup[static_cast<std::int64_t>(lab[t]) * m + i];
-      for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
-        const int a = t % w, b = t / w;
-        if (b >= q && a >= b) {
-          const int la = lab[a], lb = lab[b];
-          f.at(p + a, p + b) = la >= lb ? Borig[la + lb * kNB] : Borig[lb + la * kNB];
-        }
-      }
-    }
-    __syncthreads();
-    // ---- step D: trailing update with the q accepted pivots
-    trailing_update(f, p, q, p + q, B, pv, Ls, Ws);
-    // ---- step E: advance; move rejected columns behind the candidates
-    if (threadIdx.x == 0) {
-      st.p = p + q;
-      if (q > 0) { st.prog = 1; st.force = 0; }
-    }
-    __syncthreads();
-    const int r = w - q;
-    if (r > 0) {
-      const int np = st.p, lim = st.lim;
-      if (np + r < lim) {
-        for (int t = 0; t < r; ++t) {
-          front_swap(f, np + t, lim - r + t, plab);
-          __syncthreads();
-        }
-        if (threadIdx.x == 0) st.lim = lim - r;
-      } else {
-        if (threadIdx.x == 0) st.lim = np;
-      }
-      __syncthreads();
-    }
+    app_advance(F, q);
   }
-  if (threadIdx.x == 0) {
-    const int e = st.p;
-    if (st.neg) atomicAdd(&cnt->neg, static_cast<unsigned long long>(st.neg));
-    if (st.pos) atomicAdd(&cnt->pos, static_cast<unsigned long long>(st.pos));
-    if (st.zero) atomicAdd(&cnt->zero, static_cast<unsigned long long>(st.zero));
-    if (st.two) atomicAdd(&cnt->two_by_two, static_cast<unsigned long long>(st.two));
-    if (st.forced) atomicAdd(&cnt->forced, static_cast<unsigned long long>(st.forced));
-    if (e < k) {
-      const unsigned long long at = atomicAdd(&cnt->failed, static_cast<unsigned long long>(k - e));
-      for (int t = e; t < k; ++t)
-        if (at + (t - e) < static_cast<unsigned long long>(prm.failed_cap)) failed[at + (t - e)] = d.first + plab[t];
+}
+
+// Cooperative: the fronts of a level share the grid; front f owns CTAs [cta_start[f], cta_start[f+1]).
+// Grid-wide barriers separate the steps; the loop ends when every front has finished (level_done).
+__global__ void __launch_bounds__(kAppThreads) k_front_coop(const std::int32_t* list, const std::int32_t* cta_start,
+                                                            int nfronts, const SnDev* sn, double* panels, double* cb,
+                                                            double* scratch, signed char* piv_out,
+                                                            std::int32_t* pidx_out, FactorParams prm,
+                                                            FactorCounters* cnt, std::int32_t* failed,
+                                                            int* level_done) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ double app_dyn[];
+  double* Ls = app_dyn;
+  double* Ws = app_dyn + kNB * kTile;
+  __shared__ AppSmem sm;
+  int fi = 0;
+  while (fi + 1 < nfronts && cta_start[fi + 1] <= static_cast<int>(blockIdx.x)) ++fi;
+  const int rank = static_cast<int>(blockIdx.x) - cta_start[fi];
+  const int nr = cta_start[fi + 1] - cta_start[fi];
+  const SnDev d = sn[list[fi]];
+  AppFront F = make_front(d, panels, cb, scratch, piv_out, pidx_out);
+  const double thr = null_threshold(prm);
+  const double inv_u = 1.0 / prm.u;
+  app_init(F, rank, nr);
+  grid.sync();
+  while (true) {
+    if (rank == 0) {
+      app_control_and_block(F, prm, thr, sm.Bs, sm.tmp0, sm.tmp1, sm.slab, sm.spv, sm.bst, &sm.stop, cnt, failed,
+                            level_done);
     }
+    grid.sync();
+    if (*reinterpret_cast<volatile int*>(level_done) >= nfronts) break;
+    const bool active = F.ctrl->stop == 0;
+    if (active) app_rows(F, rank, nr, sm.Bs, sm.slab, sm.spv, sm.scm, sm.srm);
+    grid.sync();
+    int q = 0;
+    if (active) {
+      q = app_accept(F, rank, F.ctrl->force != 0, thr, inv_u, &sm.q);
+      if (q < F.ctrl->w) app_restore(F, rank, nr, q);
+    }
+    grid.sync();
+    if (active) app_update(F, rank, nr, q, Ls, Ws, sm.Bs, sm.spv);
+    grid.sync();
+    if (active && rank == 0) app_advance(F, q);
   }
 }
 
@@ -730,6 +903,28 @@ void launch_front_app(const std::int32_t* list, int nlist, const SnDev* sn, doub
   }
   note_launches(1);
   k_front_app<<<nlist, kAppThreads, smem, s>>>(list, sn, panels, cb, scratch, piv, pidx, prm, cnt, failed);
+}
+
+int coop_max_ctas(int device) {
+  constexpr std::size_t smem = 2 * kNB * kTile * sizeof(double);
+  cudaFuncSetAttribute(k_front_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  int per_sm = 0, sms = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_front_coop, kAppThreads, smem);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  return per_sm * sms;
+}
+
+cudaError_t launch_front_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
+                              const SnDev* sn, double* panels, double* cb, double* scratch, signed char* piv,
+                              std::int32_t* pidx, const FactorParams& prm, FactorCounters* cnt, std::int32_t* failed,
+                              int* level_done, cudaStream_t s) {
+  if (nfronts <= 0) return cudaSuccess;
+  constexpr std::size_t smem = 2 * kNB * kTile * sizeof(double);
+  FactorParams p = prm;
+  void* args[] = {const_cast<std::int32_t**>(&list), const_cast<std::int32_t**>(&cta_start), &nfronts,
+                  const_cast<SnDev**>(&sn), &panels, &cb, &scratch, &piv, &pidx, &p, &cnt, &failed, &level_done};
+  note_launches(1);
+  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_front_coop), dim3(nctas), dim3(kAppThreads), args, smem, s);
 }
 
 }  // namespace hsg

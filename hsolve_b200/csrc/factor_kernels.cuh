@@ -12,8 +12,15 @@ constexpr int kSmallMax = 64;          // fronts up to this order are factorized
 constexpr int kNB = 32;                // panel width of the a-posteriori pivoting kernel
 constexpr int kTile = 64;              // trailing-update tile (rows = cols)
 constexpr int kAppThreads = 256;
+constexpr int kCoopMinFront = 192;     // levels whose largest panel front is at least this use the cooperative kernel
 constexpr int kColsPerThread = kTile * kTile / kAppThreads;  // 16
 constexpr int kExtendAddCols = 8;      // contribution-block columns per extend-add CTA
+// per-front scratch of the panel kernels (doubles): control block, block, original block, labels,
+// pivot types, column maxima, backup of the panel's rows
+constexpr int kAppCtrlDoubles = 8;
+inline std::int64_t app_scratch_doubles(int m) {
+  return kAppCtrlDoubles + 2 * kNB * kNB + kNB / 2 + kNB / 8 + 2 * kNB + static_cast<std::int64_t>(m) * kNB;
+}
 
 void launch_fill(double* x, std::int64_t n, double v, cudaStream_t s);
 void launch_zero_u64(unsigned long long* x, std::int64_t n, cudaStream_t s);
@@ -33,5 +40,12 @@ void launch_front_small(int maxm, const std::int32_t* list, int nlist, const SnD
 void launch_front_app(const std::int32_t* list, int nlist, const SnDev* sn, double* panels, double* cb,
                       double* scratch, signed char* piv, std::int32_t* pidx, const FactorParams& prm,
                       FactorCounters* cnt, std::int32_t* failed, cudaStream_t s);
+
+// cooperative launch over the large fronts of a level (see factor_kernels.cu)
+int coop_max_ctas(int device);
+cudaError_t launch_front_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
+                              const SnDev* sn, double* panels, double* cb, double* scratch, signed char* piv,
+                              std::int32_t* pidx, const FactorParams& prm, FactorCounters* cnt, std::int32_t* failed,
+                              int* level_done, cudaStream_t s);
 
 }  // namespace hsg

@@ -143,7 +143,7 @@ void GpuFactor::build_plan() {
   const Symbolic& S = sym_;
   const std::int32_t ns = S.ns;
   std::vector<SnDev> sn(ns);
-  std::int64_t vec = 0;
+  std::int64_t vec = 0, inv_total = 0;
   for (std::int32_t s = 0; s < ns; ++s) {
     SnDev& d = sn[s];
     d.first = S.first[s];
@@ -157,8 +157,15 @@ void GpuFactor::build_plan() {
     d.vec_off = vec;
     vec += d.m - d.k;
     d.scratch_off = 0;
+    d.inv_off = inv_total;
+    inv_total += static_cast<std::int64_t>((d.k + 30) / 31 + 1) * 1024;
   }
   vec_total_ = vec;
+  if (coop_max_ == 0) coop_max_ = coop_max_ctas(opt_.device);
+  if (solve_coop_max_ == 0) solve_coop_max_ = solve_coop_max_ctas(opt_.device);
+  std::vector<std::int64_t> work_offs;
+  std::int64_t work_max = 0;
+  ncoop_ = 0;
   std::vector<std::int32_t> lists;
   std::vector<int2> items;
   levels_.assign(S.nlevels, LevelPlan{});
@@ -179,7 +186,7 @@ void GpuFactor::build_plan() {
       else {
         app.push_back(s);
         sn[s].scratch_off = scratch;
-        scratch += static_cast<std::int64_t>(m) * kNB;
+        scratch += app_scratch_doubles(m);
       }
     }
     scratch_max = std::max(scratch_max, scratch);
@@ -193,6 +200,82 @@ void GpuFactor::build_plan() {
     put(s64, L.s64_off, L.s64_n);
     put(app, L.app_off, L.app_n);
     put(all, L.all_off, L.all_n);
+    // solves: cooperative sweeps when the level's fronts fit the co-resident grid
+    if (!all.empty() && static_cast<int>(all.size()) <= solve_coop_max_ / 2) {
+      std::vector<double> wts(all.size());
+      double wsum = 0.0;
+      int steps = 0;
+      std::int64_t wofs = 0;
+      L.work_off_off = static_cast<std::int64_t>(work_offs.size());
+      for (std::size_t q = 0; q < all.size(); ++q) {
+        const SnDev& dd = sn[all[q]];
+        wts[q] = static_cast<double>(dd.m) * dd.k;
+        wsum += wts[q];
+        steps = std::max(steps, (dd.k + 30) / 31);
+        work_offs.push_back(wofs);
+        wofs += 8 * static_cast<std::int64_t>(dd.m) + dd.k / 2 + 2;
+      }
+      work_max = std::max(work_max, wofs);
+      std::vector<int> nr(all.size());
+      int total = 0;
+      for (std::size_t q = 0; q < all.size(); ++q) {
+        // about 32k panel entries per CTA
+        nr[q] = static_cast<int>(std::max(1.0, std::min<double>(std::ceil(wts[q] / 32768.0), solve_coop_max_)));
+        total += nr[q];
+      }
+      if (total > solve_coop_max_) {
+        const int spare = solve_coop_max_ - static_cast<int>(all.size());
+        total = 0;
+        for (std::size_t q = 0; q < all.size(); ++q) {
+          nr[q] = 1 + static_cast<int>(std::floor(spare * wts[q] / wsum));
+          total += nr[q];
+        }
+      }
+      std::vector<std::int32_t> starts(all.size() + 1, 0);
+      for (std::size_t q = 0; q < all.size(); ++q) starts[q + 1] = starts[q] + nr[q];
+      L.solve_coop = true;
+      L.solve_cta_off = static_cast<std::int64_t>(lists.size());
+      lists.insert(lists.end(), starts.begin(), starts.end());
+      L.solve_ctas = starts.back();
+      L.solve_steps = steps;
+    }
+    // cooperative launch when the level's panel fronts fit the co-resident grid
+    if (!app.empty() && static_cast<int>(app.size()) <= coop_max_) {
+      int mmax = 0;
+      for (std::int32_t s : app) mmax = std::max(mmax, sn[s].m);
+      if (mmax >= kCoopMinFront) {
+        std::vector<double> wts(app.size());
+        double wsum = 0.0;
+        for (std::size_t q = 0; q < app.size(); ++q) {
+          const double m = sn[app[q]].m;
+          wts[q] = m * m;
+          wsum += wts[q];
+        }
+        std::vector<int> nr(app.size());
+        int total = 0;
+        for (std::size_t q = 0; q < app.size(); ++q) {
+          // about 8 tiles of 64 x 64 per CTA at the first panel
+          const double want = std::ceil(wts[q] / (2.0 * 64 * 64 * 8));
+          nr[q] = static_cast<int>(std::max(1.0, std::min<double>(want, coop_max_)));
+          total += nr[q];
+        }
+        if (total > coop_max_) {
+          const int spare = coop_max_ - static_cast<int>(app.size());
+          total = 0;
+          for (std::size_t q = 0; q < app.size(); ++q) {
+            nr[q] = 1 + static_cast<int>(std::floor(spare * wts[q] / wsum));
+            total += nr[q];
+          }
+        }
+        std::vector<std::int32_t> starts(app.size() + 1, 0);
+        for (std::size_t q = 0; q < app.size(); ++q) starts[q + 1] = starts[q] + nr[q];
+        L.coop = true;
+        L.cta_off = static_cast<std::int64_t>(lists.size());
+        lists.insert(lists.end(), starts.begin(), starts.end());
+        L.coop_ctas = starts.back();
+        L.done_slot = ncoop_++;
+      }
+    }
     L.maxm = maxm;
     L.zero_chunks = static_cast<int>(std::max<std::int64_t>(1, std::min<std::int64_t>(64, (maxcb + 4095) / 4096)));
     // extend-add items by child rank
@@ -227,11 +310,20 @@ void GpuFactor::build_plan() {
   d_panels_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, S.factor_entries)));
   d_cb_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, S.cb_arena)));
   d_scratch_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, scratch_max)));
+  d_level_done_.alloc(static_cast<std::size_t>(std::max(1, ncoop_)));
+  d_inv_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, inv_total)));
+  d_work_off_.upload(work_offs, stream_);
+  d_work_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, work_max)));
+  d_blk_.alloc(static_cast<std::size_t>(n_));
+  d_nblk_.alloc(static_cast<std::size_t>(std::max(1, ns)));
+  for (std::int32_t s = 0; s < ns; ++s)
+    HSG_REQUIRE((sn[s].k + 30) / 31 <= kMaxBlocksPerFront, HSG_UNSUPPORTED, "front with " << sn[s].k << " pivots exceeds the solve block table");
 }
 
 void GpuFactor::run_numeric(double alpha, double beta, bool detection) {
   cudaStream_t s = stream_;
   cuda_check(cudaMemsetAsync(d_cnt_.p, 0, sizeof(FactorCounters), s), "memset counters");
+  cuda_check(cudaMemsetAsync(d_level_done_.p, 0, d_level_done_.n * sizeof(int), s), "memset level flags");
   launch_fill(d_scale_.p, n_, 1.0, s);
   if (opt_.scaling) {
     cuda_check(cudaMemsetAsync(d_r_.p, 0, n_ * sizeof(unsigned long long), s), "memset r");
@@ -253,8 +345,16 @@ void GpuFactor::run_numeric(double alpha, double beta, bool detection) {
     for (const auto& ea : L.ea) launch_extend_add(d_items_.p + ea.first, ea.second, d_sn_.p, d_rmap_.p, d_panels_.p, d_cb_.p, s);
     launch_front_small(32, lists + L.s32_off, L.s32_n, d_sn_.p, d_panels_.p, d_cb_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
     launch_front_small(kSmallMax, lists + L.s64_off, L.s64_n, d_sn_.p, d_panels_.p, d_cb_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
-    launch_front_app(lists + L.app_off, L.app_n, d_sn_.p, d_panels_.p, d_cb_.p, d_scratch_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
+    if (L.coop) {
+      cuda_check(launch_front_coop(lists + L.app_off, lists + L.cta_off, L.app_n, L.coop_ctas, d_sn_.p, d_panels_.p,
+                                   d_cb_.p, d_scratch_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p,
+                                   d_level_done_.p + L.done_slot, s),
+                 "cooperative front launch");
+    } else {
+      launch_front_app(lists + L.app_off, L.app_n, d_sn_.p, d_panels_.p, d_cb_.p, d_scratch_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
+    }
   }
+  launch_inv_blocks(sym_.ns, d_sn_.p, d_panels_.p, d_piv_.p, d_blk_.p, d_nblk_.p, d_inv_.p, s);
   cuda_check(cudaGetLastError(), "factorization launch");
 }
 
@@ -327,13 +427,35 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
   cuda_check(cudaEventRecord(ev0_, s), "event");
   launch_gather_scale(n_, nr, db, ld, d_scale_.p, d_iperm_.p, d_xwork_.p, s);
   const std::int32_t* lists = d_lists_.p;
-  for (const LevelPlan& L : levels_)
-    launch_solve_fwd(lists + L.all_off, L.all_n, L.maxm, d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p,
-                     d_panels_.p, d_piv_.p, d_pidx_.p, d_xwork_.p, n_, d_vec_.p, nr, s);
-  launch_solve_diag(sym_.ns, d_sn_.p, d_panels_.p, d_piv_.p, d_pidx_.p, d_xwork_.p, n_, nr, s);
-  for (auto it = levels_.rbegin(); it != levels_.rend(); ++it)
-    launch_solve_bwd(lists + it->all_off, it->all_n, it->maxm, d_sn_.p, d_rows_.p, d_panels_.p, d_piv_.p, d_pidx_.p,
-                     d_xwork_.p, n_, nr, s);
+  // chunks of at most 8 right-hand sides (the cooperative sweeps carry 8)
+  for (int c0 = 0; c0 < nr; c0 += 8) {
+    const int nc = std::min(8, nr - c0);
+    double* xw = d_xwork_.p + static_cast<std::int64_t>(c0) * n_;
+    for (const LevelPlan& L : levels_) {
+      if (L.solve_coop) {
+        cuda_check(launch_solve_fwd_coop(lists + L.all_off, lists + L.solve_cta_off, L.all_n, L.solve_ctas, L.solve_steps,
+                                         d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p, d_panels_.p, d_pidx_.p,
+                                         d_blk_.p, d_nblk_.p, d_inv_.p, xw, n_, d_vec_.p, nc, d_work_.p,
+                                         d_work_off_.p + L.work_off_off, s),
+                   "cooperative forward solve");
+      } else {
+        launch_solve_fwd(lists + L.all_off, L.all_n, L.maxm, d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p,
+                         d_panels_.p, d_piv_.p, d_pidx_.p, d_blk_.p, d_nblk_.p, d_inv_.p, xw, n_, d_vec_.p, nc, s);
+      }
+    }
+    launch_solve_diag(sym_.ns, d_sn_.p, d_panels_.p, d_piv_.p, d_pidx_.p, xw, n_, nc, s);
+    for (auto it = levels_.rbegin(); it != levels_.rend(); ++it) {
+      if (it->solve_coop) {
+        cuda_check(launch_solve_bwd_coop(lists + it->all_off, lists + it->solve_cta_off, it->all_n, it->solve_ctas,
+                                         it->solve_steps, d_sn_.p, d_rows_.p, d_panels_.p, d_pidx_.p, d_blk_.p,
+                                         d_nblk_.p, d_inv_.p, xw, n_, nc, d_work_.p, d_work_off_.p + it->work_off_off, s),
+                   "cooperative backward solve");
+      } else {
+        launch_solve_bwd(lists + it->all_off, it->all_n, it->maxm, d_sn_.p, d_rows_.p, d_panels_.p, d_pidx_.p, d_blk_.p,
+                         d_nblk_.p, d_inv_.p, xw, n_, nc, s);
+      }
+    }
+  }
   launch_scatter_scale(n_, nr, db, ld, d_scale_.p, d_iperm_.p, d_xwork_.p, s);
   cuda_check(cudaEventRecord(ev1_, s), "event");
   cuda_check(cudaGetLastError(), "solve launch");

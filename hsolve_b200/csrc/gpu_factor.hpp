@@ -92,8 +92,13 @@ class GpuFactor {
     std::int64_t s32_off = 0; int s32_n = 0;
     std::int64_t s64_off = 0; int s64_n = 0;
     std::int64_t app_off = 0; int app_n = 0;
+    bool coop = false;                 // large fronts: one cooperative launch, CTAs split by work
+    std::int64_t cta_off = 0; int coop_ctas = 0; int done_slot = 0;
     std::int64_t all_off = 0; int all_n = 0; int maxm = 0;
     std::vector<std::pair<std::int64_t, int>> ea;  // (offset into items, count) per child rank
+    bool solve_coop = false;           // few fronts: cooperative sweeps, CTAs split by panel size
+    std::int64_t solve_cta_off = 0; int solve_ctas = 0; int solve_steps = 0;
+    std::int64_t work_off_off = 0;     // offsets of the fronts' work vectors (index into d_work_off_)
   };
   void build_plan();
   void run_numeric(double alpha, double beta, bool detection);
@@ -116,13 +121,20 @@ class GpuFactor {
 
   DevBuf<std::int32_t> d_row_, d_col_, d_rmap_, d_rows_, d_child_ptr_, d_children_, d_iperm_, d_lists_, d_pidx_,
       d_failed_;
-  DevBuf<double> d_a_, d_b_, d_scale_, d_panels_, d_cb_, d_scratch_, d_vec_, d_xwork_, d_btmp_;
+  DevBuf<double> d_a_, d_b_, d_scale_, d_panels_, d_cb_, d_scratch_, d_vec_, d_xwork_, d_btmp_, d_inv_;
+  DevBuf<std::int32_t> d_blk_, d_nblk_;
   DevBuf<std::int64_t> d_dest_;
   DevBuf<unsigned long long> d_r_;
   DevBuf<SnDev> d_sn_;
   DevBuf<int2> d_items_;
   DevBuf<signed char> d_piv_;
   DevBuf<FactorCounters> d_cnt_;
+  DevBuf<int> d_level_done_;
+  DevBuf<std::int64_t> d_work_off_;
+  DevBuf<double> d_work_;
+  int solve_coop_max_ = 0;
+  int coop_max_ = 0;
+  int ncoop_ = 0;
 };
 
 }  // namespace hsg

@@ -17,14 +17,35 @@ void launch_gather_scale(std::int64_t n, int nrhs, const double* b, std::int64_t
                          const std::int32_t* iperm, double* x, cudaStream_t s);
 void launch_scatter_scale(std::int64_t n, int nrhs, double* b, std::int64_t ldb, const double* d,
                           const std::int32_t* iperm, const double* x, cudaStream_t s);
+constexpr int kMaxBlocksPerFront = 2048;  // <= 32-column solve blocks per front (fronts up to ~63k pivots)
+
+// block partition + inverse diagonal blocks of every front (after each factorization)
+void launch_inv_blocks(int ns, const SnDev* sn, const double* panels, const signed char* piv, std::int32_t* blk,
+                       std::int32_t* nblk, double* inv, cudaStream_t s);
 void launch_solve_fwd(const std::int32_t* list, int nlist, int maxm, const SnDev* sn, const std::int32_t* child_ptr,
                       const std::int32_t* children, const std::int32_t* rmap, const double* panels,
-                      const signed char* piv, const std::int32_t* pidx, double* x, std::int64_t n, double* vec,
-                      int nrhs, cudaStream_t s);
+                      const signed char* piv, const std::int32_t* pidx, const std::int32_t* blk,
+                      const std::int32_t* nblk, const double* inv, double* x, std::int64_t n, double* vec, int nrhs,
+                      cudaStream_t s);
 void launch_solve_diag(int ns, const SnDev* sn, const double* panels, const signed char* piv,
                        const std::int32_t* pidx, double* x, std::int64_t n, int nrhs, cudaStream_t s);
 void launch_solve_bwd(const std::int32_t* list, int nlist, int maxm, const SnDev* sn, const std::int32_t* rows,
-                      const double* panels, const signed char* piv, const std::int32_t* pidx, double* x,
-                      std::int64_t n, int nrhs, cudaStream_t s);
+                      const double* panels, const std::int32_t* pidx, const std::int32_t* blk,
+                      const std::int32_t* nblk, const double* inv, double* x, std::int64_t n, int nrhs,
+                      cudaStream_t s);
+
+// cooperative sweeps over the few large fronts of a level (nrhs <= 8 per launch)
+int solve_coop_max_ctas(int device);
+cudaError_t launch_solve_fwd_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
+                                  int max_steps, const SnDev* sn, const std::int32_t* child_ptr,
+                                  const std::int32_t* children, const std::int32_t* rmap, const double* panels,
+                                  const std::int32_t* pidx, const std::int32_t* blk, const std::int32_t* nblk,
+                                  const double* inv, double* x, std::int64_t n, double* vec, int nrhs, double* work,
+                                  const std::int64_t* work_off, cudaStream_t s);
+cudaError_t launch_solve_bwd_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
+                                  int max_steps, const SnDev* sn, const std::int32_t* rows, const double* panels,
+                                  const std::int32_t* pidx, const std::int32_t* blk, const std::int32_t* nblk,
+                                  const double* inv, double* x, std::int64_t n, int nrhs, double* work,
+                                  const std::int64_t* work_off, cudaStream_t s);
 
 }  // namespace hsg
