@@ -118,7 +118,7 @@ enum : int { kFail = 0, kOneJ = 1, kOneR = 2, kTwoR = 3, kNull = 4 };
 
 struct StepShared {
   int j, lim, prog, force, dec, r, stop;
-  int neg, pos, zero, two, forced;
+  int neg, pos, zero, two, forced, eb;
 };
 
 // Warp 0: decide the pivot at column j of the lower-stored matrix F (order m, ld ld) with
@@ -308,6 +308,286 @@ __device__ int dense_bk(double* F, int ld, int m, int nfs, bool root, double u, 
   return st.j;
 }
 
+
+// Threshold Bunch-Kaufman on the panel's diagonal block (order w <= 32, shared memory, ld kNB, all
+// rows candidates): warp 0 decides each pivot (same rule as dense_bk), all warps share the rank-1/2
+// update of the remaining block (warp v owns the columns c = v (mod warps), lane i row i). Returns
+// the number of eliminated columns; block positions [e, w) could not be pivoted.
+__device__ int block_bk(double* F, int w, bool root, double u, double thr, int* lab, signed char* pv, StepShared& st) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  constexpr int ld = kNB;
+  if (threadIdx.x == 0) { st.j = 0; st.lim = w; st.prog = 0; st.force = 0; st.stop = 0; }
+  __syncthreads();
+  while (true) {
+    if (threadIdx.x == 0) {
+      st.stop = 0;
+      if (st.j >= w) st.stop = 1;
+      else if (st.j >= st.lim) {
+        if (st.prog) { st.lim = w; st.prog = 0; st.stop = 2; }
+        else if (root && !st.force) { st.force = 1; st.lim = w; st.stop = 2; }
+        else st.stop = 1;
+      }
+    }
+    __syncthreads();
+    if (st.stop == 1) break;
+    if (st.stop == 2) continue;
+    const int j = st.j;
+    if (warp == 0) {
+      decide_pivot(F, ld, w, w, j, u, thr, st.force != 0, st);
+      __syncwarp();
+      // swaps (warp 0)
+      const int dec = st.dec, r = st.r;
+      int p = -1, q = -1;
+      if (dec == kFail) { p = j; q = st.lim - 1; }
+      else if (dec == kOneR) { p = j; q = r; }
+      else if (dec == kTwoR) { p = j + 1; q = r; }
+      if (p >= 0 && p != q) {
+        if (p > q) { const int tt = p; p = q; q = tt; }
+        for (int t = lane; t < w + 1; t += 32) {
+          double *x = nullptr, *y = nullptr;
+          if (t < p) { x = F + p + t * ld; y = F + q + t * ld; }
+          else if (t > p && t < q) { x = F + t + p * ld; y = F + q + t * ld; }
+          else if (t > q && t < w) { x = F + t + p * ld; y = F + t + q * ld; }
+          else if (t == p) { x = F + p + p * ld; y = F + q + q * ld; }
+          if (x) { const double v = *x; *x = *y; *y = v; }
+        }
+        if (lane == 0) { const int tl = lab[p]; lab[p] = lab[q]; lab[q] = tl; }
+      }
+      if (lane == 0 && dec == kFail) st.lim -= 1;
+    }
+    __syncthreads();
+    const int dec = st.dec;
+    if (dec == kFail) continue;
+    if (dec == kTwoR) {
+      const double a = F[j + j * ld], b = F[j + 1 + j * ld], c = F[j + 1 + (j + 1) * ld];
+      const double det = a * c - b * b;
+      const double ia = c / det, ib = -b / det, ic = a / det;
+      // column values of the pair (before scaling), then the update, then the scaled L
+      const int i = lane;
+      const double x0 = (i >= j + 2 && i < w) ? F[i + j * ld] : 0.0;
+      const double x1 = (i >= j + 2 && i < w) ? F[i + (j + 1) * ld] : 0.0;
+      const double l0 = ia * x0 + ib * x1, l1 = ib * x0 + ic * x1;
+      for (int c2 = j + 2 + warp; c2 < w; c2 += nw) {
+        const double y0 = F[c2 + j * ld], y1 = F[c2 + (j + 1) * ld];
+        if (i >= c2 && i < w) F[i + c2 * ld] -= l0 * y0 + l1 * y1;
+      }
+      __syncthreads();
+      if (warp == 0 && i >= j + 2 && i < w) { F[i + j * ld] = l0; F[i + (j + 1) * ld] = l1; }
+      if (threadIdx.x == 0) {
+        if (det < 0) { st.neg++; st.pos++; } else if (a + c < 0) st.neg += 2; else st.pos += 2;
+        st.two++;
+        if (st.force) st.forced++;
+        pv[j] = 2; pv[j + 1] = 3;
+        st.j = j + 2; st.prog = 1; st.force = 0;
+        if (st.lim < st.j) st.lim = st.j;
+      }
+    } else {
+      const bool nul = dec == kNull;
+      const double d = F[j + j * ld];
+      const int i = lane;
+      const double x = (i > j && i < w) ? F[i + j * ld] : 0.0;
+      if (!nul) {
+        const double inv = 1.0 / d;
+        for (int c2 = j + 1 + warp; c2 < w; c2 += nw) {
+          const double y = F[c2 + j * ld];
+          if (i >= c2 && i < w) F[i + c2 * ld] -= x * y * inv;
+        }
+      }
+      __syncthreads();
+      if (warp == 0 && i > j && i < w) F[i + j * ld] = nul ? 0.0 : x / d;
+      if (threadIdx.x == 0) {
+        if (nul) { st.zero++; pv[j] = 0; }
+        else { if (d < 0) st.neg++; else st.pos++; pv[j] = 1; }
+        if (st.force) st.forced++;
+        st.j = j + 1; st.prog = 1; st.force = 0;
+        if (st.lim < st.j) st.lim = st.j;
+      }
+    }
+    __syncthreads();
+  }
+  return st.j;
+}
+
+__device__ __forceinline__ float warp_maxf(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// One warp: threshold Bunch-Kaufman on the panel's diagonal block (order w <= 32, shared memory,
+// ld kNB, all rows candidates). Same acceptance rules as dense_bk; column maxima are reduced in
+// single precision (a threshold test needs no more), the argmax for a 2 x 2 partner only when the
+// 1 x 1 test fails, one reciprocal per pivot, broadcast shared-memory reads in the update.
+// Warp-synchronous: no block barriers. Returns the eliminated count; [e, w) could not be pivoted.
+__device__ int warp_block_bk(double* F, int w, bool root, double u, double thr, int* lab, signed char* pv,
+                             StepShared& st, int j0 = 0, int prog0 = 0) {
+  const int lane = threadIdx.x & 31;
+  constexpr int ld = kNB;
+  int j = j0, lim = w, prog = prog0, force = 0;
+  int neg = 0, pos = 0, zero = 0, two = 0, forced = 0;
+  while (j < w) {
+    if (j >= lim) {
+      if (prog) { lim = w; prog = 0; continue; }
+      if (root && !force) { force = 1; lim = w; continue; }
+      break;
+    }
+    const double* cj = F + j * ld;
+    const double xj = lane > j && lane < w ? cj[lane] : 0.0;
+    const float gcf = warp_maxf(static_cast<float>(fabs(xj)));
+    const double gc = static_cast<double>(gcf);
+    const double dj = cj[j];
+    const double dcc = fabs(dj);
+    int dec = kFail, r = -1;
+    if (thr >= 0.0 && fmax(dcc, gc) <= thr) dec = kNull;
+    else if (dcc > 0.0 && dcc >= u * gc) dec = kOneJ;
+    else {
+      // partner candidate: argmax over rows (j, w) of |F(i, j)|
+      float best = lane > j && lane < w ? static_cast<float>(fabs(xj)) : -1.0f;
+      int bi = lane > j && lane < w ? lane : -1;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi >= 0 && (bi < 0 || oi < bi))) { best = ob; bi = oi; }
+      }
+      r = bi;
+      if (force && (r < 0 || best <= 0.0f || dcc >= kAlphaBK * gc)) dec = dcc > 0.0 ? kOneJ : kNull;
+      else if (r >= 0 && best > 0.0f) {
+        const double* cr = F + r * ld;
+        const double xr = lane > j && lane < w && lane != r ? (lane < r ? F[r + lane * ld] : cr[lane]) : 0.0;
+        const float gr2f = warp_maxf(static_cast<float>(fabs(xr)));
+        const float gc2f = warp_maxf(lane != r ? static_cast<float>(fabs(xj)) : 0.0f);
+        const double gr2 = gr2f, gc2 = gc2f;
+        const double a = dj, b = cj[r], c = cr[r];
+        const double det = a * c - b * b;
+        if (force) dec = det != 0.0 ? kTwoR : (dcc > 0.0 ? kOneJ : kNull);
+        else {
+          if (det != 0.0) {
+            const double ia = fabs(c / det), ib = fabs(b / det), ic = fabs(a / det);
+            if (ia * gc2 + ib * gr2 <= 1.0 / u && ib * gc2 + ic * gr2 <= 1.0 / u) dec = kTwoR;
+          }
+          if (dec == kFail && fabs(c) > 0.0 && fabs(c) >= u * fmax(fabs(b), gr2)) dec = kOneR;
+        }
+      }
+    }
+    // swaps (rare)
+    int sp = -1, sq = -1;
+    if (dec == kFail) { sp = j; sq = lim - 1; }
+    else if (dec == kOneR) { sp = j; sq = r; }
+    else if (dec == kTwoR) { sp = j + 1; sq = r; }
+    if (sp >= 0 && sp != sq) {
+      int p = sp < sq ? sp : sq, q = sp < sq ? sq : sp;
+      for (int t = lane; t < w + 1; t += 32) {
+        double *x = nullptr, *y = nullptr;
+        if (t < p) { x = F + p + t * ld; y = F + q + t * ld; }
+        else if (t > p && t < q) { x = F + t + p * ld; y = F + q + t * ld; }
+        else if (t > q && t < w) { x = F + t + p * ld; y = F + t + q * ld; }
+        else if (t == p) { x = F + p + p * ld; y = F + q + q * ld; }
+        if (x) { const double v = *x; *x = *y; *y = v; }
+      }
+      if (lane == 0) { const int tl = lab[p]; lab[p] = lab[q]; lab[q] = tl; }
+      __syncwarp();
+    }
+    if (dec == kFail) { lim -= 1; continue; }
+    const int i = lane;
+    if (dec == kTwoR) {
+      const double a = F[j + j * ld], b = F[j + 1 + j * ld], c = F[j + 1 + (j + 1) * ld];
+      const double det = a * c - b * b;
+      const double idet = 1.0 / det;
+      const double ia = c * idet, ib = -b * idet, ic = a * idet;
+      const double x0 = (i >= j + 2 && i < w) ? F[i + j * ld] : 0.0;
+      const double x1 = (i >= j + 2 && i < w) ? F[i + (j + 1) * ld] : 0.0;
+      const double l0 = ia * x0 + ib * x1, l1 = ib * x0 + ic * x1;
+      __syncwarp();
+      for (int c2 = j + 2; c2 < w; ++c2) {
+        const double y0 = F[c2 + j * ld], y1 = F[c2 + (j + 1) * ld];
+        if (i >= c2 && i < w) F[i + c2 * ld] -= l0 * y0 + l1 * y1;
+      }
+      __syncwarp();
+      if (i >= j + 2 && i < w) { F[i + j * ld] = l0; F[i + (j + 1) * ld] = l1; }
+      if (lane == 0) { pv[j] = 2; pv[j + 1] = 3; }
+      if (det < 0) { neg++; pos++; } else if (a + c < 0) neg += 2; else pos += 2;
+      two++;
+      if (force) forced++;
+      j += 2;
+    } else {
+      const bool nul = dec == kNull;
+      const double d = F[j + j * ld];
+      const double inv = nul ? 0.0 : 1.0 / d;
+      const double x = (i > j && i < w) ? F[i + j * ld] : 0.0;
+      const double xs = x * inv;
+      __syncwarp();
+      if (!nul) {
+        for (int c2 = j + 1; c2 < w; ++c2) {
+          const double y = F[c2 + j * ld];
+          if (i >= c2 && i < w) F[i + c2 * ld] -= xs * y;
+        }
+      }
+      __syncwarp();
+      if (i > j && i < w) F[i + j * ld] = xs;
+      if (lane == 0) pv[j] = nul ? 0 : 1;
+      if (nul) zero++;
+      else if (d < 0) neg++;
+      else pos++;
+      if (force) forced++;
+      j += 1;
+    }
+    __syncwarp();
+    prog = 1;
+    force = 0;
+    if (lim < j) lim = j;
+  }
+  if (lane == 0) { st.neg += neg; st.pos += pos; st.zero += zero; st.two += two; st.forced += forced; }
+  return j;
+}
+
+// Register fast path of warp_block_bk for full blocks (w == 32): lane i keeps row i in registers,
+// the positions are processed in order with compile-time indices and 1 x 1 pivots on their own
+// column. The first position whose 1 x 1 test fails (or that is a null pivot) hands the partially
+// factorized block to the shared-memory routine, which continues from there with the same rules.
+__device__ int warp_block_bk_fast(double* F, int w, bool root, double u, double thr, int* lab, signed char* pv,
+                                  StepShared& st) {
+  const int lane = threadIdx.x & 31;
+  constexpr int ld = kNB;
+  if (w != kNB || root) return warp_block_bk(F, w, root, u, thr, lab, pv, st);
+  double r[kNB];
+#pragma unroll
+  for (int c = 0; c < kNB; ++c) r[c] = c <= lane ? F[lane + c * ld] : 0.0;
+  int pos = 0, neg = 0;
+  int stop = kNB;  // first position that needs the general routine
+#pragma unroll
+  for (int j = 0; j < kNB; ++j) {
+    if (stop == kNB) {
+      const double x = lane > j ? r[j] : 0.0;
+      const float gcf = warp_maxf(static_cast<float>(fabs(x)));
+      const double d = __shfl_sync(0xffffffffu, r[j], j);
+      const double dcc = fabs(d);
+      const double gc = gcf;
+      const bool ok = dcc > 0.0 && dcc >= u * gc && !(thr >= 0.0 && fmax(dcc, gc) <= thr);
+      if (!ok) {
+        stop = j;
+      } else {
+        const double inv = 1.0 / d;
+        const double xs = x * inv;
+#pragma unroll
+        for (int c = j + 1; c < kNB; ++c) {
+          const double yc = __shfl_sync(0xffffffffu, r[j], c);  // F(c, j)
+          if (lane >= c) r[c] = fma(-xs, yc, r[c]);
+        }
+        if (lane > j) r[j] = xs;
+        if (d < 0) ++neg; else ++pos;
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < kNB; ++c)
+    if (c <= lane) F[lane + c * ld] = r[c];
+  for (int t = lane; t < stop; t += 32) pv[t] = 1;
+  __syncwarp();
+  if (lane == 0) { st.neg += neg; st.pos += pos; }
+  if (stop == kNB) return kNB;
+  return warp_block_bk(F, w, root, u, thr, lab, pv, st, stop, stop > 0 ? 1 : 0);
+}
 }  // namespace
 
 // ---------------------------------------------------------------------- small fronts (smem)
@@ -393,6 +673,7 @@ struct AppFront {
   unsigned long long* cmax;
   unsigned long long* rmax;
   double* backup;  // kNB columns of m rows
+  double* W;       // W = L D of the panel's columns (kNB columns of m rows), for the trailing update
   std::int32_t* plab;
   signed char* ppv;
 };
@@ -419,6 +700,8 @@ __device__ AppFront make_front(const SnDev& d, double* panels, double* cb, doubl
   F.rmax = reinterpret_cast<unsigned long long*>(s);
   s += kNB;
   F.backup = s;
+  s += static_cast<std::int64_t>(kNB) * d.m;
+  F.W = s;
   F.plab = pidx_out + d.first;
   F.ppv = piv_out + d.first;
   return F;
@@ -505,17 +788,14 @@ __device__ void app_control_and_block(AppFront& F, const FactorParams& prm, doub
     }
   }
   for (int t = threadIdx.x; t < w; t += blockDim.x) slab[t] = t;
+  if (threadIdx.x == 0) { bst.neg = bst.pos = bst.zero = bst.two = bst.forced = 0; bst.eb = 0; }
   __syncthreads();
-  const int eb = dense_bk(Bs, kNB, w, w, force, prm.u, thr, slab, spv, tmp0, tmp1, bst);
-  // permute the L rows p..p+w-1 of the eliminated columns c < p
-  for (int c0 = 0; c0 < p; c0 += blockDim.x / kNB) {
-    const int cc = c0 + threadIdx.x / kNB, a = threadIdx.x % kNB;
-    double v = 0.0;
-    if (cc < p && a < w) v = F.f.at(p + slab[a], cc);
-    __syncthreads();
-    if (cc < p && a < w) F.f.at(p + a, cc) = v;
-    __syncthreads();
+  if (threadIdx.x < 32) {
+    const int e = warp_block_bk_fast(Bs, w, force, prm.u, thr, slab, spv, bst);
+    if (threadIdx.x == 0) bst.eb = e;
   }
+  __syncthreads();
+  const int eb = bst.eb;
   {
     int old = 0;
     if (threadIdx.x < w) old = F.plab[p + slab[threadIdx.x]];
@@ -525,6 +805,18 @@ __device__ void app_control_and_block(AppFront& F, const FactorParams& prm, doub
   for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
     const int i = t % w, j = t / w;
     if (i >= j) F.f.at(p + i, p + j) = Bs[i + j * kNB];
+  }
+  // W rows of the block: W(p+i, s) = (L D)(i, s) for eliminated s, from the factored block
+  for (int t = threadIdx.x; t < w * kNB; t += blockDim.x) {
+    const int i = t % w, s = t / w;
+    double v = 0.0;
+    if (s < eb && i > s) {
+      const signed char ty = spv[s];
+      if (ty == 1) v = Bs[i + s * kNB] * Bs[s + s * kNB];
+      else if (ty == 2 && i > s + 1) v = Bs[i + s * kNB] * Bs[s + s * kNB] + Bs[i + (s + 1) * kNB] * Bs[s + 1 + s * kNB];
+      else if (ty == 3 && i > s) v = Bs[i + (s - 1) * kNB] * Bs[s + (s - 1) * kNB] + Bs[i + s * kNB] * Bs[s + s * kNB];
+    }
+    F.W[static_cast<std::int64_t>(s) * F.f.m + p + i] = v;
   }
   for (int t = threadIdx.x; t < kNB * kNB; t += blockDim.x) F.B[t] = Bs[t];
   for (int t = threadIdx.x; t < kNB; t += blockDim.x) {
@@ -537,54 +829,119 @@ __device__ void app_control_and_block(AppFront& F, const FactorParams& prm, doub
 }
 
 // All ranks: rows [p+w, m) solved against the block (L21 = F21 P L11^-T D^-1), backup, column maxima.
+// The block's strict lower part with the 2x2 couplings masked (they belong to D) is staged in Ls
+// (shared), the substitution runs fully unrolled in registers, one row per thread.
 __device__ void app_rows(AppFront& F, int rank, int nr, double* Bs, int* slab, signed char* spv,
-                         unsigned long long* scm, unsigned long long* srm) {
+                         unsigned long long* scm, unsigned long long* srm, double* Lm) {
   const AppCtrl* c = F.ctrl;
-  const int p = c->p, w = c->w, eb = c->eb, m = F.f.m;
-  for (int t = threadIdx.x; t < kNB * kNB; t += blockDim.x) Bs[t] = F.B[t];
+  const int p = __ldcg(&c->p), w = __ldcg(&c->w), eb = __ldcg(&c->eb), m = F.f.m;
+  for (int t = threadIdx.x; t < kNB * kNB; t += blockDim.x) Bs[t] = __ldcg(&F.B[t]);
   for (int t = threadIdx.x; t < kNB; t += blockDim.x) {
-    slab[t] = F.lab[t];
+    slab[t] = __ldcg(&F.lab[t]);
     spv[t] = F.pv[t];
     scm[t] = 0ull;
     srm[t] = 0ull;
   }
   __syncthreads();
-  for (int i = p + w + rank * blockDim.x + threadIdx.x; i < m; i += nr * blockDim.x) {
-    double x[kNB], y[kNB];
+  // Lm[t * kNB + s] = L11(t, s) for s < min(t, eb), zero otherwise (row-major for broadcast reads)
+  for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+    const int t = e / kNB, s = e % kNB;
+    double v = 0.0;
+    if (t < w && s < t && s < eb && !(spv[s] == 2 && s + 1 == t)) v = Bs[t + s * kNB];
+    Lm[e] = v;
+  }
+  __syncthreads();
+  // permute the L rows p..p+w-1 of the eliminated columns c < p (a thread owns a column; the
+  // columns are split into contiguous chunks over the ranks)
+  const int cchunk = (p + nr - 1) / nr;
+  const int cend = min(p, (rank + 1) * cchunk);
+  for (int cc = rank * cchunk + threadIdx.x; cc < cend; cc += blockDim.x) {
+    double v[kNB];
+    double* colp = F.f.col(cc) + p;
 #pragma unroll
-    for (int t = 0; t < kNB; ++t) x[t] = t < w ? F.f.at(i, p + t) : 0.0;
+    for (int a = 0; a < kNB; ++a) v[a] = a < w ? colp[slab[a]] : 0.0;
+#pragma unroll
+    for (int a = 0; a < kNB; ++a)
+      if (a < w) colp[a] = v[a];
+  }
+  const int rtotal = m - (p + w);
+  const int rchunk = (rtotal + nr - 1) / nr;
+  const int rbeg = p + w + rank * rchunk, rend = min(m, rbeg + rchunk);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float* wl = reinterpret_cast<float*>(Lm + kNB * kNB);   // per-warp column maxima (8 x kNB floats)
+  double* Di = Lm + kNB * kNB + 8 * kNB;                    // D^-1 entries: a, b, c per pivot (3 x kNB)
+  for (int t = threadIdx.x; t < 8 * kNB; t += blockDim.x) wl[t] = 0.0f;
+  for (int t = threadIdx.x; t < kNB; t += blockDim.x) {
+    double ia = 0.0, ib = 0.0, ic = 0.0;
+    if (t < eb) {
+      const signed char ty = spv[t];
+      if (ty == 1) ia = 1.0 / Bs[t + t * kNB];
+      else if (ty == 2 || ty == 3) {
+        const int f0 = ty == 2 ? t : t - 1;
+        const double a = Bs[f0 + f0 * kNB], b = Bs[f0 + 1 + f0 * kNB], cc = Bs[f0 + 1 + (f0 + 1) * kNB];
+        const double idet = 1.0 / (a * cc - b * b);
+        // first of the pair: l = ia y_t + ib y_{t+1}; second: l = ib y_{t-1} + ic y_t
+        if (ty == 2) { ia = cc * idet; ib = -b * idet; }
+        else { ib = -b * idet; ic = a * idet; }
+      }
+    }
+    Di[t] = ia;
+    Di[kNB + t] = ib;
+    Di[2 * kNB + t] = ic;
+  }
+  __syncthreads();
+  float cm[kNB];
+#pragma unroll
+  for (int t = 0; t < kNB; ++t) cm[t] = 0.0f;
+  for (int i = rbeg + threadIdx.x; i < rend; i += blockDim.x) {
+    // all loads first (no store in between: they overlap), block order = the pivot permutation;
+    // the backup is stored, then the substitution runs in place
+    double y[kNB];
+#pragma unroll
+    for (int t = 0; t < kNB; ++t) y[t] = t < w ? F.f.at(i, p + slab[t]) : 0.0;
 #pragma unroll
     for (int t = 0; t < kNB; ++t)
-      if (t < w) F.backup[static_cast<std::int64_t>(t) * m + i] = x[t];
-    for (int t = 0; t < w; ++t) {
-      double v = x[slab[t]];
-      const int lim_s = t < eb ? t : eb;
-      for (int s = 0; s < lim_s; ++s) {
-        if (spv[s] == 2 && s + 1 == t) continue;
-        v -= y[s] * Bs[t + s * kNB];
-      }
+      if (t < w) F.backup[static_cast<std::int64_t>(t) * m + i] = y[t];
+#pragma unroll
+    for (int t = 1; t < kNB; ++t) {
+      double v = y[t];
+#pragma unroll
+      for (int s = 0; s < t; ++s) v = fma(-y[s], Lm[t * kNB + s], v);
       y[t] = v;
     }
-    for (int t = 0; t < w; ++t) {
+#pragma unroll
+    for (int t = 0; t < kNB; ++t) {
+      if (t >= w) continue;
       double out;
       if (t < eb) {
         const signed char ty = spv[t];
+        const double yp = t > 0 ? y[(t - 1) & (kNB - 1)] : 0.0;
+        const double yn = t + 1 < kNB ? y[(t + 1) & (kNB - 1)] : 0.0;
         if (ty == 0) out = 0.0;
-        else if (ty == 1) out = y[t] / Bs[t + t * kNB];
-        else if (ty == 2) {
-          const double a = Bs[t + t * kNB], b = Bs[t + 1 + t * kNB], cc = Bs[t + 1 + (t + 1) * kNB];
-          out = (cc * y[t] - b * y[t + 1]) / (a * cc - b * b);
-        } else {
-          const double a = Bs[t - 1 + (t - 1) * kNB], b = Bs[t + (t - 1) * kNB], cc = Bs[t + t * kNB];
-          out = (-b * y[t - 1] + a * y[t]) / (a * cc - b * b);
-        }
-        atomic_max_nonneg(&scm[t], fabs(out));
-        atomic_max_nonneg(&srm[t], fabs(y[t]));
+        else if (ty == 1) out = y[t] * Di[t];
+        else if (ty == 2) out = Di[t] * y[t] + Di[kNB + t] * yn;
+        else out = Di[kNB + t] * yp + Di[2 * kNB + t] * y[t];
+        cm[t] = fmaxf(cm[t], static_cast<float>(fabs(ty == 0 ? y[t] : out)));
+        F.W[static_cast<std::int64_t>(t) * m + i] = (ty == 0) ? 0.0 : y[t];  // W = L D = y
       } else {
         out = y[t];
       }
       F.f.at(i, p + t) = out;
     }
+  }
+#pragma unroll
+  for (int t = 0; t < kNB; ++t) {
+    const float a = warp_maxf(cm[t]);
+    if (lane == 0) wl[warp * kNB + t] = a;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < w; t += blockDim.x) {
+    float a = 0.0f;
+    for (int v = 0; v < (int)(blockDim.x >> 5); ++v) a = fmaxf(a, wl[v * kNB + t]);
+    // column maximum of |l| (|y| for a null pivot, which has l = 0), rounded up to stay conservative
+    const double ad = static_cast<double>(a) * (1.0 + 1e-7);
+    scm[t] = static_cast<unsigned long long>(__double_as_longlong(ad));
+    srm[t] = scm[t];
   }
   __syncthreads();
   for (int t = threadIdx.x; t < w; t += blockDim.x) {
@@ -593,23 +950,32 @@ __device__ void app_rows(AppFront& F, int rank, int nr, double* Bs, int* slab, s
   }
 }
 
-// All ranks: the accepted prefix q (identical in every CTA); rank 0 books the inertia.
-__device__ int app_accept(AppFront& F, int rank, bool force, double thr, double inv_u, int* sq) {
+// All ranks: the accepted prefix q (identical in every CTA); rank 0 books the inertia. The small
+// per-panel arrays are staged in shared memory first (one parallel load) so that the serial scans
+// below touch no global memory. Bs / spv already hold the panel's block and pivot types (app_rows).
+__device__ int app_accept(AppFront& F, int rank, bool force, double thr, double inv_u, int* sq, const double* Bs,
+                          const signed char* spv, unsigned long long* scm, unsigned long long* srm) {
   const AppCtrl* c = F.ctrl;
-  const int eb = c->eb;
+  const int eb = __ldcg(&c->eb);
+  const int p = __ldcg(&c->p);
+  for (int t = threadIdx.x; t < kNB; t += blockDim.x) {
+    scm[t] = __ldcg(&F.cmax[t]);
+    srm[t] = __ldcg(&F.rmax[t]);
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
     int q = 0;
     while (q < eb) {
-      const signed char ty = F.pv[q];
-      const double cm = __longlong_as_double(static_cast<long long>(F.cmax[q]));
+      const signed char ty = spv[q];
+      const double cm = __longlong_as_double(static_cast<long long>(scm[q]));
       if (ty == 0) {
-        if (!force && __longlong_as_double(static_cast<long long>(F.rmax[q])) > thr) break;
+        if (!force && __longlong_as_double(static_cast<long long>(srm[q])) > thr) break;
         q += 1;
       } else if (ty == 1) {
         if (!force && cm > inv_u) break;
         q += 1;
       } else {
-        const double cm2 = __longlong_as_double(static_cast<long long>(F.cmax[q + 1]));
+        const double cm2 = __longlong_as_double(static_cast<long long>(scm[q + 1]));
         if (!force && fmax(cm, cm2) > inv_u) break;
         q += 2;
       }
@@ -619,21 +985,26 @@ __device__ int app_accept(AppFront& F, int rank, bool force, double thr, double 
   __syncthreads();
   const int q = *sq;
   if (rank == 0) {
-    for (int t = threadIdx.x; t < q; t += blockDim.x) F.ppv[c->p + t] = F.pv[t];
+    for (int t = threadIdx.x; t < q; t += blockDim.x) F.ppv[p + t] = spv[t];
     if (threadIdx.x == 0) {
-      AppCtrl* cw = F.ctrl;
-      cw->q = q;
+      int neg = 0, pos = 0, zero = 0, two = 0;
       for (int t = 0; t < q; ++t) {
-        const signed char ty = F.pv[t];
-        if (ty == 0) cw->zero++;
-        else if (ty == 1) { if (F.B[t + t * kNB] < 0) cw->neg++; else cw->pos++; }
+        const signed char ty = spv[t];
+        if (ty == 0) zero++;
+        else if (ty == 1) { if (Bs[t + t * kNB] < 0) neg++; else pos++; }
         else if (ty == 2) {
-          const double a = F.B[t + t * kNB], b = F.B[t + 1 + t * kNB], cc = F.B[t + 1 + (t + 1) * kNB];
+          const double a = Bs[t + t * kNB], b = Bs[t + 1 + t * kNB], cc = Bs[t + 1 + (t + 1) * kNB];
           const double det = a * cc - b * b;
-          if (det < 0) { cw->neg++; cw->pos++; } else if (a + cc < 0) cw->neg += 2; else cw->pos += 2;
-          cw->two++;
+          if (det < 0) { neg++; pos++; } else if (a + cc < 0) neg += 2; else pos += 2;
+          two++;
         }
       }
+      AppCtrl* cw = F.ctrl;
+      cw->q = q;
+      cw->neg += neg;
+      cw->pos += pos;
+      cw->zero += zero;
+      cw->two += two;
       if (force) cw->forced += q;
     }
   }
@@ -644,8 +1015,11 @@ __device__ int app_accept(AppFront& F, int rank, bool force, double thr, double 
 __device__ void app_restore(AppFront& F, int rank, int nr, int q) {
   const AppCtrl* c = F.ctrl;
   const int p = c->p, w = c->w, m = F.f.m;
-  for (int i = p + w + rank * blockDim.x + threadIdx.x; i < m; i += nr * blockDim.x)
-    for (int t = q; t < w; ++t) F.f.at(i, p + t) = F.backup[static_cast<std::int64_t>(F.lab[t]) * m + i];
+  const int rtotal = m - (p + w);
+  const int rchunk = (rtotal + nr - 1) / nr;
+  const int rbeg = p + w + rank * rchunk, rend = min(m, rbeg + rchunk);
+  for (int i = rbeg + threadIdx.x; i < rend; i += blockDim.x)
+    for (int t = q; t < w; ++t) F.f.at(i, p + t) = F.backup[static_cast<std::int64_t>(t) * m + i];
   if (rank == 0) {
     for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
       const int a = t % w, b = t / w;
@@ -657,10 +1031,10 @@ __device__ void app_restore(AppFront& F, int rank, int nr, int q) {
   }
 }
 
-// All ranks: C(i, c) -= sum_{s<q} L(i, p+s) W(c, s), from <= c <= i < m, W = L D; 64 x 64 tiles
-// of the lower triangle dealt round-robin to the ranks; 4 x 4 outputs per thread.
-__device__ void app_update(AppFront& F, int rank, int nr, int q, double* Ls, double* Ws, const double* Bs,
-                           const signed char* spv) {
+// All ranks: C(i, c) -= sum_{s<q} L(i, p+s) W(c, s), from <= c <= i < m, W = L D (from scratch);
+// 64 x 64 tiles of the lower triangle dealt round-robin to the ranks; 4 x 4 outputs per thread, the
+// C values loaded before the products so that their latencies overlap.
+__device__ void app_update(AppFront& F, int rank, int nr, int q, double* Ls, double* Ws) {
   const AppCtrl* c = F.ctrl;
   const int p = c->p, from = p + q, m = F.f.m;
   const int rows = m - from;
@@ -679,14 +1053,19 @@ __device__ void app_update(AppFront& F, int rank, int nr, int q, double* Ls, dou
       const int s = t / kTile, r = t % kTile;
       const int i = i0 + r, cc = j0 + r;
       Ls[s * kTile + r] = i < m ? F.f.at(i, p + s) : 0.0;
-      double wv = 0.0;
-      if (cc < m) {
-        const signed char tyv = spv[s];
-        if (tyv == 1) wv = F.f.at(cc, p + s) * Bs[s * kNB + s];
-        else if (tyv == 2) wv = F.f.at(cc, p + s) * Bs[s * kNB + s] + F.f.at(cc, p + s + 1) * Bs[s * kNB + s + 1];
-        else if (tyv == 3) wv = F.f.at(cc, p + s - 1) * Bs[(s - 1) * kNB + s] + F.f.at(cc, p + s) * Bs[s * kNB + s];
+      Ws[s * kTile + r] = cc < m ? F.W[static_cast<std::int64_t>(s) * m + cc] : 0.0;
+    }
+    double* colp[4];
+    double cv[4][4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int cc = j0 + ty + 16 * b;
+      colp[b] = cc < m ? F.f.col(cc) : nullptr;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int i = i0 + tx + 16 * a;
+        cv[a][b] = (colp[b] && i < m && cc <= i) ? colp[b][i] : 0.0;
       }
-      Ws[s * kTile + r] = wv;
     }
     __syncthreads();
     double acc[4][4];
@@ -708,12 +1087,10 @@ __device__ void app_update(AppFront& F, int rank, int nr, int q, double* Ls, dou
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
       const int cc = j0 + ty + 16 * b;
-      if (cc >= m) continue;
-      double* colp = F.f.col(cc);
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
         const int i = i0 + tx + 16 * a;
-        if (i < m && cc <= i) colp[i] -= acc[a][b];
+        if (colp[b] && i < m && cc <= i) colp[b][i] = cv[a][b] - acc[a][b];
       }
     }
   }
@@ -771,14 +1148,14 @@ __global__ void __launch_bounds__(kAppThreads) k_front_app(const std::int32_t* l
     app_control_and_block(F, prm, thr, sm.Bs, sm.tmp0, sm.tmp1, sm.slab, sm.spv, sm.bst, &sm.stop, cnt, failed, nullptr);
     __syncthreads();
     if (sm.stop) break;
-    app_rows(F, 0, 1, sm.Bs, sm.slab, sm.spv, sm.scm, sm.srm);
+    app_rows(F, 0, 1, sm.Bs, sm.slab, sm.spv, sm.scm, sm.srm, Ls);
     __syncthreads();
     const bool force = F.ctrl->force != 0;
-    const int q = app_accept(F, 0, force, thr, inv_u, &sm.q);
+    const int q = app_accept(F, 0, force, thr, inv_u, &sm.q, sm.Bs, sm.spv, sm.scm, sm.srm);
     __syncthreads();
     if (q < F.ctrl->w) app_restore(F, 0, 1, q);
     __syncthreads();
-    app_update(F, 0, 1, q, Ls, Ws, sm.Bs, sm.spv);
+    app_update(F, 0, 1, q, Ls, Ws);
     __syncthreads();
     app_advance(F, q);
   }
@@ -816,15 +1193,15 @@ __global__ void __launch_bounds__(kAppThreads) k_front_coop(const std::int32_t* 
     grid.sync();
     if (*reinterpret_cast<volatile int*>(level_done) >= nfronts) break;
     const bool active = F.ctrl->stop == 0;
-    if (active) app_rows(F, rank, nr, sm.Bs, sm.slab, sm.spv, sm.scm, sm.srm);
+    if (active) app_rows(F, rank, nr, sm.Bs, sm.slab, sm.spv, sm.scm, sm.srm, Ls);
     grid.sync();
     int q = 0;
     if (active) {
-      q = app_accept(F, rank, F.ctrl->force != 0, thr, inv_u, &sm.q);
+      q = app_accept(F, rank, __ldcg(&F.ctrl->force) != 0, thr, inv_u, &sm.q, sm.Bs, sm.spv, sm.scm, sm.srm);
       if (q < F.ctrl->w) app_restore(F, rank, nr, q);
     }
     grid.sync();
-    if (active) app_update(F, rank, nr, q, Ls, Ws, sm.Bs, sm.spv);
+    if (active) app_update(F, rank, nr, q, Ls, Ws);
     grid.sync();
     if (active && rank == 0) app_advance(F, q);
   }

@@ -16,10 +16,10 @@ constexpr int kCoopMinFront = 192;     // levels whose largest panel front is at
 constexpr int kColsPerThread = kTile * kTile / kAppThreads;  // 16
 constexpr int kExtendAddCols = 8;      // contribution-block columns per extend-add CTA
 // per-front scratch of the panel kernels (doubles): control block, block, original block, labels,
-// pivot types, column maxima, backup of the panel's rows
+// pivot types, column maxima, backup of the panel's rows, W = L D of the panel
 constexpr int kAppCtrlDoubles = 8;
 inline std::int64_t app_scratch_doubles(int m) {
-  return kAppCtrlDoubles + 2 * kNB * kNB + kNB / 2 + kNB / 8 + 2 * kNB + static_cast<std::int64_t>(m) * kNB;
+  return kAppCtrlDoubles + 2 * kNB * kNB + kNB / 2 + kNB / 8 + 2 * kNB + 2 * static_cast<std::int64_t>(m) * kNB;
 }
 
 void launch_fill(double* x, std::int64_t n, double v, cudaStream_t s);
