@@ -59,6 +59,7 @@ SIGNATURES = {
     "hsg_factorize": (ctypes.c_int, [_P, _D, _D, _P]),
     "hsg_count": (ctypes.c_int, [_P, _D, _D, _I32, _P]),
     "hsg_solve": (ctypes.c_int, [_P, _P, _I64, _I64, _I32]),
+    "hsg_solve_static": (ctypes.c_int, [_P, _P, _I64, _I64]),
     "hsg_inertia": (ctypes.c_int, [_P, _P]),
     "hsg_release": (ctypes.c_int, [_P, _P]),
     "hsg_set_null_pivot_detection": (ctypes.c_int, [_P, _I32]),
@@ -201,6 +202,11 @@ class Factorization:
     def solve_device(self, ptr: int, nrhs: int, ld: int):
         """In-place solve of a device buffer (e.g. a torch.cuda tensor's data_ptr())."""
         check(lib().hsg_solve(self._h, ctypes.c_void_p(ptr), nrhs, ld, 1))
+
+    def solve_static(self, ptr: int, nrhs: int, ld: int):
+        """In-place solve of a device buffer that allocates no device memory (hsg_solve_static):
+        for callers that cannot call cudaMalloc; see include/hsg.h for the size limit."""
+        check(lib().hsg_solve_static(self._h, ctypes.c_void_p(ptr), nrhs, ld))
 
     def release_factors(self) -> bool:
         r = ctypes.c_int32()

@@ -23,6 +23,11 @@ const GpuFactor& get(const hsg_factor* f) {
 }
 }  // namespace
 
+namespace hsg {
+// The object behind a handle, for entry points defined in other translation units.
+GpuFactor& factor_of(hsg_factor* f) { return get(f); }
+}  // namespace hsg
+
 extern "C" {
 
 int hsg_create(const hsg_options_t* opt, hsg_factor** out) {

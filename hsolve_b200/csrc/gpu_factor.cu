@@ -474,6 +474,61 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
   last_solve_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
+std::size_t GpuFactor::solve_scratch_doubles(std::int64_t nrhs) const {
+  const std::int64_t nc = std::min<std::int64_t>(8, nrhs);
+  return static_cast<std::size_t>(n_ * nrhs + std::max<std::int64_t>(1, vec_total_) * nc);
+}
+
+void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ldb, double* scratch,
+                                   std::size_t cap) {
+  HSG_REQUIRE(factored_, HSG_INTERNAL, "solve without a valid factorization");
+  HSG_REQUIRE(nrhs >= 0 && ldb >= n_, HSG_INVALID_INPUT, "solve: nrhs < 0 or ldb < n");
+  if (nrhs == 0) return;
+  HSG_REQUIRE(b && scratch, HSG_INVALID_INPUT, "solve: null right-hand side or scratch");
+  const std::size_t need = solve_scratch_doubles(nrhs);
+  HSG_REQUIRE(need <= cap, HSG_INVALID_INPUT,
+              "solve needs " << need << " doubles of scratch for n = " << n_ << " and nrhs = " << nrhs << ", "
+                             << cap << " are available; pass fewer right-hand sides per call");
+  DeviceGuard g(opt_.device);
+  cudaStream_t s = stream_;
+  const int nr = static_cast<int>(nrhs);
+  double* xwork = scratch;
+  double* vec = scratch + static_cast<std::size_t>(n_) * nr;
+  launch_gather_scale(n_, nr, b, ldb, d_scale_.p, d_iperm_.p, xwork, s);
+  const std::int32_t* lists = d_lists_.p;
+  for (int c0 = 0; c0 < nr; c0 += 8) {
+    const int nc = std::min(8, nr - c0);
+    double* xw = xwork + static_cast<std::int64_t>(c0) * n_;
+    for (const LevelPlan& L : levels_) {
+      if (L.solve_coop) {
+        cuda_check(launch_solve_fwd_coop(lists + L.all_off, lists + L.solve_cta_off, L.all_n, L.solve_ctas, L.solve_steps,
+                                         d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p, d_panels_.p, d_pidx_.p,
+                                         d_blk_.p, d_nblk_.p, d_inv_.p, xw, n_, vec, nc, d_work_.p,
+                                         d_work_off_.p + L.work_off_off, s),
+                   "cooperative forward solve");
+      } else {
+        launch_solve_fwd(lists + L.all_off, L.all_n, L.maxm, d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p,
+                         d_panels_.p, d_piv_.p, d_pidx_.p, d_blk_.p, d_nblk_.p, d_inv_.p, xw, n_, vec, nc, s);
+      }
+    }
+    launch_solve_diag(sym_.ns, d_sn_.p, d_panels_.p, d_piv_.p, d_pidx_.p, xw, n_, nc, s);
+    for (auto it = levels_.rbegin(); it != levels_.rend(); ++it) {
+      if (it->solve_coop) {
+        cuda_check(launch_solve_bwd_coop(lists + it->all_off, lists + it->solve_cta_off, it->all_n, it->solve_ctas,
+                                         it->solve_steps, d_sn_.p, d_rows_.p, d_panels_.p, d_pidx_.p, d_blk_.p,
+                                         d_nblk_.p, d_inv_.p, xw, n_, nc, d_work_.p, d_work_off_.p + it->work_off_off, s),
+                   "cooperative backward solve");
+      } else {
+        launch_solve_bwd(lists + it->all_off, it->all_n, it->maxm, d_sn_.p, d_rows_.p, d_panels_.p, d_pidx_.p, d_blk_.p,
+                         d_nblk_.p, d_inv_.p, xw, n_, nc, s);
+      }
+    }
+  }
+  launch_scatter_scale(n_, nr, b, ldb, d_scale_.p, d_iperm_.p, xwork, s);
+  cuda_check(cudaGetLastError(), "solve launch");
+  cuda_check(cudaStreamSynchronize(s), "solve");
+}
+
 void GpuFactor::release() {
   factored_ = false;
   inertia_.valid = 0;

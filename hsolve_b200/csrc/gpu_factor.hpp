@@ -61,6 +61,13 @@ class GpuFactor {
                const std::int64_t* b_rp, const std::int32_t* b_ci, const double* b_v, const std::int32_t* order);
   hsg_inertia_t factorize(double alpha, double beta, bool detection);
   void solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_device);
+  // Doubles of work space that solve_with_scratch needs for nrhs right-hand sides: n x nrhs for the
+  // permuted, scaled right-hand sides and (contribution rows) x min(nrhs, 8) for the update vectors.
+  std::size_t solve_scratch_doubles(std::int64_t nrhs) const;
+  // The solve of a device-resident b (column-major, leading dimension ldb) with its work space in
+  // the caller's `scratch` (`cap` doubles, on this factorization's device). Allocates no device
+  // memory; every scratch entry is written before it is read, so nothing needs to start at zero.
+  void solve_with_scratch(double* b_dev, std::int64_t nrhs, std::int64_t ldb, double* scratch, std::size_t cap);
   void release();
   hsg_estimate_t estimate() const;
   const hsg_inertia_t& inertia() const { return inertia_; }

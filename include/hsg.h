@@ -119,6 +119,22 @@ HSG_API int hsg_count(hsg_factor* f, double alpha, double beta, int32_t detectio
  * ldb >= n. b_on_device: 0 host memory, 1 device memory of the handle's device. */
 HSG_API int hsg_solve(hsg_factor* f, double* b, int64_t nrhs, int64_t ldb, int32_t b_on_device);
 
+/* The same solve as hsg_solve with b in device memory, for callers that must not allocate device
+ * memory: a process whose device memory is already fully claimed by a pooling allocator (where
+ * cudaMalloc would fail), or a serving loop that cannot afford the device-wide synchronisation
+ * that cudaFree implies. This call allocates nothing: its work space is one fixed array compiled
+ * into the library, HSG_SOLVE_STATIC_SCRATCH_BYTES (16 MiB) on every device that loads the library,
+ * held until the process exits. It needs 8 * (n * nrhs + c * min(nrhs, 8)) bytes, where c is the
+ * total contribution-block row count of the factorization; a larger request returns
+ * HSG_INVALID_INPUT with the sizes in hsg_last_error(), and the caller should split its right-hand
+ * sides or use hsg_solve. The first call on a device looks up the array's device address (make
+ * that first call before any stream capture). All calls on a device share the one array, so two
+ * calls whose GPU work overlaps (from different host threads) race and give wrong results;
+ * calls from one thread are safe because each call waits for its GPU work before returning.
+ * No counterpart in hsolve. */
+#define HSG_SOLVE_STATIC_SCRATCH_BYTES (16u << 20)
+HSG_API int hsg_solve_static(hsg_factor* f, double* b_device, int64_t nrhs, int64_t ldb);
+
 /* SparseFactorization::inertia() (factor.hpp:400-406). */
 HSG_API int hsg_inertia(const hsg_factor* f, hsg_inertia_t* out);
 
