@@ -19,6 +19,7 @@ struct SnDev {
   std::int64_t vec_off;   // contribution vector (m-k entries per rhs) in the solve arena
   std::int64_t scratch_off;  // pivoting scratch of the panel kernel (doubles)
   std::int64_t inv_off;      // inverse diagonal blocks (32 x 32 each) of the solve
+  std::int64_t w_off;        // super-block solve operator (m x k, ld m) of a large front (-1: none)
 };
 
 // Counters written by the factorization kernels (integers: sums are order independent).

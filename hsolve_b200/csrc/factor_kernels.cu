@@ -779,6 +779,42 @@ __device__ void app_control_and_block(AppFront& F, const FactorParams& prm, doub
   if (*shared_stop) return;
   const int p = c->p, w = c->w;
   const bool force = c->force != 0;
+  if (force && p + 1 < k) {
+    // A root front that made no progress over all its remaining columns: Bunch-Kaufman's choice
+    // for column p without threshold, with the partner searched among all remaining fully-summed
+    // rows (not only the block's), is brought next to p before the block is factorized.
+    __shared__ double s_bv[32], s_gc[32];
+    __shared__ int s_bi[32], s_r;
+    double bv = -1.0, gc = 0.0;
+    int bi = -1;
+    for (int i = p + 1 + threadIdx.x; i < F.f.m; i += blockDim.x) {
+      const double v = fabs(F.f.at(i, p));
+      gc = fmax(gc, v);
+      if (i < k && v > bv) { bv = v; bi = i; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      gc = fmax(gc, __shfl_xor_sync(0xffffffffu, gc, o));
+      if (ov > bv || (ov == bv && oi >= 0 && (bi < 0 || oi < bi))) { bv = ov; bi = oi; }
+    }
+    if ((threadIdx.x & 31) == 0) { s_bv[threadIdx.x >> 5] = bv; s_bi[threadIdx.x >> 5] = bi; s_gc[threadIdx.x >> 5] = gc; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double b = -1.0, g = 0.0;
+      int r = -1;
+      for (int q = 0; q < static_cast<int>(blockDim.x >> 5); ++q) {
+        g = fmax(g, s_gc[q]);
+        if (s_bv[q] > b || (s_bv[q] == b && s_bi[q] >= 0 && (r < 0 || s_bi[q] < r))) { b = s_bv[q]; r = s_bi[q]; }
+      }
+      const double dcc = fabs(F.f.at(p, p));
+      s_r = (r < 0 || b <= 0.0 || dcc >= kAlphaBK * g) ? -1 : r;
+    }
+    __syncthreads();
+    const int r = s_r;
+    if (r > p + 1) front_swap(F.f, p + 1, r, F.plab);
+    __syncthreads();
+  }
   for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
     const int i = t % w, j = t / w;
     if (i >= j) {
@@ -964,19 +1000,22 @@ __device__ int app_accept(AppFront& F, int rank, bool force, double thr, double 
   }
   __syncthreads();
   if (threadIdx.x == 0) {
+    // a forced step accepts its first pivot without the threshold; the block's later pivots were
+    // chosen from the block alone and pass the a-posteriori tests like any other
     int q = 0;
     while (q < eb) {
+      const bool checked = !(force && q == 0);
       const signed char ty = spv[q];
       const double cm = __longlong_as_double(static_cast<long long>(scm[q]));
       if (ty == 0) {
-        if (!force && __longlong_as_double(static_cast<long long>(srm[q])) > thr) break;
+        if (checked && __longlong_as_double(static_cast<long long>(srm[q])) > thr) break;
         q += 1;
       } else if (ty == 1) {
-        if (!force && cm > inv_u) break;
+        if (checked && cm > inv_u) break;
         q += 1;
       } else {
         const double cm2 = __longlong_as_double(static_cast<long long>(scm[q + 1]));
-        if (!force && fmax(cm, cm2) > inv_u) break;
+        if (checked && fmax(cm, cm2) > inv_u) break;
         q += 2;
       }
     }
@@ -1005,7 +1044,7 @@ __device__ int app_accept(AppFront& F, int rank, bool force, double thr, double 
       cw->pos += pos;
       cw->zero += zero;
       cw->two += two;
-      if (force) cw->forced += q;
+      if (force && q > 0) cw->forced += spv[0] == 2 ? 2 : 1;
     }
   }
   return q;

@@ -158,6 +158,7 @@ void GpuFactor::build_plan() {
     vec += d.m - d.k;
     d.scratch_off = 0;
     d.inv_off = inv_total;
+    d.w_off = -1;
     inv_total += static_cast<std::int64_t>((d.k + 30) / 31 + 1) * 1024;
   }
   vec_total_ = vec;
@@ -165,6 +166,9 @@ void GpuFactor::build_plan() {
   if (solve_coop_max_ == 0) solve_coop_max_ = solve_coop_max_ctas(opt_.device);
   std::vector<std::int64_t> work_offs;
   std::int64_t work_max = 0;
+  std::vector<int2> sbl;
+  std::vector<int4> tiles;
+  std::int64_t w_total = 0;
   ncoop_ = 0;
   std::vector<std::int32_t> lists;
   std::vector<int2> items;
@@ -211,9 +215,17 @@ void GpuFactor::build_plan() {
         const SnDev& dd = sn[all[q]];
         wts[q] = static_cast<double>(dd.m) * dd.k;
         wsum += wts[q];
-        steps = std::max(steps, (dd.k + 30) / 31);
+        steps = std::max(steps, (dd.k + kSB - 1) / kSB);
         work_offs.push_back(wofs);
-        wofs += 8 * static_cast<std::int64_t>(dd.m) + dd.k / 2 + 2;
+        wofs += 8 * static_cast<std::int64_t>(dd.m) + 8 * static_cast<std::int64_t>(dd.k) + dd.k / 2 + 2;
+        SnDev& dw = sn[all[q]];
+        dw.w_off = w_total;
+        w_total += static_cast<std::int64_t>(dw.m) * dw.k;
+        for (int b = 0, qb = 0; b < dw.k; b += kSB, ++qb) {
+          sbl.push_back(make_int2(all[q], qb));
+          const int be = std::min(b + kSB, dw.k);
+          for (int r0 = be; r0 < dw.m; r0 += 64) tiles.push_back(make_int4(all[q], qb, r0, 0));
+        }
       }
       work_max = std::max(work_max, wofs);
       std::vector<int> nr(all.size());
@@ -314,6 +326,12 @@ void GpuFactor::build_plan() {
   d_inv_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, inv_total)));
   d_work_off_.upload(work_offs, stream_);
   d_work_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, work_max)));
+  d_w_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, w_total)));
+  d_sbl_.upload(sbl, stream_);
+  d_tiles_.upload(tiles, stream_);
+  nsbl_ = static_cast<int>(sbl.size());
+  ntiles_ = static_cast<int>(tiles.size());
+  w_ready_ = false;
   d_blk_.alloc(static_cast<std::size_t>(n_));
   d_nblk_.alloc(static_cast<std::size_t>(std::max(1, ns)));
   for (std::int32_t s = 0; s < ns; ++s)
@@ -363,6 +381,7 @@ hsg_inertia_t GpuFactor::factorize(double alpha, double beta, bool detection) {
   HSG_REQUIRE(std::isfinite(alpha) && std::isfinite(beta), HSG_INVALID_INPUT, "non-finite alpha / beta");
   DeviceGuard g(opt_.device);
   factored_ = false;
+  w_ready_ = false;
   const auto t0 = std::chrono::steady_clock::now();
   FactorCounters c{};
   int replans = 0;
@@ -425,6 +444,7 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
     ld = n_;
   }
   cuda_check(cudaEventRecord(ev0_, s), "event");
+  build_solve_operator();
   launch_gather_scale(n_, nr, db, ld, d_scale_.p, d_iperm_.p, d_xwork_.p, s);
   const std::int32_t* lists = d_lists_.p;
   // chunks of at most 8 right-hand sides (the cooperative sweeps carry 8)
@@ -434,8 +454,8 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
     for (const LevelPlan& L : levels_) {
       if (L.solve_coop) {
         cuda_check(launch_solve_fwd_coop(lists + L.all_off, lists + L.solve_cta_off, L.all_n, L.solve_ctas, L.solve_steps,
-                                         d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p, d_panels_.p, d_pidx_.p,
-                                         d_blk_.p, d_nblk_.p, d_inv_.p, xw, n_, d_vec_.p, nc, d_work_.p,
+                                         d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p, d_w_.p, d_pidx_.p, xw, n_,
+                                         d_vec_.p, nc, d_work_.p,
                                          d_work_off_.p + L.work_off_off, s),
                    "cooperative forward solve");
       } else {
@@ -447,8 +467,8 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
     for (auto it = levels_.rbegin(); it != levels_.rend(); ++it) {
       if (it->solve_coop) {
         cuda_check(launch_solve_bwd_coop(lists + it->all_off, lists + it->solve_cta_off, it->all_n, it->solve_ctas,
-                                         it->solve_steps, d_sn_.p, d_rows_.p, d_panels_.p, d_pidx_.p, d_blk_.p,
-                                         d_nblk_.p, d_inv_.p, xw, n_, nc, d_work_.p, d_work_off_.p + it->work_off_off, s),
+                                         it->solve_steps, d_sn_.p, d_rows_.p, d_w_.p, d_pidx_.p, xw, n_, nc, d_work_.p,
+                                         d_work_off_.p + it->work_off_off, s),
                    "cooperative backward solve");
       } else {
         launch_solve_bwd(lists + it->all_off, it->all_n, it->maxm, d_sn_.p, d_rows_.p, d_panels_.p, d_pidx_.p, d_blk_.p,
@@ -494,6 +514,7 @@ void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ld
   const int nr = static_cast<int>(nrhs);
   double* xwork = scratch;
   double* vec = scratch + static_cast<std::size_t>(n_) * nr;
+  build_solve_operator();
   launch_gather_scale(n_, nr, b, ldb, d_scale_.p, d_iperm_.p, xwork, s);
   const std::int32_t* lists = d_lists_.p;
   for (int c0 = 0; c0 < nr; c0 += 8) {
@@ -502,8 +523,8 @@ void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ld
     for (const LevelPlan& L : levels_) {
       if (L.solve_coop) {
         cuda_check(launch_solve_fwd_coop(lists + L.all_off, lists + L.solve_cta_off, L.all_n, L.solve_ctas, L.solve_steps,
-                                         d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p, d_panels_.p, d_pidx_.p,
-                                         d_blk_.p, d_nblk_.p, d_inv_.p, xw, n_, vec, nc, d_work_.p,
+                                         d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p, d_w_.p, d_pidx_.p, xw, n_,
+                                         vec, nc, d_work_.p,
                                          d_work_off_.p + L.work_off_off, s),
                    "cooperative forward solve");
       } else {
@@ -515,8 +536,8 @@ void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ld
     for (auto it = levels_.rbegin(); it != levels_.rend(); ++it) {
       if (it->solve_coop) {
         cuda_check(launch_solve_bwd_coop(lists + it->all_off, lists + it->solve_cta_off, it->all_n, it->solve_ctas,
-                                         it->solve_steps, d_sn_.p, d_rows_.p, d_panels_.p, d_pidx_.p, d_blk_.p,
-                                         d_nblk_.p, d_inv_.p, xw, n_, nc, d_work_.p, d_work_off_.p + it->work_off_off, s),
+                                         it->solve_steps, d_sn_.p, d_rows_.p, d_w_.p, d_pidx_.p, xw, n_, nc, d_work_.p,
+                                         d_work_off_.p + it->work_off_off, s),
                    "cooperative backward solve");
       } else {
         launch_solve_bwd(lists + it->all_off, it->all_n, it->maxm, d_sn_.p, d_rows_.p, d_panels_.p, d_pidx_.p, d_blk_.p,
@@ -527,6 +548,12 @@ void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ld
   launch_scatter_scale(n_, nr, b, ldb, d_scale_.p, d_iperm_.p, xwork, s);
   cuda_check(cudaGetLastError(), "solve launch");
   cuda_check(cudaStreamSynchronize(s), "solve");
+}
+
+void GpuFactor::build_solve_operator() {
+  if (w_ready_) return;
+  launch_sb_build(d_sbl_.p, nsbl_, d_tiles_.p, ntiles_, d_sn_.p, d_panels_.p, d_piv_.p, d_w_.p, stream_);
+  w_ready_ = true;
 }
 
 void GpuFactor::release() {

@@ -139,6 +139,13 @@ class GpuFactor {
   DevBuf<int> d_level_done_;
   DevBuf<std::int64_t> d_work_off_;
   DevBuf<double> d_work_;
+  // super-block solve operators of the large fronts (built at the first solve after a factorization)
+  DevBuf<double> d_w_;
+  DevBuf<int2> d_sbl_;
+  DevBuf<int4> d_tiles_;
+  int nsbl_ = 0, ntiles_ = 0;
+  bool w_ready_ = false;
+  void build_solve_operator();
   int solve_coop_max_ = 0;
   int coop_max_ = 0;
   int ncoop_ = 0;

@@ -293,11 +293,20 @@ __global__ void __launch_bounds__(256) k_solve_bwd(const std::int32_t* list, con
 
 // ---------------------------------------------------------------- cooperative sweeps (few large fronts)
 //
-// The fronts of a level share the grid (front f owns CTAs [cta_start[f], cta_start[f+1])); the
-// front's right-hand sides live in a global work vector t (m rows x 8 columns, column-major with
-// leading dimension m). Each block step of <= 32 pivots is one grid barrier: every CTA of the front
-// recomputes the block's 32 x 32 product from t (loaded past L1, since other CTAs wrote it) and
-// updates its share of the rows (forward) or columns (backward) that depend on it.
+// The large fronts of the top levels are solved by super-blocks of kSB = 128 pivots. For a
+// super-block B = [b, b + bs) of a front with unit lower panel L (m x k, the 2 x 2 pivots'
+// coupling entries read as zero), the solve uses
+//     W[B, B]     = L_BB^{-1}                 (lower triangular, zero above the diagonal)
+//     W[i, B]     = L[i, B] L_BB^{-1},  i >= b + bs,
+// stored like the panel (column-major, ld m) in a separate buffer and built once per factorization
+// before its first solve. Then the forward sweep L z = t is, super-block by super-block,
+//     z_B = W[B, B] t_B,     t_i -= W[i, B] t_B  (i below B),
+// and the backward sweep L^T x = t is, from the last super-block to the first,
+//     x_B = s_B,             s_j -= W[B, j]^T x_B  (every earlier pivot j),
+// with s_j initialised to (W[A, A]^T t_A)_j - W[CB rows, j]^T x_CB for j in super-block A. Every
+// step of both sweeps is one grid barrier and one read of the W entries it needs; each row (forward)
+// or column (backward) is owned by one thread group per step, so no atomics are used and the sums
+// are formed in a fixed order.
 
 namespace {
 
@@ -309,17 +318,114 @@ __device__ __forceinline__ int front_of(const std::int32_t* cta_start, int nfron
 
 }  // namespace
 
+// W[B, B] = L_BB^{-1} for one super-block per CTA: row-by-row substitution X[i, c] =
+// -sum_{c <= j < i} L[i, j] X[j, c] on packed triangles in shared memory (two threads per column).
+__global__ void __launch_bounds__(256) k_sb_inverse(const int2* sbl, const SnDev* sn, const double* panels,
+                                                     const signed char* piv, double* W) {
+  extern __shared__ double sm[];
+  double* Lp = sm;                                // strictly lower rows, row i at i(i-1)/2
+  double* Xp = sm + kSB * (kSB - 1) / 2;          // lower rows incl. diagonal, row i at i(i+1)/2
+  double* part = Xp + kSB * (kSB + 1) / 2;        // second-half partial sums
+  const int2 e = sbl[blockIdx.x];
+  const SnDev d = sn[e.x];
+  const int m = d.m;
+  const int b = e.y * kSB, bs = min(kSB, d.k - b);
+  const double* P = panels + d.panel_off;
+  const signed char* pv = piv + d.first;
+  for (int idx = threadIdx.x; idx < bs * bs; idx += blockDim.x) {
+    const int j = idx / bs, i = idx % bs;
+    if (i > j) Lp[i * (i - 1) / 2 + j] = (j + 1 == i && pv[b + j] == 2) ? 0.0 : P[(b + i) + static_cast<std::int64_t>(b + j) * m];
+  }
+  __syncthreads();
+  const int c = threadIdx.x & (kSB - 1), h = threadIdx.x / kSB;
+  for (int i = 0; i < bs; ++i) {
+    double acc = 0.0;
+    const double* Li = Lp + i * (i - 1) / 2;
+    for (int j = h; j < i; j += 2)
+      if (j >= c) acc = fma(Li[j], Xp[j * (j + 1) / 2 + c], acc);
+    if (h == 1) part[c] = acc;
+    __syncthreads();
+    if (h == 0 && c <= i) Xp[i * (i + 1) / 2 + c] = c == i ? 1.0 : -(acc + part[c]);
+    __syncthreads();
+  }
+  double* Wd = W + d.w_off + b + static_cast<std::int64_t>(b) * m;
+  for (int idx = threadIdx.x; idx < bs * bs; idx += blockDim.x) {
+    const int cc = idx / bs, i = idx % bs;
+    Wd[i + static_cast<std::int64_t>(cc) * m] = i >= cc ? Xp[i * (i + 1) / 2 + cc] : 0.0;
+  }
+}
+
+// W[r0 : r0 + 64, B] = L[r0 : r0 + 64, B] W[B, B] for one 64-row tile below a super-block per CTA.
+__global__ void __launch_bounds__(256) k_sb_apply(const int4* tiles, const SnDev* sn, const double* panels,
+                                                   const signed char* piv, double* W) {
+  __shared__ double Ls[32][64];
+  __shared__ double Xs[32][kSB];
+  const int4 e = tiles[blockIdx.x];
+  const SnDev d = sn[e.x];
+  const int m = d.m;
+  const int b = e.y * kSB, bs = min(kSB, d.k - b), r0 = e.z;
+  const double* P = panels + d.panel_off;
+  const signed char* pv = piv + d.first;
+  double* Wf = W + d.w_off;
+  const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;  // rows tr + 16 q, columns tc * 8 + p
+  double acc[4][8];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int p = 0; p < 8; ++p) acc[q][p] = 0.0;
+  for (int j0 = 0; j0 < bs; j0 += 32) {
+    for (int idx = threadIdx.x; idx < 32 * 64; idx += blockDim.x) {
+      const int jj = idx / 64, row = idx % 64, i = r0 + row, j = j0 + jj;
+      // a 2 x 2 pivot split by the super-block boundary: its coupling entry is D, not L
+      const bool coupling = i == b + j + 1 && pv[b + j] == 2;
+      Ls[jj][row] = (i < m && j < bs && !coupling) ? P[i + static_cast<std::int64_t>(b + j) * m] : 0.0;
+    }
+    for (int idx = threadIdx.x; idx < 32 * kSB; idx += blockDim.x) {
+      const int cc = idx / 32, jj = idx % 32, j = j0 + jj;
+      Xs[jj][cc] = (j < bs && cc < bs) ? Wf[(b + j) + static_cast<std::int64_t>(b + cc) * m] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int jj = 0; jj < 32; ++jj) {
+      double a[4], x[8];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) a[q] = Ls[jj][tr + 16 * q];
+#pragma unroll
+      for (int p = 0; p < 8; ++p) x[p] = Xs[jj][tc * 8 + p];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int p = 0; p < 8; ++p) acc[q][p] = fma(a[q], x[p], acc[q][p]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int i = r0 + tr + 16 * q;
+    if (i >= m) continue;
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+      const int cc = tc * 8 + p;
+      if (cc < bs) Wf[i + static_cast<std::int64_t>(b + cc) * m] = acc[q][p];
+    }
+  }
+}
+
+// Forward sweep of the level's large fronts (front f owns CTAs [cta_start[f], cta_start[f+1])).
+// Per super-block step each CTA takes 32-row groups of the rows at and below the super-block;
+// its 8 warps split the super-block's 128 columns (16 each, lane = row) and add their partial
+// sums in shared memory in warp order.
 __global__ void __launch_bounds__(256) k_solve_fwd_coop(const std::int32_t* list, const std::int32_t* cta_start,
                                                          int nfronts, int max_steps, const SnDev* sn,
                                                          const std::int32_t* child_ptr,
                                                          const std::int32_t* children, const std::int32_t* rmap,
-                                                         const double* panels, const std::int32_t* pidx,
-                                                         const std::int32_t* blk, const std::int32_t* nblk,
-                                                         const double* inv, double* x, std::int64_t n, double* vec,
-                                                         int nrhs, double* work, const std::int64_t* work_off) {
+                                                         const double* W, const std::int32_t* pidx, double* x,
+                                                         std::int64_t n, double* vec, int nrhs, double* work,
+                                                         const std::int64_t* work_off) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
-  __shared__ double zb[32 * 8];
+  __shared__ double tb[kSB * 8];
+  __shared__ double red[8][32][9];
   const int f = front_of(cta_start, nfronts);
   const int rank = static_cast<int>(blockIdx.x) - cta_start[f];
   const int nr = cta_start[f + 1] - cta_start[f];
@@ -327,14 +433,12 @@ __global__ void __launch_bounds__(256) k_solve_fwd_coop(const std::int32_t* list
   const SnDev d = sn[s];
   const int m = d.m, k = d.k, c = m - k;
   double* t = work + work_off[f];  // t[r * m + i]
-  const double* P = panels + d.panel_off;
+  const double* Wf = W + d.w_off;
   const std::int32_t* pl = pidx + d.first;
-  const std::int32_t* bst = blk + d.first;
-  const int nb = nblk[s];
-  const double* Linv = inv + d.inv_off;
   const int gt = rank * blockDim.x + threadIdx.x, gs = nr * blockDim.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // gather: pivot rows from x, zero elsewhere; rank 0 then adds the children's contributions
-  int* invp = reinterpret_cast<int*>(t + static_cast<std::int64_t>(8) * m);
+  int* invp = reinterpret_cast<int*>(t + static_cast<std::int64_t>(8) * m + static_cast<std::int64_t>(8) * k);
   for (int i = gt; i < m; i += gs)
     for (int r = 0; r < nrhs; ++r) t[r * m + i] = i < k ? x[d.first + pl[i] + static_cast<std::int64_t>(r) * n] : 0.0;
   for (int i = gt; i < k; i += gs) invp[pl[i]] = i;
@@ -354,35 +458,44 @@ __global__ void __launch_bounds__(256) k_solve_fwd_coop(const std::int32_t* list
     }
   }
   grid.sync();
+  const int nsb = (k + kSB - 1) / kSB;
   for (int step = 0; step < max_steps; ++step) {
-    if (step < nb) {
-      const int b = bst[step];
-      const int be = step + 1 < nb ? bst[step + 1] : k;
-      const int bs = be - b;
-      const double* Li = Linv + static_cast<std::int64_t>(step) * 1024;
-      {
-        const int i = threadIdx.x % 32, r = threadIdx.x / 32;
-        if (i < bs && r < nrhs) {
-          double acc = 0.0;
-          for (int cc = 0; cc <= i; ++cc) acc += Li[cc * 32 + i] * __ldcg(&t[r * m + b + cc]);
-          zb[i * 8 + r] = acc;
-        }
+    if (step < nsb) {
+      const int b = step * kSB, be = min(b + kSB, k), bs = be - b;
+      for (int idx = threadIdx.x; idx < kSB * 8; idx += blockDim.x) {
+        const int j = idx >> 3, r = idx & 7;
+        tb[idx] = (j < bs && r < nrhs) ? __ldcg(&t[r * m + b + j]) : 0.0;
       }
       __syncthreads();
-      if (rank == 0) {
-        const int i = threadIdx.x % 32, r = threadIdx.x / 32;
-        if (i < bs && r < nrhs) x[d.first + pl[b + i] + static_cast<std::int64_t>(r) * n] = zb[i * 8 + r];
-      }
-      for (int i = be + gt; i < m; i += gs) {
+      const int ng = (m - b + 31) / 32;
+      for (int g = rank; g < ng; g += nr) {
+        const int i = b + g * 32 + lane;
         double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        const double* Li0 = P + i + static_cast<std::int64_t>(b) * m;
-#pragma unroll 8
-        for (int j = 0; j < bs; ++j) {
-          const double l = Li0[static_cast<std::int64_t>(j) * m];
+        if (i < m) {
+          const int j0 = warp * 16;
+          double wv[16];
 #pragma unroll
-          for (int r = 0; r < 8; ++r) acc[r] = fma(l, zb[j * 8 + r], acc[r]);
+          for (int jj = 0; jj < 16; ++jj) wv[jj] = j0 + jj < bs ? Wf[i + static_cast<std::int64_t>(b + j0 + jj) * m] : 0.0;
+#pragma unroll
+          for (int jj = 0; jj < 16; ++jj)
+#pragma unroll
+            for (int r = 0; r < 8; ++r) acc[r] = fma(wv[jj], tb[(j0 + jj) * 8 + r], acc[r]);
         }
-        for (int r = 0; r < nrhs; ++r) t[r * m + i] -= acc[r];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) red[warp][lane][r] = acc[r];
+        __syncthreads();
+        {
+          const int row = threadIdx.x >> 3, r = threadIdx.x & 7;
+          const int ii = b + g * 32 + row;
+          if (ii < m && r < nrhs) {
+            double v = 0.0;
+#pragma unroll
+            for (int w = 0; w < 8; ++w) v += red[w][row][r];
+            if (ii < be) x[d.first + pl[ii] + static_cast<std::int64_t>(r) * n] = v;
+            else t[r * m + ii] = __ldcg(&t[r * m + ii]) - v;
+          }
+        }
+        __syncthreads();
       }
     }
     grid.sync();
@@ -392,82 +505,106 @@ __global__ void __launch_bounds__(256) k_solve_fwd_coop(const std::int32_t* list
     for (int r = 0; r < nrhs; ++r) v[a + static_cast<std::int64_t>(r) * c] = __ldcg(&t[r * m + k + a]);
 }
 
+// Backward sweep of the level's large fronts. Columns are owned by groups of 8 lanes (4 per warp);
+// a group reduces its column's dot products over the lanes with shuffles.
 __global__ void __launch_bounds__(256) k_solve_bwd_coop(const std::int32_t* list, const std::int32_t* cta_start,
                                                          int nfronts, int max_steps, const SnDev* sn,
-                                                         const std::int32_t* rows, const double* panels,
-                                                         const std::int32_t* pidx, const std::int32_t* blk,
-                                                         const std::int32_t* nblk, const double* inv, double* x,
-                                                         std::int64_t n, int nrhs, double* work,
-                                                         const std::int64_t* work_off) {
+                                                         const std::int32_t* rows, const double* W,
+                                                         const std::int32_t* pidx, double* x, std::int64_t n,
+                                                         int nrhs, double* work, const std::int64_t* work_off) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
-  __shared__ double zb[32 * 8];
+  __shared__ double xb[kSB * 8];
   const int f = front_of(cta_start, nfronts);
   const int rank = static_cast<int>(blockIdx.x) - cta_start[f];
   const int nr = cta_start[f + 1] - cta_start[f];
   const int s = list[f];
   const SnDev d = sn[s];
   const int m = d.m, k = d.k;
-  double* t = work + work_off[f];
-  const double* P = panels + d.panel_off;
+  double* t = work + work_off[f];                              // t[r * m + i]
+  double* sv = t + static_cast<std::int64_t>(8) * m;           // sv[r * k + j]
+  const double* Wf = W + d.w_off;
   const std::int32_t* pl = pidx + d.first;
   const std::int32_t* rw = rows + d.rows_off;
-  const std::int32_t* bst = blk + d.first;
-  const int nb = nblk[s];
-  const double* Linv = inv + d.inv_off;
   const int gt = rank * blockDim.x + threadIdx.x, gs = nr * blockDim.x;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gw = rank * (blockDim.x >> 5) + warp, gws = nr * (blockDim.x >> 5);
+  const int sub = threadIdx.x & 7, gsub = (threadIdx.x >> 3) & 3;
+  const int wbase = rank * (blockDim.x >> 3) + (threadIdx.x >> 5) * 4, ngrp = nr * (blockDim.x >> 3);
   for (int i = gt; i < m; i += gs)
     for (int r = 0; r < nrhs; ++r)
       t[r * m + i] = i < k ? x[d.first + pl[i] + static_cast<std::int64_t>(r) * n] : x[rw[i] + static_cast<std::int64_t>(r) * n];
   grid.sync();
-  // contributions of the contribution-block rows: warp per pivot column, lanes over rows
-  for (int j = gw; j < k; j += gws) {
+  // sv_j = (W[A, A]^T t_A)_j - W[k:m, j]^T t[k:m]; the loop bounds are uniform over each warp
+  for (int base = wbase; base < k; base += ngrp) {
+    const int j = base + gsub;
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    const double* Lj = P + static_cast<std::int64_t>(j) * m;
-    for (int i = k + lane; i < m; i += 32) {
-      const double l = Lj[i];
+    if (j < k) {
+      const double* Wj = Wf + static_cast<std::int64_t>(j) * m;
+      const int beA = min((j / kSB + 1) * kSB, k);
+      for (int i = j + sub; i < beA; i += 8) {
+        const double w = Wj[i];
 #pragma unroll
-      for (int r = 0; r < 8; ++r)
-        if (r < nrhs) acc[r] = fma(l, __ldcg(&t[r * m + i]), acc[r]);
+        for (int r = 0; r < 8; ++r)
+          if (r < nrhs) acc[r] = fma(w, __ldcg(&t[r * m + i]), acc[r]);
+      }
+      for (int i = k + sub; i < m; i += 8) {
+        const double w = Wj[i];
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+          if (r < nrhs) acc[r] = fma(-w, __ldcg(&t[r * m + i]), acc[r]);
+      }
     }
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
-      if (r >= nrhs) break;
-      const double sum = warp_sum(acc[r]);
-      if (lane == 0) t[r * m + j] -= sum;
+      acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 4);
+      acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 2);
+      acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 1);
+    }
+    if (j < k && sub == 0) {
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+        if (r < nrhs) sv[r * k + j] = acc[r];
     }
   }
   grid.sync();
+  const int nsb = (k + kSB - 1) / kSB;
   for (int step = 0; step < max_steps; ++step) {
-    const int bi = nb - 1 - step;
-    if (bi >= 0) {
-      const int b = bst[bi];
-      const int be = bi + 1 < nb ? bst[bi + 1] : k;
-      const int bs = be - b;
-      const double* Li = Linv + static_cast<std::int64_t>(bi) * 1024;
-      {
-        const int cc = threadIdx.x % 32, r = threadIdx.x / 32;
-        if (cc < bs && r < nrhs) {
-          double acc = 0.0;
-          for (int i = cc; i < bs; ++i) acc += Li[cc * 32 + i] * __ldcg(&t[r * m + b + i]);
-          zb[cc * 8 + r] = acc;
-        }
+    const int q = nsb - 1 - step;
+    if (q >= 0) {
+      const int b = q * kSB, be = min(b + kSB, k), bs = be - b;
+      for (int idx = threadIdx.x; idx < kSB * 8; idx += blockDim.x) {
+        const int i = idx >> 3, r = idx & 7;
+        xb[idx] = (i < bs && r < nrhs) ? __ldcg(&sv[r * k + b + i]) : 0.0;
       }
       __syncthreads();
-      if (rank == 0) {
-        const int cc = threadIdx.x % 32, r = threadIdx.x / 32;
-        if (cc < bs && r < nrhs) x[d.first + pl[b + cc] + static_cast<std::int64_t>(r) * n] = zb[cc * 8 + r];
-      }
-      // earlier pivots j < b: warp per column, lanes over the block's rows (contiguous in the column)
-      for (int j = gw; j < b; j += gws) {
-        const double l = lane < bs ? P[b + lane + static_cast<std::int64_t>(j) * m] : 0.0;
+      if (rank == 0)
+        for (int idx = threadIdx.x; idx < bs * 8; idx += blockDim.x) {
+          const int i = idx >> 3, r = idx & 7;
+          if (r < nrhs) x[d.first + pl[b + i] + static_cast<std::int64_t>(r) * n] = xb[idx];
+        }
+      // earlier pivots j < b: sv_j -= W[B, j]^T x_B
+      for (int base = wbase; base < b; base += ngrp) {
+        const int j = base + gsub;
+        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (j < b) {
+          const double* Wj = Wf + b + static_cast<std::int64_t>(j) * m;
+          double wv[16];
+#pragma unroll
+          for (int u = 0; u < 16; ++u) wv[u] = sub + 8 * u < bs ? Wj[sub + 8 * u] : 0.0;
+#pragma unroll
+          for (int u = 0; u < 16; ++u)
+#pragma unroll
+            for (int r = 0; r < 8; ++r) acc[r] = fma(wv[u], xb[(sub + 8 * u) * 8 + r], acc[r]);
+        }
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
-          if (r >= nrhs) break;
-          const double sum = warp_sum(l * zb[(lane < bs ? lane : 0) * 8 + r]);
-          if (lane == 0) t[r * m + j] -= sum;
+          acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 4);
+          acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 2);
+          acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 1);
+        }
+        if (j < b && sub == 0) {
+#pragma unroll
+          for (int r = 0; r < 8; ++r)
+            if (r < nrhs) sv[r * k + j] = __ldcg(&sv[r * k + j]) - acc[r];
         }
       }
     }
@@ -557,25 +694,39 @@ int solve_coop_max_ctas(int device) {
   return (a < b ? a : b) * sms;
 }
 
+void launch_sb_build(const int2* sbl, int nsb, const int4* tiles, int ntiles, const SnDev* sn, const double* panels,
+                     const signed char* piv, double* W, cudaStream_t s) {
+  if (nsb <= 0) return;
+  constexpr std::size_t smem = sizeof(double) * (kSB * (kSB - 1) / 2 + kSB * (kSB + 1) / 2 + kSB);
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_sb_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    configured = true;
+  }
+  note_launches(1);
+  k_sb_inverse<<<nsb, 256, smem, s>>>(sbl, sn, panels, piv, W);
+  if (ntiles > 0) {
+    note_launches(1);
+    k_sb_apply<<<ntiles, 256, 0, s>>>(tiles, sn, panels, piv, W);
+  }
+}
+
 cudaError_t launch_solve_fwd_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
                                   int max_steps, const SnDev* sn, const std::int32_t* child_ptr,
-                                  const std::int32_t* children, const std::int32_t* rmap, const double* panels,
-                                  const std::int32_t* pidx, const std::int32_t* blk, const std::int32_t* nblk,
-                                  const double* inv, double* x, std::int64_t n, double* vec, int nrhs, double* work,
-                                  const std::int64_t* work_off, cudaStream_t s) {
-  void* args[] = {&list, &cta_start, &nfronts, &max_steps, &sn, &child_ptr, &children, &rmap, &panels, &pidx, &blk,
-                  &nblk, &inv, &x, &n, &vec, &nrhs, &work, &work_off};
+                                  const std::int32_t* children, const std::int32_t* rmap, const double* W,
+                                  const std::int32_t* pidx, double* x, std::int64_t n, double* vec, int nrhs,
+                                  double* work, const std::int64_t* work_off, cudaStream_t s) {
+  void* args[] = {&list, &cta_start, &nfronts, &max_steps, &sn, &child_ptr, &children, &rmap, &W, &pidx,
+                  &x, &n, &vec, &nrhs, &work, &work_off};
   note_launches(1);
   return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_solve_fwd_coop), dim3(nctas), dim3(256), args, 0, s);
 }
 
 cudaError_t launch_solve_bwd_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
-                                  int max_steps, const SnDev* sn, const std::int32_t* rows, const double* panels,
-                                  const std::int32_t* pidx, const std::int32_t* blk, const std::int32_t* nblk,
-                                  const double* inv, double* x, std::int64_t n, int nrhs, double* work,
+                                  int max_steps, const SnDev* sn, const std::int32_t* rows, const double* W,
+                                  const std::int32_t* pidx, double* x, std::int64_t n, int nrhs, double* work,
                                   const std::int64_t* work_off, cudaStream_t s) {
-  void* args[] = {&list, &cta_start, &nfronts, &max_steps, &sn, &rows, &panels, &pidx, &blk, &nblk, &inv, &x, &n,
-                  &nrhs, &work, &work_off};
+  void* args[] = {&list, &cta_start, &nfronts, &max_steps, &sn, &rows, &W, &pidx, &x, &n, &nrhs, &work, &work_off};
   note_launches(1);
   return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_solve_bwd_coop), dim3(nctas), dim3(256), args, 0, s);
 }

@@ -34,18 +34,22 @@ void launch_solve_bwd(const std::int32_t* list, int nlist, int maxm, const SnDev
                       const std::int32_t* nblk, const double* inv, double* x, std::int64_t n, int nrhs,
                       cudaStream_t s);
 
-// cooperative sweeps over the few large fronts of a level (nrhs <= 8 per launch)
+// cooperative sweeps over the few large fronts of a level (nrhs <= 8 per launch), by super-blocks of
+// kSB pivots whose solve operator W (L_BB^{-1} on the diagonal block, L L_BB^{-1} below it) is built
+// once per factorization by launch_sb_build
+constexpr int kSB = 128;
+// sbl: (front, super-block) pairs; tiles: (front, super-block, first row) of the 64-row tiles below
+void launch_sb_build(const int2* sbl, int nsb, const int4* tiles, int ntiles, const SnDev* sn, const double* panels,
+                     const signed char* piv, double* W, cudaStream_t s);
 int solve_coop_max_ctas(int device);
 cudaError_t launch_solve_fwd_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
                                   int max_steps, const SnDev* sn, const std::int32_t* child_ptr,
-                                  const std::int32_t* children, const std::int32_t* rmap, const double* panels,
-                                  const std::int32_t* pidx, const std::int32_t* blk, const std::int32_t* nblk,
-                                  const double* inv, double* x, std::int64_t n, double* vec, int nrhs, double* work,
-                                  const std::int64_t* work_off, cudaStream_t s);
+                                  const std::int32_t* children, const std::int32_t* rmap, const double* W,
+                                  const std::int32_t* pidx, double* x, std::int64_t n, double* vec, int nrhs,
+                                  double* work, const std::int64_t* work_off, cudaStream_t s);
 cudaError_t launch_solve_bwd_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
-                                  int max_steps, const SnDev* sn, const std::int32_t* rows, const double* panels,
-                                  const std::int32_t* pidx, const std::int32_t* blk, const std::int32_t* nblk,
-                                  const double* inv, double* x, std::int64_t n, int nrhs, double* work,
+                                  int max_steps, const SnDev* sn, const std::int32_t* rows, const double* W,
+                                  const std::int32_t* pidx, double* x, std::int64_t n, int nrhs, double* work,
                                   const std::int64_t* work_off, cudaStream_t s);
 
 }  // namespace hsg

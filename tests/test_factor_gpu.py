@@ -145,3 +145,24 @@ def test_count_releases_factors():
         f.solve(np.ones(a.shape[0]))
     assert f.factorize(1.0, -1.0)
     f.solve(np.ones(a.shape[0]))
+
+
+@pytest.mark.parametrize("h", [125, 129, 131, 150, 195])
+def test_zero_block_dense_front_two_by_two_solves(h):
+    """One dense front K = [[0, B], [B^T, 0]]: its zero blocks stay zero under elimination, so the
+    pivots are 2 x 2 pivots and pairs fall across the 128-pivot super-blocks of the large-front
+    solve; inertia is exact and solves stay backward stable."""
+    rng = np.random.default_rng(h)
+    n = 2 * h
+    bm = rng.standard_normal((h, h))
+    k = sp.bmat([[None, sp.csr_matrix(bm)], [sp.csr_matrix(bm.T), None]]).tocsr()
+    f = Factorization()
+    f.analyze(k, None, 1.0, 0.0)
+    assert f.factorize(1.0, 0.0)
+    inr = f.inertia()
+    assert inr.two_by_two > n // 4
+    evals = np.linalg.eigvalsh(k.toarray())
+    assert inr.neg == int((evals < 0).sum())
+    b = rng.standard_normal((n, 9))
+    x = f.solve(b)
+    assert backward_error(k, x, b) < 1e-12
