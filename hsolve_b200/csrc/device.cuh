@@ -20,6 +20,15 @@ struct SnDev {
   std::int64_t scratch_off;  // pivoting scratch of the panel kernel (doubles)
   std::int64_t inv_off;      // inverse diagonal blocks (32 x 32 each) of the solve
   std::int64_t w_off;        // super-block solve operator (m x k, ld m) of a large front (-1: none)
+  std::int64_t cptr_off;     // children's contributions per front position (m + 1 offsets; large fronts)
+};
+
+// One child contribution to a front position: entry a of the child's contribution vector
+// (mc rows per right-hand side, at vec_off * nrhs in the solve arena).
+struct ContribEntry {
+  std::int64_t vec_off;
+  std::int32_t a;
+  std::int32_t mc;
 };
 
 // Counters written by the factorization kernels (integers: sums are order independent).

@@ -159,6 +159,7 @@ void GpuFactor::build_plan() {
     d.scratch_off = 0;
     d.inv_off = inv_total;
     d.w_off = -1;
+    d.cptr_off = -1;
     inv_total += static_cast<std::int64_t>((d.k + 30) / 31 + 1) * 1024;
   }
   vec_total_ = vec;
@@ -169,6 +170,9 @@ void GpuFactor::build_plan() {
   std::vector<int2> sbl;
   std::vector<int4> tiles;
   std::int64_t w_total = 0;
+  std::vector<std::int32_t> cptr;
+  std::vector<ContribEntry> cent;
+  int cnt_total = 0;
   ncoop_ = 0;
   std::vector<std::int32_t> lists;
   std::vector<int2> items;
@@ -217,8 +221,35 @@ void GpuFactor::build_plan() {
         wsum += wts[q];
         steps = std::max(steps, (dd.k + kSB - 1) / kSB);
         work_offs.push_back(wofs);
-        wofs += 8 * static_cast<std::int64_t>(dd.m) + 8 * static_cast<std::int64_t>(dd.k) + dd.k / 2 + 2;
+        wofs += 8 * static_cast<std::int64_t>(dd.m) + 8 * static_cast<std::int64_t>(dd.k) + (dd.k + 1) / 2 + 2;
         SnDev& dw = sn[all[q]];
+        // children's contribution entries per front position, in child order
+        {
+          const std::int32_t sq = all[q];
+          dw.cptr_off = static_cast<std::int64_t>(cptr.size());
+          std::vector<std::int32_t> num(dw.m + 1, 0);
+          for (std::int32_t e = S.child_ptr[sq]; e < S.child_ptr[sq + 1]; ++e) {
+            const std::int32_t ch = S.children[e];
+            const int mc = sn[ch].m - sn[ch].k;
+            for (int a = 0; a < mc; ++a) num[S.rmap[S.rmap_off[ch] + a] + 1]++;
+          }
+          for (int i = 0; i < dw.m; ++i) num[i + 1] += num[i];
+          const std::int32_t base = static_cast<std::int32_t>(cent.size());
+          for (int i = 0; i <= dw.m; ++i) cptr.push_back(base + num[i]);
+          cent.resize(cent.size() + num[dw.m]);
+          std::vector<std::int32_t> fill(num.begin(), num.end() - 1);
+          for (std::int32_t e = S.child_ptr[sq]; e < S.child_ptr[sq + 1]; ++e) {
+            const std::int32_t ch = S.children[e];
+            const int mc = sn[ch].m - sn[ch].k;
+            for (int a = 0; a < mc; ++a) {
+              ContribEntry ce;
+              ce.vec_off = sn[ch].vec_off;
+              ce.a = a;
+              ce.mc = mc;
+              cent[base + fill[S.rmap[S.rmap_off[ch] + a]]++] = ce;
+            }
+          }
+        }
         dw.w_off = w_total;
         w_total += static_cast<std::int64_t>(dw.m) * dw.k;
         for (int b = 0, qb = 0; b < dw.k; b += kSB, ++qb) {
@@ -246,6 +277,8 @@ void GpuFactor::build_plan() {
       std::vector<std::int32_t> starts(all.size() + 1, 0);
       for (std::size_t q = 0; q < all.size(); ++q) starts[q + 1] = starts[q] + nr[q];
       L.solve_coop = true;
+      L.cnt_off = cnt_total;
+      cnt_total += static_cast<int>(all.size());
       L.solve_cta_off = static_cast<std::int64_t>(lists.size());
       lists.insert(lists.end(), starts.begin(), starts.end());
       L.solve_ctas = starts.back();
@@ -327,6 +360,11 @@ void GpuFactor::build_plan() {
   d_work_off_.upload(work_offs, stream_);
   d_work_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, work_max)));
   d_w_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, w_total)));
+  d_err_.alloc(1);
+  d_cptr_.upload(cptr, stream_);
+  d_cent_.upload(cent, stream_);
+  d_sweep_cnt_.alloc(static_cast<std::size_t>(std::max(1, 2 * cnt_total)));
+  sweep_cnt_total_ = cnt_total;
   d_sbl_.upload(sbl, stream_);
   d_tiles_.upload(tiles, stream_);
   nsbl_ = static_cast<int>(sbl.size());
@@ -443,6 +481,7 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
     db = d_btmp_.p;
     ld = n_;
   }
+  cuda_check(cudaMemsetAsync(d_err_.p, 0, sizeof(int), s), "reset solve status");
   cuda_check(cudaEventRecord(ev0_, s), "event");
   build_solve_operator();
   launch_gather_scale(n_, nr, db, ld, d_scale_.p, d_iperm_.p, d_xwork_.p, s);
@@ -451,12 +490,12 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
   for (int c0 = 0; c0 < nr; c0 += 8) {
     const int nc = std::min(8, nr - c0);
     double* xw = d_xwork_.p + static_cast<std::int64_t>(c0) * n_;
+    cuda_check(cudaMemsetAsync(d_sweep_cnt_.p, 0, d_sweep_cnt_.n * sizeof(int), s), "reset sweep counters");
     for (const LevelPlan& L : levels_) {
       if (L.solve_coop) {
-        cuda_check(launch_solve_fwd_coop(lists + L.all_off, lists + L.solve_cta_off, L.all_n, L.solve_ctas, L.solve_steps,
-                                         d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p, d_w_.p, d_pidx_.p, xw, n_,
-                                         d_vec_.p, nc, d_work_.p,
-                                         d_work_off_.p + L.work_off_off, s),
+        cuda_check(launch_solve_fwd_coop(lists + L.all_off, lists + L.solve_cta_off, L.all_n, L.solve_ctas, d_sn_.p,
+                                         d_cptr_.p, d_cent_.p, d_w_.p, d_pidx_.p, xw, n_, d_vec_.p, nc, d_work_.p,
+                                         d_work_off_.p + L.work_off_off, d_sweep_cnt_.p + L.cnt_off, d_err_.p, s),
                    "cooperative forward solve");
       } else {
         launch_solve_fwd(lists + L.all_off, L.all_n, L.maxm, d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p,
@@ -467,8 +506,9 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
     for (auto it = levels_.rbegin(); it != levels_.rend(); ++it) {
       if (it->solve_coop) {
         cuda_check(launch_solve_bwd_coop(lists + it->all_off, lists + it->solve_cta_off, it->all_n, it->solve_ctas,
-                                         it->solve_steps, d_sn_.p, d_rows_.p, d_w_.p, d_pidx_.p, xw, n_, nc, d_work_.p,
-                                         d_work_off_.p + it->work_off_off, s),
+                                         d_sn_.p, d_rows_.p, d_w_.p, d_pidx_.p, xw, n_, nc, d_work_.p,
+                                         d_work_off_.p + it->work_off_off,
+                                         d_sweep_cnt_.p + sweep_cnt_total_ + it->cnt_off, d_err_.p, s),
                    "cooperative backward solve");
       } else {
         launch_solve_bwd(lists + it->all_off, it->all_n, it->maxm, d_sn_.p, d_rows_.p, d_panels_.p, d_pidx_.p, d_blk_.p,
@@ -483,7 +523,10 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
     cuda_check(cudaMemcpy2DAsync(b, ldb * sizeof(double), d_btmp_.p, n_ * sizeof(double), n_ * sizeof(double), nr,
                                  cudaMemcpyDeviceToHost, s), "D2H rhs");
   }
+  int err = 0;
+  cuda_check(cudaMemcpyAsync(&err, d_err_.p, sizeof(int), cudaMemcpyDeviceToHost, s), "solve status");
   cuda_check(cudaStreamSynchronize(s), "solve");
+  HSG_REQUIRE(err == 0, HSG_INTERNAL, "solve: a wait between the CTAs of a front timed out");
   {
     float ms = 0.0f;
     cuda_check(cudaEventElapsedTime(&ms, ev0_, ev1_), "event time");
@@ -514,18 +557,19 @@ void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ld
   const int nr = static_cast<int>(nrhs);
   double* xwork = scratch;
   double* vec = scratch + static_cast<std::size_t>(n_) * nr;
+  cuda_check(cudaMemsetAsync(d_err_.p, 0, sizeof(int), s), "reset solve status");
   build_solve_operator();
   launch_gather_scale(n_, nr, b, ldb, d_scale_.p, d_iperm_.p, xwork, s);
   const std::int32_t* lists = d_lists_.p;
   for (int c0 = 0; c0 < nr; c0 += 8) {
     const int nc = std::min(8, nr - c0);
     double* xw = xwork + static_cast<std::int64_t>(c0) * n_;
+    cuda_check(cudaMemsetAsync(d_sweep_cnt_.p, 0, d_sweep_cnt_.n * sizeof(int), s), "reset sweep counters");
     for (const LevelPlan& L : levels_) {
       if (L.solve_coop) {
-        cuda_check(launch_solve_fwd_coop(lists + L.all_off, lists + L.solve_cta_off, L.all_n, L.solve_ctas, L.solve_steps,
-                                         d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p, d_w_.p, d_pidx_.p, xw, n_,
-                                         vec, nc, d_work_.p,
-                                         d_work_off_.p + L.work_off_off, s),
+        cuda_check(launch_solve_fwd_coop(lists + L.all_off, lists + L.solve_cta_off, L.all_n, L.solve_ctas, d_sn_.p,
+                                         d_cptr_.p, d_cent_.p, d_w_.p, d_pidx_.p, xw, n_, vec, nc, d_work_.p,
+                                         d_work_off_.p + L.work_off_off, d_sweep_cnt_.p + L.cnt_off, d_err_.p, s),
                    "cooperative forward solve");
       } else {
         launch_solve_fwd(lists + L.all_off, L.all_n, L.maxm, d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p,
@@ -536,8 +580,9 @@ void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ld
     for (auto it = levels_.rbegin(); it != levels_.rend(); ++it) {
       if (it->solve_coop) {
         cuda_check(launch_solve_bwd_coop(lists + it->all_off, lists + it->solve_cta_off, it->all_n, it->solve_ctas,
-                                         it->solve_steps, d_sn_.p, d_rows_.p, d_w_.p, d_pidx_.p, xw, n_, nc, d_work_.p,
-                                         d_work_off_.p + it->work_off_off, s),
+                                         d_sn_.p, d_rows_.p, d_w_.p, d_pidx_.p, xw, n_, nc, d_work_.p,
+                                         d_work_off_.p + it->work_off_off,
+                                         d_sweep_cnt_.p + sweep_cnt_total_ + it->cnt_off, d_err_.p, s),
                    "cooperative backward solve");
       } else {
         launch_solve_bwd(lists + it->all_off, it->all_n, it->maxm, d_sn_.p, d_rows_.p, d_panels_.p, d_pidx_.p, d_blk_.p,
@@ -547,7 +592,10 @@ void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ld
   }
   launch_scatter_scale(n_, nr, b, ldb, d_scale_.p, d_iperm_.p, xwork, s);
   cuda_check(cudaGetLastError(), "solve launch");
+  int err = 0;
+  cuda_check(cudaMemcpyAsync(&err, d_err_.p, sizeof(int), cudaMemcpyDeviceToHost, s), "solve status");
   cuda_check(cudaStreamSynchronize(s), "solve");
+  HSG_REQUIRE(err == 0, HSG_INTERNAL, "solve: a wait between the CTAs of a front timed out");
 }
 
 void GpuFactor::build_solve_operator() {

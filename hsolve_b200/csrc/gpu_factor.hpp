@@ -106,6 +106,7 @@ class GpuFactor {
     bool solve_coop = false;           // few fronts: cooperative sweeps, CTAs split by panel size
     std::int64_t solve_cta_off = 0; int solve_ctas = 0; int solve_steps = 0;
     std::int64_t work_off_off = 0;     // offsets of the fronts' work vectors (index into d_work_off_)
+    int cnt_off = 0;                   // first publication counter of the level's fronts
   };
   void build_plan();
   void run_numeric(double alpha, double beta, bool detection);
@@ -141,6 +142,11 @@ class GpuFactor {
   DevBuf<double> d_work_;
   // super-block solve operators of the large fronts (built at the first solve after a factorization)
   DevBuf<double> d_w_;
+  DevBuf<int> d_err_;  // set by a solve sweep whose bounded wait ran out
+  DevBuf<std::int32_t> d_cptr_;   // large fronts: children's contributions per position
+  DevBuf<ContribEntry> d_cent_;
+  DevBuf<int> d_sweep_cnt_;       // publication counters: forward slots, then backward slots
+  int sweep_cnt_total_ = 0;
   DevBuf<int2> d_sbl_;
   DevBuf<int4> d_tiles_;
   int nsbl_ = 0, ntiles_ = 0;

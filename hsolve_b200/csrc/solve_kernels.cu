@@ -411,19 +411,62 @@ __global__ void __launch_bounds__(256) k_sb_apply(const int4* tiles, const SnDev
   }
 }
 
+// The sweeps below synchronise their CTAs through per-front publication counters instead of grid
+// barriers: every 32-row group (forward) or 32-column chunk (backward) of a front has one owner CTA
+// for the whole sweep (group G, chunk c: CTA G mod nr, c mod nr). An owner that finishes the values
+// of the next super-block writes them, fences, and adds 1 to the front's counter; a CTA starts a
+// super-block step once the counter shows all of that super-block's groups. The waits are bounded:
+// a wait that runs out sets *err and the sweep goes on with whatever it reads (the host reports it).
+
+namespace {
+
+constexpr long long kSweepSpinLimit = 1LL << 22;
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// all threads: wait until *cnt >= target (thread 0 polls)
+__device__ __forceinline__ void wait_published(const int* cnt, int target, int* err) {
+  if (threadIdx.x == 0 && target > 0) {
+    long long it = 0;
+    while (ld_acquire(cnt) < target) {
+      if (++it > kSweepSpinLimit) { atomicExch(err, 1); break; }
+      __nanosleep(32);
+    }
+  }
+  __syncthreads();
+}
+
+// all threads, after their writes: make them visible, then count one publication
+__device__ __forceinline__ void publish(int* cnt) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) atomicAdd(cnt, 1);
+}
+
+__device__ __forceinline__ int sb_groups(int q, int k) {
+  const int bs = min(kSB, k - q * kSB);
+  return (bs + 31) / 32;
+}
+
+}  // namespace
+
 // Forward sweep of the level's large fronts (front f owns CTAs [cta_start[f], cta_start[f+1])).
-// Per super-block step each CTA takes 32-row groups of the rows at and below the super-block;
-// its 8 warps split the super-block's 128 columns (16 each, lane = row) and add their partial
-// sums in shared memory in warp order.
-__global__ void __launch_bounds__(256) k_solve_fwd_coop(const std::int32_t* list, const std::int32_t* cta_start,
-                                                         int nfronts, int max_steps, const SnDev* sn,
-                                                         const std::int32_t* child_ptr,
-                                                         const std::int32_t* children, const std::int32_t* rmap,
-                                                         const double* W, const std::int32_t* pidx, double* x,
-                                                         std::int64_t n, double* vec, int nrhs, double* work,
-                                                         const std::int64_t* work_off) {
-  namespace cg = cooperative_groups;
-  cg::grid_group grid = cg::this_grid();
+// Each CTA first assembles the right-hand sides of its row groups: the pivot rows' entries of x plus
+// the children's contribution vectors, listed per front position in child order (cptr / cent).
+// In super-block step q the owner of row group G >= 4q forms the group's 32 rows of W[:, B] t_B:
+// its 8 warps split the super-block's columns (16 each, lane = row) and add their partial sums in
+// shared memory in warp order. Rows of B give z_B (written to x), rows below update t; the CB rows
+// write their final values to the front's contribution vector in the last step.
+__global__ void __launch_bounds__(256, 2) k_solve_fwd_coop(const std::int32_t* list, const std::int32_t* cta_start,
+                                                            int nfronts, const SnDev* sn, const std::int32_t* cptr,
+                                                            const ContribEntry* cent, const double* W,
+                                                            const std::int32_t* pidx, double* x, std::int64_t n,
+                                                            double* vec, int nrhs, double* work,
+                                                            const std::int64_t* work_off, int* cnts, int* err) {
   __shared__ double tb[kSB * 8];
   __shared__ double red[8][32][9];
   const int f = front_of(cta_start, nfronts);
@@ -433,85 +476,105 @@ __global__ void __launch_bounds__(256) k_solve_fwd_coop(const std::int32_t* list
   const SnDev d = sn[s];
   const int m = d.m, k = d.k, c = m - k;
   double* t = work + work_off[f];  // t[r * m + i]
+  int* cnt = cnts + f;
   const double* Wf = W + d.w_off;
   const std::int32_t* pl = pidx + d.first;
-  const int gt = rank * blockDim.x + threadIdx.x, gs = nr * blockDim.x;
+  const std::int32_t* cp = cptr + d.cptr_off;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // gather: pivot rows from x, zero elsewhere; rank 0 then adds the children's contributions
-  int* invp = reinterpret_cast<int*>(t + static_cast<std::int64_t>(8) * m + static_cast<std::int64_t>(8) * k);
-  for (int i = gt; i < m; i += gs)
-    for (int r = 0; r < nrhs; ++r) t[r * m + i] = i < k ? x[d.first + pl[i] + static_cast<std::int64_t>(r) * n] : 0.0;
-  for (int i = gt; i < k; i += gs) invp[pl[i]] = i;
-  grid.sync();
-  if (rank == 0) {
-    for (int q = child_ptr[s]; q < child_ptr[s + 1]; ++q) {
-      const SnDev cd = sn[children[q]];
-      const int mc = cd.m - cd.k;
-      const std::int32_t* rm = rmap + cd.rmap_off;
-      const double* cv = vec + cd.vec_off * nrhs;
-      for (int a = threadIdx.x; a < mc; a += blockDim.x) {
-        const int pos = rm[a];
-        const int row = pos < k ? __ldcg(&invp[pos]) : pos;
-        for (int r = 0; r < nrhs; ++r) t[r * m + row] = __ldcg(&t[r * m + row]) + cv[a + static_cast<std::int64_t>(r) * mc];
-      }
-      __syncthreads();
-    }
-  }
-  grid.sync();
+  const int row = threadIdx.x >> 3, rr = threadIdx.x & 7;
+  double* v = vec + d.vec_off * nrhs;
   const int nsb = (k + kSB - 1) / kSB;
-  for (int step = 0; step < max_steps; ++step) {
-    if (step < nsb) {
-      const int b = step * kSB, be = min(b + kSB, k), bs = be - b;
-      for (int idx = threadIdx.x; idx < kSB * 8; idx += blockDim.x) {
-        const int j = idx >> 3, r = idx & 7;
-        tb[idx] = (j < bs && r < nrhs) ? __ldcg(&t[r * m + b + j]) : 0.0;
+  const int ngt = (m + 31) / 32;
+  // assemble the owned row groups; the groups of super-block 0 are published
+  for (int G = rank; G < ngt; G += nr) {
+    const int i = G * 32 + row;
+    if (i < m && rr < nrhs) {
+      const int pos = i < k ? pl[i] : i;
+      double val = i < k ? x[d.first + pos + static_cast<std::int64_t>(rr) * n] : 0.0;
+      for (int e = cp[pos]; e < cp[pos + 1]; ++e) {
+        const ContribEntry ce = cent[e];
+        val += vec[ce.vec_off * nrhs + ce.a + static_cast<std::int64_t>(rr) * ce.mc];
       }
+      t[rr * m + i] = val;
+    }
+    if (G < sb_groups(0, k)) publish(cnt);
+  }
+  int target = 0;
+  for (int q = 0; q < nsb; ++q) {
+    const int b = q * kSB, be = min(b + kSB, k), bs = be - b;
+    target += sb_groups(q, k);
+    int G = rank;
+    if (G < b / 32) G += ((b / 32 - G + nr - 1) / nr) * nr;
+    if (G >= ngt) break;  // no rows left for this CTA
+    const bool last = q + 1 == nsb;
+    const int nb0 = (q + 1) * (kSB / 32), nb1 = last ? nb0 : nb0 + sb_groups(q + 1, k);
+    // prefetch the first group's W entries and the old values it updates (no dependence on the wait)
+    const int j0 = warp * 16;
+    double wv[16];
+    {
+      const int i = G * 32 + lane;
+#pragma unroll
+      for (int jj = 0; jj < 16; ++jj)
+        wv[jj] = (i < m && j0 + jj < bs) ? Wf[i + static_cast<std::int64_t>(b + j0 + jj) * m] : 0.0;
+    }
+    double told = 0.0;
+    {
+      const int ii = G * 32 + row;
+      if (ii >= be && ii < m && rr < nrhs) told = __ldcg(&t[rr * m + ii]);
+    }
+    wait_published(cnt, target, err);
+    for (int idx = threadIdx.x; idx < kSB * 8; idx += blockDim.x) {
+      const int j = idx >> 3, r = idx & 7;
+      tb[idx] = (j < bs && r < nrhs) ? __ldcg(&t[r * m + b + j]) : 0.0;
+    }
+    __syncthreads();
+    for (bool first = true; G < ngt; G += nr, first = false) {
+      const int i = G * 32 + lane;
+      if (!first) {
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj)
+          wv[jj] = (i < m && j0 + jj < bs) ? Wf[i + static_cast<std::int64_t>(b + j0 + jj) * m] : 0.0;
+        const int ii = G * 32 + row;
+        told = (ii >= be && ii < m && rr < nrhs) ? __ldcg(&t[rr * m + ii]) : 0.0;
+      }
+      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int jj = 0; jj < 16; ++jj)
+#pragma unroll
+        for (int r = 0; r < 8; ++r) acc[r] = fma(wv[jj], tb[(j0 + jj) * 8 + r], acc[r]);
+#pragma unroll
+      for (int r = 0; r < 8; ++r) red[warp][lane][r] = acc[r];
       __syncthreads();
-      const int ng = (m - b + 31) / 32;
-      for (int g = rank; g < ng; g += nr) {
-        const int i = b + g * 32 + lane;
-        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        if (i < m) {
-          const int j0 = warp * 16;
-          double wv[16];
+      {
+        const int ii = G * 32 + row;
+        if (ii < m && rr < nrhs) {
+          double val = 0.0;
 #pragma unroll
-          for (int jj = 0; jj < 16; ++jj) wv[jj] = j0 + jj < bs ? Wf[i + static_cast<std::int64_t>(b + j0 + jj) * m] : 0.0;
-#pragma unroll
-          for (int jj = 0; jj < 16; ++jj)
-#pragma unroll
-            for (int r = 0; r < 8; ++r) acc[r] = fma(wv[jj], tb[(j0 + jj) * 8 + r], acc[r]);
-        }
-#pragma unroll
-        for (int r = 0; r < 8; ++r) red[warp][lane][r] = acc[r];
-        __syncthreads();
-        {
-          const int row = threadIdx.x >> 3, r = threadIdx.x & 7;
-          const int ii = b + g * 32 + row;
-          if (ii < m && r < nrhs) {
-            double v = 0.0;
-#pragma unroll
-            for (int w = 0; w < 8; ++w) v += red[w][row][r];
-            if (ii < be) x[d.first + pl[ii] + static_cast<std::int64_t>(r) * n] = v;
-            else t[r * m + ii] = __ldcg(&t[r * m + ii]) - v;
+          for (int w = 0; w < 8; ++w) val += red[w][row][rr];
+          if (ii < be) {
+            x[d.first + pl[ii] + static_cast<std::int64_t>(rr) * n] = val;
+          } else {
+            const double nv = told - val;
+            if (last && ii >= k) v[(ii - k) + static_cast<std::int64_t>(rr) * c] = nv;
+            else t[rr * m + ii] = nv;
           }
         }
-        __syncthreads();
       }
+      if (G >= nb0 && G < nb1) publish(cnt);  // rows of the next super-block are final
+      else __syncthreads();
     }
-    grid.sync();
   }
-  double* v = vec + d.vec_off * nrhs;
-  for (int a = gt; a < c; a += gs)
-    for (int r = 0; r < nrhs; ++r) v[a + static_cast<std::int64_t>(r) * c] = __ldcg(&t[r * m + k + a]);
 }
 
-// Backward sweep of the level's large fronts. Columns are owned by groups of 8 lanes (4 per warp);
-// a group reduces its column's dot products over the lanes with shuffles.
-__global__ void __launch_bounds__(256) k_solve_bwd_coop(const std::int32_t* list, const std::int32_t* cta_start,
-                                                         int nfronts, int max_steps, const SnDev* sn,
-                                                         const std::int32_t* rows, const double* W,
-                                                         const std::int32_t* pidx, double* x, std::int64_t n,
-                                                         int nrhs, double* work, const std::int64_t* work_off) {
+// Backward sweep of the level's large fronts. Columns are owned by groups of 8 lanes (4 per warp,
+// 32 consecutive columns per CTA and round); a group reduces its column's dot products over its
+// lanes with shuffles. Super-blocks are processed from the last to the first; the owners of the
+// next super-block's columns write x there and publish.
+__global__ void __launch_bounds__(256, 2) k_solve_bwd_coop(const std::int32_t* list, const std::int32_t* cta_start,
+                                                            int nfronts, const SnDev* sn, const std::int32_t* rows,
+                                                            const double* W, const std::int32_t* pidx, double* x,
+                                                            std::int64_t n, int nrhs, double* work,
+                                                            const std::int64_t* work_off, int* cnts, int* err) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
   __shared__ double xb[kSB * 8];
@@ -523,19 +586,24 @@ __global__ void __launch_bounds__(256) k_solve_bwd_coop(const std::int32_t* list
   const int m = d.m, k = d.k;
   double* t = work + work_off[f];                              // t[r * m + i]
   double* sv = t + static_cast<std::int64_t>(8) * m;           // sv[r * k + j]
+  int* cnt = cnts + f;
   const double* Wf = W + d.w_off;
   const std::int32_t* pl = pidx + d.first;
   const std::int32_t* rw = rows + d.rows_off;
   const int gt = rank * blockDim.x + threadIdx.x, gs = nr * blockDim.x;
   const int sub = threadIdx.x & 7, gsub = (threadIdx.x >> 3) & 3;
-  const int wbase = rank * (blockDim.x >> 3) + (threadIdx.x >> 5) * 4, ngrp = nr * (blockDim.x >> 3);
+  const int wbase = rank * 32 + (threadIdx.x >> 5) * 4, ngrp = nr * 32;
+  const int nsb = (k + kSB - 1) / kSB;
   for (int i = gt; i < m; i += gs)
     for (int r = 0; r < nrhs; ++r)
       t[r * m + i] = i < k ? x[d.first + pl[i] + static_cast<std::int64_t>(r) * n] : x[rw[i] + static_cast<std::int64_t>(r) * n];
   grid.sync();
-  // sv_j = (W[A, A]^T t_A)_j - W[k:m, j]^T t[k:m]; the loop bounds are uniform over each warp
-  for (int base = wbase; base < k; base += ngrp) {
-    const int j = base + gsub;
+  // sv_j = (W[A, A]^T t_A)_j - W[k:m, j]^T t[k:m]; the last super-block's x is final already
+  const int blast = (nsb - 1) * kSB;
+  // chunk loop: c0 = first column of this CTA's 32-column chunk (uniform over the CTA, so the
+  // barrier in publish() is reached by every warp)
+  for (int c0 = rank * 32; c0 < k; c0 += ngrp) {
+    const int j = c0 + (threadIdx.x >> 3);
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (j < k) {
       const double* Wj = Wf + static_cast<std::int64_t>(j) * m;
@@ -559,56 +627,69 @@ __global__ void __launch_bounds__(256) k_solve_bwd_coop(const std::int32_t* list
       acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 2);
       acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 1);
     }
-    if (j < k && sub == 0) {
+    if (j < k && sub < nrhs) {
+      double a = acc[0];
 #pragma unroll
-      for (int r = 0; r < 8; ++r)
-        if (r < nrhs) sv[r * k + j] = acc[r];
+      for (int r = 1; r < 8; ++r)
+        if (sub == r) a = acc[r];
+      sv[sub * k + j] = a;
+      if (j >= blast) x[d.first + pl[j] + static_cast<std::int64_t>(sub) * n] = a;
     }
+    if (c0 >= blast) publish(cnt);  // this CTA's 32 columns of the last super-block are final
   }
-  grid.sync();
-  const int nsb = (k + kSB - 1) / kSB;
-  for (int step = 0; step < max_steps; ++step) {
+  int target = 0;
+  for (int step = 0; step < nsb; ++step) {
     const int q = nsb - 1 - step;
-    if (q >= 0) {
-      const int b = q * kSB, be = min(b + kSB, k), bs = be - b;
-      for (int idx = threadIdx.x; idx < kSB * 8; idx += blockDim.x) {
-        const int i = idx >> 3, r = idx & 7;
-        xb[idx] = (i < bs && r < nrhs) ? __ldcg(&sv[r * k + b + i]) : 0.0;
-      }
-      __syncthreads();
-      if (rank == 0)
-        for (int idx = threadIdx.x; idx < bs * 8; idx += blockDim.x) {
-          const int i = idx >> 3, r = idx & 7;
-          if (r < nrhs) x[d.first + pl[b + i] + static_cast<std::int64_t>(r) * n] = xb[idx];
-        }
-      // earlier pivots j < b: sv_j -= W[B, j]^T x_B
-      for (int base = wbase; base < b; base += ngrp) {
-        const int j = base + gsub;
-        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        if (j < b) {
-          const double* Wj = Wf + b + static_cast<std::int64_t>(j) * m;
-          double wv[16];
+    const int b = q * kSB, be = min(b + kSB, k), bs = be - b;
+    target += sb_groups(q, k);
+    if (wbase >= b) break;  // no columns left for this CTA (uniform: b is a multiple of 32)
+    const int bprev = b - kSB;  // columns of the next super-block: [bprev, b)
+    // prefetch the first column's W entries and old value
+    int j = wbase + gsub;
+    double wv[16];
+    {
+      const double* Wj = Wf + b + static_cast<std::int64_t>(j) * m;
 #pragma unroll
-          for (int u = 0; u < 16; ++u) wv[u] = sub + 8 * u < bs ? Wj[sub + 8 * u] : 0.0;
-#pragma unroll
-          for (int u = 0; u < 16; ++u)
-#pragma unroll
-            for (int r = 0; r < 8; ++r) acc[r] = fma(wv[u], xb[(sub + 8 * u) * 8 + r], acc[r]);
-        }
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 4);
-          acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 2);
-          acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 1);
-        }
-        if (j < b && sub == 0) {
-#pragma unroll
-          for (int r = 0; r < 8; ++r)
-            if (r < nrhs) sv[r * k + j] = __ldcg(&sv[r * k + j]) - acc[r];
-        }
-      }
+      for (int u = 0; u < 16; ++u) wv[u] = (j < b && sub + 8 * u < bs) ? Wj[sub + 8 * u] : 0.0;
     }
-    grid.sync();
+    double sold = (j < b && sub < nrhs) ? __ldcg(&sv[sub * k + j]) : 0.0;
+    wait_published(cnt, target, err);
+    for (int idx = threadIdx.x; idx < kSB * 8; idx += blockDim.x) {
+      const int i = idx >> 3, r = idx & 7;
+      xb[idx] = (i < bs && r < nrhs) ? __ldcg(&sv[r * k + b + i]) : 0.0;
+    }
+    __syncthreads();
+    for (int base = wbase; base < b; base += ngrp) {
+      j = base + gsub;
+      if (base != wbase) {
+        const double* Wj = Wf + b + static_cast<std::int64_t>(j) * m;
+#pragma unroll
+        for (int u = 0; u < 16; ++u) wv[u] = (j < b && sub + 8 * u < bs) ? Wj[sub + 8 * u] : 0.0;
+        sold = (j < b && sub < nrhs) ? __ldcg(&sv[sub * k + j]) : 0.0;
+      }
+      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int u = 0; u < 16; ++u)
+#pragma unroll
+        for (int r = 0; r < 8; ++r) acc[r] = fma(wv[u], xb[(sub + 8 * u) * 8 + r], acc[r]);
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 4);
+        acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 2);
+        acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 1);
+      }
+      if (j < b && sub < nrhs) {
+        double a = acc[0];
+#pragma unroll
+        for (int r = 1; r < 8; ++r)
+          if (sub == r) a = acc[r];
+        const double nv = sold - a;
+        sv[sub * k + j] = nv;
+        if (j >= bprev) x[d.first + pl[j] + static_cast<std::int64_t>(sub) * n] = nv;
+      }
+      if (base >= bprev) publish(cnt);  // this CTA's 32 columns of the next super-block are final
+      else __syncthreads();
+    }
   }
 }
 
@@ -712,21 +793,20 @@ void launch_sb_build(const int2* sbl, int nsb, const int4* tiles, int ntiles, co
 }
 
 cudaError_t launch_solve_fwd_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
-                                  int max_steps, const SnDev* sn, const std::int32_t* child_ptr,
-                                  const std::int32_t* children, const std::int32_t* rmap, const double* W,
+                                  const SnDev* sn, const std::int32_t* cptr, const ContribEntry* cent, const double* W,
                                   const std::int32_t* pidx, double* x, std::int64_t n, double* vec, int nrhs,
-                                  double* work, const std::int64_t* work_off, cudaStream_t s) {
-  void* args[] = {&list, &cta_start, &nfronts, &max_steps, &sn, &child_ptr, &children, &rmap, &W, &pidx,
-                  &x, &n, &vec, &nrhs, &work, &work_off};
+                                  double* work, const std::int64_t* work_off, int* cnts, int* err, cudaStream_t s) {
+  void* args[] = {&list, &cta_start, &nfronts, &sn, &cptr, &cent, &W, &pidx, &x, &n, &vec, &nrhs, &work, &work_off,
+                  &cnts, &err};
   note_launches(1);
   return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_solve_fwd_coop), dim3(nctas), dim3(256), args, 0, s);
 }
 
 cudaError_t launch_solve_bwd_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
-                                  int max_steps, const SnDev* sn, const std::int32_t* rows, const double* W,
-                                  const std::int32_t* pidx, double* x, std::int64_t n, int nrhs, double* work,
-                                  const std::int64_t* work_off, cudaStream_t s) {
-  void* args[] = {&list, &cta_start, &nfronts, &max_steps, &sn, &rows, &W, &pidx, &x, &n, &nrhs, &work, &work_off};
+                                  const SnDev* sn, const std::int32_t* rows, const double* W, const std::int32_t* pidx,
+                                  double* x, std::int64_t n, int nrhs, double* work, const std::int64_t* work_off,
+                                  int* cnts, int* err, cudaStream_t s) {
+  void* args[] = {&list, &cta_start, &nfronts, &sn, &rows, &W, &pidx, &x, &n, &nrhs, &work, &work_off, &cnts, &err};
   note_launches(1);
   return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_solve_bwd_coop), dim3(nctas), dim3(256), args, 0, s);
 }

@@ -42,14 +42,15 @@ constexpr int kSB = 128;
 void launch_sb_build(const int2* sbl, int nsb, const int4* tiles, int ntiles, const SnDev* sn, const double* panels,
                      const signed char* piv, double* W, cudaStream_t s);
 int solve_coop_max_ctas(int device);
+// cnts: one publication counter per front of the launch, zero at launch; err: set to 1 when a
+// wait between the CTAs of a front ran out (the solve is then not valid)
 cudaError_t launch_solve_fwd_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
-                                  int max_steps, const SnDev* sn, const std::int32_t* child_ptr,
-                                  const std::int32_t* children, const std::int32_t* rmap, const double* W,
+                                  const SnDev* sn, const std::int32_t* cptr, const ContribEntry* cent, const double* W,
                                   const std::int32_t* pidx, double* x, std::int64_t n, double* vec, int nrhs,
-                                  double* work, const std::int64_t* work_off, cudaStream_t s);
+                                  double* work, const std::int64_t* work_off, int* cnts, int* err, cudaStream_t s);
 cudaError_t launch_solve_bwd_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
-                                  int max_steps, const SnDev* sn, const std::int32_t* rows, const double* W,
-                                  const std::int32_t* pidx, double* x, std::int64_t n, int nrhs, double* work,
-                                  const std::int64_t* work_off, cudaStream_t s);
+                                  const SnDev* sn, const std::int32_t* rows, const double* W, const std::int32_t* pidx,
+                                  double* x, std::int64_t n, int nrhs, double* work, const std::int64_t* work_off,
+                                  int* cnts, int* err, cudaStream_t s);
 
 }  // namespace hsg
