@@ -518,9 +518,11 @@ __global__ void __launch_bounds__(256, 2) k_solve_fwd_coop(const std::int32_t* l
         wv[jj] = (i < m && j0 + jj < bs) ? Wf[i + static_cast<std::int64_t>(b + j0 + jj) * m] : 0.0;
     }
     double told = 0.0;
+    int plz = 0;
     {
       const int ii = G * 32 + row;
       if (ii >= be && ii < m && rr < nrhs) told = __ldcg(&t[rr * m + ii]);
+      if (ii < be) plz = pl[ii];
     }
     wait_published(cnt, target, err);
     for (int idx = threadIdx.x; idx < kSB * 8; idx += blockDim.x) {
@@ -536,6 +538,7 @@ __global__ void __launch_bounds__(256, 2) k_solve_fwd_coop(const std::int32_t* l
           wv[jj] = (i < m && j0 + jj < bs) ? Wf[i + static_cast<std::int64_t>(b + j0 + jj) * m] : 0.0;
         const int ii = G * 32 + row;
         told = (ii >= be && ii < m && rr < nrhs) ? __ldcg(&t[rr * m + ii]) : 0.0;
+        plz = ii < be ? pl[ii] : 0;
       }
       double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
@@ -552,7 +555,7 @@ __global__ void __launch_bounds__(256, 2) k_solve_fwd_coop(const std::int32_t* l
 #pragma unroll
           for (int w = 0; w < 8; ++w) val += red[w][row][rr];
           if (ii < be) {
-            x[d.first + pl[ii] + static_cast<std::int64_t>(rr) * n] = val;
+            x[d.first + plz + static_cast<std::int64_t>(rr) * n] = val;
           } else {
             const double nv = told - val;
             if (last && ii >= k) v[(ii - k) + static_cast<std::int64_t>(rr) * c] = nv;
@@ -653,9 +656,10 @@ __global__ void __launch_bounds__(256, 2) k_solve_bwd_coop(const std::int32_t* l
       for (int u = 0; u < 16; ++u) wv[u] = (j < b && sub + 8 * u < bs) ? Wj[sub + 8 * u] : 0.0;
     }
     double sold = (j < b && sub < nrhs) ? __ldcg(&sv[sub * k + j]) : 0.0;
+    int plj = (j < b && j >= bprev) ? pl[j] : 0;
     wait_published(cnt, target, err);
     for (int idx = threadIdx.x; idx < kSB * 8; idx += blockDim.x) {
-      const int i = idx >> 3, r = idx & 7;
+      const int r = idx / kSB, i = idx % kSB;  // xb[r * kSB + i]: conflict-free reads below
       xb[idx] = (i < bs && r < nrhs) ? __ldcg(&sv[r * k + b + i]) : 0.0;
     }
     __syncthreads();
@@ -666,12 +670,13 @@ __global__ void __launch_bounds__(256, 2) k_solve_bwd_coop(const std::int32_t* l
 #pragma unroll
         for (int u = 0; u < 16; ++u) wv[u] = (j < b && sub + 8 * u < bs) ? Wj[sub + 8 * u] : 0.0;
         sold = (j < b && sub < nrhs) ? __ldcg(&sv[sub * k + j]) : 0.0;
+        plj = (j < b && j >= bprev) ? pl[j] : 0;
       }
       double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
       for (int u = 0; u < 16; ++u)
 #pragma unroll
-        for (int r = 0; r < 8; ++r) acc[r] = fma(wv[u], xb[(sub + 8 * u) * 8 + r], acc[r]);
+        for (int r = 0; r < 8; ++r) acc[r] = fma(wv[u], xb[r * kSB + sub + 8 * u], acc[r]);
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
         acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 4);
@@ -685,7 +690,7 @@ __global__ void __launch_bounds__(256, 2) k_solve_bwd_coop(const std::int32_t* l
           if (sub == r) a = acc[r];
         const double nv = sold - a;
         sv[sub * k + j] = nv;
-        if (j >= bprev) x[d.first + pl[j] + static_cast<std::int64_t>(sub) * n] = nv;
+        if (j >= bprev) x[d.first + plj + static_cast<std::int64_t>(sub) * n] = nv;
       }
       if (base >= bprev) publish(cnt);  // this CTA's 32 columns of the next super-block are final
       else __syncthreads();
