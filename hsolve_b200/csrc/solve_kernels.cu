@@ -601,28 +601,32 @@ __global__ void __launch_bounds__(256, 2) k_solve_bwd_coop(const std::int32_t* l
     for (int r = 0; r < nrhs; ++r)
       t[r * m + i] = i < k ? x[d.first + pl[i] + static_cast<std::int64_t>(r) * n] : x[rw[i] + static_cast<std::int64_t>(r) * n];
   grid.sync();
-  // sv_j = (W[A, A]^T t_A)_j - W[k:m, j]^T t[k:m]; the last super-block's x is final already
+  // sv_j = (W[A, A]^T t_A)_j - W[k:m, j]^T t[k:m] for j in super-block A, 128-row chunks of t
+  // staged in shared memory (W is zero above the diagonal of W[A, A]); the last super-block's x
+  // is final already. Rounds c0 are 32-column chunks, uniform over the CTA.
   const int blast = (nsb - 1) * kSB;
-  // chunk loop: c0 = first column of this CTA's 32-column chunk (uniform over the CTA, so the
-  // barrier in publish() is reached by every warp)
   for (int c0 = rank * 32; c0 < k; c0 += ngrp) {
     const int j = c0 + (threadIdx.x >> 3);
+    const int bA = (c0 / kSB) * kSB;
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (j < k) {
-      const double* Wj = Wf + static_cast<std::int64_t>(j) * m;
-      const int beA = min((j / kSB + 1) * kSB, k);
-      for (int i = j + sub; i < beA; i += 8) {
-        const double w = Wj[i];
+    for (int i0 = bA, chunk = 0; i0 < m; ++chunk) {
+      const int i1 = chunk == 0 ? min(bA + kSB, k) : min(i0 + kSB, m);
+      const double sg = chunk == 0 ? 1.0 : -1.0;
+      double wv[16];
+      const double* Wj = Wf + i0 + static_cast<std::int64_t>(j) * m;
 #pragma unroll
-        for (int r = 0; r < 8; ++r)
-          if (r < nrhs) acc[r] = fma(w, __ldcg(&t[r * m + i]), acc[r]);
+      for (int u = 0; u < 16; ++u) wv[u] = (j < k && i0 + sub + 8 * u < i1) ? sg * Wj[sub + 8 * u] : 0.0;
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < kSB * 8; idx += blockDim.x) {
+        const int r = idx / kSB, i = idx % kSB;
+        xb[idx] = (i0 + i < i1 && r < nrhs) ? __ldcg(&t[r * m + i0 + i]) : 0.0;
       }
-      for (int i = k + sub; i < m; i += 8) {
-        const double w = Wj[i];
+      __syncthreads();
 #pragma unroll
-        for (int r = 0; r < 8; ++r)
-          if (r < nrhs) acc[r] = fma(-w, __ldcg(&t[r * m + i]), acc[r]);
-      }
+      for (int u = 0; u < 16; ++u)
+#pragma unroll
+        for (int r = 0; r < 8; ++r) acc[r] = fma(wv[u], xb[r * kSB + sub + 8 * u], acc[r]);
+      i0 = chunk == 0 ? k : i1;
     }
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
@@ -639,6 +643,7 @@ __global__ void __launch_bounds__(256, 2) k_solve_bwd_coop(const std::int32_t* l
       if (j >= blast) x[d.first + pl[j] + static_cast<std::int64_t>(sub) * n] = a;
     }
     if (c0 >= blast) publish(cnt);  // this CTA's 32 columns of the last super-block are final
+    else __syncthreads();
   }
   int target = 0;
   for (int step = 0; step < nsb; ++step) {
