@@ -163,6 +163,18 @@ void GpuFactor::build_plan() {
     inv_total += static_cast<std::int64_t>((d.k + 30) / 31 + 1) * 1024;
   }
   vec_total_ = vec;
+  {
+    // per pivot: panel index of its diagonal entry and its front's first column
+    std::vector<std::int64_t> dpos(n_);
+    std::vector<std::int32_t> pfirst(n_);
+    for (std::int32_t q = 0; q < ns; ++q)
+      for (int j = 0; j < sn[q].k; ++j) {
+        dpos[sn[q].first + j] = sn[q].panel_off + j + static_cast<std::int64_t>(j) * sn[q].m;
+        pfirst[sn[q].first + j] = sn[q].first;
+      }
+    d_dpos_.upload(dpos, stream_);
+    d_pfirst_.upload(pfirst, stream_);
+  }
   if (coop_max_ == 0) coop_max_ = coop_max_ctas(opt_.device);
   if (solve_coop_max_ == 0) solve_coop_max_ = solve_coop_max_ctas(opt_.device);
   std::vector<std::int64_t> work_offs;
@@ -209,7 +221,7 @@ void GpuFactor::build_plan() {
     put(app, L.app_off, L.app_n);
     put(all, L.all_off, L.all_n);
     // solves: cooperative sweeps when the level's fronts fit the co-resident grid
-    if (!all.empty() && static_cast<int>(all.size()) <= solve_coop_max_ / 2) {
+    if (!all.empty() && static_cast<int>(all.size()) <= solve_coop_max_) {
       std::vector<double> wts(all.size());
       double wsum = 0.0;
       int steps = 0;
@@ -502,7 +514,7 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
                          d_panels_.p, d_piv_.p, d_pidx_.p, d_blk_.p, d_nblk_.p, d_inv_.p, xw, n_, d_vec_.p, nc, s);
       }
     }
-    launch_solve_diag(sym_.ns, d_sn_.p, d_panels_.p, d_piv_.p, d_pidx_.p, xw, n_, nc, s);
+    launch_solve_diag_flat(n_, d_dpos_.p, d_pfirst_.p, d_panels_.p, d_piv_.p, d_pidx_.p, xw, n_, nc, s);
     for (auto it = levels_.rbegin(); it != levels_.rend(); ++it) {
       if (it->solve_coop) {
         cuda_check(launch_solve_bwd_coop(lists + it->all_off, lists + it->solve_cta_off, it->all_n, it->solve_ctas,
@@ -576,7 +588,7 @@ void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ld
                          d_panels_.p, d_piv_.p, d_pidx_.p, d_blk_.p, d_nblk_.p, d_inv_.p, xw, n_, vec, nc, s);
       }
     }
-    launch_solve_diag(sym_.ns, d_sn_.p, d_panels_.p, d_piv_.p, d_pidx_.p, xw, n_, nc, s);
+    launch_solve_diag_flat(n_, d_dpos_.p, d_pfirst_.p, d_panels_.p, d_piv_.p, d_pidx_.p, xw, n_, nc, s);
     for (auto it = levels_.rbegin(); it != levels_.rend(); ++it) {
       if (it->solve_coop) {
         cuda_check(launch_solve_bwd_coop(lists + it->all_off, lists + it->solve_cta_off, it->all_n, it->solve_ctas,

@@ -143,6 +143,8 @@ class GpuFactor {
   // super-block solve operators of the large fronts (built at the first solve after a factorization)
   DevBuf<double> d_w_;
   DevBuf<int> d_err_;  // set by a solve sweep whose bounded wait ran out
+  DevBuf<std::int64_t> d_dpos_;    // per pivot: panel index of its diagonal entry
+  DevBuf<std::int32_t> d_pfirst_;  // per pivot: first column of its front
   DevBuf<std::int32_t> d_cptr_;   // large fronts: children's contributions per position
   DevBuf<ContribEntry> d_cent_;
   DevBuf<int> d_sweep_cnt_;       // publication counters: forward slots, then backward slots

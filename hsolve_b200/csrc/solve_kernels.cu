@@ -209,6 +209,33 @@ __global__ void k_solve_diag(const SnDev* sn, const double* panels, const signed
   }
 }
 
+// Diagonal solve D y = z over all pivots at once (one thread per pivot position p): dpos[p] is the
+// panel index of D(p, p), pfirst[p] the first global column of p's front.
+__global__ void k_solve_diag_flat(std::int64_t npiv, const std::int64_t* dpos, const std::int32_t* pfirst,
+                                  const double* panels, const signed char* piv, const std::int32_t* pidx, double* x,
+                                  std::int64_t n, int nrhs) {
+  const std::int64_t p = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= npiv) return;
+  const signed char ty = piv[p];
+  if (ty == 3) return;
+  const std::int64_t g0 = pfirst[p] + pidx[p];
+  if (ty <= 0) {
+    for (int r = 0; r < nrhs; ++r) x[g0 + r * n] = 0.0;
+  } else if (ty == 1) {
+    const double dj = panels[dpos[p]];
+    for (int r = 0; r < nrhs; ++r) x[g0 + r * n] /= dj;
+  } else {
+    const std::int64_t g1 = pfirst[p] + pidx[p + 1];
+    const double a = panels[dpos[p]], b = panels[dpos[p] + 1], c = panels[dpos[p + 1]];
+    const double det = a * c - b * b;
+    for (int r = 0; r < nrhs; ++r) {
+      const double y0 = x[g0 + r * n], y1 = x[g1 + r * n];
+      x[g0 + r * n] = (c * y0 - b * y1) / det;
+      x[g1 + r * n] = (-b * y0 + a * y1) / det;
+    }
+  }
+}
+
 // Backward sweep of the listed fronts (ancestors done): right-looking over the blocks, last first.
 __global__ void __launch_bounds__(256) k_solve_bwd(const std::int32_t* list, const SnDev* sn, const std::int32_t* rows,
                                                     const double* panels, const std::int32_t* pidx,
@@ -752,6 +779,15 @@ void launch_solve_fwd(const std::int32_t* list, int nlist, int maxm, const SnDev
   note_launches(1);
   k_solve_fwd<<<nlist, 256, smem, s>>>(list, sn, child_ptr, children, rmap, panels, piv, pidx, blk, nblk, inv, x, n,
                                        vec, nrhs, R);
+}
+
+void launch_solve_diag_flat(std::int64_t npiv, const std::int64_t* dpos, const std::int32_t* pfirst,
+                            const double* panels, const signed char* piv, const std::int32_t* pidx, double* x,
+                            std::int64_t n, int nrhs, cudaStream_t s) {
+  if (npiv <= 0) return;
+  note_launches(1);
+  k_solve_diag_flat<<<static_cast<unsigned>((npiv + 255) / 256), 256, 0, s>>>(npiv, dpos, pfirst, panels, piv, pidx, x, n,
+                                                                             nrhs);
 }
 
 void launch_solve_diag(int ns, const SnDev* sn, const double* panels, const signed char* piv,

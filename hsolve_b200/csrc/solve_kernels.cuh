@@ -27,6 +27,10 @@ void launch_solve_fwd(const std::int32_t* list, int nlist, int maxm, const SnDev
                       const signed char* piv, const std::int32_t* pidx, const std::int32_t* blk,
                       const std::int32_t* nblk, const double* inv, double* x, std::int64_t n, double* vec, int nrhs,
                       cudaStream_t s);
+// D y = z for all pivots, one thread each (dpos: panel index of each D(p, p); pfirst: front's first column)
+void launch_solve_diag_flat(std::int64_t npiv, const std::int64_t* dpos, const std::int32_t* pfirst,
+                            const double* panels, const signed char* piv, const std::int32_t* pidx, double* x,
+                            std::int64_t n, int nrhs, cudaStream_t s);
 void launch_solve_diag(int ns, const SnDev* sn, const double* panels, const signed char* piv,
                        const std::int32_t* pidx, double* x, std::int64_t n, int nrhs, cudaStream_t s);
 void launch_solve_bwd(const std::int32_t* list, int nlist, int maxm, const SnDev* sn, const std::int32_t* rows,
