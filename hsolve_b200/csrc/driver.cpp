@@ -192,7 +192,10 @@ struct SliceRec {
   bool passed;
 };
 
-struct Timers { double setup = 0, factor = 0, iterate = 0, verify = 0, cert = 0; };
+struct Timers {
+  double setup = 0, factor = 0, iterate = 0, verify = 0, cert = 0;
+  double kry_apply = 0, kry_ortho = 0, kry_rr = 0, kry_restart = 0;  // phases of `iterate`
+};
 
 // Inertia count nu_-(A - s B) with endpoint moves on singular shifts (steps.cpp:549-571 behaviour):
 // returns the count and the (possibly moved) shift.
@@ -241,6 +244,10 @@ NearestRun run_krylov(ShiftInvertOp& op, Problem& P, double sigma, int nev, cons
   o.which = Which::LargestMagnitude;
   KsResult r = krylov_schur(op, P.n, o, P.s);
   tm.iterate += since(t0);
+  tm.kry_apply += r.t_apply;
+  tm.kry_ortho += r.t_ortho;
+  tm.kry_rr += r.t_rr;
+  tm.kry_restart += r.t_restart;
   NearestRun out;
   out.restarts = r.restarts;
   out.applies = r.applies;
@@ -589,6 +596,13 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
   j.kv("time_iterate_s", tm.iterate);
   j.kv("time_verify_s", tm.verify);
   j.kv("time_certificate_s", tm.cert);
+  j.key("iterate_split_s");
+  j.open('{');
+  j.kv("operator", tm.kry_apply);
+  j.kv("orthonormalize", tm.kry_ortho);
+  j.kv("rayleigh_ritz", tm.kry_rr);
+  j.kv("restart", tm.kry_restart);
+  j.close('}');
   j.key("factor_stats");
   j.open('{');
   j.kv("factor_entries", static_cast<long long>(est.factor_entries));

@@ -2,6 +2,7 @@
 #include "eigen.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <numeric>
 #include <random>
@@ -12,6 +13,10 @@
 namespace hsg {
 
 namespace {
+
+double seconds_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
 
 struct Basis {
   std::int64_t n;
@@ -146,11 +151,15 @@ KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, 
   while (true) {
     while (m + p <= mmax) {
       const int j0 = m;
+      auto tp = std::chrono::steady_clock::now();
       op.apply(B.v(j0), n, B.v(j0 + p), n, p);
+      res.t_apply += seconds_since(tp);
       res.applies += p;
       res.block_steps += 1;
       std::vector<double> H;
+      tp = std::chrono::steady_clock::now();
       std::vector<double> R = ortho_block(B, op, j0 + p, p, H, rng, s);
+      res.t_ortho += seconds_since(tp);
       const int jh = j0 + p;  // H is jh x p
       for (int c = 0; c < p; ++c)
         for (int i = 0; i < jh; ++i) {
@@ -171,6 +180,7 @@ KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, 
       m += p;
     }
     // Rayleigh-Ritz on T[0:m, 0:m]
+    const auto trr = std::chrono::steady_clock::now();
     S.assign(static_cast<std::size_t>(m) * m, 0.0);
     for (int j = 0; j < m; ++j)
       for (int i = 0; i < m; ++i) S[i + static_cast<std::size_t>(j) * m] = Tm(i, j);
@@ -201,6 +211,7 @@ KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, 
       const int i = order[q];
       if (rn[i] <= opt.tol * std::fabs(w[i])) ++nconv;
     }
+    res.t_rr += seconds_since(trr);
     const bool done = nconv >= std::min(nev, m) || res.restarts >= opt.max_restarts;
     if (done) {
       const int take = std::min(nev, m);
@@ -231,6 +242,7 @@ KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, 
       return res;
     }
     // thick restart
+    const auto trs = std::chrono::steady_clock::now();
     const int keep = std::min(mmax - p, std::max(nev + p, (nev + mmax) / 2));
     std::vector<double> Q(static_cast<std::size_t>(m) * keep);
     std::vector<double> th(keep);
@@ -265,6 +277,8 @@ KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, 
     T.swap(Tn);
     m = keep;
     res.restarts += 1;
+    cuda_check(cudaStreamSynchronize(s), "restart");
+    res.t_restart += seconds_since(trs);
   }
 }
 

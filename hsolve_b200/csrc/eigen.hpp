@@ -51,6 +51,9 @@ struct KsResult {
   std::vector<double> other_theta;  // the remaining Ritz values of the last basis (gap placement)
   std::vector<double> other_resid;
   DevBuf<double> X;            // n x nev Ritz vectors (B-orthonormal), if requested
+  // host wall time (s) of the phases: operator applications, block orthonormalization,
+  // Rayleigh-Ritz on the projected matrix, thick restarts
+  double t_apply = 0.0, t_ortho = 0.0, t_rr = 0.0, t_restart = 0.0;
 };
 
 KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, cudaStream_t stream);

@@ -17,33 +17,45 @@ namespace hsg {
 
 void cuda_check(cudaError_t e, const char* what);
 
+// Device memory through a per-device caching pool: blocks are rounded up to size classes of 1/8
+// octave, returned to the pool on release and reused by later allocations of the same class, so
+// the solves of a session do not call cudaMalloc / cudaFree (which synchronise the device) after
+// their first call. A failed cudaMalloc releases the cached blocks of the device and retries.
+void* pool_alloc(std::size_t bytes, std::size_t* cap, int* device);
+void pool_free(void* p, std::size_t cap, int device);
+// Releases every cached block of every device (the library's memory in use is not touched).
+void pool_trim();
+
 template <class T>
 struct DevBuf {
   T* p = nullptr;
   std::size_t n = 0;
+  std::size_t cap = 0;  // bytes of the pooled block
+  int dev = -1;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), cap(o.cap), dev(o.dev) { o.p = nullptr; o.n = 0; o.cap = 0; }
   DevBuf& operator=(DevBuf&& o) noexcept {
-    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    if (this != &o) {
+      release();
+      p = o.p; n = o.n; cap = o.cap; dev = o.dev;
+      o.p = nullptr; o.n = 0; o.cap = 0;
+    }
     return *this;
   }
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) pool_free(p, cap, dev);
     p = nullptr;
     n = 0;
+    cap = 0;
   }
   void alloc(std::size_t count) {
     if (count <= n && p) return;
     release();
     if (count == 0) return;
-    const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
-    if (e != cudaSuccess) {
-      p = nullptr;
-      HSG_THROW(HSG_OUT_OF_MEMORY_BUDGET, "cudaMalloc of " << count * sizeof(T) << " bytes failed: " << cudaGetErrorString(e));
-    }
+    p = static_cast<T*>(pool_alloc(count * sizeof(T), &cap, &dev));
     n = count;
   }
   void upload(const std::vector<T>& h, cudaStream_t s) {
