@@ -422,7 +422,6 @@ void GpuFactor::run_numeric(double alpha, double beta, bool detection) {
       launch_front_app(lists + L.app_off, L.app_n, d_sn_.p, d_panels_.p, d_cb_.p, d_scratch_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
     }
   }
-  launch_inv_blocks(sym_.ns, d_sn_.p, d_panels_.p, d_piv_.p, d_blk_.p, d_nblk_.p, d_inv_.p, s);
   cuda_check(cudaGetLastError(), "factorization launch");
 }
 
@@ -612,6 +611,7 @@ void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ld
 
 void GpuFactor::build_solve_operator() {
   if (w_ready_) return;
+  launch_inv_blocks(sym_.ns, d_sn_.p, d_panels_.p, d_piv_.p, d_blk_.p, d_nblk_.p, d_inv_.p, stream_);
   launch_sb_build(d_sbl_.p, nsbl_, d_tiles_.p, ntiles_, d_sn_.p, d_panels_.p, d_piv_.p, d_w_.p, stream_);
   w_ready_ = true;
 }

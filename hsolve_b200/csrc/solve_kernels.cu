@@ -58,6 +58,7 @@ __global__ void __launch_bounds__(256) k_inv_blocks(const SnDev* sn, const doubl
   __shared__ int nb;
   const int s = blockIdx.x;
   const SnDev d = sn[s];
+  if (d.w_off >= 0) return;  // large fronts are solved through their super-block operator
   const int k = d.k, m = d.m;
   const signed char* pv = piv + d.first;
   if (threadIdx.x == 0) {

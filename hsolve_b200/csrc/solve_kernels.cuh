@@ -19,7 +19,8 @@ void launch_scatter_scale(std::int64_t n, int nrhs, double* b, std::int64_t ldb,
                           const std::int32_t* iperm, const double* x, cudaStream_t s);
 constexpr int kMaxBlocksPerFront = 2048;  // <= 32-column solve blocks per front (fronts up to ~63k pivots)
 
-// block partition + inverse diagonal blocks of every front (after each factorization)
+// block partition + inverse diagonal blocks of the fronts solved one CTA per front (before the
+// first solve of each factorization)
 void launch_inv_blocks(int ns, const SnDev* sn, const double* panels, const signed char* piv, std::int32_t* blk,
                        std::int32_t* nblk, double* inv, cudaStream_t s);
 void launch_solve_fwd(const std::int32_t* list, int nlist, int maxm, const SnDev* sn, const std::int32_t* child_ptr,
