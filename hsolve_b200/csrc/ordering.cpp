@@ -6,7 +6,12 @@
 #include "ordering.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
+#include <cstdlib>
+#include <mutex>
+#include <thread>
 #include <cstring>
 #include <queue>
 #include <utility>
@@ -500,25 +505,53 @@ Adjacency adjacency_from_upper(std::int64_t n, const std::int64_t* rowptr, const
   return g;
 }
 
-std::vector<std::int32_t> nested_dissection(const Adjacency& g, const OrderingOptions& opt, OrderingStats* stats) {
-  const auto t0 = std::chrono::steady_clock::now();
-  const std::int64_t n = g.n;
-  std::vector<std::int32_t> order(n, -1);
-  std::vector<int> loc(n, -1);
-  Rng rng(opt.seed);
-  struct Task { std::vector<int> verts; std::int64_t lo; };
-  std::vector<Task> stack;
-  {
-    Task t;
-    t.verts.resize(n);
-    for (std::int64_t i = 0; i < n; ++i) t.verts[i] = static_cast<int>(i);
-    t.lo = 0;
-    stack.push_back(std::move(t));
-  }
-  std::int64_t nsep = 0, nleaf = 0, topsep = -1;
-  std::vector<std::int32_t> leaf_out;
+namespace {
+
+struct NdTask {
+  std::vector<int> verts;
+  std::int64_t lo = 0;
+};
+
+// Per-task random stream: a function of the seed, the task's first position and its size, so the
+// order does not depend on how the tasks are scheduled over threads.
+std::uint64_t task_seed(std::uint64_t seed, std::int64_t lo, std::size_t m) {
+  Rng r(seed ^ (static_cast<std::uint64_t>(lo) * 0xD1B54A32D192ED03ull) ^ (static_cast<std::uint64_t>(m) << 40));
+  return r.next();
+}
+
+struct NdShared {
+  const Adjacency& g;
+  const OrderingOptions& opt;
+  std::vector<std::int32_t>& order;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<NdTask> queue;
+  int active = 0;
+  std::atomic<std::int64_t> nsep{0}, nleaf{0}, topsep{-1};
+  NdShared(const Adjacency& gr, const OrderingOptions& o, std::vector<std::int32_t>& ord) : g(gr), opt(o), order(ord) {}
+};
+
+// Subproblems with more vertices than this go to the shared queue; smaller ones stay with the
+// thread that split them.
+constexpr std::size_t kNdParallelMin = 3000;
+
+// Orders one subproblem and, depth first, the small subproblems it splits into.
+void nd_process(NdShared& S, NdTask root, std::vector<int>& loc, std::vector<std::int32_t>& leaf_out) {
+  const Adjacency& g = S.g;
+  const OrderingOptions& opt = S.opt;
+  std::vector<NdTask> stack;
+  stack.push_back(std::move(root));
+  auto hand_off = [&](NdTask&& t) {
+    if (t.verts.size() > kNdParallelMin) {
+      std::lock_guard<std::mutex> lk(S.mu);
+      S.queue.push_back(std::move(t));
+      S.cv.notify_one();
+    } else {
+      stack.push_back(std::move(t));
+    }
+  };
   while (!stack.empty()) {
-    Task t = std::move(stack.back());
+    NdTask t = std::move(stack.back());
     stack.pop_back();
     const int m = static_cast<int>(t.verts.size());
     if (m == 0) continue;
@@ -526,9 +559,9 @@ std::vector<std::int32_t> nested_dissection(const Adjacency& g, const OrderingOp
     if (m <= opt.leaf_size) {
       leaf_out.clear();
       min_degree_leaf(t.verts, loc, g, leaf_out);
-      for (int i = 0; i < m; ++i) order[t.lo + i] = leaf_out[i];
+      for (int i = 0; i < m; ++i) S.order[t.lo + i] = leaf_out[i];
       for (int v : t.verts) loc[v] = -1;
-      ++nleaf;
+      S.nleaf++;
       continue;
     }
     // local graph
@@ -548,26 +581,27 @@ std::vector<std::int32_t> nested_dissection(const Adjacency& g, const OrderingOp
     std::vector<int> comp(m, -1);
     int nc = 0;
     std::vector<int> q;
-    for (int s = 0; s < m; ++s) {
-      if (comp[s] >= 0) continue;
-      q.assign(1, s);
-      comp[s] = nc;
+    for (int s0 = 0; s0 < m; ++s0) {
+      if (comp[s0] >= 0) continue;
+      q.assign(1, s0);
+      comp[s0] = nc;
       for (std::size_t h = 0; h < q.size(); ++h)
         for (std::int64_t p = w.xadj[q[h]]; p < w.xadj[q[h] + 1]; ++p)
           if (comp[w.adj[p]] < 0) { comp[w.adj[p]] = nc; q.push_back(w.adj[p]); }
       ++nc;
     }
     if (nc > 1) {
-      std::vector<Task> parts(nc);
+      std::vector<NdTask> parts(nc);
       for (int i = 0; i < m; ++i) parts[comp[i]].verts.push_back(t.verts[i]);
       std::int64_t lo = t.lo;
       for (auto& pt : parts) { pt.lo = lo; lo += static_cast<std::int64_t>(pt.verts.size()); }
       for (int v : t.verts) loc[v] = -1;
-      for (auto& pt : parts) stack.push_back(std::move(pt));
+      for (auto it = parts.rbegin(); it != parts.rend(); ++it) hand_off(std::move(*it));
       continue;
     }
+    Rng rng(task_seed(opt.seed, t.lo, t.verts.size()));
     std::vector<std::int8_t> where = separator(w, opt, rng);
-    Task a, b;
+    NdTask a, b;
     std::vector<int> sep;
     for (int i = 0; i < m; ++i) {
       if (where[i] == 0) a.verts.push_back(t.verts[i]);
@@ -576,29 +610,77 @@ std::vector<std::int32_t> nested_dissection(const Adjacency& g, const OrderingOp
     }
     for (int v : t.verts) loc[v] = -1;
     if (a.verts.empty() || b.verts.empty()) {
-      // degenerate split: order this subgraph by minimum degree in chunks (still valid)
+      // degenerate split: order this subgraph by minimum degree (still valid)
       for (int i = 0; i < m; ++i) loc[t.verts[i]] = i;
       leaf_out.clear();
       min_degree_leaf(t.verts, loc, g, leaf_out);
-      for (int i = 0; i < m; ++i) order[t.lo + i] = leaf_out[i];
+      for (int i = 0; i < m; ++i) S.order[t.lo + i] = leaf_out[i];
       for (int v : t.verts) loc[v] = -1;
-      ++nleaf;
+      S.nleaf++;
       continue;
     }
-    ++nsep;
-    if (topsep < 0) topsep = static_cast<std::int64_t>(sep.size());
+    S.nsep++;
+    if (t.lo == 0 && static_cast<std::int64_t>(t.verts.size()) == g.n) S.topsep = static_cast<std::int64_t>(sep.size());
     a.lo = t.lo;
     b.lo = t.lo + static_cast<std::int64_t>(a.verts.size());
     const std::int64_t slo = b.lo + static_cast<std::int64_t>(b.verts.size());
-    for (std::size_t i = 0; i < sep.size(); ++i) order[slo + static_cast<std::int64_t>(i)] = sep[i];
-    stack.push_back(std::move(b));
-    stack.push_back(std::move(a));
+    for (std::size_t i = 0; i < sep.size(); ++i) S.order[slo + static_cast<std::int64_t>(i)] = sep[i];
+    hand_off(std::move(b));
+    hand_off(std::move(a));
   }
+}
+
+}  // namespace
+
+std::vector<std::int32_t> nested_dissection(const Adjacency& g, const OrderingOptions& opt, OrderingStats* stats) {
+  const auto t0 = std::chrono::steady_clock::now();
+  const std::int64_t n = g.n;
+  std::vector<std::int32_t> order(n, -1);
+  NdShared S(g, opt, order);
+  {
+    NdTask t;
+    t.verts.resize(n);
+    for (std::int64_t i = 0; i < n; ++i) t.verts[i] = static_cast<int>(i);
+    S.queue.push_back(std::move(t));
+  }
+  int nthreads = opt.threads;
+  if (nthreads <= 0) {
+    const char* env = std::getenv("HSOLVE_B200_ORDERING_THREADS");
+    nthreads = env ? std::atoi(env) : 0;
+  }
+  if (nthreads <= 0) nthreads = static_cast<int>(std::thread::hardware_concurrency());
+  nthreads = std::max(1, std::min(nthreads, 32));
+  if (n < 2 * static_cast<std::int64_t>(kNdParallelMin)) nthreads = 1;
+  auto worker = [&]() {
+    std::vector<int> loc(n, -1);
+    std::vector<std::int32_t> leaf_out;
+    for (;;) {
+      NdTask t;
+      {
+        std::unique_lock<std::mutex> lk(S.mu);
+        S.cv.wait(lk, [&] { return !S.queue.empty() || S.active == 0; });
+        if (S.queue.empty()) return;  // nothing queued and nobody left to queue more
+        t = std::move(S.queue.back());
+        S.queue.pop_back();
+        ++S.active;
+      }
+      nd_process(S, std::move(t), loc, leaf_out);
+      {
+        std::lock_guard<std::mutex> lk(S.mu);
+        --S.active;
+        if (S.active == 0 && S.queue.empty()) S.cv.notify_all();
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int i = 1; i < nthreads; ++i) pool.emplace_back(worker);
+  worker();
+  for (auto& th : pool) th.join();
   if (stats) {
     stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    stats->separators = nsep;
-    stats->leaves = nleaf;
-    stats->top_separator = topsep < 0 ? 0 : topsep;
+    stats->separators = S.nsep;
+    stats->leaves = S.nleaf;
+    stats->top_separator = S.topsep < 0 ? 0 : S.topsep.load();
   }
   return order;
 }

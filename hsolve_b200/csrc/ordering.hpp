@@ -3,7 +3,8 @@
 // Replaces the reference's hs::compute_ordering (include/hsolve/factor.hpp:598-633,
 // src/factor/ordering.cpp:315), which is kept on the CPU there too: multilevel vertex separators
 // (heavy-edge matching, greedy growing, FM refinement), applied recursively, leaves ordered by
-// minimum degree. Deterministic: a function of the pattern and the seed only.
+// minimum degree. Deterministic: a function of the pattern and the seed only, whatever the number
+// of threads that order the independent subproblems.
 #pragma once
 
 #include <cstdint>
@@ -18,6 +19,8 @@ struct OrderingOptions {
   int init_tries = 7;         // greedy-growing attempts on the coarsest graph
   int refine_passes = 8;      // FM passes per level
   std::uint64_t seed = 2026;
+  int threads = 0;             // host threads (0: $HSOLVE_B200_ORDERING_THREADS, else all); the order
+                               // does not depend on it
 };
 
 struct OrderingStats {

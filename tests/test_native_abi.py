@@ -64,3 +64,23 @@ def test_nested_dissection_beats_natural_order():
     nd = _native.symbolic_stats(a, None)
     nat = _native.symbolic_stats(a, np.arange(1, a.shape[0] + 1, dtype=np.int32))
     assert nd["flops"] < 0.5 * nat["flops"]
+
+
+def test_ordering_does_not_depend_on_thread_count():
+    """The nested-dissection order is a function of the pattern and the seed only (hsolve's
+    compute_ordering is thread-count independent, include/hsolve/factor.hpp:197-242)."""
+    import os
+    import subprocess
+    import sys
+
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); import hsolve_b200 as hs; "
+            "from hsolve_b200.gen import yee; a, _ = yee.pencil(yee.Box((18, 16, 14))); "
+            "np.save(sys.argv[1], hs.compute_ordering(a))") % str(Path(__file__).resolve().parents[1])
+    outs = []
+    for threads in ("1", "3", "8"):
+        path = Path(os.environ.get("TMPDIR", "/tmp")) / f"hsg_order_{os.getpid()}_{threads}.npy"
+        env = dict(os.environ, HSOLVE_B200_ORDERING_THREADS=threads)
+        subprocess.run([sys.executable, "-c", code, str(path)], check=True, env=env)
+        outs.append(np.load(path))
+        path.unlink()
+    assert all(np.array_equal(outs[0], o) for o in outs[1:])
