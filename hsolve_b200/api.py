@@ -231,46 +231,170 @@ def _as_csr(m, name, storage):
     if m.shape[0] != m.shape[1]:
         raise InvalidInputError(f"{name}: matrix must be square, got {m.shape}")
     if np.iscomplexobj(m.data):
-        if np.any(m.data.imag != 0):
-            raise UnsupportedError(f"{name}: complex Hermitian input is not served by this build")
-        m = sp.csr_matrix(m.real)
-    m = sp.csr_matrix(m, dtype=np.float64)
+        m = sp.csr_matrix(m, dtype=np.complex128)
+        if not np.any(m.data.imag != 0):
+            m = sp.csr_matrix(m.real)  # solved as real; the eigenvectors still come back complex
+    else:
+        m = sp.csr_matrix(m, dtype=np.float64)
     m.eliminate_zeros()
     if storage == "upper":
-        m = sp.triu(m) + sp.triu(m, 1).T
+        m = sp.triu(m) + sp.triu(m, 1).conj().T
     elif storage == "lower":
-        m = sp.tril(m) + sp.tril(m, -1).T
+        m = sp.tril(m) + sp.tril(m, -1).conj().T
     elif storage == "auto":
         up, lo = sp.triu(m, 1).nnz, sp.tril(m, -1).nnz
         if (up == 0) != (lo == 0):
-            m = sp.triu(m) + sp.triu(m, 1).T if lo == 0 else sp.tril(m) + sp.tril(m, -1).T
+            m = sp.triu(m) + sp.triu(m, 1).conj().T if lo == 0 else sp.tril(m) + sp.tril(m, -1).conj().T
     m = sp.csr_matrix(m)
     m.sum_duplicates()
     m.sort_indices()
     return m
 
 
+def _complex_dtype(m) -> bool:
+    """True when the input's value type is complex (the eigenvectors are then returned complex)."""
+    import scipy.sparse as sp
+
+    if isinstance(m, (str, bytes, os.PathLike)):
+        path = os.fsdecode(m)
+        try:
+            if path.endswith(".npz"):
+                return np.iscomplexobj(sp.load_npz(path).data)
+            if path.endswith(".npy"):
+                return np.iscomplexobj(np.load(path, mmap_mode="r"))
+            if path.endswith(".mtx"):
+                import scipy.io
+
+                return scipy.io.mminfo(path)[4] == "complex"
+        except Exception:
+            return False
+        return False
+    if sp.issparse(m):
+        return np.iscomplexobj(m.data)
+    return np.iscomplexobj(np.asarray(m))
+
+
 def _hermitian_check(m, name, tol):
-    d = m - m.T
-    nrm = np.sqrt((m.data ** 2).sum())
-    defect = np.sqrt((d.data ** 2).sum()) / nrm if nrm > 0 else 0.0
+    d = m - m.conj().T
+    nrm = np.sqrt((np.abs(m.data) ** 2).sum())
+    defect = np.sqrt((np.abs(d.data) ** 2).sum()) / nrm if nrm > 0 else 0.0
     if defect > tol:
         raise NotHermitianError(f"{name}: ||M - M^H||_F / ||M||_F = {defect:.3e} > hermitian_tol = {tol:g}")
     if defect > 0:
-        m = ((m + m.T) * 0.5).tocsr()
+        m = ((m + m.conj().T) * 0.5).tocsr()
         m.sort_indices()
     return m, defect
 
 
+def _embed(m):
+    """Real symmetric 2n x 2n embedding [[Re M, -Im M], [Im M, Re M]] of a Hermitian matrix M (the
+    reference's complex path, src/factor/mumps_input.cpp:44-150): every eigenvalue of the pencil
+    appears twice and every inertia count doubles."""
+    import scipy.sparse as sp
+
+    x = sp.csr_matrix(m.real)
+    y = sp.csr_matrix(m.imag) if np.iscomplexobj(m.data) else sp.csr_matrix(m.shape)
+    e = sp.bmat([[x, -y], [y, x]], format="csr")
+    e.eliminate_zeros()
+    e.sort_indices()
+    return e
+
+
+def _unembed(w, v, report, a, b, tol, mode, sigma, k):
+    """Complex eigenpairs of the Hermitian pencil (a, b) from the solution (w, v) of its embedding:
+    each cluster of equal embedded eigenvalues (2m of them) spans an m-dimensional complex
+    eigenspace, recovered B-orthonormal from the vectors u + i v of the embedded pairs [u; v] and
+    a Rayleigh-Ritz step within the cluster. Counts of the certificate are halved; an odd count
+    means the embedding's inertia split was not even and the certificate fails."""
+    n = a.shape[0]
+    scale = float(report.get("scale", 0.0)) or 1.0
+    order = np.argsort(w, kind="stable")
+    ws, vs = w[order], v[:, order]
+    clusters, i = [], 0
+    while i < ws.size:
+        j = i + 1
+        while j < ws.size and abs(ws[j] - ws[j - 1]) <= 1e-8 * (abs(ws[j]) + scale):
+            j += 1
+        clusters.append((i, j))
+        i = j
+    lam, vecs, odd = [], [], False
+    bmul = (lambda z: b @ z) if b is not None else (lambda z: z)
+    for i, j in clusters:
+        z = vs[:n, i:j] + 1j * vs[n:, i:j]
+        s = j - i
+        m = s // 2
+        odd = odd or s % 2 == 1
+        if m == 0:
+            continue
+        g = z.conj().T @ bmul(z)
+        g = 0.5 * (g + g.conj().T)
+        gv, gq = np.linalg.eigh(g)
+        gv, gq = gv[-m:], gq[:, -m:]
+        x = z @ (gq / np.sqrt(np.maximum(gv, np.finfo(float).tiny)))
+        h = x.conj().T @ (a @ x)
+        hv, hq = np.linalg.eigh(0.5 * (h + h.conj().T))
+        lam.extend(hv.tolist())
+        vecs.append(x @ hq)
+    lam = np.asarray(lam, dtype=np.float64)
+    x = np.hstack(vecs) if vecs else np.zeros((n, 0), dtype=np.complex128)
+    if mode == "nearest":
+        o = np.argsort(np.abs(lam - sigma), kind="stable")[:k]
+    else:
+        o = np.argsort(lam, kind="stable")
+    lam, x = lam[o], np.asfortranarray(x[:, o])
+    na, nb = float(report.get("norm2_a", 0.0)), float(report.get("norm2_b", 1.0)) or 1.0
+    pairs = []
+    for q in range(lam.size):
+        r = a @ x[:, q] - lam[q] * bmul(x[:, q])
+        rn, xn = float(np.linalg.norm(r)), float(np.linalg.norm(x[:, q]))
+        eta = rn / ((na + abs(lam[q]) * nb) * xn) if xn > 0 else np.inf
+        pairs.append({"lambda_re": float(lam[q]), "lambda_im": 0.0, "abs_residual": rn,
+                      "rel_residual": rn / (abs(lam[q]) * xn) if lam[q] != 0 and xn > 0 else rn,
+                      "backward_error": eta, "accepted": bool(eta <= tol)})
+    rep = dict(report)
+    rep["n"] = n
+    rep["complex_scalars"] = True
+    rep["embedding"] = {"order": 2 * n, "embedded_eigenvalues": int(w.size), "odd_cluster": bool(odd)}
+    rep["pairs"] = pairs
+    cert = dict(rep.get("certificate", {}))
+    passed = bool(cert.get("passed", True)) and not odd
+    for key in ("count_inertia", "count_found"):
+        if key in cert and cert[key] is not None and cert[key] >= 0:
+            passed = passed and cert[key] % 2 == 0
+            cert[key] = cert[key] // 2
+    if cert:
+        cert["passed"] = passed
+        rep["certificate"] = cert
+    if "slices" in rep:
+        sl = []
+        for r0 in rep["slices"]:
+            r1 = dict(r0)
+            for key in ("count", "count_found", "count_inertia"):
+                if isinstance(r1.get(key), int):
+                    r1[key] //= 2
+            sl.append(r1)
+        rep["slices"] = sl
+    ok = all(p["accepted"] for p in pairs) and (not cert or cert["passed"])
+    if mode == "interval" and cert.get("count_inertia") is not None:
+        ok = ok and lam.size == cert["count_inertia"]
+    if mode == "nearest":
+        ok = ok and lam.size == k
+    rep["success"] = bool(ok)
+    return lam, x, rep
+
+
 def solve(A, B=None, *, sigma=None, k=_Default(6), mode=_Default("nearest"), lower=None, upper=None,
           tol=_Default(1e-10), config=None, threads=_Default(0), verbose: int = 0, storage: str = "auto"):
-    """Solve A x = lambda B x (B=None: A x = lambda x) for symmetric A, B with B positive definite,
+    """Solve A x = lambda B x (B=None: A x = lambda x) for Hermitian A, B with B positive definite,
     on the GPU: the nearest-k target around sigma or all eigenvalues in [lower, upper], each with the
-    exact Sylvester-inertia completeness certificate (hsolve.solve's contract)."""
+    exact Sylvester-inertia completeness certificate (hsolve.solve's contract). Real symmetric input
+    is factorized directly; complex Hermitian input goes through the real 2n embedding
+    [[Re, -Im], [Im, Re]] (as the reference does) and comes back as complex eigenvectors."""
     if storage not in _STORAGES:
         raise InvalidInputError(f"storage = {storage!r} is not one of {_STORAGES}")
     cfg = merge_config(config, sigma, k, mode, lower, upper, tol, threads)
     verbose = _integer(verbose, "verbose")
+    cdtype = _complex_dtype(A) or (B is not None and _complex_dtype(B))
     a = _as_csr(A, "A", storage)
     htol = float(cfg.get("hermitian_tol", 1e-10))
     a, da = _hermitian_check(a, "A", htol)
@@ -281,7 +405,40 @@ def solve(A, B=None, *, sigma=None, k=_Default(6), mode=_Default("nearest"), low
         if b.shape != a.shape:
             raise InvalidInputError(f"A is {a.shape} but B is {b.shape}")
         b, db = _hermitian_check(b, "B", htol)
-    c = _struct_from(cfg, verbose)
+    if np.iscomplexobj(a.data) or (b is not None and np.iscomplexobj(b.data)):
+        ae, be = _embed(a), (_embed(b) if b is not None else None)
+        w, v, report = _eigsolve(ae, be, _struct_from(_embedded_config(cfg), verbose))
+        return _complex_result(w, v, report, a, b, cfg, da, db)
+    w, v, report = _eigsolve(a, b, _struct_from(cfg, verbose))
+    return _finish(w, v, report, cfg, da, db, cdtype)
+
+
+def _embedded_config(cfg: dict) -> dict:
+    """The config of the embedded (2n real) problem: twice the requested number of pairs."""
+    ce = json.loads(json.dumps(cfg))
+    t = ce.setdefault("target", {})
+    if t.get("mode", "nearest") == "nearest":
+        t["k"] = 2 * int(t.get("k", 6))
+    return ce
+
+
+def _complex_result(w, v, report, a, b, cfg, da, db) -> SolveResult:
+    t = cfg.get("target", {})
+    mode = t.get("mode", "nearest")
+    lam, x, rep = _unembed(w, v, report, a, b, float(cfg.get("tol", 1e-10)), mode, float(t.get("sigma", 0.0)),
+                           int(t.get("k", 6)))
+    rep["hermitian_defect_a"] = da
+    rep["hermitian_defect_b"] = db
+    result = SolveResult(lam, x, np.zeros(0, dtype=np.complex128), np.zeros((a.shape[0], 0), dtype=np.complex128),
+                         rep, cfg)
+    if not result.success:
+        warnings.warn("hsolve: the solve finished without meeting the tolerance (see result.report['pairs'] "
+                      "and result.report['warnings'])", HsolveWarning, stacklevel=3)
+    return result
+
+
+def _eigsolve(a, b, c):
+    """hsg_eigsolve on real symmetric CSR matrices: (eigenvalues, eigenvectors, report)."""
     n = a.shape[0]
     arp = np.ascontiguousarray(a.indptr, dtype=np.int64)
     aci = np.ascontiguousarray(a.indices, dtype=np.int32)
@@ -296,10 +453,11 @@ def solve(A, B=None, *, sigma=None, k=_Default(6), mode=_Default("nearest"), low
     h = ctypes.c_void_p()
     p = _native._ptr
     _native.check(lib.hsg_eigsolve(n, p(arp), p(aci), p(av), p(brp), p(bci), p(bv), ctypes.byref(c), ctypes.byref(h)))
-    return _result(h, n, cfg, da, db)
+    return _fetch(h)
 
 
-def _result(h, n, cfg, da, db) -> SolveResult:
+def _fetch(h):
+    """(eigenvalues, eigenvectors, report) of a native solution handle, which is freed."""
     lib = _native.lib()
     p = _native._ptr
     try:
@@ -311,8 +469,15 @@ def _result(h, n, cfg, da, db) -> SolveResult:
         report = json.loads(lib.hsg_solution_report(h).decode())
     finally:
         lib.hsg_solution_free(h)
+    return w, v, report
+
+
+def _finish(w, v, report, cfg, da, db, complex_vectors=False) -> SolveResult:
+    n = v.shape[0]
     report["hermitian_defect_a"] = da
     report["hermitian_defect_b"] = db
+    if complex_vectors:
+        v = np.asfortranarray(v.astype(np.complex128))
     result = SolveResult(w, v, np.zeros(0, dtype=np.complex128), np.zeros((n, 0), dtype=np.complex128), report, cfg)
     if not result.success:
         warnings.warn("hsolve: the solve finished without meeting the tolerance (see result.report['pairs'] "
@@ -327,6 +492,7 @@ class Session:
 
     def __init__(self, A, B=None, *, device: int = 0, seed: int = 2026, storage: str = "auto",
                  hermitian_tol: float = 1e-10):
+        self._cdtype = _complex_dtype(A) or (B is not None and _complex_dtype(B))
         a = _as_csr(A, "A", storage)
         a, self._da = _hermitian_check(a, "A", hermitian_tol)
         self._db = 0.0
@@ -336,6 +502,10 @@ class Session:
             if b.shape != a.shape:
                 raise InvalidInputError(f"A is {a.shape} but B is {b.shape}")
             b, self._db = _hermitian_check(b, "B", hermitian_tol)
+        self._complex = None
+        if np.iscomplexobj(a.data) or (b is not None and np.iscomplexobj(b.data)):
+            self._complex = (a, b)  # kept for the eigenvectors; the session holds the embedding
+            a, b = _embed(a), (_embed(b) if b is not None else None)
         self.n = a.shape[0]
         self.device = device
         keep = [np.ascontiguousarray(a.indptr, dtype=np.int64), np.ascontiguousarray(a.indices, dtype=np.int32),
@@ -355,10 +525,13 @@ class Session:
               tol=_Default(1e-10), config=None, verbose: int = 0) -> SolveResult:
         cfg = merge_config(config, sigma, k, mode, lower, upper, tol, _Default(0))
         cfg.setdefault("device", self.device)
-        c = _struct_from(cfg, verbose)
+        c = _struct_from(_embedded_config(cfg) if self._complex else cfg, verbose)
         h = ctypes.c_void_p()
         _native.check(_native.lib().hsg_session_solve(self._h, ctypes.byref(c), ctypes.byref(h)))
-        return _result(h, self.n, cfg, self._da, self._db)
+        w, v, report = _fetch(h)
+        if self._complex:
+            return _complex_result(w, v, report, self._complex[0], self._complex[1], cfg, self._da, self._db)
+        return _finish(w, v, report, cfg, self._da, self._db, self._cdtype)
 
     def close(self):
         if getattr(self, "_h", None):

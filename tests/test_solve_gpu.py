@@ -113,3 +113,48 @@ def test_errors_follow_reference_classes():
         hsolve.solve(a + sp.identity(20), sigma=0.1, k=2, storage="full")
     with pytest.raises(hsolve.InvalidInputError):
         hsolve.solve(sp.identity(5), sigma=0.0, k=2, config={"no_such_key": 1})
+
+
+def test_bloch_cell_complex_example(golden):
+    """hsolve examples/bloch-cell-complex: a complex Hermitian Bloch cell, solved through the real
+    2n embedding; eigenvalues match the reference's stored spectrum and the vectors come back
+    complex and orthonormal."""
+    e, box, a, b = _example(golden, "bloch-cell-complex")
+    assert np.iscomplexobj(a.data)
+    t = e["config"]["target"]
+    res = hsolve.solve(a, b, sigma=t["sigma"], k=t["k"])
+    _check_pairs(res)
+    assert res.report["complex_scalars"] and res.eigenvectors.dtype == np.complex128
+    ref = np.array(e["ref_nearest"])
+    want = np.sort(ref[np.argsort(np.abs(ref - t["sigma"]), kind="stable")[: t["k"]]])
+    np.testing.assert_allclose(np.sort(res.eigenvalues), want, rtol=EIG_RTOL)
+    x = res.eigenvectors
+    np.testing.assert_allclose(x.conj().T @ x, np.eye(x.shape[1]), atol=1e-10)
+    cert = res.report["certificate"]
+    w = yee_exact.exact_spectrum(box.cells, box.lengths, "bloch", box.phases)
+    assert cert["passed"] and cert["count_inertia"] == cert["count_found"]
+    assert cert["count_inertia"] == yee_exact.count_below(w, cert["upper"]) - yee_exact.count_below(w, cert["lower"])
+
+
+def test_bloch_cell_complex_interval_exact_spectrum():
+    box = yee.Box((8, 7, 6), (1.0, 0.9, 0.8), "bloch", (0.4 * np.pi, 0.25 * np.pi, 0.1 * np.pi))
+    a, b = yee.pencil(box, "generalized")
+    w = yee_exact.exact_spectrum(box.cells, box.lengths, "bloch", box.phases)
+    cuts = yee_exact.mid_gap_shifts(w[w > 1.0], 12, 1e-6)
+    lo, hi = cuts[3], cuts[9]
+    sess = hsolve.Session(a, b)
+    for _ in range(2):
+        res = sess.solve(lower=lo, upper=hi)
+        _check_pairs(res)
+        want = w[(w >= lo) & (w <= hi)]
+        np.testing.assert_allclose(res.eigenvalues, want, rtol=EIG_RTOL)
+        assert res.report["certificate"]["count_inertia"] == want.size
+        x = res.eigenvectors
+        np.testing.assert_allclose(x.conj().T @ (b @ x), np.eye(want.size), atol=1e-10)
+
+
+def test_complex_dtype_with_real_values_returns_complex_vectors():
+    a, _ = yee.pencil(yee.Box((6, 5, 4)))
+    res = hsolve.solve(a.astype(np.complex128), sigma=30.0, k=4)
+    _check_pairs(res)
+    assert res.eigenvectors.dtype == np.complex128 and not res.report["complex_scalars"]
