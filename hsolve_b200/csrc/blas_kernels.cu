@@ -7,6 +7,7 @@
 //    (BlockOrthonormalizer, src/eigen/block_ortho.cpp:165,270; orthogonalize_block_cgs2,
 //    src/linalg/dense_ops.hpp:180).
 #include <cstdint>
+#include <mutex>
 
 #include "blas_kernels.cuh"
 #include "common.hpp"
@@ -227,11 +228,10 @@ void gemm_tall(std::int64_t n, int m, int q, const double* x, std::int64_t ldx, 
     return;
   }
   const std::size_t smem = static_cast<std::size_t>(m) * 16 * sizeof(double);
-  static bool configured = false;
-  if (!configured) {
+  static std::once_flag configured;
+  std::call_once(configured, [&] {
     cudaFuncSetAttribute(k_gemm_tall, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    configured = true;
-  }
+  });
   note_launches(1);
   k_gemm_tall<<<grid_for(n, 256), 256, smem, s>>>(n, m, q, x, ldx, sdev, lds, y, ldy, alpha, beta);
 }

@@ -8,6 +8,7 @@
 #include "driver.hpp"
 
 #include <algorithm>
+#include <future>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -199,10 +200,11 @@ struct Timers {
 
 // Inertia count nu_-(A - s B) with endpoint moves on singular shifts (steps.cpp:549-571 behaviour):
 // returns the count and the (possibly moved) shift.
-long long count_below(GpuFactor& F, double& s, double scale, double direction, long long& moves, Timers& tm) {
+long long count_below(GpuFactor& F, double& s, double scale, double direction, long long& moves, Timers& tm,
+                      bool shared = false) {
   const auto t0 = Clock::now();
   for (int t = 0; t < 8; ++t) {
-    hsg_inertia_t in = F.factorize(1.0, -s, true);
+    hsg_inertia_t in = F.factorize(1.0, -s, true, shared);
     if (in.valid) { tm.cert += since(t0); return in.neg; }
     s += direction * 1e-7 * (scale + std::fabs(s)) * (t + 1);
     ++moves;
@@ -211,10 +213,11 @@ long long count_below(GpuFactor& F, double& s, double scale, double direction, l
   HSG_THROW(HSG_SINGULAR, "inertia count: singular at every moved endpoint near " << s);
 }
 
-bool factorize_at(GpuFactor& F, double& sigma, double scale, int retries, int& used_retries, Timers& tm) {
+bool factorize_at(GpuFactor& F, double& sigma, double scale, int retries, int& used_retries, Timers& tm,
+                  bool shared = false) {
   const auto t0 = Clock::now();
   for (int t = 0; t <= retries; ++t) {
-    hsg_inertia_t in = F.factorize(1.0, -sigma, true);
+    hsg_inertia_t in = F.factorize(1.0, -sigma, true, shared);
     if (in.valid) { tm.factor += since(t0); return true; }
     const double step = 1e-6 * (scale + std::fabs(sigma)) * (t + 1);
     sigma += (t % 2 == 0 ? 1.0 : -2.0) * step;
@@ -231,11 +234,12 @@ struct NearestRun {
   int restarts = 0, applies = 0;
 };
 
-NearestRun run_krylov(ShiftInvertOp& op, Problem& P, double sigma, int nev, const hsg_solve_config_t& cfg, int p,
-                      std::uint64_t seed, Timers& tm) {
+NearestRun run_krylov(ShiftInvertOp& op, Problem& P, double sigma, int nev, int nev_strict,
+                      const hsg_solve_config_t& cfg, int p, std::uint64_t seed, Timers& tm) {
   const auto t0 = Clock::now();
   KsOptions o;
   o.nev = nev;
+  o.nev_strict = nev_strict;
   o.ncv = static_cast<int>(cfg.ncv);
   o.block = p;
   o.tol = cfg.tol * cfg.inner_tol_factor;
@@ -268,6 +272,18 @@ struct Session::Impl {
   CsrHost a;
   std::unique_ptr<CsrHost> b;
   std::unique_ptr<GpuFactor> F;
+  // two more factorization objects on the same analysis, created at first use: the inertia counts
+  // of the window ends run on them concurrently with each other and with F's slice factorization
+  std::unique_ptr<GpuFactor> C[2];
+  hsg_options_t fopt{};
+  GpuFactor& counter(int i) {
+    if (!C[i]) {
+      auto g = std::make_unique<GpuFactor>(fopt);
+      g->analyze_like(*F);
+      C[i] = std::move(g);
+    }
+    return *C[i];
+  }
   Problem P;
   std::string problem = "HEP";
   double scale = 0.0;
@@ -291,6 +307,7 @@ Session::Session(const CsrHost& a_in, const CsrHost* b_in, int device, std::uint
   hsg_options_t fo;
   hsg_default_options(&fo);
   fo.device = device;
+  S.fopt = fo;
   S.F = std::make_unique<GpuFactor>(fo);
   GpuFactor& F = *S.F;
   Problem& P = S.P;
@@ -387,9 +404,8 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
     const int p = cfg.block_size > 0 ? cfg.block_size : auto_block(nev);
     block_used = p;
     for (int attempt = 0; attempt < 4; ++attempt) {
-      if (attempt > 0 && !factorize_at(F, sigma, scale, cfg.max_shift_retries, shift_retries, tm))
-        HSG_THROW(HSG_SINGULAR, "A - sigma B is numerically singular at the working shift");
-      NearestRun run = run_krylov(op, P, sigma, nev, cfg, p, cfg.seed + attempt, tm);
+      // reruns keep F's factorization at sigma: the certificate's counts run on other objects
+      NearestRun run = run_krylov(op, P, sigma, nev, static_cast<int>(k), cfg, p, cfg.seed + attempt, tm);
       restarts += run.restarts;
       const std::size_t M = run.lam.size();
       if (static_cast<std::int64_t>(M) < k) {
@@ -417,8 +433,21 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
         lo = sigma - R;
         hi = sigma + R;
         double lo_m = lo, hi_m = hi;
-        const long long nlo = count_below(F, lo_m, scale, -1.0, moves, tm);
-        const long long nhi = count_below(F, hi_m, scale, +1.0, moves, tm);
+        long long moves_hi = 0;
+        Timers t_lo, t_hi;
+        GpuFactor& C0 = S.counter(0);
+        GpuFactor& C1 = S.counter(1);
+        auto f_hi = std::async(std::launch::async, [&] { return count_below(C1, hi_m, scale, +1.0, moves_hi, t_hi, true); });
+        long long nlo = -1;
+        try {
+          nlo = count_below(C0, lo_m, scale, -1.0, moves, t_lo, true);
+        } catch (...) {
+          f_hi.wait();
+          throw;
+        }
+        const long long nhi = f_hi.get();
+        moves += moves_hi;
+        tm.cert += std::max(t_lo.cert, t_hi.cert);
         cnt = nhi - nlo;
         lo = lo_m;
         hi = hi_m;
@@ -460,9 +489,34 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
     // ---------------------------------------------------------------- interval (slicing)
     double lo = cfg.lower, hi = cfg.upper;
     HSG_REQUIRE(std::isfinite(lo) && std::isfinite(hi) && lo < hi, HSG_INVALID_INPUT, "interval needs lower < upper");
-    long long moves = 0;
-    const long long nlo = count_below(F, lo, scale, -1.0, moves, tm);
-    const long long nhi = count_below(F, hi, scale, +1.0, moves, tm);
+    long long moves = 0, moves_hi = 0;
+    // the window-end counts on two objects and, speculatively, the factorization at the window
+    // midpoint (the slice shift when no split is needed, else the first cut) on F, all at once
+    const double mid0 = 0.5 * (lo + hi);
+    double sigma_mid = mid0;
+    bool mid_ok = false;
+    Timers t_lo, t_hi;
+    GpuFactor& C0 = S.counter(0);
+    GpuFactor& C1 = S.counter(1);
+    auto f_lo = std::async(std::launch::async, [&] { return count_below(C0, lo, scale, -1.0, moves, t_lo, true); });
+    auto f_hi = std::async(std::launch::async, [&] { return count_below(C1, hi, scale, +1.0, moves_hi, t_hi, true); });
+    try {
+      mid_ok = factorize_at(F, sigma_mid, scale, cfg.max_shift_retries, shift_retries, tm, true);
+    } catch (...) {
+      f_lo.wait();
+      f_hi.wait();
+      throw;
+    }
+    long long nlo = -1;
+    try {
+      nlo = f_lo.get();
+    } catch (...) {
+      f_hi.wait();
+      throw;
+    }
+    const long long nhi = f_hi.get();
+    moves += moves_hi;
+    tm.cert += std::max(t_lo.cert, t_hi.cert);
     const long long N = nhi - nlo;
     cert.performed = true;
     cert.lower = lo;
@@ -473,6 +527,12 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
     std::vector<double> cuts{lo, hi};
     std::vector<long long> below{nlo, nhi};
     const long long target = cfg.slice_size > 0 ? cfg.slice_size : 96;
+    bool spec_slice = mid_ok;  // F holds the factorization at sigma_mid
+    if (N > target && mid_ok && sigma_mid > lo && sigma_mid < hi) {
+      cuts.insert(cuts.begin() + 1, sigma_mid);
+      below.insert(below.begin() + 1, F.inertia().neg);
+      spec_slice = false;
+    }
     // split slices with too many eigenvalues at their midpoint (one count per cut)
     for (std::size_t i = 0; i + 1 < cuts.size();) {
       const long long c = below[i + 1] - below[i];
@@ -494,17 +554,20 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
       SliceRec rec{cuts[i], cuts[i + 1], 0.5 * (cuts[i] + cuts[i + 1]), c, 0, 0, 0, 0, 0, c == 0};
       if (c == 0) { slices.push_back(rec); continue; }
       double sigma = rec.sigma;
-      if (!factorize_at(F, sigma, scale, cfg.max_shift_retries, shift_retries, tm))
+      if (spec_slice && cuts.size() == 2) {
+        sigma = sigma_mid;  // factorized while the window ends were counted
+        spec_slice = false;
+      } else if (!factorize_at(F, sigma, scale, cfg.max_shift_retries, shift_retries, tm)) {
         HSG_THROW(HSG_SINGULAR, "slice shift singular near " << rec.sigma);
+      }
       rec.sigma = sigma;
       int nev = static_cast<int>(std::min<std::int64_t>(n - 1, c + std::max<long long>(4, c / 4)));
       const int p = cfg.block_size > 0 ? cfg.block_size : auto_block(nev);
       block_used = std::max(block_used, p);
       for (int attempt = 0; attempt < 4; ++attempt) {
-        if (attempt > 0 && !factorize_at(F, sigma, scale, cfg.max_shift_retries, shift_retries, tm))
-          HSG_THROW(HSG_SINGULAR, "slice shift singular");
+        // reruns reuse F's factorization at sigma (nothing else runs on F inside the slice loop)
         const long long applies0 = op.columns;
-        NearestRun run = run_krylov(op, P, sigma, nev, cfg, p, cfg.seed + 17 * i + attempt, tm);
+        NearestRun run = run_krylov(op, P, sigma, nev, static_cast<int>(c), cfg, p, cfg.seed + 17 * i + attempt, tm);
         rec.restarts += run.restarts;
         rec.op_applies += op.columns - applies0;
         rec.nev = nev;

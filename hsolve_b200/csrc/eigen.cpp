@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <limits>
 #include <numeric>
 #include <random>
 
@@ -206,10 +207,23 @@ KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, 
       }
       rn[i] = std::sqrt(acc);
     }
+    // equal Ritz values (a multiple eigenvalue, possibly with more copies in the basis than the
+    // wanted set takes) are ranked by residual, so the wanted set and the kept basis take the
+    // converged copies first instead of an arbitrary subset of the cluster
+    for (int q0 = 0; q0 < m;) {
+      int q1 = q0 + 1;
+      const double ref = std::fabs(w[order[q0]]);
+      while (q1 < m && std::fabs(w[order[q1]] - w[order[q0]]) <= 1e-12 * ref) ++q1;
+      if (q1 - q0 > 1)
+        std::stable_sort(order.begin() + q0, order.begin() + q1, [&](int a, int b) { return rn[a] < rn[b]; });
+      q0 = q1;
+    }
+    const int strict = opt.nev_strict > 0 ? std::min(opt.nev_strict, nev) : nev;
+    auto tol_at = [&](int q) { return q < strict ? opt.tol : std::max(opt.tol, opt.tol_buffer); };
     int nconv = 0;
     for (int q = 0; q < nev && q < m; ++q) {
       const int i = order[q];
-      if (rn[i] <= opt.tol * std::fabs(w[i])) ++nconv;
+      if (rn[i] <= tol_at(q) * std::fabs(w[i])) ++nconv;
     }
     res.t_rr += seconds_since(trr);
     const bool done = nconv >= std::min(nev, m) || res.restarts >= opt.max_restarts;
@@ -223,7 +237,7 @@ KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, 
         const int i = order[q];
         res.theta[q] = w[i];
         res.resid[q] = rn[i];
-        res.converged[q] = rn[i] <= opt.tol * std::fabs(w[i]);
+        res.converged[q] = rn[i] <= tol_at(q) * std::fabs(w[i]);
         std::copy(S.begin() + static_cast<std::ptrdiff_t>(i) * m, S.begin() + static_cast<std::ptrdiff_t>(i + 1) * m,
                   Q.begin() + static_cast<std::ptrdiff_t>(q) * m);
       }
@@ -274,6 +288,22 @@ KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, 
         Tnm(keep + a, q) = t;
         Tnm(q, keep + a) = t;
       }
+    // locking: a kept pair whose coupling column to the residual block is at rounding level
+    // relative to every wanted Ritz value (|b(:, q)| <= 4 eps min |theta_wanted|) is decoupled, so
+    // later cycles leave it converged (the reference's rule, src/eigen/block_lanczos.cpp:65)
+    {
+      double min_wanted = std::numeric_limits<double>::infinity();
+      for (int q = 0; q < std::min(nev, m); ++q) min_wanted = std::min(min_wanted, std::fabs(w[order[q]]));
+      const double lock_tol = 4.0 * std::numeric_limits<double>::epsilon() * min_wanted;
+      for (int q = 0; q < keep; ++q) {
+        double c2 = 0.0;
+        for (int a = 0; a < p; ++a) c2 += Tnm(keep + a, q) * Tnm(keep + a, q);
+        if (std::sqrt(c2) <= lock_tol) {
+          for (int a = 0; a < p; ++a) { Tnm(keep + a, q) = 0.0; Tnm(q, keep + a) = 0.0; }
+          ++res.locked;
+        }
+      }
+    }
     T.swap(Tn);
     m = keep;
     res.restarts += 1;

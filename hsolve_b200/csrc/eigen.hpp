@@ -34,6 +34,10 @@ struct KsOptions {
   int ncv = 0;           // basis columns (0: automatic)
   int block = 1;         // block width p
   double tol = 1e-11;    // ||OP y - theta y||_B <= tol |theta|
+  // The first nev_strict wanted pairs (by `which`) must meet tol; the others, which the callers
+  // only use to place a window in a gap of the spectrum, meet max(tol, tol_buffer). 0: all nev.
+  int nev_strict = 0;
+  double tol_buffer = 1e-8;
   int max_restarts = 1000;
   std::uint64_t seed = 2026;
   Which which = Which::LargestMagnitude;
@@ -48,6 +52,7 @@ struct KsResult {
   int restarts = 0;
   int applies = 0;             // operator applications (columns)
   int block_steps = 0;
+  long long locked = 0;         // pairs decoupled by locking, summed over restarts
   std::vector<double> other_theta;  // the remaining Ritz values of the last basis (gap placement)
   std::vector<double> other_resid;
   DevBuf<double> X;            // n x nev Ritz vectors (B-orthonormal), if requested

@@ -16,6 +16,7 @@
 // (failed) so that the host can move them into the parent front and factorize again.
 #include <cooperative_groups.h>
 #include <cstdint>
+#include <mutex>
 
 #include "common.hpp"
 #include "device.cuh"
@@ -1312,11 +1313,10 @@ void launch_front_app(const std::int32_t* list, int nlist, const SnDev* sn, doub
                       FactorCounters* cnt, std::int32_t* failed, cudaStream_t s) {
   if (nlist <= 0) return;
   constexpr std::size_t smem = 2 * kNB * kTile * sizeof(double);
-  static bool configured = false;
-  if (!configured) {
+  static std::once_flag configured;
+  std::call_once(configured, [&] {
     cudaFuncSetAttribute(k_front_app, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    configured = true;
-  }
+  });
   note_launches(1);
   k_front_app<<<nlist, kAppThreads, smem, s>>>(list, sn, panels, cb, scratch, piv, pidx, prm, cnt, failed);
 }

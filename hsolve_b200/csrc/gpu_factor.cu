@@ -139,6 +139,39 @@ void GpuFactor::analyze(std::int64_t n, const std::int64_t* a_rp, const std::int
   analysed_ = true;
 }
 
+void GpuFactor::analyze_like(const GpuFactor& src) {
+  HSG_REQUIRE(src.analysed_, HSG_INTERNAL, "analyze_like: source not analysed");
+  HSG_REQUIRE(src.opt_.device == opt_.device, HSG_INVALID_INPUT, "analyze_like: different devices");
+  DeviceGuard g(opt_.device);
+  analysed_ = false;
+  factored_ = false;
+  n_ = src.n_;
+  nnz_ = src.nnz_;
+  rp_ = src.rp_;
+  ci_ = src.ci_;
+  row_ = src.row_;
+  sym_ = src.sym_;
+  cuda_check(cudaStreamSynchronize(src.stream_), "analyze_like: source");
+  d_row_.alloc(src.d_row_.n);
+  d_col_.alloc(src.d_col_.n);
+  d_a_.alloc(src.d_a_.n);
+  d_b_.alloc(std::max<std::size_t>(1, src.d_b_.n));
+  cuda_check(cudaMemcpyAsync(d_row_.p, src.d_row_.p, src.d_row_.n * sizeof(std::int32_t), cudaMemcpyDeviceToDevice, stream_), "copy");
+  cuda_check(cudaMemcpyAsync(d_col_.p, src.d_col_.p, src.d_col_.n * sizeof(std::int32_t), cudaMemcpyDeviceToDevice, stream_), "copy");
+  cuda_check(cudaMemcpyAsync(d_a_.p, src.d_a_.p, src.d_a_.n * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy");
+  if (src.d_b_.n) cuda_check(cudaMemcpyAsync(d_b_.p, src.d_b_.p, src.d_b_.n * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy");
+  d_scale_.alloc(n_);
+  d_r_.alloc(n_);
+  d_cnt_.alloc(1);
+  d_failed_.alloc(static_cast<std::size_t>(n_));
+  d_piv_.alloc(n_);
+  d_pidx_.alloc(n_);
+  build_plan();
+  cuda_check(cudaStreamSynchronize(stream_), "analyze_like");
+  inertia_ = hsg_inertia_t{-1, -1, -1, 0, 0, 0, 0, 0};
+  analysed_ = true;
+}
+
 void GpuFactor::build_plan() {
   const Symbolic& S = sym_;
   const std::int32_t ns = S.ns;
@@ -296,40 +329,48 @@ void GpuFactor::build_plan() {
       L.solve_ctas = starts.back();
       L.solve_steps = steps;
     }
-    // cooperative launch when the level's panel fronts fit the co-resident grid
+    // cooperative launch when the level's panel fronts fit the co-resident grid; CTAs apportioned
+    // by m^2, for the whole device and for the shared budget (a third of it, used while several
+    // shifts are factorized at once)
+    const int shared_max = std::max(1, coop_max_ / kSharedParts);
     if (!app.empty() && static_cast<int>(app.size()) <= coop_max_) {
       int mmax = 0;
       for (std::int32_t s : app) mmax = std::max(mmax, sn[s].m);
       if (mmax >= kCoopMinFront) {
-        std::vector<double> wts(app.size());
-        double wsum = 0.0;
-        for (std::size_t q = 0; q < app.size(); ++q) {
-          const double m = sn[app[q]].m;
-          wts[q] = m * m;
-          wsum += wts[q];
-        }
-        std::vector<int> nr(app.size());
-        int total = 0;
-        for (std::size_t q = 0; q < app.size(); ++q) {
-          // about 8 tiles of 64 x 64 per CTA at the first panel
-          const double want = std::ceil(wts[q] / (2.0 * 64 * 64 * 8));
-          nr[q] = static_cast<int>(std::max(1.0, std::min<double>(want, coop_max_)));
-          total += nr[q];
-        }
-        if (total > coop_max_) {
-          const int spare = coop_max_ - static_cast<int>(app.size());
-          total = 0;
+        auto plan_ctas = [&](int budget, std::int64_t& off, int& ctas) {
+          std::vector<double> wts(app.size());
+          double wsum = 0.0;
           for (std::size_t q = 0; q < app.size(); ++q) {
-            nr[q] = 1 + static_cast<int>(std::floor(spare * wts[q] / wsum));
+            const double m = sn[app[q]].m;
+            wts[q] = m * m;
+            wsum += wts[q];
+          }
+          std::vector<int> nr(app.size());
+          int total = 0;
+          for (std::size_t q = 0; q < app.size(); ++q) {
+            // about 8 tiles of 64 x 64 per CTA at the first panel
+            const double want = std::ceil(wts[q] / (2.0 * 64 * 64 * 8));
+            nr[q] = static_cast<int>(std::max(1.0, std::min<double>(want, budget)));
             total += nr[q];
           }
-        }
-        std::vector<std::int32_t> starts(app.size() + 1, 0);
-        for (std::size_t q = 0; q < app.size(); ++q) starts[q + 1] = starts[q] + nr[q];
+          if (total > budget) {
+            const int spare = budget - static_cast<int>(app.size());
+            total = 0;
+            for (std::size_t q = 0; q < app.size(); ++q) {
+              nr[q] = 1 + static_cast<int>(std::floor(spare * wts[q] / wsum));
+              total += nr[q];
+            }
+          }
+          std::vector<std::int32_t> starts(app.size() + 1, 0);
+          for (std::size_t q = 0; q < app.size(); ++q) starts[q + 1] = starts[q] + nr[q];
+          off = static_cast<std::int64_t>(lists.size());
+          lists.insert(lists.end(), starts.begin(), starts.end());
+          ctas = starts.back();
+        };
         L.coop = true;
-        L.cta_off = static_cast<std::int64_t>(lists.size());
-        lists.insert(lists.end(), starts.begin(), starts.end());
-        L.coop_ctas = starts.back();
+        plan_ctas(coop_max_, L.cta_off, L.coop_ctas);
+        L.coop_shared = static_cast<int>(app.size()) <= shared_max;
+        if (L.coop_shared) plan_ctas(shared_max, L.cta_off_shared, L.coop_ctas_shared);
         L.done_slot = ncoop_++;
       }
     }
@@ -413,8 +454,10 @@ void GpuFactor::run_numeric(double alpha, double beta, bool detection) {
     for (const auto& ea : L.ea) launch_extend_add(d_items_.p + ea.first, ea.second, d_sn_.p, d_rmap_.p, d_panels_.p, d_cb_.p, s);
     launch_front_small(32, lists + L.s32_off, L.s32_n, d_sn_.p, d_panels_.p, d_cb_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
     launch_front_small(kSmallMax, lists + L.s64_off, L.s64_n, d_sn_.p, d_panels_.p, d_cb_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
-    if (L.coop) {
-      cuda_check(launch_front_coop(lists + L.app_off, lists + L.cta_off, L.app_n, L.coop_ctas, d_sn_.p, d_panels_.p,
+    if (shared_ ? L.coop_shared : L.coop) {
+      const std::int64_t cta_off = shared_ ? L.cta_off_shared : L.cta_off;
+      const int ctas = shared_ ? L.coop_ctas_shared : L.coop_ctas;
+      cuda_check(launch_front_coop(lists + L.app_off, lists + cta_off, L.app_n, ctas, d_sn_.p, d_panels_.p,
                                    d_cb_.p, d_scratch_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p,
                                    d_level_done_.p + L.done_slot, s),
                  "cooperative front launch");
@@ -425,7 +468,8 @@ void GpuFactor::run_numeric(double alpha, double beta, bool detection) {
   cuda_check(cudaGetLastError(), "factorization launch");
 }
 
-hsg_inertia_t GpuFactor::factorize(double alpha, double beta, bool detection) {
+hsg_inertia_t GpuFactor::factorize(double alpha, double beta, bool detection, bool shared) {
+  shared_ = shared;
   HSG_REQUIRE(analysed_, HSG_INTERNAL, "factorize before analyze");
   HSG_REQUIRE(std::isfinite(alpha) && std::isfinite(beta), HSG_INVALID_INPUT, "non-finite alpha / beta");
   DeviceGuard g(opt_.device);

@@ -71,7 +71,11 @@ class GpuFactor {
 
   void analyze(std::int64_t n, const std::int64_t* a_rp, const std::int32_t* a_ci, const double* a_v,
                const std::int64_t* b_rp, const std::int32_t* b_ci, const double* b_v, const std::int32_t* order);
-  hsg_inertia_t factorize(double alpha, double beta, bool detection);
+  // shared: use the cooperative plan sized for a third of the device, so that up to three
+  // factorizations (of different shifts, on different objects) can run at once
+  hsg_inertia_t factorize(double alpha, double beta, bool detection, bool shared = false);
+  // The analysis of `src` (pattern, values of A and B, symbolic analysis) without recomputing it.
+  void analyze_like(const GpuFactor& src);
   void solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_device);
   // Doubles of work space that solve_with_scratch needs for nrhs right-hand sides: n x nrhs for the
   // permuted, scaled right-hand sides and (contribution rows) x min(nrhs, 8) for the update vectors.
@@ -118,6 +122,8 @@ class GpuFactor {
     bool solve_coop = false;           // few fronts: cooperative sweeps, CTAs split by panel size
     std::int64_t solve_cta_off = 0; int solve_ctas = 0; int solve_steps = 0;
     std::int64_t work_off_off = 0;     // offsets of the fronts' work vectors (index into d_work_off_)
+    bool coop_shared = false;          // the level also fits the shared budget's co-resident grid
+    std::int64_t cta_off_shared = 0; int coop_ctas_shared = 0;  // cooperative plan of the shared budget
     int cnt_off = 0;                   // first publication counter of the level's fronts
   };
   void build_plan();
@@ -168,6 +174,8 @@ class GpuFactor {
   void build_solve_operator();
   int solve_coop_max_ = 0;
   int coop_max_ = 0;
+  bool shared_ = false;
+  static constexpr int kSharedParts = 3;
   int ncoop_ = 0;
 };
 

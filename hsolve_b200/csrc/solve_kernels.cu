@@ -9,6 +9,7 @@
 // are carried together so that every L entry is read once per chunk.
 #include <cooperative_groups.h>
 #include <cstdint>
+#include <mutex>
 
 #include "common.hpp"
 #include "device.cuh"
@@ -772,11 +773,10 @@ void launch_solve_fwd(const std::int32_t* list, int nlist, int maxm, const SnDev
   if (nlist <= 0) return;
   const int R = solve_rhs_chunk(maxm, nrhs);
   const std::size_t smem = solve_smem(maxm, R);
-  static bool configured = false;
-  if (!configured) {
+  static std::once_flag configured;
+  std::call_once(configured, [&] {
     cudaFuncSetAttribute(k_solve_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSolveSmemMax));
-    configured = true;
-  }
+  });
   note_launches(1);
   k_solve_fwd<<<nlist, 256, smem, s>>>(list, sn, child_ptr, children, rmap, panels, piv, pidx, blk, nblk, inv, x, n,
                                        vec, nrhs, R);
@@ -805,11 +805,10 @@ void launch_solve_bwd(const std::int32_t* list, int nlist, int maxm, const SnDev
   if (nlist <= 0) return;
   const int R = solve_rhs_chunk(maxm, nrhs);
   const std::size_t smem = solve_smem(maxm, R);
-  static bool configured = false;
-  if (!configured) {
+  static std::once_flag configured;
+  std::call_once(configured, [&] {
     cudaFuncSetAttribute(k_solve_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSolveSmemMax));
-    configured = true;
-  }
+  });
   note_launches(1);
   k_solve_bwd<<<nlist, 256, smem, s>>>(list, sn, rows, panels, pidx, blk, nblk, inv, x, n, nrhs, R);
 }
@@ -826,11 +825,10 @@ void launch_sb_build(const int2* sbl, int nsb, const int4* tiles, int ntiles, co
                      const signed char* piv, double* W, cudaStream_t s) {
   if (nsb <= 0) return;
   constexpr std::size_t smem = sizeof(double) * (kSB * (kSB - 1) / 2 + kSB * (kSB + 1) / 2 + kSB);
-  static bool configured = false;
-  if (!configured) {
+  static std::once_flag configured;
+  std::call_once(configured, [&] {
     cudaFuncSetAttribute(k_sb_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    configured = true;
-  }
+  });
   note_launches(1);
   k_sb_inverse<<<nsb, 256, smem, s>>>(sbl, sn, panels, piv, W);
   if (ntiles > 0) {
