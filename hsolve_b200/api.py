@@ -24,7 +24,8 @@ class _SolveConfig(ctypes.Structure):
                 ("tol", ctypes.c_double), ("inner_tol_factor", ctypes.c_double), ("ncv", ctypes.c_int64),
                 ("block_size", ctypes.c_int32), ("slice_size", ctypes.c_int64), ("max_restarts", ctypes.c_int32),
                 ("seed", ctypes.c_uint64), ("certificate", ctypes.c_int32), ("max_shift_retries", ctypes.c_int32),
-                ("factor_precision", ctypes.c_int32), ("device", ctypes.c_int32), ("verbose", ctypes.c_int32)]
+                ("factor_precision", ctypes.c_int32), ("device", ctypes.c_int32), ("verbose", ctypes.c_int32),
+                ("batch_shifts", ctypes.c_int32)]
 
 
 _P = ctypes.c_void_p
@@ -53,7 +54,7 @@ _KNOWN_KEYS = {"target", "problem", "method", "tol", "hermitian_tol", "inner_tol
                "deterministic", "blr", "out_of_core", "inertia_check", "inertia_counter", "certificate",
                "certificate_delta", "certificate_fault_drop", "inexact_fault_reject", "certificate_fault_count",
                "structure_candidates", "subspace_bound", "secure", "zero_filter_tol", "complex_tol",
-               "max_shift_retries", "device"}
+               "max_shift_retries", "device", "batch_shifts"}
 
 
 @dataclass(repr=False, eq=False)
@@ -200,6 +201,7 @@ def _struct_from(cfg: dict, verbose: int) -> _SolveConfig:
     c.factor_precision = 1 if prec == "single" else 0
     c.device = int(cfg.get("device", 0))
     c.verbose = int(verbose)
+    c.batch_shifts = 1 if bool(cfg.get("batch_shifts", True)) else 0
     if not (0.0 < c.tol < 1.0):
         raise InvalidInputError("tol must be in (0, 1)")
     return c

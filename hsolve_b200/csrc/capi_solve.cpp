@@ -58,6 +58,7 @@ void hsg_default_solve_config(hsg_solve_config_t* c) {
   c->factor_precision = 0;
   c->device = 0;
   c->verbose = 0;
+  c->batch_shifts = 1;
 }
 
 int hsg_eigsolve(int64_t n, const int64_t* a_rowptr, const int32_t* a_col, const double* a_val,

@@ -390,6 +390,8 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
   long long applies_before = 0;
   double sigma_used = cfg.sigma;
   const bool certify = cfg.certificate == 0;
+  const bool batch = cfg.batch_shifts != 0;
+  bool f_stale = false;  // F's factorization was overwritten by a count at another shift
 
   if (cfg.mode == 0) {
     // ---------------------------------------------------------------- nearest
@@ -404,7 +406,10 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
     const int p = cfg.block_size > 0 ? cfg.block_size : auto_block(nev);
     block_used = p;
     for (int attempt = 0; attempt < 4; ++attempt) {
-      // reruns keep F's factorization at sigma: the certificate's counts run on other objects
+      // reruns keep F's factorization at sigma when the certificate's counts ran on other objects
+      if (f_stale && !factorize_at(F, sigma, scale, cfg.max_shift_retries, shift_retries, tm))
+        HSG_THROW(HSG_SINGULAR, "A - sigma B is numerically singular at the working shift");
+      f_stale = false;
       NearestRun run = run_krylov(op, P, sigma, nev, static_cast<int>(k), cfg, p, cfg.seed + attempt, tm);
       restarts += run.restarts;
       const std::size_t M = run.lam.size();
@@ -433,21 +438,28 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
         lo = sigma - R;
         hi = sigma + R;
         double lo_m = lo, hi_m = hi;
-        long long moves_hi = 0;
-        Timers t_lo, t_hi;
-        GpuFactor& C0 = S.counter(0);
-        GpuFactor& C1 = S.counter(1);
-        auto f_hi = std::async(std::launch::async, [&] { return count_below(C1, hi_m, scale, +1.0, moves_hi, t_hi, true); });
-        long long nlo = -1;
-        try {
-          nlo = count_below(C0, lo_m, scale, -1.0, moves, t_lo, true);
-        } catch (...) {
-          f_hi.wait();
-          throw;
+        long long nlo = -1, nhi = -1;
+        if (batch) {
+          long long moves_hi = 0;
+          Timers t_lo, t_hi;
+          GpuFactor& C0 = S.counter(0);
+          GpuFactor& C1 = S.counter(1);
+          auto f_hi = std::async(std::launch::async, [&] { return count_below(C1, hi_m, scale, +1.0, moves_hi, t_hi, true); });
+          try {
+            nlo = count_below(C0, lo_m, scale, -1.0, moves, t_lo, true);
+          } catch (...) {
+            f_hi.wait();
+            throw;
+          }
+          nhi = f_hi.get();
+          moves += moves_hi;
+          tm.cert += std::max(t_lo.cert, t_hi.cert);
+        } else {
+          // plain path: the counts overwrite F's factorization, so a rerun refactorizes
+          nlo = count_below(F, lo_m, scale, -1.0, moves, tm);
+          nhi = count_below(F, hi_m, scale, +1.0, moves, tm);
+          f_stale = true;
         }
-        const long long nhi = f_hi.get();
-        moves += moves_hi;
-        tm.cert += std::max(t_lo.cert, t_hi.cert);
         cnt = nhi - nlo;
         lo = lo_m;
         hi = hi_m;
@@ -490,33 +502,38 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
     double lo = cfg.lower, hi = cfg.upper;
     HSG_REQUIRE(std::isfinite(lo) && std::isfinite(hi) && lo < hi, HSG_INVALID_INPUT, "interval needs lower < upper");
     long long moves = 0, moves_hi = 0;
-    // the window-end counts on two objects and, speculatively, the factorization at the window
-    // midpoint (the slice shift when no split is needed, else the first cut) on F, all at once
     const double mid0 = 0.5 * (lo + hi);
     double sigma_mid = mid0;
     bool mid_ok = false;
-    Timers t_lo, t_hi;
-    GpuFactor& C0 = S.counter(0);
-    GpuFactor& C1 = S.counter(1);
-    auto f_lo = std::async(std::launch::async, [&] { return count_below(C0, lo, scale, -1.0, moves, t_lo, true); });
-    auto f_hi = std::async(std::launch::async, [&] { return count_below(C1, hi, scale, +1.0, moves_hi, t_hi, true); });
-    try {
-      mid_ok = factorize_at(F, sigma_mid, scale, cfg.max_shift_retries, shift_retries, tm, true);
-    } catch (...) {
-      f_lo.wait();
-      f_hi.wait();
-      throw;
+    long long nlo = -1, nhi = -1;
+    if (batch) {
+      // the window-end counts on two objects and, speculatively, the factorization at the window
+      // midpoint (the slice shift when no split is needed, else the first cut) on F, all at once
+      Timers t_lo, t_hi;
+      GpuFactor& C0 = S.counter(0);
+      GpuFactor& C1 = S.counter(1);
+      auto f_lo = std::async(std::launch::async, [&] { return count_below(C0, lo, scale, -1.0, moves, t_lo, true); });
+      auto f_hi = std::async(std::launch::async, [&] { return count_below(C1, hi, scale, +1.0, moves_hi, t_hi, true); });
+      try {
+        mid_ok = factorize_at(F, sigma_mid, scale, cfg.max_shift_retries, shift_retries, tm, true);
+      } catch (...) {
+        f_lo.wait();
+        f_hi.wait();
+        throw;
+      }
+      try {
+        nlo = f_lo.get();
+      } catch (...) {
+        f_hi.wait();
+        throw;
+      }
+      nhi = f_hi.get();
+      moves += moves_hi;
+      tm.cert += std::max(t_lo.cert, t_hi.cert);
+    } else {
+      nlo = count_below(F, lo, scale, -1.0, moves, tm);
+      nhi = count_below(F, hi, scale, +1.0, moves, tm);
     }
-    long long nlo = -1;
-    try {
-      nlo = f_lo.get();
-    } catch (...) {
-      f_hi.wait();
-      throw;
-    }
-    const long long nhi = f_hi.get();
-    moves += moves_hi;
-    tm.cert += std::max(t_lo.cert, t_hi.cert);
     const long long N = nhi - nlo;
     cert.performed = true;
     cert.lower = lo;

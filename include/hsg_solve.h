@@ -35,6 +35,10 @@ typedef struct {
   int32_t factor_precision;   /* hs::FactorPrecision: 0 double, 1 single (FP32 factors + FP64 refinement) */
   int32_t device;             /* CUDA device */
   int32_t verbose;
+  int32_t batch_shifts;       /* 1 (default): independent shifts of one solve (window-end counts, the
+                                 slice factorization) run at once on several factorization objects;
+                                 0: one after another on one object (the plain path). No counterpart
+                                 in hsolve. */
 } hsg_solve_config_t;
 
 typedef struct hsg_solution hsg_solution;
