@@ -5,6 +5,9 @@
 #include <chrono>
 #include <cmath>
 #include <numeric>
+#include <mutex>
+#include <memory>
+#include <list>
 
 #include "factor_kernels.cuh"
 #include "solve_kernels.cuh"
@@ -16,6 +19,55 @@ void cuda_check(cudaError_t e, const char* what) {
 }
 
 namespace {
+
+// Process-wide cache of nested-dissection analyses keyed by the union pattern and the ordering
+// seed (a hit is confirmed by comparing the whole pattern): repeated solves on one sparsity
+// pattern (new values, new shifts, new Bloch wavevectors) skip the ordering and the symbolic
+// factorization. It holds the analysis as computed, before any delayed-pivot re-plan.
+struct AnalysisEntry {
+  std::uint64_t key;
+  std::uint64_t seed;
+  std::vector<std::int64_t> rp;
+  std::vector<std::int32_t> ci;
+  std::shared_ptr<const Symbolic> sym;
+};
+
+constexpr std::size_t kAnalysisCacheEntries = 8;
+std::mutex g_analysis_mu;
+std::list<AnalysisEntry> g_analysis_cache;  // most recently used first
+
+std::uint64_t pattern_key(const std::vector<std::int64_t>& rp, const std::vector<std::int32_t>& ci, std::uint64_t seed) {
+  std::uint64_t h = 0xcbf29ce484222325ull ^ seed;
+  auto mix = [&](std::uint64_t v) {
+    h ^= v + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
+  };
+  mix(rp.size());
+  for (std::int64_t v : rp) mix(static_cast<std::uint64_t>(v));
+  for (std::int32_t v : ci) mix(static_cast<std::uint32_t>(v));
+  return h;
+}
+
+Symbolic cached_analysis(std::int64_t n, const std::vector<std::int64_t>& rp, const std::vector<std::int32_t>& ci,
+                         const SymbolicOptions& so) {
+  const std::uint64_t key = pattern_key(rp, ci, so.ordering.seed);
+  {
+    std::lock_guard<std::mutex> lk(g_analysis_mu);
+    for (auto it = g_analysis_cache.begin(); it != g_analysis_cache.end(); ++it) {
+      if (it->key == key && it->seed == so.ordering.seed && it->rp == rp && it->ci == ci) {
+        g_analysis_cache.splice(g_analysis_cache.begin(), g_analysis_cache, it);
+        Symbolic s = *g_analysis_cache.front().sym;
+        s.ordering_seconds = 0.0;
+        s.symbolic_seconds = 0.0;
+        return s;
+      }
+    }
+  }
+  Symbolic s = analyze_pattern(n, rp.data(), ci.data(), nullptr, so);
+  std::lock_guard<std::mutex> lk(g_analysis_mu);
+  g_analysis_cache.push_front(AnalysisEntry{key, so.ordering.seed, rp, ci, std::make_shared<const Symbolic>(s)});
+  if (g_analysis_cache.size() > kAnalysisCacheEntries) g_analysis_cache.pop_back();
+  return s;
+}
 
 struct DeviceGuard {
   int prev = -1;
@@ -119,7 +171,11 @@ void GpuFactor::analyze(std::int64_t n, const std::int64_t* a_rp, const std::int
   }
   SymbolicOptions so;
   so.ordering.seed = opt_.ordering_seed;
-  sym_ = analyze_pattern(n, rp_.data(), ci_.data(), order ? perm.data() : nullptr, so);
+  if (order) {
+    sym_ = analyze_pattern(n, rp_.data(), ci_.data(), perm.data(), so);
+  } else {
+    sym_ = cached_analysis(n, rp_, ci_, so);
+  }
   row_.resize(nnz_);
   for (std::int64_t i = 0; i < n; ++i)
     for (std::int64_t p = rp_[i]; p < rp_[i + 1]; ++p) row_[p] = static_cast<std::int32_t>(i);

@@ -158,3 +158,21 @@ def test_complex_dtype_with_real_values_returns_complex_vectors():
     res = hsolve.solve(a.astype(np.complex128), sigma=30.0, k=4)
     _check_pairs(res)
     assert res.eigenvectors.dtype == np.complex128 and not res.report["complex_scalars"]
+
+
+def test_repeated_pattern_reuses_analysis_with_new_values():
+    """Solves on one sparsity pattern reuse the cached nested-dissection analysis; new values on
+    that pattern (here 2A) still give the right certified eigenpairs."""
+    box = yee.Box((10, 9, 8))
+    a, _ = yee.pencil(box)
+    w = yee_exact.exact_spectrum(box.cells)
+    cuts = yee_exact.mid_gap_shifts(w[w > 1.0], 10, 1e-6)
+    lo, hi = cuts[2], cuts[5]
+    r1 = hsolve.solve(a, lower=lo, upper=hi)
+    r2 = hsolve.solve(2.0 * a, lower=2.0 * lo, upper=2.0 * hi)
+    _check_pairs(r1)
+    _check_pairs(r2)
+    want = w[(w >= lo) & (w <= hi)]
+    np.testing.assert_allclose(r1.eigenvalues, want, rtol=EIG_RTOL)
+    np.testing.assert_allclose(r2.eigenvalues, 2.0 * want, rtol=EIG_RTOL)
+    assert r2.report["factor_stats"]["ordering_s"] == 0.0  # the second call found the analysis cached
