@@ -409,10 +409,10 @@ __device__ int block_bk(double* F, int w, bool root, double u, double thr, int* 
   return st.j;
 }
 
+// Warp maximum of non-negative floats: their bit patterns order like the values, so one integer
+// warp reduction replaces a shuffle tree.
 __device__ __forceinline__ float warp_maxf(float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
+  return __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(v)));
 }
 
 // One warp: threshold Bunch-Kaufman on the panel's diagonal block (order w <= 32, shared memory,
@@ -551,6 +551,7 @@ __device__ int warp_block_bk_fast(double* F, int w, bool root, double u, double 
   const int lane = threadIdx.x & 31;
   constexpr int ld = kNB;
   if (w != kNB || root) return warp_block_bk(F, w, root, u, thr, lab, pv, st);
+  __shared__ __align__(16) double s_col[kNB];
   double r[kNB];
 #pragma unroll
   for (int c = 0; c < kNB; ++c) r[c] = c <= lane ? F[lane + c * ld] : 0.0;
@@ -570,11 +571,22 @@ __device__ int warp_block_bk_fast(double* F, int w, bool root, double u, double 
       } else {
         const double inv = 1.0 / d;
         const double xs = x * inv;
-#pragma unroll
-        for (int c = j + 1; c < kNB; ++c) {
-          const double yc = __shfl_sync(0xffffffffu, r[j], c);  // F(c, j)
-          if (lane >= c) r[c] = fma(-xs, yc, r[c]);
+        // column j to shared memory once, then broadcast 16-byte reads of F(c, j), c > j
+        s_col[lane] = r[j];
+        __syncwarp();
+        int c0 = j + 1;
+        if (c0 & 1) {
+          if (lane >= c0) r[c0] = fma(-xs, s_col[c0], r[c0]);
+          ++c0;
         }
+#pragma unroll
+        for (int c = 0; c < kNB; c += 2) {
+          if (c < c0) continue;
+          const double2 y2 = *reinterpret_cast<const double2*>(&s_col[c]);
+          if (lane >= c) r[c] = fma(-xs, y2.x, r[c]);
+          if (lane >= c + 1) r[c + 1] = fma(-xs, y2.y, r[c + 1]);
+        }
+        __syncwarp();
         if (lane > j) r[j] = xs;
         if (d < 0) ++neg; else ++pos;
       }
