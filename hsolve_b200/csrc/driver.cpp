@@ -193,6 +193,8 @@ struct SliceRec {
   bool passed;
 };
 
+constexpr double kBatchFlopsMax = 5e11;  // per factorization
+
 struct Timers {
   double setup = 0, factor = 0, iterate = 0, verify = 0, cert = 0;
   double kry_apply = 0, kry_ortho = 0, kry_rr = 0, kry_restart = 0;  // phases of `iterate`
@@ -390,7 +392,9 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
   long long applies_before = 0;
   double sigma_used = cfg.sigma;
   const bool certify = cfg.certificate == 0;
-  const bool batch = cfg.batch_shifts != 0;
+  // concurrent shifts pay while a factorization is latency-bound; above kBatchFlopsMax flops the
+  // fronts keep the whole device busy and shifts run one after another
+  const bool batch = cfg.batch_shifts != 0 && F.estimate().flops <= kBatchFlopsMax;
   bool f_stale = false;  // F's factorization was overwritten by a count at another shift
 
   if (cfg.mode == 0) {
@@ -676,6 +680,7 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
   j.kv("time_iterate_s", tm.iterate);
   j.kv("time_verify_s", tm.verify);
   j.kv("time_certificate_s", tm.cert);
+  j.kv("batch_shifts", batch);
   j.key("iterate_split_s");
   j.open('{');
   j.kv("operator", tm.kry_apply);
