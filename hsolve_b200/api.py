@@ -39,6 +39,7 @@ _SOLVE_SIGS = {
     "hsg_session_create": (ctypes.c_int, [ctypes.c_int64, _P, _P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_uint64, _P]),
     "hsg_session_solve": (ctypes.c_int, [_P, _P, _P]),
     "hsg_session_free": (None, [_P]),
+    "hsg_session_estimate": (ctypes.c_int, [_P, _P]),
 }
 _native.SIGNATURES.update(_SOLVE_SIGS)
 
@@ -534,6 +535,13 @@ class Session:
         if self._complex:
             return _complex_result(w, v, report, self._complex[0], self._complex[1], cfg, self._da, self._db)
         return _finish(w, v, report, cfg, self._da, self._db, self._cdtype)
+
+    def estimate(self) -> dict:
+        """Analysis of the session's pencil (for a complex pencil, of its real 2n embedding): factor
+        entries, nnz(L), flops and device memory (MB) of one factorization object."""
+        e = _native._Estimate()
+        _native.check(_native.lib().hsg_session_estimate(self._h, ctypes.byref(e)))
+        return {f: getattr(e, f) for f, _ in _native._Estimate._fields_}
 
     def close(self):
         if getattr(self, "_h", None):

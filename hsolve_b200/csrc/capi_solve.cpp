@@ -96,6 +96,13 @@ int hsg_session_create(int64_t n, const int64_t* a_rowptr, const int32_t* a_col,
   });
 }
 
+int hsg_session_estimate(const hsg_session* s, hsg_estimate_t* out) {
+  return guarded([&] {
+    HSG_REQUIRE(s && s->impl && out, HSG_INVALID_INPUT, "hsg_session_estimate: null argument");
+    *out = s->impl->estimate();
+  });
+}
+
 int hsg_session_solve(hsg_session* s, const hsg_solve_config_t* cfg, hsg_solution** out) {
   return guarded([&] {
     HSG_REQUIRE(s && s->impl && out, HSG_INVALID_INPUT, "hsg_session_solve: null argument");

@@ -362,6 +362,8 @@ Session::~Session() = default;
 
 std::int64_t Session::order() const { return d_->a.n; }
 
+hsg_estimate_t Session::estimate() const { return d_->F->estimate(); }
+
 SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
   const auto t_start = Clock::now();
   Impl& S = *d_;

@@ -35,6 +35,7 @@ class Session {
   Session& operator=(const Session&) = delete;
   SolveOutput solve(const hsg_solve_config_t& cfg, bool include_setup = false);
   std::int64_t order() const;
+  hsg_estimate_t estimate() const;
 
  private:
   struct Impl;

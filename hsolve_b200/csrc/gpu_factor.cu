@@ -69,6 +69,20 @@ Symbolic cached_analysis(std::int64_t n, const std::vector<std::int64_t>& rp, co
   return s;
 }
 
+// A factorization that had to move delayed pivots to their parent fronts leaves its analysis with
+// those pivots moved; that structure is valid for any values on the pattern, so the cached entry
+// takes it and later analyses of the pattern start without those re-plans.
+void learn_delays(const std::vector<std::int64_t>& rp, const std::vector<std::int32_t>& ci, std::uint64_t seed,
+                  const Symbolic& sym) {
+  const std::uint64_t key = pattern_key(rp, ci, seed);
+  std::lock_guard<std::mutex> lk(g_analysis_mu);
+  for (auto& e : g_analysis_cache)
+    if (e.key == key && e.seed == seed && e.rp == rp && e.ci == ci) {
+      if (sym.delayed_moves > e.sym->delayed_moves) e.sym = std::make_shared<const Symbolic>(sym);
+      return;
+    }
+}
+
 struct DeviceGuard {
   int prev = -1;
   explicit DeviceGuard(int dev) {
@@ -176,6 +190,7 @@ void GpuFactor::analyze(std::int64_t n, const std::int64_t* a_rp, const std::int
   } else {
     sym_ = cached_analysis(n, rp_, ci_, so);
   }
+  cached_analysis_ = order == nullptr;
   row_.resize(nnz_);
   for (std::int64_t i = 0; i < n; ++i)
     for (std::int64_t p = rp_[i]; p < rp_[i + 1]; ++p) row_[p] = static_cast<std::int32_t>(i);
@@ -207,6 +222,7 @@ void GpuFactor::analyze_like(const GpuFactor& src) {
   ci_ = src.ci_;
   row_ = src.row_;
   sym_ = src.sym_;
+  cached_analysis_ = src.cached_analysis_;
   cuda_check(cudaStreamSynchronize(src.stream_), "analyze_like: source");
   d_row_.alloc(src.d_row_.n);
   d_col_.alloc(src.d_col_.n);
@@ -565,6 +581,7 @@ hsg_inertia_t GpuFactor::factorize(double alpha, double beta, bool detection, bo
   inertia_.two_by_two = static_cast<std::int64_t>(c.two_by_two);
   inertia_.delayed_pivots = sym_.delayed_moves;
   inertia_.replans = replans;
+  if (replans > 0 && cached_analysis_) learn_delays(rp_, ci_, opt_.ordering_seed, sym_);
   inertia_.valid = c.zero == 0 ? 1 : 0;
   factored_ = inertia_.valid != 0;
   last_factor_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -175,6 +175,7 @@ class GpuFactor {
   int solve_coop_max_ = 0;
   int coop_max_ = 0;
   bool shared_ = false;
+  bool cached_analysis_ = false;  // the analysis came from (and teaches) the pattern cache
   static constexpr int kSharedParts = 3;
   int ncoop_ = 0;
 };

@@ -1,0 +1,167 @@
+"""Request-stream serving of certified eigensolves on one GPU.
+
+    srv = Server(workers=3)
+    fut = srv.submit(A, B, lower=lo, upper=hi)      # returns at once; fut.result() -> SolveResult
+    ...
+    srv.close(); print(srv.stats())                 # throughput and p50 / p99 latency
+
+Requests of different sizes and shifts share the device: each runs in its own `Session` (its own
+CUDA streams and factorization objects) on one of `workers` host threads, so the GPU interleaves the
+latency-bound phases of several solves. A request is admitted only when its device memory (from
+the analysis of its pattern: factor storage of its factorization objects plus its Krylov basis)
+fits the memory budget next to the requests already running; a pattern not seen before runs alone
+the first time so that its footprint is known. Analyses are cached per sparsity pattern inside the
+library, so a family of requests on one mesh (new Bloch wavevectors, new shifts, new values) reuses
+one ordering and symbolic factorization. Latency is measured from submission (the request's
+arrival) to completion.
+"""
+from __future__ import annotations
+
+import threading
+import time
+from concurrent.futures import Future, ThreadPoolExecutor
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .api import Session
+
+
+@dataclass
+class RequestRecord:
+    n: int
+    arrival: float
+    start: float = 0.0
+    end: float = 0.0
+    device_mb: float = 0.0
+    success: bool = False
+    error: str = ""
+
+
+@dataclass
+class _Budget:
+    total_mb: float
+    used_mb: float = 0.0
+    exclusive: bool = False
+    active: int = 0
+    cond: threading.Condition = field(default_factory=threading.Condition)
+
+
+# device memory (MB) of a request, learned per (n, nnz(A), nnz(B), complex) the first time it runs
+_KNOWN_MB: dict[tuple, float] = {}
+
+
+def _free_device_mb(device: int) -> float:
+    import torch
+
+    free, _ = torch.cuda.mem_get_info(device)
+    return free / 1e6
+
+
+class Server:
+    """Admits certified eigensolve requests by device memory and runs up to `workers` of them at
+    once on `device` (see the module docstring)."""
+
+    def __init__(self, workers: int = 3, memory_budget_gb: float | None = None, device: int = 0,
+                 config: dict | None = None):
+        if workers < 1:
+            raise ValueError("workers must be >= 1")
+        self.device = device
+        self.config = dict(config or {})
+        total = memory_budget_gb * 1e3 if memory_budget_gb is not None else 0.8 * _free_device_mb(device)
+        self._budget = _Budget(total_mb=total)
+        self._pool = ThreadPoolExecutor(max_workers=workers, thread_name_prefix="hsolve-serve")
+        self._known_mb = _KNOWN_MB
+        self._records: list[RequestRecord] = []
+        self._lock = threading.Lock()
+
+    # ------------------------------------------------------------------------------ admission
+    def _acquire(self, key, rec: RequestRecord) -> bool:
+        """Blocks until the request fits; returns True when it runs alone (unknown footprint)."""
+        b = self._budget
+        with b.cond:
+            known = self._known_mb.get(key)
+            if known is None:
+                b.cond.wait_for(lambda: b.active == 0)
+                b.exclusive = True
+                b.active += 1
+                return True
+            need = min(known, b.total_mb)
+            b.cond.wait_for(lambda: not b.exclusive and b.used_mb + need <= b.total_mb)
+            b.used_mb += need
+            b.active += 1
+            rec.device_mb = need
+            return False
+
+    def _release(self, alone: bool, rec: RequestRecord) -> None:
+        b = self._budget
+        with b.cond:
+            if alone:
+                b.exclusive = False
+            else:
+                b.used_mb -= rec.device_mb
+            b.active -= 1
+            b.cond.notify_all()
+
+    # ------------------------------------------------------------------------------ requests
+    def submit(self, A, B=None, **target) -> Future:
+        """Queue one solve (target keywords as in `hsolve_b200.solve`: sigma/k, lower/upper, tol,
+        config); the future's result is the SolveResult."""
+        rec = RequestRecord(n=A.shape[0], arrival=time.perf_counter())
+        with self._lock:
+            self._records.append(rec)
+        return self._pool.submit(self._run, A, B, target, rec)
+
+    def _run(self, A, B, target, rec: RequestRecord):
+        key = (A.shape[0], getattr(A, "nnz", None), None if B is None else getattr(B, "nnz", None),
+               bool(np.iscomplexobj(getattr(A, "data", np.zeros(0)))))
+        alone = self._acquire(key, rec)
+        rec.start = time.perf_counter()
+        try:
+            sess = Session(A, B, device=self.device)
+            try:
+                if alone:
+                    est = sess.estimate()
+                    # factor storage of up to three factorization objects plus the Krylov basis
+                    basis_mb = 8.0 * 2 * sess.n * 160 / 1e6
+                    rec.device_mb = 3.0 * est["device_mb"] + basis_mb
+                    with self._budget.cond:
+                        self._known_mb[key] = rec.device_mb
+                cfg = dict(self.config)
+                cfg.update(target.pop("config", None) or {})
+                res = sess.solve(config=cfg, **target)
+            finally:
+                sess.close()
+            rec.success = bool(res.success and res.report.get("certificate", {}).get("passed", True))
+            return res
+        except Exception as e:  # recorded, then re-raised through the future
+            rec.error = f"{type(e).__name__}: {e}"
+            raise
+        finally:
+            rec.end = time.perf_counter()
+            self._release(alone, rec)
+
+    def close(self, wait: bool = True) -> None:
+        self._pool.shutdown(wait=wait)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------------------------ metrics
+    def stats(self) -> dict:
+        """Throughput of certified solves and latency percentiles of the completed requests."""
+        with self._lock:
+            done = [r for r in self._records if r.end > 0]
+        if not done:
+            return {"requests": 0}
+        lat = np.array([r.end - r.arrival for r in done])
+        service = np.array([r.end - r.start for r in done])
+        span = max(r.end for r in done) - min(r.arrival for r in done)
+        ok = sum(r.success for r in done)
+        return {"requests": len(done), "certified": ok, "failed": [r.error for r in done if r.error],
+                "solves_per_s": ok / span if span > 0 else 0.0, "makespan_s": span,
+                "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+                "service_mean_s": float(service.mean())}

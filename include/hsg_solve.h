@@ -62,6 +62,9 @@ HSG_API int hsg_session_create(int64_t n, const int64_t* a_rowptr, const int32_t
                                uint64_t seed, hsg_session** out);
 HSG_API int hsg_session_solve(hsg_session* s, const hsg_solve_config_t* cfg, hsg_solution** out);
 HSG_API void hsg_session_free(hsg_session* s);
+/* The analysis of the session's pencil: factor entries, nnz(L), flops and device memory of one
+ * factorization object (a session holds one, or three while it batches shifts). */
+HSG_API int hsg_session_estimate(const hsg_session* s, hsg_estimate_t* out);
 
 /* Solution<double>::eigenvalues.size() and n. */
 HSG_API int hsg_solution_sizes(const hsg_solution* s, int64_t* n, int64_t* m);

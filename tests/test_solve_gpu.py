@@ -176,3 +176,27 @@ def test_repeated_pattern_reuses_analysis_with_new_values():
     np.testing.assert_allclose(r1.eigenvalues, want, rtol=EIG_RTOL)
     np.testing.assert_allclose(r2.eigenvalues, 2.0 * want, rtol=EIG_RTOL)
     assert r2.report["factor_stats"]["ordering_s"] == 0.0  # the second call found the analysis cached
+
+
+def test_server_runs_mixed_requests_concurrently():
+    """The request-stream server: real and complex pencils of different sizes, admitted by device
+    memory and solved concurrently, each certified and equal to its exact spectrum."""
+    from hsolve_b200.serve import Server
+
+    cases = []
+    for cells, boundary, phases in [((8, 7, 6), "pec", (0.0, 0.0, 0.0)), ((7, 6, 6), "bloch", (0.9, 0.4, 0.2)),
+                                    ((9, 8, 7), "pec", (0.0, 0.0, 0.0)), ((7, 6, 6), "bloch", (1.3, 0.7, 0.1))]:
+        box = yee.Box(cells, (1.0, 0.9, 0.8), boundary, phases)
+        a, b = yee.pencil(box, "generalized")
+        w = yee_exact.exact_spectrum(box.cells, box.lengths, boundary, box.phases)
+        cuts = yee_exact.mid_gap_shifts(w[w > 1.0], 8, 1e-6)
+        cases.append((a, b, cuts[1], cuts[6], w))
+    with Server(workers=2) as srv:
+        futs = [srv.submit(a, b, lower=lo, upper=hi) for a, b, lo, hi, _ in cases]
+        results = [f.result() for f in futs]
+    for (a, b, lo, hi, w), res in zip(cases, results):
+        _check_pairs(res)
+        np.testing.assert_allclose(res.eigenvalues, w[(w >= lo) & (w <= hi)], rtol=EIG_RTOL)
+    st = srv.stats()
+    assert st["requests"] == 4 and st["certified"] == 4 and not st["failed"]
+    assert st["latency_p99_s"] >= st["latency_p50_s"] > 0
