@@ -142,6 +142,18 @@ def captured_traffic(workload):
     return None, None
 
 
+def reduce_over_ranks(dist, times, counts, device):
+    """Cross-rank aggregation of a replicated run: the max over ranks of each time (the job ends
+    with its slowest rank) and the sum over ranks of each count (solves completed by all ranks)."""
+    import torch
+
+    tv = torch.tensor(list(times) + [0.0], device=device, dtype=torch.float64)
+    cv = torch.tensor(list(counts) + [0.0], device=device, dtype=torch.float64)
+    dist.all_reduce(tv, op=dist.ReduceOp.MAX)
+    dist.all_reduce(cv, op=dist.ReduceOp.SUM)
+    return [float(x) for x in tv[:-1]], [float(x) for x in cv[:-1]]
+
+
 def run_ours(args, w, rank, world, local):
     import torch
 
@@ -230,13 +242,8 @@ def run_ours(args, w, rank, world, local):
         d2h = int(r2.eigenvectors.nbytes + r2.eigenvalues.nbytes)
     e2e_t = float(np.sum(e2e_lat))
     if dist is not None:
-        vals = torch.tensor([t, e2e_t, float(ok), plain_t], device="cuda", dtype=torch.float64)
-        tmax = vals.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = vals.clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        t, e2e_t, plain_t = float(tmax[0]), float(tmax[1]), float(tmax[3])
-        ok_total = int(tsum[2])
+        (t, e2e_t, plain_t), (ok_total,) = reduce_over_ranks(dist, [t, e2e_t, plain_t], [ok], "cuda")
+        ok_total = int(ok_total)
         dist.barrier()
         dist.destroy_process_group()
     else:
@@ -448,9 +455,7 @@ def run_serving(args, w, rank, world, local):
         import torch.distributed as dist
 
         dist.init_process_group("nccl")
-        v = torch.tensor([value], device="cuda", dtype=torch.float64)
-        dist.all_reduce(v, op=dist.ReduceOp.SUM)
-        value = float(v[0])
+        _, (value,) = reduce_over_ranks(dist, [], [value], "cuda")
         dist.destroy_process_group()
     if rank != 0:
         return None
