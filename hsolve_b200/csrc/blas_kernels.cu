@@ -139,6 +139,29 @@ __global__ void k_copy_cols(std::int64_t n, int p, const double* x, std::int64_t
   }
 }
 
+// Standard normal entries y(i, c) from a counter-based stream: a SplitMix64 hash of (seed, element
+// index) gives two uniforms, Box-Muller turns them into one normal deviate. Deterministic in the
+// seed and independent of the launch shape.
+__device__ __forceinline__ std::uint64_t splitmix64(std::uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void k_fill_normal(std::int64_t n, int p, double* y, std::int64_t ldy, std::uint64_t seed) {
+  const std::int64_t total = n * p;
+  for (std::int64_t t = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
+    const std::uint64_t h1 = splitmix64(seed ^ (static_cast<std::uint64_t>(t) * 2 + 1));
+    const std::uint64_t h2 = splitmix64(h1 ^ 0xD1B54A32D192ED03ull);
+    const double u1 = (static_cast<double>(h1 >> 11) + 0.5) * 0x1.0p-53;  // (0, 1)
+    const double u2 = static_cast<double>(h2 >> 11) * 0x1.0p-53;          // [0, 1)
+    const std::int64_t i = t % n, c = t / n;
+    y[i + c * ldy] = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+  }
+}
+
 // r = a - lam .* b (column c uses lam[c]); y holds r
 __global__ void k_residual_cols(std::int64_t n, int p, const double* ax, std::int64_t lda, const double* bx,
                                 std::int64_t ldb, const double* lam, double* r, std::int64_t ldr) {
@@ -266,6 +289,11 @@ void diag_scale(std::int64_t n, int p, const double* d, const double* x, std::in
 void copy_cols(std::int64_t n, int p, const double* x, std::int64_t ldx, double* y, std::int64_t ldy, cudaStream_t s) {
   note_launches(1);
   k_copy_cols<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, x, ldx, y, ldy);
+}
+
+void fill_normal(std::int64_t n, int p, double* y, std::int64_t ldy, std::uint64_t seed, cudaStream_t s) {
+  note_launches(1);
+  k_fill_normal<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, y, ldy, seed);
 }
 
 void residual_cols(std::int64_t n, int p, const double* ax, std::int64_t lda, const double* bx, std::int64_t ldb,

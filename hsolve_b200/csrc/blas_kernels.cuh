@@ -33,6 +33,8 @@ void scale_cols(std::int64_t n, int p, double a, double* y, std::int64_t ldy, cu
 void diag_scale(std::int64_t n, int p, const double* d, const double* x, std::int64_t ldx, double* y,
                 std::int64_t ldy, cudaStream_t s);
 void copy_cols(std::int64_t n, int p, const double* x, std::int64_t ldx, double* y, std::int64_t ldy, cudaStream_t s);
+// standard normal entries from a counter-based stream (deterministic in seed)
+void fill_normal(std::int64_t n, int p, double* y, std::int64_t ldy, std::uint64_t seed, cudaStream_t s);
 void residual_cols(std::int64_t n, int p, const double* ax, std::int64_t lda, const double* bx, std::int64_t ldb,
                    const double* lam, double* r, std::int64_t ldr, cudaStream_t s);
 

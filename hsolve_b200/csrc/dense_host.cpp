@@ -21,7 +21,7 @@ void tridiagonalize(int n, std::vector<double>& a, std::vector<double>& d, std::
   std::vector<double> q(static_cast<std::size_t>(n) * n, 0.0);
   auto Q = [&](int i, int j) -> double& { return q[static_cast<std::size_t>(i) + static_cast<std::size_t>(j) * n]; };
   for (int i = 0; i < n; ++i) Q(i, i) = 1.0;
-  std::vector<double> v(n), pv(n), wv(n);
+  std::vector<double> v(n), pv(n), wv(n), uq(n);
   d.assign(n, 0.0);
   e.assign(n, 0.0);
   for (int k = 0; k + 2 < n; ++k) {
@@ -38,10 +38,12 @@ void tridiagonalize(int n, std::vector<double>& a, std::vector<double>& d, std::
     for (int i = k + 1; i < n; ++i) vnorm2 += v[i] * v[i];
     if (vnorm2 == 0.0) continue;
     const double beta = 2.0 / vnorm2;
-    // p = beta * A v (trailing block), K = beta/2 v^T p, w = p - K v
+    // p = beta * A v (trailing block; A symmetric, so column i gives row i contiguously),
+    // K = beta/2 v^T p, w = p - K v
     for (int i = k + 1; i < n; ++i) {
+      const double* ai = &A(0, i);
       double sum = 0.0;
-      for (int j = k + 1; j < n; ++j) sum += A(i, j) * v[j];
+      for (int j = k + 1; j < n; ++j) sum += ai[j] * v[j];
       pv[i] = beta * sum;
     }
     double kk = 0.0;
@@ -53,12 +55,17 @@ void tridiagonalize(int n, std::vector<double>& a, std::vector<double>& d, std::
     A(k + 1, k) = s;
     A(k, k + 1) = s;
     for (int i = k + 2; i < n; ++i) { A(i, k) = 0.0; A(k, i) = 0.0; }
-    // Q = Q H, H = I - beta v v^T
-    for (int i = 0; i < n; ++i) {
-      double sum = 0.0;
-      for (int j = k + 1; j < n; ++j) sum += Q(i, j) * v[j];
-      sum *= beta;
-      for (int j = k + 1; j < n; ++j) Q(i, j) -= sum * v[j];
+    // Q = Q H, H = I - beta v v^T: u = Q v by columns, then Q -= beta u v^T by columns
+    std::fill(uq.begin(), uq.end(), 0.0);
+    for (int j = k + 1; j < n; ++j) {
+      const double vj = v[j];
+      const double* qj = &Q(0, j);
+      for (int i = 0; i < n; ++i) uq[i] += qj[i] * vj;
+    }
+    for (int j = k + 1; j < n; ++j) {
+      const double c = beta * v[j];
+      double* qj = &Q(0, j);
+      for (int i = 0; i < n; ++i) qj[i] -= uq[i] * c;
     }
   }
   for (int i = 0; i < n; ++i) d[i] = A(i, i);

@@ -88,11 +88,7 @@ std::vector<double> normalize(Basis& B, KrylovOperator& op, int j, int p, cudaSt
 }
 
 void random_block(Basis& B, int j, int p, std::mt19937_64& rng, cudaStream_t s) {
-  std::normal_distribution<double> nd;
-  std::vector<double> h(static_cast<std::size_t>(B.n) * p);
-  for (auto& x : h) x = nd(rng);
-  to_dev(B.v(j), h, s);
-  cuda_check(cudaStreamSynchronize(s), "random block");
+  fill_normal(B.n, p, B.v(j), B.n, rng(), s);
 }
 
 // New block [j, j+p) made orthonormal to [0, j); breakdown columns replaced by random ones.
