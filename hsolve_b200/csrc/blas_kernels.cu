@@ -79,12 +79,24 @@ __global__ void k_gram_partial(std::int64_t n, int m, int p, const double* x, st
   }
 }
 
-// Fixed-order sum of the partials: g[t] = sum_b part[b][t]
-__global__ void k_gram_reduce(int nparts, int mp, const double* part, double* g) {
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mp; t += gridDim.x * blockDim.x) {
-    double s = 0.0;
-    for (int b = 0; b < nparts; ++b) s += part[static_cast<std::int64_t>(b) * mp + t];
-    g[t] = s;
+// Fixed-order sum of the partials: g[t] = sum_b part[b][t]. A block takes 32 consecutive outputs;
+// its 8 thread rows stride over the partials (reads coalesced over the outputs) and their 8 sums are
+// added in shared memory in row order, so the result does not depend on the launch.
+constexpr int kReduceRows = 8;
+__global__ void __launch_bounds__(32 * kReduceRows) k_gram_reduce(int nparts, int mp, const double* part, double* g) {
+  __shared__ double acc[kReduceRows][33];
+  const int tl = threadIdx.x & 31, row = threadIdx.x >> 5;
+  const int t = blockIdx.x * 32 + tl;
+  double s = 0.0;
+  if (t < mp)
+    for (int b = row; b < nparts; b += kReduceRows) s += part[static_cast<std::int64_t>(b) * mp + t];
+  acc[row][tl] = s;
+  __syncthreads();
+  if (row == 0 && t < mp) {
+    double v = 0.0;
+#pragma unroll
+    for (int r = 0; r < kReduceRows; ++r) v += acc[r][tl];
+    g[t] = v;
   }
 }
 
@@ -239,7 +251,8 @@ void gram(std::int64_t n, int m, int p, const double* x, std::int64_t ldx, const
     note_launches(1);
     k_gram_partial<<<static_cast<int>(nparts), 256, smem, s>>>(n, m, pc, x, ldx, y + c0 * ldy, ldy, chunk, part);
     note_launches(1);
-    k_gram_reduce<<<grid_for(m * pc, 256), 256, 0, s>>>(static_cast<int>(nparts), m * pc, part, g + static_cast<std::int64_t>(c0) * m);
+    k_gram_reduce<<<(m * pc + 31) / 32, 32 * kReduceRows, 0, s>>>(static_cast<int>(nparts), m * pc, part,
+                                                               g + static_cast<std::int64_t>(c0) * m);
   }
 }
 
