@@ -101,29 +101,33 @@ __global__ void __launch_bounds__(32 * kReduceRows) k_gram_reduce(int nparts, in
 }
 
 // Y[:, c0:c0+q] = beta Y + alpha X S[:, c0:c0+q] (X n x m, S m x q in shared memory), 16 columns a pass.
+// y (n x q) = alpha X S + beta y: one thread per row, S staged in shared memory QC columns at a time
+// (QC = 8 for the Krylov block width, 16 for wider products).
+template <int QC>
 __global__ void k_gemm_tall(std::int64_t n, int m, int q, const double* x, std::int64_t ldx, const double* s, int lds,
                             double* y, std::int64_t ldy, double alpha, double beta) {
-  extern __shared__ double ss[];  // m x 16
-  for (int c0 = 0; c0 < q; c0 += 16) {
-    const int qc = q - c0 < 16 ? q - c0 : 16;
+  extern __shared__ double ss[];  // m x QC
+  for (int c0 = 0; c0 < q; c0 += QC) {
+    const int qc = q - c0 < QC ? q - c0 : QC;
     __syncthreads();
-    for (int t = threadIdx.x; t < m * 16; t += blockDim.x) {
+    for (int t = threadIdx.x; t < m * QC; t += blockDim.x) {
       const int i = t % m, c = t / m;
       ss[c * m + i] = c < qc ? s[i + static_cast<std::int64_t>(c0 + c) * lds] : 0.0;
     }
     __syncthreads();
     for (std::int64_t row = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; row < n;
          row += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
-      double acc[16];
+      double acc[QC];
 #pragma unroll
-      for (int c = 0; c < 16; ++c) acc[c] = 0.0;
+      for (int c = 0; c < QC; ++c) acc[c] = 0.0;
+#pragma unroll 4
       for (int i = 0; i < m; ++i) {
         const double xv = x[row + static_cast<std::int64_t>(i) * ldx];
 #pragma unroll
-        for (int c = 0; c < 16; ++c) acc[c] += xv * ss[c * m + i];
+        for (int c = 0; c < QC; ++c) acc[c] += xv * ss[c * m + i];
       }
 #pragma unroll
-      for (int c = 0; c < 16; ++c) {
+      for (int c = 0; c < QC; ++c) {
         if (c >= qc) break;
         double* yp = y + row + static_cast<std::int64_t>(c0 + c) * ldy;
         *yp = alpha * acc[c] + (beta == 0.0 ? 0.0 : beta * *yp);
@@ -263,13 +267,19 @@ void gemm_tall(std::int64_t n, int m, int q, const double* x, std::int64_t ldx, 
     if (beta != 1.0) { note_launches(1); k_scale_cols<<<grid_for(n * q, 256), 256, 0, s>>>(n, q, beta, y, ldy); }
     return;
   }
-  const std::size_t smem = static_cast<std::size_t>(m) * 16 * sizeof(double);
   static std::once_flag configured;
   std::call_once(configured, [&] {
-    cudaFuncSetAttribute(k_gemm_tall, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_gemm_tall<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_gemm_tall<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   });
   note_launches(1);
-  k_gemm_tall<<<grid_for(n, 256), 256, smem, s>>>(n, m, q, x, ldx, sdev, lds, y, ldy, alpha, beta);
+  if (q <= 8) {
+    const std::size_t smem = static_cast<std::size_t>(m) * 8 * sizeof(double);
+    k_gemm_tall<8><<<grid_for(n, 256), 256, smem, s>>>(n, m, q, x, ldx, sdev, lds, y, ldy, alpha, beta);
+  } else {
+    const std::size_t smem = static_cast<std::size_t>(m) * 16 * sizeof(double);
+    k_gemm_tall<16><<<grid_for(n, 256), 256, smem, s>>>(n, m, q, x, ldx, sdev, lds, y, ldy, alpha, beta);
+  }
 }
 
 std::int64_t gram_part_size(std::int64_t n, int m, int p) {
