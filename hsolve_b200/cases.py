@@ -9,7 +9,8 @@ runs `repeat` in-place solves of `nrhs` device-resident right-hand sides; `eigs`
 solve of the case's target through a session `repeat` times. Each prints its wall times (and, for
 `eigs`, the phase split of the solve report). The cases are the workloads of bench.py: box1e5 is
 the PEC box 44 x 34 x 26 (lengths 1 x 0.75 x 0.55, generalized form, n = 109,744, all eigenvalues in
-[40, 200]); cube20 is the PEC cube 20^3 (standard form, n = 21,660, 10 nearest to 25).
+[40, 200]); cube20 is the PEC cube 20^3 (standard form, n = 21,660, 10 nearest to 25); cube70 is the
+PEC cube 70^3 (n = 999,810, 21 nearest to 1071.43, between two exact levels).
 """
 from __future__ import annotations
 
@@ -23,6 +24,8 @@ from .gen import yee
 CASES = {
     "box1e5": (yee.BOX_1E5, "generalized", dict(lower=40.0, upper=200.0)),
     "cube20": (yee.CUBE20, "standard", dict(sigma=25.0, k=10)),
+    # PEC cube 70^3, n = 999,810: 21 nearest to a shift midway between two exact levels
+    "cube70": (yee.Box((70, 70, 70)), "standard", dict(sigma=1071.4257927949998, k=21)),
 }
 
 

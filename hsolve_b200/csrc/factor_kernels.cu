@@ -1086,6 +1086,17 @@ __device__ void app_restore(AppFront& F, int rank, int nr, int q) {
 // All ranks: C(i, c) -= sum_{s<q} L(i, p+s) W(c, s), from <= c <= i < m, W = L D (from scratch);
 // 64 x 64 tiles of the lower triangle dealt round-robin to the ranks; 4 x 4 outputs per thread, the
 // C values loaded before the products so that their latencies overlap.
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
+// Trailing update C -= L W^T of the lower 64 x 64 tiles on the FP64 tensor cores (mma.sync m8n8k4,
+// D = A B + C with A 8 x 4, B 4 x 8): the tile's q <= 32 columns of L (rows of the tile) and of W
+// (rows of the tile's columns) are staged row-major with stride kUpdK, so every fragment read of a
+// half-warp hits 32 distinct banks; warp w (of 8) computes rows 16 (w % 4) .. +16 and columns
+// 32 (w / 4) .. +32 of the tile as 2 x 4 blocks of 8 x 8. A thread's fragment element (g, t) is
+// row g = lane / 4, column t = lane % 4 of A; row t, column g of B; row g, columns 2t, 2t + 1 of C.
 __device__ void app_update(AppFront& F, int rank, int nr, int q, double* Ls, double* Ws) {
   const AppCtrl* c = F.ctrl;
   const int p = c->p, from = p + q, m = F.f.m;
@@ -1093,7 +1104,10 @@ __device__ void app_update(AppFront& F, int rank, int nr, int q, double* Ls, dou
   if (rows <= 0 || q <= 0) return;
   const int nt = (rows + kTile - 1) / kTile;
   const int ntiles = nt * (nt + 1) / 2;
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int rbase = (warp & 3) * 16, cbase = (warp >> 2) * 32;
+  const int qpad = (q + 3) & ~3;
   for (int tile = rank; tile < ntiles; tile += nr) {
     int ti = static_cast<int>((sqrt(8.0 * tile + 1.0) - 1.0) * 0.5);
     while ((ti + 1) * (ti + 2) / 2 <= tile) ++ti;
@@ -1101,50 +1115,55 @@ __device__ void app_update(AppFront& F, int rank, int nr, int q, double* Ls, dou
     const int tj = tile - ti * (ti + 1) / 2;
     const int i0 = from + ti * kTile, j0 = from + tj * kTile;
     __syncthreads();
-    for (int t = threadIdx.x; t < q * kTile; t += blockDim.x) {
+    for (int t = threadIdx.x; t < qpad * kTile; t += blockDim.x) {
       const int s = t / kTile, r = t % kTile;
       const int i = i0 + r, cc = j0 + r;
-      Ls[s * kTile + r] = i < m ? F.f.at(i, p + s) : 0.0;
-      Ws[s * kTile + r] = cc < m ? F.W[static_cast<std::int64_t>(s) * m + cc] : 0.0;
+      Ls[r * kUpdK + s] = (s < q && i < m) ? F.f.at(i, p + s) : 0.0;
+      Ws[r * kUpdK + s] = (s < q && cc < m) ? F.W[static_cast<std::int64_t>(s) * m + cc] : 0.0;
     }
-    double* colp[4];
-    double cv[4][4];
+    // prefetch this thread's C entries (rows rbase + 8a + g, columns cbase + 8b + 2 t4 + e)
+    double* colp[4][2];
+    double cv[2][4][2];
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int cc = j0 + ty + 16 * b;
-      colp[b] = cc < m ? F.f.col(cc) : nullptr;
+    for (int b = 0; b < 4; ++b)
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const int i = i0 + tx + 16 * a;
-        cv[a][b] = (colp[b] && i < m && cc <= i) ? colp[b][i] : 0.0;
+      for (int e = 0; e < 2; ++e) {
+        const int cc = j0 + cbase + 8 * b + 2 * t4 + e;
+        colp[b][e] = cc < m ? F.f.col(cc) : nullptr;
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+          const int i = i0 + rbase + 8 * a + g;
+          cv[a][b][e] = (colp[b][e] && i < m && cc <= i) ? colp[b][e][i] : 0.0;
+        }
       }
-    }
     __syncthreads();
-    double acc[4][4];
+    double acc[2][4][2];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-    for (int s = 0; s < q; ++s) {
-      double l[4], wv[4];
+      for (int b = 0; b < 4; ++b) { acc[a][b][0] = 0.0; acc[a][b][1] = 0.0; }
+    for (int s0 = 0; s0 < qpad; s0 += 4) {
+      double af[2], bf[4];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) l[a] = Ls[s * kTile + tx + 16 * a];
+      for (int a = 0; a < 2; ++a) af[a] = Ls[(rbase + 8 * a + g) * kUpdK + s0 + t4];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) wv[b] = Ws[s * kTile + ty + 16 * b];
+      for (int b = 0; b < 4; ++b) bf[b] = Ws[(cbase + 8 * b + g) * kUpdK + s0 + t4];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < 2; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(l[a], wv[b], acc[a][b]);
+        for (int b = 0; b < 4; ++b) dmma_m8n8k4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
     }
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int cc = j0 + ty + 16 * b;
+    for (int b = 0; b < 4; ++b)
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const int i = i0 + tx + 16 * a;
-        if (colp[b] && i < m && cc <= i) colp[b][i] = cv[a][b] - acc[a][b];
+      for (int e = 0; e < 2; ++e) {
+        const int cc = j0 + cbase + 8 * b + 2 * t4 + e;
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+          const int i = i0 + rbase + 8 * a + g;
+          if (colp[b][e] && i < m && cc <= i) colp[b][e][i] = cv[a][b][e] - acc[a][b][e];
+        }
       }
-    }
   }
 }
 
@@ -1188,7 +1207,7 @@ __global__ void __launch_bounds__(kAppThreads) k_front_app(const std::int32_t* l
                                                            FactorCounters* cnt, std::int32_t* failed) {
   extern __shared__ double app_dyn[];
   double* Ls = app_dyn;
-  double* Ws = app_dyn + kNB * kTile;
+  double* Ws = app_dyn + kTile * kUpdK;
   __shared__ AppSmem sm;
   const SnDev d = sn[list[blockIdx.x]];
   AppFront F = make_front(d, panels, cb, scratch, piv_out, pidx_out);
@@ -1225,7 +1244,7 @@ __global__ void __launch_bounds__(kAppThreads) k_front_coop(const std::int32_t* 
   cg::grid_group grid = cg::this_grid();
   extern __shared__ double app_dyn[];
   double* Ls = app_dyn;
-  double* Ws = app_dyn + kNB * kTile;
+  double* Ws = app_dyn + kTile * kUpdK;
   __shared__ AppSmem sm;
   int fi = 0;
   while (fi + 1 < nfronts && cta_start[fi + 1] <= static_cast<int>(blockIdx.x)) ++fi;
@@ -1324,7 +1343,7 @@ void launch_front_app(const std::int32_t* list, int nlist, const SnDev* sn, doub
                       double* scratch, signed char* piv, std::int32_t* pidx, const FactorParams& prm,
                       FactorCounters* cnt, std::int32_t* failed, cudaStream_t s) {
   if (nlist <= 0) return;
-  constexpr std::size_t smem = 2 * kNB * kTile * sizeof(double);
+  constexpr std::size_t smem = kAppDynDoubles * sizeof(double);
   static std::once_flag configured;
   std::call_once(configured, [&] {
     cudaFuncSetAttribute(k_front_app, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
@@ -1334,7 +1353,7 @@ void launch_front_app(const std::int32_t* list, int nlist, const SnDev* sn, doub
 }
 
 int coop_max_ctas(int device) {
-  constexpr std::size_t smem = 2 * kNB * kTile * sizeof(double);
+  constexpr std::size_t smem = kAppDynDoubles * sizeof(double);
   cudaFuncSetAttribute(k_front_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   int per_sm = 0, sms = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_front_coop, kAppThreads, smem);
@@ -1347,7 +1366,7 @@ cudaError_t launch_front_coop(const std::int32_t* list, const std::int32_t* cta_
                               std::int32_t* pidx, const FactorParams& prm, FactorCounters* cnt, std::int32_t* failed,
                               int* level_done, cudaStream_t s) {
   if (nfronts <= 0) return cudaSuccess;
-  constexpr std::size_t smem = 2 * kNB * kTile * sizeof(double);
+  constexpr std::size_t smem = kAppDynDoubles * sizeof(double);
   FactorParams p = prm;
   void* args[] = {const_cast<std::int32_t**>(&list), const_cast<std::int32_t**>(&cta_start), &nfronts,
                   const_cast<SnDev**>(&sn), &panels, &cb, &scratch, &piv, &pidx, &p, &cnt, &failed, &level_done};

@@ -11,6 +11,8 @@ namespace hsg {
 constexpr int kSmallMax = 64;          // fronts up to this order are factorized in shared memory
 constexpr int kNB = 32;                // panel width of the a-posteriori pivoting kernel
 constexpr int kTile = 64;              // trailing-update tile (rows = cols)
+constexpr int kUpdK = kNB + 4;         // row stride of the staged update operands (conflict-free fragment reads)
+constexpr int kAppDynDoubles = 2 * kTile * kUpdK;  // dynamic shared memory of the panel kernels
 constexpr int kAppThreads = 256;
 constexpr int kCoopMinFront = 192;     // levels whose largest panel front is at least this use the cooperative kernel
 constexpr int kColsPerThread = kTile * kTile / kAppThreads;  // 16
