@@ -671,7 +671,7 @@ struct FrontView {
 
 struct AppCtrl {
   int p, lim, prog, force, stop, w, eb, q;
-  int neg, pos, zero, two, forced, finished, pad0, pad1;
+  int neg, pos, zero, two, forced, finished, fb, pad1;  // fb: first pivot whose trailing update is pending
 };
 
 struct AppFront {
@@ -686,7 +686,6 @@ struct AppFront {
   unsigned long long* cmax;
   unsigned long long* rmax;
   double* backup;  // kNB columns of m rows
-  double* W;       // W = L D of the panel's columns (kNB columns of m rows), for the trailing update
   std::int32_t* plab;
   signed char* ppv;
 };
@@ -713,8 +712,6 @@ __device__ AppFront make_front(const SnDev& d, double* panels, double* cb, doubl
   F.rmax = reinterpret_cast<unsigned long long*>(s);
   s += kNB;
   F.backup = s;
-  s += static_cast<std::int64_t>(kNB) * d.m;
-  F.W = s;
   F.plab = pidx_out + d.first;
   F.ppv = piv_out + d.first;
   return F;
@@ -855,18 +852,6 @@ __device__ void app_control_and_block(AppFront& F, const FactorParams& prm, doub
     const int i = t % w, j = t / w;
     if (i >= j) F.f.at(p + i, p + j) = Bs[i + j * kNB];
   }
-  // W rows of the block: W(p+i, s) = (L D)(i, s) for eliminated s, from the factored block
-  for (int t = threadIdx.x; t < w * kNB; t += blockDim.x) {
-    const int i = t % w, s = t / w;
-    double v = 0.0;
-    if (s < eb && i > s) {
-      const signed char ty = spv[s];
-      if (ty == 1) v = Bs[i + s * kNB] * Bs[s + s * kNB];
-      else if (ty == 2 && i > s + 1) v = Bs[i + s * kNB] * Bs[s + s * kNB] + Bs[i + (s + 1) * kNB] * Bs[s + 1 + s * kNB];
-      else if (ty == 3 && i > s) v = Bs[i + (s - 1) * kNB] * Bs[s + (s - 1) * kNB] + Bs[i + s * kNB] * Bs[s + s * kNB];
-    }
-    F.W[static_cast<std::int64_t>(s) * F.f.m + p + i] = v;
-  }
   for (int t = threadIdx.x; t < kNB * kNB; t += blockDim.x) F.B[t] = Bs[t];
   for (int t = threadIdx.x; t < kNB; t += blockDim.x) {
     F.lab[t] = slab[t];
@@ -971,7 +956,6 @@ __device__ void app_rows(AppFront& F, int rank, int nr, double* Bs, int* slab, s
         else if (ty == 2) out = Di[t] * y[t] + Di[kNB + t] * yn;
         else out = Di[kNB + t] * yp + Di[2 * kNB + t] * y[t];
         cm[t] = fmaxf(cm[t], static_cast<float>(fabs(ty == 0 ? y[t] : out)));
-        F.W[static_cast<std::int64_t>(t) * m + i] = (ty == 0) ? 0.0 : y[t];  // W = L D = y
       } else {
         out = y[t];
       }
@@ -1083,43 +1067,103 @@ __device__ void app_restore(AppFront& F, int rank, int nr, int q) {
   }
 }
 
-// All ranks: C(i, c) -= sum_{s<q} L(i, p+s) W(c, s), from <= c <= i < m, W = L D (from scratch);
-// 64 x 64 tiles of the lower triangle dealt round-robin to the ranks; 4 x 4 outputs per thread, the
-// C values loaded before the products so that their latencies overlap.
 __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
                : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
 }
 
-// Trailing update C -= L W^T of the lower 64 x 64 tiles on the FP64 tensor cores (mma.sync m8n8k4,
-// D = A B + C with A 8 x 4, B 4 x 8): the tile's q <= 32 columns of L (rows of the tile) and of W
-// (rows of the tile's columns) are staged row-major with stride kUpdK, so every fragment read of a
-// half-warp hits 32 distinct banks; warp w (of 8) computes rows 16 (w % 4) .. +16 and columns
-// 32 (w / 4) .. +32 of the tile as 2 x 4 blocks of 8 x 8. A thread's fragment element (g, t) is
-// row g = lane / 4, column t = lane % 4 of A; row t, column g of B; row g, columns 2t, 2t + 1 of C.
-__device__ void app_update(AppFront& F, int rank, int nr, int q, double* Ls, double* Ws) {
+// Blocked step. The pivots [fb, p + q) eliminated since the last full update are pending: their
+// Schur update has reached only the panels factorized since. After a panel the pending update goes
+// either to the whole trailing matrix (a flush: the panel rejected columns, the candidate range
+// ends, or kKB pivots would be pending after the next panel) or to the next panel's columns only.
+// A column is therefore up to date when its panel is factorized, and every other trailing column
+// receives the pending pivots in one rank-(<= kKB) update instead of one update per panel.
+__device__ __forceinline__ bool app_flushes(int p, int w, int q, int lim, int fb) {
+  return q < w || p + q >= lim || p + q + kNB - fb > kKB;
+}
+
+// All ranks: C(i, c) -= sum_{s in [fb, p+q)} L(i, s) W(c, s), W = L D, over the lower triangle
+// c <= i < m of the columns c in [p+q, col_hi): all trailing columns when the step flushes, else the
+// next panel's. Rejected columns [p+q, p+w) of a flushing panel already hold the updates of
+// [fb, p) (they were part of the panel) and take only those of [p, p+q). W is formed while staging
+// from L and the pivots' D (1x1: d; 2x2 [a b; b c]: W(c, s) = a L(c, s) + b L(c, s+1) and
+// W(c, s+1) = b L(c, s) + c L(c, s+1)); null pivots have L = 0.
+//
+// The update runs on the FP64 tensor cores (mma.sync m8n8k4, D = A B + C with A 8 x 4, B 4 x 8) by
+// 64 x 64 tiles of C dealt round-robin to the ranks: the tile's rows of L and its columns' rows of
+// L (<= kKB pivots) are copied asynchronously (cp.async, zero-filled outside the front) into shared
+// memory, column-major with stride kUpdLd = 4 (mod 16), so that the copies of consecutive rows are
+// contiguous and every fragment read of a half-warp hits 32 distinct banks; D is then applied to the
+// second copy in place. Warp w (of 8) computes rows 16 (w % 4) .. +16 and columns 32 (w / 4) .. +32
+// of the tile as 2 x 4 blocks of 8 x 8. A thread's fragment element (g, t) is row g = lane / 4,
+// column t = lane % 4 of A; row t, column g of B; row g, columns 2t, 2t + 1 of C.
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, int bytes) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+__device__ void app_update(AppFront& F, int rank, int nr, int q, double* Ls, double* Ws, double* ca, double* cb,
+                           int* cd) {
   const AppCtrl* c = F.ctrl;
-  const int p = c->p, from = p + q, m = F.f.m;
+  const int p = c->p, w = c->w, lim = c->lim, fb = c->fb, m = F.f.m;
+  const int from = p + q;
+  const int K = from - fb;
   const int rows = m - from;
-  if (rows <= 0 || q <= 0) return;
+  if (rows <= 0 || K <= 0) return;
+  const bool flush = app_flushes(p, w, q, lim, fb);
+  const int col_hi = flush ? m : min(m, from + min(kNB, lim - from));
+  const int rej_hi = flush && q < w ? p + w : 0;  // columns below this take only the pivots >= p
+  // staging coefficients of the pending pivots: W(c, fb+s) = ca[s] L(c, fb+s) + cb[s] L(c, fb+s+cd[s])
+  for (int s = threadIdx.x; s < K; s += blockDim.x) {
+    const int j = fb + s;
+    const signed char ty = __ldcg(&F.ppv[j]);
+    double x = 0.0, y = 0.0;
+    int d = 0;
+    if (ty == 1) x = __ldcg(&F.f.at(j, j));
+    else if (ty == 2) { x = __ldcg(&F.f.at(j, j)); y = __ldcg(&F.f.at(j + 1, j)); d = 1; }
+    else if (ty == 3) { x = __ldcg(&F.f.at(j, j)); y = __ldcg(&F.f.at(j, j - 1)); d = -1; }
+    ca[s] = x;
+    cb[s] = y;
+    cd[s] = d;
+  }
   const int nt = (rows + kTile - 1) / kTile;
-  const int ntiles = nt * (nt + 1) / 2;
+  const int nct = (col_hi - from + kTile - 1) / kTile;
+  const int ntiles = nct * nt - nct * (nct - 1) / 2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t4 = lane & 3;
   const int rbase = (warp & 3) * 16, cbase = (warp >> 2) * 32;
-  const int qpad = (q + 3) & ~3;
+  const int Kpad = (K + 3) & ~3;
   for (int tile = rank; tile < ntiles; tile += nr) {
-    int ti = static_cast<int>((sqrt(8.0 * tile + 1.0) - 1.0) * 0.5);
-    while ((ti + 1) * (ti + 2) / 2 <= tile) ++ti;
-    while (ti * (ti + 1) / 2 > tile) --ti;
-    const int tj = tile - ti * (ti + 1) / 2;
+    int ti, tj;
+    if (nct == nt) {
+      ti = static_cast<int>((sqrt(8.0 * tile + 1.0) - 1.0) * 0.5);
+      while ((ti + 1) * (ti + 2) / 2 <= tile) ++ti;
+      while (ti * (ti + 1) / 2 > tile) --ti;
+      tj = tile - ti * (ti + 1) / 2;
+    } else {
+      int rest = tile;
+      tj = 0;
+      while (rest >= nt - tj) { rest -= nt - tj; ++tj; }
+      ti = tj + rest;
+    }
     const int i0 = from + ti * kTile, j0 = from + tj * kTile;
     __syncthreads();
-    for (int t = threadIdx.x; t < qpad * kTile; t += blockDim.x) {
-      const int s = t / kTile, r = t % kTile;
+    {
+      // thread: tile row r, pivots s = sg, sg + 4, ...: all copies in flight at once
+      const int r = threadIdx.x & (kTile - 1), sg = threadIdx.x >> 6;
       const int i = i0 + r, cc = j0 + r;
-      Ls[r * kUpdK + s] = (s < q && i < m) ? F.f.at(i, p + s) : 0.0;
-      Ws[r * kUpdK + s] = (s < q && cc < m) ? F.W[static_cast<std::int64_t>(s) * m + cc] : 0.0;
+      const int li = i < m ? i : from, lc = cc < m ? cc : from;
+      const int lb = i < m ? 8 : 0, wb = cc < col_hi ? 8 : 0;
+#pragma unroll 8
+      for (int s = sg; s < Kpad; s += kAppThreads / kTile) {
+        const bool in = s < K;
+        const double* lj = F.f.col(fb + (in ? s : 0));
+        cp_async8(&Ls[s * kUpdLd + r], lj + li, in ? lb : 0);
+        cp_async8(&Ws[s * kUpdLd + r], lj + lc, in ? wb : 0);
+      }
     }
     // prefetch this thread's C entries (rows rbase + 8a + g, columns cbase + 8b + 2 t4 + e)
     double* colp[4][2];
@@ -1129,25 +1173,48 @@ __device__ void app_update(AppFront& F, int rank, int nr, int q, double* Ls, dou
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int cc = j0 + cbase + 8 * b + 2 * t4 + e;
-        colp[b][e] = cc < m ? F.f.col(cc) : nullptr;
+        colp[b][e] = cc < col_hi ? F.f.col(cc) : nullptr;
 #pragma unroll
         for (int a = 0; a < 2; ++a) {
           const int i = i0 + rbase + 8 * a + g;
           cv[a][b][e] = (colp[b][e] && i < m && cc <= i) ? colp[b][e][i] : 0.0;
         }
       }
+    cp_async_wait_all();
     __syncthreads();
+    // W = L D in place (a 2x2 pair by its first column), zero for the rejected columns' old pivots
+    for (int t = threadIdx.x; t < K * kTile; t += blockDim.x) {
+      const int s = t / kTile, r = t % kTile;
+      const int d = cd[s];
+      if (d < 0) continue;
+      const bool masked = j0 + r < rej_hi && fb + s < p;
+      double* w0 = &Ws[s * kUpdLd + r];
+      if (d == 0) {
+        *w0 = masked ? 0.0 : ca[s] * *w0;
+      } else {
+        double* w1 = w0 + kUpdLd;
+        const double x0 = *w0, x1 = *w1;
+        *w0 = masked ? 0.0 : fma(ca[s], x0, cb[s] * x1);
+        *w1 = masked ? 0.0 : fma(cb[s + 1], x0, ca[s + 1] * x1);
+      }
+    }
+    __syncthreads();
+    // warps whose 32 columns all lie at or beyond col_hi (the second half of a panel's tile) or
+    // whose 16 rows all lie above their first column have nothing to update
+    const bool idle = j0 + cbase >= col_hi || i0 + rbase + 15 < j0 + cbase;
+    if (idle) continue;
     double acc[2][4][2];
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
       for (int b = 0; b < 4; ++b) { acc[a][b][0] = 0.0; acc[a][b][1] = 0.0; }
-    for (int s0 = 0; s0 < qpad; s0 += 4) {
+#pragma unroll 2
+    for (int s0 = 0; s0 < Kpad; s0 += 4) {
       double af[2], bf[4];
 #pragma unroll
-      for (int a = 0; a < 2; ++a) af[a] = Ls[(rbase + 8 * a + g) * kUpdK + s0 + t4];
+      for (int a = 0; a < 2; ++a) af[a] = Ls[(s0 + t4) * kUpdLd + rbase + 8 * a + g];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) bf[b] = Ws[(cbase + 8 * b + g) * kUpdK + s0 + t4];
+      for (int b = 0; b < 4; ++b) bf[b] = Ws[(s0 + t4) * kUpdLd + cbase + 8 * b + g];
 #pragma unroll
       for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -1173,6 +1240,7 @@ __device__ void app_advance(AppFront& F, int q) {
   const int p = c->p, w = c->w;
   const int np = p + q, r = w - q;
   const int lim = c->lim;
+  const bool flushed = app_flushes(p, w, q, lim, c->fb);
   if (r > 0 && np + r < lim) {
     for (int t = 0; t < r; ++t) {
       front_swap(F.f, np + t, lim - r + t, F.plab);
@@ -1182,6 +1250,7 @@ __device__ void app_advance(AppFront& F, int q) {
   __syncthreads();
   if (threadIdx.x == 0) {
     c->p = np;
+    if (flushed) c->fb = np;
     if (q > 0) { c->prog = 1; c->force = 0; }
     if (r > 0) c->lim = np + r < lim ? lim - r : np;
   }
@@ -1195,6 +1264,8 @@ struct AppSmem {
   signed char spv[kNB];
   unsigned long long scm[kNB], srm[kNB];
   StepShared bst;
+  double ca[kKB], cb[kKB];
+  int cd[kKB];
   int stop, q;
 };
 
@@ -1207,7 +1278,7 @@ __global__ void __launch_bounds__(kAppThreads) k_front_app(const std::int32_t* l
                                                            FactorCounters* cnt, std::int32_t* failed) {
   extern __shared__ double app_dyn[];
   double* Ls = app_dyn;
-  double* Ws = app_dyn + kTile * kUpdK;
+  double* Ws = app_dyn + kKB * kUpdLd;
   __shared__ AppSmem sm;
   const SnDev d = sn[list[blockIdx.x]];
   AppFront F = make_front(d, panels, cb, scratch, piv_out, pidx_out);
@@ -1226,7 +1297,7 @@ __global__ void __launch_bounds__(kAppThreads) k_front_app(const std::int32_t* l
     __syncthreads();
     if (q < F.ctrl->w) app_restore(F, 0, 1, q);
     __syncthreads();
-    app_update(F, 0, 1, q, Ls, Ws);
+    app_update(F, 0, 1, q, Ls, Ws, sm.ca, sm.cb, sm.cd);
     __syncthreads();
     app_advance(F, q);
   }
@@ -1244,7 +1315,7 @@ __global__ void __launch_bounds__(kAppThreads) k_front_coop(const std::int32_t* 
   cg::grid_group grid = cg::this_grid();
   extern __shared__ double app_dyn[];
   double* Ls = app_dyn;
-  double* Ws = app_dyn + kTile * kUpdK;
+  double* Ws = app_dyn + kKB * kUpdLd;
   __shared__ AppSmem sm;
   int fi = 0;
   while (fi + 1 < nfronts && cta_start[fi + 1] <= static_cast<int>(blockIdx.x)) ++fi;
@@ -1272,7 +1343,7 @@ __global__ void __launch_bounds__(kAppThreads) k_front_coop(const std::int32_t* 
       if (q < F.ctrl->w) app_restore(F, rank, nr, q);
     }
     grid.sync();
-    if (active) app_update(F, rank, nr, q, Ls, Ws);
+    if (active) app_update(F, rank, nr, q, Ls, Ws, sm.ca, sm.cb, sm.cd);
     grid.sync();
     if (active && rank == 0) app_advance(F, q);
   }

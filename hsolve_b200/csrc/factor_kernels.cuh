@@ -11,17 +11,18 @@ namespace hsg {
 constexpr int kSmallMax = 64;          // fronts up to this order are factorized in shared memory
 constexpr int kNB = 32;                // panel width of the a-posteriori pivoting kernel
 constexpr int kTile = 64;              // trailing-update tile (rows = cols)
-constexpr int kUpdK = kNB + 4;         // row stride of the staged update operands (conflict-free fragment reads)
-constexpr int kAppDynDoubles = 2 * kTile * kUpdK;  // dynamic shared memory of the panel kernels
+constexpr int kKB = 128;               // pending pivots whose trailing update is applied at once (blocked step)
+constexpr int kUpdLd = kTile + 4;      // column stride of the staged update operands (conflict-free fragment reads)
+constexpr int kAppDynDoubles = 2 * kKB * kUpdLd;  // dynamic shared memory of the panel kernels
 constexpr int kAppThreads = 256;
 constexpr int kCoopMinFront = 192;     // levels whose largest panel front is at least this use the cooperative kernel
 constexpr int kColsPerThread = kTile * kTile / kAppThreads;  // 16
 constexpr int kExtendAddCols = 8;      // contribution-block columns per extend-add CTA
 // per-front scratch of the panel kernels (doubles): control block, block, original block, labels,
-// pivot types, column maxima, backup of the panel's rows, W = L D of the panel
+// pivot types, column maxima, backup of the panel's rows
 constexpr int kAppCtrlDoubles = 8;
 inline std::int64_t app_scratch_doubles(int m) {
-  return kAppCtrlDoubles + 2 * kNB * kNB + kNB / 2 + kNB / 8 + 2 * kNB + 2 * static_cast<std::int64_t>(m) * kNB;
+  return kAppCtrlDoubles + 2 * kNB * kNB + kNB / 2 + kNB / 8 + 2 * kNB + static_cast<std::int64_t>(m) * kNB;
 }
 
 void launch_fill(double* x, std::int64_t n, double v, cudaStream_t s);
