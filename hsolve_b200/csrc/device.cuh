@@ -40,7 +40,7 @@ struct FactorCounters {
   unsigned long long failed;     // columns that could not be pivoted in their front
   unsigned long long forced;     // pivots accepted without the threshold test (roots)
   unsigned long long amax_bits;  // max |entry| of the scaled matrix (double bits)
-  unsigned long long pad;
+  unsigned long long sync_timeouts;  // front barriers that gave up waiting (must stay 0)
 };
 
 struct FactorParams {

@@ -671,7 +671,15 @@ struct FrontView {
 
 struct AppCtrl {
   int p, lim, prog, force, stop, w, eb, q;
-  int neg, pos, zero, two, forced, finished, fb, pad1;  // fb: first pivot whose trailing update is pending
+  int neg, pos, zero, two, forced, finished, fb, bar;  // fb: first pivot whose trailing update is pending;
+                                                       // bar: arrivals at the front's barrier
+};
+
+// The fields of the control block that a panel step reads, copied by every CTA of the front right
+// after a barrier: rank 0 may already change the control block for the next panel while slower
+// CTAs still work on this one.
+struct StepView {
+  int p, w, lim, fb, eb, force, stop;
 };
 
 struct AppFront {
@@ -679,6 +687,7 @@ struct AppFront {
   int first;
   bool root;
   AppCtrl* ctrl;
+  double* slots;   // two sets of the per-panel arrays below, used by alternate panels
   double* B;       // factored diagonal block, kNB x kNB col-major
   double* Borig;   // the block before factorization
   int* lab;        // block permutation
@@ -690,15 +699,9 @@ struct AppFront {
   signed char* ppv;
 };
 
-__device__ AppFront make_front(const SnDev& d, double* panels, double* cb, double* scratch, signed char* piv_out,
-                               std::int32_t* pidx_out) {
-  AppFront F;
-  F.f = FrontView{panels + d.panel_off, d.cb_off >= 0 ? cb + d.cb_off : nullptr, d.m, d.k};
-  F.first = d.first;
-  F.root = d.parent < 0;
-  double* s = scratch + d.scratch_off;
-  F.ctrl = reinterpret_cast<AppCtrl*>(s);
-  s += kAppCtrlDoubles;
+// point the per-panel arrays at set `slot` (0 or 1)
+__device__ __forceinline__ void set_slot(AppFront& F, int slot) {
+  double* s = F.slots + slot * kAppSlotDoubles;
   F.B = s;
   s += kNB * kNB;
   F.Borig = s;
@@ -710,10 +713,35 @@ __device__ AppFront make_front(const SnDev& d, double* panels, double* cb, doubl
   F.cmax = reinterpret_cast<unsigned long long*>(s);
   s += kNB;
   F.rmax = reinterpret_cast<unsigned long long*>(s);
-  s += kNB;
+}
+
+__device__ __forceinline__ StepView step_view(const AppCtrl* c) {
+  StepView v;
+  v.p = __ldcg(&c->p);
+  v.w = __ldcg(&c->w);
+  v.lim = __ldcg(&c->lim);
+  v.fb = __ldcg(&c->fb);
+  v.eb = __ldcg(&c->eb);
+  v.force = __ldcg(&c->force);
+  v.stop = __ldcg(&c->stop);
+  return v;
+}
+
+__device__ AppFront make_front(const SnDev& d, double* panels, double* cb, double* scratch, signed char* piv_out,
+                               std::int32_t* pidx_out) {
+  AppFront F;
+  F.f = FrontView{panels + d.panel_off, d.cb_off >= 0 ? cb + d.cb_off : nullptr, d.m, d.k};
+  F.first = d.first;
+  F.root = d.parent < 0;
+  double* s = scratch + d.scratch_off;
+  F.ctrl = reinterpret_cast<AppCtrl*>(s);
+  s += kAppCtrlDoubles;
+  F.slots = s;
+  s += 2 * kAppSlotDoubles;
   F.backup = s;
   F.plab = pidx_out + d.first;
   F.ppv = piv_out + d.first;
+  set_slot(F, 0);
   return F;
 }
 
@@ -865,14 +893,13 @@ __device__ void app_control_and_block(AppFront& F, const FactorParams& prm, doub
 // All ranks: rows [p+w, m) solved against the block (L21 = F21 P L11^-T D^-1), backup, column maxima.
 // The block's strict lower part with the 2x2 couplings masked (they belong to D) is staged in Ls
 // (shared), the substitution runs fully unrolled in registers, one row per thread.
-__device__ void app_rows(AppFront& F, int rank, int nr, double* Bs, int* slab, signed char* spv,
+__device__ void app_rows(AppFront& F, const StepView& v, int rank, int nr, double* Bs, int* slab, signed char* spv,
                          unsigned long long* scm, unsigned long long* srm, double* Lm) {
-  const AppCtrl* c = F.ctrl;
-  const int p = __ldcg(&c->p), w = __ldcg(&c->w), eb = __ldcg(&c->eb), m = F.f.m;
+  const int p = v.p, w = v.w, eb = v.eb, m = F.f.m;
   for (int t = threadIdx.x; t < kNB * kNB; t += blockDim.x) Bs[t] = __ldcg(&F.B[t]);
   for (int t = threadIdx.x; t < kNB; t += blockDim.x) {
     slab[t] = __ldcg(&F.lab[t]);
-    spv[t] = F.pv[t];
+    spv[t] = __ldcg(&F.pv[t]);
     scm[t] = 0ull;
     srm[t] = 0ull;
   }
@@ -880,9 +907,9 @@ __device__ void app_rows(AppFront& F, int rank, int nr, double* Bs, int* slab, s
   // Lm[t * kNB + s] = L11(t, s) for s < min(t, eb), zero otherwise (row-major for broadcast reads)
   for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
     const int t = e / kNB, s = e % kNB;
-    double v = 0.0;
-    if (t < w && s < t && s < eb && !(spv[s] == 2 && s + 1 == t)) v = Bs[t + s * kNB];
-    Lm[e] = v;
+    double x = 0.0;
+    if (t < w && s < t && s < eb && !(spv[s] == 2 && s + 1 == t)) x = Bs[t + s * kNB];
+    Lm[e] = x;
   }
   __syncthreads();
   // permute the L rows p..p+w-1 of the eliminated columns c < p (a thread owns a column; the
@@ -890,13 +917,13 @@ __device__ void app_rows(AppFront& F, int rank, int nr, double* Bs, int* slab, s
   const int cchunk = (p + nr - 1) / nr;
   const int cend = min(p, (rank + 1) * cchunk);
   for (int cc = rank * cchunk + threadIdx.x; cc < cend; cc += blockDim.x) {
-    double v[kNB];
+    double x[kNB];
     double* colp = F.f.col(cc) + p;
 #pragma unroll
-    for (int a = 0; a < kNB; ++a) v[a] = a < w ? colp[slab[a]] : 0.0;
+    for (int a = 0; a < kNB; ++a) x[a] = a < w ? colp[slab[a]] : 0.0;
 #pragma unroll
     for (int a = 0; a < kNB; ++a)
-      if (a < w) colp[a] = v[a];
+      if (a < w) colp[a] = x[a];
   }
   const int rtotal = m - (p + w);
   const int rchunk = (rtotal + nr - 1) / nr;
@@ -938,10 +965,10 @@ __device__ void app_rows(AppFront& F, int rank, int nr, double* Bs, int* slab, s
       if (t < w) F.backup[static_cast<std::int64_t>(t) * m + i] = y[t];
 #pragma unroll
     for (int t = 1; t < kNB; ++t) {
-      double v = y[t];
+      double acc = y[t];
 #pragma unroll
-      for (int s = 0; s < t; ++s) v = fma(-y[s], Lm[t * kNB + s], v);
-      y[t] = v;
+      for (int s = 0; s < t; ++s) acc = fma(-y[s], Lm[t * kNB + s], acc);
+      y[t] = acc;
     }
 #pragma unroll
     for (int t = 0; t < kNB; ++t) {
@@ -986,11 +1013,12 @@ __device__ void app_rows(AppFront& F, int rank, int nr, double* Bs, int* slab, s
 // All ranks: the accepted prefix q (identical in every CTA); rank 0 books the inertia. The small
 // per-panel arrays are staged in shared memory first (one parallel load) so that the serial scans
 // below touch no global memory. Bs / spv already hold the panel's block and pivot types (app_rows).
-__device__ int app_accept(AppFront& F, int rank, bool force, double thr, double inv_u, int* sq, const double* Bs,
-                          const signed char* spv, unsigned long long* scm, unsigned long long* srm) {
-  const AppCtrl* c = F.ctrl;
-  const int eb = __ldcg(&c->eb);
-  const int p = __ldcg(&c->p);
+__device__ int app_accept(AppFront& F, const StepView& v, int rank, double thr, double inv_u, int* sq,
+                          const double* Bs, const signed char* spv, unsigned long long* scm,
+                          unsigned long long* srm) {
+  const int eb = v.eb;
+  const int p = v.p;
+  const bool force = v.force != 0;
   for (int t = threadIdx.x; t < kNB; t += blockDim.x) {
     scm[t] = __ldcg(&F.cmax[t]);
     srm[t] = __ldcg(&F.rmax[t]);
@@ -1048,9 +1076,8 @@ __device__ int app_accept(AppFront& F, int rank, bool force, double thr, double 
 }
 
 // All ranks: restore the rejected block columns [q, w) from the backup / original block.
-__device__ void app_restore(AppFront& F, int rank, int nr, int q) {
-  const AppCtrl* c = F.ctrl;
-  const int p = c->p, w = c->w, m = F.f.m;
+__device__ void app_restore(AppFront& F, const StepView& v, int rank, int nr, int q) {
+  const int p = v.p, w = v.w, m = F.f.m;
   const int rtotal = m - (p + w);
   const int rchunk = (rtotal + nr - 1) / nr;
   const int rbeg = p + w + rank * rchunk, rend = min(m, rbeg + rchunk);
@@ -1105,10 +1132,13 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
-__device__ void app_update(AppFront& F, int rank, int nr, int q, double* Ls, double* Ws, double* ca, double* cb,
-                           int* cd) {
-  const AppCtrl* c = F.ctrl;
-  const int p = c->p, w = c->w, lim = c->lim, fb = c->fb, m = F.f.m;
+//
+// With look-ahead (la: the panel was accepted whole and the next one follows directly), rank 0 takes
+// only tile 0, which holds the next panel's diagonal block, so that it can factorize that block
+// while the other ranks finish the remaining tiles.
+__device__ void app_update(AppFront& F, const StepView& v, int rank, int nr, int q, bool la, double* Ls, double* Ws,
+                           double* ca, double* cb, int* cd, const double* Bs, const signed char* spv) {
+  const int p = v.p, w = v.w, lim = v.lim, fb = v.fb, m = F.f.m;
   const int from = p + q;
   const int K = from - fb;
   const int rows = m - from;
@@ -1117,14 +1147,24 @@ __device__ void app_update(AppFront& F, int rank, int nr, int q, double* Ls, dou
   const int col_hi = flush ? m : min(m, from + min(kNB, lim - from));
   const int rej_hi = flush && q < w ? p + w : 0;  // columns below this take only the pivots >= p
   // staging coefficients of the pending pivots: W(c, fb+s) = ca[s] L(c, fb+s) + cb[s] L(c, fb+s+cd[s])
+  // (the panel's own pivots from the block in shared memory: rank 0 books their types in global
+  // memory while the other ranks may already be here)
   for (int s = threadIdx.x; s < K; s += blockDim.x) {
     const int j = fb + s;
-    const signed char ty = __ldcg(&F.ppv[j]);
     double x = 0.0, y = 0.0;
     int d = 0;
-    if (ty == 1) x = __ldcg(&F.f.at(j, j));
-    else if (ty == 2) { x = __ldcg(&F.f.at(j, j)); y = __ldcg(&F.f.at(j + 1, j)); d = 1; }
-    else if (ty == 3) { x = __ldcg(&F.f.at(j, j)); y = __ldcg(&F.f.at(j, j - 1)); d = -1; }
+    if (j >= p) {
+      const int t = j - p;
+      const signed char ty = spv[t];
+      if (ty == 1) x = Bs[t + t * kNB];
+      else if (ty == 2) { x = Bs[t + t * kNB]; y = Bs[t + 1 + t * kNB]; d = 1; }
+      else if (ty == 3) { x = Bs[t + t * kNB]; y = Bs[t + (t - 1) * kNB]; d = -1; }
+    } else {
+      const signed char ty = __ldcg(&F.ppv[j]);
+      if (ty == 1) x = __ldcg(&F.f.at(j, j));
+      else if (ty == 2) { x = __ldcg(&F.f.at(j, j)); y = __ldcg(&F.f.at(j + 1, j)); d = 1; }
+      else if (ty == 3) { x = __ldcg(&F.f.at(j, j)); y = __ldcg(&F.f.at(j, j - 1)); d = -1; }
+    }
     ca[s] = x;
     cb[s] = y;
     cd[s] = d;
@@ -1136,7 +1176,11 @@ __device__ void app_update(AppFront& F, int rank, int nr, int q, double* Ls, dou
   const int g = lane >> 2, t4 = lane & 3;
   const int rbase = (warp & 3) * 16, cbase = (warp >> 2) * 32;
   const int Kpad = (K + 3) & ~3;
-  for (int tile = rank; tile < ntiles; tile += nr) {
+  // tiles of this rank: round-robin, or with look-ahead tile 0 for rank 0 and the rest over ranks 1..
+  const bool split = la && nr > 1;
+  const int tfirst = split ? (rank == 0 ? 0 : rank) : rank;
+  const int tstep = split ? (rank == 0 ? ntiles : nr - 1) : nr;
+  for (int tile = tfirst; tile < ntiles; tile += tstep) {
     int ti, tj;
     if (nct == nt) {
       ti = static_cast<int>((sqrt(8.0 * tile + 1.0) - 1.0) * 0.5);
@@ -1266,8 +1310,104 @@ struct AppSmem {
   StepShared bst;
   double ca[kKB], cb[kKB];
   int cd[kKB];
-  int stop, q;
+  int stop, q, ok;
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Barrier of the nr CTAs of one front (all co-resident: cooperative launch). Arrivals count up in
+// the front's control block; a CTA waits until the count reaches the next multiple of nr. The wait
+// gives up after kBarrierTimeoutNs (or when another front has given up), books the timeout in the
+// counters and returns false, so that a stuck front ends the kernel instead of hanging it.
+constexpr unsigned long long kBarrierTimeoutNs = 5ull * 1000 * 1000 * 1000;
+
+__device__ bool front_barrier(int* bar, int nr, unsigned long long* timeouts, int* s_ok) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    if (nr > 1) {
+      __threadfence();
+      const int old = atomicAdd(bar, 1);
+      const int target = (old / nr + 1) * nr;
+      unsigned long long t0 = 0;
+      for (unsigned it = 0;; ++it) {
+        int arrived;
+        asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(arrived) : "l"(bar) : "memory");
+        if (arrived >= target) break;
+        if ((it & 63u) == 63u) {
+          if (*reinterpret_cast<volatile unsigned long long*>(timeouts) != 0ull) { ok = 0; break; }
+          const unsigned long long t = global_ns();
+          if (t0 == 0) t0 = t;
+          else if (t - t0 > kBarrierTimeoutNs) { atomicAdd(timeouts, 1ull); ok = 0; break; }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+    *s_ok = ok;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
+// The panel loop of one front, run by its nr CTAs (rank 0 .. nr-1). A step is
+//   [control: rank 0 advances past the previous panel and factorizes the next block] barrier
+//   rows (all) barrier  accept (all, identical)  [restore (all) barrier]  update (all) barrier
+// and when a panel is accepted whole and the next one follows directly (look-ahead), rank 0
+// advances and factorizes the next block right after its update tile, so that the control phase
+// and its barrier are skipped. Alternate panels use alternate per-panel arrays, so the next
+// block's arrays never overlap the ones slower CTAs still read.
+template <bool kCoop>
+__device__ void app_front(AppFront& F, int rank, int nr, const FactorParams& prm, FactorCounters* cnt,
+                          std::int32_t* failed, int* level_done, AppSmem& sm, double* Ls, double* Ws) {
+  const double thr = null_threshold(prm);
+  const double inv_u = 1.0 / prm.u;
+  int* bar = &F.ctrl->bar;
+  auto sync = [&]() -> bool {
+    if (kCoop) return front_barrier(bar, nr, &cnt->sync_timeouts, &sm.ok);
+    __syncthreads();
+    return true;
+  };
+  bool la = false;
+  int j = 0, qprev = 0;
+  while (true) {
+    if (!la) {
+      if (rank == 0) {
+        if (j > 0) app_advance(F, qprev);
+        set_slot(F, j & 1);
+        app_control_and_block(F, prm, thr, sm.Bs, sm.tmp0, sm.tmp1, sm.slab, sm.spv, sm.bst, &sm.stop, cnt, failed,
+                              level_done);
+      }
+      if (!sync()) break;
+    }
+    set_slot(F, j & 1);
+    const StepView v = step_view(F.ctrl);
+    if (v.stop) break;
+    app_rows(F, v, rank, nr, sm.Bs, sm.slab, sm.spv, sm.scm, sm.srm, Ls);
+    if (!sync()) break;
+    const int q = app_accept(F, v, rank, thr, inv_u, &sm.q, sm.Bs, sm.spv, sm.scm, sm.srm);
+    if (q < v.w) {
+      app_restore(F, v, rank, nr, q);
+      if (!sync()) break;
+    }
+    la = q == v.w && v.p + v.w < v.lim;
+    app_update(F, v, rank, nr, q, la, Ls, Ws, sm.ca, sm.cb, sm.cd, sm.Bs, sm.spv);
+    if (la && rank == 0) {
+      __syncthreads();
+      app_advance(F, q);
+      set_slot(F, (j + 1) & 1);
+      app_control_and_block(F, prm, thr, sm.Bs, sm.tmp0, sm.tmp1, sm.slab, sm.spv, sm.bst, &sm.stop, cnt, failed,
+                            level_done);
+    }
+    if (!sync()) break;
+    qprev = q;
+    ++j;
+  }
+}
 
 }  // namespace
 
@@ -1282,29 +1422,13 @@ __global__ void __launch_bounds__(kAppThreads) k_front_app(const std::int32_t* l
   __shared__ AppSmem sm;
   const SnDev d = sn[list[blockIdx.x]];
   AppFront F = make_front(d, panels, cb, scratch, piv_out, pidx_out);
-  const double thr = null_threshold(prm);
-  const double inv_u = 1.0 / prm.u;
   app_init(F, 0, 1);
   __syncthreads();
-  while (true) {
-    app_control_and_block(F, prm, thr, sm.Bs, sm.tmp0, sm.tmp1, sm.slab, sm.spv, sm.bst, &sm.stop, cnt, failed, nullptr);
-    __syncthreads();
-    if (sm.stop) break;
-    app_rows(F, 0, 1, sm.Bs, sm.slab, sm.spv, sm.scm, sm.srm, Ls);
-    __syncthreads();
-    const bool force = F.ctrl->force != 0;
-    const int q = app_accept(F, 0, force, thr, inv_u, &sm.q, sm.Bs, sm.spv, sm.scm, sm.srm);
-    __syncthreads();
-    if (q < F.ctrl->w) app_restore(F, 0, 1, q);
-    __syncthreads();
-    app_update(F, 0, 1, q, Ls, Ws, sm.ca, sm.cb, sm.cd);
-    __syncthreads();
-    app_advance(F, q);
-  }
+  app_front<false>(F, 0, 1, prm, cnt, failed, nullptr, sm, Ls, Ws);
 }
 
-// Cooperative: the fronts of a level share the grid; front f owns CTAs [cta_start[f], cta_start[f+1]).
-// Grid-wide barriers separate the steps; the loop ends when every front has finished (level_done).
+// Cooperative: the fronts of a level share the grid; front f owns CTAs [cta_start[f], cta_start[f+1])
+// and runs its panel loop with its own barriers, independently of the other fronts.
 __global__ void __launch_bounds__(kAppThreads) k_front_coop(const std::int32_t* list, const std::int32_t* cta_start,
                                                             int nfronts, const SnDev* sn, double* panels, double* cb,
                                                             double* scratch, signed char* piv_out,
@@ -1323,30 +1447,9 @@ __global__ void __launch_bounds__(kAppThreads) k_front_coop(const std::int32_t* 
   const int nr = cta_start[fi + 1] - cta_start[fi];
   const SnDev d = sn[list[fi]];
   AppFront F = make_front(d, panels, cb, scratch, piv_out, pidx_out);
-  const double thr = null_threshold(prm);
-  const double inv_u = 1.0 / prm.u;
   app_init(F, rank, nr);
-  grid.sync();
-  while (true) {
-    if (rank == 0) {
-      app_control_and_block(F, prm, thr, sm.Bs, sm.tmp0, sm.tmp1, sm.slab, sm.spv, sm.bst, &sm.stop, cnt, failed,
-                            level_done);
-    }
-    grid.sync();
-    if (*reinterpret_cast<volatile int*>(level_done) >= nfronts) break;
-    const bool active = F.ctrl->stop == 0;
-    if (active) app_rows(F, rank, nr, sm.Bs, sm.slab, sm.spv, sm.scm, sm.srm, Ls);
-    grid.sync();
-    int q = 0;
-    if (active) {
-      q = app_accept(F, rank, __ldcg(&F.ctrl->force) != 0, thr, inv_u, &sm.q, sm.Bs, sm.spv, sm.scm, sm.srm);
-      if (q < F.ctrl->w) app_restore(F, rank, nr, q);
-    }
-    grid.sync();
-    if (active) app_update(F, rank, nr, q, Ls, Ws, sm.ca, sm.cb, sm.cd);
-    grid.sync();
-    if (active && rank == 0) app_advance(F, q);
-  }
+  grid.sync();  // the control blocks (and their barrier counts) are initialized
+  app_front<true>(F, rank, nr, prm, cnt, failed, level_done, sm, Ls, Ws);
 }
 
 // ------------------------------------------------------------------------------ launchers

@@ -18,11 +18,12 @@ constexpr int kAppThreads = 256;
 constexpr int kCoopMinFront = 192;     // levels whose largest panel front is at least this use the cooperative kernel
 constexpr int kColsPerThread = kTile * kTile / kAppThreads;  // 16
 constexpr int kExtendAddCols = 8;      // contribution-block columns per extend-add CTA
-// per-front scratch of the panel kernels (doubles): control block, block, original block, labels,
-// pivot types, column maxima, backup of the panel's rows
+// per-front scratch of the panel kernels (doubles): control block, two sets (alternate panels) of
+// block, original block, labels, pivot types and column maxima, backup of the panel's rows
 constexpr int kAppCtrlDoubles = 8;
+constexpr int kAppSlotDoubles = 2 * kNB * kNB + kNB / 2 + kNB / 8 + 2 * kNB;
 inline std::int64_t app_scratch_doubles(int m) {
-  return kAppCtrlDoubles + 2 * kNB * kNB + kNB / 2 + kNB / 8 + 2 * kNB + static_cast<std::int64_t>(m) * kNB;
+  return kAppCtrlDoubles + 2 * kAppSlotDoubles + static_cast<std::int64_t>(m) * kNB;
 }
 
 void launch_fill(double* x, std::int64_t n, double v, cudaStream_t s);

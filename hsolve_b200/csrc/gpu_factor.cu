@@ -563,6 +563,7 @@ hsg_inertia_t GpuFactor::factorize(double alpha, double beta, bool detection, bo
       dstats_.factor_ms += ms;
       dstats_.factorizations += 1;
     }
+    HSG_REQUIRE(c.sync_timeouts == 0, HSG_INTERNAL, "factorization: a front barrier timed out");
     if (c.failed == 0) break;
     HSG_REQUIRE(replans < 16, HSG_FACTORIZATION_FAILED, "delayed pivots could not be placed after " << replans << " re-plans");
     const std::int64_t nf = std::min<std::int64_t>(static_cast<std::int64_t>(c.failed), n_);
