@@ -120,17 +120,22 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-# ncu DRAM captures committed under profiles/ (dram__bytes_read.sum + dram__bytes_write.sum),
-# per workload: (file, key, what the bytes cover)
+# ncu DRAM captures committed under profiles/ (dram__bytes_read.sum + dram__bytes_write.sum), per
+# workload and kernel class: (file, key, what the bytes cover)
 TRAFFIC_CAPTURES = {
-    "interval_box1e5": ("factorization_box1e5.md", "dram_bytes_per_factorization_k_front_coop",
-                        "k_front_coop launches of one factorization (87 % of its device time)"),
+    "interval_box1e5": {
+        "factor": ("factorization_box1e5.md", "dram_bytes_per_factorization_k_front_coop",
+                   "k_front_coop launches of one factorization (83 % of its device time)"),
+        "solve": ("solve_sweeps_box1e5.md", "dram_bytes_per_solve_call_8_columns",
+                  "all launches of one 8-column solve call"),
+    },
 }
 
 
-def captured_traffic(workload):
-    """DRAM bytes per factorization from the committed ncu summary of this workload, or None."""
-    cap = TRAFFIC_CAPTURES.get(workload)
+def captured_traffic(workload, cls):
+    """DRAM bytes per launch of kernel class `cls` ("factor" or "solve") from the committed ncu
+    summary of this workload, or None."""
+    cap = TRAFFIC_CAPTURES.get(workload, {}).get(cls)
     if cap is None:
         return None, None
     path = Path(__file__).resolve().parent / "profiles" / cap[0]
@@ -265,14 +270,16 @@ def run_ours(args, w, rank, world, local):
                    "kernel": "multifrontal LDL^T (all launches of a factorization)",
                    "launches": acc["factorizations"], "avg_ms": acc["factor_ms"] / max(1, acc["factorizations"])}
     factor_roof["frac"] = factor_roof["achieved"] / fp64_peak
-    factor_roof["traffic"], factor_roof["traffic_scope"] = captured_traffic(args.workload)
+    factor_roof["traffic"], factor_roof["traffic_scope"] = captured_traffic(args.workload, "factor")
     solve_roof = {"bound": "hbm", "achieved": sb / sol_s / 1e9 if sol_s > 0 else 0.0, "peak": peaks["hbm_gbs"],
                   "unit": "GB/s", "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_src})",
                   "kernel": "supernodal fwd+diag+bwd solve (all launches of a solve call)",
                   "launches": acc["solves"], "avg_ms": acc["solve_ms"] / max(1, acc["solves"]),
                   "avg_columns": avg_p}
     solve_roof["frac"] = solve_roof["achieved"] / peaks["hbm_gbs"]
-    solve_roof["traffic"] = None
+    solve_roof["traffic"], solve_roof["traffic_scope"] = captured_traffic(args.workload, "solve")
+    if solve_roof["traffic"] is not None and abs(avg_p - 8.0) > 1e-9:
+        solve_roof["traffic"] = None  # the capture is of an 8-column solve
     dominant, other = (factor_roof, solve_roof) if fac_s >= sol_s else (solve_roof, factor_roof)
     counts = {"factorizations": acc["factorizations"] / args.steps, "solves": acc["solves"] / args.steps,
               "solve_columns": acc["solve_columns"] / args.steps}
