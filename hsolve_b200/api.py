@@ -239,17 +239,30 @@ def _as_csr(m, name, storage):
             m = sp.csr_matrix(m.real)  # solved as real; the eigenvectors still come back complex
     else:
         m = sp.csr_matrix(m, dtype=np.float64)
-    m.eliminate_zeros()
+    # the caller's matrix is never modified: copy before any in-place clean-up
+    copied = False
+    if not m.has_canonical_format:
+        m = m.copy()
+        copied = True
+        m.sum_duplicates()
+    if m.nnz and not np.all(m.data):
+        if not copied:
+            m = m.copy()
+        m.eliminate_zeros()
     if storage == "upper":
         m = sp.triu(m) + sp.triu(m, 1).conj().T
     elif storage == "lower":
         m = sp.tril(m) + sp.tril(m, -1).conj().T
     elif storage == "auto":
-        up, lo = sp.triu(m, 1).nnz, sp.tril(m, -1).nnz
+        # entries strictly above / below the diagonal, counted on the CSR arrays
+        rows = np.repeat(np.arange(m.shape[0], dtype=m.indices.dtype), np.diff(m.indptr))
+        up = int(np.count_nonzero(m.indices > rows))
+        lo = int(np.count_nonzero(m.indices < rows))
         if (up == 0) != (lo == 0):
             m = sp.triu(m) + sp.triu(m, 1).conj().T if lo == 0 else sp.tril(m) + sp.tril(m, -1).conj().T
     m = sp.csr_matrix(m)
-    m.sum_duplicates()
+    if not m.has_canonical_format:
+        m.sum_duplicates()
     m.sort_indices()
     return m
 
@@ -278,14 +291,30 @@ def _complex_dtype(m) -> bool:
 
 
 def _hermitian_check(m, name, tol):
-    d = m - m.conj().T
-    nrm = np.sqrt((np.abs(m.data) ** 2).sum())
-    defect = np.sqrt((np.abs(d.data) ** 2).sum()) / nrm if nrm > 0 else 0.0
+    """||M - M^H||_F / ||M||_F of a canonical CSR matrix (sorted, no duplicates); raises
+    NotHermitianError above tol, else returns (M + M^H) / 2 (M itself when the defect is 0) and the
+    defect. With a structurally symmetric pattern M^H has M's index arrays, and the defect is an
+    entrywise difference of the two value arrays."""
+    import scipy.sparse as sp
+
+    t = m.T.tocsr()
+    t.sort_indices()
+    same = np.array_equal(t.indptr, m.indptr) and np.array_equal(t.indices, m.indices)
+    if same:
+        th = t.data.conj() if np.iscomplexobj(t.data) else t.data
+        dd = m.data - th
+    else:
+        dd = (m - m.conj().T).data
+    nrm = float(np.sqrt(np.vdot(m.data, m.data).real))
+    defect = float(np.sqrt(np.vdot(dd, dd).real)) / nrm if nrm > 0 else 0.0
     if defect > tol:
         raise NotHermitianError(f"{name}: ||M - M^H||_F / ||M||_F = {defect:.3e} > hermitian_tol = {tol:g}")
     if defect > 0:
-        m = ((m + m.conj().T) * 0.5).tocsr()
-        m.sort_indices()
+        if same:
+            m = sp.csr_matrix(((m.data + th) * 0.5, m.indices.copy(), m.indptr.copy()), shape=m.shape)
+        else:
+            m = ((m + m.conj().T) * 0.5).tocsr()
+            m.sort_indices()
     return m, defect
 
 
