@@ -10,7 +10,9 @@ solve of the case's target through a session `repeat` times. Each prints its wal
 `eigs`, the phase split of the solve report). The cases are the workloads of bench.py: box1e5 is
 the PEC box 44 x 34 x 26 (lengths 1 x 0.75 x 0.55, generalized form, n = 109,744, all eigenvalues in
 [40, 200]); cube20 is the PEC cube 20^3 (standard form, n = 21,660, 10 nearest to 25); cube70 is the
-PEC cube 70^3 (n = 999,810, 21 nearest to 1071.43, between two exact levels).
+PEC cube 70^3 (n = 999,810, 21 nearest to 1071.43, between two exact levels); nedelec1e5 is the PEC
+box 2 x 1 x 0.5 on 50 x 25 x 13 cells of six tetrahedra with lowest-order Nedelec elements
+(consistent, non-diagonal mass; n = 107,163), all eigenvalues in [40, 200].
 """
 from __future__ import annotations
 
@@ -19,20 +21,27 @@ import time
 
 import numpy as np
 
-from .gen import yee
+from .gen import nedelec, yee
+
+
+def _yee(box, form):
+    a, b = yee.pencil(box, form)
+    return a, (b if form == "generalized" else None)
+
 
 CASES = {
-    "box1e5": (yee.BOX_1E5, "generalized", dict(lower=40.0, upper=200.0)),
-    "cube20": (yee.CUBE20, "standard", dict(sigma=25.0, k=10)),
+    "box1e5": (lambda: _yee(yee.BOX_1E5, "generalized"), dict(lower=40.0, upper=200.0)),
+    "cube20": (lambda: _yee(yee.CUBE20, "standard"), dict(sigma=25.0, k=10)),
     # PEC cube 70^3, n = 999,810: 21 nearest to a shift midway between two exact levels
-    "cube70": (yee.Box((70, 70, 70)), "standard", dict(sigma=1071.4257927949998, k=21)),
+    "cube70": (lambda: _yee(yee.Box((70, 70, 70)), "standard"), dict(sigma=1071.4257927949998, k=21)),
+    "nedelec1e5": (lambda: nedelec.pencil(nedelec.BOX_2x1x05_1E5), dict(lower=40.0, upper=200.0)),
 }
 
 
 def _pencil(case):
-    box, form, target = CASES[case]
-    a, b = yee.pencil(box, form)
-    return a, (b if form == "generalized" else None), target
+    make, target = CASES[case]
+    a, b = make()
+    return a, b, target
 
 
 def factor(case: str, shift: float, repeat: int) -> None:
