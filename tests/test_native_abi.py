@@ -4,6 +4,7 @@ import re
 from pathlib import Path
 
 import numpy as np
+import pytest
 import scipy.sparse as sp
 
 from hsolve_b200 import _native
@@ -57,6 +58,43 @@ def test_symbolic_matches_oracle_fill():
     st2 = _native.symbolic_stats(a, pos, amalgamate=True)
     assert st2["supernodes"] < st["supernodes"]
     assert st["flops"] <= st2["flops"] <= 1.2 * st["flops"]
+
+
+def _brute_force_fill(a, pos):
+    """Column counts of L for the 1-based pivot positions `pos` by explicit elimination of the graph:
+    eliminating a vertex joins its not-yet-eliminated neighbours into a clique."""
+    n = a.shape[0]
+    order = np.argsort(pos)                      # pivot step -> vertex
+    step = np.empty(n, dtype=np.int64)
+    step[order] = np.arange(n)
+    g = sp.csr_matrix(abs(a) + abs(a.T))
+    adj = [set(g.indices[g.indptr[v]:g.indptr[v + 1]]) - {v} for v in range(n)]
+    counts = np.zeros(n, dtype=np.int64)
+    for v in order:
+        later = [u for u in adj[v] if step[u] > step[v]]
+        counts[step[v]] = len(later)
+        for u in later:
+            adj[u].update(w for w in later if w != u)
+    return counts
+
+
+@pytest.mark.parametrize("which", ["nd", "random", "natural"])
+def test_symbolic_matches_brute_force_elimination(which):
+    """nnz(L) and the RINFOG(1) flop count of the fundamental-supernode analysis equal an explicit
+    elimination of the graph on the same order."""
+    a, _ = yee.pencil(yee.Box((5, 4, 4)))
+    n = a.shape[0]
+    if which == "nd":
+        pos = _native.compute_ordering(a)
+    elif which == "random":
+        pos = (np.random.default_rng(1).permutation(n) + 1).astype(np.int32)
+    else:
+        pos = np.arange(1, n + 1, dtype=np.int32)
+    c = _brute_force_fill(a, pos)
+    st = _native.symbolic_stats(a, pos, amalgamate=False)
+    assert st["nnz_l"] == n + int(c.sum())
+    flops = float(np.sum(c + c * (c + 1)))
+    assert abs(st["flops"] - flops) <= 1e-12 * flops
 
 
 def test_nested_dissection_beats_natural_order():
