@@ -165,6 +165,10 @@ def merge_config(config, sigma, k, mode, lower, upper, tol, threads) -> dict:
         cfg["tol"] = _real(tol, "tol")
     if not isinstance(threads, _Default):
         cfg["threads"] = _integer(threads, "threads")
+    try:  # the config is a JSON document: no inf / nan anywhere in it
+        json.dumps(cfg, allow_nan=False)
+    except ValueError as e:
+        raise InvalidInputError(f"config: {e} (JSON has no inf/nan)") from None
     return cfg
 
 
