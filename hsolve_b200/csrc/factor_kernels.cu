@@ -309,106 +309,6 @@ __device__ int dense_bk(double* F, int ld, int m, int nfs, bool root, double u, 
   return st.j;
 }
 
-
-// Threshold Bunch-Kaufman on the panel's diagonal block (order w <= 32, shared memory, ld kNB, all
-// rows candidates): warp 0 decides each pivot (same rule as dense_bk), all warps share the rank-1/2
-// update of the remaining block (warp v owns the columns c = v (mod warps), lane i row i). Returns
-// the number of eliminated columns; block positions [e, w) could not be pivoted.
-__device__ int block_bk(double* F, int w, bool root, double u, double thr, int* lab, signed char* pv, StepShared& st) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  constexpr int ld = kNB;
-  if (threadIdx.x == 0) { st.j = 0; st.lim = w; st.prog = 0; st.force = 0; st.stop = 0; }
-  __syncthreads();
-  while (true) {
-    if (threadIdx.x == 0) {
-      st.stop = 0;
-      if (st.j >= w) st.stop = 1;
-      else if (st.j >= st.lim) {
-        if (st.prog) { st.lim = w; st.prog = 0; st.stop = 2; }
-        else if (root && !st.force) { st.force = 1; st.lim = w; st.stop = 2; }
-        else st.stop = 1;
-      }
-    }
-    __syncthreads();
-    if (st.stop == 1) break;
-    if (st.stop == 2) continue;
-    const int j = st.j;
-    if (warp == 0) {
-      decide_pivot(F, ld, w, w, j, u, thr, st.force != 0, st);
-      __syncwarp();
-      // swaps (warp 0)
-      const int dec = st.dec, r = st.r;
-      int p = -1, q = -1;
-      if (dec == kFail) { p = j; q = st.lim - 1; }
-      else if (dec == kOneR) { p = j; q = r; }
-      else if (dec == kTwoR) { p = j + 1; q = r; }
-      if (p >= 0 && p != q) {
-        if (p > q) { const int tt = p; p = q; q = tt; }
-        for (int t = lane; t < w + 1; t += 32) {
-          double *x = nullptr, *y = nullptr;
-          if (t < p) { x = F + p + t * ld; y = F + q + t * ld; }
-          else if (t > p && t < q) { x = F + t + p * ld; y = F + q + t * ld; }
-          else if (t > q && t < w) { x = F + t + p * ld; y = F + t + q * ld; }
-          else if (t == p) { x = F + p + p * ld; y = F + q + q * ld; }
-          if (x) { const double v = *x; *x = *y; *y = v; }
-        }
-        if (lane == 0) { const int tl = lab[p]; lab[p] = lab[q]; lab[q] = tl; }
-      }
-      if (lane == 0 && dec == kFail) st.lim -= 1;
-    }
-    __syncthreads();
-    const int dec = st.dec;
-    if (dec == kFail) continue;
-    if (dec == kTwoR) {
-      const double a = F[j + j * ld], b = F[j + 1 + j * ld], c = F[j + 1 + (j + 1) * ld];
-      const double det = a * c - b * b;
-      const double ia = c / det, ib = -b / det, ic = a / det;
-      // column values of the pair (before scaling), then the update, then the scaled L
-      const int i = lane;
-      const double x0 = (i >= j + 2 && i < w) ? F[i + j * ld] : 0.0;
-      const double x1 = (i >= j + 2 && i < w) ? F[i + (j + 1) * ld] : 0.0;
-      const double l0 = ia * x0 + ib * x1, l1 = ib * x0 + ic * x1;
-      for (int c2 = j + 2 + warp; c2 < w; c2 += nw) {
-        const double y0 = F[c2 + j * ld], y1 = F[c2 + (j + 1) * ld];
-        if (i >= c2 && i < w) F[i + c2 * ld] -= l0 * y0 + l1 * y1;
-      }
-      __syncthreads();
-      if (warp == 0 && i >= j + 2 && i < w) { F[i + j * ld] = l0; F[i + (j + 1) * ld] = l1; }
-      if (threadIdx.x == 0) {
-        if (det < 0) { st.neg++; st.pos++; } else if (a + c < 0) st.neg += 2; else st.pos += 2;
-        st.two++;
-        if (st.force) st.forced++;
-        pv[j] = 2; pv[j + 1] = 3;
-        st.j = j + 2; st.prog = 1; st.force = 0;
-        if (st.lim < st.j) st.lim = st.j;
-      }
-    } else {
-      const bool nul = dec == kNull;
-      const double d = F[j + j * ld];
-      const int i = lane;
-      const double x = (i > j && i < w) ? F[i + j * ld] : 0.0;
-      if (!nul) {
-        const double inv = 1.0 / d;
-        for (int c2 = j + 1 + warp; c2 < w; c2 += nw) {
-          const double y = F[c2 + j * ld];
-          if (i >= c2 && i < w) F[i + c2 * ld] -= x * y * inv;
-        }
-      }
-      __syncthreads();
-      if (warp == 0 && i > j && i < w) F[i + j * ld] = nul ? 0.0 : x / d;
-      if (threadIdx.x == 0) {
-        if (nul) { st.zero++; pv[j] = 0; }
-        else { if (d < 0) st.neg++; else st.pos++; pv[j] = 1; }
-        if (st.force) st.forced++;
-        st.j = j + 1; st.prog = 1; st.force = 0;
-        if (st.lim < st.j) st.lim = st.j;
-      }
-    }
-    __syncthreads();
-  }
-  return st.j;
-}
-
 // Warp maximum of non-negative floats: their bit patterns order like the values, so one integer
 // warp reduction replaces a shuffle tree.
 __device__ __forceinline__ float warp_maxf(float v) {
