@@ -8,7 +8,7 @@ import scipy.sparse as sp
 
 from hsolve_b200 import Factorization
 from hsolve_b200.gen import yee
-from oracle import yee_exact
+from oracle import ref, yee_exact
 from oracle.ldlt import OracleLDLT
 from tests.helpers import laplacian_1d, laplacian_2d, random_spd, random_symmetric, saddle_point
 
@@ -115,6 +115,31 @@ def test_saddle_point_needs_pivoting():
     assert inr.two_by_two + inr.delayed_pivots > 0
     b = np.random.default_rng(2).standard_normal((n, 2))
     assert backward_error(k, f.solve(b), b) < 1e-12
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built (make -C oracle ref)")
+def test_factorization_under_the_reference_pivot_order():
+    """The GPU factorization analysed with the reference's own nested-dissection PERM_IN (its
+    compute_ordering, built from its sources): inertia equal to the exact counts and to the oracle's
+    under the same order, and backward-stable solves."""
+    box = yee.Box((10, 9, 8))
+    a, _ = yee.pencil(box)
+    n = a.shape[0]
+    w = yee_exact.exact_spectrum(box.cells)
+    perm, _ = ref.compute_ordering(a)
+    gaps = np.flatnonzero(np.diff(w) > 1e-6 * w[-1])
+    shifts = [0.5 * (w[i] + w[i + 1]) for i in (gaps[gaps >= n // 3][0], gaps[gaps >= 2 * n // 3][0])]
+    f = Factorization()
+    f.analyze(a, None, 1.0, -shifts[0], pivot_order=perm)
+    o = OracleLDLT(a, order=np.argsort(perm).astype(np.int32))
+    for s in shifts:
+        assert f.factorize(1.0, -s)
+        inr = f.inertia()
+        k = (a - s * sp.identity(n)).tocsr()
+        ok, (oneg, ozero, _), _ = o.factorize(k)
+        assert ok and inr.valid and inr.neg == oneg == yee_exact.count_below(w, s) and inr.zero == ozero == 0
+        b = np.random.default_rng(1).standard_normal((n, 3))
+        assert backward_error(k, f.solve(b), b) < 1e-12
 
 
 def test_singular_shift_flagged(golden):
