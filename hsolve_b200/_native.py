@@ -65,6 +65,9 @@ SIGNATURES = {
     "hsg_set_null_pivot_detection": (ctypes.c_int, [_P, _I32]),
     "hsg_pivot_order": (ctypes.c_int, [_P, _P]),
     "hsg_order": (_I64, [_P]),
+    "hsg_spmm": (ctypes.c_int, [_I64, _P, _P, _P, _P, _I64, _P, _I64, _I64, _D, _D]),
+    "hsg_shifted_residual": (ctypes.c_int, [_I64, _P, _P, _P, _P, _P, _P, _D, _P, _I64, _P, _I64, _P, _I64, _I64,
+                                            _P]),
     "hsg_compute_ordering": (ctypes.c_int, [_I64, _P, _P, ctypes.c_uint64, _P]),
     "hsg_symbolic_stats": (ctypes.c_int, [_I64, _P, _P, _P, _I32, _P]),
 }
@@ -239,6 +242,45 @@ def symbolic_stats(A, pivot_order=None, amalgamate=True) -> dict:
     po = None if pivot_order is None else np.ascontiguousarray(pivot_order, dtype=np.int32)
     check(lib().hsg_symbolic_stats(A.shape[0], _ptr(rp), _ptr(ci), _ptr(po), int(amalgamate), ctypes.byref(e)))
     return {f: getattr(e, f) for f, _ in _Estimate._fields_}
+
+
+class DeviceCsr:
+    """A full (both triangles) CSR matrix copied to the current CUDA device for hsg_spmm /
+    hsg_shifted_residual; the device arrays are torch tensors (allocation only)."""
+
+    def __init__(self, m, device: str = "cuda:0"):
+        import scipy.sparse as sp
+        import torch
+
+        m = sp.csr_matrix(m, dtype=np.float64)
+        m.sum_duplicates()
+        m.sort_indices()
+        self.n = m.shape[0]
+        self.rp = torch.from_numpy(np.ascontiguousarray(m.indptr, dtype=np.int64)).to(device)
+        self.ci = torch.from_numpy(np.ascontiguousarray(m.indices, dtype=np.int32)).to(device)
+        self.v = torch.from_numpy(np.ascontiguousarray(m.data, dtype=np.float64)).to(device)
+
+    def ptrs(self):
+        return ctypes.c_void_p(self.rp.data_ptr()), ctypes.c_void_p(self.ci.data_ptr()), ctypes.c_void_p(self.v.data_ptr())
+
+
+def spmm_device(a: DeviceCsr, x, y, alpha: float = 1.0, beta: float = 0.0) -> None:
+    """y = alpha A x + beta y with x, y column-major device tensors (torch, shape (p, ld))."""
+    p, ldx = x.shape
+    check(lib().hsg_spmm(a.n, *a.ptrs(), ctypes.c_void_p(x.data_ptr()), ldx, ctypes.c_void_p(y.data_ptr()), y.shape[1],
+                         p, float(alpha), float(beta)))
+
+
+def shifted_residual_device(a: DeviceCsr, b, sigma: float, x, y, r, omega=None) -> None:
+    """r = B x - (A y - sigma B y) and omega (per column) on device tensors of shape (p, ld);
+    b None: B = I."""
+    p = x.shape[0]
+    bp = b.ptrs() if b is not None else (None, None, None)
+    check(lib().hsg_shifted_residual(a.n, *a.ptrs(), *bp, float(sigma), ctypes.c_void_p(x.data_ptr()), x.shape[1],
+                                     ctypes.c_void_p(y.data_ptr()), y.shape[1],
+                                     None if r is None else ctypes.c_void_p(r.data_ptr()),
+                                     a.n if r is None else r.shape[1], p,
+                                     None if omega is None else ctypes.c_void_p(omega.data_ptr())))
 
 
 def kernel_launches() -> int:

@@ -9,11 +9,15 @@
 #include <cstdint>
 #include <mutex>
 
+#include <math_constants.h>
+
 #include "blas_kernels.cuh"
 #include "common.hpp"
 #include "device.cuh"
 
 namespace hsg {
+
+void cuda_check(cudaError_t e, const char* what);
 
 namespace {
 
@@ -178,6 +182,89 @@ __global__ void k_fill_normal(std::int64_t n, int p, double* y, std::int64_t ldy
   }
 }
 
+// Shifted residual of a shift-invert solve, one warp per row and all P columns at once:
+//   r(i, c) = (B w_c)(i) - (A y_c)(i),  w = x + sigma y  (B = null: B = I),
+//   s(i, c) = (|B| |w_c|)(i) + (|A| |y_c|)(i),
+// and the componentwise backward error omega_c = max_i |r(i, c)| / s(i, c) with 0/0 = 0, r/0 = inf and
+// inf for a row whose r or s is not finite (the contract of hsolve's shifted_residual,
+// include/hsolve/sparse.hpp:157-174). omega must hold zeros at launch; the maximum is taken by an
+// integer atomic max on the bit patterns of non-negative doubles (order independent).
+template <int P>
+__global__ void k_shifted_residual(std::int64_t n, const std::int64_t* arp, const std::int32_t* aci, const double* av,
+                                   const std::int64_t* brp, const std::int32_t* bci, const double* bv, double sigma,
+                                   const double* x, std::int64_t ldx, const double* y, std::int64_t ldy, double* r,
+                                   std::int64_t ldr, int p, unsigned long long* omega) {
+  const int lane = threadIdx.x & 31;
+  const std::int64_t warp = (blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x) >> 5;
+  const std::int64_t nwarps = (static_cast<std::int64_t>(gridDim.x) * blockDim.x) >> 5;
+  double om[P];
+#pragma unroll
+  for (int c = 0; c < P; ++c) om[c] = 0.0;
+  for (std::int64_t i = warp; i < n; i += nwarps) {
+    double ra[P], sa[P];
+#pragma unroll
+    for (int c = 0; c < P; ++c) { ra[c] = 0.0; sa[c] = 0.0; }
+    for (std::int64_t q = arp[i] + lane; q < arp[i + 1]; q += 32) {
+      const double a = av[q];
+      const std::int64_t j = aci[q];
+#pragma unroll
+      for (int c = 0; c < P; ++c)
+        if (c < p) {
+          const double yj = y[j + c * ldy];
+          ra[c] = fma(-a, yj, ra[c]);
+          sa[c] = fma(fabs(a), fabs(yj), sa[c]);
+        }
+    }
+    if (brp) {
+      for (std::int64_t q = brp[i] + lane; q < brp[i + 1]; q += 32) {
+        const double b = bv[q];
+        const std::int64_t j = bci[q];
+#pragma unroll
+        for (int c = 0; c < P; ++c)
+          if (c < p) {
+            const double wj = fma(sigma, y[j + c * ldy], x[j + c * ldx]);
+            ra[c] = fma(b, wj, ra[c]);
+            sa[c] = fma(fabs(b), fabs(wj), sa[c]);
+          }
+      }
+    } else if (lane == 0) {
+#pragma unroll
+      for (int c = 0; c < P; ++c)
+        if (c < p) {
+          const double wi = fma(sigma, y[i + c * ldy], x[i + c * ldx]);
+          ra[c] += wi;
+          sa[c] += fabs(wi);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < P; ++c) {
+      if (c >= p) break;
+      const double rs = warp_sum(ra[c]);
+      const double ss = warp_sum(sa[c]);
+      if (lane == 0) {
+        if (r) r[i + c * ldr] = rs;
+        const double ar = fabs(rs);
+        double w;
+        if (!isfinite(rs) || !isfinite(ss)) w = CUDART_INF;
+        else if (ss > 0.0) w = ar / ss;
+        else w = ar > 0.0 ? CUDART_INF : 0.0;
+        om[c] = fmax(om[c], w);
+      }
+    }
+  }
+  if (omega && lane == 0) {
+#pragma unroll
+    for (int c = 0; c < P; ++c)
+      if (c < p && om[c] > 0.0) atomic_max_nonneg(&omega[c], om[c]);
+  }
+}
+
+// bits of a non-negative double array (atomic max slots) -> doubles, in place
+__global__ void k_bits_to_double(int p, unsigned long long* w) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < p) reinterpret_cast<double*>(w)[c] = __longlong_as_double(static_cast<long long>(w[c]));
+}
+
 // r = a - lam .* b (column c uses lam[c]); y holds r
 __global__ void k_residual_cols(std::int64_t n, int p, const double* ax, std::int64_t lda, const double* bx,
                                 std::int64_t ldb, const double* lam, double* r, std::int64_t ldr) {
@@ -317,6 +404,38 @@ void copy_cols(std::int64_t n, int p, const double* x, std::int64_t ldx, double*
 void fill_normal(std::int64_t n, int p, double* y, std::int64_t ldy, std::uint64_t seed, cudaStream_t s) {
   note_launches(1);
   k_fill_normal<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, y, ldy, seed);
+}
+
+void shifted_residual(const CsrDev& A, const CsrDev* B, double sigma, const double* x, std::int64_t ldx,
+                      const double* y, std::int64_t ldy, double* r, std::int64_t ldr, int p, double* omega,
+                      cudaStream_t s) {
+  if (p <= 0 || A.n == 0) return;
+  const int threads = 256;
+  const int blocks = grid_for(A.n * 32, threads);
+  if (omega) cuda_check(cudaMemsetAsync(omega, 0, static_cast<std::size_t>(p) * sizeof(double), s), "memset omega");
+  for (int c0 = 0; c0 < p; c0 += 8) {
+    const int pc = p - c0 < 8 ? p - c0 : 8;
+    const double* xc = x + c0 * ldx;
+    const double* yc = y + c0 * ldy;
+    double* rc = r ? r + c0 * ldr : nullptr;
+    unsigned long long* oc = omega ? reinterpret_cast<unsigned long long*>(omega + c0) : nullptr;
+    const std::int64_t* brp = B ? B->rp : nullptr;
+    const std::int32_t* bci = B ? B->ci : nullptr;
+    const double* bvv = B ? B->v : nullptr;
+    note_launches(1);
+    if (pc == 1)
+      k_shifted_residual<1><<<blocks, threads, 0, s>>>(A.n, A.rp, A.ci, A.v, brp, bci, bvv, sigma, xc, ldx, yc, ldy, rc, ldr, pc, oc);
+    else if (pc <= 2)
+      k_shifted_residual<2><<<blocks, threads, 0, s>>>(A.n, A.rp, A.ci, A.v, brp, bci, bvv, sigma, xc, ldx, yc, ldy, rc, ldr, pc, oc);
+    else if (pc <= 4)
+      k_shifted_residual<4><<<blocks, threads, 0, s>>>(A.n, A.rp, A.ci, A.v, brp, bci, bvv, sigma, xc, ldx, yc, ldy, rc, ldr, pc, oc);
+    else
+      k_shifted_residual<8><<<blocks, threads, 0, s>>>(A.n, A.rp, A.ci, A.v, brp, bci, bvv, sigma, xc, ldx, yc, ldy, rc, ldr, pc, oc);
+  }
+  if (omega) {
+    note_launches(1);
+    k_bits_to_double<<<(p + 127) / 128, 128, 0, s>>>(p, reinterpret_cast<unsigned long long*>(omega));
+  }
 }
 
 void residual_cols(std::int64_t n, int p, const double* ax, std::int64_t lda, const double* bx, std::int64_t ldb,

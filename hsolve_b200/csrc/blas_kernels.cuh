@@ -35,6 +35,12 @@ void diag_scale(std::int64_t n, int p, const double* d, const double* x, std::in
 void copy_cols(std::int64_t n, int p, const double* x, std::int64_t ldx, double* y, std::int64_t ldy, cudaStream_t s);
 // standard normal entries from a counter-based stream (deterministic in seed)
 void fill_normal(std::int64_t n, int p, double* y, std::int64_t ldy, std::uint64_t seed, cudaStream_t s);
+// R = B (X + sigma Y) - A Y (B == null: B = I) for p columns in one sweep over the rows of A and B,
+// and omega[c] = max_i |R(i, c)| / (|B| |X + sigma Y| + |A| |Y|)(i, c), the componentwise backward
+// error of every column (device array of p doubles, or null). r may be null (omega only).
+void shifted_residual(const CsrDev& A, const CsrDev* B, double sigma, const double* x, std::int64_t ldx,
+                      const double* y, std::int64_t ldy, double* r, std::int64_t ldr, int p, double* omega,
+                      cudaStream_t s);
 void residual_cols(std::int64_t n, int p, const double* ax, std::int64_t lda, const double* bx, std::int64_t ldb,
                    const double* lam, double* r, std::int64_t ldr, cudaStream_t s);
 

@@ -81,7 +81,11 @@ int hsg_count(hsg_factor* f, double alpha, double beta, int32_t detection, hsg_i
 }
 
 int hsg_solve(hsg_factor* f, double* b, int64_t nrhs, int64_t ldb, int32_t b_on_device) {
-  return guarded([&] { get(f).solve(b, nrhs, ldb, b_on_device != 0); });
+  return guarded([&] {
+    GpuFactor& g = get(f);
+    if (b_on_device) g.order_after_legacy_stream();
+    g.solve(b, nrhs, ldb, b_on_device != 0);
+  });
 }
 
 int hsg_inertia(const hsg_factor* f, hsg_inertia_t* out) {

@@ -149,6 +149,13 @@ GpuFactor::GpuFactor(const hsg_options_t& opt) : opt_(opt) {
   cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   cuda_check(cudaEventCreate(&ev0_), "cudaEventCreate");
   cuda_check(cudaEventCreate(&ev1_), "cudaEventCreate");
+  cuda_check(cudaEventCreateWithFlags(&ev_in_, cudaEventDisableTiming), "cudaEventCreate");
+}
+
+void GpuFactor::order_after_legacy_stream() {
+  DeviceGuard g(opt_.device);
+  cuda_check(cudaEventRecord(ev_in_, cudaStreamLegacy), "event on the default stream");
+  cuda_check(cudaStreamWaitEvent(stream_, ev_in_, 0), "wait for the default stream");
 }
 
 GpuFactor::~GpuFactor() {
@@ -159,6 +166,7 @@ GpuFactor::~GpuFactor() {
   }
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
+  if (ev_in_) cudaEventDestroy(ev_in_);
 }
 
 void GpuFactor::analyze(std::int64_t n, const std::int64_t* a_rp, const std::int32_t* a_ci, const double* a_v,

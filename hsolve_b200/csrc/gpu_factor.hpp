@@ -84,6 +84,10 @@ class GpuFactor {
   // the caller's `scratch` (`cap` doubles, on this factorization's device). Allocates no device
   // memory; every scratch entry is written before it is read, so nothing needs to start at zero.
   void solve_with_scratch(double* b_dev, std::int64_t nrhs, std::int64_t ldb, double* scratch, std::size_t cap);
+  // Orders the handle's stream (a non-blocking stream) after all work queued so far on the legacy
+  // default stream, where a caller's own copies into a device right-hand side usually run; work on
+  // the caller's other streams must be complete before a device solve is called.
+  void order_after_legacy_stream();
   void release();
   hsg_estimate_t estimate() const;
   const hsg_inertia_t& inertia() const { return inertia_; }
@@ -142,7 +146,7 @@ class GpuFactor {
   hsg_inertia_t inertia_{};
   double last_factor_s_ = 0.0, last_solve_s_ = 0.0;
   DeviceStats dstats_;
-  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, ev_in_ = nullptr;
   std::int64_t vec_total_ = 0;
 
   DevBuf<std::int32_t> d_row_, d_col_, d_rmap_, d_rows_, d_child_ptr_, d_children_, d_iperm_, d_lists_, d_pidx_,

@@ -8,6 +8,8 @@
 // a plain pointer. The solve writes every scratch entry it reads (the gathered right-hand sides and
 // the children's update vectors), so the array keeps the last call's contents and none of it has to
 // be cleared between calls. Calls on one device share the array: calls whose GPU work overlaps race.
+#include <algorithm>
+#include <cstdint>
 #include <mutex>
 
 #include <cuda_runtime.h>
@@ -55,12 +57,30 @@ extern "C" int hsg_solve_static(hsg_factor* f, double* b_device, int64_t nrhs, i
   return hsg::guarded([&] {
     hsg::GpuFactor& g = hsg::factor_of(f);
     HSG_REQUIRE(nrhs >= 0, HSG_INVALID_INPUT, "hsg_solve_static: nrhs < 0");
+    // the right-hand sides alone (n per column) must fit before the exact size is formed, so that
+    // a huge nrhs cannot overflow the 64-bit product below
+    const std::int64_t n = std::max<std::int64_t>(1, g.order());
+    HSG_REQUIRE(nrhs <= static_cast<std::int64_t>(kScratchDoubles) / n, HSG_INVALID_INPUT,
+                "hsg_solve_static: " << nrhs << " right-hand sides of order " << g.order()
+                                     << " exceed what the static array holds (" << kScratchDoubles * 8
+                                     << " bytes); split the right-hand sides or use hsg_solve");
     const std::size_t need = nrhs > 0 ? g.solve_scratch_doubles(nrhs) : 0;
     HSG_REQUIRE(need <= kScratchDoubles, HSG_INVALID_INPUT,
                 "hsg_solve_static: " << nrhs << " right-hand sides of order " << g.order() << " need " << need * 8
                                      << " bytes of scratch, the static array holds " << kScratchDoubles * 8
                                      << "; split the right-hand sides or use hsg_solve");
     if (nrhs == 0) return;
+    HSG_REQUIRE(b_device, HSG_INVALID_INPUT, "hsg_solve_static: null right-hand side");
+    // b must be device (or managed) memory of the factorization's device: a host pointer or another
+    // device's memory would make the solve kernels fault
+    cudaPointerAttributes attr{};
+    const cudaError_t pe = cudaPointerGetAttributes(&attr, b_device);
+    if (pe != cudaSuccess) cudaGetLastError();  // clear the sticky-free error of an unknown pointer
+    HSG_REQUIRE(pe == cudaSuccess &&
+                    (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged) &&
+                    attr.device == g.device(),
+                HSG_INVALID_INPUT, "hsg_solve_static: b_device is not device memory of device " << g.device());
+    g.order_after_legacy_stream();
     g.solve_with_scratch(b_device, nrhs, ldb, scratch_on(g.device()), kScratchDoubles);
   });
 }

@@ -116,7 +116,11 @@ HSG_API int hsg_factorize(hsg_factor* f, double alpha, double beta, hsg_inertia_
 HSG_API int hsg_count(hsg_factor* f, double alpha, double beta, int32_t detection, hsg_inertia_t* out);
 
 /* SparseFactorization::solve(b, nrhs, ldb) (factor.hpp:394-398): K X = B in place, column-major,
- * ldb >= n. b_on_device: 0 host memory, 1 device memory of the handle's device. */
+ * ldb >= n. b_on_device: 0 host memory, 1 device memory of the handle's device.
+ * Stream contract of a device b: the solve runs on the handle's own (non-blocking) stream, ordered
+ * after the work already queued on the legacy default stream (stream 0) when the call is made; a
+ * caller that writes b on any other stream must complete that work (cudaStreamSynchronize, or an
+ * event it waits on) before the call. The call returns after the solve has finished on the GPU. */
 HSG_API int hsg_solve(hsg_factor* f, double* b, int64_t nrhs, int64_t ldb, int32_t b_on_device);
 
 /* The same solve as hsg_solve with b in device memory, for callers that must not allocate device
@@ -131,6 +135,9 @@ HSG_API int hsg_solve(hsg_factor* f, double* b, int64_t nrhs, int64_t ldb, int32
  * that first call before any stream capture). All calls on a device share the one array, so two
  * calls whose GPU work overlaps (from different host threads) race and give wrong results;
  * calls from one thread are safe because each call waits for its GPU work before returning.
+ * b_device must be device (or managed) memory of the handle's device (HSG_INVALID_INPUT otherwise),
+ * and the stream contract of a device b in hsg_solve applies: work on streams other than the legacy
+ * default stream that writes b_device must be complete before the call.
  * No counterpart in hsolve. */
 #define HSG_SOLVE_STATIC_SCRATCH_BYTES (16u << 20)
 HSG_API int hsg_solve_static(hsg_factor* f, double* b_device, int64_t nrhs, int64_t ldb);
@@ -153,6 +160,27 @@ HSG_API int64_t hsg_order(const hsg_factor* f);
 /* Measured FP64 FMA throughput of the device (TFLOP/s), the denominator of the factorization's
  * roofline (instrumentation; no counterpart in hsolve). */
 HSG_API int hsg_fp64_peak_probe(int32_t device, double* tflops);
+
+/* ------------------------------------------------------- sparse kernels on device pointers */
+/* The CSR arguments below hold FULL matrices (both triangles; int64 row pointers, int32 columns,
+ * double values) in device memory of the current CUDA device, as do x, y and r (column-major).
+ * Each call runs on the legacy default stream (ordered after the caller's work queued there) and
+ * returns when its GPU work has finished. */
+
+/* hs::spmm (include/hsolve/sparse.hpp:140-147): Y = alpha A X + beta Y for p columns; beta == 0
+ * never reads Y. */
+HSG_API int hsg_spmm(int64_t n, const int64_t* a_rowptr, const int32_t* a_col, const double* a_val,
+                     const double* x, int64_t ldx, double* y, int64_t ldy, int64_t p, double alpha, double beta);
+
+/* hs::shifted_residual (include/hsolve/sparse.hpp:149-174): R = B X - (A Y - sigma B Y) for p
+ * columns (b_rowptr == NULL: B = I), computed as B (X + sigma Y) - A Y in one sweep over the rows,
+ * and, when backward_error is not NULL (device, p doubles), every column's componentwise backward
+ * error omega_k = max_i |r_ik| / (|B| |x_k + sigma y_k| + |A| |y_k|)_i with 0/0 = 0, r/0 = inf and
+ * inf for a row whose r or s is not finite. r may be NULL (backward errors only). */
+HSG_API int hsg_shifted_residual(int64_t n, const int64_t* a_rowptr, const int32_t* a_col, const double* a_val,
+                                 const int64_t* b_rowptr, const int32_t* b_col, const double* b_val, double sigma,
+                                 const double* x, int64_t ldx, const double* y, int64_t ldy, double* r, int64_t ldr,
+                                 int64_t p, double* backward_error);
 
 /* ----------------------------------------------------------------- host-only (no GPU needed) */
 

@@ -1,9 +1,9 @@
 """Regenerate the golden fixtures of tests/golden from the reference (hsolve) checkout.
 
-Run in a container that has the reference at REF (default /root/reference); the fixtures it writes
-are committed, so the tests never read the reference at run time:
+Run in a container that has a checkout of the reference; its path REF is a required argument. The
+fixtures it writes are committed, so the tests never read the reference at run time:
 
-    python tests/golden/make_golden.py [REF]
+    python tests/golden/make_golden.py REF
 
 Fixtures
 * yee_spectra.npz   exact discrete Yee spectra from the reference's own closed form
@@ -39,7 +39,7 @@ def digest(m) -> dict:
                                              + np.ascontiguousarray(m.indptr.astype(np.int64)).tobytes()).hexdigest()}
 
 
-def main(ref: str = "/root/reference") -> None:
+def main(ref: str) -> None:
     sys.path.insert(0, ref)
     from tools.gen import yee as R  # the reference generator
 
@@ -123,4 +123,6 @@ def main(ref: str = "/root/reference") -> None:
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py REF  (path of the reference checkout)")
+    main(sys.argv[1])

@@ -41,6 +41,7 @@ def test_static_solve_matches_hsg_solve_twice_in_a_row(cells, sigma, nrhs):
         ld = n + 5  # a leading dimension larger than n
         dev = torch.zeros((nrhs, ld), dtype=torch.float64, device="cuda:0")
         dev[:, :n] = torch.from_numpy(b.T.copy())
+        torch.cuda.synchronize()  # the copy into dev is complete before the solve reads it
         f.solve_static(dev.data_ptr(), nrhs, ld)
         torch.cuda.synchronize()
         got = dev[:, :n].cpu().numpy().T
@@ -48,6 +49,52 @@ def test_static_solve_matches_hsg_solve_twice_in_a_row(cells, sigma, nrhs):
         assert np.all(dev[:, n:].cpu().numpy() == 0.0)  # rows past n untouched
         be = np.abs(k @ got - b).max() / (abs(k).sum(axis=0).max() * np.abs(got).max())
         assert be < 1e-12, be
+    f.close()
+
+
+def test_first_solve_of_a_fresh_factorization_allocates_nothing():
+    """The first solve after a factorization also builds the solve operators; through
+    hsg_solve_static it does so without allocating device memory, and its result matches the
+    oracle's solve."""
+    import torch
+
+    from oracle.ldlt import OracleLDLT
+
+    warm, _ = _factor((6, 5, 4), 20.5)  # loads the library's kernels and the static array
+    wn = warm.order()
+    wb = torch.ones((1, wn), dtype=torch.float64, device="cuda:0")
+    torch.cuda.synchronize()
+    warm.solve_static(wb.data_ptr(), 1, wn)
+    warm.close()
+
+    cells, sigma, nrhs = (12, 10, 9), 47.3, 4
+    f, k = _factor(cells, sigma)  # factorized, never solved
+    n = k.shape[0]
+    b = np.random.default_rng(3).standard_normal((n, nrhs))
+    dev = torch.from_numpy(b.T.copy()).to("cuda:0")
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    f.solve_static(dev.data_ptr(), nrhs, n)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0, (free0, free1)
+    got = dev.cpu().numpy().T
+    a, _ = yee.pencil(yee.Box(cells))
+    ok, _, _ = (o := OracleLDLT(a)).factorize(k)
+    assert ok
+    want = o.solve(b)
+    assert np.allclose(got, want, rtol=1e-10, atol=1e-10 * np.abs(want).max())
+    f.close()
+
+
+def test_static_solve_rejects_host_memory_and_huge_counts():
+    f, _ = _factor((6, 5, 4), 20.5)
+    n = f.order()
+    host = np.zeros((2, n))
+    status = _native.lib().hsg_solve_static(f._h, ctypes.c_void_p(host.ctypes.data), 2, n)
+    assert status == 1 and "not device memory" in _native.lib().hsg_last_error().decode()
+    status = _native.lib().hsg_solve_static(f._h, ctypes.c_void_p(host.ctypes.data), 1 << 62, n)
+    assert status == 1 and "static array holds" in _native.lib().hsg_last_error().decode()
     f.close()
 
 
