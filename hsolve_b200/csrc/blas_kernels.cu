@@ -259,6 +259,28 @@ __global__ void k_shifted_residual(std::int64_t n, const std::int64_t* arp, cons
   }
 }
 
+// z = x + y (p columns)
+__global__ void k_add_cols(std::int64_t n, int p, const double* x, std::int64_t ldx, const double* y,
+                           std::int64_t ldy, double* z, std::int64_t ldz) {
+  const std::int64_t total = n * p;
+  for (std::int64_t t = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
+    const std::int64_t i = t % n, c = t / n;
+    z[i + c * ldz] = x[i + c * ldx] + y[i + c * ldy];
+  }
+}
+
+// y(:, c) = x(:, c) for the columns with mask bit c set (p <= 32)
+__global__ void k_copy_cols_masked(std::int64_t n, int p, unsigned mask, const double* x, std::int64_t ldx, double* y,
+                                   std::int64_t ldy) {
+  const std::int64_t total = n * p;
+  for (std::int64_t t = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
+    const std::int64_t i = t % n, c = t / n;
+    if ((mask >> c) & 1u) y[i + c * ldy] = x[i + c * ldx];
+  }
+}
+
 // bits of a non-negative double array (atomic max slots) -> doubles, in place
 __global__ void k_bits_to_double(int p, unsigned long long* w) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -436,6 +458,20 @@ void shifted_residual(const CsrDev& A, const CsrDev* B, double sigma, const doub
     note_launches(1);
     k_bits_to_double<<<(p + 127) / 128, 128, 0, s>>>(p, reinterpret_cast<unsigned long long*>(omega));
   }
+}
+
+void add_cols(std::int64_t n, int p, const double* x, std::int64_t ldx, const double* y, std::int64_t ldy, double* z,
+              std::int64_t ldz, cudaStream_t s) {
+  if (p <= 0 || n <= 0) return;
+  note_launches(1);
+  k_add_cols<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, x, ldx, y, ldy, z, ldz);
+}
+
+void copy_cols_masked(std::int64_t n, int p, unsigned mask, const double* x, std::int64_t ldx, double* y,
+                      std::int64_t ldy, cudaStream_t s) {
+  if (p <= 0 || n <= 0 || mask == 0u) return;
+  note_launches(1);
+  k_copy_cols_masked<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, mask, x, ldx, y, ldy);
 }
 
 void residual_cols(std::int64_t n, int p, const double* ax, std::int64_t lda, const double* bx, std::int64_t ldb,

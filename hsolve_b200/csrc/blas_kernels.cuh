@@ -41,6 +41,12 @@ void fill_normal(std::int64_t n, int p, double* y, std::int64_t ldy, std::uint64
 void shifted_residual(const CsrDev& A, const CsrDev* B, double sigma, const double* x, std::int64_t ldx,
                       const double* y, std::int64_t ldy, double* r, std::int64_t ldr, int p, double* omega,
                       cudaStream_t s);
+// z = x + y (p columns)
+void add_cols(std::int64_t n, int p, const double* x, std::int64_t ldx, const double* y, std::int64_t ldy, double* z,
+              std::int64_t ldz, cudaStream_t s);
+// y(:, c) = x(:, c) for every column c < p whose bit is set in mask (p <= 32)
+void copy_cols_masked(std::int64_t n, int p, unsigned mask, const double* x, std::int64_t ldx, double* y,
+                      std::int64_t ldy, cudaStream_t s);
 void residual_cols(std::int64_t n, int p, const double* ax, std::int64_t lda, const double* bx, std::int64_t ldb,
                    const double* lam, double* r, std::int64_t ldr, cudaStream_t s);
 

@@ -84,15 +84,130 @@ struct SpmvOp : KrylovOperator {
   }
 };
 
+// An operator application with an FP32 factor whose refinement did not reach the accuracy the
+// driver needs (hsolve's InexactFactorFailure, src/driver/steps.cpp:133-143): the solve falls back
+// to FP64 factors.
+struct InexactFactorFailure : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+// Refinement policy of applications with an inexact (FP32) factor (hsolve SolveRefinement,
+// include/hsolve/operator.hpp:51-57, with the driver's values, src/driver/internal.hpp:233-236):
+// at most 10 corrections per apply, a column is done at ||r|| <= 0.1 tol_inner ||B x|| or when its
+// componentwise backward error is at the rounding level (8 eps); a correction that does not reduce
+// ||r|| is discarded (every column keeps its best iterate).
+constexpr int kRefineSteps = 10;
+constexpr double kRefineTolFactor = 0.1;
+constexpr double kRoundingLevel = 8.0 * std::numeric_limits<double>::epsilon();
+
 struct ShiftInvertOp : KrylovOperator {
   Problem& P;
   GpuFactor& F;
   long long columns = 0;
+  // refinement (FP32 factors): sigma of the factor, relative tolerances, statistics
+  bool refine = false;
+  double sigma = 0.0, rel_tol = 0.0, accept_rel = 0.0;
+  long long refine_steps = 0, refined_applies = 0;
+  double worst_rel = 0.0, worst_omega = 0.0;
+  DevBuf<double> R, C, stats;
   ShiftInvertOp(Problem& pr, GpuFactor& f) : P(pr), F(f) {}
+  void set_refinement(double sig, double tol_inner) {
+    refine = F.single();
+    sigma = sig;
+    rel_tol = tol_inner * kRefineTolFactor;
+    accept_rel = tol_inner;
+  }
   void apply(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p) override {
     P.bprod(x, ldx, y, ldy, p);
-    F.solve(y, p, ldy, true);
+    if (!refine) {
+      F.solve(y, p, ldy, true);
+      columns += p;
+      return;
+    }
+    apply_refined(x, ldx, y, ldy, p);
     columns += p;
+  }
+  // Y = K^{-1} B X with the FP32 factor K~ of K = A - sigma B and FP64 iterative refinement
+  // y <- y + K~^{-1} (B x - K y), the residual r = B (x + sigma y) - A y from the FP64 pencil in one
+  // sweep (ShiftInvertOperator::do_apply, hsolve src/ops/shift_invert_operator.cpp:83-177).
+  void apply_refined(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p) {
+    const std::int64_t n = P.n;
+    cudaStream_t s = P.s;
+    R.alloc(static_cast<std::size_t>(n) * p);
+    C.alloc(static_cast<std::size_t>(n) * p);
+    stats.alloc(3 * static_cast<std::size_t>(p));  // ||Bx||^2 | ||r||^2 | omega
+    double* bxn = stats.p;
+    double* rn = stats.p + p;
+    double* om = stats.p + 2 * p;
+    const CsrDev A = P.A.view(n);
+    const CsrDev B = P.B.view(n);
+    const CsrDev* Bp = P.b_identity ? nullptr : &B;
+    col_dots(n, p, y, ldy, y, ldy, bxn, s);  // y = B x here
+    F.solve(y, p, ldy, true);
+    shifted_residual(A, Bp, sigma, x, ldx, y, ldy, R.p, n, p, om, s);
+    col_dots(n, p, R.p, n, R.p, n, rn, s);
+    std::vector<double> h(3 * static_cast<std::size_t>(p));
+    auto fetch = [&] {
+      cuda_check(cudaMemcpyAsync(h.data(), stats.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s), "refine stats");
+      cuda_check(cudaStreamSynchronize(s), "refine stats");
+    };
+    fetch();
+    std::vector<double> bx(p), rel(p), omega(p);
+    std::vector<char> active(p);
+    int remaining = 0;
+    auto relative = [&](int k) {
+      const double r = std::sqrt(h[p + k]);
+      if (r == 0.0) return 0.0;
+      return bx[k] > 0.0 ? r / bx[k] : std::numeric_limits<double>::infinity();
+    };
+    for (int k = 0; k < p; ++k) {
+      bx[k] = std::sqrt(h[k]);
+      rel[k] = relative(k);
+      omega[k] = h[2 * p + k];
+      active[k] = rel[k] > rel_tol && omega[k] > kRoundingLevel;
+      remaining += active[k];
+    }
+    for (int step = 0; step < kRefineSteps && remaining > 0; ++step) {
+      // corrections of all p columns in one block solve (the solve's time hardly depends on the
+      // column count), candidates y + K~^{-1} r and their residuals
+      F.solve(R.p, p, n, true);
+      add_cols(n, p, y, ldy, R.p, n, C.p, n, s);
+      shifted_residual(A, Bp, sigma, x, ldx, C.p, n, R.p, n, p, om, s);
+      col_dots(n, p, R.p, n, R.p, n, rn, s);
+      ++refine_steps;
+      fetch();
+      unsigned take = 0u;
+      for (int k = 0; k < p; ++k) {
+        if (!active[k]) continue;
+        const double cr = relative(k);
+        if (cr < rel[k]) {
+          take |= 1u << k;
+          rel[k] = cr;
+          omega[k] = h[2 * p + k];
+          if (cr > rel_tol && omega[k] > kRoundingLevel) continue;
+        }
+        active[k] = 0;  // converged, at the rounding level, or the correction was rejected
+        --remaining;
+      }
+      copy_cols_masked(n, p, take, C.p, n, y, ldy, s);
+    }
+    ++refined_applies;
+    double wr = 0.0, wo = 0.0;
+    bool converged = true;
+    for (int k = 0; k < p; ++k) {
+      wr = std::max(wr, rel[k]);
+      wo = std::max(wo, omega[k]);
+      converged = converged && (rel[k] <= rel_tol || omega[k] <= kRoundingLevel);
+    }
+    worst_rel = std::max(worst_rel, wr);
+    worst_omega = std::max(worst_omega, wo);
+    if (!converged && !(wr <= accept_rel)) {
+      std::ostringstream os;
+      os.precision(3);
+      os << "the refinement of an operator application at sigma = " << sigma << " did not converge (relative residual "
+         << wr << ", backward error " << wo << "): eps_factor * cond(K) is too large at this shift";
+      throw InexactFactorFailure(os.str());
+    }
   }
   bool b_identity() const override { return P.b_identity; }
   void bprod(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p) override { P.bprod(x, ldx, y, ldy, p); }
@@ -286,6 +401,18 @@ struct Session::Impl {
     }
     return *C[i];
   }
+  // the FP32 operator factorization of the mixed-precision path (same analysis), created at first use
+  std::unique_ptr<GpuFactor> FS;
+  GpuFactor& single_op() {
+    if (!FS) {
+      hsg_options_t o = fopt;
+      o.precision = 1;
+      auto g = std::make_unique<GpuFactor>(o);
+      g->analyze_like(*F);
+      FS = std::move(g);
+    }
+    return *FS;
+  }
   Problem P;
   std::string problem = "HEP";
   double scale = 0.0;
@@ -364,7 +491,26 @@ std::int64_t Session::order() const { return d_->a.n; }
 
 hsg_estimate_t Session::estimate() const { return d_->F->estimate(); }
 
+// factor_precision = single: the shift factorizations that serve the operator are FP32 with FP64
+// refinement of every application; the inertia counts stay FP64. As in hsolve (solver.hpp:116-126),
+// the attempt is abandoned for FP64 factors when an application's refinement does not converge or
+// the result is not accepted (a pair above tol or a failed certificate).
 SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
+  if (cfg.factor_precision != 1) return solve_once(cfg, include_setup, "");
+  std::string why;
+  try {
+    SolveOutput out = solve_once(cfg, include_setup, "");
+    if (out.report_json.find("\"success\":true") != std::string::npos) return out;
+    why = "the single-precision result was not accepted";
+  } catch (const InexactFactorFailure& e) {
+    why = e.what();
+  }
+  hsg_solve_config_t c2 = cfg;
+  c2.factor_precision = 0;
+  return solve_once(c2, include_setup, why);
+}
+
+SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setup, const std::string& fallback) {
   const auto t_start = Clock::now();
   Impl& S = *d_;
   Timers tm;
@@ -378,12 +524,19 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
   HSG_REQUIRE(cfg.device == S.device, HSG_INVALID_INPUT, "config device differs from the session's device");
   GpuFactor& F = *S.F;
   Problem& P = S.P;
+  // the factorization object that serves the operator: F itself (FP64), or the FP32 object of the
+  // mixed-precision path; F, C0 and C1 keep every inertia count in FP64
+  const bool single = cfg.factor_precision == 1;
+  GpuFactor& OPF = single ? S.single_op() : F;
   F.reset_device_stats();
+  if (single) OPF.reset_device_stats();
   const long long launches0 = hsg_kernel_launches();
   const double scale = S.scale;
   const std::string problem = S.problem;
   std::vector<std::string> warnings;
-  ShiftInvertOp op(P, F);
+  if (!fallback.empty()) warnings.push_back("single-precision factors abandoned: " + fallback);
+  ShiftInvertOp op(P, OPF);
+  const double tol_inner = cfg.tol * cfg.inner_tol_factor;
   SolveOutput out;
   out.n = n;
   Certificate cert;
@@ -405,15 +558,17 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
     HSG_REQUIRE(k >= 1 && k < n, HSG_INVALID_INPUT, "k must be in [1, n)");
     double sigma = cfg.sigma;
     HSG_REQUIRE(std::isfinite(sigma), HSG_INVALID_INPUT, "sigma must be finite");
-    if (!factorize_at(F, sigma, scale, cfg.max_shift_retries, shift_retries, tm))
+    if (!factorize_at(OPF, sigma, scale, cfg.max_shift_retries, shift_retries, tm))
       HSG_THROW(HSG_SINGULAR, "A - sigma B is numerically singular at and near sigma = " << cfg.sigma);
+    op.set_refinement(sigma, tol_inner);
     sigma_used = sigma;
     int nev = static_cast<int>(std::min<std::int64_t>(n - 1, k + std::max<std::int64_t>(4, (k + 1) / 2)));
     const int p = cfg.block_size > 0 ? cfg.block_size : auto_block(nev);
     block_used = p;
     for (int attempt = 0; attempt < 4; ++attempt) {
-      // reruns keep F's factorization at sigma when the certificate's counts ran on other objects
-      if (f_stale && !factorize_at(F, sigma, scale, cfg.max_shift_retries, shift_retries, tm))
+      // reruns keep the operator's factorization at sigma when the certificate's counts ran on
+      // other objects
+      if (f_stale && !factorize_at(OPF, sigma, scale, cfg.max_shift_retries, shift_retries, tm))
         HSG_THROW(HSG_SINGULAR, "A - sigma B is numerically singular at the working shift");
       f_stale = false;
       NearestRun run = run_krylov(op, P, sigma, nev, static_cast<int>(k), cfg, p, cfg.seed + attempt, tm);
@@ -464,7 +619,7 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
           // plain path: the counts overwrite F's factorization, so a rerun refactorizes
           nlo = count_below(F, lo_m, scale, -1.0, moves, tm);
           nhi = count_below(F, hi_m, scale, +1.0, moves, tm);
-          f_stale = true;
+          f_stale = &OPF == &F;
         }
         cnt = nhi - nlo;
         lo = lo_m;
@@ -521,7 +676,7 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
       auto f_lo = std::async(std::launch::async, [&] { return count_below(C0, lo, scale, -1.0, moves, t_lo, true); });
       auto f_hi = std::async(std::launch::async, [&] { return count_below(C1, hi, scale, +1.0, moves_hi, t_hi, true); });
       try {
-        mid_ok = factorize_at(F, sigma_mid, scale, cfg.max_shift_retries, shift_retries, tm, true);
+        mid_ok = factorize_at(OPF, sigma_mid, scale, cfg.max_shift_retries, shift_retries, tm, true);
       } catch (...) {
         f_lo.wait();
         f_hi.wait();
@@ -550,10 +705,13 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
     std::vector<double> cuts{lo, hi};
     std::vector<long long> below{nlo, nhi};
     const long long target = cfg.slice_size > 0 ? cfg.slice_size : 96;
-    bool spec_slice = mid_ok;  // F holds the factorization at sigma_mid
+    bool spec_slice = mid_ok;  // OPF holds the factorization at sigma_mid
     if (N > target && mid_ok && sigma_mid > lo && sigma_mid < hi) {
-      cuts.insert(cuts.begin() + 1, sigma_mid);
-      below.insert(below.begin() + 1, F.inertia().neg);
+      // the midpoint becomes the first cut; its count must be an FP64 one
+      double cut = sigma_mid;
+      const long long nm = single ? count_below(F, cut, scale, +1.0, cert.endpoint_moves, tm) : F.inertia().neg;
+      cuts.insert(cuts.begin() + 1, cut);
+      below.insert(below.begin() + 1, nm);
       spec_slice = false;
     }
     // split slices with too many eigenvalues at their midpoint (one count per cut)
@@ -580,10 +738,11 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
       if (spec_slice && cuts.size() == 2) {
         sigma = sigma_mid;  // factorized while the window ends were counted
         spec_slice = false;
-      } else if (!factorize_at(F, sigma, scale, cfg.max_shift_retries, shift_retries, tm)) {
+      } else if (!factorize_at(OPF, sigma, scale, cfg.max_shift_retries, shift_retries, tm)) {
         HSG_THROW(HSG_SINGULAR, "slice shift singular near " << rec.sigma);
       }
       rec.sigma = sigma;
+      op.set_refinement(sigma, tol_inner);
       int nev = static_cast<int>(std::min<std::int64_t>(n - 1, c + std::max<long long>(4, c / 4)));
       const int p = cfg.block_size > 0 ? cfg.block_size : auto_block(nev);
       block_used = std::max(block_used, p);
@@ -705,9 +864,19 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
   j.kv("two_by_two", static_cast<long long>(inr.two_by_two));
   j.close('}');
   {
-    const GpuFactor::DeviceStats& ds = F.device_stats();
+    // F's work plus the FP32 operator object's (its factorizations and solves) on the mixed path
+    GpuFactor::DeviceStats ds = F.device_stats();
+    if (&OPF != &F) {
+      const GpuFactor::DeviceStats& o = OPF.device_stats();
+      ds.factorizations += o.factorizations;
+      ds.factor_ms += o.factor_ms;
+      ds.solves += o.solves;
+      ds.solve_columns += o.solve_columns;
+      ds.solve_ms += o.solve_ms;
+    }
     j.key("device_timing");
     j.open('{');
+    j.kv("factor_precision", std::string(single ? "single" : "double"));
     j.kv("factorizations", ds.factorizations);
     j.kv("factor_ms", ds.factor_ms);
     j.kv("flops_per_factorization", est.flops);
@@ -721,8 +890,16 @@ SolveOutput Session::solve(const hsg_solve_config_t& cfg, bool include_setup) {
   }
   j.key("precision");
   j.open('{');
-  j.kv("requested", std::string(cfg.factor_precision == 1 ? "single" : "double"));
-  j.kv("used", std::string("double"));
+  j.kv("requested", std::string(cfg.factor_precision == 1 || !fallback.empty() ? "single" : "double"));
+  j.kv("used", std::string(single ? "single" : "double"));
+  j.kv("fallback", fallback);
+  j.key("refinement");
+  j.open('{');
+  j.kv("applies", op.refined_applies);
+  j.kv("steps", op.refine_steps);
+  j.kv("max_relative_residual", op.worst_rel);
+  j.kv("max_backward_error", op.worst_omega);
+  j.close('}');
   j.close('}');
   j.key("pairs");
   j.open('[');

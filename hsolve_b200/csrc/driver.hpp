@@ -38,6 +38,9 @@ class Session {
   hsg_estimate_t estimate() const;
 
  private:
+  // one attempt at the requested precision; `fallback` (non-empty) records why an earlier FP32
+  // attempt was abandoned
+  SolveOutput solve_once(const hsg_solve_config_t& cfg, bool include_setup, const std::string& fallback);
   struct Impl;
   std::unique_ptr<Impl> d_;
 };

@@ -28,6 +28,31 @@ namespace {
 
 constexpr double kAlphaBK = 0.6403882032022076;  // (1 + sqrt(17)) / 8
 
+// Determinant of a 2x2 pivot [a b; b c] in the factor's arithmetic R (the pivot test and the
+// elimination use the same value).
+template <class R>
+__device__ __forceinline__ double pivot_det(double a, double b, double c) {
+  const R ra = static_cast<R>(a), rb = static_cast<R>(b), rc = static_cast<R>(c);
+  return static_cast<double>(ra * rc - rb * rb);
+}
+
+// two consecutive shared-memory values in one vector load (16-byte aligned pairs of doubles,
+// 8-byte aligned pairs of floats)
+__device__ __forceinline__ double2 load_pair(const double* p) { return *reinterpret_cast<const double2*>(p); }
+__device__ __forceinline__ float2 load_pair(const float* p) { return *reinterpret_cast<const float2*>(p); }
+
+// Asynchronous copy of one factor element (sizeof(R) bytes) from global to shared memory;
+// valid == false fills the destination with zero.
+template <class R>
+__device__ __forceinline__ void cp_async_elem(R* dst, const R* src, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  if constexpr (sizeof(R) == 8) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+  }
+}
+
 // ------------------------------------------------------------------ scaling and assembly
 
 __global__ void k_fill(double* x, std::int64_t n, double v) {
@@ -63,16 +88,18 @@ __global__ void k_scale_update(std::int64_t n, double* d, unsigned long long* r)
   }
 }
 
-// panels[dest[p]] = d_i d_j (alpha a_p + beta b_p); records max |.| for the null-pivot threshold
+// panels[dest[p]] = d_i d_j (alpha a_p + beta b_p) (rounded to the factor type R); records max |.|
+// for the null-pivot threshold
+template <class R>
 __global__ void k_scatter(std::int64_t nnz, const std::int32_t* row, const std::int32_t* col, const double* a,
                           const double* b, double alpha, double beta, const double* d, const std::int64_t* dest,
-                          double* panels, FactorCounters* cnt) {
+                          R* panels, FactorCounters* cnt) {
   double mx = 0.0;
   for (std::int64_t p = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; p < nnz;
        p += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
     const std::int32_t i = row[p], j = col[p];
     const double v = (alpha * a[p] + beta * b[p]) * d[i] * d[j];
-    panels[dest[p]] = v;
+    panels[dest[p]] = static_cast<R>(v);
     mx = fmax(mx, fabs(v));
   }
   mx = warp_max(mx);
@@ -80,34 +107,36 @@ __global__ void k_scatter(std::int64_t nnz, const std::int32_t* row, const std::
 }
 
 // zero the contribution blocks of the listed fronts (grid: fronts x chunks)
-__global__ void k_zero_cb(const std::int32_t* list, const SnDev* sn, double* cb) {
+template <class R>
+__global__ void k_zero_cb(const std::int32_t* list, const SnDev* sn, R* cb) {
   const SnDev s = sn[list[blockIdx.x]];
   const std::int64_t c = s.m - s.k;
   const std::int64_t total = c * c;
-  double* base = cb + s.cb_off;
+  R* base = cb + s.cb_off;
   for (std::int64_t i = blockIdx.y * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < total;
        i += static_cast<std::int64_t>(gridDim.y) * blockDim.x)
-    base[i] = 0.0;
+    base[i] = R(0);
 }
 
 // Extend-add: item = (child, first column of a column block). Adds the child's lower CB
 // columns [b0, b0 + EA_COLS) into its parent front (panel part or contribution block).
-__global__ void k_extend_add(const int2* items, const SnDev* sn, const std::int32_t* rmap, double* panels, double* cb) {
+template <class R>
+__global__ void k_extend_add(const int2* items, const SnDev* sn, const std::int32_t* rmap, R* panels, R* cb) {
   const int2 it = items[blockIdx.x];
   const SnDev c = sn[it.x];
   const SnDev p = sn[c.parent];
   const std::int32_t mc = c.m - c.k;
   const std::int32_t* rm = rmap + c.rmap_off;
-  const double* src = cb + c.cb_off;
+  const R* src = cb + c.cb_off;
   const std::int32_t pc = p.m - p.k;
   const std::int32_t bend = min(it.y + kExtendAddCols, mc);
   for (std::int32_t bb = it.y; bb < bend; ++bb) {
     const std::int32_t pb = rm[bb];
-    double* dst;
+    R* dst;
     std::int64_t ld_off;
     if (pb < p.k) { dst = panels + p.panel_off + static_cast<std::int64_t>(pb) * p.m; ld_off = 0; }
     else { dst = cb + p.cb_off + static_cast<std::int64_t>(pb - p.k) * pc; ld_off = p.k; }
-    const double* col = src + static_cast<std::int64_t>(bb) * mc;
+    const R* col = src + static_cast<std::int64_t>(bb) * mc;
     for (std::int32_t a = bb + threadIdx.x; a < mc; a += blockDim.x) dst[rm[a] - ld_off] += col[a];
   }
 }
@@ -124,10 +153,11 @@ struct StepShared {
 
 // Warp 0: decide the pivot at column j of the lower-stored matrix F (order m, ld ld) with
 // candidates [j, nfs). Row maxima cover all rows [j, m).
-__device__ void decide_pivot(const double* F, int ld, int m, int nfs, int j, double u, double thr, bool force,
+template <class R>
+__device__ void decide_pivot(const R* F, int ld, int m, int nfs, int j, double u, double thr, bool force,
                              StepShared& st) {
   const int lane = threadIdx.x & 31;
-  const double* cj = F + static_cast<std::int64_t>(j) * ld;
+  const R* cj = F + static_cast<std::int64_t>(j) * ld;
   double gc = 0.0, best = 0.0;
   int r = -1;
   for (int i = j + 1 + lane; i < m; i += 32) {
@@ -149,17 +179,17 @@ __device__ void decide_pivot(const double* F, int ld, int m, int nfs, int j, dou
   else if (force && (r < 0 || best == 0.0 || dcc >= kAlphaBK * gc)) dec = dcc > 0.0 ? kOneJ : kNull;
   if (dec == kFail && r >= 0 && best > 0.0) {
     // maxima of columns j and r excluding rows {j, r}
-    const double* cr = F + static_cast<std::int64_t>(r) * ld;
+    const R* cr = F + static_cast<std::int64_t>(r) * ld;
     double gc2 = 0.0, gr2 = 0.0;
     for (int i = j + 1 + lane; i < m; i += 32) {
-      if (i != r) gc2 = fmax(gc2, fabs(cj[i]));
-      if (i < r && i != j) gr2 = fmax(gr2, fabs(F[r + static_cast<std::int64_t>(i) * ld]));
-      if (i > r) gr2 = fmax(gr2, fabs(cr[i]));
+      if (i != r) gc2 = fmax(gc2, static_cast<double>(fabs(cj[i])));
+      if (i < r && i != j) gr2 = fmax(gr2, static_cast<double>(fabs(F[r + static_cast<std::int64_t>(i) * ld])));
+      if (i > r) gr2 = fmax(gr2, static_cast<double>(fabs(cr[i])));
     }
     gc2 = warp_max(gc2);
     gr2 = warp_max(gr2);
     const double a = cj[j], b = cj[r], c = cr[r];
-    const double det = a * c - b * b;
+    const double det = pivot_det<R>(a, b, c);
     if (force) {
       dec = det != 0.0 ? kTwoR : (dcc > 0.0 ? kOneJ : kNull);
     } else {
@@ -177,34 +207,36 @@ __device__ void decide_pivot(const double* F, int ld, int m, int nfs, int j, dou
 }
 
 // symmetric swap of positions p, q (< m) of the lower-stored matrix; labels follow
-__device__ void sym_swap(double* F, int ld, int m, int p, int q, int* lab) {
+template <class R>
+__device__ void sym_swap(R* F, int ld, int m, int p, int q, int* lab) {
   if (p == q) return;
   if (p > q) { const int t = p; p = q; q = t; }
   const int n1 = p, n2 = q - p - 1, n3 = m - q - 1;
   for (int t = threadIdx.x; t < n1 + n2 + n3 + 1; t += blockDim.x) {
-    double *x, *y;
+    R *x, *y;
     if (t < n1) { x = F + p + static_cast<std::int64_t>(t) * ld; y = F + q + static_cast<std::int64_t>(t) * ld; }
     else if (t < n1 + n2) { const int c = p + 1 + (t - n1); x = F + c + static_cast<std::int64_t>(p) * ld; y = F + q + static_cast<std::int64_t>(c) * ld; }
     else if (t < n1 + n2 + n3) { const int i = q + 1 + (t - n1 - n2); x = F + i + static_cast<std::int64_t>(p) * ld; y = F + i + static_cast<std::int64_t>(q) * ld; }
     else { x = F + p + static_cast<std::int64_t>(p) * ld; y = F + q + static_cast<std::int64_t>(q) * ld; }
-    const double v = *x; *x = *y; *y = v;
+    const R v = *x; *x = *y; *y = v;
   }
   if (threadIdx.x == 0 && lab) { const int t = lab[p]; lab[p] = lab[q]; lab[q] = t; }
 }
 
 // eliminate a 1x1 (or null) pivot at j: column scaled to l, trailing rows/cols [j+1, m) updated
-__device__ void elim1(double* F, int ld, int m, int j, bool null_piv, double* tmp) {
-  const double d = F[j + static_cast<std::int64_t>(j) * ld];
-  double* cj = F + static_cast<std::int64_t>(j) * ld;
+template <class R>
+__device__ void elim1(R* F, int ld, int m, int j, bool null_piv, R* tmp) {
+  const R d = F[j + static_cast<std::int64_t>(j) * ld];
+  R* cj = F + static_cast<std::int64_t>(j) * ld;
   for (int i = j + 1 + threadIdx.x; i < m; i += blockDim.x) {
-    const double x = cj[i];
-    tmp[i] = null_piv ? 0.0 : x;
-    cj[i] = null_piv ? 0.0 : x / d;
+    const R x = cj[i];
+    tmp[i] = null_piv ? R(0) : x;
+    cj[i] = null_piv ? R(0) : x / d;
   }
   __syncthreads();
   if (!null_piv) {
     const int w = m - j - 1;
-    const double inv = 1.0 / d;
+    const R inv = R(1) / d;
     for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
       const int i = j + 1 + t % w, c = j + 1 + t / w;
       if (i >= c) F[i + static_cast<std::int64_t>(c) * ld] -= tmp[i] * tmp[c] * inv;
@@ -214,15 +246,16 @@ __device__ void elim1(double* F, int ld, int m, int j, bool null_piv, double* tm
 }
 
 // eliminate the 2x2 pivot (j, j+1)
-__device__ void elim2(double* F, int ld, int m, int j, double* tmp0, double* tmp1) {
-  const double a = F[j + static_cast<std::int64_t>(j) * ld], b = F[j + 1 + static_cast<std::int64_t>(j) * ld];
-  const double c = F[j + 1 + static_cast<std::int64_t>(j + 1) * ld];
-  const double det = a * c - b * b;
-  const double ia = c / det, ib = -b / det, ic = a / det;
-  double* c0 = F + static_cast<std::int64_t>(j) * ld;
-  double* c1 = F + static_cast<std::int64_t>(j + 1) * ld;
+template <class R>
+__device__ void elim2(R* F, int ld, int m, int j, R* tmp0, R* tmp1) {
+  const R a = F[j + static_cast<std::int64_t>(j) * ld], b = F[j + 1 + static_cast<std::int64_t>(j) * ld];
+  const R c = F[j + 1 + static_cast<std::int64_t>(j + 1) * ld];
+  const R det = a * c - b * b;
+  const R ia = c / det, ib = -b / det, ic = a / det;
+  R* c0 = F + static_cast<std::int64_t>(j) * ld;
+  R* c1 = F + static_cast<std::int64_t>(j + 1) * ld;
   for (int i = j + 2 + threadIdx.x; i < m; i += blockDim.x) {
-    const double x0 = c0[i], x1 = c1[i];
+    const R x0 = c0[i], x1 = c1[i];
     tmp0[i] = x0;
     tmp1[i] = x1;
     c0[i] = ia * x0 + ib * x1;
@@ -240,8 +273,9 @@ __device__ void elim2(double* F, int ld, int m, int j, double* tmp0, double* tmp
 // Threshold Bunch-Kaufman on a lower-stored dense matrix in shared memory: candidates [0, nfs),
 // rows [0, m). root: pivots may be forced (never fail). Returns the number of eliminated columns
 // (positions [e, nfs) failed); pv[t] in {0 null, 1 1x1, 2/3 2x2}; lab follows the swaps.
-__device__ int dense_bk(double* F, int ld, int m, int nfs, bool root, double u, double thr, int* lab, signed char* pv,
-                        double* tmp0, double* tmp1, StepShared& st) {
+template <class R>
+__device__ int dense_bk(R* F, int ld, int m, int nfs, bool root, double u, double thr, int* lab, signed char* pv,
+                        R* tmp0, R* tmp1, StepShared& st) {
   if (threadIdx.x == 0) {
     st.j = 0; st.lim = nfs; st.prog = 0; st.force = 0; st.stop = 0;
     st.neg = st.pos = st.zero = st.two = st.forced = 0;
@@ -275,9 +309,9 @@ __device__ int dense_bk(double* F, int ld, int m, int nfs, bool root, double u, 
     if (dec == kTwoR) { sym_swap(F, ld, m, j + 1, r, lab); __syncthreads(); }
     if (dec == kTwoR) {
       if (threadIdx.x == 0) {
-        const double a = F[j + static_cast<std::int64_t>(j) * ld], b = F[j + 1 + static_cast<std::int64_t>(j) * ld];
-        const double c = F[j + 1 + static_cast<std::int64_t>(j + 1) * ld];
-        const double det = a * c - b * b;
+        const R a = F[j + static_cast<std::int64_t>(j) * ld], b = F[j + 1 + static_cast<std::int64_t>(j) * ld];
+        const R c = F[j + 1 + static_cast<std::int64_t>(j + 1) * ld];
+        const R det = a * c - b * b;
         if (det < 0) { st.neg++; st.pos++; } else if (a + c < 0) st.neg += 2; else st.pos += 2;
         st.two++;
         if (st.force) st.forced++;
@@ -320,7 +354,8 @@ __device__ __forceinline__ float warp_maxf(float v) {
 // single precision (a threshold test needs no more), the argmax for a 2 x 2 partner only when the
 // 1 x 1 test fails, one reciprocal per pivot, broadcast shared-memory reads in the update.
 // Warp-synchronous: no block barriers. Returns the eliminated count; [e, w) could not be pivoted.
-__device__ int warp_block_bk(double* F, int w, bool root, double u, double thr, int* lab, signed char* pv,
+template <class R>
+__device__ int warp_block_bk(R* F, int w, bool root, double u, double thr, int* lab, signed char* pv,
                              StepShared& st, int j0 = 0, int prog0 = 0) {
   const int lane = threadIdx.x & 31;
   constexpr int ld = kNB;
@@ -332,7 +367,7 @@ __device__ int warp_block_bk(double* F, int w, bool root, double u, double thr, 
       if (root && !force) { force = 1; lim = w; continue; }
       break;
     }
-    const double* cj = F + j * ld;
+    const R* cj = F + j * ld;
     const double xj = lane > j && lane < w ? cj[lane] : 0.0;
     const float gcf = warp_maxf(static_cast<float>(fabs(xj)));
     const double gc = static_cast<double>(gcf);
@@ -354,13 +389,13 @@ __device__ int warp_block_bk(double* F, int w, bool root, double u, double thr, 
       r = bi;
       if (force && (r < 0 || best <= 0.0f || dcc >= kAlphaBK * gc)) dec = dcc > 0.0 ? kOneJ : kNull;
       else if (r >= 0 && best > 0.0f) {
-        const double* cr = F + r * ld;
+        const R* cr = F + r * ld;
         const double xr = lane > j && lane < w && lane != r ? (lane < r ? F[r + lane * ld] : cr[lane]) : 0.0;
         const float gr2f = warp_maxf(static_cast<float>(fabs(xr)));
         const float gc2f = warp_maxf(lane != r ? static_cast<float>(fabs(xj)) : 0.0f);
         const double gr2 = gr2f, gc2 = gc2f;
         const double a = dj, b = cj[r], c = cr[r];
-        const double det = a * c - b * b;
+        const double det = pivot_det<R>(a, b, c);
         if (force) dec = det != 0.0 ? kTwoR : (dcc > 0.0 ? kOneJ : kNull);
         else {
           if (det != 0.0) {
@@ -379,12 +414,12 @@ __device__ int warp_block_bk(double* F, int w, bool root, double u, double thr, 
     if (sp >= 0 && sp != sq) {
       int p = sp < sq ? sp : sq, q = sp < sq ? sq : sp;
       for (int t = lane; t < w + 1; t += 32) {
-        double *x = nullptr, *y = nullptr;
+        R *x = nullptr, *y = nullptr;
         if (t < p) { x = F + p + t * ld; y = F + q + t * ld; }
         else if (t > p && t < q) { x = F + t + p * ld; y = F + q + t * ld; }
         else if (t > q && t < w) { x = F + t + p * ld; y = F + t + q * ld; }
         else if (t == p) { x = F + p + p * ld; y = F + q + q * ld; }
-        if (x) { const double v = *x; *x = *y; *y = v; }
+        if (x) { const R v = *x; *x = *y; *y = v; }
       }
       if (lane == 0) { const int tl = lab[p]; lab[p] = lab[q]; lab[q] = tl; }
       __syncwarp();
@@ -392,16 +427,16 @@ __device__ int warp_block_bk(double* F, int w, bool root, double u, double thr, 
     if (dec == kFail) { lim -= 1; continue; }
     const int i = lane;
     if (dec == kTwoR) {
-      const double a = F[j + j * ld], b = F[j + 1 + j * ld], c = F[j + 1 + (j + 1) * ld];
-      const double det = a * c - b * b;
-      const double idet = 1.0 / det;
-      const double ia = c * idet, ib = -b * idet, ic = a * idet;
-      const double x0 = (i >= j + 2 && i < w) ? F[i + j * ld] : 0.0;
-      const double x1 = (i >= j + 2 && i < w) ? F[i + (j + 1) * ld] : 0.0;
-      const double l0 = ia * x0 + ib * x1, l1 = ib * x0 + ic * x1;
+      const R a = F[j + j * ld], b = F[j + 1 + j * ld], c = F[j + 1 + (j + 1) * ld];
+      const R det = a * c - b * b;
+      const R idet = R(1) / det;
+      const R ia = c * idet, ib = -b * idet, ic = a * idet;
+      const R x0 = (i >= j + 2 && i < w) ? F[i + j * ld] : R(0);
+      const R x1 = (i >= j + 2 && i < w) ? F[i + (j + 1) * ld] : R(0);
+      const R l0 = ia * x0 + ib * x1, l1 = ib * x0 + ic * x1;
       __syncwarp();
       for (int c2 = j + 2; c2 < w; ++c2) {
-        const double y0 = F[c2 + j * ld], y1 = F[c2 + (j + 1) * ld];
+        const R y0 = F[c2 + j * ld], y1 = F[c2 + (j + 1) * ld];
         if (i >= c2 && i < w) F[i + c2 * ld] -= l0 * y0 + l1 * y1;
       }
       __syncwarp();
@@ -413,14 +448,14 @@ __device__ int warp_block_bk(double* F, int w, bool root, double u, double thr, 
       j += 2;
     } else {
       const bool nul = dec == kNull;
-      const double d = F[j + j * ld];
-      const double inv = nul ? 0.0 : 1.0 / d;
-      const double x = (i > j && i < w) ? F[i + j * ld] : 0.0;
-      const double xs = x * inv;
+      const R d = F[j + j * ld];
+      const R inv = nul ? R(0) : R(1) / d;
+      const R x = (i > j && i < w) ? F[i + j * ld] : R(0);
+      const R xs = x * inv;
       __syncwarp();
       if (!nul) {
         for (int c2 = j + 1; c2 < w; ++c2) {
-          const double y = F[c2 + j * ld];
+          const R y = F[c2 + j * ld];
           if (i >= c2 && i < w) F[i + c2 * ld] -= xs * y;
         }
       }
@@ -446,31 +481,32 @@ __device__ int warp_block_bk(double* F, int w, bool root, double u, double thr, 
 // the positions are processed in order with compile-time indices and 1 x 1 pivots on their own
 // column. The first position whose 1 x 1 test fails (or that is a null pivot) hands the partially
 // factorized block to the shared-memory routine, which continues from there with the same rules.
-__device__ int warp_block_bk_fast(double* F, int w, bool root, double u, double thr, int* lab, signed char* pv,
+template <class R>
+__device__ int warp_block_bk_fast(R* F, int w, bool root, double u, double thr, int* lab, signed char* pv,
                                   StepShared& st) {
   const int lane = threadIdx.x & 31;
   constexpr int ld = kNB;
   if (w != kNB || root) return warp_block_bk(F, w, root, u, thr, lab, pv, st);
-  __shared__ __align__(16) double s_col[kNB];
-  double r[kNB];
+  __shared__ __align__(16) R s_col[kNB];
+  R r[kNB];
 #pragma unroll
-  for (int c = 0; c < kNB; ++c) r[c] = c <= lane ? F[lane + c * ld] : 0.0;
+  for (int c = 0; c < kNB; ++c) r[c] = c <= lane ? F[lane + c * ld] : R(0);
   int pos = 0, neg = 0;
   int stop = kNB;  // first position that needs the general routine
 #pragma unroll
   for (int j = 0; j < kNB; ++j) {
     if (stop == kNB) {
-      const double x = lane > j ? r[j] : 0.0;
+      const R x = lane > j ? r[j] : R(0);
       const float gcf = warp_maxf(static_cast<float>(fabs(x)));
-      const double d = __shfl_sync(0xffffffffu, r[j], j);
+      const R d = __shfl_sync(0xffffffffu, r[j], j);
       const double dcc = fabs(d);
       const double gc = gcf;
       const bool ok = dcc > 0.0 && dcc >= u * gc && !(thr >= 0.0 && fmax(dcc, gc) <= thr);
       if (!ok) {
         stop = j;
       } else {
-        const double inv = 1.0 / d;
-        const double xs = x * inv;
+        const R inv = R(1) / d;
+        const R xs = x * inv;
         // column j to shared memory once, then broadcast 16-byte reads of F(c, j), c > j
         s_col[lane] = r[j];
         __syncwarp();
@@ -482,7 +518,7 @@ __device__ int warp_block_bk_fast(double* F, int w, bool root, double u, double 
 #pragma unroll
         for (int c = 0; c < kNB; c += 2) {
           if (c < c0) continue;
-          const double2 y2 = *reinterpret_cast<const double2*>(&s_col[c]);
+          const auto y2 = load_pair(&s_col[c]);
           if (lane >= c) r[c] = fma(-xs, y2.x, r[c]);
           if (lane >= c + 1) r[c + 1] = fma(-xs, y2.y, r[c + 1]);
         }
@@ -505,12 +541,13 @@ __device__ int warp_block_bk_fast(double* F, int w, bool root, double u, double 
 
 // ---------------------------------------------------------------------- small fronts (smem)
 
-template <int MAXM>
-__global__ void __launch_bounds__(256) k_front_small(const std::int32_t* list, const SnDev* sn, double* panels,
-                                                      double* cb, signed char* piv_out, std::int32_t* pidx_out,
+template <int MAXM, class R>
+__global__ void __launch_bounds__(256) k_front_small(const std::int32_t* list, const SnDev* sn, R* panels,
+                                                      R* cb, signed char* piv_out, std::int32_t* pidx_out,
                                                       FactorParams prm, FactorCounters* cnt, std::int32_t* failed) {
-  extern __shared__ double F[];
-  __shared__ double tmp0[MAXM], tmp1[MAXM];
+  extern __shared__ __align__(16) unsigned char small_dyn[];
+  R* F = reinterpret_cast<R*>(small_dyn);
+  __shared__ R tmp0[MAXM], tmp1[MAXM];
   __shared__ int lab[MAXM];
   __shared__ signed char pv[MAXM];
   __shared__ StepShared st;
@@ -559,14 +596,15 @@ __global__ void __launch_bounds__(256) k_front_small(const std::int32_t* list, c
 
 namespace {
 
+template <class R>
 struct FrontView {
-  double* panel;  // m x k, ld m
-  double* cbb;    // (m-k)^2, ld m-k
+  R* panel;  // m x k, ld m
+  R* cbb;    // (m-k)^2, ld m-k
   int m, k;
-  __device__ double* col(int c) const {
+  __device__ R* col(int c) const {
     return c < k ? panel + static_cast<std::int64_t>(c) * m : cbb + static_cast<std::int64_t>(c - k) * (m - k) - k;
   }
-  __device__ double& at(int i, int c) const { return col(c)[i]; }
+  __device__ R& at(int i, int c) const { return col(c)[i]; }
 };
 
 struct AppCtrl {
@@ -582,29 +620,33 @@ struct StepView {
   int p, w, lim, fb, eb, force, stop;
 };
 
+// The scratch of a front is laid out in units of doubles whatever the factor type R; the R-typed
+// arrays (B, Borig, backup) occupy the first sizeof(R) / 8 of their double-sized regions.
+template <class R>
 struct AppFront {
-  FrontView f;
+  FrontView<R> f;
   int first;
   bool root;
   AppCtrl* ctrl;
   double* slots;   // two sets of the per-panel arrays below, used by alternate panels
-  double* B;       // factored diagonal block, kNB x kNB col-major
-  double* Borig;   // the block before factorization
+  R* B;            // factored diagonal block, kNB x kNB col-major
+  R* Borig;        // the block before factorization
   int* lab;        // block permutation
   signed char* pv; // block pivot types
   unsigned long long* cmax;
   unsigned long long* rmax;
-  double* backup;  // kNB columns of m rows
+  R* backup;       // kNB columns of m rows
   std::int32_t* plab;
   signed char* ppv;
 };
 
 // point the per-panel arrays at set `slot` (0 or 1)
-__device__ __forceinline__ void set_slot(AppFront& F, int slot) {
+template <class R>
+__device__ __forceinline__ void set_slot(AppFront<R>& F, int slot) {
   double* s = F.slots + slot * kAppSlotDoubles;
-  F.B = s;
+  F.B = reinterpret_cast<R*>(s);
   s += kNB * kNB;
-  F.Borig = s;
+  F.Borig = reinterpret_cast<R*>(s);
   s += kNB * kNB;
   F.lab = reinterpret_cast<int*>(s);
   s += kNB / 2;
@@ -627,10 +669,11 @@ __device__ __forceinline__ StepView step_view(const AppCtrl* c) {
   return v;
 }
 
-__device__ AppFront make_front(const SnDev& d, double* panels, double* cb, double* scratch, signed char* piv_out,
-                               std::int32_t* pidx_out) {
-  AppFront F;
-  F.f = FrontView{panels + d.panel_off, d.cb_off >= 0 ? cb + d.cb_off : nullptr, d.m, d.k};
+template <class R>
+__device__ AppFront<R> make_front(const SnDev& d, R* panels, R* cb, double* scratch, signed char* piv_out,
+                                  std::int32_t* pidx_out) {
+  AppFront<R> F;
+  F.f = FrontView<R>{panels + d.panel_off, d.cb_off >= 0 ? cb + d.cb_off : nullptr, d.m, d.k};
   F.first = d.first;
   F.root = d.parent < 0;
   double* s = scratch + d.scratch_off;
@@ -638,7 +681,7 @@ __device__ AppFront make_front(const SnDev& d, double* panels, double* cb, doubl
   s += kAppCtrlDoubles;
   F.slots = s;
   s += 2 * kAppSlotDoubles;
-  F.backup = s;
+  F.backup = reinterpret_cast<R*>(s);
   F.plab = pidx_out + d.first;
   F.ppv = piv_out + d.first;
   set_slot(F, 0);
@@ -646,23 +689,25 @@ __device__ AppFront make_front(const SnDev& d, double* panels, double* cb, doubl
 }
 
 // symmetric swap of fully-summed positions a, b (< k) of the front in global memory
-__device__ void front_swap(const FrontView& f, int a, int b, std::int32_t* lab) {
+template <class R>
+__device__ void front_swap(const FrontView<R>& f, int a, int b, std::int32_t* lab) {
   if (a == b) return;
   if (a > b) { const int t = a; a = b; b = t; }
   const int n1 = a, n2 = b - a - 1, n3 = f.m - b - 1;
   for (int t = threadIdx.x; t < n1 + n2 + n3 + 1; t += blockDim.x) {
-    double *x, *y;
+    R *x, *y;
     if (t < n1) { x = &f.at(a, t); y = &f.at(b, t); }
     else if (t < n1 + n2) { const int c = a + 1 + (t - n1); x = &f.at(c, a); y = &f.at(b, c); }
     else if (t < n1 + n2 + n3) { const int i = b + 1 + (t - n1 - n2); x = &f.at(i, a); y = &f.at(i, b); }
     else { x = &f.at(a, a); y = &f.at(b, b); }
-    const double v = *x; *x = *y; *y = v;
+    const R v = *x; *x = *y; *y = v;
   }
   if (threadIdx.x == 0) { const std::int32_t t = lab[a]; lab[a] = lab[b]; lab[b] = t; }
 }
 
 // Init (all ranks split the label work; rank 0 the control block).
-__device__ void app_init(AppFront& F, int rank, int nr) {
+template <class R>
+__device__ void app_init(AppFront<R>& F, int rank, int nr) {
   const int k = F.f.k;
   for (int t = rank * blockDim.x + threadIdx.x; t < k; t += nr * blockDim.x) { F.plab[t] = t; F.ppv[t] = -1; }
   if (rank == 0 && threadIdx.x == 0) {
@@ -674,8 +719,9 @@ __device__ void app_init(AppFront& F, int rank, int nr) {
 
 // Rank 0: decide what the next panel is (stop = 1: front finished), and factorize its diagonal block
 // with block-restricted threshold Bunch-Kaufman; permute the L rows of the block; publish to scratch.
-__device__ void app_control_and_block(AppFront& F, const FactorParams& prm, double thr, double* Bs, double* tmp0,
-                                      double* tmp1, int* slab, signed char* spv, StepShared& bst, int* shared_stop,
+template <class R>
+__device__ void app_control_and_block(AppFront<R>& F, const FactorParams& prm, double thr, R* Bs, R* tmp0,
+                                      R* tmp1, int* slab, signed char* spv, StepShared& bst, int* shared_stop,
                                       FactorCounters* cnt, std::int32_t* failed, int* level_done) {
   AppCtrl* c = F.ctrl;
   const int k = F.f.k;
@@ -793,8 +839,9 @@ __device__ void app_control_and_block(AppFront& F, const FactorParams& prm, doub
 // All ranks: rows [p+w, m) solved against the block (L21 = F21 P L11^-T D^-1), backup, column maxima.
 // The block's strict lower part with the 2x2 couplings masked (they belong to D) is staged in Ls
 // (shared), the substitution runs fully unrolled in registers, one row per thread.
-__device__ void app_rows(AppFront& F, const StepView& v, int rank, int nr, double* Bs, int* slab, signed char* spv,
-                         unsigned long long* scm, unsigned long long* srm, double* Lm) {
+template <class R>
+__device__ void app_rows(AppFront<R>& F, const StepView& v, int rank, int nr, R* Bs, int* slab, signed char* spv,
+                         unsigned long long* scm, unsigned long long* srm, R* Lm) {
   const int p = v.p, w = v.w, eb = v.eb, m = F.f.m;
   for (int t = threadIdx.x; t < kNB * kNB; t += blockDim.x) Bs[t] = __ldcg(&F.B[t]);
   for (int t = threadIdx.x; t < kNB; t += blockDim.x) {
@@ -807,7 +854,7 @@ __device__ void app_rows(AppFront& F, const StepView& v, int rank, int nr, doubl
   // Lm[t * kNB + s] = L11(t, s) for s < min(t, eb), zero otherwise (row-major for broadcast reads)
   for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
     const int t = e / kNB, s = e % kNB;
-    double x = 0.0;
+    R x = R(0);
     if (t < w && s < t && s < eb && !(spv[s] == 2 && s + 1 == t)) x = Bs[t + s * kNB];
     Lm[e] = x;
   }
@@ -817,10 +864,10 @@ __device__ void app_rows(AppFront& F, const StepView& v, int rank, int nr, doubl
   const int cchunk = (p + nr - 1) / nr;
   const int cend = min(p, (rank + 1) * cchunk);
   for (int cc = rank * cchunk + threadIdx.x; cc < cend; cc += blockDim.x) {
-    double x[kNB];
-    double* colp = F.f.col(cc) + p;
+    R x[kNB];
+    R* colp = F.f.col(cc) + p;
 #pragma unroll
-    for (int a = 0; a < kNB; ++a) x[a] = a < w ? colp[slab[a]] : 0.0;
+    for (int a = 0; a < kNB; ++a) x[a] = a < w ? colp[slab[a]] : R(0);
 #pragma unroll
     for (int a = 0; a < kNB; ++a)
       if (a < w) colp[a] = x[a];
@@ -830,17 +877,17 @@ __device__ void app_rows(AppFront& F, const StepView& v, int rank, int nr, doubl
   const int rbeg = p + w + rank * rchunk, rend = min(m, rbeg + rchunk);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float* wl = reinterpret_cast<float*>(Lm + kNB * kNB);   // per-warp column maxima (8 x kNB floats)
-  double* Di = Lm + kNB * kNB + 8 * kNB;                    // D^-1 entries: a, b, c per pivot (3 x kNB)
+  R* Di = Lm + kNB * kNB + 8 * kNB;                         // D^-1 entries: a, b, c per pivot (3 x kNB)
   for (int t = threadIdx.x; t < 8 * kNB; t += blockDim.x) wl[t] = 0.0f;
   for (int t = threadIdx.x; t < kNB; t += blockDim.x) {
-    double ia = 0.0, ib = 0.0, ic = 0.0;
+    R ia = R(0), ib = R(0), ic = R(0);
     if (t < eb) {
       const signed char ty = spv[t];
-      if (ty == 1) ia = 1.0 / Bs[t + t * kNB];
+      if (ty == 1) ia = R(1) / Bs[t + t * kNB];
       else if (ty == 2 || ty == 3) {
         const int f0 = ty == 2 ? t : t - 1;
-        const double a = Bs[f0 + f0 * kNB], b = Bs[f0 + 1 + f0 * kNB], cc = Bs[f0 + 1 + (f0 + 1) * kNB];
-        const double idet = 1.0 / (a * cc - b * b);
+        const R a = Bs[f0 + f0 * kNB], b = Bs[f0 + 1 + f0 * kNB], cc = Bs[f0 + 1 + (f0 + 1) * kNB];
+        const R idet = R(1) / (a * cc - b * b);
         // first of the pair: l = ia y_t + ib y_{t+1}; second: l = ib y_{t-1} + ic y_t
         if (ty == 2) { ia = cc * idet; ib = -b * idet; }
         else { ib = -b * idet; ic = a * idet; }
@@ -857,15 +904,15 @@ __device__ void app_rows(AppFront& F, const StepView& v, int rank, int nr, doubl
   for (int i = rbeg + threadIdx.x; i < rend; i += blockDim.x) {
     // all loads first (no store in between: they overlap), block order = the pivot permutation;
     // the backup is stored, then the substitution runs in place
-    double y[kNB];
+    R y[kNB];
 #pragma unroll
-    for (int t = 0; t < kNB; ++t) y[t] = t < w ? F.f.at(i, p + slab[t]) : 0.0;
+    for (int t = 0; t < kNB; ++t) y[t] = t < w ? F.f.at(i, p + slab[t]) : R(0);
 #pragma unroll
     for (int t = 0; t < kNB; ++t)
       if (t < w) F.backup[static_cast<std::int64_t>(t) * m + i] = y[t];
 #pragma unroll
     for (int t = 1; t < kNB; ++t) {
-      double acc = y[t];
+      R acc = y[t];
 #pragma unroll
       for (int s = 0; s < t; ++s) acc = fma(-y[s], Lm[t * kNB + s], acc);
       y[t] = acc;
@@ -873,12 +920,12 @@ __device__ void app_rows(AppFront& F, const StepView& v, int rank, int nr, doubl
 #pragma unroll
     for (int t = 0; t < kNB; ++t) {
       if (t >= w) continue;
-      double out;
+      R out;
       if (t < eb) {
         const signed char ty = spv[t];
-        const double yp = t > 0 ? y[(t - 1) & (kNB - 1)] : 0.0;
-        const double yn = t + 1 < kNB ? y[(t + 1) & (kNB - 1)] : 0.0;
-        if (ty == 0) out = 0.0;
+        const R yp = t > 0 ? y[(t - 1) & (kNB - 1)] : R(0);
+        const R yn = t + 1 < kNB ? y[(t + 1) & (kNB - 1)] : R(0);
+        if (ty == 0) out = R(0);
         else if (ty == 1) out = y[t] * Di[t];
         else if (ty == 2) out = Di[t] * y[t] + Di[kNB + t] * yn;
         else out = Di[kNB + t] * yp + Di[2 * kNB + t] * y[t];
@@ -913,8 +960,9 @@ __device__ void app_rows(AppFront& F, const StepView& v, int rank, int nr, doubl
 // All ranks: the accepted prefix q (identical in every CTA); rank 0 books the inertia. The small
 // per-panel arrays are staged in shared memory first (one parallel load) so that the serial scans
 // below touch no global memory. Bs / spv already hold the panel's block and pivot types (app_rows).
-__device__ int app_accept(AppFront& F, const StepView& v, int rank, double thr, double inv_u, int* sq,
-                          const double* Bs, const signed char* spv, unsigned long long* scm,
+template <class R>
+__device__ int app_accept(AppFront<R>& F, const StepView& v, int rank, double thr, double inv_u, int* sq,
+                          const R* Bs, const signed char* spv, unsigned long long* scm,
                           unsigned long long* srm) {
   const int eb = v.eb;
   const int p = v.p;
@@ -957,8 +1005,8 @@ __device__ int app_accept(AppFront& F, const StepView& v, int rank, double thr, 
         if (ty == 0) zero++;
         else if (ty == 1) { if (Bs[t + t * kNB] < 0) neg++; else pos++; }
         else if (ty == 2) {
-          const double a = Bs[t + t * kNB], b = Bs[t + 1 + t * kNB], cc = Bs[t + 1 + (t + 1) * kNB];
-          const double det = a * cc - b * b;
+          const R a = Bs[t + t * kNB], b = Bs[t + 1 + t * kNB], cc = Bs[t + 1 + (t + 1) * kNB];
+          const R det = a * cc - b * b;
           if (det < 0) { neg++; pos++; } else if (a + cc < 0) neg += 2; else pos += 2;
           two++;
         }
@@ -976,7 +1024,8 @@ __device__ int app_accept(AppFront& F, const StepView& v, int rank, double thr, 
 }
 
 // All ranks: restore the rejected block columns [q, w) from the backup / original block.
-__device__ void app_restore(AppFront& F, const StepView& v, int rank, int nr, int q) {
+template <class R>
+__device__ void app_restore(AppFront<R>& F, const StepView& v, int rank, int nr, int q) {
   const int p = v.p, w = v.w, m = F.f.m;
   const int rtotal = m - (p + w);
   const int rchunk = (rtotal + nr - 1) / nr;
@@ -1024,10 +1073,9 @@ __device__ __forceinline__ bool app_flushes(int p, int w, int q, int lim, int fb
 // second copy in place. Warp w (of 8) computes rows 16 (w % 4) .. +16 and columns 32 (w / 4) .. +32
 // of the tile as 2 x 4 blocks of 8 x 8. A thread's fragment element (g, t) is row g = lane / 4,
 // column t = lane % 4 of A; row t, column g of B; row g, columns 2t, 2t + 1 of C.
-__device__ __forceinline__ void cp_async8(double* dst, const double* src, int bytes) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
-}
+// FP32 factors (the operator factorization of the mixed-precision path) keep the same staging and
+// the same output ownership per thread, and accumulate with FP32 FMAs (there is no FP32 tensor
+// instruction with full FP32 operands; the FP64 refinement of every solve absorbs FP32 rounding).
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
@@ -1036,8 +1084,9 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // With look-ahead (la: the panel was accepted whole and the next one follows directly), rank 0 takes
 // only tile 0, which holds the next panel's diagonal block, so that it can factorize that block
 // while the other ranks finish the remaining tiles.
-__device__ void app_update(AppFront& F, const StepView& v, int rank, int nr, int q, bool la, double* Ls, double* Ws,
-                           double* ca, double* cb, int* cd, const double* Bs, const signed char* spv) {
+template <class R>
+__device__ void app_update(AppFront<R>& F, const StepView& v, int rank, int nr, int q, bool la, R* Ls, R* Ws,
+                           R* ca, R* cb, int* cd, const R* Bs, const signed char* spv) {
   const int p = v.p, w = v.w, lim = v.lim, fb = v.fb, m = F.f.m;
   const int from = p + q;
   const int K = from - fb;
@@ -1051,7 +1100,7 @@ __device__ void app_update(AppFront& F, const StepView& v, int rank, int nr, int
   // memory while the other ranks may already be here)
   for (int s = threadIdx.x; s < K; s += blockDim.x) {
     const int j = fb + s;
-    double x = 0.0, y = 0.0;
+    R x = R(0), y = R(0);
     int d = 0;
     if (j >= p) {
       const int t = j - p;
@@ -1100,18 +1149,18 @@ __device__ void app_update(AppFront& F, const StepView& v, int rank, int nr, int
       const int r = threadIdx.x & (kTile - 1), sg = threadIdx.x >> 6;
       const int i = i0 + r, cc = j0 + r;
       const int li = i < m ? i : from, lc = cc < m ? cc : from;
-      const int lb = i < m ? 8 : 0, wb = cc < col_hi ? 8 : 0;
+      const bool lb = i < m, wb = cc < col_hi;
 #pragma unroll 8
       for (int s = sg; s < Kpad; s += kAppThreads / kTile) {
         const bool in = s < K;
-        const double* lj = F.f.col(fb + (in ? s : 0));
-        cp_async8(&Ls[s * kUpdLd + r], lj + li, in ? lb : 0);
-        cp_async8(&Ws[s * kUpdLd + r], lj + lc, in ? wb : 0);
+        const R* lj = F.f.col(fb + (in ? s : 0));
+        cp_async_elem(&Ls[s * kUpdLd + r], lj + li, in && lb);
+        cp_async_elem(&Ws[s * kUpdLd + r], lj + lc, in && wb);
       }
     }
     // prefetch this thread's C entries (rows rbase + 8a + g, columns cbase + 8b + 2 t4 + e)
-    double* colp[4][2];
-    double cv[2][4][2];
+    R* colp[4][2];
+    R cv[2][4][2];
 #pragma unroll
     for (int b = 0; b < 4; ++b)
 #pragma unroll
@@ -1121,7 +1170,7 @@ __device__ void app_update(AppFront& F, const StepView& v, int rank, int nr, int
 #pragma unroll
         for (int a = 0; a < 2; ++a) {
           const int i = i0 + rbase + 8 * a + g;
-          cv[a][b][e] = (colp[b][e] && i < m && cc <= i) ? colp[b][e][i] : 0.0;
+          cv[a][b][e] = (colp[b][e] && i < m && cc <= i) ? colp[b][e][i] : R(0);
         }
       }
     cp_async_wait_all();
@@ -1132,14 +1181,14 @@ __device__ void app_update(AppFront& F, const StepView& v, int rank, int nr, int
       const int d = cd[s];
       if (d < 0) continue;
       const bool masked = j0 + r < rej_hi && fb + s < p;
-      double* w0 = &Ws[s * kUpdLd + r];
+      R* w0 = &Ws[s * kUpdLd + r];
       if (d == 0) {
-        *w0 = masked ? 0.0 : ca[s] * *w0;
+        *w0 = masked ? R(0) : ca[s] * *w0;
       } else {
-        double* w1 = w0 + kUpdLd;
-        const double x0 = *w0, x1 = *w1;
-        *w0 = masked ? 0.0 : fma(ca[s], x0, cb[s] * x1);
-        *w1 = masked ? 0.0 : fma(cb[s + 1], x0, ca[s + 1] * x1);
+        R* w1 = w0 + kUpdLd;
+        const R x0 = *w0, x1 = *w1;
+        *w0 = masked ? R(0) : fma(ca[s], x0, cb[s] * x1);
+        *w1 = masked ? R(0) : fma(cb[s + 1], x0, ca[s + 1] * x1);
       }
     }
     __syncthreads();
@@ -1147,22 +1196,40 @@ __device__ void app_update(AppFront& F, const StepView& v, int rank, int nr, int
     // whose 16 rows all lie above their first column have nothing to update
     const bool idle = j0 + cbase >= col_hi || i0 + rbase + 15 < j0 + cbase;
     if (idle) continue;
-    double acc[2][4][2];
+    R acc[2][4][2];
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) { acc[a][b][0] = 0.0; acc[a][b][1] = 0.0; }
+      for (int b = 0; b < 4; ++b) { acc[a][b][0] = R(0); acc[a][b][1] = R(0); }
+    if constexpr (sizeof(R) == 8) {
 #pragma unroll 2
-    for (int s0 = 0; s0 < Kpad; s0 += 4) {
-      double af[2], bf[4];
+      for (int s0 = 0; s0 < Kpad; s0 += 4) {
+        double af[2], bf[4];
 #pragma unroll
-      for (int a = 0; a < 2; ++a) af[a] = Ls[(s0 + t4) * kUpdLd + rbase + 8 * a + g];
+        for (int a = 0; a < 2; ++a) af[a] = Ls[(s0 + t4) * kUpdLd + rbase + 8 * a + g];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) bf[b] = Ws[(s0 + t4) * kUpdLd + cbase + 8 * b + g];
+        for (int b = 0; b < 4; ++b) bf[b] = Ws[(s0 + t4) * kUpdLd + cbase + 8 * b + g];
 #pragma unroll
-      for (int a = 0; a < 2; ++a)
+        for (int a = 0; a < 2; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) dmma_m8n8k4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+          for (int b = 0; b < 4; ++b) dmma_m8n8k4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+      }
+    } else {
+      // FP32: the thread's own 2 x 8 outputs by rank-1 steps (two L values, four W pairs per pivot)
+#pragma unroll 4
+      for (int s = 0; s < K; ++s) {
+        const R* ls = Ls + s * kUpdLd + rbase + g;
+        const R* ws = Ws + s * kUpdLd + cbase + 2 * t4;
+        const R l0 = ls[0], l1 = ls[8];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const auto w2 = load_pair(ws + 8 * b);
+          acc[0][b][0] = fma(l0, w2.x, acc[0][b][0]);
+          acc[0][b][1] = fma(l0, w2.y, acc[0][b][1]);
+          acc[1][b][0] = fma(l1, w2.x, acc[1][b][0]);
+          acc[1][b][1] = fma(l1, w2.y, acc[1][b][1]);
+        }
+      }
     }
 #pragma unroll
     for (int b = 0; b < 4; ++b)
@@ -1179,7 +1246,8 @@ __device__ void app_update(AppFront& F, const StepView& v, int rank, int nr, int
 }
 
 // Rank 0: advance past the accepted pivots; move rejected columns behind the candidates.
-__device__ void app_advance(AppFront& F, int q) {
+template <class R>
+__device__ void app_advance(AppFront<R>& F, int q) {
   AppCtrl* c = F.ctrl;
   const int p = c->p, w = c->w;
   const int np = p + q, r = w - q;
@@ -1201,14 +1269,15 @@ __device__ void app_advance(AppFront& F, int q) {
   __syncthreads();
 }
 
+template <class R>
 struct AppSmem {
-  double Bs[kNB * kNB];
-  double tmp0[kNB], tmp1[kNB];
+  R Bs[kNB * kNB];
+  R tmp0[kNB], tmp1[kNB];
   int slab[kNB];
   signed char spv[kNB];
   unsigned long long scm[kNB], srm[kNB];
   StepShared bst;
-  double ca[kKB], cb[kKB];
+  R ca[kKB], cb[kKB];
   int cd[kKB];
   int stop, q, ok;
 };
@@ -1261,9 +1330,9 @@ __device__ bool front_barrier(int* bar, int nr, unsigned long long* timeouts, in
 // advances and factorizes the next block right after its update tile, so that the control phase
 // and its barrier are skipped. Alternate panels use alternate per-panel arrays, so the next
 // block's arrays never overlap the ones slower CTAs still read.
-template <bool kCoop>
-__device__ void app_front(AppFront& F, int rank, int nr, const FactorParams& prm, FactorCounters* cnt,
-                          std::int32_t* failed, int* level_done, AppSmem& sm, double* Ls, double* Ws) {
+template <bool kCoop, class R>
+__device__ void app_front(AppFront<R>& F, int rank, int nr, const FactorParams& prm, FactorCounters* cnt,
+                          std::int32_t* failed, int* level_done, AppSmem<R>& sm, R* Ls, R* Ws) {
   const double thr = null_threshold(prm);
   const double inv_u = 1.0 / prm.u;
   int* bar = &F.ctrl->bar;
@@ -1312,16 +1381,17 @@ __device__ void app_front(AppFront& F, int rank, int nr, const FactorParams& prm
 }  // namespace
 
 // One CTA per front (nr = 1), fronts listed in `list`.
-__global__ void __launch_bounds__(kAppThreads) k_front_app(const std::int32_t* list, const SnDev* sn, double* panels,
-                                                           double* cb, double* scratch, signed char* piv_out,
+template <class R>
+__global__ void __launch_bounds__(kAppThreads) k_front_app(const std::int32_t* list, const SnDev* sn, R* panels,
+                                                           R* cb, double* scratch, signed char* piv_out,
                                                            std::int32_t* pidx_out, FactorParams prm,
                                                            FactorCounters* cnt, std::int32_t* failed) {
-  extern __shared__ double app_dyn[];
-  double* Ls = app_dyn;
-  double* Ws = app_dyn + kKB * kUpdLd;
-  __shared__ AppSmem sm;
+  extern __shared__ __align__(16) unsigned char app_dyn[];
+  R* Ls = reinterpret_cast<R*>(app_dyn);
+  R* Ws = Ls + kKB * kUpdLd;
+  __shared__ AppSmem<R> sm;
   const SnDev d = sn[list[blockIdx.x]];
-  AppFront F = make_front(d, panels, cb, scratch, piv_out, pidx_out);
+  AppFront<R> F = make_front(d, panels, cb, scratch, piv_out, pidx_out);
   app_init(F, 0, 1);
   __syncthreads();
   app_front<false>(F, 0, 1, prm, cnt, failed, nullptr, sm, Ls, Ws);
@@ -1329,24 +1399,25 @@ __global__ void __launch_bounds__(kAppThreads) k_front_app(const std::int32_t* l
 
 // Cooperative: the fronts of a level share the grid; front f owns CTAs [cta_start[f], cta_start[f+1])
 // and runs its panel loop with its own barriers, independently of the other fronts.
+template <class R>
 __global__ void __launch_bounds__(kAppThreads) k_front_coop(const std::int32_t* list, const std::int32_t* cta_start,
-                                                            int nfronts, const SnDev* sn, double* panels, double* cb,
+                                                            int nfronts, const SnDev* sn, R* panels, R* cb,
                                                             double* scratch, signed char* piv_out,
                                                             std::int32_t* pidx_out, FactorParams prm,
                                                             FactorCounters* cnt, std::int32_t* failed,
                                                             int* level_done) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
-  extern __shared__ double app_dyn[];
-  double* Ls = app_dyn;
-  double* Ws = app_dyn + kKB * kUpdLd;
-  __shared__ AppSmem sm;
+  extern __shared__ __align__(16) unsigned char app_dyn[];
+  R* Ls = reinterpret_cast<R*>(app_dyn);
+  R* Ws = Ls + kKB * kUpdLd;
+  __shared__ AppSmem<R> sm;
   int fi = 0;
   while (fi + 1 < nfronts && cta_start[fi + 1] <= static_cast<int>(blockIdx.x)) ++fi;
   const int rank = static_cast<int>(blockIdx.x) - cta_start[fi];
   const int nr = cta_start[fi + 1] - cta_start[fi];
   const SnDev d = sn[list[fi]];
-  AppFront F = make_front(d, panels, cb, scratch, piv_out, pidx_out);
+  AppFront<R> F = make_front(d, panels, cb, scratch, piv_out, pidx_out);
   app_init(F, rank, nr);
   grid.sync();  // the control blocks (and their barrier counts) are initialized
   app_front<true>(F, rank, nr, prm, cnt, failed, level_done, sm, Ls, Ws);
@@ -1382,70 +1453,106 @@ void launch_scale_update(std::int64_t n, double* d, unsigned long long* r, cudaS
   k_scale_update<<<blocks, 256, 0, s>>>(n, d, r);
 }
 
+template <class R>
 void launch_scatter(std::int64_t nnz, const std::int32_t* row, const std::int32_t* col, const double* a,
                     const double* b, double alpha, double beta, const double* d, const std::int64_t* dest,
-                    double* panels, FactorCounters* cnt, cudaStream_t s) {
+                    R* panels, FactorCounters* cnt, cudaStream_t s) {
   const int blocks = static_cast<int>(std::min<std::int64_t>((nnz + 255) / 256, 148 * 16));
   note_launches(1);
-  k_scatter<<<blocks, 256, 0, s>>>(nnz, row, col, a, b, alpha, beta, d, dest, panels, cnt);
+  k_scatter<R><<<blocks, 256, 0, s>>>(nnz, row, col, a, b, alpha, beta, d, dest, panels, cnt);
 }
 
-void launch_zero_cb(const std::int32_t* list, int nlist, int chunks, const SnDev* sn, double* cb, cudaStream_t s) {
+template <class R>
+void launch_zero_cb(const std::int32_t* list, int nlist, int chunks, const SnDev* sn, R* cb, cudaStream_t s) {
   if (nlist <= 0) return;
   dim3 grid(nlist, chunks);
   note_launches(1);
-  k_zero_cb<<<grid, 256, 0, s>>>(list, sn, cb);
+  k_zero_cb<R><<<grid, 256, 0, s>>>(list, sn, cb);
 }
 
-void launch_extend_add(const int2* items, int nitems, const SnDev* sn, const std::int32_t* rmap, double* panels,
-                       double* cb, cudaStream_t s) {
+template <class R>
+void launch_extend_add(const int2* items, int nitems, const SnDev* sn, const std::int32_t* rmap, R* panels, R* cb,
+                       cudaStream_t s) {
   if (nitems <= 0) return;
   note_launches(1);
-  k_extend_add<<<nitems, 128, 0, s>>>(items, sn, rmap, panels, cb);
+  k_extend_add<R><<<nitems, 128, 0, s>>>(items, sn, rmap, panels, cb);
 }
 
-void launch_front_small(int maxm, const std::int32_t* list, int nlist, const SnDev* sn, double* panels, double* cb,
+template <class R>
+void launch_front_small(int maxm, const std::int32_t* list, int nlist, const SnDev* sn, R* panels, R* cb,
                         signed char* piv, std::int32_t* pidx, const FactorParams& prm, FactorCounters* cnt,
                         std::int32_t* failed, cudaStream_t s) {
   if (nlist <= 0) return;
-  const std::size_t smem = static_cast<std::size_t>(maxm) * maxm * sizeof(double);
-  if (maxm <= 32) { note_launches(1); k_front_small<32><<<nlist, 128, smem, s>>>(list, sn, panels, cb, piv, pidx, prm, cnt, failed); }
-  else { note_launches(1); k_front_small<kSmallMax><<<nlist, 256, smem, s>>>(list, sn, panels, cb, piv, pidx, prm, cnt, failed); }
+  const std::size_t smem = static_cast<std::size_t>(maxm) * maxm * sizeof(R);
+  note_launches(1);
+  if (maxm <= 32) k_front_small<32, R><<<nlist, 128, smem, s>>>(list, sn, panels, cb, piv, pidx, prm, cnt, failed);
+  else k_front_small<kSmallMax, R><<<nlist, 256, smem, s>>>(list, sn, panels, cb, piv, pidx, prm, cnt, failed);
 }
 
-void launch_front_app(const std::int32_t* list, int nlist, const SnDev* sn, double* panels, double* cb,
-                      double* scratch, signed char* piv, std::int32_t* pidx, const FactorParams& prm,
-                      FactorCounters* cnt, std::int32_t* failed, cudaStream_t s) {
+template <class R>
+constexpr std::size_t app_dyn_bytes() { return static_cast<std::size_t>(kAppDynDoubles) * sizeof(R); }
+
+template <class R>
+void launch_front_app(const std::int32_t* list, int nlist, const SnDev* sn, R* panels, R* cb, double* scratch,
+                      signed char* piv, std::int32_t* pidx, const FactorParams& prm, FactorCounters* cnt,
+                      std::int32_t* failed, cudaStream_t s) {
   if (nlist <= 0) return;
-  constexpr std::size_t smem = kAppDynDoubles * sizeof(double);
+  constexpr std::size_t smem = app_dyn_bytes<R>();
   static std::once_flag configured;
   std::call_once(configured, [&] {
-    cudaFuncSetAttribute(k_front_app, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaFuncSetAttribute(k_front_app<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   });
   note_launches(1);
-  k_front_app<<<nlist, kAppThreads, smem, s>>>(list, sn, panels, cb, scratch, piv, pidx, prm, cnt, failed);
+  k_front_app<R><<<nlist, kAppThreads, smem, s>>>(list, sn, panels, cb, scratch, piv, pidx, prm, cnt, failed);
 }
 
-int coop_max_ctas(int device) {
-  constexpr std::size_t smem = kAppDynDoubles * sizeof(double);
-  cudaFuncSetAttribute(k_front_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+namespace {
+template <class R>
+int coop_max_ctas_of(int device) {
+  constexpr std::size_t smem = app_dyn_bytes<R>();
+  cudaFuncSetAttribute(k_front_coop<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   int per_sm = 0, sms = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_front_coop, kAppThreads, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_front_coop<R>, kAppThreads, smem);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   return per_sm * sms;
 }
+}  // namespace
 
+// co-resident CTAs of the cooperative panel kernel, valid for both factor types (one plan serves a
+// factorization object of either precision)
+int coop_max_ctas(int device) { return std::min(coop_max_ctas_of<double>(device), coop_max_ctas_of<float>(device)); }
+
+template <class R>
 cudaError_t launch_front_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
-                              const SnDev* sn, double* panels, double* cb, double* scratch, signed char* piv,
-                              std::int32_t* pidx, const FactorParams& prm, FactorCounters* cnt, std::int32_t* failed,
-                              int* level_done, cudaStream_t s) {
+                              const SnDev* sn, R* panels, R* cb, double* scratch, signed char* piv, std::int32_t* pidx,
+                              const FactorParams& prm, FactorCounters* cnt, std::int32_t* failed, int* level_done,
+                              cudaStream_t s) {
   if (nfronts <= 0) return cudaSuccess;
-  constexpr std::size_t smem = kAppDynDoubles * sizeof(double);
+  constexpr std::size_t smem = app_dyn_bytes<R>();
   FactorParams p = prm;
   void* args[] = {const_cast<std::int32_t**>(&list), const_cast<std::int32_t**>(&cta_start), &nfronts,
                   const_cast<SnDev**>(&sn), &panels, &cb, &scratch, &piv, &pidx, &p, &cnt, &failed, &level_done};
   note_launches(1);
-  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_front_coop), dim3(nctas), dim3(kAppThreads), args, smem, s);
+  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_front_coop<R>), dim3(nctas), dim3(kAppThreads), args,
+                                     smem, s);
 }
+
+#define HSG_FACTOR_INSTANTIATE(R)                                                                                     \
+  template void launch_scatter<R>(std::int64_t, const std::int32_t*, const std::int32_t*, const double*,             \
+                                  const double*, double, double, const double*, const std::int64_t*, R*,              \
+                                  FactorCounters*, cudaStream_t);                                                     \
+  template void launch_zero_cb<R>(const std::int32_t*, int, int, const SnDev*, R*, cudaStream_t);                     \
+  template void launch_extend_add<R>(const int2*, int, const SnDev*, const std::int32_t*, R*, R*, cudaStream_t);     \
+  template void launch_front_small<R>(int, const std::int32_t*, int, const SnDev*, R*, R*, signed char*,              \
+                                      std::int32_t*, const FactorParams&, FactorCounters*, std::int32_t*,             \
+                                      cudaStream_t);                                                                  \
+  template void launch_front_app<R>(const std::int32_t*, int, const SnDev*, R*, R*, double*, signed char*,            \
+                                    std::int32_t*, const FactorParams&, FactorCounters*, std::int32_t*, cudaStream_t); \
+  template cudaError_t launch_front_coop<R>(const std::int32_t*, const std::int32_t*, int, int, const SnDev*, R*, R*, \
+                                            double*, signed char*, std::int32_t*, const FactorParams&,                 \
+                                            FactorCounters*, std::int32_t*, int*, cudaStream_t);
+HSG_FACTOR_INSTANTIATE(double)
+HSG_FACTOR_INSTANTIATE(float)
+#undef HSG_FACTOR_INSTANTIATE
 
 }  // namespace hsg

@@ -32,24 +32,34 @@ void launch_scale_rowmax(std::int64_t nnz, const std::int32_t* row, const std::i
                          const double* b, double alpha, double beta, const double* d, unsigned long long* r,
                          cudaStream_t s);
 void launch_scale_update(std::int64_t n, double* d, unsigned long long* r, cudaStream_t s);
+// The front kernels are instantiated for R = double (the FP64 factorization that certifies inertia)
+// and R = float (the FP32 operator factorization of the mixed-precision path): panels and
+// contribution blocks hold R, the pivot scratch stays in units of doubles.
+template <class R>
 void launch_scatter(std::int64_t nnz, const std::int32_t* row, const std::int32_t* col, const double* a,
                     const double* b, double alpha, double beta, const double* d, const std::int64_t* dest,
-                    double* panels, FactorCounters* cnt, cudaStream_t s);
-void launch_zero_cb(const std::int32_t* list, int nlist, int chunks, const SnDev* sn, double* cb, cudaStream_t s);
-void launch_extend_add(const int2* items, int nitems, const SnDev* sn, const std::int32_t* rmap, double* panels,
-                       double* cb, cudaStream_t s);
-void launch_front_small(int maxm, const std::int32_t* list, int nlist, const SnDev* sn, double* panels, double* cb,
+                    R* panels, FactorCounters* cnt, cudaStream_t s);
+template <class R>
+void launch_zero_cb(const std::int32_t* list, int nlist, int chunks, const SnDev* sn, R* cb, cudaStream_t s);
+template <class R>
+void launch_extend_add(const int2* items, int nitems, const SnDev* sn, const std::int32_t* rmap, R* panels, R* cb,
+                       cudaStream_t s);
+template <class R>
+void launch_front_small(int maxm, const std::int32_t* list, int nlist, const SnDev* sn, R* panels, R* cb,
                         signed char* piv, std::int32_t* pidx, const FactorParams& prm, FactorCounters* cnt,
                         std::int32_t* failed, cudaStream_t s);
-void launch_front_app(const std::int32_t* list, int nlist, const SnDev* sn, double* panels, double* cb,
-                      double* scratch, signed char* piv, std::int32_t* pidx, const FactorParams& prm,
-                      FactorCounters* cnt, std::int32_t* failed, cudaStream_t s);
+template <class R>
+void launch_front_app(const std::int32_t* list, int nlist, const SnDev* sn, R* panels, R* cb, double* scratch,
+                      signed char* piv, std::int32_t* pidx, const FactorParams& prm, FactorCounters* cnt,
+                      std::int32_t* failed, cudaStream_t s);
 
-// cooperative launch over the large fronts of a level (see factor_kernels.cu)
+// cooperative launch over the large fronts of a level (see factor_kernels.cu); the co-resident grid
+// is the smaller of the two instantiations'
 int coop_max_ctas(int device);
+template <class R>
 cudaError_t launch_front_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
-                              const SnDev* sn, double* panels, double* cb, double* scratch, signed char* piv,
-                              std::int32_t* pidx, const FactorParams& prm, FactorCounters* cnt, std::int32_t* failed,
-                              int* level_done, cudaStream_t s);
+                              const SnDev* sn, R* panels, R* cb, double* scratch, signed char* piv, std::int32_t* pidx,
+                              const FactorParams& prm, FactorCounters* cnt, std::int32_t* failed, int* level_done,
+                              cudaStream_t s);
 
 }  // namespace hsg

@@ -142,7 +142,9 @@ GpuFactor::GpuFactor(const hsg_options_t& opt) : opt_(opt) {
   int count = 0;
   cuda_check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
   HSG_REQUIRE(opt_.device >= 0 && opt_.device < count, HSG_INVALID_INPUT, "no CUDA device " << opt_.device);
-  HSG_REQUIRE(opt_.precision == 0, HSG_UNSUPPORTED, "only double-precision factors are built into this handle type");
+  HSG_REQUIRE(opt_.precision == 0 || opt_.precision == 1, HSG_INVALID_INPUT, "precision must be 0 (double) or 1 (single)");
+  HSG_REQUIRE(opt_.precision == 0 || (opt_.single_null_pivot_tol > 0.0 && opt_.single_null_pivot_tol < 1.0),
+              HSG_INVALID_INPUT, "single_null_pivot_tol outside (0, 1)");
   HSG_REQUIRE(opt_.pivot_threshold > 0.0 && opt_.pivot_threshold <= 0.5, HSG_INVALID_INPUT, "pivot threshold outside (0, 0.5]");
   HSG_REQUIRE(opt_.null_pivot_tol > 0.0 && opt_.null_pivot_tol < 1.0, HSG_INVALID_INPUT, "null_pivot_tol outside (0, 1)");
   DeviceGuard g(opt_.device);
@@ -485,14 +487,25 @@ void GpuFactor::build_plan() {
   d_children_.upload(S.children, stream_);
   d_iperm_.upload(S.iperm, stream_);
   d_dest_.upload(S.dest, stream_);
-  d_panels_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, S.factor_entries)));
-  d_cb_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, S.cb_arena)));
+  const std::size_t fe = static_cast<std::size_t>(std::max<std::int64_t>(1, S.factor_entries));
+  const std::size_t cbe = static_cast<std::size_t>(std::max<std::int64_t>(1, S.cb_arena));
+  const std::size_t inve = static_cast<std::size_t>(std::max<std::int64_t>(1, inv_total));
+  const std::size_t we = static_cast<std::size_t>(std::max<std::int64_t>(1, w_total));
+  if (single()) {
+    d_panels_f_.alloc(fe);
+    d_cb_f_.alloc(cbe);
+    d_inv_f_.alloc(inve);
+    d_w_f_.alloc(we);
+  } else {
+    d_panels_.alloc(fe);
+    d_cb_.alloc(cbe);
+    d_inv_.alloc(inve);
+    d_w_.alloc(we);
+  }
   d_scratch_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, scratch_max)));
   d_level_done_.alloc(static_cast<std::size_t>(std::max(1, ncoop_)));
-  d_inv_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, inv_total)));
   d_work_off_.upload(work_offs, stream_);
   d_work_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, work_max)));
-  d_w_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, w_total)));
   d_err_.alloc(1);
   d_cptr_.upload(cptr, stream_);
   d_cent_.upload(cent, stream_);
@@ -509,8 +522,30 @@ void GpuFactor::build_plan() {
     HSG_REQUIRE((sn[s].k + 30) / 31 <= kMaxBlocksPerFront, HSG_UNSUPPORTED, "front with " << sn[s].k << " pivots exceeds the solve block table");
 }
 
+template <> double* GpuFactor::panels_of<double>() { return d_panels_.p; }
+template <> float* GpuFactor::panels_of<float>() { return d_panels_f_.p; }
+template <> double* GpuFactor::cb_of<double>() { return d_cb_.p; }
+template <> float* GpuFactor::cb_of<float>() { return d_cb_f_.p; }
+template <> double* GpuFactor::w_of<double>() { return d_w_.p; }
+template <> float* GpuFactor::w_of<float>() { return d_w_f_.p; }
+template <> double* GpuFactor::inv_of<double>() { return d_inv_.p; }
+template <> float* GpuFactor::inv_of<float>() { return d_inv_f_.p; }
+
+std::size_t GpuFactor::factor_bytes() const {
+  const std::size_t el = single() ? sizeof(float) : sizeof(double);
+  return el * (d_panels_.n + d_panels_f_.n + d_w_.n + d_w_f_.n + d_inv_.n + d_inv_f_.n);
+}
+
 void GpuFactor::run_numeric(double alpha, double beta, bool detection) {
+  if (single()) run_numeric_t<float>(alpha, beta, detection);
+  else run_numeric_t<double>(alpha, beta, detection);
+}
+
+template <class R>
+void GpuFactor::run_numeric_t(double alpha, double beta, bool detection) {
   cudaStream_t s = stream_;
+  R* panels = panels_of<R>();
+  R* cb = cb_of<R>();
   cuda_check(cudaMemsetAsync(d_cnt_.p, 0, sizeof(FactorCounters), s), "memset counters");
   cuda_check(cudaMemsetAsync(d_level_done_.p, 0, d_level_done_.n * sizeof(int), s), "memset level flags");
   launch_fill(d_scale_.p, n_, 1.0, s);
@@ -521,32 +556,37 @@ void GpuFactor::run_numeric(double alpha, double beta, bool detection) {
       launch_scale_update(n_, d_scale_.p, d_r_.p, s);
     }
   }
-  cuda_check(cudaMemsetAsync(d_panels_.p, 0, sym_.factor_entries * sizeof(double), s), "memset panels");
-  launch_scatter(nnz_, d_row_.p, d_col_.p, d_a_.p, d_b_.p, alpha, beta, d_scale_.p, d_dest_.p, d_panels_.p, d_cnt_.p, s);
+  cuda_check(cudaMemsetAsync(panels, 0, sym_.factor_entries * sizeof(R), s), "memset panels");
+  launch_scatter<R>(nnz_, d_row_.p, d_col_.p, d_a_.p, d_b_.p, alpha, beta, d_scale_.p, d_dest_.p, panels, d_cnt_.p, s);
   FactorParams prm;
   prm.u = opt_.pivot_threshold;
-  prm.null_tol = detection ? opt_.null_pivot_tol : 0.0;
+  // null pivots relative to the largest scaled entry: 1e-8 for FP64 factors, 1e-4 for FP32
+  // (include/hsolve/factor.hpp:279-283 in hsolve)
+  prm.null_tol = detection ? (single() ? opt_.single_null_pivot_tol : opt_.null_pivot_tol) : 0.0;
   prm.cnt = d_cnt_.p;
   prm.failed_cap = static_cast<std::int32_t>(n_);
   const std::int32_t* lists = d_lists_.p;
   for (const LevelPlan& L : levels_) {
-    launch_zero_cb(lists + L.zero_off, L.zero_n, L.zero_chunks, d_sn_.p, d_cb_.p, s);
-    for (const auto& ea : L.ea) launch_extend_add(d_items_.p + ea.first, ea.second, d_sn_.p, d_rmap_.p, d_panels_.p, d_cb_.p, s);
-    launch_front_small(32, lists + L.s32_off, L.s32_n, d_sn_.p, d_panels_.p, d_cb_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
-    launch_front_small(kSmallMax, lists + L.s64_off, L.s64_n, d_sn_.p, d_panels_.p, d_cb_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
+    launch_zero_cb<R>(lists + L.zero_off, L.zero_n, L.zero_chunks, d_sn_.p, cb, s);
+    for (const auto& ea : L.ea) launch_extend_add<R>(d_items_.p + ea.first, ea.second, d_sn_.p, d_rmap_.p, panels, cb, s);
+    launch_front_small<R>(32, lists + L.s32_off, L.s32_n, d_sn_.p, panels, cb, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
+    launch_front_small<R>(kSmallMax, lists + L.s64_off, L.s64_n, d_sn_.p, panels, cb, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
     if (shared_ ? L.coop_shared : L.coop) {
       const std::int64_t cta_off = shared_ ? L.cta_off_shared : L.cta_off;
       const int ctas = shared_ ? L.coop_ctas_shared : L.coop_ctas;
-      cuda_check(launch_front_coop(lists + L.app_off, lists + cta_off, L.app_n, ctas, d_sn_.p, d_panels_.p,
-                                   d_cb_.p, d_scratch_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p,
-                                   d_level_done_.p + L.done_slot, s),
+      cuda_check(launch_front_coop<R>(lists + L.app_off, lists + cta_off, L.app_n, ctas, d_sn_.p, panels, cb,
+                                      d_scratch_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p,
+                                      d_level_done_.p + L.done_slot, s),
                  "cooperative front launch");
     } else {
-      launch_front_app(lists + L.app_off, L.app_n, d_sn_.p, d_panels_.p, d_cb_.p, d_scratch_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
+      launch_front_app<R>(lists + L.app_off, L.app_n, d_sn_.p, panels, cb, d_scratch_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
     }
   }
   cuda_check(cudaGetLastError(), "factorization launch");
 }
+
+template void GpuFactor::run_numeric_t<double>(double, double, bool);
+template void GpuFactor::run_numeric_t<float>(double, double, bool);
 
 hsg_inertia_t GpuFactor::factorize(double alpha, double beta, bool detection, bool shared) {
   shared_ = shared;
@@ -622,37 +662,7 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
   cuda_check(cudaEventRecord(ev0_, s), "event");
   build_solve_operator();
   launch_gather_scale(n_, nr, db, ld, d_scale_.p, d_iperm_.p, d_xwork_.p, s);
-  const std::int32_t* lists = d_lists_.p;
-  // chunks of at most 8 right-hand sides (the cooperative sweeps carry 8)
-  for (int c0 = 0; c0 < nr; c0 += 8) {
-    const int nc = std::min(8, nr - c0);
-    double* xw = d_xwork_.p + static_cast<std::int64_t>(c0) * n_;
-    cuda_check(cudaMemsetAsync(d_sweep_cnt_.p, 0, d_sweep_cnt_.n * sizeof(int), s), "reset sweep counters");
-    for (const LevelPlan& L : levels_) {
-      if (L.solve_coop) {
-        cuda_check(launch_solve_fwd_coop(lists + L.all_off, lists + L.solve_cta_off, L.all_n, L.solve_ctas, d_sn_.p,
-                                         d_cptr_.p, d_cent_.p, d_w_.p, d_pidx_.p, xw, n_, d_vec_.p, nc, d_work_.p,
-                                         d_work_off_.p + L.work_off_off, d_sweep_cnt_.p + L.cnt_off, d_err_.p, s),
-                   "cooperative forward solve");
-      } else {
-        launch_solve_fwd(lists + L.all_off, L.all_n, L.maxm, d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p,
-                         d_panels_.p, d_piv_.p, d_pidx_.p, d_blk_.p, d_nblk_.p, d_inv_.p, xw, n_, d_vec_.p, nc, s);
-      }
-    }
-    launch_solve_diag_flat(n_, d_dpos_.p, d_pfirst_.p, d_panels_.p, d_piv_.p, d_pidx_.p, xw, n_, nc, s);
-    for (auto it = levels_.rbegin(); it != levels_.rend(); ++it) {
-      if (it->solve_coop) {
-        cuda_check(launch_solve_bwd_coop(lists + it->all_off, lists + it->solve_cta_off, it->all_n, it->solve_ctas,
-                                         d_sn_.p, d_rows_.p, d_w_.p, d_pidx_.p, xw, n_, nc, d_work_.p,
-                                         d_work_off_.p + it->work_off_off,
-                                         d_sweep_cnt_.p + sweep_cnt_total_ + it->cnt_off, d_err_.p, s),
-                   "cooperative backward solve");
-      } else {
-        launch_solve_bwd(lists + it->all_off, it->all_n, it->maxm, d_sn_.p, d_rows_.p, d_panels_.p, d_pidx_.p, d_blk_.p,
-                         d_nblk_.p, d_inv_.p, xw, n_, nc, s);
-      }
-    }
-  }
+  run_sweeps(d_xwork_.p, d_vec_.p, nr);
   launch_scatter_scale(n_, nr, db, ld, d_scale_.p, d_iperm_.p, d_xwork_.p, s);
   cuda_check(cudaEventRecord(ev1_, s), "event");
   cuda_check(cudaGetLastError(), "solve launch");
@@ -697,36 +707,7 @@ void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ld
   cuda_check(cudaMemsetAsync(d_err_.p, 0, sizeof(int), s), "reset solve status");
   build_solve_operator();
   launch_gather_scale(n_, nr, b, ldb, d_scale_.p, d_iperm_.p, xwork, s);
-  const std::int32_t* lists = d_lists_.p;
-  for (int c0 = 0; c0 < nr; c0 += 8) {
-    const int nc = std::min(8, nr - c0);
-    double* xw = xwork + static_cast<std::int64_t>(c0) * n_;
-    cuda_check(cudaMemsetAsync(d_sweep_cnt_.p, 0, d_sweep_cnt_.n * sizeof(int), s), "reset sweep counters");
-    for (const LevelPlan& L : levels_) {
-      if (L.solve_coop) {
-        cuda_check(launch_solve_fwd_coop(lists + L.all_off, lists + L.solve_cta_off, L.all_n, L.solve_ctas, d_sn_.p,
-                                         d_cptr_.p, d_cent_.p, d_w_.p, d_pidx_.p, xw, n_, vec, nc, d_work_.p,
-                                         d_work_off_.p + L.work_off_off, d_sweep_cnt_.p + L.cnt_off, d_err_.p, s),
-                   "cooperative forward solve");
-      } else {
-        launch_solve_fwd(lists + L.all_off, L.all_n, L.maxm, d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p,
-                         d_panels_.p, d_piv_.p, d_pidx_.p, d_blk_.p, d_nblk_.p, d_inv_.p, xw, n_, vec, nc, s);
-      }
-    }
-    launch_solve_diag_flat(n_, d_dpos_.p, d_pfirst_.p, d_panels_.p, d_piv_.p, d_pidx_.p, xw, n_, nc, s);
-    for (auto it = levels_.rbegin(); it != levels_.rend(); ++it) {
-      if (it->solve_coop) {
-        cuda_check(launch_solve_bwd_coop(lists + it->all_off, lists + it->solve_cta_off, it->all_n, it->solve_ctas,
-                                         d_sn_.p, d_rows_.p, d_w_.p, d_pidx_.p, xw, n_, nc, d_work_.p,
-                                         d_work_off_.p + it->work_off_off,
-                                         d_sweep_cnt_.p + sweep_cnt_total_ + it->cnt_off, d_err_.p, s),
-                   "cooperative backward solve");
-      } else {
-        launch_solve_bwd(lists + it->all_off, it->all_n, it->maxm, d_sn_.p, d_rows_.p, d_panels_.p, d_pidx_.p, d_blk_.p,
-                         d_nblk_.p, d_inv_.p, xw, n_, nc, s);
-      }
-    }
-  }
+  run_sweeps(xwork, vec, nr);
   launch_scatter_scale(n_, nr, b, ldb, d_scale_.p, d_iperm_.p, xwork, s);
   cuda_check(cudaGetLastError(), "solve launch");
   int err = 0;
@@ -735,11 +716,61 @@ void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ld
   HSG_REQUIRE(err == 0, HSG_INTERNAL, "solve: a wait between the CTAs of a front timed out");
 }
 
+void GpuFactor::run_sweeps(double* xwork, double* vec, int nr) {
+  if (single()) run_sweeps_t<float>(xwork, vec, nr);
+  else run_sweeps_t<double>(xwork, vec, nr);
+}
+
+template <class F>
+void GpuFactor::run_sweeps_t(double* xwork, double* vec, int nr) {
+  cudaStream_t s = stream_;
+  const F* panels = panels_of<F>();
+  const F* W = w_of<F>();
+  const F* inv = inv_of<F>();
+  const std::int32_t* lists = d_lists_.p;
+  // chunks of at most 8 right-hand sides (the cooperative sweeps carry 8)
+  for (int c0 = 0; c0 < nr; c0 += 8) {
+    const int nc = std::min(8, nr - c0);
+    double* xw = xwork + static_cast<std::int64_t>(c0) * n_;
+    cuda_check(cudaMemsetAsync(d_sweep_cnt_.p, 0, d_sweep_cnt_.n * sizeof(int), s), "reset sweep counters");
+    for (const LevelPlan& L : levels_) {
+      if (L.solve_coop) {
+        cuda_check(launch_solve_fwd_coop<F>(lists + L.all_off, lists + L.solve_cta_off, L.all_n, L.solve_ctas, d_sn_.p,
+                                            d_cptr_.p, d_cent_.p, W, d_pidx_.p, xw, n_, vec, nc, d_work_.p,
+                                            d_work_off_.p + L.work_off_off, d_sweep_cnt_.p + L.cnt_off, d_err_.p, s),
+                   "cooperative forward solve");
+      } else {
+        launch_solve_fwd<F>(lists + L.all_off, L.all_n, L.maxm, d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p,
+                            panels, d_piv_.p, d_pidx_.p, d_blk_.p, d_nblk_.p, inv, xw, n_, vec, nc, s);
+      }
+    }
+    launch_solve_diag_flat<F>(n_, d_dpos_.p, d_pfirst_.p, panels, d_piv_.p, d_pidx_.p, xw, n_, nc, s);
+    for (auto it = levels_.rbegin(); it != levels_.rend(); ++it) {
+      if (it->solve_coop) {
+        cuda_check(launch_solve_bwd_coop<F>(lists + it->all_off, lists + it->solve_cta_off, it->all_n, it->solve_ctas,
+                                            d_sn_.p, d_rows_.p, W, d_pidx_.p, xw, n_, nc, d_work_.p,
+                                            d_work_off_.p + it->work_off_off,
+                                            d_sweep_cnt_.p + sweep_cnt_total_ + it->cnt_off, d_err_.p, s),
+                   "cooperative backward solve");
+      } else {
+        launch_solve_bwd<F>(lists + it->all_off, it->all_n, it->maxm, d_sn_.p, d_rows_.p, panels, d_pidx_.p, d_blk_.p,
+                            d_nblk_.p, inv, xw, n_, nc, s);
+      }
+    }
+  }
+}
+
 void GpuFactor::build_solve_operator() {
   if (w_ready_) return;
-  launch_inv_blocks(sym_.ns, d_sn_.p, d_panels_.p, d_piv_.p, d_blk_.p, d_nblk_.p, d_inv_.p, stream_);
-  launch_sb_build(d_sbl_.p, nsbl_, d_tiles_.p, ntiles_, d_sn_.p, d_panels_.p, d_piv_.p, d_w_.p, stream_);
+  if (single()) build_solve_operator_t<float>();
+  else build_solve_operator_t<double>();
   w_ready_ = true;
+}
+
+template <class F>
+void GpuFactor::build_solve_operator_t() {
+  launch_inv_blocks<F>(sym_.ns, d_sn_.p, panels_of<F>(), d_piv_.p, d_blk_.p, d_nblk_.p, inv_of<F>(), stream_);
+  launch_sb_build<F>(d_sbl_.p, nsbl_, d_tiles_.p, ntiles_, d_sn_.p, panels_of<F>(), d_piv_.p, w_of<F>(), stream_);
 }
 
 void GpuFactor::release() {
@@ -753,7 +784,8 @@ hsg_estimate_t GpuFactor::estimate() const {
   e.factor_entries = sym_.factor_entries;
   e.nnz_l = sym_.nnz_l;
   e.flops = sym_.flops;
-  e.device_mb = 8.0 * static_cast<double>(sym_.factor_entries + sym_.cb_arena + 4 * nnz_ + 4 * n_) / 1e6;
+  const double el = single() ? 4.0 : 8.0;  // bytes of a factor entry
+  e.device_mb = (el * static_cast<double>(sym_.factor_entries + sym_.cb_arena) + 8.0 * static_cast<double>(4 * nnz_ + 4 * n_)) / 1e6;
   e.supernodes = sym_.ns;
   e.levels = sym_.nlevels;
   e.max_front = sym_.max_front;

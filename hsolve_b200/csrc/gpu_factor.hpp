@@ -132,6 +132,31 @@ class GpuFactor {
   };
   void build_plan();
   void run_numeric(double alpha, double beta, bool detection);
+  template <class R>
+  void run_numeric_t(double alpha, double beta, bool detection);
+  // forward, diagonal and backward sweeps of nr right-hand sides gathered in xwork (n x nr)
+  void run_sweeps(double* xwork, double* vec, int nr);
+  template <class F>
+  void run_sweeps_t(double* xwork, double* vec, int nr);
+  template <class F>
+  void build_solve_operator_t();
+  template <class R>
+  R* panels_of();
+  template <class R>
+  R* cb_of();
+  template <class R>
+  R* w_of();
+  template <class R>
+  R* inv_of();
+
+ public:
+  // FP32 factors (hsg_options_t.precision == 1): the operator factorization of the mixed-precision
+  // path, solved with FP64 right-hand sides and refined by the caller against the FP64 pencil.
+  bool single() const { return opt_.precision == 1; }
+  // Entries of the factor storage (panels + solve operators) times the element size.
+  std::size_t factor_bytes() const;
+
+ private:
 
   hsg_options_t opt_;
   cudaStream_t stream_ = nullptr;
@@ -152,6 +177,7 @@ class GpuFactor {
   DevBuf<std::int32_t> d_row_, d_col_, d_rmap_, d_rows_, d_child_ptr_, d_children_, d_iperm_, d_lists_, d_pidx_,
       d_failed_;
   DevBuf<double> d_a_, d_b_, d_scale_, d_panels_, d_cb_, d_scratch_, d_vec_, d_xwork_, d_btmp_, d_inv_;
+  DevBuf<float> d_panels_f_, d_cb_f_, d_w_f_, d_inv_f_;  // the same, for FP32 factors
   DevBuf<std::int32_t> d_blk_, d_nblk_;
   DevBuf<std::int64_t> d_dest_;
   DevBuf<unsigned long long> d_r_;

@@ -53,8 +53,9 @@ __device__ __forceinline__ int block_size_at(const signed char* pv, int b, int k
 // excluded), so that the solves apply each block as one small matrix-vector product instead of a
 // chain of dependent pivot steps. One CTA per front; warp w inverts blocks w, w + 8, ...; lane c
 // computes column c by forward substitution.
-__global__ void __launch_bounds__(256) k_inv_blocks(const SnDev* sn, const double* panels, const signed char* piv,
-                                                     std::int32_t* blk, std::int32_t* nblk, double* inv) {
+template <class F>
+__global__ void __launch_bounds__(256) k_inv_blocks(const SnDev* sn, const F* panels, const signed char* piv,
+                                                     std::int32_t* blk, std::int32_t* nblk, F* inv) {
   __shared__ int starts[kMaxBlocksPerFront];
   __shared__ int nb;
   const int s = blockIdx.x;
@@ -73,12 +74,12 @@ __global__ void __launch_bounds__(256) k_inv_blocks(const SnDev* sn, const doubl
   }
   __syncthreads();
   for (int i = threadIdx.x; i < nb; i += blockDim.x) blk[d.first + i] = starts[i];
-  const double* P = panels + d.panel_off;
+  const F* P = panels + d.panel_off;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   for (int bi = warp; bi < nb; bi += nwarps) {
     const int b = starts[bi];
     const int bs = bi + 1 < nb ? starts[bi + 1] - b : k - b;
-    double* out = inv + d.inv_off + static_cast<std::int64_t>(bi) * 1024;
+    F* out = inv + d.inv_off + static_cast<std::int64_t>(bi) * 1024;
     double x[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) x[i] = 0.0;
@@ -94,17 +95,18 @@ __global__ void __launch_bounds__(256) k_inv_blocks(const SnDev* sn, const doubl
       }
     }
 #pragma unroll
-    for (int i = 0; i < 32; ++i) out[lane * 32 + i] = (lane < bs) ? x[i] : 0.0;
+    for (int i = 0; i < 32; ++i) out[lane * 32 + i] = static_cast<F>((lane < bs) ? x[i] : 0.0);
   }
 }
 
 // Forward sweep of the listed fronts. t (m x R, row-major) in dynamic shared memory.
+template <class F>
 __global__ void __launch_bounds__(256) k_solve_fwd(const std::int32_t* list, const SnDev* sn,
                                                     const std::int32_t* child_ptr, const std::int32_t* children,
-                                                    const std::int32_t* rmap, const double* panels,
+                                                    const std::int32_t* rmap, const F* panels,
                                                     const signed char* piv, const std::int32_t* pidx,
                                                     const std::int32_t* blk, const std::int32_t* nblk,
-                                                    const double* inv, double* x, std::int64_t n, double* vec,
+                                                    const F* inv, double* x, std::int64_t n, double* vec,
                                                     int nrhs, int R) {
   extern __shared__ double smem[];
   __shared__ double zb[32 * 8];
@@ -113,11 +115,11 @@ __global__ void __launch_bounds__(256) k_solve_fwd(const std::int32_t* list, con
   const int m = d.m, k = d.k, c = m - k;
   double* t = smem;
   int* invp = reinterpret_cast<int*>(smem + static_cast<std::int64_t>(m) * R);
-  const double* P = panels + d.panel_off;
+  const F* P = panels + d.panel_off;
   const std::int32_t* pl = pidx + d.first;
   const std::int32_t* bst = blk + d.first;
   const int nb = nblk[s];
-  const double* Linv = inv + d.inv_off;
+  const F* Linv = inv + d.inv_off;
   for (int i = threadIdx.x; i < k; i += blockDim.x) invp[pl[i]] = i;
   for (int r0 = 0; r0 < nrhs; r0 += R) {
     const int rr = nrhs - r0 < R ? nrhs - r0 : R;
@@ -145,7 +147,7 @@ __global__ void __launch_bounds__(256) k_solve_fwd(const std::int32_t* list, con
       const int b = bst[bi];
       const int be = bi + 1 < nb ? bst[bi + 1] : k;
       const int bs = be - b;
-      const double* Li = Linv + static_cast<std::int64_t>(bi) * 1024;
+      const F* Li = Linv + static_cast<std::int64_t>(bi) * 1024;
       // z_blk = Linv t_blk   (thread (i, r))
       {
         const int i = threadIdx.x % 32, r = threadIdx.x / 32;
@@ -184,10 +186,11 @@ __global__ void __launch_bounds__(256) k_solve_fwd(const std::int32_t* list, con
 }
 
 // Diagonal solve D y = z, one CTA per front.
-__global__ void k_solve_diag(const SnDev* sn, const double* panels, const signed char* piv, const std::int32_t* pidx,
+template <class F>
+__global__ void k_solve_diag(const SnDev* sn, const F* panels, const signed char* piv, const std::int32_t* pidx,
                              double* x, std::int64_t n, int nrhs) {
   const SnDev d = sn[blockIdx.x];
-  const double* P = panels + d.panel_off;
+  const F* P = panels + d.panel_off;
   for (int j = threadIdx.x; j < d.k; j += blockDim.x) {
     const signed char ty = piv[d.first + j];
     if (ty == 3) continue;
@@ -213,8 +216,9 @@ __global__ void k_solve_diag(const SnDev* sn, const double* panels, const signed
 
 // Diagonal solve D y = z over all pivots at once (one thread per pivot position p): dpos[p] is the
 // panel index of D(p, p), pfirst[p] the first global column of p's front.
+template <class F>
 __global__ void k_solve_diag_flat(std::int64_t npiv, const std::int64_t* dpos, const std::int32_t* pfirst,
-                                  const double* panels, const signed char* piv, const std::int32_t* pidx, double* x,
+                                  const F* panels, const signed char* piv, const std::int32_t* pidx, double* x,
                                   std::int64_t n, int nrhs) {
   const std::int64_t p = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (p >= npiv) return;
@@ -239,22 +243,23 @@ __global__ void k_solve_diag_flat(std::int64_t npiv, const std::int64_t* dpos, c
 }
 
 // Backward sweep of the listed fronts (ancestors done): right-looking over the blocks, last first.
+template <class F>
 __global__ void __launch_bounds__(256) k_solve_bwd(const std::int32_t* list, const SnDev* sn, const std::int32_t* rows,
-                                                    const double* panels, const std::int32_t* pidx,
+                                                    const F* panels, const std::int32_t* pidx,
                                                     const std::int32_t* blk, const std::int32_t* nblk,
-                                                    const double* inv, double* x, std::int64_t n, int nrhs, int R) {
+                                                    const F* inv, double* x, std::int64_t n, int nrhs, int R) {
   extern __shared__ double smem[];
   __shared__ double zb[32 * 8];
   const int s = list[blockIdx.x];
   const SnDev d = sn[s];
   const int m = d.m, k = d.k;
   double* t = smem;
-  const double* P = panels + d.panel_off;
+  const F* P = panels + d.panel_off;
   const std::int32_t* pl = pidx + d.first;
   const std::int32_t* rw = rows + d.rows_off;
   const std::int32_t* bst = blk + d.first;
   const int nb = nblk[s];
-  const double* Linv = inv + d.inv_off;
+  const F* Linv = inv + d.inv_off;
   for (int r0 = 0; r0 < nrhs; r0 += R) {
     const int rr = nrhs - r0 < R ? nrhs - r0 : R;
     __syncthreads();
@@ -268,7 +273,7 @@ __global__ void __launch_bounds__(256) k_solve_bwd(const std::int32_t* list, con
     // t_j -= sum_{i >= k} L[i, j] t_i  (thread per column; the column is contiguous)
     for (int j = threadIdx.x; j < k; j += blockDim.x) {
       double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      const double* Lj = P + static_cast<std::int64_t>(j) * m;
+      const F* Lj = P + static_cast<std::int64_t>(j) * m;
       for (int i = k; i < m; ++i) {
         const double l = Lj[i];
 #pragma unroll
@@ -284,7 +289,7 @@ __global__ void __launch_bounds__(256) k_solve_bwd(const std::int32_t* list, con
       const int b = bst[bi];
       const int be = bi + 1 < nb ? bst[bi + 1] : k;
       const int bs = be - b;
-      const double* Li = Linv + static_cast<std::int64_t>(bi) * 1024;
+      const F* Li = Linv + static_cast<std::int64_t>(bi) * 1024;
       // x_blk = Linv^T t_blk  (thread (c, r))
       {
         const int cc = threadIdx.x % 32, r = threadIdx.x / 32;
@@ -302,7 +307,7 @@ __global__ void __launch_bounds__(256) k_solve_bwd(const std::int32_t* list, con
       // earlier pivots: t_j -= sum_{i in blk} L[i, j] x_i  (thread per column j < b)
       for (int j = threadIdx.x; j < b; j += blockDim.x) {
         double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        const double* Lj = P + static_cast<std::int64_t>(j) * m + b;
+        const F* Lj = P + static_cast<std::int64_t>(j) * m + b;
         for (int i = 0; i < bs; ++i) {
           const double l = Lj[i];
 #pragma unroll
@@ -349,8 +354,9 @@ __device__ __forceinline__ int front_of(const std::int32_t* cta_start, int nfron
 
 // W[B, B] = L_BB^{-1} for one super-block per CTA: row-by-row substitution X[i, c] =
 // -sum_{c <= j < i} L[i, j] X[j, c] on packed triangles in shared memory (two threads per column).
-__global__ void __launch_bounds__(256) k_sb_inverse(const int2* sbl, const SnDev* sn, const double* panels,
-                                                     const signed char* piv, double* W) {
+template <class F>
+__global__ void __launch_bounds__(256) k_sb_inverse(const int2* sbl, const SnDev* sn, const F* panels,
+                                                     const signed char* piv, F* W) {
   extern __shared__ double sm[];
   double* Lp = sm;                                // strictly lower rows, row i at i(i-1)/2
   double* Xp = sm + kSB * (kSB - 1) / 2;          // lower rows incl. diagonal, row i at i(i+1)/2
@@ -359,7 +365,7 @@ __global__ void __launch_bounds__(256) k_sb_inverse(const int2* sbl, const SnDev
   const SnDev d = sn[e.x];
   const int m = d.m;
   const int b = e.y * kSB, bs = min(kSB, d.k - b);
-  const double* P = panels + d.panel_off;
+  const F* P = panels + d.panel_off;
   const signed char* pv = piv + d.first;
   for (int idx = threadIdx.x; idx < bs * bs; idx += blockDim.x) {
     const int j = idx / bs, i = idx % bs;
@@ -377,25 +383,26 @@ __global__ void __launch_bounds__(256) k_sb_inverse(const int2* sbl, const SnDev
     if (h == 0 && c <= i) Xp[i * (i + 1) / 2 + c] = c == i ? 1.0 : -(acc + part[c]);
     __syncthreads();
   }
-  double* Wd = W + d.w_off + b + static_cast<std::int64_t>(b) * m;
+  F* Wd = W + d.w_off + b + static_cast<std::int64_t>(b) * m;
   for (int idx = threadIdx.x; idx < bs * bs; idx += blockDim.x) {
     const int cc = idx / bs, i = idx % bs;
-    Wd[i + static_cast<std::int64_t>(cc) * m] = i >= cc ? Xp[i * (i + 1) / 2 + cc] : 0.0;
+    Wd[i + static_cast<std::int64_t>(cc) * m] = static_cast<F>(i >= cc ? Xp[i * (i + 1) / 2 + cc] : 0.0);
   }
 }
 
 // W[r0 : r0 + 64, B] = L[r0 : r0 + 64, B] W[B, B] for one 64-row tile below a super-block per CTA.
-__global__ void __launch_bounds__(256) k_sb_apply(const int4* tiles, const SnDev* sn, const double* panels,
-                                                   const signed char* piv, double* W) {
+template <class F>
+__global__ void __launch_bounds__(256) k_sb_apply(const int4* tiles, const SnDev* sn, const F* panels,
+                                                   const signed char* piv, F* W) {
   __shared__ double Ls[32][64];
   __shared__ double Xs[32][kSB];
   const int4 e = tiles[blockIdx.x];
   const SnDev d = sn[e.x];
   const int m = d.m;
   const int b = e.y * kSB, bs = min(kSB, d.k - b), r0 = e.z;
-  const double* P = panels + d.panel_off;
+  const F* P = panels + d.panel_off;
   const signed char* pv = piv + d.first;
-  double* Wf = W + d.w_off;
+  F* Wf = W + d.w_off;
   const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;  // rows tr + 16 q, columns tc * 8 + p
   double acc[4][8];
 #pragma unroll
@@ -435,7 +442,7 @@ __global__ void __launch_bounds__(256) k_sb_apply(const int4* tiles, const SnDev
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
       const int cc = tc * 8 + p;
-      if (cc < bs) Wf[i + static_cast<std::int64_t>(b + cc) * m] = acc[q][p];
+      if (cc < bs) Wf[i + static_cast<std::int64_t>(b + cc) * m] = static_cast<F>(acc[q][p]);
     }
   }
 }
@@ -490,9 +497,10 @@ __device__ __forceinline__ int sb_groups(int q, int k) {
 // its 8 warps split the super-block's columns (16 each, lane = row) and add their partial sums in
 // shared memory in warp order. Rows of B give z_B (written to x), rows below update t; the CB rows
 // write their final values to the front's contribution vector in the last step.
+template <class F>
 __global__ void __launch_bounds__(256, 2) k_solve_fwd_coop(const std::int32_t* list, const std::int32_t* cta_start,
                                                             int nfronts, const SnDev* sn, const std::int32_t* cptr,
-                                                            const ContribEntry* cent, const double* W,
+                                                            const ContribEntry* cent, const F* W,
                                                             const std::int32_t* pidx, double* x, std::int64_t n,
                                                             double* vec, int nrhs, double* work,
                                                             const std::int64_t* work_off, int* cnts, int* err) {
@@ -506,7 +514,7 @@ __global__ void __launch_bounds__(256, 2) k_solve_fwd_coop(const std::int32_t* l
   const int m = d.m, k = d.k, c = m - k;
   double* t = work + work_off[f];  // t[r * m + i]
   int* cnt = cnts + f;
-  const double* Wf = W + d.w_off;
+  const F* Wf = W + d.w_off;
   const std::int32_t* pl = pidx + d.first;
   const std::int32_t* cp = cptr + d.cptr_off;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -602,9 +610,10 @@ __global__ void __launch_bounds__(256, 2) k_solve_fwd_coop(const std::int32_t* l
 // 32 consecutive columns per CTA and round); a group reduces its column's dot products over its
 // lanes with shuffles. Super-blocks are processed from the last to the first; the owners of the
 // next super-block's columns write x there and publish.
+template <class F>
 __global__ void __launch_bounds__(256, 2) k_solve_bwd_coop(const std::int32_t* list, const std::int32_t* cta_start,
                                                             int nfronts, const SnDev* sn, const std::int32_t* rows,
-                                                            const double* W, const std::int32_t* pidx, double* x,
+                                                            const F* W, const std::int32_t* pidx, double* x,
                                                             std::int64_t n, int nrhs, double* work,
                                                             const std::int64_t* work_off, int* cnts, int* err) {
   namespace cg = cooperative_groups;
@@ -619,7 +628,7 @@ __global__ void __launch_bounds__(256, 2) k_solve_bwd_coop(const std::int32_t* l
   double* t = work + work_off[f];                              // t[r * m + i]
   double* sv = t + static_cast<std::int64_t>(8) * m;           // sv[r * k + j]
   int* cnt = cnts + f;
-  const double* Wf = W + d.w_off;
+  const F* Wf = W + d.w_off;
   const std::int32_t* pl = pidx + d.first;
   const std::int32_t* rw = rows + d.rows_off;
   const int gt = rank * blockDim.x + threadIdx.x, gs = nr * blockDim.x;
@@ -642,7 +651,7 @@ __global__ void __launch_bounds__(256, 2) k_solve_bwd_coop(const std::int32_t* l
       const int i1 = chunk == 0 ? min(bA + kSB, k) : min(i0 + kSB, m);
       const double sg = chunk == 0 ? 1.0 : -1.0;
       double wv[16];
-      const double* Wj = Wf + i0 + static_cast<std::int64_t>(j) * m;
+      const F* Wj = Wf + i0 + static_cast<std::int64_t>(j) * m;
 #pragma unroll
       for (int u = 0; u < 16; ++u) wv[u] = (j < k && i0 + sub + 8 * u < i1) ? sg * Wj[sub + 8 * u] : 0.0;
       __syncthreads();
@@ -685,7 +694,7 @@ __global__ void __launch_bounds__(256, 2) k_solve_bwd_coop(const std::int32_t* l
     int j = wbase + gsub;
     double wv[16];
     {
-      const double* Wj = Wf + b + static_cast<std::int64_t>(j) * m;
+      const F* Wj = Wf + b + static_cast<std::int64_t>(j) * m;
 #pragma unroll
       for (int u = 0; u < 16; ++u) wv[u] = (j < b && sub + 8 * u < bs) ? Wj[sub + 8 * u] : 0.0;
     }
@@ -700,7 +709,7 @@ __global__ void __launch_bounds__(256, 2) k_solve_bwd_coop(const std::int32_t* l
     for (int base = wbase; base < b; base += ngrp) {
       j = base + gsub;
       if (base != wbase) {
-        const double* Wj = Wf + b + static_cast<std::int64_t>(j) * m;
+        const F* Wj = Wf + b + static_cast<std::int64_t>(j) * m;
 #pragma unroll
         for (int u = 0; u < 16; ++u) wv[u] = (j < b && sub + 8 * u < bs) ? Wj[sub + 8 * u] : 0.0;
         sold = (j < b && sub < nrhs) ? __ldcg(&sv[sub * k + j]) : 0.0;
@@ -758,102 +767,147 @@ int solve_rhs_chunk(int maxm, int nrhs) {
   return R < 1 ? 1 : R;
 }
 
-void launch_inv_blocks(int ns, const SnDev* sn, const double* panels, const signed char* piv, std::int32_t* blk,
-                       std::int32_t* nblk, double* inv, cudaStream_t s) {
+template <class F>
+void launch_inv_blocks(int ns, const SnDev* sn, const F* panels, const signed char* piv, std::int32_t* blk,
+                       std::int32_t* nblk, F* inv, cudaStream_t s) {
   if (ns <= 0) return;
   note_launches(1);
-  k_inv_blocks<<<ns, 256, 0, s>>>(sn, panels, piv, blk, nblk, inv);
+  k_inv_blocks<F><<<ns, 256, 0, s>>>(sn, panels, piv, blk, nblk, inv);
 }
 
+template <class F>
 void launch_solve_fwd(const std::int32_t* list, int nlist, int maxm, const SnDev* sn, const std::int32_t* child_ptr,
-                      const std::int32_t* children, const std::int32_t* rmap, const double* panels,
+                      const std::int32_t* children, const std::int32_t* rmap, const F* panels,
                       const signed char* piv, const std::int32_t* pidx, const std::int32_t* blk,
-                      const std::int32_t* nblk, const double* inv, double* x, std::int64_t n, double* vec, int nrhs,
+                      const std::int32_t* nblk, const F* inv, double* x, std::int64_t n, double* vec, int nrhs,
                       cudaStream_t s) {
   if (nlist <= 0) return;
   const int R = solve_rhs_chunk(maxm, nrhs);
   const std::size_t smem = solve_smem(maxm, R);
   static std::once_flag configured;
   std::call_once(configured, [&] {
-    cudaFuncSetAttribute(k_solve_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSolveSmemMax));
+    cudaFuncSetAttribute(k_solve_fwd<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSolveSmemMax));
   });
   note_launches(1);
-  k_solve_fwd<<<nlist, 256, smem, s>>>(list, sn, child_ptr, children, rmap, panels, piv, pidx, blk, nblk, inv, x, n,
-                                       vec, nrhs, R);
+  k_solve_fwd<F><<<nlist, 256, smem, s>>>(list, sn, child_ptr, children, rmap, panels, piv, pidx, blk, nblk, inv, x, n,
+                                          vec, nrhs, R);
 }
 
-void launch_solve_diag_flat(std::int64_t npiv, const std::int64_t* dpos, const std::int32_t* pfirst,
-                            const double* panels, const signed char* piv, const std::int32_t* pidx, double* x,
-                            std::int64_t n, int nrhs, cudaStream_t s) {
+template <class F>
+void launch_solve_diag_flat(std::int64_t npiv, const std::int64_t* dpos, const std::int32_t* pfirst, const F* panels,
+                            const signed char* piv, const std::int32_t* pidx, double* x, std::int64_t n, int nrhs,
+                            cudaStream_t s) {
   if (npiv <= 0) return;
   note_launches(1);
-  k_solve_diag_flat<<<static_cast<unsigned>((npiv + 255) / 256), 256, 0, s>>>(npiv, dpos, pfirst, panels, piv, pidx, x, n,
-                                                                             nrhs);
+  k_solve_diag_flat<F><<<static_cast<unsigned>((npiv + 255) / 256), 256, 0, s>>>(npiv, dpos, pfirst, panels, piv, pidx,
+                                                                                x, n, nrhs);
 }
 
-void launch_solve_diag(int ns, const SnDev* sn, const double* panels, const signed char* piv,
-                       const std::int32_t* pidx, double* x, std::int64_t n, int nrhs, cudaStream_t s) {
+template <class F>
+void launch_solve_diag(int ns, const SnDev* sn, const F* panels, const signed char* piv, const std::int32_t* pidx,
+                       double* x, std::int64_t n, int nrhs, cudaStream_t s) {
   if (ns <= 0) return;
   note_launches(1);
-  k_solve_diag<<<ns, 128, 0, s>>>(sn, panels, piv, pidx, x, n, nrhs);
+  k_solve_diag<F><<<ns, 128, 0, s>>>(sn, panels, piv, pidx, x, n, nrhs);
 }
 
+template <class F>
 void launch_solve_bwd(const std::int32_t* list, int nlist, int maxm, const SnDev* sn, const std::int32_t* rows,
-                      const double* panels, const std::int32_t* pidx, const std::int32_t* blk,
-                      const std::int32_t* nblk, const double* inv, double* x, std::int64_t n, int nrhs,
-                      cudaStream_t s) {
+                      const F* panels, const std::int32_t* pidx, const std::int32_t* blk, const std::int32_t* nblk,
+                      const F* inv, double* x, std::int64_t n, int nrhs, cudaStream_t s) {
   if (nlist <= 0) return;
   const int R = solve_rhs_chunk(maxm, nrhs);
   const std::size_t smem = solve_smem(maxm, R);
   static std::once_flag configured;
   std::call_once(configured, [&] {
-    cudaFuncSetAttribute(k_solve_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSolveSmemMax));
+    cudaFuncSetAttribute(k_solve_bwd<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSolveSmemMax));
   });
   note_launches(1);
-  k_solve_bwd<<<nlist, 256, smem, s>>>(list, sn, rows, panels, pidx, blk, nblk, inv, x, n, nrhs, R);
+  k_solve_bwd<F><<<nlist, 256, smem, s>>>(list, sn, rows, panels, pidx, blk, nblk, inv, x, n, nrhs, R);
 }
 
-int solve_coop_max_ctas(int device) {
+namespace {
+template <class F>
+int solve_coop_max_of(int device) {
   int a = 0, b = 0, sms = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_solve_fwd_coop, 256, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_solve_bwd_coop, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_solve_fwd_coop<F>, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_solve_bwd_coop<F>, 256, 0);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   return (a < b ? a : b) * sms;
 }
+}  // namespace
 
-void launch_sb_build(const int2* sbl, int nsb, const int4* tiles, int ntiles, const SnDev* sn, const double* panels,
-                     const signed char* piv, double* W, cudaStream_t s) {
+// co-resident CTAs of the cooperative sweeps, valid for both factor types
+int solve_coop_max_ctas(int device) {
+  const int a = solve_coop_max_of<double>(device), b = solve_coop_max_of<float>(device);
+  return a < b ? a : b;
+}
+
+template <class F>
+void launch_sb_build(const int2* sbl, int nsb, const int4* tiles, int ntiles, const SnDev* sn, const F* panels,
+                     const signed char* piv, F* W, cudaStream_t s) {
   if (nsb <= 0) return;
   constexpr std::size_t smem = sizeof(double) * (kSB * (kSB - 1) / 2 + kSB * (kSB + 1) / 2 + kSB);
   static std::once_flag configured;
   std::call_once(configured, [&] {
-    cudaFuncSetAttribute(k_sb_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaFuncSetAttribute(k_sb_inverse<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   });
   note_launches(1);
-  k_sb_inverse<<<nsb, 256, smem, s>>>(sbl, sn, panels, piv, W);
+  k_sb_inverse<F><<<nsb, 256, smem, s>>>(sbl, sn, panels, piv, W);
   if (ntiles > 0) {
     note_launches(1);
-    k_sb_apply<<<ntiles, 256, 0, s>>>(tiles, sn, panels, piv, W);
+    k_sb_apply<F><<<ntiles, 256, 0, s>>>(tiles, sn, panels, piv, W);
   }
 }
 
+template <class F>
 cudaError_t launch_solve_fwd_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
-                                  const SnDev* sn, const std::int32_t* cptr, const ContribEntry* cent, const double* W,
+                                  const SnDev* sn, const std::int32_t* cptr, const ContribEntry* cent, const F* W,
                                   const std::int32_t* pidx, double* x, std::int64_t n, double* vec, int nrhs,
                                   double* work, const std::int64_t* work_off, int* cnts, int* err, cudaStream_t s) {
   void* args[] = {&list, &cta_start, &nfronts, &sn, &cptr, &cent, &W, &pidx, &x, &n, &vec, &nrhs, &work, &work_off,
                   &cnts, &err};
   note_launches(1);
-  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_solve_fwd_coop), dim3(nctas), dim3(256), args, 0, s);
+  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_solve_fwd_coop<F>), dim3(nctas), dim3(256), args, 0, s);
 }
 
+template <class F>
 cudaError_t launch_solve_bwd_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
-                                  const SnDev* sn, const std::int32_t* rows, const double* W, const std::int32_t* pidx,
+                                  const SnDev* sn, const std::int32_t* rows, const F* W, const std::int32_t* pidx,
                                   double* x, std::int64_t n, int nrhs, double* work, const std::int64_t* work_off,
                                   int* cnts, int* err, cudaStream_t s) {
   void* args[] = {&list, &cta_start, &nfronts, &sn, &rows, &W, &pidx, &x, &n, &nrhs, &work, &work_off, &cnts, &err};
   note_launches(1);
-  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_solve_bwd_coop), dim3(nctas), dim3(256), args, 0, s);
+  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_solve_bwd_coop<F>), dim3(nctas), dim3(256), args, 0, s);
 }
+
+#define HSG_SOLVE_INSTANTIATE(F)                                                                                       \
+  template void launch_inv_blocks<F>(int, const SnDev*, const F*, const signed char*, std::int32_t*, std::int32_t*,   \
+                                     F*, cudaStream_t);                                                                \
+  template void launch_solve_fwd<F>(const std::int32_t*, int, int, const SnDev*, const std::int32_t*,                 \
+                                    const std::int32_t*, const std::int32_t*, const F*, const signed char*,            \
+                                    const std::int32_t*, const std::int32_t*, const std::int32_t*, const F*, double*,  \
+                                    std::int64_t, double*, int, cudaStream_t);                                         \
+  template void launch_solve_diag_flat<F>(std::int64_t, const std::int64_t*, const std::int32_t*, const F*,          \
+                                          const signed char*, const std::int32_t*, double*, std::int64_t, int,        \
+                                          cudaStream_t);                                                               \
+  template void launch_solve_diag<F>(int, const SnDev*, const F*, const signed char*, const std::int32_t*, double*,   \
+                                     std::int64_t, int, cudaStream_t);                                                 \
+  template void launch_solve_bwd<F>(const std::int32_t*, int, int, const SnDev*, const std::int32_t*, const F*,      \
+                                    const std::int32_t*, const std::int32_t*, const std::int32_t*, const F*, double*,  \
+                                    std::int64_t, int, cudaStream_t);                                                  \
+  template void launch_sb_build<F>(const int2*, int, const int4*, int, const SnDev*, const F*, const signed char*,    \
+                                   F*, cudaStream_t);                                                                  \
+  template cudaError_t launch_solve_fwd_coop<F>(const std::int32_t*, const std::int32_t*, int, int, const SnDev*,    \
+                                                const std::int32_t*, const ContribEntry*, const F*,                    \
+                                                const std::int32_t*, double*, std::int64_t, double*, int, double*,      \
+                                                const std::int64_t*, int*, int*, cudaStream_t);                        \
+  template cudaError_t launch_solve_bwd_coop<F>(const std::int32_t*, const std::int32_t*, int, int, const SnDev*,    \
+                                                const std::int32_t*, const F*, const std::int32_t*, double*,            \
+                                                std::int64_t, int, double*, const std::int64_t*, int*, int*,            \
+                                                cudaStream_t);
+HSG_SOLVE_INSTANTIATE(double)
+HSG_SOLVE_INSTANTIATE(float)
+#undef HSG_SOLVE_INSTANTIATE
 
 }  // namespace hsg
