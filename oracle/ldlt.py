@@ -34,6 +34,8 @@ def _lib():
         i64 = ctypes.c_int64
         lib.mf_analyze.restype = P
         lib.mf_analyze.argtypes = [i64, P, P, P]
+        lib.mf_analyze_relaxed.restype = P
+        lib.mf_analyze_relaxed.argtypes = [i64, P, P, P, ctypes.c_int]
         lib.mf_factor.restype = ctypes.c_int
         lib.mf_factor.argtypes = [P, P, P, P, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, P]
         lib.mf_solve.restype = ctypes.c_int
@@ -46,8 +48,44 @@ def _lib():
         lib.mf_supernodes.restype = ctypes.c_int32
         lib.mf_supernodes.argtypes = [P]
         lib.mf_threads.restype = ctypes.c_int
+        lib.mf_set_dgemm.argtypes = [P]
+        lib.mf_set_dgemm.restype = None
+        fn = _scipy_dgemm()
+        if fn:
+            lib.mf_set_dgemm(fn)
         _LIB = lib
     return _LIB
+
+
+def _scipy_dgemm():
+    """Address of the Fortran dgemm of the BLAS that scipy loads (scipy.linalg.cython_blas), or None.
+    The frontal updates of the restatement run through it; its own threads are limited to one while
+    the restatement runs (the fronts are parallel in OpenMP)."""
+    try:
+        from scipy.linalg import cython_blas
+    except Exception:
+        return None
+    cap = cython_blas.__pyx_capi__.get("dgemm")
+    if cap is None:
+        return None
+    get_name = ctypes.pythonapi.PyCapsule_GetName
+    get_name.restype = ctypes.c_char_p
+    get_name.argtypes = [ctypes.py_object]
+    get_ptr = ctypes.pythonapi.PyCapsule_GetPointer
+    get_ptr.restype = ctypes.c_void_p
+    get_ptr.argtypes = [ctypes.py_object, ctypes.c_char_p]
+    return get_ptr(cap, get_name(cap))
+
+
+def _one_blas_thread():
+    try:
+        from threadpoolctl import threadpool_limits
+
+        return threadpool_limits(limits=1, user_api="blas")
+    except Exception:  # threadpoolctl is optional
+        import contextlib
+
+        return contextlib.nullcontext()
 
 
 def upper_csr(m) -> sp.csr_matrix:
@@ -63,16 +101,19 @@ def _ptr(a):
 
 
 class OracleLDLT:
-    """K = alpha A + beta B on a fixed pattern; factorize(...) returns (valid, inertia, stats)."""
+    """K = alpha A + beta B on a fixed pattern; factorize(...) returns (valid, inertia, stats).
+    relax: amalgamate the fundamental supernodes (fewer, larger fronts with a few explicit zeros;
+    the exact-fill comparisons of the tests use the fundamental ones)."""
 
-    def __init__(self, pattern, order=None):
+    def __init__(self, pattern, order=None, relax=False):
         u = upper_csr(pattern)
         self.n = u.shape[0]
         self.rp = np.ascontiguousarray(u.indptr, dtype=np.int64)
         self.ci = np.ascontiguousarray(u.indices, dtype=np.int32)
         self._pattern = u
         o = None if order is None else np.ascontiguousarray(order, dtype=np.int32)
-        self._h = _lib().mf_analyze(self.n, _ptr(self.rp), _ptr(self.ci), None if o is None else _ptr(o))
+        self._h = _lib().mf_analyze_relaxed(self.n, _ptr(self.rp), _ptr(self.ci), None if o is None else _ptr(o),
+                                            int(relax))
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -101,8 +142,10 @@ class OracleLDLT:
     def factorize(self, k, u=0.01, null_tol=1e-8, detect=True, scaling=True):
         v = self.values_of(k)
         out = np.zeros(6, dtype=np.int64)
-        valid = _lib().mf_factor(self._h, _ptr(self.rp), _ptr(self.ci), _ptr(v), u, null_tol,
-                                 int(detect), int(scaling), _ptr(out))
+        lib = _lib()
+        with _one_blas_thread():
+            valid = lib.mf_factor(self._h, _ptr(self.rp), _ptr(self.ci), _ptr(v), u, null_tol,
+                                  int(detect), int(scaling), _ptr(out))
         neg, zero, pos, delayed, two, null = (int(x) for x in out)
         return bool(valid), (neg, zero, pos), {"delayed": delayed, "two_by_two": two, "null_pivots": null}
 
@@ -110,7 +153,9 @@ class OracleLDLT:
         x = np.array(b, dtype=np.float64, order="F", copy=True)
         if x.ndim == 1:
             x = x.reshape(-1, 1, order="F")
-        _lib().mf_solve(self._h, _ptr(x), x.shape[1], x.shape[0])
+        lib = _lib()
+        with _one_blas_thread():
+            lib.mf_solve(self._h, _ptr(x), x.shape[1], x.shape[0])
         return x if np.ndim(b) == 2 else x[:, 0]
 
     @property
