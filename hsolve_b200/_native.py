@@ -65,6 +65,7 @@ SIGNATURES = {
     "hsg_set_null_pivot_detection": (ctypes.c_int, [_P, _I32]),
     "hsg_pivot_order": (ctypes.c_int, [_P, _P]),
     "hsg_order": (_I64, [_P]),
+    "hsg_clear_analysis_cache": (ctypes.c_int, []),
     "hsg_spmm": (ctypes.c_int, [_I64, _P, _P, _P, _P, _I64, _P, _I64, _I64, _D, _D]),
     "hsg_shifted_residual": (ctypes.c_int, [_I64, _P, _P, _P, _P, _P, _P, _D, _P, _I64, _P, _I64, _P, _I64, _I64,
                                             _P]),
@@ -281,6 +282,11 @@ def shifted_residual_device(a: DeviceCsr, b, sigma: float, x, y, r, omega=None) 
                                      None if r is None else ctypes.c_void_p(r.data_ptr()),
                                      a.n if r is None else r.shape[1], p,
                                      None if omega is None else ctypes.c_void_p(omega.data_ptr())))
+
+
+def clear_analysis_cache() -> None:
+    """Empties the process-wide analysis cache (the next solve on any pattern analyses afresh)."""
+    check(lib().hsg_clear_analysis_cache())
 
 
 def kernel_launches() -> int:

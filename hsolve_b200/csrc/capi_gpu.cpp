@@ -26,6 +26,7 @@ const GpuFactor& get(const hsg_factor* f) {
 namespace hsg {
 // The object behind a handle, for entry points defined in other translation units.
 GpuFactor& factor_of(hsg_factor* f) { return get(f); }
+void clear_analysis_cache();
 }  // namespace hsg
 
 extern "C" {
@@ -113,6 +114,10 @@ int hsg_pivot_order(const hsg_factor* f, int32_t* out) {
     HSG_REQUIRE(out, HSG_INVALID_INPUT, "hsg_pivot_order: null output");
     get(f).pivot_order(out);
   });
+}
+
+int hsg_clear_analysis_cache(void) {
+  return guarded([] { clear_analysis_cache(); });
 }
 
 int64_t hsg_order(const hsg_factor* f) {

@@ -83,6 +83,15 @@ void learn_delays(const std::vector<std::int64_t>& rp, const std::vector<std::in
     }
 }
 
+}  // namespace
+
+void clear_analysis_cache() {
+  std::lock_guard<std::mutex> lk(g_analysis_mu);
+  g_analysis_cache.clear();
+}
+
+namespace {
+
 struct DeviceGuard {
   int prev = -1;
   explicit DeviceGuard(int dev) {

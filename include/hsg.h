@@ -157,6 +157,12 @@ HSG_API int hsg_pivot_order(const hsg_factor* f, int32_t* out);
 /* SparseFactorization::order() (factor.hpp:441-442). */
 HSG_API int64_t hsg_order(const hsg_factor* f);
 
+/* Empties the process-wide cache of nested-dissection analyses (keyed by sparsity pattern), so that
+ * the next analysis of any pattern runs the ordering and the symbolic factorization again; handles
+ * that already hold an analysis keep it (instrumentation for cold-call timing; no counterpart in
+ * hsolve, whose every hs::solve call analyses afresh). */
+HSG_API int hsg_clear_analysis_cache(void);
+
 /* Measured FP64 FMA throughput of the device (TFLOP/s), the denominator of the factorization's
  * roofline (instrumentation; no counterpart in hsolve). */
 HSG_API int hsg_fp64_peak_probe(int32_t device, double* tflops);
