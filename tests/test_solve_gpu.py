@@ -200,3 +200,20 @@ def test_server_runs_mixed_requests_concurrently():
     st = srv.stats()
     assert st["requests"] == 4 and st["certified"] == 4 and not st["failed"]
     assert st["latency_p99_s"] >= st["latency_p50_s"] > 0
+
+
+def test_dealer_parts_of_one_window_compose_to_the_exact_spectrum():
+    """hsolve_b200.parallel on one GPU: the window cut into three parts by FP64 counts, each part a
+    certified solve of its own, the gathered result equal to the exact spectrum of the whole window."""
+    from hsolve_b200.parallel import Dealer
+
+    box = yee.Box((12, 11, 10), (1.0, 0.75, 0.55))
+    a, b = yee.pencil(box, "generalized")
+    w = yee_exact.exact_spectrum(box.cells, box.lengths)
+    lo, hi = 40.0, 200.0
+    with Dealer() as d:
+        lam, vec, rep = d.solve_interval(a, b, lo, hi, parts=3)
+    want = w[(w >= lo) & (w < hi)]
+    assert rep["passed"] and len(rep["parts"]) == 3 and rep["count_inertia"] == want.size
+    np.testing.assert_allclose(lam, want, rtol=EIG_RTOL)
+    assert np.abs(vec.T @ (b @ vec) - np.eye(want.size)).max() < 1e-10
