@@ -47,8 +47,20 @@ class _Budget:
     cond: threading.Condition = field(default_factory=threading.Condition)
 
 
-# device memory (MB) of a request, learned per (n, nnz(A), nnz(B), complex) the first time it runs
+# device memory (MB) of a request, learned per (n, nnz(A), nnz(B), complex) the first time it runs;
+# shared by every Server of the process, so reads and writes take _KNOWN_LOCK
 _KNOWN_MB: dict[tuple, float] = {}
+_KNOWN_LOCK = threading.Lock()
+
+
+def _known_get(key):
+    with _KNOWN_LOCK:
+        return _KNOWN_MB.get(key)
+
+
+def _known_set(key, mb: float) -> None:
+    with _KNOWN_LOCK:
+        _KNOWN_MB[key] = mb
 
 
 def _free_device_mb(device: int) -> float:
@@ -71,7 +83,6 @@ class Server:
         total = memory_budget_gb * 1e3 if memory_budget_gb is not None else 0.8 * _free_device_mb(device)
         self._budget = _Budget(total_mb=total)
         self._pool = ThreadPoolExecutor(max_workers=workers, thread_name_prefix="hsolve-serve")
-        self._known_mb = _KNOWN_MB
         self._records: list[RequestRecord] = []
         self._lock = threading.Lock()
 
@@ -80,7 +91,7 @@ class Server:
         """Blocks until the request fits; returns True when it runs alone (unknown footprint)."""
         b = self._budget
         with b.cond:
-            known = self._known_mb.get(key)
+            known = _known_get(key)
             if known is None:
                 b.cond.wait_for(lambda: b.active == 0)
                 b.exclusive = True
@@ -125,8 +136,7 @@ class Server:
                     # factor storage of up to three factorization objects plus the Krylov basis
                     basis_mb = 8.0 * 2 * sess.n * 160 / 1e6
                     rec.device_mb = 3.0 * est["device_mb"] + basis_mb
-                    with self._budget.cond:
-                        self._known_mb[key] = rec.device_mb
+                    _known_set(key, rec.device_mb)
                 cfg = dict(self.config)
                 cfg.update(target.pop("config", None) or {})
                 res = sess.solve(config=cfg, **target)

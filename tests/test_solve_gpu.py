@@ -217,3 +217,35 @@ def test_dealer_parts_of_one_window_compose_to_the_exact_spectrum():
     assert rep["passed"] and len(rep["parts"]) == 3 and rep["count_inertia"] == want.size
     np.testing.assert_allclose(lam, want, rtol=EIG_RTOL)
     assert np.abs(vec.T @ (b @ vec) - np.eye(want.size)).max() < 1e-10
+
+
+def test_server_results_are_the_same_alone_and_in_the_mix():
+    """Continuous batching must not change results: every request solved alone (one worker, one
+    request at a time) and again in a mixed stream of real and complex pencils of different sizes
+    (three workers, all submitted at once) gives the same certified eigenvalues (within 1e-10
+    relative) and the same certificate counts."""
+    from hsolve_b200.serve import Server
+
+    reqs = []
+    for cells, boundary, phases in [((8, 7, 6), "pec", (0.0, 0.0, 0.0)), ((7, 6, 6), "bloch", (0.9, 0.4, 0.2)),
+                                    ((10, 9, 8), "pec", (0.0, 0.0, 0.0)), ((6, 6, 6), "bloch", (1.3, 0.7, 0.1)),
+                                    ((9, 8, 7), "pec", (0.0, 0.0, 0.0))]:
+        box = yee.Box(cells, (1.0, 0.9, 0.8), boundary, phases)
+        a, b = yee.pencil(box, "generalized")
+        w = yee_exact.exact_spectrum(box.cells, box.lengths, boundary, box.phases)
+        cuts = yee_exact.mid_gap_shifts(w[w > 1.0], 8, 1e-6)
+        reqs.append((a, b, dict(lower=cuts[1], upper=cuts[6])))
+    alone = []
+    with Server(workers=1) as srv:
+        for a, b, t in reqs:
+            alone.append(srv.submit(a, b, **t).result())
+    with Server(workers=3) as srv:
+        futs = [srv.submit(a, b, **t) for a, b, t in reqs]
+        mixed = [f.result() for f in futs]
+    for r1, r2 in zip(alone, mixed):
+        _check_pairs(r1)
+        _check_pairs(r2)
+        assert r1.eigenvalues.size == r2.eigenvalues.size > 0
+        np.testing.assert_allclose(r2.eigenvalues, r1.eigenvalues, rtol=EIG_RTOL)
+        c1, c2 = r1.report["certificate"], r2.report["certificate"]
+        assert c1["count_inertia"] == c2["count_inertia"] and c1["passed"] and c2["passed"]
