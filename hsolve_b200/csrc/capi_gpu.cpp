@@ -75,8 +75,7 @@ int hsg_factorize(hsg_factor* f, double alpha, double beta, hsg_inertia_t* out) 
 int hsg_count(hsg_factor* f, double alpha, double beta, int32_t detection, hsg_inertia_t* out) {
   return guarded([&] {
     GpuFactor& g = get(f);
-    const hsg_inertia_t in = g.factorize(alpha, beta, detection != 0);
-    g.release();
+    const hsg_inertia_t in = g.count(alpha, beta, detection != 0);
     if (out) *out = in;
   });
 }

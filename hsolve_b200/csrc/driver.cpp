@@ -321,7 +321,7 @@ long long count_below(GpuFactor& F, double& s, double scale, double direction, l
                       bool shared = false) {
   const auto t0 = Clock::now();
   for (int t = 0; t < 8; ++t) {
-    hsg_inertia_t in = F.factorize(1.0, -s, true, shared);
+    hsg_inertia_t in = F.count(1.0, -s, true, shared);  // inertia only: no factor kept
     if (in.valid) { tm.cert += since(t0); return in.neg; }
     s += direction * 1e-7 * (scale + std::fabs(s)) * (t + 1);
     ++moves;

@@ -106,6 +106,30 @@ __global__ void k_scatter(std::int64_t nnz, const std::int32_t* row, const std::
   if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&cnt->amax_bits, mx);
 }
 
+// max |d_i d_j (alpha a_p + beta b_p)| alone (the null-pivot threshold of an inertia-only count,
+// whose entries are scattered level by level)
+__global__ void k_amax(std::int64_t nnz, const std::int32_t* row, const std::int32_t* col, const double* a,
+                       const double* b, double alpha, double beta, const double* d, FactorCounters* cnt) {
+  double mx = 0.0;
+  for (std::int64_t p = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; p < nnz;
+       p += static_cast<std::int64_t>(gridDim.x) * blockDim.x)
+    mx = fmax(mx, fabs((alpha * a[p] + beta * b[p]) * d[row[p]] * d[col[p]]));
+  mx = warp_max(mx);
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&cnt->amax_bits, mx);
+}
+
+// panels[dest[p]] = d_i d_j (alpha a_p + beta b_p) for the listed entries p = idx[t] (one level's)
+template <class R>
+__global__ void k_scatter_list(const std::int64_t* idx, std::int64_t count, const std::int32_t* row,
+                               const std::int32_t* col, const double* a, const double* b, double alpha, double beta,
+                               const double* d, const std::int64_t* dest, R* panels) {
+  for (std::int64_t t = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; t < count;
+       t += static_cast<std::int64_t>(gridDim.x) * blockDim.x) {
+    const std::int64_t p = idx[t];
+    panels[dest[p]] = static_cast<R>((alpha * a[p] + beta * b[p]) * d[row[p]] * d[col[p]]);
+  }
+}
+
 // zero the contribution blocks of the listed fronts (grid: fronts x chunks)
 template <class R>
 __global__ void k_zero_cb(const std::int32_t* list, const SnDev* sn, R* cb) {
@@ -1462,6 +1486,23 @@ void launch_scatter(std::int64_t nnz, const std::int32_t* row, const std::int32_
   k_scatter<R><<<blocks, 256, 0, s>>>(nnz, row, col, a, b, alpha, beta, d, dest, panels, cnt);
 }
 
+void launch_amax(std::int64_t nnz, const std::int32_t* row, const std::int32_t* col, const double* a, const double* b,
+                 double alpha, double beta, const double* d, FactorCounters* cnt, cudaStream_t s) {
+  const int blocks = static_cast<int>(std::min<std::int64_t>((nnz + 255) / 256, 148 * 16));
+  note_launches(1);
+  k_amax<<<blocks, 256, 0, s>>>(nnz, row, col, a, b, alpha, beta, d, cnt);
+}
+
+template <class R>
+void launch_scatter_list(const std::int64_t* idx, std::int64_t count, const std::int32_t* row, const std::int32_t* col,
+                         const double* a, const double* b, double alpha, double beta, const double* d,
+                         const std::int64_t* dest, R* panels, cudaStream_t s) {
+  if (count <= 0) return;
+  const int blocks = static_cast<int>(std::min<std::int64_t>((count + 255) / 256, 148 * 16));
+  note_launches(1);
+  k_scatter_list<R><<<blocks, 256, 0, s>>>(idx, count, row, col, a, b, alpha, beta, d, dest, panels);
+}
+
 template <class R>
 void launch_zero_cb(const std::int32_t* list, int nlist, int chunks, const SnDev* sn, R* cb, cudaStream_t s) {
   if (nlist <= 0) return;
@@ -1542,6 +1583,9 @@ cudaError_t launch_front_coop(const std::int32_t* list, const std::int32_t* cta_
                                   const double*, double, double, const double*, const std::int64_t*, R*,              \
                                   FactorCounters*, cudaStream_t);                                                     \
   template void launch_zero_cb<R>(const std::int32_t*, int, int, const SnDev*, R*, cudaStream_t);                     \
+  template void launch_scatter_list<R>(const std::int64_t*, std::int64_t, const std::int32_t*, const std::int32_t*,   \
+                                       const double*, const double*, double, double, const double*,                  \
+                                       const std::int64_t*, R*, cudaStream_t);                                       \
   template void launch_extend_add<R>(const int2*, int, const SnDev*, const std::int32_t*, R*, R*, cudaStream_t);     \
   template void launch_front_small<R>(int, const std::int32_t*, int, const SnDev*, R*, R*, signed char*,              \
                                       std::int32_t*, const FactorParams&, FactorCounters*, std::int32_t*,             \

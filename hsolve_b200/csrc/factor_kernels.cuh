@@ -39,6 +39,13 @@ template <class R>
 void launch_scatter(std::int64_t nnz, const std::int32_t* row, const std::int32_t* col, const double* a,
                     const double* b, double alpha, double beta, const double* d, const std::int64_t* dest,
                     R* panels, FactorCounters* cnt, cudaStream_t s);
+// inertia-only counts: the largest scaled entry alone, and the scatter of one level's entries
+void launch_amax(std::int64_t nnz, const std::int32_t* row, const std::int32_t* col, const double* a, const double* b,
+                 double alpha, double beta, const double* d, FactorCounters* cnt, cudaStream_t s);
+template <class R>
+void launch_scatter_list(const std::int64_t* idx, std::int64_t count, const std::int32_t* row, const std::int32_t* col,
+                         const double* a, const double* b, double alpha, double beta, const double* d,
+                         const std::int64_t* dest, R* panels, cudaStream_t s);
 template <class R>
 void launch_zero_cb(const std::int32_t* list, int nlist, int chunks, const SnDev* sn, R* cb, cudaStream_t s);
 template <class R>

@@ -487,6 +487,45 @@ void GpuFactor::build_plan() {
     }
   }
   std::vector<std::int32_t> rows(S.rows.begin(), S.rows.end());
+  {
+    // inertia-only counts: the panels of one level packed at the start of an arena (the next level
+    // reuses it), and the pencil's entries grouped by the level of the front they scatter into
+    std::vector<SnDev> snc = sn;
+    std::vector<std::int32_t> level_of(ns, 0);
+    arena_entries_ = 1;
+    for (std::int32_t l = 0; l < S.nlevels; ++l) {
+      std::int64_t off = 0;
+      for (std::int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+        const std::int32_t s = S.level_sn[q];
+        level_of[s] = l;
+        snc[s].panel_off = off;
+        off += static_cast<std::int64_t>(sn[s].m) * sn[s].k;
+      }
+      levels_[l].arena_used = off;
+      arena_entries_ = std::max(arena_entries_, off);
+    }
+    std::vector<std::int64_t> dest_cnt(nnz_), lcount(S.nlevels + 1, 0);
+    std::vector<std::int32_t> ent_level(nnz_);
+    for (std::int64_t p = 0; p < nnz_; ++p) {
+      const std::int64_t dst = S.dest[p];
+      const std::int32_t s = static_cast<std::int32_t>(
+          std::upper_bound(S.panel_off.begin(), S.panel_off.begin() + ns + 1, dst) - S.panel_off.begin() - 1);
+      dest_cnt[p] = dst - S.panel_off[s] + snc[s].panel_off;
+      ent_level[p] = level_of[s];
+      lcount[level_of[s] + 1]++;
+    }
+    for (std::int32_t l = 0; l < S.nlevels; ++l) lcount[l + 1] += lcount[l];
+    std::vector<std::int64_t> ent_idx(std::max<std::int64_t>(1, nnz_));
+    std::vector<std::int64_t> fill(lcount.begin(), lcount.end() - 1);
+    for (std::int64_t p = 0; p < nnz_; ++p) ent_idx[fill[ent_level[p]]++] = p;
+    for (std::int32_t l = 0; l < S.nlevels; ++l) {
+      levels_[l].ent_off = lcount[l];
+      levels_[l].ent_n = lcount[l + 1] - lcount[l];
+    }
+    d_sn_cnt_.upload(snc, stream_);
+    d_dest_cnt_.upload(dest_cnt, stream_);
+    d_ent_idx_.upload(ent_idx, stream_);
+  }
   d_sn_.upload(sn, stream_);
   d_lists_.upload(lists, stream_);
   d_items_.upload(items, stream_);
@@ -545,16 +584,23 @@ std::size_t GpuFactor::factor_bytes() const {
   return el * (d_panels_.n + d_panels_f_.n + d_w_.n + d_w_f_.n + d_inv_.n + d_inv_f_.n);
 }
 
-void GpuFactor::run_numeric(double alpha, double beta, bool detection) {
-  if (single()) run_numeric_t<float>(alpha, beta, detection);
-  else run_numeric_t<double>(alpha, beta, detection);
+void GpuFactor::run_numeric(double alpha, double beta, bool detection, bool count_only) {
+  if (single()) run_numeric_t<float>(alpha, beta, detection, count_only);
+  else run_numeric_t<double>(alpha, beta, detection, count_only);
 }
 
 template <class R>
-void GpuFactor::run_numeric_t(double alpha, double beta, bool detection) {
+void GpuFactor::run_numeric_t(double alpha, double beta, bool detection, bool count_only) {
   cudaStream_t s = stream_;
   R* panels = panels_of<R>();
   R* cb = cb_of<R>();
+  const SnDev* sn = d_sn_.p;
+  if (count_only) {
+    // the level's panels live in the arena; entries are scattered level by level below
+    if constexpr (sizeof(R) == 8) { d_arena_.alloc(static_cast<std::size_t>(arena_entries_)); panels = reinterpret_cast<R*>(d_arena_.p); }
+    else { d_arena_f_.alloc(static_cast<std::size_t>(arena_entries_)); panels = reinterpret_cast<R*>(d_arena_f_.p); }
+    sn = d_sn_cnt_.p;
+  }
   cuda_check(cudaMemsetAsync(d_cnt_.p, 0, sizeof(FactorCounters), s), "memset counters");
   cuda_check(cudaMemsetAsync(d_level_done_.p, 0, d_level_done_.n * sizeof(int), s), "memset level flags");
   launch_fill(d_scale_.p, n_, 1.0, s);
@@ -565,8 +611,12 @@ void GpuFactor::run_numeric_t(double alpha, double beta, bool detection) {
       launch_scale_update(n_, d_scale_.p, d_r_.p, s);
     }
   }
-  cuda_check(cudaMemsetAsync(panels, 0, sym_.factor_entries * sizeof(R), s), "memset panels");
-  launch_scatter<R>(nnz_, d_row_.p, d_col_.p, d_a_.p, d_b_.p, alpha, beta, d_scale_.p, d_dest_.p, panels, d_cnt_.p, s);
+  if (count_only) {
+    launch_amax(nnz_, d_row_.p, d_col_.p, d_a_.p, d_b_.p, alpha, beta, d_scale_.p, d_cnt_.p, s);
+  } else {
+    cuda_check(cudaMemsetAsync(panels, 0, sym_.factor_entries * sizeof(R), s), "memset panels");
+    launch_scatter<R>(nnz_, d_row_.p, d_col_.p, d_a_.p, d_b_.p, alpha, beta, d_scale_.p, d_dest_.p, panels, d_cnt_.p, s);
+  }
   FactorParams prm;
   prm.u = opt_.pivot_threshold;
   // null pivots relative to the largest scaled entry: 1e-8 for FP64 factors, 1e-4 for FP32
@@ -576,28 +626,43 @@ void GpuFactor::run_numeric_t(double alpha, double beta, bool detection) {
   prm.failed_cap = static_cast<std::int32_t>(n_);
   const std::int32_t* lists = d_lists_.p;
   for (const LevelPlan& L : levels_) {
-    launch_zero_cb<R>(lists + L.zero_off, L.zero_n, L.zero_chunks, d_sn_.p, cb, s);
-    for (const auto& ea : L.ea) launch_extend_add<R>(d_items_.p + ea.first, ea.second, d_sn_.p, d_rmap_.p, panels, cb, s);
-    launch_front_small<R>(32, lists + L.s32_off, L.s32_n, d_sn_.p, panels, cb, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
-    launch_front_small<R>(kSmallMax, lists + L.s64_off, L.s64_n, d_sn_.p, panels, cb, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
+    if (count_only) {
+      cuda_check(cudaMemsetAsync(panels, 0, static_cast<std::size_t>(L.arena_used) * sizeof(R), s), "memset arena");
+      launch_scatter_list<R>(d_ent_idx_.p + L.ent_off, L.ent_n, d_row_.p, d_col_.p, d_a_.p, d_b_.p, alpha, beta,
+                             d_scale_.p, d_dest_cnt_.p, panels, s);
+    }
+    launch_zero_cb<R>(lists + L.zero_off, L.zero_n, L.zero_chunks, sn, cb, s);
+    for (const auto& ea : L.ea) launch_extend_add<R>(d_items_.p + ea.first, ea.second, sn, d_rmap_.p, panels, cb, s);
+    launch_front_small<R>(32, lists + L.s32_off, L.s32_n, sn, panels, cb, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
+    launch_front_small<R>(kSmallMax, lists + L.s64_off, L.s64_n, sn, panels, cb, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
     if (shared_ ? L.coop_shared : L.coop) {
       const std::int64_t cta_off = shared_ ? L.cta_off_shared : L.cta_off;
       const int ctas = shared_ ? L.coop_ctas_shared : L.coop_ctas;
-      cuda_check(launch_front_coop<R>(lists + L.app_off, lists + cta_off, L.app_n, ctas, d_sn_.p, panels, cb,
+      cuda_check(launch_front_coop<R>(lists + L.app_off, lists + cta_off, L.app_n, ctas, sn, panels, cb,
                                       d_scratch_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p,
                                       d_level_done_.p + L.done_slot, s),
                  "cooperative front launch");
     } else {
-      launch_front_app<R>(lists + L.app_off, L.app_n, d_sn_.p, panels, cb, d_scratch_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
+      launch_front_app<R>(lists + L.app_off, L.app_n, sn, panels, cb, d_scratch_.p, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
     }
   }
   cuda_check(cudaGetLastError(), "factorization launch");
 }
 
-template void GpuFactor::run_numeric_t<double>(double, double, bool);
-template void GpuFactor::run_numeric_t<float>(double, double, bool);
+template void GpuFactor::run_numeric_t<double>(double, double, bool, bool);
+template void GpuFactor::run_numeric_t<float>(double, double, bool, bool);
 
 hsg_inertia_t GpuFactor::factorize(double alpha, double beta, bool detection, bool shared) {
+  return run_factorization(alpha, beta, detection, shared, false);
+}
+
+hsg_inertia_t GpuFactor::count(double alpha, double beta, bool detection, bool shared) {
+  const hsg_inertia_t in = run_factorization(alpha, beta, detection, shared, true);
+  factored_ = false;  // no factor was kept
+  return in;
+}
+
+hsg_inertia_t GpuFactor::run_factorization(double alpha, double beta, bool detection, bool shared, bool count_only) {
   shared_ = shared;
   HSG_REQUIRE(analysed_, HSG_INTERNAL, "factorize before analyze");
   HSG_REQUIRE(std::isfinite(alpha) && std::isfinite(beta), HSG_INVALID_INPUT, "non-finite alpha / beta");
@@ -610,7 +675,7 @@ hsg_inertia_t GpuFactor::factorize(double alpha, double beta, bool detection, bo
   std::int64_t delayed = 0;
   for (;;) {
     cuda_check(cudaEventRecord(ev0_, stream_), "event");
-    run_numeric(alpha, beta, detection);
+    run_numeric(alpha, beta, detection, count_only);
     cuda_check(cudaEventRecord(ev1_, stream_), "event");
     cuda_check(cudaMemcpyAsync(&c, d_cnt_.p, sizeof(c), cudaMemcpyDeviceToHost, stream_), "counters");
     cuda_check(cudaStreamSynchronize(stream_), "factorization");

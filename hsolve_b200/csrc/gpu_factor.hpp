@@ -74,6 +74,11 @@ class GpuFactor {
   // shared: use the cooperative plan sized for a third of the device, so that up to three
   // factorizations (of different shifts, on different objects) can run at once
   hsg_inertia_t factorize(double alpha, double beta, bool detection, bool shared = false);
+  // Inertia only (SparseFactorization::count / InertiaCounter::count): the same pivoting and D, but
+  // no factor is kept - the fronts of one tree level are factorized in a panel arena that the next
+  // level overwrites (max over levels of the level's panel sizes instead of all of them), and no
+  // solve operator is built. The handle holds no usable factorization afterwards.
+  hsg_inertia_t count(double alpha, double beta, bool detection, bool shared = false);
   // The analysis of `src` (pattern, values of A and B, symbolic analysis) without recomputing it.
   void analyze_like(const GpuFactor& src);
   void solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_device);
@@ -129,11 +134,14 @@ class GpuFactor {
     bool coop_shared = false;          // the level also fits the shared budget's co-resident grid
     std::int64_t cta_off_shared = 0; int coop_ctas_shared = 0;  // cooperative plan of the shared budget
     int cnt_off = 0;                   // first publication counter of the level's fronts
+    std::int64_t ent_off = 0, ent_n = 0;  // inertia-only counts: this level's entries in d_ent_idx_
+    std::int64_t arena_used = 0;       // ... and its panels' extent in the arena
   };
   void build_plan();
-  void run_numeric(double alpha, double beta, bool detection);
+  hsg_inertia_t run_factorization(double alpha, double beta, bool detection, bool shared, bool count_only);
+  void run_numeric(double alpha, double beta, bool detection, bool count_only);
   template <class R>
-  void run_numeric_t(double alpha, double beta, bool detection);
+  void run_numeric_t(double alpha, double beta, bool detection, bool count_only);
   // forward, diagonal and backward sweeps of nr right-hand sides gathered in xwork (n x nr)
   void run_sweeps(double* xwork, double* vec, int nr);
   template <class F>
@@ -178,6 +186,12 @@ class GpuFactor {
       d_failed_;
   DevBuf<double> d_a_, d_b_, d_scale_, d_panels_, d_cb_, d_scratch_, d_vec_, d_xwork_, d_btmp_, d_inv_;
   DevBuf<float> d_panels_f_, d_cb_f_, d_w_f_, d_inv_f_;  // the same, for FP32 factors
+  // inertia-only counts: fronts with arena offsets, entries by level and their arena destinations
+  DevBuf<SnDev> d_sn_cnt_;
+  DevBuf<std::int64_t> d_ent_idx_, d_dest_cnt_;
+  DevBuf<double> d_arena_;
+  DevBuf<float> d_arena_f_;
+  std::int64_t arena_entries_ = 0;
   DevBuf<std::int32_t> d_blk_, d_nblk_;
   DevBuf<std::int64_t> d_dest_;
   DevBuf<unsigned long long> d_r_;

@@ -112,7 +112,10 @@ HSG_API int hsg_estimate(const hsg_factor* f, hsg_estimate_t* out);
 HSG_API int hsg_factorize(hsg_factor* f, double alpha, double beta, hsg_inertia_t* out);
 
 /* SparseFactorization::count(alpha, beta) / InertiaCounter::count (factor.hpp:383-390,
- * :557-565): inertia of K without keeping usable factors. detection: null-pivot detection on/off. */
+ * :557-565): inertia of K without keeping usable factors. detection: null-pivot detection on/off.
+ * The fronts of one tree level are factorized in a panel arena that the next level reuses, so the
+ * count needs the largest level's panels instead of the whole factor; the handle holds no usable
+ * factorization afterwards (hsg_solve fails until the next hsg_factorize). */
 HSG_API int hsg_count(hsg_factor* f, double alpha, double beta, int32_t detection, hsg_inertia_t* out);
 
 /* SparseFactorization::solve(b, nrhs, ldb) (factor.hpp:394-398): K X = B in place, column-major,

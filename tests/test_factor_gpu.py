@@ -191,3 +191,54 @@ def test_zero_block_dense_front_two_by_two_solves(h):
     b = rng.standard_normal((n, 9))
     x = f.solve(b)
     assert backward_error(k, x, b) < 1e-12
+
+
+@pytest.mark.parametrize("case", ["yee", "box1e5", "saddle", "singular", "single"])
+def test_inertia_only_count_equals_the_factorization(case, golden):
+    """hsg_count (fronts factorized level by level in a recycled panel arena, no factor kept) gives
+    the inertia of hsg_factorize - exact counts, 2x2 and delayed pivots with re-plans, null pivots
+    of a singular shift, FP32 objects - and leaves no usable factorization
+    (SparseFactorization::count / InertiaCounter::count, include/hsolve/factor.hpp:383-390)."""
+    opts = {}
+    if case in ("yee", "single"):
+        box = yee.Box((12, 11, 10), (1.0, 0.75, 0.55))
+        a, b = yee.pencil(box, "generalized")
+        w = yee_exact.exact_spectrum(box.cells, box.lengths)
+        shifts = yee_exact.mid_gap_shifts(w[w > 1.0], 5, 1.0)
+        order = None
+        if case == "single":
+            opts = {"precision": 1}
+    elif case == "box1e5":
+        a, b = yee.pencil(yee.BOX_1E5, "generalized")
+        w = yee_exact.exact_spectrum(yee.BOX_1E5.cells, yee.BOX_1E5.lengths)
+        shifts, order = [40.0, 120.0, 200.0], None
+    elif case == "saddle":
+        a, b = saddle_point(400, 150, 5), None
+        n = a.shape[0]
+        w = np.linalg.eigvalsh(a.toarray())
+        order = np.empty(n, dtype=np.int32)
+        order[np.concatenate((np.arange(400, n), np.arange(400)))] = np.arange(1, n + 1)
+        shifts = [0.0, 0.37]
+    else:
+        z = np.load(golden / "near_singular.npz")
+        a, b = sp.csr_matrix((z["data"], z["indices"], z["indptr"])), None
+        import json
+        w = z["eigenvalues"]
+        shifts = [json.loads((golden / "examples.json").read_text())["near-singular-shift"]["config"]["target"]["sigma"],
+                  yee_exact.mid_gap_shifts(w, 3, 1e-6)[1]]
+        order = None
+    f, c = Factorization(**opts), Factorization(**opts)
+    f.analyze(a, b, 1.0, -shifts[0], pivot_order=order)
+    c.analyze(a, b, 1.0, -shifts[0], pivot_order=order)
+    for s in shifts:
+        ok = f.factorize(1.0, -s)
+        fi = f.inertia()
+        ci = c.count(1.0, -s)
+        assert (ci.neg, ci.zero, ci.pos, ci.valid) == (fi.neg, fi.zero, fi.pos, fi.valid == ok), (s, ci, fi)
+        assert ci.two_by_two == fi.two_by_two
+        if case != "saddle" and ok:
+            assert ci.neg == yee_exact.count_below(w, s)
+        with pytest.raises(Exception):
+            c.solve(np.ones(a.shape[0]))
+    f.close()
+    c.close()
