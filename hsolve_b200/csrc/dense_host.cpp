@@ -4,6 +4,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
+#include <limits>
 #include <numeric>
 #include <stdexcept>
 
@@ -188,6 +190,197 @@ std::vector<double> matmul(int m, int k, int n, const std::vector<double>& a, co
       for (int i = 0; i < m; ++i) c[i + static_cast<std::size_t>(j) * m] += a[i + static_cast<std::size_t>(q) * m] * bv;
     }
   return c;
+}
+
+
+// ------------------------------------------------------------- general (non-symmetric) matrices
+//
+// Complex Schur form T = U^H A U of a real matrix, written for this project from the standard
+// algorithm: Householder reduction to upper Hessenberg form, then the shifted QR iteration with
+// Wilkinson shifts in complex arithmetic (Givens rotations, one shift per step; a 2 x 2 window is
+// resolved the same way), deflation when a subdiagonal entry falls below eps times its neighbours.
+
+namespace {
+
+using cplx = std::complex<double>;
+
+// rotation G = [c s; -conj(s) c] (c real) with G [x; y] = [r; 0]
+void givens(cplx x, cplx y, double& c, cplx& s) {
+  const double ax = std::abs(x), ay = std::abs(y);
+  if (ay == 0.0) { c = 1.0; s = 0.0; return; }
+  if (ax == 0.0) { c = 0.0; s = std::conj(y) / ay; return; }
+  const double r = std::hypot(ax, ay);
+  c = ax / r;
+  s = (x / ax) * std::conj(y) / r;
+}
+
+}  // namespace
+
+void complex_schur(int n, const std::vector<double>& a, std::vector<cplx>& T, std::vector<cplx>& U) {
+  // Householder reduction to Hessenberg form (real), Q accumulated
+  std::vector<double> h(a), q(static_cast<std::size_t>(n) * n, 0.0);
+  auto H = [&](int i, int j) -> double& { return h[static_cast<std::size_t>(i) + static_cast<std::size_t>(j) * n]; };
+  auto Q = [&](int i, int j) -> double& { return q[static_cast<std::size_t>(i) + static_cast<std::size_t>(j) * n]; };
+  for (int i = 0; i < n; ++i) Q(i, i) = 1.0;
+  std::vector<double> v(n);
+  for (int k = 0; k + 2 < n; ++k) {
+    double alpha = 0.0;
+    for (int i = k + 1; i < n; ++i) alpha += H(i, k) * H(i, k);
+    alpha = std::sqrt(alpha);
+    if (alpha == 0.0) continue;
+    const double x0 = H(k + 1, k);
+    const double s = x0 >= 0 ? -alpha : alpha;
+    for (int i = k + 1; i < n; ++i) v[i] = H(i, k);
+    v[k + 1] = x0 - s;
+    double vn = 0.0;
+    for (int i = k + 1; i < n; ++i) vn += v[i] * v[i];
+    if (vn == 0.0) continue;
+    const double beta = 2.0 / vn;
+    for (int j = 0; j < n; ++j) {  // H = (I - beta v v^T) H
+      double t = 0.0;
+      for (int i = k + 1; i < n; ++i) t += v[i] * H(i, j);
+      t *= beta;
+      for (int i = k + 1; i < n; ++i) H(i, j) -= t * v[i];
+    }
+    for (int i = 0; i < n; ++i) {  // H = H (I - beta v v^T), Q = Q (I - beta v v^T)
+      double t = 0.0, u = 0.0;
+      for (int j = k + 1; j < n; ++j) { t += H(i, j) * v[j]; u += Q(i, j) * v[j]; }
+      t *= beta;
+      u *= beta;
+      for (int j = k + 1; j < n; ++j) { H(i, j) -= t * v[j]; Q(i, j) -= u * v[j]; }
+    }
+    for (int i = k + 2; i < n; ++i) H(i, k) = 0.0;
+  }
+  T.assign(h.begin(), h.end());
+  U.assign(q.begin(), q.end());
+  auto t = [&](int i, int j) -> cplx& { return T[static_cast<std::size_t>(i) + static_cast<std::size_t>(j) * n]; };
+  auto u = [&](int i, int j) -> cplx& { return U[static_cast<std::size_t>(i) + static_cast<std::size_t>(j) * n]; };
+  const double eps = std::numeric_limits<double>::epsilon();
+  double anorm = 0.0;
+  for (std::size_t e = 0; e < T.size(); ++e) anorm = std::max(anorm, std::abs(T[e]));
+  int hi = n - 1, iter = 0, total = 0;
+  while (hi > 0) {
+    int l = hi;
+    while (l > 0) {
+      const double sub = std::abs(t(l, l - 1));
+      const double nb = std::abs(t(l, l)) + std::abs(t(l - 1, l - 1));
+      if (sub <= eps * (nb > 0.0 ? nb : anorm)) { t(l, l - 1) = 0.0; break; }
+      --l;
+    }
+    if (l == hi) { --hi; iter = 0; continue; }
+    if (++total > 100 * n) throw std::runtime_error("complex_schur: QR iteration did not converge");
+    ++iter;
+    // Wilkinson shift from the trailing 2 x 2 of the window (an exceptional shift now and then)
+    const cplx a11 = t(hi - 1, hi - 1), a12 = t(hi - 1, hi), a21 = t(hi, hi - 1), a22 = t(hi, hi);
+    cplx mu;
+    if (iter % 11 == 10) {
+      mu = a22 + cplx(std::abs(a21), 0.0) * 0.75;
+    } else {
+      const cplx half = 0.5 * (a11 - a22);
+      const cplx disc = std::sqrt(half * half + a12 * a21);
+      const cplx m1 = a22 + half + disc, m2 = a22 + half - disc;
+      mu = std::abs(m1 - a22) <= std::abs(m2 - a22) ? m1 : m2;
+    }
+    cplx x = t(l, l) - mu, y = t(l + 1, l);
+    for (int k = l; k < hi; ++k) {
+      double c;
+      cplx s;
+      givens(x, y, c, s);
+      // rows k, k+1 (columns from k-1, or l at the first step, to the right end)
+      for (int j = (k > l ? k - 1 : l); j < n; ++j) {
+        const cplx r0 = t(k, j), r1 = t(k + 1, j);
+        t(k, j) = c * r0 + s * r1;
+        t(k + 1, j) = -std::conj(s) * r0 + c * r1;
+      }
+      // columns k, k+1 (rows up to k+2) and the Schur vectors
+      const int rmax = std::min(k + 2, hi);
+      for (int i = 0; i <= rmax; ++i) {
+        const cplx c0 = t(i, k), c1 = t(i, k + 1);
+        t(i, k) = c * c0 + std::conj(s) * c1;
+        t(i, k + 1) = -s * c0 + c * c1;
+      }
+      for (int i = 0; i < n; ++i) {
+        const cplx c0 = u(i, k), c1 = u(i, k + 1);
+        u(i, k) = c * c0 + std::conj(s) * c1;
+        u(i, k + 1) = -s * c0 + c * c1;
+      }
+      if (k + 1 < hi) {
+        x = t(k + 1, k);
+        y = t(k + 2, k);
+      }
+    }
+  }
+  for (int j = 0; j < n; ++j)
+    for (int i = j + 1; i < n; ++i) t(i, j) = 0.0;
+}
+
+void schur_sort(int n, std::vector<cplx>& T, std::vector<cplx>& U, const std::vector<double>& key) {
+  auto t = [&](int i, int j) -> cplx& { return T[static_cast<std::size_t>(i) + static_cast<std::size_t>(j) * n]; };
+  auto u = [&](int i, int j) -> cplx& { return U[static_cast<std::size_t>(i) + static_cast<std::size_t>(j) * n]; };
+  // keys travel with the diagonal entries they were computed for
+  std::vector<double> kk(key);
+  for (int pos = 0; pos < n; ++pos) {
+    int best = pos;
+    for (int i = pos + 1; i < n; ++i)
+      if (kk[i] < kk[best]) best = i;
+    for (int k = best - 1; k >= pos; --k) {
+      // swap diagonal entries k and k+1: G's first column is the eigenvector of the 2 x 2 block for
+      // its second eigenvalue
+      const cplx a = t(k, k), b = t(k, k + 1), d = t(k + 1, k + 1);
+      cplx g1 = b, g2 = d - a;
+      const double nr = std::hypot(std::abs(g1), std::abs(g2));
+      if (nr == 0.0) { std::swap(kk[k], kk[k + 1]); continue; }
+      g1 /= nr;
+      g2 /= nr;
+      // G = [g1 -conj(g2); g2 conj(g1)]; T = G^H T G, U = U G
+      for (int j = k; j < n; ++j) {
+        const cplx r0 = t(k, j), r1 = t(k + 1, j);
+        t(k, j) = std::conj(g1) * r0 + std::conj(g2) * r1;
+        t(k + 1, j) = -g2 * r0 + g1 * r1;
+      }
+      for (int i = 0; i <= k + 1; ++i) {
+        const cplx c0 = t(i, k), c1 = t(i, k + 1);
+        t(i, k) = c0 * g1 + c1 * g2;
+        t(i, k + 1) = -c0 * std::conj(g2) + c1 * std::conj(g1);
+      }
+      for (int i = 0; i < n; ++i) {
+        const cplx c0 = u(i, k), c1 = u(i, k + 1);
+        u(i, k) = c0 * g1 + c1 * g2;
+        u(i, k + 1) = -c0 * std::conj(g2) + c1 * std::conj(g1);
+      }
+      t(k + 1, k) = 0.0;
+      std::swap(kk[k], kk[k + 1]);
+    }
+  }
+}
+
+std::vector<cplx> schur_eigenvectors(int n, const std::vector<cplx>& T, int count, double cluster_rtol) {
+  auto t = [&](int i, int j) { return T[static_cast<std::size_t>(i) + static_cast<std::size_t>(j) * n]; };
+  double tnorm = 0.0;
+  for (const cplx& z : T) tnorm = std::max(tnorm, std::abs(z));
+  const double smin = std::max(tnorm * std::numeric_limits<double>::epsilon(), 1e-300);
+  std::vector<cplx> Y(static_cast<std::size_t>(n) * count, cplx(0.0));
+  for (int k = 0; k < count; ++k) {
+    const cplx lam = t(k, k);
+    // the cluster of entries equal to lam just above k is treated as one block: its members' own
+    // coordinates are set (unit vector), only the entries above the cluster are solved for
+    int a = k;
+    while (a > 0 && std::abs(t(a - 1, a - 1) - lam) <= cluster_rtol * std::max(std::abs(lam), smin)) --a;
+    cplx* y = &Y[static_cast<std::size_t>(k) * n];
+    y[k] = 1.0;
+    for (int i = a - 1; i >= 0; --i) {
+      cplx s = 0.0;
+      for (int j = i + 1; j <= k; ++j) s += t(i, j) * y[j];
+      cplx den = t(i, i) - lam;
+      if (std::abs(den) < smin) den = smin;
+      y[i] = -s / den;
+    }
+    double nr = 0.0;
+    for (int i = 0; i <= k; ++i) nr += std::norm(y[i]);
+    nr = std::sqrt(nr);
+    for (int i = 0; i <= k; ++i) y[i] /= nr;
+  }
+  return Y;
 }
 
 }  // namespace hsg

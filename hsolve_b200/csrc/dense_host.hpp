@@ -1,6 +1,7 @@
 // Small dense linear algebra on the host (projected Krylov matrices, p x p block factors).
 #pragma once
 
+#include <complex>
 #include <cstdint>
 #include <vector>
 
@@ -20,5 +21,21 @@ std::vector<double> lower_inverse(int p, const std::vector<double>& l);
 
 // c = a * b (column-major, a: m x k, b: k x n)
 std::vector<double> matmul(int m, int k, int n, const std::vector<double>& a, const std::vector<double>& b);
+
+// Complex Schur form of the real n x n column-major matrix a: a = U T U^H with T upper triangular
+// and U unitary (both column-major, complex). Throws std::runtime_error if the QR iteration fails.
+void complex_schur(int n, const std::vector<double>& a, std::vector<std::complex<double>>& T,
+                   std::vector<std::complex<double>>& U);
+
+// Reorders a complex Schur form so that the diagonal entries appear by ascending key (key[i] belongs
+// to the entry at position i on entry), by adjacent swaps (unitary, T stays triangular).
+void schur_sort(int n, std::vector<std::complex<double>>& T, std::vector<std::complex<double>>& U,
+                const std::vector<double>& key);
+
+// Eigenvectors y_k (k < count, unit 2-norm, in Schur coordinates: x_k = U y_k) of the upper
+// triangular T. Diagonal entries within cluster_rtol of T(k, k) just above k form one block whose
+// members keep their own coordinates, so a multiple eigenvalue gets independent vectors.
+std::vector<std::complex<double>> schur_eigenvectors(int n, const std::vector<std::complex<double>>& T, int count,
+                                                     double cluster_rtol);
 
 }  // namespace hsg

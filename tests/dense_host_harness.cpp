@@ -1,5 +1,6 @@
 // Test harness: plain C entry points over the host dense routines of hsolve_b200/csrc/dense_host.cpp,
 // built by tests/test_dense_host.py into a temporary shared object and called through ctypes.
+#include <complex>
 #include <cstring>
 #include <vector>
 
@@ -39,3 +40,27 @@ void t_matmul(int m, int k, int n, const double* a_in, const double* b_in, doubl
 }
 
 }  // extern "C"
+
+// complex Schur form, sorted by key, and the first `count` eigenvectors (interleaved re/im)
+extern "C" int t_schur(int n, const double* a_in, const double* key, int count, double cluster_rtol, double* t_out, double* u_out,
+            double* y_out) {
+  std::vector<double> a(a_in, a_in + static_cast<std::size_t>(n) * n);
+  std::vector<std::complex<double>> T, U;
+  try {
+    hsg::complex_schur(n, a, T, U);
+    if (key) {
+      // keys computed by the caller for the eigenvalues as the unsorted form lists them are not
+      // available; the harness sorts by -|t_ii| (largest magnitude first)
+      std::vector<double> k(n);
+      for (int i = 0; i < n; ++i) k[i] = -std::abs(T[static_cast<std::size_t>(i) * (n + 1)]);
+      hsg::schur_sort(n, T, U, k);
+    }
+    const std::vector<std::complex<double>> Y = hsg::schur_eigenvectors(n, T, count, cluster_rtol);
+    std::memcpy(t_out, T.data(), sizeof(double) * 2 * T.size());
+    std::memcpy(u_out, U.data(), sizeof(double) * 2 * U.size());
+    std::memcpy(y_out, Y.data(), sizeof(double) * 2 * Y.size());
+  } catch (...) {
+    return 1;
+  }
+  return 0;
+}

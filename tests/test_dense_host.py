@@ -30,6 +30,8 @@ def lib(tmp_path_factory):
     L.t_cholesky.restype = I
     L.t_lower_inverse.argtypes = [I, P, P]
     L.t_matmul.argtypes = [I, I, I, P, P, P]
+    L.t_schur.argtypes = [I, P, P, I, D, P, P, P]
+    L.t_schur.restype = I
     return L
 
 
@@ -126,3 +128,52 @@ def test_matmul(lib):
         c = np.zeros((m, n), order="F")
         lib.t_matmul(m, k, n, _p(a), _p(b), _p(c))
         np.testing.assert_allclose(c, a @ b, rtol=1e-14, atol=1e-13)
+
+
+def _schur(lib, a, count, sort=True, cluster_rtol=1e-8):
+    n = a.shape[0]
+    af = np.asfortranarray(a, dtype=np.float64)
+    t = np.zeros((n, n), dtype=np.complex128, order="F")
+    u = np.zeros((n, n), dtype=np.complex128, order="F")
+    y = np.zeros((n, count), dtype=np.complex128, order="F")
+    key = np.zeros(n) if sort else None
+    rc = lib.t_schur(n, _p(af), None if key is None else _p(key), count, cluster_rtol, _p(t), _p(u), _p(y))
+    assert rc == 0
+    return t, u, y
+
+
+@pytest.mark.parametrize("n,seed", [(1, 0), (2, 1), (7, 2), (40, 3), (120, 4)])
+def test_complex_schur_of_random_matrices(lib, n, seed):
+    a = np.random.default_rng(seed).standard_normal((n, n))
+    t, u, y = _schur(lib, a, n)
+    assert np.abs(u.conj().T @ u - np.eye(n)).max() < 1e-12
+    assert np.abs(np.tril(t, -1)).max(initial=0.0) == 0.0
+    assert np.abs(u @ t @ u.conj().T - a).max() < 1e-12 * max(1.0, np.abs(a).max()) * n
+    lam = np.diag(t)
+    ref = np.linalg.eigvals(a)
+    assert np.all(np.diff(np.abs(lam)) <= 1e-12 * np.abs(lam).max())  # sorted by magnitude, largest first
+    for z in ref:
+        assert np.min(np.abs(lam - z)) <= 1e-9 * max(1.0, np.abs(ref).max())
+    x = u @ y
+    for k in range(n):
+        assert np.linalg.norm(a @ x[:, k] - lam[k] * x[:, k]) <= 1e-9 * max(1.0, np.abs(a).max()) * np.sqrt(n)
+
+
+def test_schur_eigenvectors_of_a_multiple_eigenvalue_are_independent(lib):
+    """A diagonalizable matrix with triple and double real eigenvalues and a complex pair: the
+    vectors of each multiple eigenvalue span its eigenspace."""
+    rng = np.random.default_rng(7)
+    d = np.array([5.0, 5.0, 5.0, -2.0, -2.0, 0.5, 0.1])
+    blk = np.diag(d)
+    blk[5:7, 5:7] = [[0.5, 1.0], [-1.0, 0.5]]  # eigenvalues 0.5 +- i
+    s = rng.standard_normal((7, 7))
+    a = s @ blk @ np.linalg.inv(s)
+    t, u, y = _schur(lib, a, 7, cluster_rtol=1e-7)
+    lam = np.diag(t)
+    x = u @ y
+    for k in range(7):
+        assert np.linalg.norm(a @ x[:, k] - lam[k] * x[:, k]) < 1e-8
+    for value, mult in ((5.0, 3), (-2.0, 2)):
+        idx = np.flatnonzero(np.abs(lam - value) < 1e-6)
+        assert idx.size == mult
+        assert np.linalg.matrix_rank(x[:, idx], tol=1e-6) == mult
