@@ -25,7 +25,8 @@ class _SolveConfig(ctypes.Structure):
                 ("block_size", ctypes.c_int32), ("slice_size", ctypes.c_int64), ("max_restarts", ctypes.c_int32),
                 ("seed", ctypes.c_uint64), ("certificate", ctypes.c_int32), ("max_shift_retries", ctypes.c_int32),
                 ("factor_precision", ctypes.c_int32), ("device", ctypes.c_int32), ("verbose", ctypes.c_int32),
-                ("batch_shifts", ctypes.c_int32)]
+                ("batch_shifts", ctypes.c_int32), ("complex_tol", ctypes.c_double),
+                ("zero_filter_tol", ctypes.c_double)]
 
 
 _P = ctypes.c_void_p
@@ -34,6 +35,8 @@ _SOLVE_SIGS = {
     "hsg_eigsolve": (ctypes.c_int, [ctypes.c_int64, _P, _P, _P, _P, _P, _P, _P, _P]),
     "hsg_solution_sizes": (ctypes.c_int, [_P, _P, _P]),
     "hsg_solution_copy": (ctypes.c_int, [_P, _P, _P]),
+    "hsg_solution_complex_count": (ctypes.c_int, [_P, _P]),
+    "hsg_solution_complex_copy": (ctypes.c_int, [_P, _P, _P]),
     "hsg_solution_report": (ctypes.c_char_p, [_P]),
     "hsg_solution_free": (None, [_P]),
     "hsg_session_create": (ctypes.c_int, [ctypes.c_int64, _P, _P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_uint64, _P]),
@@ -207,6 +210,8 @@ def _struct_from(cfg: dict, verbose: int) -> _SolveConfig:
     c.device = int(cfg.get("device", 0))
     c.verbose = int(verbose)
     c.batch_shifts = 1 if bool(cfg.get("batch_shifts", True)) else 0
+    c.complex_tol = float(cfg.get("complex_tol", 1e-8))
+    c.zero_filter_tol = float(cfg.get("zero_filter_tol", -1.0))
     if not (0.0 < c.tol < 1.0):
         raise InvalidInputError("tol must be in (0, 1)")
     return c
@@ -443,10 +448,10 @@ def solve(A, B=None, *, sigma=None, k=_Default(6), mode=_Default("nearest"), low
         b, db = _hermitian_check(b, "B", htol)
     if np.iscomplexobj(a.data) or (b is not None and np.iscomplexobj(b.data)):
         ae, be = _embed(a), (_embed(b) if b is not None else None)
-        w, v, report = _eigsolve(ae, be, _struct_from(_embedded_config(cfg), verbose))
+        w, v, report, _ = _eigsolve(ae, be, _struct_from(_embedded_config(cfg), verbose))
         return _complex_result(w, v, report, a, b, cfg, da, db)
-    w, v, report = _eigsolve(a, b, _struct_from(cfg, verbose))
-    return _finish(w, v, report, cfg, da, db, cdtype)
+    w, v, report, cplx = _eigsolve(a, b, _struct_from(cfg, verbose))
+    return _finish(w, v, report, cfg, da, db, cdtype, cplx)
 
 
 def _embedded_config(cfg: dict) -> dict:
@@ -493,28 +498,35 @@ def _eigsolve(a, b, c):
 
 
 def _fetch(h):
-    """(eigenvalues, eigenvectors, report) of a native solution handle, which is freed."""
+    """(eigenvalues, eigenvectors, report, (complex eigenvalues, complex eigenvectors)) of a native
+    solution handle, which is freed."""
     lib = _native.lib()
     p = _native._ptr
     try:
-        nn, m = ctypes.c_int64(), ctypes.c_int64()
+        nn, m, mc = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         _native.check(lib.hsg_solution_sizes(h, ctypes.byref(nn), ctypes.byref(m)))
         w = np.zeros(m.value)
         v = np.zeros((nn.value, m.value), order="F")
         _native.check(lib.hsg_solution_copy(h, p(w), p(v)))
+        _native.check(lib.hsg_solution_complex_count(h, ctypes.byref(mc)))
+        cw = np.zeros(mc.value, dtype=np.complex128)
+        cv = np.zeros((nn.value, mc.value), dtype=np.complex128, order="F")
+        if mc.value:
+            _native.check(lib.hsg_solution_complex_copy(h, p(cw), p(cv)))
         report = json.loads(lib.hsg_solution_report(h).decode())
     finally:
         lib.hsg_solution_free(h)
-    return w, v, report
+    return w, v, report, (cw, cv)
 
 
-def _finish(w, v, report, cfg, da, db, complex_vectors=False) -> SolveResult:
+def _finish(w, v, report, cfg, da, db, complex_vectors=False, cplx=None) -> SolveResult:
     n = v.shape[0]
     report["hermitian_defect_a"] = da
     report["hermitian_defect_b"] = db
     if complex_vectors:
         v = np.asfortranarray(v.astype(np.complex128))
-    result = SolveResult(w, v, np.zeros(0, dtype=np.complex128), np.zeros((n, 0), dtype=np.complex128), report, cfg)
+    cw, cv = cplx if cplx is not None else (np.zeros(0, dtype=np.complex128), np.zeros((n, 0), dtype=np.complex128))
+    result = SolveResult(w, v, cw, cv, report, cfg)
     if not result.success:
         warnings.warn("hsolve: the solve finished without meeting the tolerance (see result.report['pairs'] "
                       "and result.report['warnings'])", HsolveWarning, stacklevel=3)
@@ -564,10 +576,10 @@ class Session:
         c = _struct_from(_embedded_config(cfg) if self._complex else cfg, verbose)
         h = ctypes.c_void_p()
         _native.check(_native.lib().hsg_session_solve(self._h, ctypes.byref(c), ctypes.byref(h)))
-        w, v, report = _fetch(h)
+        w, v, report, cplx = _fetch(h)
         if self._complex:
             return _complex_result(w, v, report, self._complex[0], self._complex[1], cfg, self._da, self._db)
-        return _finish(w, v, report, cfg, self._da, self._db, self._cdtype)
+        return _finish(w, v, report, cfg, self._da, self._db, self._cdtype, cplx)
 
     def estimate(self) -> dict:
         """Analysis of the session's pencil (for a complex pencil, of its real 2n embedding): factor

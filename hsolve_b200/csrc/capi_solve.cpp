@@ -59,6 +59,8 @@ void hsg_default_solve_config(hsg_solve_config_t* c) {
   c->device = 0;
   c->verbose = 0;
   c->batch_shifts = 1;
+  c->complex_tol = 1e-8;
+  c->zero_filter_tol = -1.0;
 }
 
 int hsg_eigsolve(int64_t n, const int64_t* a_rowptr, const int32_t* a_col, const double* a_val,
@@ -131,6 +133,21 @@ int hsg_solution_copy(const hsg_solution* s, double* eigenvalues, double* eigenv
     HSG_REQUIRE(s, HSG_INVALID_INPUT, "null solution");
     if (eigenvalues) std::copy(s->out.eigenvalues.begin(), s->out.eigenvalues.end(), eigenvalues);
     if (eigenvectors) std::copy(s->out.vectors.begin(), s->out.vectors.end(), eigenvectors);
+  });
+}
+
+int hsg_solution_complex_count(const hsg_solution* s, int64_t* mc) {
+  return guarded([&] {
+    HSG_REQUIRE(s && mc, HSG_INVALID_INPUT, "null argument");
+    *mc = static_cast<int64_t>(s->out.complex_eigenvalues.size() / 2);
+  });
+}
+
+int hsg_solution_complex_copy(const hsg_solution* s, double* eigenvalues, double* eigenvectors) {
+  return guarded([&] {
+    HSG_REQUIRE(s, HSG_INVALID_INPUT, "null solution");
+    if (eigenvalues) std::copy(s->out.complex_eigenvalues.begin(), s->out.complex_eigenvalues.end(), eigenvalues);
+    if (eigenvectors) std::copy(s->out.complex_vectors.begin(), s->out.complex_vectors.end(), eigenvectors);
   });
 }
 

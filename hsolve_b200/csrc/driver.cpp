@@ -11,6 +11,7 @@
 #include <future>
 #include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <map>
 #include <memory>
@@ -18,6 +19,7 @@
 
 #include "blas_kernels.cuh"
 #include "common.hpp"
+#include "dense_host.hpp"
 #include "eigen.hpp"
 #include "gpu_factor.hpp"
 
@@ -383,6 +385,271 @@ NearestRun run_krylov(ShiftInvertOp& op, Problem& P, double sigma, int nev, int 
 
 int auto_block(int nev) { return nev >= 32 ? 8 : (nev >= 8 ? 4 : (nev >= 3 ? 2 : 1)); }
 
+// ------------------------------------------------------------------------------------ GHIEP
+// Nearest target of a pencil whose B is indefinite (hsolve src/driver/indefinite.cpp:723-1000,
+// solve_indefinite, the plain run at sigma): one general Krylov-Schur run of OP = (A - sigma B)^{-1} B
+// in the Euclidean inner product, candidates lambda = sigma + 1/theta from its wanted Ritz values,
+// real/complex classification by SolverConfig::complex_tol (solver.hpp:231-233, the test of
+// indefinite.cpp:477-479), and the k candidates nearest sigma by complex distance with trustworthy
+// pairs first (select_nearest, indefinite.cpp:534-557).
+constexpr double kTrustworthy = 1e-6;    // pairs above this backward error only fill a shortfall
+constexpr double kGhiepZeroBand = 1e-8;  // |lambda| <= kGhiepZeroBand * scale: the zero cluster of A
+
+struct GhiepCand {
+  std::complex<double> lambda;
+  bool real = true;
+  PairMetrics pm{};
+  int col = 0;  // real: column of the coefficient matrix; complex: its vector in GhiepRun::xc
+};
+
+struct GhiepRun {
+  std::vector<GhiepCand> sel;             // the selection, nearest first
+  std::vector<double> coef;               // m x cols real coefficients of the candidates' vectors
+  int m = 0, cols = 0;
+  DevBuf<double> V;                       // the run's basis (n x m)
+  std::vector<double> xc;                 // host vectors (n x 2: re, im) of the complex candidates
+  int restarts = 0, applies = 0, block = 0;
+  long long good = 0, in_band = 0;
+};
+
+// Metrics of a pair given x, A x, B x on the host (complex lambda, vectors as re / im columns).
+PairMetrics complex_metrics(const Problem& P, std::int64_t n, const double* x, const double* ax, const double* bx,
+                            std::complex<double> lam, double tol) {
+  double rr = 0.0, xx = 0.0, bb = 0.0;
+  for (std::int64_t i = 0; i < n; ++i) {
+    const std::complex<double> xv(x[i], x[n + i]), av(ax[i], ax[n + i]), bv(bx[i], bx[n + i]);
+    rr += std::norm(av - lam * bv);
+    xx += std::norm(xv);
+    bb += std::norm(bv);
+  }
+  PairMetrics q{};
+  q.lambda = lam.real();
+  q.abs_res = std::sqrt(rr);
+  const double al = std::abs(lam);
+  q.rel_res = al != 0.0 ? q.abs_res / (al * std::sqrt(bb)) : q.abs_res / std::sqrt(bb);
+  q.eta = q.abs_res / ((P.normA + al * P.normB) * std::sqrt(xx));
+  q.accepted = q.eta <= tol;
+  return q;
+}
+
+GhiepRun ghiep_run(ShiftInvertOp& op, Problem& P, double sigma, int nev, int k, const hsg_solve_config_t& cfg, int p,
+                   double scale, double band_user, double complex_tol, Timers& tm) {
+  using cplx = std::complex<double>;
+  const std::int64_t n = P.n;
+  cudaStream_t s = P.s;
+  const auto t0 = Clock::now();
+  KsOptions o;
+  o.nev = nev;
+  o.nev_strict = k;
+  o.ncv = static_cast<int>(cfg.ncv);
+  o.block = p;
+  o.tol = cfg.tol * cfg.inner_tol_factor;
+  o.max_restarts = cfg.max_restarts;
+  o.seed = cfg.seed;
+  GeneralKsResult r = krylov_schur_general(op, n, o, s);
+  tm.iterate += since(t0);
+  tm.kry_apply += r.t_apply;
+  tm.kry_ortho += r.t_ortho;
+  tm.kry_rr += r.t_rr;
+  tm.kry_restart += r.t_restart;
+  const auto tv = Clock::now();
+  GhiepRun out;
+  out.restarts = r.restarts;
+  out.applies = r.applies;
+  out.block = p;
+  const int m = r.m;
+  std::vector<cplx> mu;
+  std::vector<int> src;
+  for (std::size_t j = 0; j < r.theta.size(); ++j) {
+    if (r.theta[j] == cplx(0.0)) continue;
+    mu.push_back(sigma + 1.0 / r.theta[j]);
+    src.push_back(static_cast<int>(j));
+  }
+  const int nc = static_cast<int>(mu.size());
+  auto cf = [&](int q, int i) { return r.coef[static_cast<std::size_t>(src[q]) * m + i]; };
+  std::vector<char> small(nc);
+  for (int q = 0; q < nc; ++q) small[q] = std::fabs(mu[q].imag()) <= complex_tol * std::max(std::abs(mu[q]), scale);
+  // real vector of every candidate: the real part of e^{i phi} c with the phase that maximizes its
+  // norm (the top eigenvector of the 2 x 2 Gram matrix of Re c, Im c; the basis is orthonormal, so
+  // this works on the coefficients)
+  std::vector<int> cidx;
+  for (int q = 0; q < nc; ++q)
+    if (!small[q]) cidx.push_back(q);
+  const int cols = nc + 2 * static_cast<int>(cidx.size());
+  std::vector<double> Y(static_cast<std::size_t>(m) * std::max(cols, 1), 0.0);
+  for (int q = 0; q < nc; ++q) {
+    double aa = 0.0, bb = 0.0, ab = 0.0;
+    for (int i = 0; i < m; ++i) {
+      const cplx z = cf(q, i);
+      aa += z.real() * z.real();
+      bb += z.imag() * z.imag();
+      ab += z.real() * z.imag();
+    }
+    const double phi = 0.5 * std::atan2(-2.0 * ab, aa - bb);
+    const double c = std::cos(phi), sn = std::sin(phi);
+    double nr = 0.0;
+    double* y = &Y[static_cast<std::size_t>(q) * m];
+    for (int i = 0; i < m; ++i) {
+      y[i] = cf(q, i).real() * c - cf(q, i).imag() * sn;
+      nr += y[i] * y[i];
+    }
+    nr = std::sqrt(nr);
+    if (nr > 0.0)
+      for (int i = 0; i < m; ++i) y[i] /= nr;
+  }
+  // a multiple real eigenvalue: its candidates take an orthonormal basis of the real span of their
+  // vectors (the eigenspace of a real eigenvalue of a real pencil is real), so they stay independent
+  {
+    std::vector<int> rs;
+    for (int q = 0; q < nc; ++q)
+      if (small[q]) rs.push_back(q);
+    std::stable_sort(rs.begin(), rs.end(), [&](int a, int b) { return mu[a].real() < mu[b].real(); });
+    for (std::size_t g0 = 0; g0 < rs.size();) {
+      std::size_t g1 = g0 + 1;
+      while (g1 < rs.size() && std::fabs(mu[rs[g1]].real() - mu[rs[g1 - 1]].real()) <=
+                                   1e-8 * std::max(std::fabs(mu[rs[g1]].real()), scale))
+        ++g1;
+      const int g = static_cast<int>(g1 - g0);
+      if (g > 1) {
+        std::vector<cplx> Cg(static_cast<std::size_t>(m) * g);
+        for (int t = 0; t < g; ++t)
+          for (int i = 0; i < m; ++i) Cg[static_cast<std::size_t>(t) * m + i] = cf(rs[g0 + t], i);
+        int rank = 0;
+        std::vector<double> Qg = real_span(m, g, Cg, rank, g);
+        if (rank == g)
+          for (int t = 0; t < g; ++t)
+            std::copy(Qg.begin() + static_cast<std::ptrdiff_t>(t) * m, Qg.begin() + static_cast<std::ptrdiff_t>(t + 1) * m,
+                      Y.begin() + static_cast<std::ptrdiff_t>(rs[g0 + t]) * m);
+      }
+      g0 = g1;
+    }
+  }
+  for (std::size_t t = 0; t < cidx.size(); ++t)
+    for (int i = 0; i < m; ++i) {
+      Y[static_cast<std::size_t>(nc + 2 * t) * m + i] = cf(cidx[t], i).real();
+      Y[static_cast<std::size_t>(nc + 2 * t + 1) * m + i] = cf(cidx[t], i).imag();
+    }
+  // vectors and their images on the device
+  DevBuf<double> Yd, X, AX, BX, R, lamd, dots;
+  Yd.upload(Y, s);
+  X.alloc(static_cast<std::size_t>(n) * std::max(cols, 1));
+  AX.alloc(static_cast<std::size_t>(n) * std::max(cols, 1));
+  BX.alloc(static_cast<std::size_t>(n) * std::max(cols, 1));
+  R.alloc(static_cast<std::size_t>(n) * std::max(nc, 1));
+  dots.alloc(4 * static_cast<std::size_t>(std::max(nc, 1)));
+  std::vector<double> h(4 * static_cast<std::size_t>(nc));
+  std::vector<double> lam_r(nc);
+  if (nc > 0) {
+    gemm_tall(n, m, cols, r.V.p, n, Yd.p, m, X.p, n, 1.0, 0.0, s);
+    spmm(P.A.view(n), X.p, n, AX.p, n, cols, 1.0, 0.0, s);
+    P.bprod(X.p, n, BX.p, n, cols);
+    col_dots(n, nc, X.p, n, AX.p, n, dots.p, s);
+    col_dots(n, nc, X.p, n, BX.p, n, dots.p + nc, s);
+    col_dots(n, nc, BX.p, n, BX.p, n, dots.p + 2 * nc, s);
+    cuda_check(cudaMemcpyAsync(h.data(), dots.p, 3 * nc * sizeof(double), cudaMemcpyDeviceToHost, s), "ghiep dots");
+    cuda_check(cudaStreamSynchronize(s), "ghiep dots");
+    // lambda of a real vector: its Rayleigh quotient x^T A x / x^T B x (x^T is also a left
+    // eigenvector of a real symmetric pencil, so the quotient is accurate to second order), unless
+    // x^T B x is too small for it or it leaves the Ritz estimate; then Re(mu)
+    for (int q = 0; q < nc; ++q) {
+      lam_r[q] = mu[q].real();
+      const double xbx = h[nc + q], bxn = std::sqrt(h[2 * nc + q]);
+      if (std::fabs(xbx) >= 1e-3 * bxn && bxn > 0.0) {
+        const double rq = h[q] / xbx;
+        if (std::fabs(rq - mu[q].real()) <= 1e-6 * std::max(std::abs(mu[q]), scale)) lam_r[q] = rq;
+      }
+    }
+    lamd.upload(lam_r, s);
+    residual_cols(n, nc, AX.p, n, BX.p, n, lamd.p, R.p, n, s);
+    col_dots(n, nc, R.p, n, R.p, n, dots.p, s);
+    col_dots(n, nc, X.p, n, X.p, n, dots.p + nc, s);
+    cuda_check(cudaMemcpyAsync(h.data(), dots.p, 2 * nc * sizeof(double), cudaMemcpyDeviceToHost, s), "ghiep dots");
+    cuda_check(cudaStreamSynchronize(s), "ghiep dots");
+  }
+  std::vector<GhiepCand> cands(nc);
+  for (int q = 0; q < nc; ++q) {
+    GhiepCand& c = cands[q];
+    c.lambda = cplx(lam_r[q], 0.0);
+    c.col = q;
+    PairMetrics& pm = c.pm;
+    const double rn = std::sqrt(h[q]), xn = std::sqrt(h[nc + q]), bxn = std::sqrt(h[2 * nc + q]);
+    pm.lambda = lam_r[q];
+    pm.abs_res = rn;
+    pm.rel_res = lam_r[q] != 0.0 ? rn / (std::fabs(lam_r[q]) * bxn) : rn / bxn;
+    pm.eta = rn / ((P.normA + std::fabs(lam_r[q]) * P.normB) * xn);
+    pm.accepted = pm.eta <= cfg.tol;
+  }
+  // candidates with a significant imaginary part: the complex pair is kept when the real
+  // projection fails the tolerance and the complex pair does at least as well
+  if (!cidx.empty()) {
+    const std::size_t w = static_cast<std::size_t>(n) * 2;
+    std::vector<double> hx(w * cidx.size()), hax(hx.size()), hbx(hx.size());
+    const std::size_t off = static_cast<std::size_t>(n) * nc;
+    cuda_check(cudaMemcpyAsync(hx.data(), X.p + off, hx.size() * sizeof(double), cudaMemcpyDeviceToHost, s), "ghiep x");
+    cuda_check(cudaMemcpyAsync(hax.data(), AX.p + off, hx.size() * sizeof(double), cudaMemcpyDeviceToHost, s), "ghiep ax");
+    cuda_check(cudaMemcpyAsync(hbx.data(), BX.p + off, hx.size() * sizeof(double), cudaMemcpyDeviceToHost, s), "ghiep bx");
+    cuda_check(cudaStreamSynchronize(s), "ghiep complex");
+    out.xc = hx;
+    for (std::size_t t = 0; t < cidx.size(); ++t) {
+      const int q = cidx[t];
+      const double* x = &hx[t * w];
+      const double* ax = &hax[t * w];
+      const double* bx = &hbx[t * w];
+      // the unconjugated quotient x^T A x / x^T B x of the complex vector, under the same guard
+      cplx lam = mu[q];
+      cplx xax = 0.0, xbx = 0.0;
+      double bb = 0.0;
+      for (std::int64_t i = 0; i < n; ++i) {
+        const cplx xv(x[i], x[n + i]);
+        xax += xv * cplx(ax[i], ax[n + i]);
+        xbx += xv * cplx(bx[i], bx[n + i]);
+        bb += std::norm(cplx(bx[i], bx[n + i]));
+      }
+      if (std::abs(xbx) >= 1e-3 * std::sqrt(bb) && bb > 0.0) {
+        const cplx rq = xax / xbx;
+        if (std::abs(rq - mu[q]) <= 1e-6 * std::max(std::abs(mu[q]), scale)) lam = rq;
+      }
+      const PairMetrics pc = complex_metrics(P, n, x, ax, bx, lam, cfg.tol);
+      GhiepCand& c = cands[q];
+      if (c.pm.eta > cfg.tol && pc.eta <= c.pm.eta) {
+        c.real = false;
+        c.lambda = lam;
+        c.pm = pc;
+        c.col = static_cast<int>(t);
+      }
+    }
+  }
+  // selection (select_nearest): outside the user's zero band, trustworthy pairs first
+  auto dist = [&](const GhiepCand& c) { return std::abs(c.lambda - cplx(sigma)); };
+  std::vector<GhiepCand> good, poor;
+  for (const auto& c : cands) {
+    const bool trusted = c.pm.eta <= std::max(kTrustworthy, cfg.tol);
+    if (band_user >= 0.0 && std::abs(c.lambda) <= band_user) {
+      out.in_band += trusted;
+      continue;
+    }
+    (trusted ? good : poor).push_back(c);
+  }
+  auto nearer = [&](const GhiepCand& a, const GhiepCand& b) { return dist(a) < dist(b); };
+  std::stable_sort(good.begin(), good.end(), nearer);
+  std::stable_sort(poor.begin(), poor.end(), nearer);
+  if (good.size() > static_cast<std::size_t>(k)) good.resize(static_cast<std::size_t>(k));
+  out.good = static_cast<long long>(good.size());
+  out.sel = good;
+  for (const auto& c : poor) {
+    if (out.sel.size() >= static_cast<std::size_t>(k)) break;
+    out.sel.push_back(c);
+  }
+  std::stable_sort(out.sel.begin(), out.sel.end(), nearer);
+  out.coef = std::move(Y);
+  out.m = m;
+  out.cols = cols;
+  out.V = std::move(r.V);
+  cuda_check(cudaStreamSynchronize(s), "ghiep");
+  tm.verify += since(tv);
+  return out;
+}
+
 }  // namespace
 
 struct Session::Impl {
@@ -456,7 +723,7 @@ Session::Session(const CsrHost& a_in, const CsrHost* b_in, int device, std::uint
           if (b->ci[q] == i) d[i] += b->v[q];
       double mx = 0.0, mn = std::numeric_limits<double>::infinity();
       for (double x : d) { mx = std::max(mx, std::fabs(x)); mn = std::min(mn, x); }
-      HSG_REQUIRE(mn > 0.0, HSG_UNSUPPORTED, "B is indefinite (GHIEP): not served by this build");
+      if (!(mn > 0.0)) S.problem = "GHIEP";  // a non-positive diagonal entry: B is not positive definite
       P.bdiag.upload(d, P.s);
       P.normB = mx;
     }
@@ -478,10 +745,12 @@ Session::Session(const CsrHost& a_in, const CsrHost* b_in, int device, std::uint
     tm.factor += since(t0);
   }
   if (b && !P.b_diagonal) {
+    // definiteness of B by its inertia (hsolve src/driver/solver.cpp:426-441): B singular or with a
+    // negative pivot makes the pencil a GHIEP
     const auto t0 = Clock::now();
     hsg_inertia_t in = F.factorize(0.0, 1.0, true);
     tm.factor += since(t0);
-    HSG_REQUIRE(in.valid && in.neg == 0 && in.zero == 0, HSG_UNSUPPORTED, "B is not positive definite (GHIEP): not served by this build");
+    if (!(in.valid && in.neg == 0 && in.zero == 0)) S.problem = "GHIEP";
   }
 }
 
@@ -551,8 +820,99 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
   // fronts keep the whole device busy and shifts run one after another
   const bool batch = cfg.batch_shifts != 0 && F.estimate().flops <= kBatchFlopsMax;
   bool f_stale = false;  // F's factorization was overwritten by a count at another shift
+  // GHIEP: B indefinite (detected), or the indefinite path asked for (problem = 3)
+  HSG_REQUIRE(!(cfg.problem == 2 && problem == "GHIEP"), HSG_INVALID_INPUT,
+              "problem = generalized_definite, but B is not positive definite");
+  HSG_REQUIRE(!(cfg.problem == 3 && !b), HSG_INVALID_INPUT, "problem = generalized_indefinite needs B");
+  const bool ghiep = problem == "GHIEP" || cfg.problem == 3;
+  HSG_REQUIRE(!ghiep || cfg.mode == 0, HSG_UNSUPPORTED,
+              "indefinite-B problems support target mode 'nearest' only: interval / smallest / largest need "
+              "eigenvalue counts, which Sylvester inertia does not give for indefinite B");
+  std::vector<PairMetrics> cpm;  // GHIEP: metrics of the complex pairs (lambda_re in .lambda)
+  std::vector<double> c_im;      // and their imaginary parts
+  long long zero_cluster_dim = -1;
 
-  if (cfg.mode == 0) {
+  if (cfg.mode == 0 && ghiep) {
+    // ---------------------------------------------------------------- nearest, B indefinite
+    const std::int64_t k = cfg.k;
+    HSG_REQUIRE(k >= 1 && k < n, HSG_INVALID_INPUT, "k must be in [1, n)");
+    double sigma = cfg.sigma;
+    HSG_REQUIRE(std::isfinite(sigma), HSG_INVALID_INPUT, "sigma must be finite");
+    HSG_REQUIRE(cfg.complex_tol >= 0.0, HSG_INVALID_INPUT, "complex_tol must be >= 0");
+    cert.note = "not available for indefinite B (Sylvester inertia does not count eigenvalues)";
+    const double band_user = cfg.zero_filter_tol >= 0.0 ? cfg.zero_filter_tol * scale : -1.0;
+    const double band_zero = std::max(band_user, kGhiepZeroBand * scale);
+    if (!factorize_at(OPF, sigma, scale, cfg.max_shift_retries, shift_retries, tm))
+      HSG_THROW(HSG_SINGULAR, "A - sigma B is numerically singular at and near sigma = " << cfg.sigma);
+    op.set_refinement(sigma, tol_inner);
+    sigma_used = sigma;
+    int nev = static_cast<int>(std::min<std::int64_t>(n - 1, k + std::max<std::int64_t>(4, (k + 1) / 2)));
+    // the block width: multi-column solves cost little more than single ones on the GPU, and a block
+    // of p takes up to p copies of a multiple eigenvalue at once
+    const int p = cfg.block_size > 0
+                      ? static_cast<int>(std::max<std::int64_t>(1, std::min<std::int64_t>({cfg.block_size, nev, kMaxBlock, n / 16})))
+                      : auto_block(nev);
+    block_used = p;
+    GhiepRun run;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+      run = ghiep_run(op, P, sigma, nev, static_cast<int>(k), cfg, p, scale, band_user, cfg.complex_tol, tm);
+      restarts += run.restarts;
+      if (run.good >= k || nev >= n - 1) break;
+      warnings.push_back("fewer trustworthy pairs than k; rerun with more");
+      nev = static_cast<int>(std::min<std::int64_t>(n - 1, 2 * nev));
+    }
+    // does the zero cluster of A interfere: a selected pair in its band, too few pairs, or the
+    // selection disk reaching the band (indefinite.cpp:763-772)
+    double radius = 0.0;
+    bool touches = static_cast<std::int64_t>(run.sel.size()) < k;
+    for (const auto& c : run.sel) {
+      radius = std::max(radius, std::abs(c.lambda - std::complex<double>(sigma)));
+      touches = touches || std::abs(c.lambda) <= band_zero;
+    }
+    touches = touches || radius >= std::fabs(sigma) - band_zero;
+    if (touches) {
+      // dim null(A): null pivots of an LDL^T of A on the same analysis (indefinite.cpp:561)
+      const auto t0 = Clock::now();
+      zero_cluster_dim = static_cast<long long>(F.factorize(1.0, 0.0, true).null_pivots);
+      tm.factor += since(t0);
+      HSG_REQUIRE(band_user < 0.0 && zero_cluster_dim == 0, HSG_UNSUPPORTED,
+                  "the " << k << " eigenvalues nearest sigma = " << sigma << " reach the zero cluster of A (dimension "
+                         << zero_cluster_dim << ", |lambda| <= " << band_zero
+                         << "): the one-sided runs around the cluster are not built; choose sigma so that the k "
+                            "nearest eigenvalues lie closer to sigma than 0 does");
+    }
+    // outputs: real pairs nearest first, then the complex ones
+    std::vector<double> S;
+    for (const auto& c : run.sel) {
+      if (c.real) {
+        lam_out.push_back(c.lambda.real());
+        S.insert(S.end(), run.coef.begin() + static_cast<std::ptrdiff_t>(c.col) * run.m,
+                 run.coef.begin() + static_cast<std::ptrdiff_t>(c.col + 1) * run.m);
+      } else {
+        out.complex_eigenvalues.push_back(c.lambda.real());
+        out.complex_eigenvalues.push_back(c.lambda.imag());
+        const double* x = &run.xc[static_cast<std::size_t>(c.col) * 2 * n];
+        for (std::int64_t i = 0; i < n; ++i) {
+          out.complex_vectors.push_back(x[i]);
+          out.complex_vectors.push_back(x[n + i]);
+        }
+        cpm.push_back(c.pm);
+        c_im.push_back(c.lambda.imag());
+      }
+    }
+    const int kr = static_cast<int>(lam_out.size());
+    Xout.alloc(static_cast<std::size_t>(n) * std::max(kr, 1));
+    if (kr > 0) {
+      DevBuf<double> Sd;
+      Sd.upload(S, P.s);
+      gemm_tall(n, run.m, kr, run.V.p, n, Sd.p, run.m, Xout.p, n, 1.0, 0.0, P.s);
+      cuda_check(cudaStreamSynchronize(P.s), "ghiep vectors");
+    }
+    if (!cpm.empty())
+      warnings.push_back(std::to_string(cpm.size()) + " genuinely complex eigenvalue(s) returned separately");
+    if (static_cast<std::int64_t>(run.sel.size()) < k)
+      warnings.push_back("only " + std::to_string(run.sel.size()) + " of " + std::to_string(k) + " pairs found");
+  } else if (cfg.mode == 0) {
     // ---------------------------------------------------------------- nearest
     const std::int64_t k = cfg.k;
     HSG_REQUIRE(k >= 1 && k < n, HSG_INVALID_INPUT, "k must be in [1, n)");
@@ -812,6 +1172,8 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
   tm.verify += since(t_ver);
   bool all_ok = true;
   for (const auto& q : pm) all_ok = all_ok && q.accepted;
+  for (const auto& q : cpm) all_ok = all_ok && q.accepted;
+  if (ghiep) all_ok = all_ok && static_cast<std::int64_t>(m + cpm.size()) == cfg.k;
   const bool success = all_ok && (!cert.performed || cert.passed) && (cfg.mode != 1 || m == cert.count_inertia);
   // report
   const hsg_estimate_t est = F.estimate();
@@ -822,11 +1184,11 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
   j.kv("nnz_a", static_cast<long long>(a.rp[n]));
   j.kv("nnz_b", static_cast<long long>(b ? b->rp[n] : 0));
   j.kv("complex_scalars", false);
-  j.kv("problem", problem);
+  j.kv("problem", std::string(ghiep ? "GHIEP" : problem));
   j.kv("norm2_a", P.normA);
   j.kv("norm2_b", P.normB);
   j.kv("scale", scale);
-  j.kv("method", std::string("shift_invert_lanczos"));
+  j.kv("method", std::string(ghiep ? "shift_invert_krylov_schur" : "shift_invert_lanczos"));
   j.kv("candidate_source", std::string("iterative"));
   j.kv("sigma_requested", cfg.mode == 0 ? cfg.sigma : 0.5 * (cfg.lower + cfg.upper));
   j.kv("sigma_used", sigma_used);
@@ -903,10 +1265,11 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
   j.close('}');
   j.key("pairs");
   j.open('[');
-  for (const auto& q : pm) {
+  for (std::size_t i = 0; i < pm.size() + cpm.size(); ++i) {
+    const PairMetrics& q = i < pm.size() ? pm[i] : cpm[i - pm.size()];
     j.open('{');
     j.kv("lambda_re", q.lambda);
-    j.kv("lambda_im", 0.0);
+    j.kv("lambda_im", i < pm.size() ? 0.0 : c_im[i - pm.size()]);
     j.kv("abs_residual", q.abs_res);
     j.kv("rel_residual", q.rel_res);
     j.kv("backward_error", q.eta);
@@ -914,6 +1277,7 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
     j.close('}');
   }
   j.close(']');
+  j.kv("zero_cluster_dim", zero_cluster_dim);
   j.key("certificate");
   j.open('{');
   j.kv("performed", cert.performed);

@@ -1,5 +1,6 @@
-// Top-level shift-invert driver: the device-resident equivalent of hs::solve for HEP / GHEP
-// (hsolve include/hsolve/solver.hpp:545-547; src/driver/solver.cpp:307-520, definite.cpp).
+// Top-level shift-invert driver: the device-resident equivalent of hs::solve for HEP / GHEP / GHIEP
+// (hsolve include/hsolve/solver.hpp:545-547; src/driver/solver.cpp:307-520, definite.cpp,
+// indefinite.cpp).
 #pragma once
 
 #include <cstdint>
@@ -21,6 +22,9 @@ struct CsrHost {
 struct SolveOutput {
   std::vector<double> eigenvalues;
   std::vector<double> vectors;  // n x m, column-major
+  // GHIEP: genuinely complex pairs, values and n x mc vectors as interleaved (re, im) doubles
+  std::vector<double> complex_eigenvalues;
+  std::vector<double> complex_vectors;
   std::int64_t n = 0;
   std::string report_json;
 };

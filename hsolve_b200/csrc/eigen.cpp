@@ -309,3 +309,150 @@ KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, 
 }
 
 }  // namespace hsg
+
+namespace hsg {
+
+GeneralKsResult krylov_schur_general(KrylovOperator& op, std::int64_t n, const KsOptions& opt, cudaStream_t s) {
+  using cplx = std::complex<double>;
+  const int p = std::max(1, std::min(opt.block, kMaxBlock));
+  const int nev = std::max(1, opt.nev);
+  int mmax = opt.ncv > 0 ? opt.ncv : std::max(2 * nev + 1, nev + 16) + 4 * p;
+  mmax = std::max(mmax, nev + 2 * p + 2);
+  mmax = (mmax + p - 1) / p * p;
+  if (mmax > n) mmax = static_cast<int>(n / p * p);
+  HSG_REQUIRE(mmax >= p + 1 && nev < mmax, HSG_INVALID_INPUT, "Krylov basis larger than the problem (n = " << n << ")");
+  Basis B;
+  B.n = n;
+  B.bid = true;  // Euclidean inner product: B is indefinite, no inner product comes from it
+  B.cols = mmax + p;
+  B.V.alloc(static_cast<std::size_t>(n) * B.cols);
+  B.tmp.alloc(static_cast<std::size_t>(n) * std::max(p, mmax));
+  B.g.alloc(static_cast<std::size_t>(B.cols) * std::max(p, mmax));
+  B.part_cap = gram_part_size(n, B.cols, p);
+  B.part.alloc(static_cast<std::size_t>(B.part_cap));
+  B.small.alloc(static_cast<std::size_t>(std::max(p * p, mmax * mmax)));
+  std::mt19937_64 rng(opt.seed);
+  GeneralKsResult res;
+  random_block(B, 0, p, rng, s);
+  {
+    std::vector<double> H;
+    ortho_block(B, op, 0, p, H, rng, s);
+  }
+  const int hd = mmax + p;
+  std::vector<double> Hm(static_cast<std::size_t>(hd) * hd, 0.0);
+  auto Hij = [&](int i, int j) -> double& { return Hm[static_cast<std::size_t>(i) + static_cast<std::size_t>(j) * hd]; };
+  int m = 0;
+  const int strict = opt.nev_strict > 0 ? std::min(opt.nev_strict, nev) : nev;
+  while (true) {
+    while (m + p <= mmax) {
+      const int j0 = m;
+      auto tp = std::chrono::steady_clock::now();
+      op.apply(B.v(j0), n, B.v(j0 + p), n, p);
+      res.t_apply += seconds_since(tp);
+      res.applies += p;
+      std::vector<double> H;
+      tp = std::chrono::steady_clock::now();
+      std::vector<double> R = ortho_block(B, op, j0 + p, p, H, rng, s);
+      res.t_ortho += seconds_since(tp);
+      const int jh = j0 + p;
+      for (int c = 0; c < p; ++c) {
+        for (int i = 0; i < jh; ++i) Hij(i, j0 + c) = H[i + static_cast<std::size_t>(c) * jh];
+        for (int a = 0; a < p; ++a) Hij(jh + a, j0 + c) = R[a + c * p];
+      }
+      m += p;
+    }
+    // Rayleigh-Ritz: complex Schur form of G = H[0:m, 0:m], wanted values (largest |theta|) first
+    const auto trr = std::chrono::steady_clock::now();
+    std::vector<double> G(static_cast<std::size_t>(m) * m);
+    for (int j = 0; j < m; ++j)
+      for (int i = 0; i < m; ++i) G[i + static_cast<std::size_t>(j) * m] = Hij(i, j);
+    std::vector<cplx> T, U;
+    complex_schur(m, G, T, U);
+    std::vector<double> key(m);
+    for (int i = 0; i < m; ++i) key[i] = -std::abs(T[static_cast<std::size_t>(i) * (m + 1)]);
+    schur_sort(m, T, U, key);
+    auto diag = [&](int i) { return T[static_cast<std::size_t>(i) * (m + 1)]; };
+    // a set closed under conjugation: a complex value at its end takes its partner along
+    auto closed = [&](int w) {
+      if (w > 0 && w < m && std::abs(diag(w - 1).imag()) > 1e-12 * std::abs(diag(w - 1)) &&
+          std::abs(diag(w) - std::conj(diag(w - 1))) <= 1e-8 * std::abs(diag(w - 1)))
+        ++w;
+      return w;
+    };
+    const int want = closed(std::min(nev, m));
+    const std::vector<cplx> Y = schur_eigenvectors(m, T, want, 1e-8);
+    std::vector<cplx> C(static_cast<std::size_t>(m) * want, cplx(0.0));  // U Y
+    for (int k = 0; k < want; ++k)
+      for (int t = 0; t < m; ++t) {
+        const cplx y = Y[static_cast<std::size_t>(k) * m + t];
+        if (y == cplx(0.0)) continue;
+        for (int i = 0; i < m; ++i) C[static_cast<std::size_t>(k) * m + i] += U[static_cast<std::size_t>(t) * m + i] * y;
+      }
+    std::vector<double> rn(want);
+    int nconv = 0, nstrict = 0;
+    for (int k = 0; k < want; ++k) {
+      double acc = 0.0;
+      for (int a = 0; a < p; ++a) {
+        cplx v = 0.0;
+        for (int i = 0; i < m; ++i) v += Hij(m + a, i) * C[static_cast<std::size_t>(k) * m + i];
+        acc += std::norm(v);
+      }
+      rn[k] = std::sqrt(acc);
+      const double tl = k < strict ? opt.tol : std::max(opt.tol, opt.tol_buffer);
+      if (rn[k] <= tl * std::abs(diag(k))) {
+        ++nconv;
+        if (k < strict) ++nstrict;
+      }
+    }
+    res.t_rr += seconds_since(trr);
+    if (nconv >= want || res.restarts >= opt.max_restarts) {
+      res.theta.resize(want);
+      res.resid = rn;
+      res.converged.resize(want);
+      for (int k = 0; k < want; ++k) {
+        res.theta[k] = diag(k);
+        const double tl = k < strict ? opt.tol : std::max(opt.tol, opt.tol_buffer);
+        res.converged[k] = rn[k] <= tl * std::abs(diag(k));
+      }
+      res.coef = C;
+      res.m = m;
+      res.V = std::move(B.V);
+      return res;
+    }
+    // thick restart on the real basis of the invariant subspace of the first `keep` Schur vectors
+    const auto trs = std::chrono::steady_clock::now();
+    // a conjugate pair split at the end of the kept set is completed, or dropped when the basis has
+    // no room for its partner
+    int keep0 = std::min(mmax - p, std::max(nev + p, (nev + mmax) / 2));
+    if (closed(keep0) != keep0) keep0 += keep0 + 1 <= mmax - p ? 1 : -1;
+    int keep = 0;
+    std::vector<double> Q = real_span(m, keep0, U, keep, keep0);
+    HSG_REQUIRE(keep >= 1 && keep + p <= mmax, HSG_NOT_CONVERGED, "general Krylov-Schur: restart basis degenerate");
+    // Tn = Q^T G Q, coupling Hres Q
+    std::vector<double> GQ = matmul(m, m, keep, G, Q);
+    std::vector<double> QT(static_cast<std::size_t>(keep) * m);
+    for (int a = 0; a < keep; ++a)
+      for (int i = 0; i < m; ++i) QT[a + static_cast<std::size_t>(i) * keep] = Q[i + static_cast<std::size_t>(a) * m];
+    std::vector<double> Tn = matmul(keep, m, keep, QT, GQ);
+    std::vector<double> Hres(static_cast<std::size_t>(p) * m);
+    for (int j = 0; j < m; ++j)
+      for (int a = 0; a < p; ++a) Hres[a + static_cast<std::size_t>(j) * p] = Hij(m + a, j);
+    std::vector<double> Cp = matmul(p, m, keep, Hres, Q);
+    B.small.alloc(Q.size());
+    to_dev(B.small.p, Q, s);
+    gemm_tall(n, m, keep, B.v(0), n, B.small.p, m, B.tmp.p, n, 1.0, 0.0, s);
+    copy_cols(n, p, B.v(m), n, B.v(keep), n, s);
+    copy_cols(n, keep, B.tmp.p, n, B.v(0), n, s);
+    std::fill(Hm.begin(), Hm.end(), 0.0);
+    for (int j = 0; j < keep; ++j) {
+      for (int i = 0; i < keep; ++i) Hij(i, j) = Tn[i + static_cast<std::size_t>(j) * keep];
+      for (int a = 0; a < p; ++a) Hij(keep + a, j) = Cp[a + static_cast<std::size_t>(j) * p];
+    }
+    m = keep;
+    res.restarts += 1;
+    cuda_check(cudaStreamSynchronize(s), "restart");
+    res.t_restart += seconds_since(trs);
+  }
+}
+
+}  // namespace hsg

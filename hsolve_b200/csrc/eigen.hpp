@@ -7,6 +7,7 @@
 // matrix on the host, thick restart keeping the wanted Ritz vectors.
 #pragma once
 
+#include <complex>
 #include <cstdint>
 #include <vector>
 
@@ -62,5 +63,26 @@ struct KsResult {
 };
 
 KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, cudaStream_t stream);
+
+}  // namespace hsg
+
+namespace hsg {
+
+// Block Krylov-Schur for a general (non-symmetric) operator, such as OP = (A - sigma B)^{-1} B with
+// B indefinite (hsolve's krylov_schur_general, include/hsolve/eigen.hpp:254-256): Euclidean CGS2 /
+// CholQR2 basis, projected matrix in complex Schur form (host), wanted Ritz values (largest |theta|)
+// moved to the front, thick restart on the real basis of their invariant subspace.
+struct GeneralKsResult {
+  std::vector<std::complex<double>> theta;  // the wanted Ritz values, by decreasing |theta|
+  std::vector<double> resid;
+  std::vector<char> converged;
+  std::vector<std::complex<double>> coef;   // m x wanted coefficients of the Ritz vectors in V
+  int m = 0;
+  DevBuf<double> V;                         // n x m basis (orthonormal)
+  int restarts = 0, applies = 0;
+  double t_apply = 0.0, t_ortho = 0.0, t_rr = 0.0, t_restart = 0.0;
+};
+
+GeneralKsResult krylov_schur_general(KrylovOperator& op, std::int64_t n, const KsOptions& opt, cudaStream_t stream);
 
 }  // namespace hsg

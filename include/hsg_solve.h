@@ -39,6 +39,11 @@ typedef struct {
                                  slice factorization) run at once on several factorization objects;
                                  0: one after another on one object (the plain path). No counterpart
                                  in hsolve. */
+  double complex_tol;         /* GHIEP: a pair is complex only if |Im lambda| > complex_tol *
+                                 max(|lambda|, scale) and its real projection fails tol while the
+                                 complex pair does at least as well; default 1e-8 */
+  double zero_filter_tol;     /* GHIEP: < 0 (default) off; else eigenvalues with |lambda| <=
+                                 zero_filter_tol * scale are zero modes, left out of the selection */
 } hsg_solve_config_t;
 
 typedef struct hsg_solution hsg_solution;
@@ -70,6 +75,11 @@ HSG_API int hsg_session_estimate(const hsg_session* s, hsg_estimate_t* out);
 HSG_API int hsg_solution_sizes(const hsg_solution* s, int64_t* n, int64_t* m);
 /* Copies eigenvalues (m) and eigenvectors (n x m column-major; NULL to skip). */
 HSG_API int hsg_solution_copy(const hsg_solution* s, double* eigenvalues, double* eigenvectors);
+/* Solution<double>::complex_eigenvalues.size(): the genuinely complex pairs of a GHIEP (usually 0). */
+HSG_API int hsg_solution_complex_count(const hsg_solution* s, int64_t* mc);
+/* Copies complex_eigenvalues (mc, as re, im pairs) and complex_eigenvectors (n x mc column-major,
+ * every entry as re, im; NULL to skip), the layout of C99 double complex / std::complex<double>. */
+HSG_API int hsg_solution_complex_copy(const hsg_solution* s, double* eigenvalues, double* eigenvectors);
 /* SolveReport::to_json(). Valid until hsg_solution_free. */
 HSG_API const char* hsg_solution_report(const hsg_solution* s);
 HSG_API void hsg_solution_free(hsg_solution* s);
