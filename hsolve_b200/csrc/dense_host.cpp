@@ -383,34 +383,33 @@ std::vector<cplx> schur_eigenvectors(int n, const std::vector<cplx>& T, int coun
   return Y;
 }
 
-std::vector<double> real_span(int m, int k, const std::vector<std::complex<double>>& c, int& r, int max_r,
-                              double drop_tol) {
+std::vector<double> pivoted_basis(int m, int count, const std::vector<double>& pool, int want, double min_norm, int& r) {
   std::vector<double> q;
   r = 0;
-  std::vector<double> v(m);
-  for (int j = 0; j < 2 * k && r < max_r; ++j) {
-    for (int i = 0; i < m; ++i) {
-      const std::complex<double> z = c[static_cast<std::size_t>(i) + static_cast<std::size_t>(j / 2) * m];
-      v[i] = j % 2 == 0 ? z.real() : z.imag();
-    }
-    double n0 = 0.0;
-    for (double x : v) n0 += x * x;
-    n0 = std::sqrt(n0);
-    if (n0 == 0.0) continue;
-    for (int pass = 0; pass < 2; ++pass)
-      for (int t = 0; t < r; ++t) {
-        const double* qt = &q[static_cast<std::size_t>(t) * m];
-        double d = 0.0;
-        for (int i = 0; i < m; ++i) d += qt[i] * v[i];
-        for (int i = 0; i < m; ++i) v[i] -= d * qt[i];
+  std::vector<double> v(m), best(m);
+  for (; r < want; ++r) {
+    double best_norm = -1.0;
+    for (int j = 0; j < count; ++j) {
+      std::copy(pool.begin() + static_cast<std::ptrdiff_t>(j) * m, pool.begin() + static_cast<std::ptrdiff_t>(j + 1) * m,
+                v.begin());
+      for (int pass = 0; pass < 2; ++pass)
+        for (int t = 0; t < r; ++t) {
+          const double* qt = &q[static_cast<std::size_t>(t) * m];
+          double d = 0.0;
+          for (int i = 0; i < m; ++i) d += qt[i] * v[i];
+          for (int i = 0; i < m; ++i) v[i] -= d * qt[i];
+        }
+      double nr = 0.0;
+      for (double x : v) nr += x * x;
+      nr = std::sqrt(nr);
+      if (nr > best_norm) {
+        best_norm = nr;
+        best = v;
       }
-    double n1 = 0.0;
-    for (double x : v) n1 += x * x;
-    n1 = std::sqrt(n1);
-    if (n1 <= drop_tol * n0) continue;
-    for (double& x : v) x /= n1;
-    q.insert(q.end(), v.begin(), v.end());
-    ++r;
+    }
+    if (!(best_norm >= min_norm)) break;
+    for (double& x : best) x /= best_norm;
+    q.insert(q.end(), best.begin(), best.end());
   }
   return q;
 }

@@ -38,11 +38,12 @@ void schur_sort(int n, std::vector<std::complex<double>>& T, std::vector<std::co
 std::vector<std::complex<double>> schur_eigenvectors(int n, const std::vector<std::complex<double>>& T, int count,
                                                      double cluster_rtol);
 
-// Orthonormal real basis (m x r, column-major, r returned) of the span of the columns of the complex
-// m x k matrix c and of their conjugates, i.e. of [Re c_0, Im c_0, Re c_1, ...], by Gram-Schmidt
-// with re-orthogonalization; a column whose remainder is below drop_tol of its own norm adds
-// nothing, and the basis stops at max_r columns.
-std::vector<double> real_span(int m, int k, const std::vector<std::complex<double>>& c, int& r, int max_r,
-                              double drop_tol = 1e-9);
+// Greedy orthonormal basis (m x r, column-major, r <= want returned) drawn from the `count` pool
+// vectors (m x count, column-major; parts of unit vectors, so norms are comparable): each step takes
+// the pool vector with the largest remainder norm after projection on the basis so far (two passes),
+// and the basis stops when that largest remainder falls below min_norm. A direction that is only
+// rounding noise (a tiny part, such as the imaginary part of a nearly real vector) is therefore never
+// taken while a genuine one is left.
+std::vector<double> pivoted_basis(int m, int count, const std::vector<double>& pool, int want, double min_norm, int& r);
 
 }  // namespace hsg

@@ -497,8 +497,10 @@ GhiepRun ghiep_run(ShiftInvertOp& op, Problem& P, double sigma, int nev, int k, 
     if (nr > 0.0)
       for (int i = 0; i < m; ++i) y[i] /= nr;
   }
-  // a multiple real eigenvalue: its candidates take an orthonormal basis of the real span of their
-  // vectors (the eigenspace of a real eigenvalue of a real pencil is real), so they stay independent
+  // a multiple real eigenvalue: its candidates take an orthonormal basis of its (real) eigenspace,
+  // drawn greedily from their real vectors and the real and imaginary parts of their Ritz vectors
+  // (the best-separated directions first, so that a part that is only rounding noise is never
+  // taken), so the copies stay independent
   {
     std::vector<int> rs;
     for (int q = 0; q < nc; ++q)
@@ -511,11 +513,15 @@ GhiepRun ghiep_run(ShiftInvertOp& op, Problem& P, double sigma, int nev, int k, 
         ++g1;
       const int g = static_cast<int>(g1 - g0);
       if (g > 1) {
-        std::vector<cplx> Cg(static_cast<std::size_t>(m) * g);
+        std::vector<double> pool(static_cast<std::size_t>(m) * 3 * g);
         for (int t = 0; t < g; ++t)
-          for (int i = 0; i < m; ++i) Cg[static_cast<std::size_t>(t) * m + i] = cf(rs[g0 + t], i);
+          for (int i = 0; i < m; ++i) {
+            pool[static_cast<std::size_t>(t) * m + i] = Y[static_cast<std::size_t>(rs[g0 + t]) * m + i];
+            pool[static_cast<std::size_t>(g + 2 * t) * m + i] = cf(rs[g0 + t], i).real();
+            pool[static_cast<std::size_t>(g + 2 * t + 1) * m + i] = cf(rs[g0 + t], i).imag();
+          }
         int rank = 0;
-        std::vector<double> Qg = real_span(m, g, Cg, rank, g);
+        std::vector<double> Qg = pivoted_basis(m, 3 * g, pool, g, 1e-3, rank);
         if (rank == g)
           for (int t = 0; t < g; ++t)
             std::copy(Qg.begin() + static_cast<std::ptrdiff_t>(t) * m, Qg.begin() + static_cast<std::ptrdiff_t>(t + 1) * m,

@@ -425,8 +425,16 @@ GeneralKsResult krylov_schur_general(KrylovOperator& op, std::int64_t n, const K
     // no room for its partner
     int keep0 = std::min(mmax - p, std::max(nev + p, (nev + mmax) / 2));
     if (closed(keep0) != keep0) keep0 += keep0 + 1 <= mmax - p ? 1 : -1;
+    // (greedy on the real and imaginary parts of the Schur vectors: for a conjugation-closed set the
+    // invariant subspace is real, of dimension keep0, and rounding-noise parts are never taken)
+    std::vector<double> pool(static_cast<std::size_t>(m) * 2 * keep0);
+    for (int t = 0; t < keep0; ++t)
+      for (int i = 0; i < m; ++i) {
+        pool[static_cast<std::size_t>(2 * t) * m + i] = U[static_cast<std::size_t>(t) * m + i].real();
+        pool[static_cast<std::size_t>(2 * t + 1) * m + i] = U[static_cast<std::size_t>(t) * m + i].imag();
+      }
     int keep = 0;
-    std::vector<double> Q = real_span(m, keep0, U, keep, keep0);
+    std::vector<double> Q = pivoted_basis(m, 2 * keep0, pool, keep0, 1e-6, keep);
     HSG_REQUIRE(keep >= 1 && keep + p <= mmax, HSG_NOT_CONVERGED, "general Krylov-Schur: restart basis degenerate");
     // Tn = Q^T G Q, coupling Hres Q
     std::vector<double> GQ = matmul(m, m, keep, G, Q);

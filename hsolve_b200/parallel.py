@@ -50,33 +50,70 @@ class WindowPart:
     count: int
 
 
+def _count_near(count_below, s: float, step: float, tries: int = 4):
+    """(point, count) at s, or at s + step, s - 2 step, s + 3 step, ... when the count at s is None
+    (a singular factorization: s lies on an eigenvalue to working precision); (s, None) if every
+    try was singular."""
+    for t in range(tries + 1):
+        x = s + (t if t % 2 else -t) * step if t else s
+        n = count_below(x)
+        if n is not None:
+            return x, n
+    return s, None
+
+
+def _bisect(count_below, lo: float, hi: float, goal: int, steps: int):
+    """First bisection point s of (lo, hi) with count_below(s) == goal: (s, None), or (None, (a, b,
+    n_a, n_b)) with the final bracket when no point of the search had that count."""
+    a, b = lo, hi
+    na = nb = None
+    for _ in range(steps):
+        mid, nm = _count_near(count_below, 0.5 * (a + b), 1e-3 * (b - a))
+        if nm is None:
+            break
+        if nm == goal:
+            return mid, None
+        if nm < goal:
+            a, na = mid, nm
+        else:
+            b, nb = mid, nm
+    return None, (a, b, na, nb)
+
+
 def plan_window(count_below, lower: float, upper: float, parts: int, max_bisect: int = 40) -> list[WindowPart]:
     """Sub-windows of [lower, upper) holding about equal numbers of eigenvalues: `count_below(s)`
-    is the Sylvester count nu_-(A - s B) (an FP64 inertia count). Cut points are placed by bisection
-    on the count; every part carries its certified count."""
-    n_lo, n_hi = count_below(lower), count_below(upper)
+    is the Sylvester count nu_-(A - s B) of an FP64 factorization, or None when that factorization
+    is singular (s on an eigenvalue to working precision; such a point is never used). Cut points
+    are placed by bisection on the count; every part carries its certified count. A multiple
+    eigenvalue that straddles a goal count cannot be split: the search then takes the count just
+    below it (or, if that adds nothing, just above it) and cuts at the first bisection point of the
+    gap next to it, so that no cut converges onto an eigenvalue. A singular window end is moved by
+    a few multiples of 1e-9 of the window width until its factorization is regular."""
+    width = upper - lower
+    lower, n_lo = _count_near(count_below, lower, -1e-9 * width)
+    upper, n_hi = _count_near(count_below, upper, 1e-9 * width)
+    if n_lo is None or n_hi is None:
+        raise ValueError("plan_window: the window ends stay singular after moves")
     total = n_hi - n_lo
     parts = max(1, min(parts, total)) if total > 0 else 1
     cuts, below = [lower], [n_lo]
     for q in range(1, parts):
         goal = n_lo + round(q * total / parts)
-        a, b = cuts[-1], upper
-        na = below[-1]
-        if goal <= na:
+        if goal <= below[-1] or goal >= n_hi:
             continue
-        for _ in range(max_bisect):
-            mid = 0.5 * (a + b)
-            nm = count_below(mid)
-            if nm < goal:
-                a, na = mid, nm
-            else:
-                b = mid
-            if nm == goal:
-                a, na = mid, nm
-                break
-        if na > below[-1]:
-            cuts.append(a)
-            below.append(na)
+        s, bracket = _bisect(count_below, cuts[-1], upper, goal, max_bisect)
+        got = goal
+        if s is None:
+            a, b, na, nb = bracket
+            if na is not None and na > below[-1]:
+                got = na
+                s, _ = _bisect(count_below, cuts[-1], a, na, max_bisect)
+            elif nb is not None and nb < n_hi:
+                got = nb
+                s, _ = _bisect(count_below, b, upper, nb, max_bisect)
+        if s is not None and got > below[-1]:
+            cuts.append(s)
+            below.append(got)
     cuts.append(upper)
     below.append(n_hi)
     return [WindowPart(cuts[i], cuts[i + 1], below[i + 1] - below[i]) for i in range(len(cuts) - 1)]
@@ -126,7 +163,8 @@ class Dealer:
                 f.analyze(A, B, 1.0, -0.5 * (lower + upper))
 
                 def counter(s, _f=f):
-                    return _f.count(1.0, -s).neg
+                    r = _f.count(1.0, -s)
+                    return r.neg if r.valid else None
 
             if solver is None:
                 sess = Session(A, B, device=self.device)

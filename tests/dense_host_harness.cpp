@@ -64,3 +64,12 @@ extern "C" int t_schur(int n, const double* a_in, const double* key, int count, 
   }
   return 0;
 }
+
+// greedy orthonormal basis of a pool of vectors; returns its column count
+extern "C" int t_pivoted_basis(int m, int count, const double* pool_in, int want, double min_norm, double* q_out) {
+  std::vector<double> pool(pool_in, pool_in + static_cast<std::size_t>(m) * count);
+  int r = 0;
+  const std::vector<double> q = hsg::pivoted_basis(m, count, pool, want, min_norm, r);
+  std::memcpy(q_out, q.data(), sizeof(double) * q.size());
+  return r;
+}

@@ -32,6 +32,8 @@ def lib(tmp_path_factory):
     L.t_matmul.argtypes = [I, I, I, P, P, P]
     L.t_schur.argtypes = [I, P, P, I, D, P, P, P]
     L.t_schur.restype = I
+    L.t_pivoted_basis.argtypes = [I, I, P, I, D, P]
+    L.t_pivoted_basis.restype = I
     return L
 
 
@@ -177,3 +179,27 @@ def test_schur_eigenvectors_of_a_multiple_eigenvalue_are_independent(lib):
         idx = np.flatnonzero(np.abs(lam - value) < 1e-6)
         assert idx.size == mult
         assert np.linalg.matrix_rank(x[:, idx], tol=1e-6) == mult
+
+
+def test_pivoted_basis_takes_genuine_directions_before_rounding_noise(lib):
+    """The real basis of a double real eigenvalue's eigenspace from complex Ritz vectors: each is a
+    phase times a real eigenvector plus noise, so its imaginary part after the phase is mostly noise;
+    the greedy basis must span the two true directions and ignore the noise."""
+    rng = np.random.default_rng(5)
+    m = 30
+    u, _ = np.linalg.qr(rng.standard_normal((m, 2)))
+    noise = 1e-9 * rng.standard_normal((m, 4))
+    c1 = np.exp(0.3j) * u[:, 0] + noise[:, 0] + 1j * noise[:, 1]
+    c2 = np.exp(-1.1j) * (0.6 * u[:, 0] + 0.8 * u[:, 1]) + noise[:, 2] + 1j * noise[:, 3]
+    # pool: the two imaginary-part noise directions first, then the real and imaginary parts
+    pool = np.column_stack([noise[:, 1] / 1e-9 * 1e-9, c1.real, c1.imag, c2.real, c2.imag])
+    pool = np.asfortranarray(pool)
+    q = np.zeros((m, 2), order="F")
+    r = lib.t_pivoted_basis(m, pool.shape[1], _p(pool), 2, 1e-3, _p(q))
+    assert r == 2
+    assert np.abs(q.T @ q - np.eye(2)).max() < 1e-12
+    # q spans span(u): the projection of u on q is complete
+    assert np.linalg.norm(u - q @ (q.T @ u)) < 1e-7
+    # a pool of one genuine direction yields one column
+    pool1 = np.asfortranarray(np.column_stack([u[:, 0], 1e-10 * rng.standard_normal(m)]))
+    assert lib.t_pivoted_basis(m, 2, _p(pool1), 2, 1e-3, _p(q)) == 1

@@ -234,7 +234,8 @@ def test_inertia_only_count_equals_the_factorization(case, golden):
         ok = f.factorize(1.0, -s)
         fi = f.inertia()
         ci = c.count(1.0, -s)
-        assert (ci.neg, ci.zero, ci.pos, ci.valid) == (fi.neg, fi.zero, fi.pos, fi.valid == ok), (s, ci, fi)
+        assert (ci.neg, ci.zero, ci.pos, ci.valid) == (fi.neg, fi.zero, fi.pos, fi.valid), (s, ci, fi)
+        assert bool(fi.valid) == bool(ok)
         assert ci.two_by_two == fi.two_by_two
         if case != "saddle" and ok:
             assert ci.neg == yee_exact.count_below(w, s)

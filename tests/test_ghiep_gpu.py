@@ -57,12 +57,12 @@ def _complex_pencil(seed=7):
     """A block pencil (2 x 2 blocks with B = diag(1, -1) and complex eigenvalue pairs, 1 x 1 blocks
     with B = +-1) under the congruence P^T (.) P with P = I + 0.3 (superdiagonal): eigenvalues known."""
     rng = np.random.default_rng(seed)
-    q, r = 40, 200
+    q, r = 30, 60
     n = 2 * q + r
     ra, rb = [], []
     lam = []
     for i in range(q):
-        re, im = rng.uniform(-2.0, 2.0), rng.uniform(0.05, 0.5)
+        re, im = rng.uniform(-1.0, 1.0), rng.uniform(0.01, 0.15)
         # lambda = ((a - c) +- sqrt((a + c)^2 - 4 b^2)) / 2 with a + c = s, b > |s| / 2
         s = rng.uniform(-0.5, 0.5)
         av, cv = (2 * re + s) / 2, (s - 2 * re) / 2
@@ -75,7 +75,8 @@ def _complex_pencil(seed=7):
         ra.append(np.array([[sg * d]]))
         rb.append(np.array([[sg]]))
         lam.append(complex(d, 0.0))
-    a0, b0 = sp.block_diag(ra, format="csr"), sp.block_diag(rb, format="csr")
+    a0 = sp.block_diag([sp.csr_matrix(m) for m in ra], format="csr")
+    b0 = sp.block_diag([sp.csr_matrix(m) for m in rb], format="csr")
     p = sp.eye(n, format="csr") + 0.3 * sp.eye(n, k=1, format="csr")
     a = (p.T @ a0 @ p).tocsr()
     b = (p.T @ b0 @ p).tocsr()

@@ -44,6 +44,48 @@ def test_plan_window_parts_count_the_whole_window():
             assert len(plan) >= 2
 
 
+def test_plan_window_never_cuts_onto_a_multiple_eigenvalue():
+    """Every eigenvalue of a spectrum of double eigenvalues: a goal count that falls between the two
+    copies cannot be met, and the cut must go into a gap, well away from every eigenvalue."""
+    base = np.sort(np.random.default_rng(3).uniform(40.0, 200.0, 25))
+    w = np.repeat(base, 2)
+
+    def count(s):
+        return int(np.searchsorted(w, s, side="left"))
+
+    for parts in (2, 3, 4, 7):
+        plan = parallel.plan_window(count, 40.0, 200.0, parts)
+        assert sum(p.count for p in plan) == w.size
+        for p in plan[1:]:
+            assert np.min(np.abs(w - p.lower)) > 1e-6 * 200.0, (parts, p)
+            assert count(p.lower) % 2 == 0
+
+
+def test_plan_window_skips_singular_counts():
+    """A counter that reports None (a singular factorization) within 1e-9 of an eigenvalue, as the
+    GPU count does when null-pivot detection fires: the plan must never take such a point, and a
+    goal count between the copies of a double eigenvalue must not pull a cut onto it."""
+    base = np.sort(np.random.default_rng(4).uniform(40.0, 200.0, 20))
+    w = np.repeat(base, 2)
+    seen = []
+
+    def count(s):
+        seen.append(s)
+        if np.abs(w - s).min() < 1e-9 * 200.0:
+            return None
+        return int(np.searchsorted(w, s, side="left"))
+
+    for parts in (2, 3, 5):
+        plan = parallel.plan_window(count, 40.0, 200.0, parts)
+        assert sum(p.count for p in plan) == w.size
+        for p in plan[1:]:
+            assert np.min(np.abs(w - p.lower)) > 1e-6 * 200.0, (parts, p)
+    # a window end on an eigenvalue is moved until its count is regular
+    plan = parallel.plan_window(count, float(base[0]), 200.0, 2)
+    assert plan[0].lower != base[0] and abs(plan[0].lower - base[0]) < 1e-7 * 200.0
+    assert sum(p.count for p in plan) == int(np.searchsorted(w, 200.0)) - int(np.searchsorted(w, plan[0].lower))
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
