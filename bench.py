@@ -11,11 +11,17 @@ certificate passed) of the workload on one GPU:
 * nearest_cube20: the 10 eigenvalues nearest sigma = 25 of the HEP of the 20^3 PEC cube
   (n = 21,660), exact certificate, Krylov seed 0.
 
-value: certified solves/s with the pencil resident in HBM (a Session: device copies and the
-symbolic analysis reused across solves), device-timed. e2e: the same solves through the public
-API hsolve_b200.solve with host scipy matrices (H2D copies, analysis, D2H of the eigenvectors
-inside the timed region). Under torchrun each rank serves its own replica of the workload (no data
-exchange; weak scaling) and rank 0 prints the aggregate.
+value: certified solves/s of the served form with the pencil resident in HBM: the pencil is
+registered with a request server (hsolve_b200.serve.Server) whose workers each keep a session on it
+(device copies, analysis, front plan) and take queued requests continuously, so several certified
+solves share the GPU; a step is one request per worker, device-timed (CUDA events around the whole
+stream). latency_s: p50 / p99 of requests arriving as a seeded Poisson stream. plain_fp64: one
+request at a time with the shifts one after another (batch_shifts off), the baseline of
+vs_plain_fp64; single_request: one request at a time with the shifts batched; mixed_precision: one
+request at a time with the slice operator in FP32 and FP64 refinement. e2e: the served form through
+the public API hsolve_b200.solve with host scipy matrices (H2D copies, analysis lookup, D2H of the
+eigenvectors inside the timed region), one caller per worker. Under torchrun each rank serves its
+own replica of the workload (no data exchange; weak scaling) and rank 0 prints the aggregate.
 """
 from __future__ import annotations
 
@@ -32,6 +38,10 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+
+# concurrent certified solves of the served form (measured: 3 to 6 workers reach the same throughput
+# on the n = 1e5 pencil, and fewer would leave the GPU idle between the latency-bound phases)
+SERVE_WORKERS = 4
 
 WORKLOADS = {
     "interval_box1e5": dict(cells=(44, 34, 26), lengths=(1.0, 0.75, 0.55), form="generalized",
@@ -145,43 +155,73 @@ def run_ours(args, w, rank, world, local):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from hsolve_b200.serve import Server
+
     a, b = build_pencil(w)
     n = a.shape[0]
     cfg = dict(w["config"], device=local)
-    sess = hsolve.Session(a, b, device=local, seed=cfg.get("seed", 2026))
-    for _ in range(args.warmup):
-        res = sess.solve(**w["target"], config=cfg)
-        assert certified(res), res.report
-    lat = []
-    ok = 0
-    rep = None
-    acc = {"factor_ms": 0.0, "factorizations": 0, "solve_ms": 0.0, "solves": 0, "solve_columns": 0,
-           "kernel_launches": 0}
+    workers = SERVE_WORKERS
 
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
 
+    # ---- headline: the served form. The pencil is registered with a request server: each of its
+    # `workers` threads keeps a resident session (device copies, analysis, front plan) and takes the
+    # next queued request as soon as its last one finished, so up to `workers` certified solves share
+    # the GPU at once, each with its window-end counts and slice factorization batched. A step is one
+    # request per worker; every request has its own Krylov start vectors.
+    srv = Server(workers=workers, device=local, config=cfg)
+    h = srv.register(a, b)
+    seed0 = cfg.get("seed", 2026)
+
+    def requests(count, base):
+        return [srv.submit(pencil=h, **w["target"], config={"seed": seed0 + base + i}) for i in range(count)]
+
+    for r in range(args.warmup):
+        for f in requests(workers, 1000 * (r + 1)):
+            assert certified(f.result())
+    n_req = args.steps * workers
     barrier()
+    launches0 = hsolve._native.kernel_launches()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
+        rec0 = len(srv._records)
         start.record()
-        for _ in range(args.steps):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            res = sess.solve(**w["target"], config=cfg)
-            torch.cuda.synchronize()
-            e1.record()
-            torch.cuda.synchronize()
-            lat.append(e0.elapsed_time(e1) / 1e3)
-            ok += int(certified(res))
-            rep = res.report
-            for key in acc:
-                acc[key] += rep["device_timing"][key]
+        futs = requests(n_req, 0)
+        served = [f.result() for f in futs]
+        torch.cuda.synchronize()
         end.record()
         barrier()
     t = start.elapsed_time(end) / 1e3
+    gpu_launches = hsolve._native.kernel_launches() - launches0
+    ok = sum(int(certified(r)) for r in served)
+    queued_lat = [r.end - r.arrival for r in srv._records[rec0:]]
+    # ---- one request at a time on one resident session: the batched path (the single-request
+    # latency and the kernel rooflines below come from these runs) and the plain path
+    sess = hsolve.Session(a, b, device=local, seed=seed0)
+    for _ in range(args.warmup):
+        res = sess.solve(**w["target"], config=cfg)
+        assert certified(res), res.report
+    lat = []
+    rep = None
+    acc = {"factor_ms": 0.0, "factorizations": 0, "solve_ms": 0.0, "solves": 0, "solve_columns": 0,
+           "kernel_launches": 0}
+    barrier()
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = sess.solve(**w["target"], config=cfg)
+        torch.cuda.synchronize()
+        e1.record()
+        torch.cuda.synchronize()
+        lat.append(e0.elapsed_time(e1) / 1e3)
+        assert certified(res), res.report
+        rep = res.report
+        for key in acc:
+            acc[key] += rep["device_timing"][key]
+    single_t = float(np.sum(lat))
     # the plain FP64 GPU path on the same inputs, beside the headline: the window-end counts and
     # the slice factorization one after another on one factorization object (batch_shifts off)
     plain_cfg = dict(cfg, batch_shifts=False)
@@ -223,26 +263,60 @@ def run_ours(args, w, rank, world, local):
         assert certified(res), res.report
         mixed_rep = res.report
     mixed_t = float(np.sum(mixed_lat))
-    # e2e: public API with host matrices (H2D, analysis, solve, D2H)
-    e2e_lat = []
+    # ---- latency under seeded Poisson arrivals at 80 % of the plain path's capacity: the served
+    # form against the plain path serving the same arrivals one request at a time
+    rate = 0.8 * len(plain_lat) / plain_t
+    n_poisson = max(2 * workers, min(4 * workers, int(round(8.0 * rate))))
+    gaps = np.random.default_rng(7 + rank).exponential(1.0 / rate, size=n_poisson)
+
+    def poisson(server, handle):
+        r0 = len(server._records)
+        futs = []
+        for i in range(n_poisson):
+            time.sleep(gaps[i])
+            futs.append(server.submit(pencil=handle, **w["target"], config={"seed": seed0 + 5000 + i}))
+        res_ok = all(certified(f.result()) for f in futs)
+        return [r.end - r.arrival for r in server._records[r0:]], res_ok
+
+    served_p, served_p_ok = poisson(srv, h)
+    srv.close()
+    plain_srv = Server(workers=1, device=local, config=dict(cfg, batch_shifts=False))
+    hp = plain_srv.register(a, b)
+    assert certified(plain_srv.submit(pencil=hp, **w["target"]).result())
+    plain_p, plain_p_ok = poisson(plain_srv, hp)
+    plain_srv.close()
+    # ---- e2e: the served form through the public API, host matrices in and eigenpairs out on
+    # every request (H2D, analysis lookup, solve, D2H), `workers` callers at once
+    from concurrent.futures import ThreadPoolExecutor
+
     h2d = int(a.data.nbytes + a.indices.nbytes + a.indptr.nbytes)
     if b is not None:
         h2d += int(b.data.nbytes + b.indices.nbytes + b.indptr.nbytes)
     d2h = 0
     e2e_steps = max(1, min(args.steps, 3))
-    barrier()
-    for _ in range(e2e_steps):
-        torch.cuda.synchronize()
+    e2e_lat = []
+
+    def call(i):
+        t0 = time.perf_counter()
+        r2 = hsolve.solve(a, b, **w["target"], config=dict(cfg, seed=seed0 + 9000 + i))
+        return time.perf_counter() - t0, r2
+
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        for r2 in pool.map(lambda i: call(i)[1], range(workers)):  # warm: every caller thread once
+            assert certified(r2)
+        barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        r2 = hsolve.solve(a, b, **w["target"], config=cfg)
+        outs = list(pool.map(call, range(e2e_steps * workers)))
         torch.cuda.synchronize()
         e1.record()
         torch.cuda.synchronize()
+    for dt_i, r2 in outs:
         assert certified(r2)
-        e2e_lat.append(e0.elapsed_time(e1) / 1e3)
+        e2e_lat.append(dt_i)
         d2h = int(r2.eigenvectors.nbytes + r2.eigenvalues.nbytes)
-    e2e_t = float(np.sum(e2e_lat))
+    e2e_t = e0.elapsed_time(e1) / 1e3
+    e2e_n = len(outs)
     # a cold first call: the process-wide analysis cache emptied, so the call orders and analyses
     # the pattern as hsolve's hs::solve does on every call
     hsolve._native.clear_analysis_cache()
@@ -254,8 +328,8 @@ def run_ours(args, w, rank, world, local):
     assert certified(r2)
     cold_analysis_s = r2.report["factor_stats"]["analyze_s"]
     if dist is not None:
-        (t, e2e_t, plain_t, mixed_t), (ok_total,) = reduce_over_ranks(dist, [t, e2e_t, plain_t, mixed_t], [ok],
-                                                                       "cuda")
+        (t, e2e_t, plain_t, mixed_t, single_t), (ok_total,) = reduce_over_ranks(
+            dist, [t, e2e_t, plain_t, mixed_t, single_t], [ok], "cuda")
         ok_total = int(ok_total)
         dist.barrier()
         dist.destroy_process_group()
@@ -301,25 +375,44 @@ def run_ours(args, w, rank, world, local):
         "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": 1e3 * t / args.steps,
+        "requests_per_step": workers,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (Yee/FIT generator, exact spectrum known)",
         "config": {"workload": args.workload, "n": int(n), "target": w["target"],
-                   "path": "batched shifts: window-end inertia counts and the slice factorization at once "
-                           "on three factorization objects sharing one analysis; FP64",
+                   "path": f"served: the pencil registered with a request server, {workers} workers with a "
+                           "resident session each take queued requests continuously (up to "
+                           f"{workers} certified solves at once), each request batching its window-end "
+                           "inertia counts and slice factorization on three factorization objects; FP64",
+                   "step": f"{workers} requests (one per worker), each a whole certified solve with its own "
+                           "Krylov start vectors",
+                   "requests_timed": n_req,
                    "l2": "inputs larger than L2 (factor storage > 126 MB)" if n > 50000 else "L2 flushed by factorization",
                    "parallelism": f"replicas x{world}"},
-        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "latency_s": {"p50": float(np.percentile(served_p, 50)), "p99": float(np.percentile(served_p, 99)),
+                      "arrivals": f"seeded Poisson, {rate:.2f} requests/s (0.8 x the plain path's capacity), "
+                                  f"{n_poisson} requests",
+                      "queued_p50": float(np.percentile(queued_lat, 50)),
+                      "queued_p99": float(np.percentile(queued_lat, 99)), "all_certified": bool(served_p_ok)},
         "clocks": clocks.summary(),
-        "e2e": {"value": world * e2e_steps / e2e_t, "unit": "certified solves/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "latency_p50_s": float(np.percentile(e2e_lat, 50)),
-                "analysis": "cached per pattern after the first call (process-wide analysis cache)",
+        "e2e": {"value": world * e2e_n / e2e_t, "unit": "certified solves/s", "h2d_bytes_per_step": h2d * workers,
+                "d2h_bytes_per_step": d2h * workers, "latency_p50_s": float(np.percentile(e2e_lat, 50)),
+                "path": f"hsolve_b200.solve with host CSR matrices, {workers} callers at once",
+                "analysis": "cached per pattern after the first call (process-wide analysis and plan cache)",
                 "cold_first_call_s": cold_s, "cold_first_call_analysis_s": cold_analysis_s},
+        "single_request": {"value": world * len(lat) / single_t, "unit": "certified solves/s",
+                           "ms_per_step": 1e3 * single_t / len(lat), "steps": len(lat),
+                           "latency_p50_s": float(np.percentile(lat, 50)),
+                           "latency_p99_s": float(np.percentile(lat, 99)),
+                           "path": "one request at a time on a resident session, batched shifts"},
         "plain_fp64": {"value": world * len(plain_lat) / plain_t, "unit": "certified solves/s",
                        "ms_per_step": 1e3 * plain_t / len(plain_lat), "steps": len(plain_lat),
-                       "path": "shifts one after another on one factorization object (batch_shifts off)"},
+                       "latency_p50_s": float(np.percentile(plain_p, 50)),
+                       "latency_p99_s": float(np.percentile(plain_p, 99)), "latency_all_certified": bool(plain_p_ok),
+                       "path": "one request at a time, shifts one after another on one factorization object "
+                               "(batch_shifts off); latency under the same Poisson arrivals"},
         "vs_plain_fp64": (ok_total / t) / (world * len(plain_lat) / plain_t),
         "mixed_precision": {"value": world * len(mixed_lat) / mixed_t, "unit": "certified solves/s",
                             "ms_per_step": 1e3 * mixed_t / len(mixed_lat), "steps": len(mixed_lat),
@@ -327,7 +420,7 @@ def run_ours(args, w, rank, world, local):
                             "precision": mixed_rep["precision"],
                             "path": "slice operator factorized in FP32 with FP64 refinement of every application; "
                                     "FP64 window-end counts; batched shifts"},
-        "gpu_launches": int(acc["kernel_launches"]),
+        "gpu_launches": int(gpu_launches),
         "roofline": dominant,
         "roofline_secondary": other,
         "device_time_split_s": {"factorizations": fac_s / args.steps, "solves": sol_s / args.steps},

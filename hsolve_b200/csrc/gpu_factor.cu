@@ -24,12 +24,15 @@ namespace {
 // seed (a hit is confirmed by comparing the whole pattern): repeated solves on one sparsity
 // pattern (new values, new shifts, new Bloch wavevectors) skip the ordering and the symbolic
 // factorization. It holds the analysis as computed, before any delayed-pivot re-plan.
+// Beside each analysis it keeps the front plan built from it on each device (FrontPlan), so that a
+// new factorization object on a known pattern neither builds nor uploads a plan.
 struct AnalysisEntry {
   std::uint64_t key;
   std::uint64_t seed;
   std::vector<std::int64_t> rp;
   std::vector<std::int32_t> ci;
   std::shared_ptr<const Symbolic> sym;
+  std::vector<std::shared_ptr<const FrontPlan>> plans;  // at most one per device
 };
 
 constexpr std::size_t kAnalysisCacheEntries = 8;
@@ -47,26 +50,48 @@ std::uint64_t pattern_key(const std::vector<std::int64_t>& rp, const std::vector
   return h;
 }
 
-Symbolic cached_analysis(std::int64_t n, const std::vector<std::int64_t>& rp, const std::vector<std::int32_t>& ci,
-                         const SymbolicOptions& so) {
+// The analysis of the pattern (rp, ci) from the cache, or computed and cached; `hit` tells which,
+// and `plan` receives the cached front plan of `device` (null if none).
+std::shared_ptr<const Symbolic> cached_analysis(std::int64_t n, const std::vector<std::int64_t>& rp,
+                                                const std::vector<std::int32_t>& ci, const SymbolicOptions& so,
+                                                int device, std::shared_ptr<const FrontPlan>& plan, bool& hit) {
   const std::uint64_t key = pattern_key(rp, ci, so.ordering.seed);
+  plan.reset();
+  hit = false;
   {
     std::lock_guard<std::mutex> lk(g_analysis_mu);
     for (auto it = g_analysis_cache.begin(); it != g_analysis_cache.end(); ++it) {
       if (it->key == key && it->seed == so.ordering.seed && it->rp == rp && it->ci == ci) {
         g_analysis_cache.splice(g_analysis_cache.begin(), g_analysis_cache, it);
-        Symbolic s = *g_analysis_cache.front().sym;
-        s.ordering_seconds = 0.0;
-        s.symbolic_seconds = 0.0;
-        return s;
+        const AnalysisEntry& e = g_analysis_cache.front();
+        for (const auto& pl : e.plans)
+          if (pl->device == device) plan = pl;
+        hit = true;
+        return e.sym;
       }
     }
   }
-  Symbolic s = analyze_pattern(n, rp.data(), ci.data(), nullptr, so);
+  auto s = std::make_shared<const Symbolic>(analyze_pattern(n, rp.data(), ci.data(), nullptr, so));
   std::lock_guard<std::mutex> lk(g_analysis_mu);
-  g_analysis_cache.push_front(AnalysisEntry{key, so.ordering.seed, rp, ci, std::make_shared<const Symbolic>(s)});
+  g_analysis_cache.push_front(AnalysisEntry{key, so.ordering.seed, rp, ci, s, {}});
   if (g_analysis_cache.size() > kAnalysisCacheEntries) g_analysis_cache.pop_back();
   return s;
+}
+
+// Keeps `plan` (built from the cached analysis `origin`) with that cache entry, if it still holds
+// `origin`.
+void remember_plan(const std::shared_ptr<const Symbolic>& origin, const std::shared_ptr<const FrontPlan>& plan) {
+  std::lock_guard<std::mutex> lk(g_analysis_mu);
+  for (auto& e : g_analysis_cache)
+    if (e.sym == origin) {
+      for (auto& pl : e.plans)
+        if (pl->device == plan->device) {
+          pl = plan;
+          return;
+        }
+      e.plans.push_back(plan);
+      return;
+    }
 }
 
 // A factorization that had to move delayed pivots to their parent fronts leaves its analysis with
@@ -78,7 +103,10 @@ void learn_delays(const std::vector<std::int64_t>& rp, const std::vector<std::in
   std::lock_guard<std::mutex> lk(g_analysis_mu);
   for (auto& e : g_analysis_cache)
     if (e.key == key && e.seed == seed && e.rp == rp && e.ci == ci) {
-      if (sym.delayed_moves > e.sym->delayed_moves) e.sym = std::make_shared<const Symbolic>(sym);
+      if (sym.delayed_moves > e.sym->delayed_moves) {
+        e.sym = std::make_shared<const Symbolic>(sym);
+        e.plans.clear();  // they belong to the structure before the moves
+      }
       return;
     }
 }
@@ -204,17 +232,23 @@ void GpuFactor::analyze(std::int64_t n, const std::int64_t* a_rp, const std::int
   }
   SymbolicOptions so;
   so.ordering.seed = opt_.ordering_seed;
+  std::shared_ptr<const FrontPlan> known_plan;
   if (order) {
     sym_ = analyze_pattern(n, rp_.data(), ci_.data(), perm.data(), so);
+    sym_origin_.reset();
   } else {
-    sym_ = cached_analysis(n, rp_, ci_, so);
+    bool hit = false;
+    sym_origin_ = cached_analysis(n, rp_, ci_, so, opt_.device, known_plan, hit);
+    sym_ = *sym_origin_;
+    if (hit) {
+      sym_.ordering_seconds = 0.0;
+      sym_.symbolic_seconds = 0.0;
+    }
   }
   cached_analysis_ = order == nullptr;
   row_.resize(nnz_);
   for (std::int64_t i = 0; i < n; ++i)
     for (std::int64_t p = rp_[i]; p < rp_[i + 1]; ++p) row_[p] = static_cast<std::int32_t>(i);
-  d_row_.upload(row_, stream_);
-  d_col_.upload(ci_, stream_);
   d_a_.upload(av, stream_);
   d_b_.upload(bv, stream_);
   d_scale_.alloc(n);
@@ -223,7 +257,16 @@ void GpuFactor::analyze(std::int64_t n, const std::int64_t* a_rp, const std::int
   d_failed_.alloc(static_cast<std::size_t>(n));
   d_piv_.alloc(n);
   d_pidx_.alloc(n);
-  build_plan();
+  if (known_plan) {
+    plan_ = known_plan;
+  } else {
+    plan_ = make_plan();
+    // the uploads ran on this object's stream: complete them before another object (on another
+    // stream, possibly another thread) can take the plan from the cache
+    cuda_check(cudaStreamSynchronize(stream_), "plan upload");
+    if (sym_origin_) remember_plan(sym_origin_, plan_);
+  }
+  alloc_work();
   cuda_check(cudaStreamSynchronize(stream_), "analyze");
   inertia_ = hsg_inertia_t{-1, -1, -1, 0, 0, 0, 0, 0};
   analysed_ = true;
@@ -241,14 +284,12 @@ void GpuFactor::analyze_like(const GpuFactor& src) {
   ci_ = src.ci_;
   row_ = src.row_;
   sym_ = src.sym_;
+  sym_origin_ = src.sym_origin_;
+  plan_ = src.plan_;  // shared: the plan is immutable
   cached_analysis_ = src.cached_analysis_;
   cuda_check(cudaStreamSynchronize(src.stream_), "analyze_like: source");
-  d_row_.alloc(src.d_row_.n);
-  d_col_.alloc(src.d_col_.n);
   d_a_.alloc(src.d_a_.n);
   d_b_.alloc(std::max<std::size_t>(1, src.d_b_.n));
-  cuda_check(cudaMemcpyAsync(d_row_.p, src.d_row_.p, src.d_row_.n * sizeof(std::int32_t), cudaMemcpyDeviceToDevice, stream_), "copy");
-  cuda_check(cudaMemcpyAsync(d_col_.p, src.d_col_.p, src.d_col_.n * sizeof(std::int32_t), cudaMemcpyDeviceToDevice, stream_), "copy");
   cuda_check(cudaMemcpyAsync(d_a_.p, src.d_a_.p, src.d_a_.n * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy");
   if (src.d_b_.n) cuda_check(cudaMemcpyAsync(d_b_.p, src.d_b_.p, src.d_b_.n * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy");
   d_scale_.alloc(n_);
@@ -257,14 +298,19 @@ void GpuFactor::analyze_like(const GpuFactor& src) {
   d_failed_.alloc(static_cast<std::size_t>(n_));
   d_piv_.alloc(n_);
   d_pidx_.alloc(n_);
-  build_plan();
+  alloc_work();
   cuda_check(cudaStreamSynchronize(stream_), "analyze_like");
   inertia_ = hsg_inertia_t{-1, -1, -1, 0, 0, 0, 0, 0};
   analysed_ = true;
 }
 
-void GpuFactor::build_plan() {
+std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
   const Symbolic& S = sym_;
+  auto plan = std::make_shared<FrontPlan>();
+  FrontPlan& P = *plan;
+  P.device = opt_.device;
+  P.row.upload(row_, stream_);
+  P.col.upload(ci_, stream_);
   const std::int32_t ns = S.ns;
   std::vector<SnDev> sn(ns);
   std::int64_t vec = 0, inv_total = 0;
@@ -286,7 +332,7 @@ void GpuFactor::build_plan() {
     d.cptr_off = -1;
     inv_total += static_cast<std::int64_t>((d.k + 30) / 31 + 1) * 1024;
   }
-  vec_total_ = vec;
+  P.vec_total = vec;
   {
     // per pivot: panel index of its diagonal entry and its front's first column
     std::vector<std::int64_t> dpos(n_);
@@ -296,8 +342,8 @@ void GpuFactor::build_plan() {
         dpos[sn[q].first + j] = sn[q].panel_off + j + static_cast<std::int64_t>(j) * sn[q].m;
         pfirst[sn[q].first + j] = sn[q].first;
       }
-    d_dpos_.upload(dpos, stream_);
-    d_pfirst_.upload(pfirst, stream_);
+    P.dpos.upload(dpos, stream_);
+    P.pfirst.upload(pfirst, stream_);
   }
   if (coop_max_ == 0) coop_max_ = coop_max_ctas(opt_.device);
   if (solve_coop_max_ == 0) solve_coop_max_ = solve_coop_max_ctas(opt_.device);
@@ -309,13 +355,12 @@ void GpuFactor::build_plan() {
   std::vector<std::int32_t> cptr;
   std::vector<ContribEntry> cent;
   int cnt_total = 0;
-  ncoop_ = 0;
   std::vector<std::int32_t> lists;
   std::vector<int2> items;
-  levels_.assign(S.nlevels, LevelPlan{});
+  P.levels.assign(S.nlevels, LevelPlan{});
   std::int64_t scratch_max = 0;
   for (std::int32_t l = 0; l < S.nlevels; ++l) {
-    LevelPlan& L = levels_[l];
+    LevelPlan& L = P.levels[l];
     std::vector<std::int32_t> zero, s32, s64, app, all;
     std::int64_t maxcb = 0, scratch = 0;
     int maxm = 0;
@@ -462,7 +507,7 @@ void GpuFactor::build_plan() {
         plan_ctas(coop_max_, L.cta_off, L.coop_ctas);
         L.coop_shared = static_cast<int>(app.size()) <= shared_max;
         if (L.coop_shared) plan_ctas(shared_max, L.cta_off_shared, L.coop_ctas_shared);
-        L.done_slot = ncoop_++;
+        L.done_slot = P.ncoop++;
       }
     }
     L.maxm = maxm;
@@ -492,7 +537,7 @@ void GpuFactor::build_plan() {
     // reuses it), and the pencil's entries grouped by the level of the front they scatter into
     std::vector<SnDev> snc = sn;
     std::vector<std::int32_t> level_of(ns, 0);
-    arena_entries_ = 1;
+    P.arena_entries = 1;
     for (std::int32_t l = 0; l < S.nlevels; ++l) {
       std::int64_t off = 0;
       for (std::int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
@@ -501,8 +546,8 @@ void GpuFactor::build_plan() {
         snc[s].panel_off = off;
         off += static_cast<std::int64_t>(sn[s].m) * sn[s].k;
       }
-      levels_[l].arena_used = off;
-      arena_entries_ = std::max(arena_entries_, off);
+      P.levels[l].arena_used = off;
+      P.arena_entries = std::max(P.arena_entries, off);
     }
     std::vector<std::int64_t> dest_cnt(nnz_), lcount(S.nlevels + 1, 0);
     std::vector<std::int32_t> ent_level(nnz_);
@@ -519,26 +564,45 @@ void GpuFactor::build_plan() {
     std::vector<std::int64_t> fill(lcount.begin(), lcount.end() - 1);
     for (std::int64_t p = 0; p < nnz_; ++p) ent_idx[fill[ent_level[p]]++] = p;
     for (std::int32_t l = 0; l < S.nlevels; ++l) {
-      levels_[l].ent_off = lcount[l];
-      levels_[l].ent_n = lcount[l + 1] - lcount[l];
+      P.levels[l].ent_off = lcount[l];
+      P.levels[l].ent_n = lcount[l + 1] - lcount[l];
     }
-    d_sn_cnt_.upload(snc, stream_);
-    d_dest_cnt_.upload(dest_cnt, stream_);
-    d_ent_idx_.upload(ent_idx, stream_);
+    P.sn_cnt.upload(snc, stream_);
+    P.dest_cnt.upload(dest_cnt, stream_);
+    P.ent_idx.upload(ent_idx, stream_);
   }
-  d_sn_.upload(sn, stream_);
-  d_lists_.upload(lists, stream_);
-  d_items_.upload(items, stream_);
-  d_rmap_.upload(S.rmap, stream_);
-  d_rows_.upload(rows, stream_);
-  d_child_ptr_.upload(S.child_ptr, stream_);
-  d_children_.upload(S.children, stream_);
-  d_iperm_.upload(S.iperm, stream_);
-  d_dest_.upload(S.dest, stream_);
-  const std::size_t fe = static_cast<std::size_t>(std::max<std::int64_t>(1, S.factor_entries));
-  const std::size_t cbe = static_cast<std::size_t>(std::max<std::int64_t>(1, S.cb_arena));
-  const std::size_t inve = static_cast<std::size_t>(std::max<std::int64_t>(1, inv_total));
-  const std::size_t we = static_cast<std::size_t>(std::max<std::int64_t>(1, w_total));
+  P.sn.upload(sn, stream_);
+  P.lists.upload(lists, stream_);
+  P.items.upload(items, stream_);
+  P.rmap.upload(S.rmap, stream_);
+  P.rows.upload(rows, stream_);
+  P.child_ptr.upload(S.child_ptr, stream_);
+  P.children.upload(S.children, stream_);
+  P.iperm.upload(S.iperm, stream_);
+  P.dest.upload(S.dest, stream_);
+  P.work_off.upload(work_offs, stream_);
+  P.cptr.upload(cptr, stream_);
+  P.cent.upload(cent, stream_);
+  P.sweep_cnt_total = cnt_total;
+  P.sbl.upload(sbl, stream_);
+  P.tiles.upload(tiles, stream_);
+  P.nsbl = static_cast<int>(sbl.size());
+  P.ntiles = static_cast<int>(tiles.size());
+  P.scratch_max = scratch_max;
+  P.work_max = work_max;
+  P.w_total = w_total;
+  P.inv_total = inv_total;
+  for (std::int32_t s = 0; s < ns; ++s)
+    HSG_REQUIRE((sn[s].k + 30) / 31 <= kMaxBlocksPerFront, HSG_UNSUPPORTED, "front with " << sn[s].k << " pivots exceeds the solve block table");
+  return plan;
+}
+
+void GpuFactor::alloc_work() {
+  const FrontPlan& P = *plan_;
+  const std::size_t fe = static_cast<std::size_t>(std::max<std::int64_t>(1, sym_.factor_entries));
+  const std::size_t cbe = static_cast<std::size_t>(std::max<std::int64_t>(1, sym_.cb_arena));
+  const std::size_t inve = static_cast<std::size_t>(std::max<std::int64_t>(1, P.inv_total));
+  const std::size_t we = static_cast<std::size_t>(std::max<std::int64_t>(1, P.w_total));
   if (single()) {
     d_panels_f_.alloc(fe);
     d_cb_f_.alloc(cbe);
@@ -550,24 +614,20 @@ void GpuFactor::build_plan() {
     d_inv_.alloc(inve);
     d_w_.alloc(we);
   }
-  d_scratch_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, scratch_max)));
-  d_level_done_.alloc(static_cast<std::size_t>(std::max(1, ncoop_)));
-  d_work_off_.upload(work_offs, stream_);
-  d_work_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, work_max)));
+  d_scratch_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, P.scratch_max)));
+  d_level_done_.alloc(static_cast<std::size_t>(std::max(1, P.ncoop)));
+  d_work_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, P.work_max)));
   d_err_.alloc(1);
-  d_cptr_.upload(cptr, stream_);
-  d_cent_.upload(cent, stream_);
-  d_sweep_cnt_.alloc(static_cast<std::size_t>(std::max(1, 2 * cnt_total)));
-  sweep_cnt_total_ = cnt_total;
-  d_sbl_.upload(sbl, stream_);
-  d_tiles_.upload(tiles, stream_);
-  nsbl_ = static_cast<int>(sbl.size());
-  ntiles_ = static_cast<int>(tiles.size());
+  d_sweep_cnt_.alloc(static_cast<std::size_t>(std::max(1, 2 * P.sweep_cnt_total)));
   w_ready_ = false;
   d_blk_.alloc(static_cast<std::size_t>(n_));
-  d_nblk_.alloc(static_cast<std::size_t>(std::max(1, ns)));
-  for (std::int32_t s = 0; s < ns; ++s)
-    HSG_REQUIRE((sn[s].k + 30) / 31 <= kMaxBlocksPerFront, HSG_UNSUPPORTED, "front with " << sn[s].k << " pivots exceeds the solve block table");
+  d_nblk_.alloc(static_cast<std::size_t>(std::max(1, sym_.ns)));
+}
+
+void GpuFactor::build_plan() {
+  plan_ = make_plan();
+  sym_origin_.reset();
+  alloc_work();
 }
 
 template <> double* GpuFactor::panels_of<double>() { return d_panels_.p; }
@@ -594,12 +654,12 @@ void GpuFactor::run_numeric_t(double alpha, double beta, bool detection, bool co
   cudaStream_t s = stream_;
   R* panels = panels_of<R>();
   R* cb = cb_of<R>();
-  const SnDev* sn = d_sn_.p;
+  const SnDev* sn = plan_->sn.p;
   if (count_only) {
     // the level's panels live in the arena; entries are scattered level by level below
-    if constexpr (sizeof(R) == 8) { d_arena_.alloc(static_cast<std::size_t>(arena_entries_)); panels = reinterpret_cast<R*>(d_arena_.p); }
-    else { d_arena_f_.alloc(static_cast<std::size_t>(arena_entries_)); panels = reinterpret_cast<R*>(d_arena_f_.p); }
-    sn = d_sn_cnt_.p;
+    if constexpr (sizeof(R) == 8) { d_arena_.alloc(static_cast<std::size_t>(plan_->arena_entries)); panels = reinterpret_cast<R*>(d_arena_.p); }
+    else { d_arena_f_.alloc(static_cast<std::size_t>(plan_->arena_entries)); panels = reinterpret_cast<R*>(d_arena_f_.p); }
+    sn = plan_->sn_cnt.p;
   }
   cuda_check(cudaMemsetAsync(d_cnt_.p, 0, sizeof(FactorCounters), s), "memset counters");
   cuda_check(cudaMemsetAsync(d_level_done_.p, 0, d_level_done_.n * sizeof(int), s), "memset level flags");
@@ -607,15 +667,15 @@ void GpuFactor::run_numeric_t(double alpha, double beta, bool detection, bool co
   if (opt_.scaling) {
     cuda_check(cudaMemsetAsync(d_r_.p, 0, n_ * sizeof(unsigned long long), s), "memset r");
     for (int it = 0; it < 10; ++it) {
-      launch_scale_rowmax(nnz_, d_row_.p, d_col_.p, d_a_.p, d_b_.p, alpha, beta, d_scale_.p, d_r_.p, s);
+      launch_scale_rowmax(nnz_, plan_->row.p, plan_->col.p, d_a_.p, d_b_.p, alpha, beta, d_scale_.p, d_r_.p, s);
       launch_scale_update(n_, d_scale_.p, d_r_.p, s);
     }
   }
   if (count_only) {
-    launch_amax(nnz_, d_row_.p, d_col_.p, d_a_.p, d_b_.p, alpha, beta, d_scale_.p, d_cnt_.p, s);
+    launch_amax(nnz_, plan_->row.p, plan_->col.p, d_a_.p, d_b_.p, alpha, beta, d_scale_.p, d_cnt_.p, s);
   } else {
     cuda_check(cudaMemsetAsync(panels, 0, sym_.factor_entries * sizeof(R), s), "memset panels");
-    launch_scatter<R>(nnz_, d_row_.p, d_col_.p, d_a_.p, d_b_.p, alpha, beta, d_scale_.p, d_dest_.p, panels, d_cnt_.p, s);
+    launch_scatter<R>(nnz_, plan_->row.p, plan_->col.p, d_a_.p, d_b_.p, alpha, beta, d_scale_.p, plan_->dest.p, panels, d_cnt_.p, s);
   }
   FactorParams prm;
   prm.u = opt_.pivot_threshold;
@@ -624,15 +684,15 @@ void GpuFactor::run_numeric_t(double alpha, double beta, bool detection, bool co
   prm.null_tol = detection ? (single() ? opt_.single_null_pivot_tol : opt_.null_pivot_tol) : 0.0;
   prm.cnt = d_cnt_.p;
   prm.failed_cap = static_cast<std::int32_t>(n_);
-  const std::int32_t* lists = d_lists_.p;
-  for (const LevelPlan& L : levels_) {
+  const std::int32_t* lists = plan_->lists.p;
+  for (const LevelPlan& L : plan_->levels) {
     if (count_only) {
       cuda_check(cudaMemsetAsync(panels, 0, static_cast<std::size_t>(L.arena_used) * sizeof(R), s), "memset arena");
-      launch_scatter_list<R>(d_ent_idx_.p + L.ent_off, L.ent_n, d_row_.p, d_col_.p, d_a_.p, d_b_.p, alpha, beta,
-                             d_scale_.p, d_dest_cnt_.p, panels, s);
+      launch_scatter_list<R>(plan_->ent_idx.p + L.ent_off, L.ent_n, plan_->row.p, plan_->col.p, d_a_.p, d_b_.p, alpha, beta,
+                             d_scale_.p, plan_->dest_cnt.p, panels, s);
     }
     launch_zero_cb<R>(lists + L.zero_off, L.zero_n, L.zero_chunks, sn, cb, s);
-    for (const auto& ea : L.ea) launch_extend_add<R>(d_items_.p + ea.first, ea.second, sn, d_rmap_.p, panels, cb, s);
+    for (const auto& ea : L.ea) launch_extend_add<R>(plan_->items.p + ea.first, ea.second, sn, plan_->rmap.p, panels, cb, s);
     launch_front_small<R>(32, lists + L.s32_off, L.s32_n, sn, panels, cb, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
     launch_front_small<R>(kSmallMax, lists + L.s64_off, L.s64_n, sn, panels, cb, d_piv_.p, d_pidx_.p, prm, d_cnt_.p, d_failed_.p, s);
     if (shared_ ? L.coop_shared : L.coop) {
@@ -722,7 +782,7 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
   cudaStream_t s = stream_;
   const int nr = static_cast<int>(nrhs);
   d_xwork_.alloc(static_cast<std::size_t>(n_) * nr);
-  d_vec_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, vec_total_)) * nr);
+  d_vec_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, plan_->vec_total)) * nr);
   double* db = b;
   std::int64_t ld = ldb;
   if (!on_device) {
@@ -735,9 +795,9 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
   cuda_check(cudaMemsetAsync(d_err_.p, 0, sizeof(int), s), "reset solve status");
   cuda_check(cudaEventRecord(ev0_, s), "event");
   build_solve_operator();
-  launch_gather_scale(n_, nr, db, ld, d_scale_.p, d_iperm_.p, d_xwork_.p, s);
+  launch_gather_scale(n_, nr, db, ld, d_scale_.p, plan_->iperm.p, d_xwork_.p, s);
   run_sweeps(d_xwork_.p, d_vec_.p, nr);
-  launch_scatter_scale(n_, nr, db, ld, d_scale_.p, d_iperm_.p, d_xwork_.p, s);
+  launch_scatter_scale(n_, nr, db, ld, d_scale_.p, plan_->iperm.p, d_xwork_.p, s);
   cuda_check(cudaEventRecord(ev1_, s), "event");
   cuda_check(cudaGetLastError(), "solve launch");
   if (!on_device) {
@@ -760,7 +820,7 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
 
 std::size_t GpuFactor::solve_scratch_doubles(std::int64_t nrhs) const {
   const std::int64_t nc = std::min<std::int64_t>(8, nrhs);
-  return static_cast<std::size_t>(n_ * nrhs + std::max<std::int64_t>(1, vec_total_) * nc);
+  return static_cast<std::size_t>(n_ * nrhs + std::max<std::int64_t>(1, plan_->vec_total) * nc);
 }
 
 void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ldb, double* scratch,
@@ -780,9 +840,9 @@ void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ld
   double* vec = scratch + static_cast<std::size_t>(n_) * nr;
   cuda_check(cudaMemsetAsync(d_err_.p, 0, sizeof(int), s), "reset solve status");
   build_solve_operator();
-  launch_gather_scale(n_, nr, b, ldb, d_scale_.p, d_iperm_.p, xwork, s);
+  launch_gather_scale(n_, nr, b, ldb, d_scale_.p, plan_->iperm.p, xwork, s);
   run_sweeps(xwork, vec, nr);
-  launch_scatter_scale(n_, nr, b, ldb, d_scale_.p, d_iperm_.p, xwork, s);
+  launch_scatter_scale(n_, nr, b, ldb, d_scale_.p, plan_->iperm.p, xwork, s);
   cuda_check(cudaGetLastError(), "solve launch");
   int err = 0;
   cuda_check(cudaMemcpyAsync(&err, d_err_.p, sizeof(int), cudaMemcpyDeviceToHost, s), "solve status");
@@ -801,33 +861,33 @@ void GpuFactor::run_sweeps_t(double* xwork, double* vec, int nr) {
   const F* panels = panels_of<F>();
   const F* W = w_of<F>();
   const F* inv = inv_of<F>();
-  const std::int32_t* lists = d_lists_.p;
+  const std::int32_t* lists = plan_->lists.p;
   // chunks of at most 8 right-hand sides (the cooperative sweeps carry 8)
   for (int c0 = 0; c0 < nr; c0 += 8) {
     const int nc = std::min(8, nr - c0);
     double* xw = xwork + static_cast<std::int64_t>(c0) * n_;
     cuda_check(cudaMemsetAsync(d_sweep_cnt_.p, 0, d_sweep_cnt_.n * sizeof(int), s), "reset sweep counters");
-    for (const LevelPlan& L : levels_) {
+    for (const LevelPlan& L : plan_->levels) {
       if (L.solve_coop) {
-        cuda_check(launch_solve_fwd_coop<F>(lists + L.all_off, lists + L.solve_cta_off, L.all_n, L.solve_ctas, d_sn_.p,
-                                            d_cptr_.p, d_cent_.p, W, d_pidx_.p, xw, n_, vec, nc, d_work_.p,
-                                            d_work_off_.p + L.work_off_off, d_sweep_cnt_.p + L.cnt_off, d_err_.p, s),
+        cuda_check(launch_solve_fwd_coop<F>(lists + L.all_off, lists + L.solve_cta_off, L.all_n, L.solve_ctas, plan_->sn.p,
+                                            plan_->cptr.p, plan_->cent.p, W, d_pidx_.p, xw, n_, vec, nc, d_work_.p,
+                                            plan_->work_off.p + L.work_off_off, d_sweep_cnt_.p + L.cnt_off, d_err_.p, s),
                    "cooperative forward solve");
       } else {
-        launch_solve_fwd<F>(lists + L.all_off, L.all_n, L.maxm, d_sn_.p, d_child_ptr_.p, d_children_.p, d_rmap_.p,
+        launch_solve_fwd<F>(lists + L.all_off, L.all_n, L.maxm, plan_->sn.p, plan_->child_ptr.p, plan_->children.p, plan_->rmap.p,
                             panels, d_piv_.p, d_pidx_.p, d_blk_.p, d_nblk_.p, inv, xw, n_, vec, nc, s);
       }
     }
-    launch_solve_diag_flat<F>(n_, d_dpos_.p, d_pfirst_.p, panels, d_piv_.p, d_pidx_.p, xw, n_, nc, s);
-    for (auto it = levels_.rbegin(); it != levels_.rend(); ++it) {
+    launch_solve_diag_flat<F>(n_, plan_->dpos.p, plan_->pfirst.p, panels, d_piv_.p, d_pidx_.p, xw, n_, nc, s);
+    for (auto it = plan_->levels.rbegin(); it != plan_->levels.rend(); ++it) {
       if (it->solve_coop) {
         cuda_check(launch_solve_bwd_coop<F>(lists + it->all_off, lists + it->solve_cta_off, it->all_n, it->solve_ctas,
-                                            d_sn_.p, d_rows_.p, W, d_pidx_.p, xw, n_, nc, d_work_.p,
-                                            d_work_off_.p + it->work_off_off,
-                                            d_sweep_cnt_.p + sweep_cnt_total_ + it->cnt_off, d_err_.p, s),
+                                            plan_->sn.p, plan_->rows.p, W, d_pidx_.p, xw, n_, nc, d_work_.p,
+                                            plan_->work_off.p + it->work_off_off,
+                                            d_sweep_cnt_.p + plan_->sweep_cnt_total + it->cnt_off, d_err_.p, s),
                    "cooperative backward solve");
       } else {
-        launch_solve_bwd<F>(lists + it->all_off, it->all_n, it->maxm, d_sn_.p, d_rows_.p, panels, d_pidx_.p, d_blk_.p,
+        launch_solve_bwd<F>(lists + it->all_off, it->all_n, it->maxm, plan_->sn.p, plan_->rows.p, panels, d_pidx_.p, d_blk_.p,
                             d_nblk_.p, inv, xw, n_, nc, s);
       }
     }
@@ -843,8 +903,8 @@ void GpuFactor::build_solve_operator() {
 
 template <class F>
 void GpuFactor::build_solve_operator_t() {
-  launch_inv_blocks<F>(sym_.ns, d_sn_.p, panels_of<F>(), d_piv_.p, d_blk_.p, d_nblk_.p, inv_of<F>(), stream_);
-  launch_sb_build<F>(d_sbl_.p, nsbl_, d_tiles_.p, ntiles_, d_sn_.p, panels_of<F>(), d_piv_.p, w_of<F>(), stream_);
+  launch_inv_blocks<F>(sym_.ns, plan_->sn.p, panels_of<F>(), d_piv_.p, d_blk_.p, d_nblk_.p, inv_of<F>(), stream_);
+  launch_sb_build<F>(plan_->sbl.p, plan_->nsbl, plan_->tiles.p, plan_->ntiles, plan_->sn.p, panels_of<F>(), d_piv_.p, w_of<F>(), stream_);
 }
 
 void GpuFactor::release() {

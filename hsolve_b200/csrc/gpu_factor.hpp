@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -64,6 +65,55 @@ struct DevBuf {
   }
 };
 
+// Launch plan of one tree level of the fronts (built with the FrontPlan).
+struct LevelPlan {
+  std::int64_t zero_off = 0; int zero_n = 0; int zero_chunks = 1;
+  std::int64_t s32_off = 0; int s32_n = 0;
+  std::int64_t s64_off = 0; int s64_n = 0;
+  std::int64_t app_off = 0; int app_n = 0;
+  bool coop = false;                 // large fronts: one cooperative launch, CTAs split by work
+  std::int64_t cta_off = 0; int coop_ctas = 0; int done_slot = 0;
+  std::int64_t all_off = 0; int all_n = 0; int maxm = 0;
+  std::vector<std::pair<std::int64_t, int>> ea;  // (offset into items, count) per child rank
+  bool solve_coop = false;           // few fronts: cooperative sweeps, CTAs split by panel size
+  std::int64_t solve_cta_off = 0; int solve_ctas = 0; int solve_steps = 0;
+  std::int64_t work_off_off = 0;     // offsets of the fronts' work vectors (index into FrontPlan::work_off)
+  bool coop_shared = false;          // the level also fits the shared budget's co-resident grid
+  std::int64_t cta_off_shared = 0; int coop_ctas_shared = 0;  // cooperative plan of the shared budget
+  int cnt_off = 0;                   // first publication counter of the level's fronts
+  std::int64_t ent_off = 0, ent_n = 0;  // inertia-only counts: this level's entries in FrontPlan::ent_idx
+  std::int64_t arena_used = 0;       // ... and its panels' extent in the arena
+};
+
+// The read-only front structure of one analysis on one device: level lists, cooperative CTA plans,
+// scatter destinations and the solve tables, with the sizes of the per-object work arrays. Built
+// once per analysis and shared, immutable, by every factorization object of that analysis
+// (analyze_like), and kept beside the process-wide analysis cache, so that a new object on a known
+// pattern builds and uploads no plan. A delayed-pivot re-plan gives its object a plan of its own.
+struct FrontPlan {
+  int device = -1;
+  std::vector<LevelPlan> levels;
+  std::int64_t vec_total = 0;      // contribution-vector rows of a solve
+  std::int64_t arena_entries = 1;  // inertia-only counts: the largest level's panels
+  std::int64_t scratch_max = 0, work_max = 0, w_total = 0, inv_total = 0;
+  int ncoop = 0, nsbl = 0, ntiles = 0, sweep_cnt_total = 0;
+  DevBuf<std::int32_t> row, col;   // the union pattern's entries (row, column)
+  DevBuf<std::int64_t> dest;       // their positions in the factor storage
+  DevBuf<SnDev> sn;
+  DevBuf<std::int32_t> lists, rmap, rows, child_ptr, children, iperm;
+  DevBuf<int2> items;              // extend-add items by child rank
+  // inertia-only counts: fronts with arena offsets, entries by level and their arena destinations
+  DevBuf<SnDev> sn_cnt;
+  DevBuf<std::int64_t> ent_idx, dest_cnt;
+  DevBuf<std::int64_t> work_off;   // solve work-vector offsets of the cooperatively solved fronts
+  DevBuf<std::int64_t> dpos;       // per pivot: panel index of its diagonal entry
+  DevBuf<std::int32_t> pfirst;     // per pivot: first column of its front
+  DevBuf<std::int32_t> cptr;       // large fronts: children's contributions per position
+  DevBuf<ContribEntry> cent;
+  DevBuf<int2> sbl;                // super-blocks of the solve operators
+  DevBuf<int4> tiles;
+};
+
 class GpuFactor {
  public:
   explicit GpuFactor(const hsg_options_t& opt);
@@ -119,25 +169,10 @@ class GpuFactor {
   void reset_device_stats() { dstats_ = DeviceStats{}; }
 
  private:
-  struct LevelPlan {
-    std::int64_t zero_off = 0; int zero_n = 0; int zero_chunks = 1;
-    std::int64_t s32_off = 0; int s32_n = 0;
-    std::int64_t s64_off = 0; int s64_n = 0;
-    std::int64_t app_off = 0; int app_n = 0;
-    bool coop = false;                 // large fronts: one cooperative launch, CTAs split by work
-    std::int64_t cta_off = 0; int coop_ctas = 0; int done_slot = 0;
-    std::int64_t all_off = 0; int all_n = 0; int maxm = 0;
-    std::vector<std::pair<std::int64_t, int>> ea;  // (offset into items, count) per child rank
-    bool solve_coop = false;           // few fronts: cooperative sweeps, CTAs split by panel size
-    std::int64_t solve_cta_off = 0; int solve_ctas = 0; int solve_steps = 0;
-    std::int64_t work_off_off = 0;     // offsets of the fronts' work vectors (index into d_work_off_)
-    bool coop_shared = false;          // the level also fits the shared budget's co-resident grid
-    std::int64_t cta_off_shared = 0; int coop_ctas_shared = 0;  // cooperative plan of the shared budget
-    int cnt_off = 0;                   // first publication counter of the level's fronts
-    std::int64_t ent_off = 0, ent_n = 0;  // inertia-only counts: this level's entries in d_ent_idx_
-    std::int64_t arena_used = 0;       // ... and its panels' extent in the arena
-  };
+  // plan_ = a new plan of sym_ (make_plan) and the per-object work arrays sized for it
   void build_plan();
+  std::shared_ptr<FrontPlan> make_plan();
+  void alloc_work();
   hsg_inertia_t run_factorization(double alpha, double beta, bool detection, bool shared, bool count_only);
   void run_numeric(double alpha, double beta, bool detection, bool count_only);
   template <class R>
@@ -175,45 +210,29 @@ class GpuFactor {
   std::vector<std::int64_t> rp_;
   std::vector<std::int32_t> ci_, row_;
   Symbolic sym_;
-  std::vector<LevelPlan> levels_;
+  std::shared_ptr<const FrontPlan> plan_;
+  // the cached analysis sym_ was copied from (null: own analysis, or re-planned since)
+  std::shared_ptr<const Symbolic> sym_origin_;
   hsg_inertia_t inertia_{};
   double last_factor_s_ = 0.0, last_solve_s_ = 0.0;
   DeviceStats dstats_;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, ev_in_ = nullptr;
-  std::int64_t vec_total_ = 0;
 
-  DevBuf<std::int32_t> d_row_, d_col_, d_rmap_, d_rows_, d_child_ptr_, d_children_, d_iperm_, d_lists_, d_pidx_,
-      d_failed_;
+  DevBuf<std::int32_t> d_pidx_, d_failed_;
   DevBuf<double> d_a_, d_b_, d_scale_, d_panels_, d_cb_, d_scratch_, d_vec_, d_xwork_, d_btmp_, d_inv_;
   DevBuf<float> d_panels_f_, d_cb_f_, d_w_f_, d_inv_f_;  // the same, for FP32 factors
-  // inertia-only counts: fronts with arena offsets, entries by level and their arena destinations
-  DevBuf<SnDev> d_sn_cnt_;
-  DevBuf<std::int64_t> d_ent_idx_, d_dest_cnt_;
-  DevBuf<double> d_arena_;
+  DevBuf<double> d_arena_;  // inertia-only counts: the panels of one level
   DevBuf<float> d_arena_f_;
-  std::int64_t arena_entries_ = 0;
   DevBuf<std::int32_t> d_blk_, d_nblk_;
-  DevBuf<std::int64_t> d_dest_;
   DevBuf<unsigned long long> d_r_;
-  DevBuf<SnDev> d_sn_;
-  DevBuf<int2> d_items_;
   DevBuf<signed char> d_piv_;
   DevBuf<FactorCounters> d_cnt_;
   DevBuf<int> d_level_done_;
-  DevBuf<std::int64_t> d_work_off_;
   DevBuf<double> d_work_;
   // super-block solve operators of the large fronts (built at the first solve after a factorization)
   DevBuf<double> d_w_;
   DevBuf<int> d_err_;  // set by a solve sweep whose bounded wait ran out
-  DevBuf<std::int64_t> d_dpos_;    // per pivot: panel index of its diagonal entry
-  DevBuf<std::int32_t> d_pfirst_;  // per pivot: first column of its front
-  DevBuf<std::int32_t> d_cptr_;   // large fronts: children's contributions per position
-  DevBuf<ContribEntry> d_cent_;
   DevBuf<int> d_sweep_cnt_;       // publication counters: forward slots, then backward slots
-  int sweep_cnt_total_ = 0;
-  DevBuf<int2> d_sbl_;
-  DevBuf<int4> d_tiles_;
-  int nsbl_ = 0, ntiles_ = 0;
   bool w_ready_ = false;
   void build_solve_operator();
   int solve_coop_max_ = 0;
@@ -221,7 +240,6 @@ class GpuFactor {
   bool shared_ = false;
   bool cached_analysis_ = false;  // the analysis came from (and teaches) the pattern cache
   static constexpr int kSharedParts = 3;
-  int ncoop_ = 0;
 };
 
 }  // namespace hsg

@@ -148,3 +148,31 @@ def test_mixed_sizes_keys_are_separate(monkeypatch):
             firsts[n] = active
     assert firsts == {20: 1, 30: 1}
     assert np.isfinite(srv.stats()["makespan_s"])
+
+
+def test_registered_pencil_keeps_one_session_per_worker(monkeypatch):
+    """A registered pencil: each worker builds its own session once and reuses it for every later
+    request; the sessions' memory stays reserved until close() releases it."""
+    tr = _Tracker()
+    made = []
+    base = _fake_session_class(tr, lambda n: 2.0)
+
+    class Counting(base):
+        def __init__(self, *a, **k):
+            super().__init__(*a, **k)
+            made.append(self)
+
+    monkeypatch.setattr(serve, "Session", Counting)
+    srv = serve.Server(workers=3, memory_budget_gb=100.0)
+    h = srv.register(_mat(40))
+    futs = [srv.submit(pencil=h, sigma=0.5, k=2) for _ in range(12)]
+    assert all(f.result().success for f in futs)
+    assert 1 <= len(made) <= 3
+    assert tr.max_active <= 3
+    assert srv._budget.used_mb > 0  # resident sessions hold their factor storage
+    srv.close()
+    assert abs(srv._budget.used_mb) < 1e-9
+    st = srv.stats()
+    assert st["requests"] == 12 and st["certified"] == 12
+    with pytest.raises(ValueError):
+        srv.submit(pencil=99, sigma=0.0, k=1)
