@@ -7,7 +7,8 @@
 `factor` analyzes K = A - shift B once and factorizes it `repeat` times; `solve` factorizes once and
 runs `repeat` in-place solves of `nrhs` device-resident right-hand sides; `eigs` runs the certified
 solve of the case's target through a session `repeat` times. Each prints its wall times (and, for
-`eigs`, the phase split of the solve report). The cases are the workloads of bench.py: box1e5 is
+`eigs`, the phase split of the solve report and the library's kernel launches before and during each
+solve, which locate one solve in a profiler's launch list). The cases are the workloads of bench.py: box1e5 is
 the PEC box 44 x 34 x 26 (lengths 1 x 0.75 x 0.55, generalized form, n = 109,744, all eigenvalues in
 [40, 200]); cube20 is the PEC cube 20^3 (standard form, n = 21,660, 10 nearest to 25); cube70 is the
 PEC cube 70^3 (n = 999,810, 21 nearest to 1071.43, between two exact levels); nedelec1e5 is the PEC
@@ -86,16 +87,19 @@ def solve(case: str, shift: float, nrhs: int, repeat: int) -> None:
 
 
 def eigs(case: str, repeat: int) -> None:
+    from ._native import kernel_launches
     from .api import Session
 
     a, b, target = _pencil(case)
     s = Session(a, b)
     for _ in range(repeat):
+        l0 = kernel_launches()
         t = time.perf_counter()
         r = s.solve(**target)
         dt = time.perf_counter() - t
         rp = r.report
-        print(f"solve {dt:.3f} s success={r.success} eigenvalues={r.eigenvalues.size} "
+        print(f"solve {dt:.3f} s launches_before={l0} launches={kernel_launches() - l0} "
+              f"success={r.success} eigenvalues={r.eigenvalues.size} "
               f"factor={rp['time_factor_s']:.4f} iterate={rp['time_iterate_s']:.4f} "
               f"certificate={rp['time_certificate_s']:.4f} verify={rp['time_verify_s']:.4f} "
               f"split={ {k: round(v, 4) for k, v in rp['iterate_split_s'].items()} }", flush=True)

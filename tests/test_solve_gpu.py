@@ -249,3 +249,29 @@ def test_server_results_are_the_same_alone_and_in_the_mix():
         np.testing.assert_allclose(r2.eigenvalues, r1.eigenvalues, rtol=EIG_RTOL)
         c1, c2 = r1.report["certificate"], r2.report["certificate"]
         assert c1["count_inertia"] == c2["count_inertia"] and c1["passed"] and c2["passed"]
+
+
+def test_registered_pencil_served_concurrently_matches_alone():
+    """A registered (resident) pencil served by four workers at once, every request with its own
+    Krylov seed and target: each result equals the same request solved alone on a session, and the
+    intervals match the exact spectrum."""
+    from hsolve_b200.serve import Server
+
+    box = yee.Box((12, 11, 10), (1.0, 0.75, 0.55))
+    a, b = yee.pencil(box, "generalized")
+    w = yee_exact.exact_spectrum(box.cells, box.lengths)
+    cuts = yee_exact.mid_gap_shifts(w[(w > 1.0) & (w < 600.0)], 40, 1e-6)
+    targets = [dict(lower=cuts[i], upper=cuts[i + 6], config={"seed": 100 + i}) for i in range(0, 24, 3)]
+    with Server(workers=4) as srv:
+        h = srv.register(a, b)
+        futs = [srv.submit(pencil=h, **t) for t in targets]
+        served = [f.result() for f in futs]
+    s = hsolve.Session(a, b)
+    for t, r in zip(targets, served):
+        _check_pairs(r)
+        alone = s.solve(**t)
+        want = w[(w >= t["lower"]) & (w < t["upper"])]
+        np.testing.assert_allclose(r.eigenvalues, want, rtol=EIG_RTOL)
+        np.testing.assert_allclose(r.eigenvalues, alone.eigenvalues, rtol=EIG_RTOL)
+        assert r.report["certificate"]["count_inertia"] == want.size
+    s.close()
