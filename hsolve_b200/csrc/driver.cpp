@@ -121,6 +121,9 @@ struct ShiftInvertOp : KrylovOperator {
   }
   void apply(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p) override {
     P.bprod(x, ldx, y, ldy, p);
+    // the factor's object may run on its own stream (the FP32 object of the mixed path): its solve
+    // waits for the work queued on the pencil's stream; it returns after its own stream finished
+    F.order_after(P.s);
     if (!refine) {
       F.solve(y, p, ldy, true);
       columns += p;
@@ -145,6 +148,7 @@ struct ShiftInvertOp : KrylovOperator {
     const CsrDev B = P.B.view(n);
     const CsrDev* Bp = P.b_identity ? nullptr : &B;
     col_dots(n, p, y, ldy, y, ldy, bxn, s);  // y = B x here
+    F.order_after(s);
     F.solve(y, p, ldy, true);
     shifted_residual(A, Bp, sigma, x, ldx, y, ldy, R.p, n, p, om, s);
     col_dots(n, p, R.p, n, R.p, n, rn, s);
@@ -172,6 +176,7 @@ struct ShiftInvertOp : KrylovOperator {
     for (int step = 0; step < kRefineSteps && remaining > 0; ++step) {
       // corrections of all p columns in one block solve (the solve's time hardly depends on the
       // column count), candidates y + K~^{-1} r and their residuals
+      F.order_after(s);
       F.solve(R.p, p, n, true);
       add_cols(n, p, y, ldy, R.p, n, C.p, n, s);
       shifted_residual(A, Bp, sigma, x, ldx, C.p, n, R.p, n, p, om, s);
@@ -716,6 +721,7 @@ Session::Session(const CsrHost& a_in, const CsrHost* b_in, int device, std::uint
   P.n = n;
   P.s = F.stream();
   cuda_check(cudaSetDevice(device), "cudaSetDevice");
+  PoolStreamScope scope(P.s);
   upload(P.A, a, P.s);
   if (b) {
     upload(P.B, *b, P.s);
@@ -799,6 +805,7 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
   HSG_REQUIRE(cfg.device == S.device, HSG_INVALID_INPUT, "config device differs from the session's device");
   GpuFactor& F = *S.F;
   Problem& P = S.P;
+  PoolStreamScope scope(P.s);  // buffers released below are stream-ordered on the pencil's stream
   // the factorization object that serves the operator: F itself (FP64), or the FP32 object of the
   // mixed-precision path; F, C0 and C1 keep every inertia count in FP64
   const bool single = cfg.factor_precision == 1;

@@ -191,10 +191,13 @@ GpuFactor::GpuFactor(const hsg_options_t& opt) : opt_(opt) {
   cuda_check(cudaEventCreateWithFlags(&ev_in_, cudaEventDisableTiming), "cudaEventCreate");
 }
 
-void GpuFactor::order_after_legacy_stream() {
+void GpuFactor::order_after_legacy_stream() { order_after(cudaStreamLegacy); }
+
+void GpuFactor::order_after(cudaStream_t other) {
+  if (other == stream_) return;
   DeviceGuard g(opt_.device);
-  cuda_check(cudaEventRecord(ev_in_, cudaStreamLegacy), "event on the default stream");
-  cuda_check(cudaStreamWaitEvent(stream_, ev_in_, 0), "wait for the default stream");
+  cuda_check(cudaEventRecord(ev_in_, other), "event on the producing stream");
+  cuda_check(cudaStreamWaitEvent(stream_, ev_in_, 0), "wait for the producing stream");
 }
 
 GpuFactor::~GpuFactor() {
@@ -215,6 +218,7 @@ void GpuFactor::analyze(std::int64_t n, const std::int64_t* a_rp, const std::int
   HSG_REQUIRE(n < (std::int64_t(1) << 31) - 1, HSG_UNSUPPORTED, "order above the 32-bit index range");
   HSG_REQUIRE(!b_rp || (b_ci && b_v), HSG_INVALID_INPUT, "analyze: incomplete B");
   DeviceGuard g(opt_.device);
+  PoolStreamScope scope(stream_);
   analysed_ = false;
   factored_ = false;
   std::vector<double> av, bv;
@@ -276,6 +280,7 @@ void GpuFactor::analyze_like(const GpuFactor& src) {
   HSG_REQUIRE(src.analysed_, HSG_INTERNAL, "analyze_like: source not analysed");
   HSG_REQUIRE(src.opt_.device == opt_.device, HSG_INVALID_INPUT, "analyze_like: different devices");
   DeviceGuard g(opt_.device);
+  PoolStreamScope scope(stream_);
   analysed_ = false;
   factored_ = false;
   n_ = src.n_;
@@ -727,6 +732,7 @@ hsg_inertia_t GpuFactor::run_factorization(double alpha, double beta, bool detec
   HSG_REQUIRE(analysed_, HSG_INTERNAL, "factorize before analyze");
   HSG_REQUIRE(std::isfinite(alpha) && std::isfinite(beta), HSG_INVALID_INPUT, "non-finite alpha / beta");
   DeviceGuard g(opt_.device);
+  PoolStreamScope scope(stream_);
   factored_ = false;
   w_ready_ = false;
   const auto t0 = std::chrono::steady_clock::now();
@@ -778,6 +784,7 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
   if (nrhs == 0) return;
   HSG_REQUIRE(b, HSG_INVALID_INPUT, "solve: null right-hand side");
   DeviceGuard g(opt_.device);
+  PoolStreamScope scope(stream_);
   const auto t0 = std::chrono::steady_clock::now();
   cudaStream_t s = stream_;
   const int nr = static_cast<int>(nrhs);

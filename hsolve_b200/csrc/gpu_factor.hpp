@@ -27,6 +27,22 @@ void pool_free(void* p, std::size_t cap, int device);
 // Releases every cached block of every device (the library's memory in use is not touched).
 void pool_trim();
 
+// The stream on which the calling thread queues the library's work while the scope is open. A
+// block released inside a scope gets an event recorded on that stream, and a later allocation of
+// the block (from any thread) waits for it: stream-ordered on its own scope's stream, or on the
+// host without a scope. A block released outside every scope must be idle already (its stream
+// synchronized). Scopes nest; the innermost one counts.
+class PoolStreamScope {
+ public:
+  explicit PoolStreamScope(cudaStream_t s);
+  ~PoolStreamScope();
+  PoolStreamScope(const PoolStreamScope&) = delete;
+  PoolStreamScope& operator=(const PoolStreamScope&) = delete;
+
+ private:
+  cudaStream_t prev_;
+};
+
 template <class T>
 struct DevBuf {
   T* p = nullptr;
@@ -143,6 +159,8 @@ class GpuFactor {
   // default stream, where a caller's own copies into a device right-hand side usually run; work on
   // the caller's other streams must be complete before a device solve is called.
   void order_after_legacy_stream();
+  // Orders the handle's stream after the work queued so far on `other` (an event, no host wait).
+  void order_after(cudaStream_t other);
   void release();
   hsg_estimate_t estimate() const;
   const hsg_inertia_t& inertia() const { return inertia_; }

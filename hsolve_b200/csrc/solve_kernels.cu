@@ -690,8 +690,12 @@ __global__ void __launch_bounds__(256, 2) k_solve_bwd_coop(const std::int32_t* l
     target += sb_groups(q, k);
     if (wbase >= b) break;  // no columns left for this CTA (uniform: b is a multiple of 32)
     const int bprev = b - kSB;  // columns of the next super-block: [bprev, b)
+    // the CTA's column chunks below b are updated from the highest down: the next super-block's
+    // columns (the highest ones) are finished and published first, so the next step can start
+    // while the rest of the update runs (every column has one owner, so nothing else reads it)
+    const int top = wbase + ((b - 1 - wbase) / ngrp) * ngrp;  // uniform over the CTA
     // prefetch the first column's W entries and old value
-    int j = wbase + gsub;
+    int j = top + gsub;
     double wv[16];
     {
       const F* Wj = Wf + b + static_cast<std::int64_t>(j) * m;
@@ -706,9 +710,9 @@ __global__ void __launch_bounds__(256, 2) k_solve_bwd_coop(const std::int32_t* l
       xb[idx] = (i < bs && r < nrhs) ? __ldcg(&sv[r * k + b + i]) : 0.0;
     }
     __syncthreads();
-    for (int base = wbase; base < b; base += ngrp) {
+    for (int base = top; base >= wbase; base -= ngrp) {
       j = base + gsub;
-      if (base != wbase) {
+      if (base != top) {
         const F* Wj = Wf + b + static_cast<std::int64_t>(j) * m;
 #pragma unroll
         for (int u = 0; u < 16; ++u) wv[u] = (j < b && sub + 8 * u < bs) ? Wj[sub + 8 * u] : 0.0;

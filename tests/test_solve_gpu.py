@@ -275,3 +275,46 @@ def test_registered_pencil_served_concurrently_matches_alone():
         np.testing.assert_allclose(r.eigenvalues, alone.eigenvalues, rtol=EIG_RTOL)
         assert r.report["certificate"]["count_inertia"] == want.size
     s.close()
+
+
+def test_concurrent_sessions_nearest_and_interval_stay_exact():
+    """Four threads, each with its own session on the same pencil, alternate nearest and interval
+    targets back to back: buffers that one request releases while its last kernels are still
+    queued are reused by the others only after those kernels ran, so every result stays equal to
+    the exact spectrum."""
+    import threading
+
+    box = yee.Box((11, 10, 9), (1.0, 0.85, 0.7))
+    a, b = yee.pencil(box, "generalized")
+    w = yee_exact.exact_spectrum(box.cells, box.lengths)
+    wl = w[(w > 1.0) & (w < 500.0)]
+    cuts = yee_exact.mid_gap_shifts(wl, 24, 1e-6)
+    errors = []
+
+    def worker(t):
+        s = hsolve.Session(a, b)
+        try:
+            for i in range(6):
+                q = (4 * t + i) % (len(cuts) - 4)
+                if i % 2:
+                    r = s.solve(lower=cuts[q], upper=cuts[q + 3], config={"seed": 10 * t + i})
+                    want = w[(w >= cuts[q]) & (w < cuts[q + 3])]
+                    got = r.eigenvalues
+                else:
+                    sigma = cuts[q] + 0.3 * (cuts[q + 1] - cuts[q])
+                    r = s.solve(sigma=sigma, k=6, config={"seed": 10 * t + i})
+                    order = np.argsort(np.abs(w - sigma), kind="stable")
+                    want, got = np.sort(w[order[:6]]), np.sort(r.eigenvalues)
+                if not r.success or got.size != want.size or np.max(np.abs(got - want) / want) > EIG_RTOL:
+                    errors.append((t, i, r.success, got.size, want.size))
+        except Exception as e:  # reported below
+            errors.append((t, repr(e)))
+        finally:
+            s.close()
+
+    ths = [threading.Thread(target=worker, args=(t,)) for t in range(4)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    assert not errors, errors
