@@ -380,6 +380,10 @@ def _unembed(w, v, report, a, b, tol, mode, sigma, k):
     x = np.hstack(vecs) if vecs else np.zeros((n, 0), dtype=np.complex128)
     if mode == "nearest":
         o = np.argsort(np.abs(lam - sigma), kind="stable")[:k]
+    elif mode == "smallest":
+        o = np.argsort(lam, kind="stable")[:k]
+    elif mode == "largest":
+        o = np.argsort(-lam, kind="stable")[:k]
     else:
         o = np.argsort(lam, kind="stable")
     lam, x = lam[o], np.asfortranarray(x[:, o])
@@ -418,7 +422,7 @@ def _unembed(w, v, report, a, b, tol, mode, sigma, k):
     ok = all(p["accepted"] for p in pairs) and (not cert or cert["passed"])
     if mode == "interval" and cert.get("count_inertia") is not None:
         ok = ok and lam.size == cert["count_inertia"]
-    if mode == "nearest":
+    if mode in ("nearest", "smallest", "largest"):
         ok = ok and lam.size == k
     rep["success"] = bool(ok)
     return lam, x, rep
@@ -458,7 +462,7 @@ def _embedded_config(cfg: dict) -> dict:
     """The config of the embedded (2n real) problem: twice the requested number of pairs."""
     ce = json.loads(json.dumps(cfg))
     t = ce.setdefault("target", {})
-    if t.get("mode", "nearest") == "nearest":
+    if t.get("mode", "nearest") in ("nearest", "smallest", "largest"):
         t["k"] = 2 * int(t.get("k", 6))
     return ce
 

@@ -8,6 +8,9 @@
 #include "driver.hpp"
 
 #include <algorithm>
+#include <atomic>
+#include <exception>
+#include <mutex>
 #include <future>
 #include <chrono>
 #include <cmath>
@@ -30,17 +33,18 @@ namespace {
 using Clock = std::chrono::steady_clock;
 double since(Clock::time_point t) { return std::chrono::duration<double>(Clock::now() - t).count(); }
 
+// A full CSR matrix on the device; copies share the arrays (the views of concurrent slices).
 struct DevCsr {
-  DevBuf<std::int64_t> rp;
-  DevBuf<std::int32_t> ci;
-  DevBuf<double> v;
-  CsrDev view(std::int64_t n) const { return CsrDev{n, rp.p, ci.p, v.p}; }
+  std::shared_ptr<DevBuf<std::int64_t>> rp = std::make_shared<DevBuf<std::int64_t>>();
+  std::shared_ptr<DevBuf<std::int32_t>> ci = std::make_shared<DevBuf<std::int32_t>>();
+  std::shared_ptr<DevBuf<double>> v = std::make_shared<DevBuf<double>>();
+  CsrDev view(std::int64_t n) const { return CsrDev{n, rp->p, ci->p, v->p}; }
 };
 
 void upload(DevCsr& d, const CsrHost& h, cudaStream_t s) {
-  d.rp.upload(h.rp, s);
-  d.ci.upload(h.ci, s);
-  d.v.upload(h.v, s);
+  d.rp->upload(h.rp, s);
+  d.ci->upload(h.ci, s);
+  d.v->upload(h.v, s);
 }
 
 CsrHost upper_of(const CsrHost& m) {
@@ -62,17 +66,19 @@ bool is_diagonal(const CsrHost& m) {
   return true;
 }
 
+// The pencil on the device and the stream its vector work is queued on. Copies share the device
+// data, so concurrent slices each take a copy with a stream of their own.
 struct Problem {
   std::int64_t n = 0;
   DevCsr A, B;
   bool b_identity = true;
   bool b_diagonal = false;
-  DevBuf<double> bdiag;
+  std::shared_ptr<DevBuf<double>> bdiag = std::make_shared<DevBuf<double>>();
   double normA = 0.0, normB = 1.0;
   cudaStream_t s = nullptr;
   void bprod(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p) {
     if (b_identity) copy_cols(n, p, x, ldx, y, ldy, s);
-    else if (b_diagonal) diag_scale(n, p, bdiag.p, x, ldx, y, ldy, s);
+    else if (b_diagonal) diag_scale(n, p, bdiag->p, x, ldx, y, ldy, s);
     else spmm(B.view(n), x, ldx, y, ldy, p, 1.0, 0.0, s);
   }
 };
@@ -316,6 +322,7 @@ struct SliceRec {
 };
 
 constexpr double kBatchFlopsMax = 5e11;  // per factorization
+constexpr std::size_t kConcurrentSlices = 3;  // slices of one window factorized and iterated at once
 
 struct Timers {
   double setup = 0, factor = 0, iterate = 0, verify = 0, cert = 0;
@@ -389,6 +396,57 @@ NearestRun run_krylov(ShiftInvertOp& op, Problem& P, double sigma, int nev, int 
 }
 
 int auto_block(int nev) { return nev >= 32 ? 8 : (nev >= 8 ? 4 : (nev >= 3 ? 2 : 1)); }
+
+// B^{-1} A (B = I: A), self-adjoint in the B inner product: the operator of the spectrum-end estimate.
+struct PencilOp : KrylovOperator {
+  Problem& P;
+  GpuFactor* FB;            // B's factorization (general B)
+  DevBuf<double> inv_diag;  // 1 / diag(B) (diagonal B)
+  PencilOp(Problem& pr, GpuFactor* fb) : P(pr), FB(fb) {}
+  void apply(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p) override {
+    spmm(P.A.view(P.n), x, ldx, y, ldy, p, 1.0, 0.0, P.s);
+    if (P.b_identity) return;
+    if (P.b_diagonal) {
+      diag_scale(P.n, p, inv_diag.p, y, ldy, y, ldy, P.s);
+      return;
+    }
+    FB->order_after(P.s);
+    FB->solve(y, p, ldy, true);
+  }
+  bool b_identity() const override { return P.b_identity; }
+  void bprod(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, int p) override { P.bprod(x, ldx, y, ldy, p); }
+};
+
+// Ritz estimate of the smallest (or largest) eigenvalue of the pencil: one cycle of Lanczos on
+// B^{-1} A in the B inner product, the seed of the inertia search of one-end targets (hsolve
+// src/driver/solver.cpp:452-480; a general B is factorized on F for it).
+double spectrum_end_estimate(Problem& P, GpuFactor& F, const CsrHost* b, bool smallest, std::uint64_t seed,
+                             Timers& tm) {
+  const auto t0 = Clock::now();
+  PencilOp op(P, &F);
+  if (!P.b_identity && P.b_diagonal) {
+    std::vector<double> d(P.n, 0.0);
+    for (std::int64_t i = 0; i < P.n; ++i)
+      for (std::int64_t q = b->rp[i]; q < b->rp[i + 1]; ++q)
+        if (b->ci[q] == i) d[i] += b->v[q];
+    for (double& x : d) x = 1.0 / x;
+    op.inv_diag.upload(d, P.s);
+  } else if (!P.b_identity) {
+    HSG_REQUIRE(F.factorize(0.0, 1.0, true).valid, HSG_INVALID_INPUT, "B is singular: not a definite generalized problem");
+  }
+  KsOptions o;
+  o.nev = 1;
+  o.ncv = static_cast<int>(std::min<std::int64_t>(30, P.n - 1));
+  o.block = 1;
+  o.max_restarts = 0;
+  o.tol = 0.0;
+  o.which = smallest ? Which::SmallestAlgebraic : Which::LargestAlgebraic;
+  o.ritz_vectors = false;
+  o.seed = seed;
+  KsResult r = krylov_schur(op, P.n, o, P.s);
+  tm.setup += since(t0);
+  return r.theta.at(0);
+}
 
 // ------------------------------------------------------------------------------------ GHIEP
 // Nearest target of a pencil whose B is indefinite (hsolve src/driver/indefinite.cpp:723-1000,
@@ -691,6 +749,24 @@ struct Session::Impl {
     }
     return *FS;
   }
+  // factorization objects of concurrent slices (lane 0: F, or the FP32 object of the mixed path;
+  // further lanes created at first use, per precision)
+  std::vector<std::unique_ptr<GpuFactor>> lanes[2];
+  std::mutex lanes_mu;
+  GpuFactor& slice_object(int lane, bool single) {
+    if (lane == 0) return single ? single_op() : *F;
+    std::lock_guard<std::mutex> lk(lanes_mu);
+    auto& v = lanes[single ? 1 : 0];
+    if (static_cast<int>(v.size()) < lane) v.resize(lane);
+    if (!v[lane - 1]) {
+      hsg_options_t o = fopt;
+      o.precision = single ? 1 : 0;
+      auto g = std::make_unique<GpuFactor>(o);
+      g->analyze_like(*F);
+      v[lane - 1] = std::move(g);
+    }
+    return *v[lane - 1];
+  }
   Problem P;
   std::string problem = "HEP";
   double scale = 0.0;
@@ -736,7 +812,7 @@ Session::Session(const CsrHost& a_in, const CsrHost* b_in, int device, std::uint
       double mx = 0.0, mn = std::numeric_limits<double>::infinity();
       for (double x : d) { mx = std::max(mx, std::fabs(x)); mn = std::min(mn, x); }
       if (!(mn > 0.0)) S.problem = "GHIEP";  // a non-positive diagonal entry: B is not positive definite
-      P.bdiag.upload(d, P.s);
+      P.bdiag->upload(d, P.s);
       P.normB = mx;
     }
   }
@@ -800,7 +876,7 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
   const CsrHost* b = S.b.get();
   const std::int64_t n = a.n;
   HSG_REQUIRE(cfg.tol > 0.0 && cfg.tol < 1.0, HSG_INVALID_INPUT, "tol outside (0, 1)");
-  HSG_REQUIRE(cfg.mode == 0 || cfg.mode == 1, HSG_UNSUPPORTED, "only 'nearest' and 'interval' targets are served by this build");
+  HSG_REQUIRE(cfg.mode >= 0 && cfg.mode <= 3, HSG_INVALID_INPUT, "target mode must be nearest, interval, smallest or largest");
   HSG_REQUIRE(cfg.factor_precision == 0 || cfg.factor_precision == 1, HSG_INVALID_INPUT, "factor_precision");
   HSG_REQUIRE(cfg.device == S.device, HSG_INVALID_INPUT, "config device differs from the session's device");
   GpuFactor& F = *S.F;
@@ -841,6 +917,57 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
   HSG_REQUIRE(!ghiep || cfg.mode == 0, HSG_UNSUPPORTED,
               "indefinite-B problems support target mode 'nearest' only: interval / smallest / largest need "
               "eigenvalue counts, which Sylvester inertia does not give for indefinite B");
+  // smallest / largest k: the window (-inf, U] with nu(U) >= k, or [L, +inf) with n - nu(L) >= k, by
+  // inertia search from a Ritz estimate of the spectrum's end (hsolve src/driver/definite.cpp:1918-
+  // 1993), closed at a point beyond the end (count 0, or n); then solved as an interval and the k
+  // smallest (ascending) or largest (descending) kept
+  const bool one_end = !ghiep && (cfg.mode == 2 || cfg.mode == 3);
+  double win_lo = cfg.lower, win_hi = cfg.upper;
+  long long window_count = -1;
+  if (one_end) {
+    const std::int64_t k = cfg.k;
+    HSG_REQUIRE(k >= 1 && k <= n, HSG_INVALID_INPUT, "k must be in [1, n]");
+    const bool smallest = cfg.mode == 2;
+    const double est = spectrum_end_estimate(P, F, b, smallest, cfg.seed + 3, tm);
+    const double step0 = 1e-2 * (std::fabs(est) + scale);
+    const double dir = smallest ? 1.0 : -1.0;  // from the end into the spectrum
+    const long long slack = std::max<long long>(4, k / 4);
+    long long moves = 0;
+    // the closing point beyond the end: nu = 0 (smallest) or n (largest)
+    double end = est - dir * step0;
+    const long long end_count = smallest ? 0 : n;
+    long long ne = count_below(F, end, scale, -dir, moves, tm);
+    for (int t = 0; ne != end_count; ++t) {
+      HSG_REQUIRE(t < 60, HSG_NOT_CONVERGED, "one-end target: no point beyond the end of the spectrum found");
+      end -= dir * step0 * std::ldexp(1.0, t + 1);
+      ne = count_below(F, end, scale, -dir, moves, tm);
+    }
+    // the inner end: grow the step until the window holds k, then bisect down to at most k + slack
+    auto held = [&](long long nu) { return smallest ? nu : n - nu; };
+    double a = end, c = est + dir * step0;
+    long long nc = count_below(F, c, scale, dir, moves, tm);
+    for (int t = 0; held(nc) < k; ++t) {
+      HSG_REQUIRE(t < 60, HSG_NOT_CONVERGED, "one-end target: the window never reached k eigenvalues");
+      a = c;
+      c += dir * step0 * std::ldexp(1.0, t + 1);
+      nc = count_below(F, c, scale, dir, moves, tm);
+    }
+    for (int t = 0; t < 40 && held(nc) > k + slack && std::fabs(c - a) > 1e-9 * (scale + std::fabs(c)); ++t) {
+      double mid = 0.5 * (a + c);
+      const long long nm = count_below(F, mid, scale, dir, moves, tm);
+      if (held(nm) >= k) {
+        c = mid;
+        nc = nm;
+      } else {
+        a = mid;
+      }
+    }
+    win_lo = smallest ? end : c;
+    win_hi = smallest ? c : end;
+    window_count = held(nc);
+    if (window_count < k)
+      warnings.push_back("the target window holds only " + std::to_string(window_count) + " eigenvalue(s), fewer than k");
+  }
   std::vector<PairMetrics> cpm;  // GHIEP: metrics of the complex pairs (lambda_re in .lambda)
   std::vector<double> c_im;      // and their imaginary parts
   long long zero_cluster_dim = -1;
@@ -1033,7 +1160,7 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
     HSG_REQUIRE(!lam_out.empty(), HSG_NOT_CONVERGED, "nearest target: no certified set of eigenpairs after reruns");
   } else {
     // ---------------------------------------------------------------- interval (slicing)
-    double lo = cfg.lower, hi = cfg.upper;
+    double lo = win_lo, hi = win_hi;
     HSG_REQUIRE(std::isfinite(lo) && std::isfinite(hi) && lo < hi, HSG_INVALID_INPUT, "interval needs lower < upper");
     long long moves = 0, moves_hi = 0;
     const double mid0 = 0.5 * (lo + hi);
@@ -1099,64 +1226,144 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
       }
       ++i;
     }
+    // one slice: its shift factorized on G (unless G holds it already), block Krylov-Schur of the
+    // shift-invert operator with reruns for missing pairs, the slice's vectors; Q is the pencil with
+    // G's stream, so slices on different objects run concurrently
+    struct SliceOut {
+      SliceRec rec{};
+      std::vector<double> lam;
+      DevBuf<double> X;
+      int retries = 0;
+      long long columns = 0, refine_steps = 0, refined_applies = 0;
+      double worst_rel = 0.0, worst_omega = 0.0;
+      Timers tm;
+    };
+    auto run_slice = [&](std::size_t i, GpuFactor& G, Problem Q, bool prefactored, double sigma0, bool shared) {
+      PoolStreamScope scope(Q.s);
+      SliceOut o;
+      const long long c = below[i + 1] - below[i];
+      o.rec = SliceRec{cuts[i], cuts[i + 1], 0.5 * (cuts[i] + cuts[i + 1]), c, 0, 0, 0, 0, 0, c == 0};
+      if (c == 0) return o;
+      double sigma = prefactored ? sigma0 : o.rec.sigma;
+      if (!prefactored && !factorize_at(G, sigma, scale, cfg.max_shift_retries, o.retries, o.tm, shared))
+        HSG_THROW(HSG_SINGULAR, "slice shift singular near " << o.rec.sigma);
+      o.rec.sigma = sigma;
+      ShiftInvertOp sop(Q, G);
+      sop.set_refinement(sigma, tol_inner);
+      int nev = static_cast<int>(std::min<std::int64_t>(n - 1, c + std::max<long long>(4, c / 4)));
+      const int p = cfg.block_size > 0 ? cfg.block_size : auto_block(nev);
+      for (int attempt = 0; attempt < 4; ++attempt) {
+        // reruns reuse G's factorization at sigma
+        const long long applies0 = sop.columns;
+        NearestRun run = run_krylov(sop, Q, sigma, nev, static_cast<int>(c), cfg, p, cfg.seed + 17 * i + attempt, o.tm);
+        o.rec.restarts += run.restarts;
+        o.rec.op_applies += sop.columns - applies0;
+        o.rec.nev = nev;
+        std::vector<int> inside;
+        for (std::size_t j = 0; j < run.lam.size(); ++j)
+          if (run.lam[j] >= cuts[i] && run.lam[j] < cuts[i + 1]) inside.push_back(static_cast<int>(j));
+        o.rec.count_found = static_cast<long long>(inside.size());
+        if (o.rec.count_found != c && attempt + 1 < 4) {
+          ++o.rec.reruns;
+          nev = static_cast<int>(std::min<std::int64_t>(n - 1, nev + std::max<long long>(4, c - o.rec.count_found + 4)));
+          continue;
+        }
+        o.rec.passed = o.rec.count_found == c;
+        const int ncols = static_cast<int>(run.X.n / n);
+        std::vector<double> Sel(static_cast<std::size_t>(ncols) * inside.size(), 0.0);
+        for (std::size_t q = 0; q < inside.size(); ++q) {
+          Sel[static_cast<std::size_t>(run.col[inside[q]]) + q * ncols] = 1.0;
+          o.lam.push_back(run.lam[inside[q]]);
+        }
+        DevBuf<double> Sd;
+        Sd.upload(Sel, Q.s);
+        o.X.alloc(static_cast<std::size_t>(n) * std::max<std::size_t>(1, inside.size()));
+        if (!inside.empty())
+          gemm_tall(n, ncols, static_cast<int>(inside.size()), run.X.p, n, Sd.p, ncols, o.X.p, n, 1.0, 0.0, Q.s);
+        cuda_check(cudaStreamSynchronize(Q.s), "slice vectors");
+        break;
+      }
+      o.rec.op_applies = sop.columns;
+      o.columns = sop.columns;
+      o.refine_steps = sop.refine_steps;
+      o.refined_applies = sop.refined_applies;
+      o.worst_rel = sop.worst_rel;
+      o.worst_omega = sop.worst_omega;
+      return o;
+    };
+    const std::size_t nslices = cuts.size() - 1;
+    std::vector<SliceOut> outs(nslices);
+    std::size_t nonempty = 0;
+    for (std::size_t i = 0; i < nslices; ++i) nonempty += below[i + 1] > below[i];
+    auto view = [&](GpuFactor& G) {
+      Problem Q = P;
+      Q.s = G.stream();
+      return Q;
+    };
+    if (spec_slice && nslices == 1) {
+      outs[0] = run_slice(0, OPF, view(OPF), true, sigma_mid, false);  // factorized during the counts
+    } else if (batch && nonempty > 1) {
+      // the slices' shifts at once: up to kConcurrentSlices factorization objects sharing the
+      // analysis (each with the shared cooperative plan), each taking the next slice when done
+      const int lanes = static_cast<int>(std::min<std::size_t>(kConcurrentSlices, nonempty));
+      std::atomic<std::size_t> next{0};
+      std::vector<std::exception_ptr> errs(lanes);
+      std::vector<std::future<void>> futs;
+      for (int lane = 0; lane < lanes; ++lane) {
+        GpuFactor& G = S.slice_object(lane, single);
+        futs.push_back(std::async(std::launch::async, [&, lane] {
+          GpuFactor& Gl = S.slice_object(lane, single);
+          try {
+            for (std::size_t i = next++; i < nslices; i = next++) outs[i] = run_slice(i, Gl, view(Gl), false, 0.0, true);
+          } catch (...) {
+            errs[lane] = std::current_exception();
+            next = nslices;  // the other lanes stop after their current slice
+          }
+        }));
+        (void)G;
+      }
+      for (auto& f : futs) f.wait();
+      for (auto& e : errs)
+        if (e) std::rethrow_exception(e);
+    } else {
+      for (std::size_t i = 0; i < nslices; ++i) outs[i] = run_slice(i, OPF, view(OPF), false, 0.0, false);
+    }
     std::vector<std::vector<double>> vals;
     std::vector<DevBuf<double>> vecs;
     long long found_total = 0;
     bool all_pass = true;
-    for (std::size_t i = 0; i + 1 < cuts.size(); ++i) {
-      const long long c = below[i + 1] - below[i];
-      SliceRec rec{cuts[i], cuts[i + 1], 0.5 * (cuts[i] + cuts[i + 1]), c, 0, 0, 0, 0, 0, c == 0};
-      if (c == 0) { slices.push_back(rec); continue; }
-      double sigma = rec.sigma;
-      if (spec_slice && cuts.size() == 2) {
-        sigma = sigma_mid;  // factorized while the window ends were counted
-        spec_slice = false;
-      } else if (!factorize_at(OPF, sigma, scale, cfg.max_shift_retries, shift_retries, tm)) {
-        HSG_THROW(HSG_SINGULAR, "slice shift singular near " << rec.sigma);
-      }
-      rec.sigma = sigma;
-      op.set_refinement(sigma, tol_inner);
-      int nev = static_cast<int>(std::min<std::int64_t>(n - 1, c + std::max<long long>(4, c / 4)));
-      const int p = cfg.block_size > 0 ? cfg.block_size : auto_block(nev);
-      block_used = std::max(block_used, p);
-      for (int attempt = 0; attempt < 4; ++attempt) {
-        // reruns reuse F's factorization at sigma (nothing else runs on F inside the slice loop)
-        const long long applies0 = op.columns;
-        NearestRun run = run_krylov(op, P, sigma, nev, static_cast<int>(c), cfg, p, cfg.seed + 17 * i + attempt, tm);
-        rec.restarts += run.restarts;
-        rec.op_applies += op.columns - applies0;
-        rec.nev = nev;
-        std::vector<int> inside;
-        for (std::size_t j = 0; j < run.lam.size(); ++j)
-          if (run.lam[j] >= cuts[i] && run.lam[j] < cuts[i + 1]) inside.push_back(static_cast<int>(j));
-        rec.count_found = static_cast<long long>(inside.size());
-        if (rec.count_found != c && attempt + 1 < 4) {
-          ++rec.reruns;
-          nev = static_cast<int>(std::min<std::int64_t>(n - 1, nev + std::max<long long>(4, c - rec.count_found + 4)));
-          continue;
-        }
-        rec.passed = rec.count_found == c;
-        const int ncols = static_cast<int>(run.X.n / n);
-        std::vector<double> S(static_cast<std::size_t>(ncols) * inside.size(), 0.0);
-        std::vector<double> lv;
-        for (std::size_t q = 0; q < inside.size(); ++q) {
-          S[static_cast<std::size_t>(run.col[inside[q]]) + q * ncols] = 1.0;
-          lv.push_back(run.lam[inside[q]]);
-        }
-        DevBuf<double> Sd, Xs;
-        Sd.upload(S, P.s);
-        Xs.alloc(static_cast<std::size_t>(n) * std::max<std::size_t>(1, inside.size()));
-        if (!inside.empty()) gemm_tall(n, ncols, static_cast<int>(inside.size()), run.X.p, n, Sd.p, ncols, Xs.p, n, 1.0, 0.0, P.s);
-        cuda_check(cudaStreamSynchronize(P.s), "slice vectors");
-        vals.push_back(lv);
-        vecs.push_back(std::move(Xs));
-        break;
-      }
-      found_total += rec.count_found;
-      all_pass = all_pass && rec.passed;
-      restarts += static_cast<int>(rec.restarts);
-      slices.push_back(rec);
+    Timers slice_max;
+    for (auto& o : outs) {
+      slices.push_back(o.rec);
+      shift_retries += o.retries;
+      op.columns += o.columns;
+      op.refine_steps += o.refine_steps;
+      op.refined_applies += o.refined_applies;
+      op.worst_rel = std::max(op.worst_rel, o.worst_rel);
+      op.worst_omega = std::max(op.worst_omega, o.worst_omega);
+      slice_max.factor += o.tm.factor;
+      slice_max.iterate += o.tm.iterate;
+      slice_max.kry_apply += o.tm.kry_apply;
+      slice_max.kry_ortho += o.tm.kry_ortho;
+      slice_max.kry_rr += o.tm.kry_rr;
+      slice_max.kry_restart += o.tm.kry_restart;
+      if (o.rec.count_inertia == 0) continue;
+      block_used = std::max(block_used, cfg.block_size > 0 ? static_cast<int>(cfg.block_size)
+                                                             : auto_block(static_cast<int>(o.rec.nev)));
+      found_total += o.rec.count_found;
+      all_pass = all_pass && o.rec.passed;
+      restarts += static_cast<int>(o.rec.restarts);
+      vals.push_back(o.lam);
+      vecs.push_back(std::move(o.X));
     }
+    // concurrent slices overlap: their summed phase times over the concurrency (a wall estimate)
+    const double par = batch && nonempty > 1 ? static_cast<double>(std::min<std::size_t>(kConcurrentSlices, nonempty)) : 1.0;
+    tm.factor += slice_max.factor / par;
+    tm.iterate += slice_max.iterate / par;
+    tm.kry_apply += slice_max.kry_apply / par;
+    tm.kry_ortho += slice_max.kry_ortho / par;
+    tm.kry_rr += slice_max.kry_rr / par;
+    tm.kry_restart += slice_max.kry_restart / par;
     cert.count_found = found_total;
     cert.passed = all_pass && found_total == N;
     // gather ascending
@@ -1173,6 +1380,23 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
     sigma_used = slices.empty() ? 0.5 * (lo + hi) : slices.front().sigma;
   }
   (void)applies_before;
+  if (one_end) {
+    // keep the k smallest (ascending) or the k largest (descending) of the window's eigenpairs
+    const std::size_t m_all = lam_out.size();
+    const std::size_t keep = std::min<std::size_t>(m_all, static_cast<std::size_t>(cfg.k));
+    DevBuf<double> Xk;
+    Xk.alloc(static_cast<std::size_t>(n) * std::max<std::size_t>(1, keep));
+    std::vector<double> lk;
+    for (std::size_t j = 0; j < keep; ++j) {
+      const std::size_t src = cfg.mode == 2 ? j : m_all - 1 - j;
+      lk.push_back(lam_out[src]);
+      copy_cols(n, 1, Xout.p + static_cast<std::int64_t>(src) * n, n, Xk.p + static_cast<std::int64_t>(j) * n, n, P.s);
+    }
+    lam_out = lk;
+    Xout = std::move(Xk);
+    if (cfg.mode == 2) cert.lower = -std::numeric_limits<double>::infinity();
+    else cert.upper = std::numeric_limits<double>::infinity();
+  }
   // verification
   const auto t_ver = Clock::now();
   const int m = static_cast<int>(lam_out.size());
@@ -1187,7 +1411,8 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
   for (const auto& q : pm) all_ok = all_ok && q.accepted;
   for (const auto& q : cpm) all_ok = all_ok && q.accepted;
   if (ghiep) all_ok = all_ok && static_cast<std::int64_t>(m + cpm.size()) == cfg.k;
-  const bool success = all_ok && (!cert.performed || cert.passed) && (cfg.mode != 1 || m == cert.count_inertia);
+  const bool success = all_ok && (!cert.performed || cert.passed) && (cfg.mode != 1 || m == cert.count_inertia) &&
+                       (!one_end || m == std::min<long long>(cfg.k, window_count));
   // report
   const hsg_estimate_t est = F.estimate();
   const hsg_inertia_t inr = F.inertia();
@@ -1203,7 +1428,7 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
   j.kv("scale", scale);
   j.kv("method", std::string(ghiep ? "shift_invert_krylov_schur" : "shift_invert_lanczos"));
   j.kv("candidate_source", std::string("iterative"));
-  j.kv("sigma_requested", cfg.mode == 0 ? cfg.sigma : 0.5 * (cfg.lower + cfg.upper));
+  j.kv("sigma_requested", cfg.mode == 0 ? cfg.sigma : 0.5 * (win_lo + win_hi));
   j.kv("sigma_used", sigma_used);
   j.kv("shift_retries", shift_retries);
   j.kv("block_size", block_used);

@@ -53,9 +53,24 @@ std::vector<double> orthogonalize(Basis& B, int j, int p, cudaStream_t s) {
   return Htot;
 }
 
-// B-orthonormalize columns [j, j+p) in place (CholQR2). Returns R (p x p, upper in the sense
-// W_old = W_new R, stored column-major) or an empty vector on breakdown.
-std::vector<double> normalize(Basis& B, KrylovOperator& op, int j, int p, cudaStream_t s) {
+// Thresholds of the block orthonormalization (the contract of hsolve's BlockOrthonormalizer,
+// src/eigen/block_ortho.hpp:28-64, with this project's values): Cholesky-QR is trusted while the
+// column-scaled condition number of the first pass's R stays below kMaxCholQrCond and the second
+// pass's Gram matrix stays within kMaxSecondPassDeviation of I; a column whose B-norm falls to
+// kDeficientRatio of its input norm is dependent on the basis to working precision.
+constexpr double kMaxCholQrCond = 1e5;
+constexpr double kMaxSecondPassDeviation = 0.5;
+constexpr double kDeficientRatio = 1e-10;
+
+// B-orthonormalize columns [j, j+p) in place (CholQR2) when the block is well conditioned:
+// returns R (p x p, upper in the sense W_old = W_new R, column-major), or an empty vector with the
+// block unchanged when the fast path must not be taken: a column of B-norm <= kDeficientRatio *
+// before[c] (its norm before the projection on the basis), G not numerically positive definite,
+// the scaled condition number of R1 above kMaxCholQrCond, or the second pass's G far from I.
+// before[c] is computed here from hn2[c] (the squared projections of the input column on the basis)
+// and the first pass's G: ||w_c||^2 = ||h_c||^2 + G_cc, the basis being B-orthonormal.
+std::vector<double> normalize(Basis& B, KrylovOperator& op, int j, int p, const std::vector<double>& hn2,
+                              std::vector<double>& before, cudaStream_t s) {
   std::vector<double> Rtot(static_cast<std::size_t>(p) * p, 0.0);
   for (int i = 0; i < p; ++i) Rtot[i + i * p] = 1.0;
   std::vector<double> G, L;
@@ -65,7 +80,38 @@ std::vector<double> normalize(Basis& B, KrylovOperator& op, int j, int p, cudaSt
     to_host(G, B.g.p, static_cast<std::size_t>(p) * p, s);
     for (int a = 0; a < p; ++a)
       for (int b = 0; b < a; ++b) { const double m = 0.5 * (G[a + b * p] + G[b + a * p]); G[a + b * p] = m; G[b + a * p] = m; }
-    if (!cholesky(p, G, L, 1e-28)) return {};
+    bool ok = true;
+    if (pass == 0) {
+      before.resize(p);
+      for (int a = 0; a < p; ++a) before[a] = std::sqrt(std::max(0.0, hn2[a] + G[a + a * p]));
+      // every column keeps more than its deficiency share, and the column-scaled G is well enough
+      // conditioned for Cholesky-QR: cond(R1) = sqrt(cond(D^-1/2 G D^-1/2))
+      std::vector<double> Gs(G);
+      for (int a = 0; a < p && ok; ++a) ok = G[a + a * p] > kDeficientRatio * kDeficientRatio * before[a] * before[a];
+      if (ok) {
+        for (int a = 0; a < p; ++a)
+          for (int b = 0; b < p; ++b) Gs[a + b * p] = G[a + b * p] / std::sqrt(G[a + a * p] * G[b + b * p]);
+        std::vector<double> w;
+        sym_eig(p, Gs, w);
+        ok = w[0] > 0.0 && w[p - 1] <= kMaxCholQrCond * kMaxCholQrCond * w[0];
+      }
+    } else {
+      double dev = 0.0;
+      for (int a = 0; a < p; ++a)
+        for (int b = 0; b < p; ++b) dev += (G[a + b * p] - (a == b ? 1.0 : 0.0)) * (G[a + b * p] - (a == b ? 1.0 : 0.0));
+      ok = std::sqrt(dev) <= kMaxSecondPassDeviation;
+    }
+    ok = ok && cholesky(p, G, L, 1e-28);
+    if (!ok) {
+      if (pass == 1) {
+        // undo the first pass (W = Q1 R1), so the caller's column path starts from the block
+        std::vector<double> Rt(Rtot);
+        to_dev(B.small.p, Rt, s);
+        gemm_tall(B.n, p, p, B.v(j), B.n, B.small.p, p, B.tmp.p, B.n, 1.0, 0.0, s);
+        copy_cols(B.n, p, B.tmp.p, B.n, B.v(j), B.n, s);
+      }
+      return {};
+    }
     // W = W L^{-T}  (W^T B W = L L^T -> (W L^{-T})^T B (W L^{-T}) = I)
     std::vector<double> Linv = lower_inverse(p, L);
     std::vector<double> LinvT(static_cast<std::size_t>(p) * p);
@@ -84,6 +130,15 @@ std::vector<double> normalize(Basis& B, KrylovOperator& op, int j, int p, cudaSt
       for (int b = 0; b < p; ++b) LT[a + b * p] = L[b + a * p];
     Rtot = matmul(p, p, p, LT, Rtot);
   }
+  for (int i = 0; i < p; ++i)
+    if (!(std::fabs(Rtot[i + i * p]) > kDeficientRatio * before[i])) {
+      // a column left with no more than its deficiency share after both passes: the column path
+      std::vector<double> Rt(Rtot);
+      to_dev(B.small.p, Rt, s);
+      gemm_tall(B.n, p, p, B.v(j), B.n, B.small.p, p, B.tmp.p, B.n, 1.0, 0.0, s);
+      copy_cols(B.n, p, B.tmp.p, B.n, B.v(j), B.n, s);
+      return {};
+    }
   return Rtot;
 }
 
@@ -91,21 +146,77 @@ void random_block(Basis& B, int j, int p, std::mt19937_64& rng, cudaStream_t s) 
   fill_normal(B.n, p, B.v(j), B.n, rng(), s);
 }
 
-// New block [j, j+p) made orthonormal to [0, j); breakdown columns replaced by random ones.
-// Returns R (coupling) of the original block; zero rows where random vectors were drawn.
+// B-norm of column c of the basis (after refreshing B v(c) when B is not the identity).
+double column_norm(Basis& B, KrylovOperator& op, int c, cudaStream_t s) {
+  if (!B.bid) op.bprod(B.v(c), B.n, B.bv(c), B.n, 1);
+  gram(B.n, 1, 1, B.v(c), B.n, B.bv(c), B.n, B.g.p, B.part.p, B.part_cap, s);
+  std::vector<double> g;
+  to_host(g, B.g.p, 1, s);
+  return std::sqrt(std::max(g[0], 0.0));
+}
+
+// Column c projected twice (CGS2) against columns [0, c) in the B inner product; returns the
+// accumulated coefficients (c of them).
+std::vector<double> project_column(Basis& B, int c, cudaStream_t s) {
+  std::vector<double> tot(c, 0.0), g;
+  if (c == 0) return tot;
+  for (int pass = 0; pass < 2; ++pass) {
+    gram(B.n, c, 1, B.bid ? B.v(0) : B.bv(0), B.n, B.v(c), B.n, B.g.p, B.part.p, B.part_cap, s);
+    gemm_tall(B.n, c, 1, B.v(0), B.n, B.g.p, c, B.v(c), B.n, -1.0, 1.0, s);
+    to_host(g, B.g.p, static_cast<std::size_t>(c), s);
+    for (int t = 0; t < c; ++t) tot[t] += g[t];
+  }
+  return tot;
+}
+
+// Column-by-column fallback (hsolve's column_fallback, src/eigen/block_ortho.cpp:340): each column
+// of the block is projected by CGS2 against the basis and the block's earlier columns; a column
+// whose B-norm falls to kDeficientRatio of its input norm is dependent on the basis (a block
+// breakdown), gets R(c, c) = 0 and is replaced by a random vector projected the same way; where no
+// direction is left (the basis spans the space), the column stays zero with zero coupling.
+std::vector<double> column_fallback(Basis& B, KrylovOperator& op, int j, int p, std::vector<double>& H,
+                                    const std::vector<double>& before, std::mt19937_64& rng, cudaStream_t s) {
+  std::vector<double> R(static_cast<std::size_t>(p) * p, 0.0);
+  for (int c = 0; c < p; ++c) {
+    const int col = j + c;
+    std::vector<double> g = project_column(B, col, s);
+    for (int t = 0; t < j; ++t) H[t + static_cast<std::size_t>(c) * j] += g[t];
+    for (int t = j; t < col; ++t) R[(t - j) + static_cast<std::size_t>(c) * p] = g[t];
+    double nrm = column_norm(B, op, col, s);
+    if (nrm > kDeficientRatio * before[c]) {
+      R[c + static_cast<std::size_t>(c) * p] = nrm;
+    } else {
+      nrm = 0.0;
+      for (int attempt = 0; attempt < 3 && !(nrm > 0.0); ++attempt) {
+        random_block(B, col, 1, rng, s);
+        const double r0 = column_norm(B, op, col, s);
+        project_column(B, col, s);
+        nrm = column_norm(B, op, col, s);
+        if (!(nrm > 1e-8 * r0)) nrm = 0.0;  // the random vector lies in the basis' span as well
+      }
+    }
+    if (nrm > 0.0) {
+      scale_cols(B.n, 1, 1.0 / nrm, B.v(col), B.n, s);
+      if (!B.bid) scale_cols(B.n, 1, 1.0 / nrm, B.bv(col), B.n, s);
+    } else {
+      scale_cols(B.n, 1, 0.0, B.v(col), B.n, s);
+      if (!B.bid) scale_cols(B.n, 1, 0.0, B.bv(col), B.n, s);
+    }
+  }
+  return R;
+}
+
+// New block [j, j+p) made orthonormal to [0, j): returns R (the coupling W_old = W_new R, zero in
+// the columns that had to be replaced) and the projections H (j x p) on the basis.
 std::vector<double> ortho_block(Basis& B, KrylovOperator& op, int j, int p, std::vector<double>& H, std::mt19937_64& rng,
                                 cudaStream_t s) {
   H = orthogonalize(B, j, p, s);
-  std::vector<double> R = normalize(B, op, j, p, s);
+  std::vector<double> hn2(p, 0.0), before;
+  for (int c = 0; c < p; ++c)
+    for (int t = 0; t < j; ++t) hn2[c] += H[t + static_cast<std::size_t>(c) * j] * H[t + static_cast<std::size_t>(c) * j];
+  std::vector<double> R = normalize(B, op, j, p, hn2, before, s);
   if (!R.empty()) return R;
-  // breakdown (invariant subspace): restart the block from random vectors, no coupling
-  for (int attempt = 0; attempt < 3; ++attempt) {
-    random_block(B, j, p, rng, s);
-    std::vector<double> Hr = orthogonalize(B, j, p, s);
-    std::vector<double> Rr = normalize(B, op, j, p, s);
-    if (!Rr.empty()) return std::vector<double>(static_cast<std::size_t>(p) * p, 0.0);
-  }
-  HSG_THROW(HSG_NOT_CONVERGED, "Krylov basis: could not extend the basis (breakdown)");
+  return column_fallback(B, op, j, p, H, before, rng, s);
 }
 
 }  // namespace

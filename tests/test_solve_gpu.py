@@ -318,3 +318,67 @@ def test_concurrent_sessions_nearest_and_interval_stay_exact():
     for th in ths:
         th.join()
     assert not errors, errors
+
+
+def _laplacian_2d(nx, ny):
+    t1 = sp.diags([-np.ones(nx - 1), 2 * np.ones(nx), -np.ones(nx - 1)], [-1, 0, 1])
+    t2 = sp.diags([-np.ones(ny - 1), 2 * np.ones(ny), -np.ones(ny - 1)], [-1, 0, 1])
+    return (sp.kron(sp.identity(ny), t1) + sp.kron(t2, sp.identity(nx))).tocsr()
+
+
+def test_smallest_and_largest_targets_standard_and_generalized():
+    """Target modes smallest / largest (hsolve TargetMode::Smallest / Largest): the window closed by
+    inertia search from a Ritz estimate of the spectrum's end, certified by counts; the k smallest
+    ascending and the k largest descending, against dense eigenvalues."""
+    import scipy.linalg as sla
+
+    a = _laplacian_2d(30, 27)
+    n = a.shape[0]
+    rng = np.random.default_rng(11)
+    off = sp.random(n, n, density=2.0 / n, random_state=3, format="csr")
+    off = 0.05 * (off + off.T)
+    bg = (off + sp.diags(1.0 + rng.uniform(0.0, 1.0, n) + abs(off).sum(axis=1).A1)).tocsr()
+    bd = sp.diags(1.0 + rng.uniform(0.0, 1.0, n)).tocsr()
+    for b in (None, bd, bg):
+        w = sla.eigh(a.toarray(), None if b is None else b.toarray(), eigvals_only=True)
+        r = hsolve.solve(a, b, k=7, mode="smallest")
+        _check_pairs(r)
+        np.testing.assert_allclose(r.eigenvalues, w[:7], rtol=EIG_RTOL)
+        c = r.report["certificate"]
+        assert c["passed"] and c["count_inertia"] >= 7
+        r = hsolve.solve(a, b, k=5, mode="largest")
+        _check_pairs(r)
+        np.testing.assert_allclose(r.eigenvalues, w[::-1][:5], rtol=EIG_RTOL)
+    # the Yee box's top end, against the exact spectrum
+    box = yee.Box((8, 7, 6), (1.0, 0.9, 0.8))
+    ay, by = yee.pencil(box, "generalized")
+    wy = np.sort(yee_exact.exact_spectrum(box.cells, box.lengths))
+    r = hsolve.solve(ay, by, k=6, mode="largest")
+    _check_pairs(r)
+    np.testing.assert_allclose(r.eigenvalues, wy[::-1][:6], rtol=EIG_RTOL)
+
+
+@pytest.mark.parametrize("p", [1, 4, 8])
+def test_krylov_basis_that_spans_the_whole_space(p):
+    """A pencil so small that the Krylov basis spans the whole space: the next block is dependent on
+    the basis to working precision (a block breakdown), the column-wise fallback leaves it with zero
+    coupling instead of failing, and the Ritz pairs are exact. Also a block whose columns are nearly
+    dependent (eigenvalues clustered to 1e-9): the conditioned CholQR2 path or its fallback must keep
+    the basis orthonormal."""
+    n = 48
+    rng = np.random.default_rng(5)
+    q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    d = np.arange(1.0, n + 1.0)
+    a = sp.csr_matrix(q @ np.diag(d) @ q.T)
+    r = hsolve.solve(a, sigma=10.3, k=20, config={"block_size": p})
+    _check_pairs(r)
+    order = np.argsort(np.abs(d - 10.3), kind="stable")
+    np.testing.assert_allclose(np.sort(r.eigenvalues), np.sort(d[order[:20]]), rtol=EIG_RTOL)
+    d2 = np.concatenate([1.0 + 1e-9 * np.arange(8), np.linspace(3.0, 40.0, n - 8)])
+    a2 = sp.csr_matrix(q @ np.diag(d2) @ q.T)
+    r = hsolve.solve(a2, lower=0.5, upper=2.0, config={"block_size": p})
+    _check_pairs(r)
+    assert r.eigenvalues.size == 8
+    np.testing.assert_allclose(r.eigenvalues, d2[:8], rtol=1e-9)
+    x = r.eigenvectors
+    assert np.abs(x.T @ x - np.eye(8)).max() < 1e-8
