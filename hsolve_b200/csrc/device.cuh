@@ -18,9 +18,8 @@ struct SnDev {
   std::int64_t rmap_off;  // its CB rows' positions in the parent's rows
   std::int64_t vec_off;   // contribution vector (m-k entries per rhs) in the solve arena
   std::int64_t scratch_off;  // pivoting scratch of the panel kernel (doubles)
-  std::int64_t inv_off;      // inverse diagonal blocks (32 x 32 each) of the solve
-  std::int64_t w_off;        // super-block solve operator (m x k, ld m) of a large front (-1: none)
-  std::int64_t cptr_off;     // children's contributions per front position (m + 1 offsets; large fronts)
+  std::int64_t w_off;        // super-block solve operator (m x k, ld m) in the operator storage
+  std::int64_t cptr_off;     // children's contributions per front position (m + 1 offsets)
 };
 
 // One child contribution to a front position: entry a of the child's contribution vector
@@ -29,6 +28,16 @@ struct ContribEntry {
   std::int64_t vec_off;
   std::int32_t a;
   std::int32_t mc;
+};
+
+// One CTA of a solve sweep level: front s, the CTA's rank among the front's nr CTAs, and the offset
+// of the front's work vectors.
+struct SolveTask {
+  std::int32_t s;
+  std::int32_t rank;
+  std::int32_t nr;
+  std::int32_t pad;
+  std::int64_t wofs;
 };
 
 // Counters written by the factorization kernels (integers: sums are order independent).

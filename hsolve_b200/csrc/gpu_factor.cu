@@ -36,6 +36,8 @@ struct AnalysisEntry {
 };
 
 constexpr std::size_t kAnalysisCacheEntries = 8;
+// panel entries per CTA of a solve sweep
+constexpr double kSolveEntriesPerCta = 32768.0;
 std::mutex g_analysis_mu;
 std::list<AnalysisEntry> g_analysis_cache;  // most recently used first
 
@@ -318,7 +320,7 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
   P.col.upload(ci_, stream_);
   const std::int32_t ns = S.ns;
   std::vector<SnDev> sn(ns);
-  std::int64_t vec = 0, inv_total = 0;
+  std::int64_t vec = 0;
   for (std::int32_t s = 0; s < ns; ++s) {
     SnDev& d = sn[s];
     d.first = S.first[s];
@@ -332,10 +334,8 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
     d.vec_off = vec;
     vec += d.m - d.k;
     d.scratch_off = 0;
-    d.inv_off = inv_total;
     d.w_off = -1;
     d.cptr_off = -1;
-    inv_total += static_cast<std::int64_t>((d.k + 30) / 31 + 1) * 1024;
   }
   P.vec_total = vec;
   {
@@ -352,14 +352,13 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
   }
   if (coop_max_ == 0) coop_max_ = coop_max_ctas(opt_.device);
   if (solve_coop_max_ == 0) solve_coop_max_ = solve_coop_max_ctas(opt_.device);
-  std::vector<std::int64_t> work_offs;
+  std::vector<SolveTask> tasks;
   std::int64_t work_max = 0;
   std::vector<int2> sbl;
   std::vector<int4> tiles;
   std::int64_t w_total = 0;
   std::vector<std::int32_t> cptr;
   std::vector<ContribEntry> cent;
-  int cnt_total = 0;
   std::vector<std::int32_t> lists;
   std::vector<int2> items;
   P.levels.assign(S.nlevels, LevelPlan{});
@@ -394,81 +393,81 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
     put(s64, L.s64_off, L.s64_n);
     put(app, L.app_off, L.app_n);
     put(all, L.all_off, L.all_n);
-    // solves: cooperative sweeps when the level's fronts fit the co-resident grid
-    if (!all.empty() && static_cast<int>(all.size()) <= solve_coop_max_) {
-      std::vector<double> wts(all.size());
-      double wsum = 0.0;
-      int steps = 0;
+    // solve sweeps: every front gets its children's contribution lists and a solve operator, and
+    // CTAs by its panel size (about kSolveEntriesPerCta entries each, at most one per 32-row group
+    // forward and one per 32-column chunk backward); a level whose CTAs would exceed the
+    // co-resident bound shares what fits by panel size, or runs one CTA per front
+    {
       std::int64_t wofs = 0;
-      L.work_off_off = static_cast<std::int64_t>(work_offs.size());
+      std::vector<std::int64_t> fwofs(all.size());
       for (std::size_t q = 0; q < all.size(); ++q) {
-        const SnDev& dd = sn[all[q]];
-        wts[q] = static_cast<double>(dd.m) * dd.k;
-        wsum += wts[q];
-        steps = std::max(steps, (dd.k + kSB - 1) / kSB);
-        work_offs.push_back(wofs);
-        wofs += 8 * static_cast<std::int64_t>(dd.m) + 8 * static_cast<std::int64_t>(dd.k) + (dd.k + 1) / 2 + 2;
-        SnDev& dw = sn[all[q]];
-        // children's contribution entries per front position, in child order
-        {
-          const std::int32_t sq = all[q];
-          dw.cptr_off = static_cast<std::int64_t>(cptr.size());
-          std::vector<std::int32_t> num(dw.m + 1, 0);
-          for (std::int32_t e = S.child_ptr[sq]; e < S.child_ptr[sq + 1]; ++e) {
-            const std::int32_t ch = S.children[e];
-            const int mc = sn[ch].m - sn[ch].k;
-            for (int a = 0; a < mc; ++a) num[S.rmap[S.rmap_off[ch] + a] + 1]++;
-          }
-          for (int i = 0; i < dw.m; ++i) num[i + 1] += num[i];
-          const std::int32_t base = static_cast<std::int32_t>(cent.size());
-          for (int i = 0; i <= dw.m; ++i) cptr.push_back(base + num[i]);
-          cent.resize(cent.size() + num[dw.m]);
-          std::vector<std::int32_t> fill(num.begin(), num.end() - 1);
-          for (std::int32_t e = S.child_ptr[sq]; e < S.child_ptr[sq + 1]; ++e) {
-            const std::int32_t ch = S.children[e];
-            const int mc = sn[ch].m - sn[ch].k;
-            for (int a = 0; a < mc; ++a) {
-              ContribEntry ce;
-              ce.vec_off = sn[ch].vec_off;
-              ce.a = a;
-              ce.mc = mc;
-              cent[base + fill[S.rmap[S.rmap_off[ch] + a]]++] = ce;
-            }
+        const std::int32_t sq = all[q];
+        SnDev& dw = sn[sq];
+        fwofs[q] = wofs;
+        wofs += std::max<std::int64_t>(8 * static_cast<std::int64_t>(dw.m), 16 * static_cast<std::int64_t>(dw.k));
+        dw.cptr_off = static_cast<std::int64_t>(cptr.size());
+        std::vector<std::int32_t> num(dw.m + 1, 0);
+        for (std::int32_t e = S.child_ptr[sq]; e < S.child_ptr[sq + 1]; ++e) {
+          const std::int32_t ch = S.children[e];
+          const int mc = sn[ch].m - sn[ch].k;
+          for (int a = 0; a < mc; ++a) num[S.rmap[S.rmap_off[ch] + a] + 1]++;
+        }
+        for (int i = 0; i < dw.m; ++i) num[i + 1] += num[i];
+        const std::int32_t base = static_cast<std::int32_t>(cent.size());
+        for (int i = 0; i <= dw.m; ++i) cptr.push_back(base + num[i]);
+        cent.resize(cent.size() + num[dw.m]);
+        std::vector<std::int32_t> fill(num.begin(), num.end() - 1);
+        for (std::int32_t e = S.child_ptr[sq]; e < S.child_ptr[sq + 1]; ++e) {
+          const std::int32_t ch = S.children[e];
+          const int mc = sn[ch].m - sn[ch].k;
+          for (int a = 0; a < mc; ++a) {
+            ContribEntry ce;
+            ce.vec_off = sn[ch].vec_off;
+            ce.a = a;
+            ce.mc = mc;
+            cent[base + fill[S.rmap[S.rmap_off[ch] + a]]++] = ce;
           }
         }
         dw.w_off = w_total;
         w_total += static_cast<std::int64_t>(dw.m) * dw.k;
         for (int b = 0, qb = 0; b < dw.k; b += kSB, ++qb) {
-          sbl.push_back(make_int2(all[q], qb));
+          sbl.push_back(make_int2(sq, qb));
           const int be = std::min(b + kSB, dw.k);
-          for (int r0 = be; r0 < dw.m; r0 += 64) tiles.push_back(make_int4(all[q], qb, r0, 0));
+          for (int r0 = be; r0 < dw.m; r0 += 64) tiles.push_back(make_int4(sq, qb, r0, 0));
         }
       }
       work_max = std::max(work_max, wofs);
-      std::vector<int> nr(all.size());
-      int total = 0;
-      for (std::size_t q = 0; q < all.size(); ++q) {
-        // about 32k panel entries per CTA
-        nr[q] = static_cast<int>(std::max(1.0, std::min<double>(std::ceil(wts[q] / 32768.0), solve_coop_max_)));
-        total += nr[q];
-      }
-      if (total > solve_coop_max_) {
-        const int spare = solve_coop_max_ - static_cast<int>(all.size());
-        total = 0;
+      auto plan_tasks = [&](bool bwd, std::int64_t& off, int& ctas, bool& coop) {
+        auto cap = [&](const SnDev& dd) { return std::max(1, ((bwd ? dd.k : dd.m) + 31) / 32); };
+        std::vector<int> nr(all.size());
+        double wsum = 0.0;
+        int total = 0;
         for (std::size_t q = 0; q < all.size(); ++q) {
-          nr[q] = 1 + static_cast<int>(std::floor(spare * wts[q] / wsum));
+          const SnDev& dd = sn[all[q]];
+          const double w = static_cast<double>(dd.m) * dd.k;
+          wsum += w;
+          nr[q] = static_cast<int>(std::min<double>(cap(dd), std::max(1.0, std::ceil(w / kSolveEntriesPerCta))));
           total += nr[q];
         }
-      }
-      std::vector<std::int32_t> starts(all.size() + 1, 0);
-      for (std::size_t q = 0; q < all.size(); ++q) starts[q + 1] = starts[q] + nr[q];
-      L.solve_coop = true;
-      L.cnt_off = cnt_total;
-      cnt_total += static_cast<int>(all.size());
-      L.solve_cta_off = static_cast<std::int64_t>(lists.size());
-      lists.insert(lists.end(), starts.begin(), starts.end());
-      L.solve_ctas = starts.back();
-      L.solve_steps = steps;
+        if (total > solve_coop_max_) {
+          const int spare = solve_coop_max_ - static_cast<int>(all.size());
+          for (std::size_t q = 0; q < all.size(); ++q) {
+            const SnDev& dd = sn[all[q]];
+            const double w = static_cast<double>(dd.m) * dd.k;
+            nr[q] = spare > 0 && wsum > 0.0 ? std::min(cap(dd), 1 + static_cast<int>(std::floor(spare * w / wsum))) : 1;
+          }
+        }
+        off = static_cast<std::int64_t>(tasks.size());
+        coop = false;
+        for (std::size_t q = 0; q < all.size(); ++q)
+          for (int r = 0; r < nr[q]; ++r) {
+            tasks.push_back(SolveTask{all[q], r, nr[q], 0, fwofs[q]});
+            coop = coop || nr[q] > 1;
+          }
+        ctas = static_cast<int>(static_cast<std::int64_t>(tasks.size()) - off);
+      };
+      plan_tasks(false, L.fwd_task_off, L.fwd_ctas, L.fwd_coop);
+      plan_tasks(true, L.bwd_task_off, L.bwd_ctas, L.bwd_coop);
     }
     // cooperative launch when the level's panel fronts fit the co-resident grid; CTAs apportioned
     // by m^2, for the whole device and for the shared budget (a third of it, used while several
@@ -585,10 +584,9 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
   P.children.upload(S.children, stream_);
   P.iperm.upload(S.iperm, stream_);
   P.dest.upload(S.dest, stream_);
-  P.work_off.upload(work_offs, stream_);
+  P.tasks.upload(tasks, stream_);
   P.cptr.upload(cptr, stream_);
   P.cent.upload(cent, stream_);
-  P.sweep_cnt_total = cnt_total;
   P.sbl.upload(sbl, stream_);
   P.tiles.upload(tiles, stream_);
   P.nsbl = static_cast<int>(sbl.size());
@@ -596,9 +594,6 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
   P.scratch_max = scratch_max;
   P.work_max = work_max;
   P.w_total = w_total;
-  P.inv_total = inv_total;
-  for (std::int32_t s = 0; s < ns; ++s)
-    HSG_REQUIRE((sn[s].k + 30) / 31 <= kMaxBlocksPerFront, HSG_UNSUPPORTED, "front with " << sn[s].k << " pivots exceeds the solve block table");
   return plan;
 }
 
@@ -606,27 +601,22 @@ void GpuFactor::alloc_work() {
   const FrontPlan& P = *plan_;
   const std::size_t fe = static_cast<std::size_t>(std::max<std::int64_t>(1, sym_.factor_entries));
   const std::size_t cbe = static_cast<std::size_t>(std::max<std::int64_t>(1, sym_.cb_arena));
-  const std::size_t inve = static_cast<std::size_t>(std::max<std::int64_t>(1, P.inv_total));
   const std::size_t we = static_cast<std::size_t>(std::max<std::int64_t>(1, P.w_total));
   if (single()) {
     d_panels_f_.alloc(fe);
     d_cb_f_.alloc(cbe);
-    d_inv_f_.alloc(inve);
     d_w_f_.alloc(we);
   } else {
     d_panels_.alloc(fe);
     d_cb_.alloc(cbe);
-    d_inv_.alloc(inve);
     d_w_.alloc(we);
   }
   d_scratch_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, P.scratch_max)));
   d_level_done_.alloc(static_cast<std::size_t>(std::max(1, P.ncoop)));
   d_work_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, P.work_max)));
   d_err_.alloc(1);
-  d_sweep_cnt_.alloc(static_cast<std::size_t>(std::max(1, 2 * P.sweep_cnt_total)));
+  d_sweep_cnt_.alloc(static_cast<std::size_t>(3 * std::max(1, sym_.ns)));
   w_ready_ = false;
-  d_blk_.alloc(static_cast<std::size_t>(n_));
-  d_nblk_.alloc(static_cast<std::size_t>(std::max(1, sym_.ns)));
 }
 
 void GpuFactor::build_plan() {
@@ -641,12 +631,10 @@ template <> double* GpuFactor::cb_of<double>() { return d_cb_.p; }
 template <> float* GpuFactor::cb_of<float>() { return d_cb_f_.p; }
 template <> double* GpuFactor::w_of<double>() { return d_w_.p; }
 template <> float* GpuFactor::w_of<float>() { return d_w_f_.p; }
-template <> double* GpuFactor::inv_of<double>() { return d_inv_.p; }
-template <> float* GpuFactor::inv_of<float>() { return d_inv_f_.p; }
 
 std::size_t GpuFactor::factor_bytes() const {
   const std::size_t el = single() ? sizeof(float) : sizeof(double);
-  return el * (d_panels_.n + d_panels_f_.n + d_w_.n + d_w_f_.n + d_inv_.n + d_inv_f_.n);
+  return el * (d_panels_.n + d_panels_f_.n + d_w_.n + d_w_f_.n);
 }
 
 void GpuFactor::run_numeric(double alpha, double beta, bool detection, bool count_only) {
@@ -867,37 +855,25 @@ void GpuFactor::run_sweeps_t(double* xwork, double* vec, int nr) {
   cudaStream_t s = stream_;
   const F* panels = panels_of<F>();
   const F* W = w_of<F>();
-  const F* inv = inv_of<F>();
-  const std::int32_t* lists = plan_->lists.p;
-  // chunks of at most 8 right-hand sides (the cooperative sweeps carry 8)
+  const SolveTask* tasks = plan_->tasks.p;
+  const int ns = sym_.ns;
+  int* fcnt = d_sweep_cnt_.p;
+  int* bcnt = fcnt + ns;
+  int* arrive = bcnt + ns;
+  // chunks of at most 8 right-hand sides (the sweeps carry 8)
   for (int c0 = 0; c0 < nr; c0 += 8) {
     const int nc = std::min(8, nr - c0);
     double* xw = xwork + static_cast<std::int64_t>(c0) * n_;
     cuda_check(cudaMemsetAsync(d_sweep_cnt_.p, 0, d_sweep_cnt_.n * sizeof(int), s), "reset sweep counters");
-    for (const LevelPlan& L : plan_->levels) {
-      if (L.solve_coop) {
-        cuda_check(launch_solve_fwd_coop<F>(lists + L.all_off, lists + L.solve_cta_off, L.all_n, L.solve_ctas, plan_->sn.p,
-                                            plan_->cptr.p, plan_->cent.p, W, d_pidx_.p, xw, n_, vec, nc, d_work_.p,
-                                            plan_->work_off.p + L.work_off_off, d_sweep_cnt_.p + L.cnt_off, d_err_.p, s),
-                   "cooperative forward solve");
-      } else {
-        launch_solve_fwd<F>(lists + L.all_off, L.all_n, L.maxm, plan_->sn.p, plan_->child_ptr.p, plan_->children.p, plan_->rmap.p,
-                            panels, d_piv_.p, d_pidx_.p, d_blk_.p, d_nblk_.p, inv, xw, n_, vec, nc, s);
-      }
-    }
+    for (const LevelPlan& L : plan_->levels)
+      cuda_check(launch_fwd_level<F>(tasks + L.fwd_task_off, L.fwd_ctas, L.fwd_coop, plan_->sn.p, plan_->cptr.p,
+                                     plan_->cent.p, W, d_pidx_.p, xw, n_, vec, nc, d_work_.p, fcnt, d_err_.p, s),
+                 "forward solve");
     launch_solve_diag_flat<F>(n_, plan_->dpos.p, plan_->pfirst.p, panels, d_piv_.p, d_pidx_.p, xw, n_, nc, s);
-    for (auto it = plan_->levels.rbegin(); it != plan_->levels.rend(); ++it) {
-      if (it->solve_coop) {
-        cuda_check(launch_solve_bwd_coop<F>(lists + it->all_off, lists + it->solve_cta_off, it->all_n, it->solve_ctas,
-                                            plan_->sn.p, plan_->rows.p, W, d_pidx_.p, xw, n_, nc, d_work_.p,
-                                            plan_->work_off.p + it->work_off_off,
-                                            d_sweep_cnt_.p + plan_->sweep_cnt_total + it->cnt_off, d_err_.p, s),
-                   "cooperative backward solve");
-      } else {
-        launch_solve_bwd<F>(lists + it->all_off, it->all_n, it->maxm, plan_->sn.p, plan_->rows.p, panels, d_pidx_.p, d_blk_.p,
-                            d_nblk_.p, inv, xw, n_, nc, s);
-      }
-    }
+    for (auto it = plan_->levels.rbegin(); it != plan_->levels.rend(); ++it)
+      cuda_check(launch_bwd_level<F>(tasks + it->bwd_task_off, it->bwd_ctas, it->bwd_coop, plan_->sn.p, plan_->rows.p, W,
+                                     d_pidx_.p, xw, n_, nc, d_work_.p, bcnt, arrive, d_err_.p, s),
+                 "backward solve");
   }
 }
 
@@ -910,7 +886,6 @@ void GpuFactor::build_solve_operator() {
 
 template <class F>
 void GpuFactor::build_solve_operator_t() {
-  launch_inv_blocks<F>(sym_.ns, plan_->sn.p, panels_of<F>(), d_piv_.p, d_blk_.p, d_nblk_.p, inv_of<F>(), stream_);
   launch_sb_build<F>(plan_->sbl.p, plan_->nsbl, plan_->tiles.p, plan_->ntiles, plan_->sn.p, panels_of<F>(), d_piv_.p, w_of<F>(), stream_);
 }
 

@@ -91,12 +91,12 @@ struct LevelPlan {
   std::int64_t cta_off = 0; int coop_ctas = 0; int done_slot = 0;
   std::int64_t all_off = 0; int all_n = 0; int maxm = 0;
   std::vector<std::pair<std::int64_t, int>> ea;  // (offset into items, count) per child rank
-  bool solve_coop = false;           // few fronts: cooperative sweeps, CTAs split by panel size
-  std::int64_t solve_cta_off = 0; int solve_ctas = 0; int solve_steps = 0;
-  std::int64_t work_off_off = 0;     // offsets of the fronts' work vectors (index into FrontPlan::work_off)
+  // solve sweeps: the level's CTA tasks (FrontPlan::tasks) of the forward and the backward sweep;
+  // coop: some front has several CTAs (cooperative launch)
+  std::int64_t fwd_task_off = 0; int fwd_ctas = 0; bool fwd_coop = false;
+  std::int64_t bwd_task_off = 0; int bwd_ctas = 0; bool bwd_coop = false;
   bool coop_shared = false;          // the level also fits the shared budget's co-resident grid
   std::int64_t cta_off_shared = 0; int coop_ctas_shared = 0;  // cooperative plan of the shared budget
-  int cnt_off = 0;                   // first publication counter of the level's fronts
   std::int64_t ent_off = 0, ent_n = 0;  // inertia-only counts: this level's entries in FrontPlan::ent_idx
   std::int64_t arena_used = 0;       // ... and its panels' extent in the arena
 };
@@ -111,8 +111,8 @@ struct FrontPlan {
   std::vector<LevelPlan> levels;
   std::int64_t vec_total = 0;      // contribution-vector rows of a solve
   std::int64_t arena_entries = 1;  // inertia-only counts: the largest level's panels
-  std::int64_t scratch_max = 0, work_max = 0, w_total = 0, inv_total = 0;
-  int ncoop = 0, nsbl = 0, ntiles = 0, sweep_cnt_total = 0;
+  std::int64_t scratch_max = 0, work_max = 0, w_total = 0;
+  int ncoop = 0, nsbl = 0, ntiles = 0;
   DevBuf<std::int32_t> row, col;   // the union pattern's entries (row, column)
   DevBuf<std::int64_t> dest;       // their positions in the factor storage
   DevBuf<SnDev> sn;
@@ -121,10 +121,10 @@ struct FrontPlan {
   // inertia-only counts: fronts with arena offsets, entries by level and their arena destinations
   DevBuf<SnDev> sn_cnt;
   DevBuf<std::int64_t> ent_idx, dest_cnt;
-  DevBuf<std::int64_t> work_off;   // solve work-vector offsets of the cooperatively solved fronts
+  DevBuf<SolveTask> tasks;         // solve sweep CTAs, level by level (forward and backward lists)
   DevBuf<std::int64_t> dpos;       // per pivot: panel index of its diagonal entry
   DevBuf<std::int32_t> pfirst;     // per pivot: first column of its front
-  DevBuf<std::int32_t> cptr;       // large fronts: children's contributions per position
+  DevBuf<std::int32_t> cptr;       // children's contributions per front position
   DevBuf<ContribEntry> cent;
   DevBuf<int2> sbl;                // super-blocks of the solve operators
   DevBuf<int4> tiles;
@@ -207,8 +207,6 @@ class GpuFactor {
   R* cb_of();
   template <class R>
   R* w_of();
-  template <class R>
-  R* inv_of();
 
  public:
   // FP32 factors (hsg_options_t.precision == 1): the operator factorization of the mixed-precision
@@ -237,20 +235,19 @@ class GpuFactor {
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, ev_in_ = nullptr;
 
   DevBuf<std::int32_t> d_pidx_, d_failed_;
-  DevBuf<double> d_a_, d_b_, d_scale_, d_panels_, d_cb_, d_scratch_, d_vec_, d_xwork_, d_btmp_, d_inv_;
-  DevBuf<float> d_panels_f_, d_cb_f_, d_w_f_, d_inv_f_;  // the same, for FP32 factors
+  DevBuf<double> d_a_, d_b_, d_scale_, d_panels_, d_cb_, d_scratch_, d_vec_, d_xwork_, d_btmp_;
+  DevBuf<float> d_panels_f_, d_cb_f_, d_w_f_;  // the same, for FP32 factors
   DevBuf<double> d_arena_;  // inertia-only counts: the panels of one level
   DevBuf<float> d_arena_f_;
-  DevBuf<std::int32_t> d_blk_, d_nblk_;
   DevBuf<unsigned long long> d_r_;
   DevBuf<signed char> d_piv_;
   DevBuf<FactorCounters> d_cnt_;
   DevBuf<int> d_level_done_;
   DevBuf<double> d_work_;
-  // super-block solve operators of the large fronts (built at the first solve after a factorization)
+  // super-block solve operators of every front (built at the first solve after a factorization)
   DevBuf<double> d_w_;
   DevBuf<int> d_err_;  // set by a solve sweep whose bounded wait ran out
-  DevBuf<int> d_sweep_cnt_;       // publication counters: forward slots, then backward slots
+  DevBuf<int> d_sweep_cnt_;       // per front: forward and backward publication counters, backward arrivals
   bool w_ready_ = false;
   void build_solve_operator();
   int solve_coop_max_ = 0;

@@ -1,13 +1,26 @@
-// Supernodal forward / diagonal / backward solves with nrhs right-hand sides (replaces MUMPS JOB=3,
-// hsolve src/factor/mumps_factorization.cpp:459-527; MUMPS dsol_fwd.F / dsol_bwd.F).
+// Supernodal forward / diagonal / backward solves with up to 8 right-hand sides per sweep (replaces
+// MUMPS JOB=3, hsolve src/factor/mumps_factorization.cpp:459-527; MUMPS dsol_fwd.F / dsol_bwd.F).
 //
-// The forward sweep runs level by level like the factorization: a front gathers its pivot rows from
-// the solution vector and its children's contribution vectors (fixed order, no atomics, so results
-// are bitwise reproducible), solves with its unit-lower L11 in blocks of at most 32 columns (never
-// splitting a 2x2 pivot), and leaves its contribution -L21 z for the parent. The backward sweep
-// runs top-down and only gathers (ancestors' values are final). All right-hand sides of a chunk
-// are carried together so that every L entry is read once per chunk.
-#include <cooperative_groups.h>
+// Solve operator. The pivots of every front are cut into super-blocks of kSB = 128 (a 2 x 2 pivot may
+// straddle a boundary: its coupling entry is D, not L, and reads as zero). For a super-block
+// B = [b, b + bs) of a front with unit lower panel L (m x k, column-major, ld m):
+//     W[B, B] = L_BB^{-1}                 (lower triangular, zero above the diagonal)
+//     W[i, B] = L[i, B] L_BB^{-1},  i >= b + bs  (later pivot rows and the contribution rows),
+// stored like the panel in a separate buffer and built once per factorization before its first
+// solve. Forward L z = t, super-block by super-block: z_B = W[B, B] t_B and t_i -= W[i, B] t_B below
+// B (both read only t_B, so they run at once). Backward L^T x = y, from the last super-block down:
+//     s_j = (W[A, A]^T y_A)_j - W[CB, j]^T x_CB        for every pivot j (A = j's super-block),
+//     x_B = s_B after every later super-block C has been applied by s_j -= W[C, j]^T x_C.
+//
+// Schedule. Fronts are solved level by level of the elimination tree (children first forward,
+// parents first backward), one launch per level and sweep. A front gets nr CTAs by its panel size
+// (a task per CTA: front, rank, nr). Forward, 32-row groups belong to CTA (group mod nr) for the
+// whole sweep; backward, 32-column chunks to CTA (chunk mod nr). The CTAs of a front publish the
+// groups / chunks they finish through a per-front counter (fence + atomic add; the readers poll
+// with acquire loads and a bound), so a front's steps need no grid barrier. A level whose fronts
+// each have one CTA is an ordinary launch, any other level a cooperative launch (co-resident CTAs).
+// No data is accumulated with atomics: every value has one writer and every sum is formed in a
+// fixed order, so the results are bitwise reproducible.
 #include <cstdint>
 #include <mutex>
 
@@ -39,180 +52,7 @@ __global__ void k_scatter_scale(std::int64_t n, int nrhs, double* b, std::int64_
   }
 }
 
-// block partition of the k pivots: at most 32 columns, a 2x2 pivot never split
-__device__ __forceinline__ int block_size_at(const signed char* pv, int b, int k) {
-  int bs = k - b < 32 ? k - b : 32;
-  if (bs == 32 && pv[b + 31] == 2) bs = 31;
-  return bs;
-}
-
 }  // namespace
-
-// After a factorization: the block partition of every front's pivots (<= 32 columns, 2x2 pivots
-// never split) and the inverses of its unit-lower diagonal blocks (2x2 couplings are D, not L, and
-// excluded), so that the solves apply each block as one small matrix-vector product instead of a
-// chain of dependent pivot steps. One CTA per front; warp w inverts blocks w, w + 8, ...; lane c
-// computes column c by forward substitution.
-template <class F>
-__global__ void __launch_bounds__(256) k_inv_blocks(const SnDev* sn, const F* panels, const signed char* piv,
-                                                     std::int32_t* blk, std::int32_t* nblk, F* inv) {
-  __shared__ int starts[kMaxBlocksPerFront];
-  __shared__ int nb;
-  const int s = blockIdx.x;
-  const SnDev d = sn[s];
-  if (d.w_off >= 0) return;  // large fronts are solved through their super-block operator
-  const int k = d.k, m = d.m;
-  const signed char* pv = piv + d.first;
-  if (threadIdx.x == 0) {
-    int c = 0;
-    for (int b = 0; b < k && c < kMaxBlocksPerFront;) {
-      starts[c++] = b;
-      b += block_size_at(pv, b, k);
-    }
-    nb = c;
-    nblk[s] = c;
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) blk[d.first + i] = starts[i];
-  const F* P = panels + d.panel_off;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  for (int bi = warp; bi < nb; bi += nwarps) {
-    const int b = starts[bi];
-    const int bs = bi + 1 < nb ? starts[bi + 1] - b : k - b;
-    F* out = inv + d.inv_off + static_cast<std::int64_t>(bi) * 1024;
-    double x[32];
-#pragma unroll
-    for (int i = 0; i < 32; ++i) x[i] = 0.0;
-    if (lane < bs) {
-      x[lane] = 1.0;
-      for (int i = lane + 1; i < bs; ++i) {
-        double acc = 0.0;
-        for (int j = lane; j < i; ++j) {
-          if (j + 1 == i && pv[b + j] == 2) continue;  // D coupling of a 2x2 pivot
-          acc += P[(b + i) + static_cast<std::int64_t>(b + j) * m] * x[j];
-        }
-        x[i] = -acc;
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < 32; ++i) out[lane * 32 + i] = static_cast<F>((lane < bs) ? x[i] : 0.0);
-  }
-}
-
-// Forward sweep of the listed fronts. t (m x R, row-major) in dynamic shared memory.
-template <class F>
-__global__ void __launch_bounds__(256) k_solve_fwd(const std::int32_t* list, const SnDev* sn,
-                                                    const std::int32_t* child_ptr, const std::int32_t* children,
-                                                    const std::int32_t* rmap, const F* panels,
-                                                    const signed char* piv, const std::int32_t* pidx,
-                                                    const std::int32_t* blk, const std::int32_t* nblk,
-                                                    const F* inv, double* x, std::int64_t n, double* vec,
-                                                    int nrhs, int R) {
-  extern __shared__ double smem[];
-  __shared__ double zb[32 * 8];
-  const int s = list[blockIdx.x];
-  const SnDev d = sn[s];
-  const int m = d.m, k = d.k, c = m - k;
-  double* t = smem;
-  int* invp = reinterpret_cast<int*>(smem + static_cast<std::int64_t>(m) * R);
-  const F* P = panels + d.panel_off;
-  const std::int32_t* pl = pidx + d.first;
-  const std::int32_t* bst = blk + d.first;
-  const int nb = nblk[s];
-  const F* Linv = inv + d.inv_off;
-  for (int i = threadIdx.x; i < k; i += blockDim.x) invp[pl[i]] = i;
-  for (int r0 = 0; r0 < nrhs; r0 += R) {
-    const int rr = nrhs - r0 < R ? nrhs - r0 : R;
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < m * R; idx += blockDim.x) {
-      const int i = idx / R, r = idx % R;
-      double v = 0.0;
-      if (i < k && r < rr) v = x[d.first + pl[i] + (r0 + r) * n];
-      t[idx] = v;
-    }
-    __syncthreads();
-    for (int q = child_ptr[s]; q < child_ptr[s + 1]; ++q) {
-      const SnDev cd = sn[children[q]];
-      const int mc = cd.m - cd.k;
-      const std::int32_t* rm = rmap + cd.rmap_off;
-      const double* cv = vec + cd.vec_off * nrhs;
-      for (int a = threadIdx.x; a < mc; a += blockDim.x) {
-        const int pos = rm[a];
-        const int row = pos < k ? invp[pos] : pos;
-        for (int r = 0; r < rr; ++r) t[row * R + r] += cv[a + static_cast<std::int64_t>(r0 + r) * mc];
-      }
-      __syncthreads();
-    }
-    for (int bi = 0; bi < nb; ++bi) {
-      const int b = bst[bi];
-      const int be = bi + 1 < nb ? bst[bi + 1] : k;
-      const int bs = be - b;
-      const F* Li = Linv + static_cast<std::int64_t>(bi) * 1024;
-      // z_blk = Linv t_blk   (thread (i, r))
-      {
-        const int i = threadIdx.x % 32, r = threadIdx.x / 32;
-        if (i < bs && r < rr) {
-          double acc = 0.0;
-          for (int cc = 0; cc <= i; ++cc) acc += Li[cc * 32 + i] * t[(b + cc) * R + r];
-          zb[i * 8 + r] = acc;
-        }
-      }
-      __syncthreads();
-      {
-        const int i = threadIdx.x % 32, r = threadIdx.x / 32;
-        if (i < bs && r < rr) t[(b + i) * R + r] = zb[i * 8 + r];
-      }
-      // rows below: t_i -= L[i, blk] z_blk
-      for (int i = be + threadIdx.x; i < m; i += blockDim.x) {
-        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (int j = 0; j < bs; ++j) {
-          const double l = P[i + static_cast<std::int64_t>(b + j) * m];
-#pragma unroll
-          for (int r = 0; r < 8; ++r)
-            if (r < rr) acc[r] += l * zb[j * 8 + r];
-        }
-#pragma unroll
-        for (int r = 0; r < 8; ++r)
-          if (r < rr) t[i * R + r] -= acc[r];
-      }
-      __syncthreads();
-    }
-    for (int i = threadIdx.x; i < k; i += blockDim.x)
-      for (int r = 0; r < rr; ++r) x[d.first + pl[i] + (r0 + r) * n] = t[i * R + r];
-    double* v = vec + d.vec_off * nrhs;
-    for (int a = threadIdx.x; a < c; a += blockDim.x)
-      for (int r = 0; r < rr; ++r) v[a + static_cast<std::int64_t>(r0 + r) * c] = t[(k + a) * R + r];
-  }
-}
-
-// Diagonal solve D y = z, one CTA per front.
-template <class F>
-__global__ void k_solve_diag(const SnDev* sn, const F* panels, const signed char* piv, const std::int32_t* pidx,
-                             double* x, std::int64_t n, int nrhs) {
-  const SnDev d = sn[blockIdx.x];
-  const F* P = panels + d.panel_off;
-  for (int j = threadIdx.x; j < d.k; j += blockDim.x) {
-    const signed char ty = piv[d.first + j];
-    if (ty == 3) continue;
-    const std::int64_t g0 = d.first + pidx[d.first + j];
-    if (ty == 0 || ty < 0) {
-      for (int r = 0; r < nrhs; ++r) x[g0 + r * n] = 0.0;
-    } else if (ty == 1) {
-      const double dj = P[j + static_cast<std::int64_t>(j) * d.m];
-      for (int r = 0; r < nrhs; ++r) x[g0 + r * n] /= dj;
-    } else {
-      const std::int64_t g1 = d.first + pidx[d.first + j + 1];
-      const double a = P[j + static_cast<std::int64_t>(j) * d.m], b = P[j + 1 + static_cast<std::int64_t>(j) * d.m];
-      const double c = P[j + 1 + static_cast<std::int64_t>(j + 1) * d.m];
-      const double det = a * c - b * b;
-      for (int r = 0; r < nrhs; ++r) {
-        const double y0 = x[g0 + r * n], y1 = x[g1 + r * n];
-        x[g0 + r * n] = (c * y0 - b * y1) / det;
-        x[g1 + r * n] = (-b * y0 + a * y1) / det;
-      }
-    }
-  }
-}
 
 // Diagonal solve D y = z over all pivots at once (one thread per pivot position p): dpos[p] is the
 // panel index of D(p, p), pfirst[p] the first global column of p's front.
@@ -241,116 +81,6 @@ __global__ void k_solve_diag_flat(std::int64_t npiv, const std::int64_t* dpos, c
     }
   }
 }
-
-// Backward sweep of the listed fronts (ancestors done): right-looking over the blocks, last first.
-template <class F>
-__global__ void __launch_bounds__(256) k_solve_bwd(const std::int32_t* list, const SnDev* sn, const std::int32_t* rows,
-                                                    const F* panels, const std::int32_t* pidx,
-                                                    const std::int32_t* blk, const std::int32_t* nblk,
-                                                    const F* inv, double* x, std::int64_t n, int nrhs, int R) {
-  extern __shared__ double smem[];
-  __shared__ double zb[32 * 8];
-  const int s = list[blockIdx.x];
-  const SnDev d = sn[s];
-  const int m = d.m, k = d.k;
-  double* t = smem;
-  const F* P = panels + d.panel_off;
-  const std::int32_t* pl = pidx + d.first;
-  const std::int32_t* rw = rows + d.rows_off;
-  const std::int32_t* bst = blk + d.first;
-  const int nb = nblk[s];
-  const F* Linv = inv + d.inv_off;
-  for (int r0 = 0; r0 < nrhs; r0 += R) {
-    const int rr = nrhs - r0 < R ? nrhs - r0 : R;
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < m * R; idx += blockDim.x) {
-      const int i = idx / R, r = idx % R;
-      double v = 0.0;
-      if (r < rr) v = i < k ? x[d.first + pl[i] + (r0 + r) * n] : x[rw[i] + (r0 + r) * n];
-      t[idx] = v;
-    }
-    __syncthreads();
-    // t_j -= sum_{i >= k} L[i, j] t_i  (thread per column; the column is contiguous)
-    for (int j = threadIdx.x; j < k; j += blockDim.x) {
-      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      const F* Lj = P + static_cast<std::int64_t>(j) * m;
-      for (int i = k; i < m; ++i) {
-        const double l = Lj[i];
-#pragma unroll
-        for (int r = 0; r < 8; ++r)
-          if (r < rr) acc[r] += l * t[i * R + r];
-      }
-#pragma unroll
-      for (int r = 0; r < 8; ++r)
-        if (r < rr) t[j * R + r] -= acc[r];
-    }
-    __syncthreads();
-    for (int bi = nb - 1; bi >= 0; --bi) {
-      const int b = bst[bi];
-      const int be = bi + 1 < nb ? bst[bi + 1] : k;
-      const int bs = be - b;
-      const F* Li = Linv + static_cast<std::int64_t>(bi) * 1024;
-      // x_blk = Linv^T t_blk  (thread (c, r))
-      {
-        const int cc = threadIdx.x % 32, r = threadIdx.x / 32;
-        if (cc < bs && r < rr) {
-          double acc = 0.0;
-          for (int i = cc; i < bs; ++i) acc += Li[cc * 32 + i] * t[(b + i) * R + r];
-          zb[cc * 8 + r] = acc;
-        }
-      }
-      __syncthreads();
-      {
-        const int cc = threadIdx.x % 32, r = threadIdx.x / 32;
-        if (cc < bs && r < rr) t[(b + cc) * R + r] = zb[cc * 8 + r];
-      }
-      // earlier pivots: t_j -= sum_{i in blk} L[i, j] x_i  (thread per column j < b)
-      for (int j = threadIdx.x; j < b; j += blockDim.x) {
-        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        const F* Lj = P + static_cast<std::int64_t>(j) * m + b;
-        for (int i = 0; i < bs; ++i) {
-          const double l = Lj[i];
-#pragma unroll
-          for (int r = 0; r < 8; ++r)
-            if (r < rr) acc[r] += l * zb[i * 8 + r];
-        }
-#pragma unroll
-        for (int r = 0; r < 8; ++r)
-          if (r < rr) t[j * R + r] -= acc[r];
-      }
-      __syncthreads();
-    }
-    for (int i = threadIdx.x; i < k; i += blockDim.x)
-      for (int r = 0; r < rr; ++r) x[d.first + pl[i] + (r0 + r) * n] = t[i * R + r];
-  }
-}
-
-// ---------------------------------------------------------------- cooperative sweeps (few large fronts)
-//
-// The large fronts of the top levels are solved by super-blocks of kSB = 128 pivots. For a
-// super-block B = [b, b + bs) of a front with unit lower panel L (m x k, the 2 x 2 pivots'
-// coupling entries read as zero), the solve uses
-//     W[B, B]     = L_BB^{-1}                 (lower triangular, zero above the diagonal)
-//     W[i, B]     = L[i, B] L_BB^{-1},  i >= b + bs,
-// stored like the panel (column-major, ld m) in a separate buffer and built once per factorization
-// before its first solve. Then the forward sweep L z = t is, super-block by super-block,
-//     z_B = W[B, B] t_B,     t_i -= W[i, B] t_B  (i below B),
-// and the backward sweep L^T x = t is, from the last super-block to the first,
-//     x_B = s_B,             s_j -= W[B, j]^T x_B  (every earlier pivot j),
-// with s_j initialised to (W[A, A]^T t_A)_j - W[CB rows, j]^T x_CB for j in super-block A. Every
-// step of both sweeps is one grid barrier and one read of the W entries it needs; each row (forward)
-// or column (backward) is owned by one thread group per step, so no atomics are used and the sums
-// are formed in a fixed order.
-
-namespace {
-
-__device__ __forceinline__ int front_of(const std::int32_t* cta_start, int nfronts) {
-  int f = 0;
-  while (f + 1 < nfronts && cta_start[f + 1] <= static_cast<int>(blockIdx.x)) ++f;
-  return f;
-}
-
-}  // namespace
 
 // W[B, B] = L_BB^{-1} for one super-block per CTA: row-by-row substitution X[i, c] =
 // -sum_{c <= j < i} L[i, j] X[j, c] on packed triangles in shared memory (two threads per column).
@@ -447,16 +177,14 @@ __global__ void __launch_bounds__(256) k_sb_apply(const int4* tiles, const SnDev
   }
 }
 
-// The sweeps below synchronise their CTAs through per-front publication counters instead of grid
-// barriers: every 32-row group (forward) or 32-column chunk (backward) of a front has one owner CTA
-// for the whole sweep (group G, chunk c: CTA G mod nr, c mod nr). An owner that finishes the values
-// of the next super-block writes them, fences, and adds 1 to the front's counter; a CTA starts a
-// super-block step once the counter shows all of that super-block's groups. The waits are bounded:
-// a wait that runs out sets *err and the sweep goes on with whatever it reads (the host reports it).
-
 namespace {
 
 constexpr long long kSweepSpinLimit = 1LL << 22;
+constexpr int kTilePitch = 33;  // padded column pitch of a 32 x 32 W tile in shared memory
+constexpr int kRowPitch = 9;    // padded row pitch of a tile's right-hand sides
+constexpr int kWarpSmem = 32 * kTilePitch + 32 * kRowPitch;
+// backward sweep: one W tile and its right-hand-side rows per warp, then the step buffer
+constexpr std::size_t kBwdSmemBytes = sizeof(double) * (8 * kWarpSmem + kSB * 8);
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -464,25 +192,40 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
   return v;
 }
 
-// all threads: wait until *cnt >= target (thread 0 polls)
-__device__ __forceinline__ void wait_published(const int* cnt, int target, int* err) {
-  if (threadIdx.x == 0 && target > 0) {
+// thread 0 polls until *cnt >= target, then the whole CTA proceeds. The wait gives up, setting
+// *err, after kSweepSpinLimit polls or as soon as another wait has given up (the solve is then
+// reported invalid by the host).
+__device__ __forceinline__ void wait_count(const int* cnt, int target, int* err) {
+  if (threadIdx.x == 0) {
     long long it = 0;
     while (ld_acquire(cnt) < target) {
-      if (++it > kSweepSpinLimit) { atomicExch(err, 1); break; }
+      ++it;
+      if (it > kSweepSpinLimit || ((it & 255) == 0 && *reinterpret_cast<volatile int*>(err) != 0)) {
+        atomicExch(err, 1);
+        break;
+      }
       __nanosleep(32);
     }
   }
   __syncthreads();
 }
 
-// all threads, after their writes: make them visible, then count one publication
-__device__ __forceinline__ void publish(int* cnt) {
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) atomicAdd(cnt, 1);
+// all threads, after their writes: make them visible to the front's other CTAs and add `count` to
+// the front's counter. A front solved by one CTA only synchronizes its threads.
+__device__ __forceinline__ void publish(int* cnt, int count, int nr) {
+  if (nr > 1) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0 && count > 0) atomicAdd(cnt, count);
+  } else {
+    __syncthreads();
+  }
 }
 
+// groups / chunks g belong to CTA g mod nr: how many of `rank`'s lie below `hi`
+__device__ __forceinline__ int owned_below(int hi, int rank, int nr) { return hi > rank ? (hi - rank + nr - 1) / nr : 0; }
+
+// 32-row groups (32-column chunks) of super-block q of a front with k pivots
 __device__ __forceinline__ int sb_groups(int q, int k) {
   const int bs = min(kSB, k - q * kSB);
   return (bs + 31) / 32;
@@ -490,260 +233,304 @@ __device__ __forceinline__ int sb_groups(int q, int k) {
 
 }  // namespace
 
-// Forward sweep of the level's large fronts (front f owns CTAs [cta_start[f], cta_start[f+1])).
-// Each CTA first assembles the right-hand sides of its row groups: the pivot rows' entries of x plus
-// the children's contribution vectors, listed per front position in child order (cptr / cent).
-// In super-block step q the owner of row group G >= 4q forms the group's 32 rows of W[:, B] t_B:
-// its 8 warps split the super-block's columns (16 each, lane = row) and add their partial sums in
-// shared memory in warp order. Rows of B give z_B (written to x), rows below update t; the CB rows
-// write their final values to the front's contribution vector in the last step.
+// Forward sweep of one level. t (the front's rows, t[i * 8 + r]) lives in the work array.
+// Assembly: each owned row gathers its pivot entry of x and its children's contributions (listed per
+// front position in child order: cptr / cent). Step q: the owned groups at or below super-block q
+// form their rows of W[:, B] t_B - one warp per group when the CTA has at least four groups, else the
+// eight warps share each group's columns and add their partial sums in warp order. Rows of B give
+// z_B (written to x), rows below update t, and at the last step the contribution rows go to the
+// front's contribution vector.
 template <class F>
-__global__ void __launch_bounds__(256, 2) k_solve_fwd_coop(const std::int32_t* list, const std::int32_t* cta_start,
-                                                            int nfronts, const SnDev* sn, const std::int32_t* cptr,
-                                                            const ContribEntry* cent, const F* W,
-                                                            const std::int32_t* pidx, double* x, std::int64_t n,
-                                                            double* vec, int nrhs, double* work,
-                                                            const std::int64_t* work_off, int* cnts, int* err) {
+__global__ void __launch_bounds__(256, 2) k_fwd_level(const SolveTask* tasks, const SnDev* sn, const std::int32_t* cptr,
+                                                       const ContribEntry* cent, const F* W,
+                                                       const std::int32_t* pidx, double* x, std::int64_t n,
+                                                       double* vec, int nrhs, double* work, int* cnts, int* err) {
   __shared__ double tb[kSB * 8];
   __shared__ double red[8][32][9];
-  const int f = front_of(cta_start, nfronts);
-  const int rank = static_cast<int>(blockIdx.x) - cta_start[f];
-  const int nr = cta_start[f + 1] - cta_start[f];
-  const int s = list[f];
-  const SnDev d = sn[s];
-  const int m = d.m, k = d.k, c = m - k;
-  double* t = work + work_off[f];  // t[r * m + i]
-  int* cnt = cnts + f;
+  const SolveTask tk = tasks[blockIdx.x];
+  const SnDev d = sn[tk.s];
+  const int m = d.m, k = d.k, c = m - k, rank = tk.rank, nr = tk.nr;
+  double* t = work + tk.wofs;
+  int* cnt = cnts + tk.s;
   const F* Wf = W + d.w_off;
   const std::int32_t* pl = pidx + d.first;
   const std::int32_t* cp = cptr + d.cptr_off;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row = threadIdx.x >> 3, rr = threadIdx.x & 7;
   double* v = vec + d.vec_off * nrhs;
-  const int nsb = (k + kSB - 1) / kSB;
-  const int ngt = (m + 31) / 32;
-  // assemble the owned row groups; the groups of super-block 0 are published
-  for (int G = rank; G < ngt; G += nr) {
-    const int i = G * 32 + row;
-    if (i < m && rr < nrhs) {
-      const int pos = i < k ? pl[i] : i;
-      double val = i < k ? x[d.first + pos + static_cast<std::int64_t>(rr) * n] : 0.0;
-      for (int e = cp[pos]; e < cp[pos + 1]; ++e) {
-        const ContribEntry ce = cent[e];
-        val += vec[ce.vec_off * nrhs + ce.a + static_cast<std::int64_t>(rr) * ce.mc];
-      }
-      t[rr * m + i] = val;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nsb = (k + kSB - 1) / kSB, ngt = (m + 31) / 32;
+  const int nown = owned_below(ngt, rank, nr);
+  for (int idx = threadIdx.x; idx < nown * 32; idx += blockDim.x) {
+    const int i = (rank + (idx >> 5) * nr) * 32 + (idx & 31);
+    if (i >= m) continue;
+    const int pos = i < k ? pl[i] : i;
+    double val[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+      val[r] = (i < k && r < nrhs) ? x[d.first + pos + static_cast<std::int64_t>(r) * n] : 0.0;
+    const int e1 = cp[pos + 1];
+    for (int e = cp[pos]; e < e1; ++e) {
+      const ContribEntry ce = cent[e];
+      const double* src = vec + ce.vec_off * nrhs + ce.a;
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+        if (r < nrhs) val[r] += src[static_cast<std::int64_t>(r) * ce.mc];
     }
-    if (G < sb_groups(0, k)) publish(cnt);
+    if (nsb == 0) {  // no pivots: the rows pass to the parent unchanged
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+        if (r < nrhs) v[(i - k) + static_cast<std::int64_t>(r) * c] = val[r];
+    } else {
+#pragma unroll
+      for (int r = 0; r < 8; ++r) t[static_cast<std::int64_t>(i) * 8 + r] = val[r];
+    }
   }
+  if (nsb == 0) return;
+  publish(cnt, owned_below(sb_groups(0, k), rank, nr), nr);
   int target = 0;
   for (int q = 0; q < nsb; ++q) {
     const int b = q * kSB, be = min(b + kSB, k), bs = be - b;
     target += sb_groups(q, k);
-    int G = rank;
-    if (G < b / 32) G += ((b / 32 - G + nr - 1) / nr) * nr;
-    if (G >= ngt) break;  // no rows left for this CTA
+    const int g0 = owned_below(b / 32, rank, nr);
+    const int ng = nown - g0;  // owned groups at or below super-block q (uniform over the CTA)
+    if (ng <= 0) break;
     const bool last = q + 1 == nsb;
     const int nb0 = (q + 1) * (kSB / 32), nb1 = last ? nb0 : nb0 + sb_groups(q + 1, k);
-    // prefetch the first group's W entries and the old values it updates (no dependence on the wait)
-    const int j0 = warp * 16;
-    double wv[16];
-    {
-      const int i = G * 32 + lane;
-#pragma unroll
-      for (int jj = 0; jj < 16; ++jj)
-        wv[jj] = (i < m && j0 + jj < bs) ? Wf[i + static_cast<std::int64_t>(b + j0 + jj) * m] : 0.0;
-    }
-    double told = 0.0;
-    int plz = 0;
-    {
-      const int ii = G * 32 + row;
-      if (ii >= be && ii < m && rr < nrhs) told = __ldcg(&t[rr * m + ii]);
-      if (ii < be) plz = pl[ii];
-    }
-    wait_published(cnt, target, err);
+    if (nr > 1) wait_count(cnt, target, err);
     for (int idx = threadIdx.x; idx < kSB * 8; idx += blockDim.x) {
-      const int j = idx >> 3, r = idx & 7;
-      tb[idx] = (j < bs && r < nrhs) ? __ldcg(&t[r * m + b + j]) : 0.0;
+      const int j = idx >> 3;
+      tb[idx] = j < bs ? __ldcg(&t[static_cast<std::int64_t>(b + j) * 8 + (idx & 7)]) : 0.0;
     }
     __syncthreads();
-    for (bool first = true; G < ngt; G += nr, first = false) {
-      const int i = G * 32 + lane;
-      if (!first) {
+    if (ng >= 4) {
+      for (int gi = warp; gi < ng; gi += 8) {
+        const int i = (rank + (g0 + gi) * nr) * 32 + lane;
+        if (i >= m) continue;
+        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        const F* Wi = Wf + i + static_cast<std::int64_t>(b) * m;
+        for (int j0 = 0; j0 < bs; j0 += 8) {
+          double wv[8];
 #pragma unroll
-        for (int jj = 0; jj < 16; ++jj)
-          wv[jj] = (i < m && j0 + jj < bs) ? Wf[i + static_cast<std::int64_t>(b + j0 + jj) * m] : 0.0;
-        const int ii = G * 32 + row;
-        told = (ii >= be && ii < m && rr < nrhs) ? __ldcg(&t[rr * m + ii]) : 0.0;
-        plz = ii < be ? pl[ii] : 0;
-      }
-      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+          for (int u = 0; u < 8; ++u)
+            wv[u] = j0 + u < bs ? static_cast<double>(Wi[static_cast<std::int64_t>(j0 + u) * m]) : 0.0;
 #pragma unroll
-      for (int jj = 0; jj < 16; ++jj)
+          for (int u = 0; u < 8; ++u)
 #pragma unroll
-        for (int r = 0; r < 8; ++r) acc[r] = fma(wv[jj], tb[(j0 + jj) * 8 + r], acc[r]);
+            for (int r = 0; r < 8; ++r) acc[r] = fma(wv[u], tb[(j0 + u) * 8 + r], acc[r]);
+        }
+        double* ti = t + static_cast<std::int64_t>(i) * 8;
+        if (i < be) {
 #pragma unroll
-      for (int r = 0; r < 8; ++r) red[warp][lane][r] = acc[r];
-      __syncthreads();
-      {
-        const int ii = G * 32 + row;
-        if (ii < m && rr < nrhs) {
-          double val = 0.0;
+          for (int r = 0; r < 8; ++r)
+            if (r < nrhs) x[d.first + pl[i] + static_cast<std::int64_t>(r) * n] = acc[r];
+        } else if (last && i >= k) {
 #pragma unroll
-          for (int w = 0; w < 8; ++w) val += red[w][row][rr];
-          if (ii < be) {
-            x[d.first + plz + static_cast<std::int64_t>(rr) * n] = val;
-          } else {
-            const double nv = told - val;
-            if (last && ii >= k) v[(ii - k) + static_cast<std::int64_t>(rr) * c] = nv;
-            else t[rr * m + ii] = nv;
-          }
+          for (int r = 0; r < 8; ++r)
+            if (r < nrhs) v[(i - k) + static_cast<std::int64_t>(r) * c] = __ldcg(&ti[r]) - acc[r];
+        } else {
+#pragma unroll
+          for (int r = 0; r < 8; ++r) ti[r] = __ldcg(&ti[r]) - acc[r];
         }
       }
-      if (G >= nb0 && G < nb1) publish(cnt);  // rows of the next super-block are final
-      else __syncthreads();
+    } else {
+      const int j0 = warp * 16;
+      for (int gi = 0; gi < ng; ++gi) {
+        const int G = rank + (g0 + gi) * nr;
+        const int i = G * 32 + lane;
+        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (i < m) {
+          double wv[16];
+#pragma unroll
+          for (int u = 0; u < 16; ++u)
+            wv[u] = j0 + u < bs ? static_cast<double>(Wf[i + static_cast<std::int64_t>(b + j0 + u) * m]) : 0.0;
+#pragma unroll
+          for (int u = 0; u < 16; ++u)
+#pragma unroll
+            for (int r = 0; r < 8; ++r) acc[r] = fma(wv[u], tb[(j0 + u) * 8 + r], acc[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) red[warp][lane][r] = acc[r];
+        __syncthreads();
+        {
+          const int row = threadIdx.x >> 3, rr = threadIdx.x & 7;
+          const int ii = G * 32 + row;
+          if (ii < m) {
+            double val = 0.0;
+#pragma unroll
+            for (int w = 0; w < 8; ++w) val += red[w][row][rr];
+            double* tr = t + static_cast<std::int64_t>(ii) * 8 + rr;
+            if (ii < be) {
+              if (rr < nrhs) x[d.first + pl[ii] + static_cast<std::int64_t>(rr) * n] = val;
+            } else if (last && ii >= k) {
+              if (rr < nrhs) v[(ii - k) + static_cast<std::int64_t>(rr) * c] = __ldcg(tr) - val;
+            } else {
+              *tr = __ldcg(tr) - val;
+            }
+          }
+        }
+        __syncthreads();
+      }
     }
+    publish(cnt, owned_below(nb1, rank, nr) - owned_below(nb0, rank, nr), nr);
   }
 }
 
-// Backward sweep of the level's large fronts. Columns are owned by groups of 8 lanes (4 per warp,
-// 32 consecutive columns per CTA and round); a group reduces its column's dot products over its
-// lanes with shuffles. Super-blocks are processed from the last to the first; the owners of the
-// next super-block's columns write x there and publish.
+// Backward sweep of one level. sv (s_j, sv[j * 8 + r]) and ta (the front's pivot rows of x on entry,
+// ta[i * 8 + r]) live in the work array. (1) Each CTA copies the pivot rows of its chunks to ta; once
+// every CTA of the front has done so, the front's pivot rows of x are only written (final values).
+// (2) For each owned chunk, s_j over rows A and CB: 32 x 32 tiles of W, one tile per warp at a time,
+// staged in shared memory so that lane c forms column c's sums (no shuffles), warps added in order.
+// (3) From the last super-block down: the owners of the columns below super-block B apply x_B; the
+// owners of the next super-block's columns write their final x and publish.
 template <class F>
-__global__ void __launch_bounds__(256, 2) k_solve_bwd_coop(const std::int32_t* list, const std::int32_t* cta_start,
-                                                            int nfronts, const SnDev* sn, const std::int32_t* rows,
-                                                            const F* W, const std::int32_t* pidx, double* x,
-                                                            std::int64_t n, int nrhs, double* work,
-                                                            const std::int64_t* work_off, int* cnts, int* err) {
-  namespace cg = cooperative_groups;
-  cg::grid_group grid = cg::this_grid();
-  __shared__ double xb[kSB * 8];
-  const int f = front_of(cta_start, nfronts);
-  const int rank = static_cast<int>(blockIdx.x) - cta_start[f];
-  const int nr = cta_start[f + 1] - cta_start[f];
-  const int s = list[f];
-  const SnDev d = sn[s];
-  const int m = d.m, k = d.k;
-  double* t = work + work_off[f];                              // t[r * m + i]
-  double* sv = t + static_cast<std::int64_t>(8) * m;           // sv[r * k + j]
-  int* cnt = cnts + f;
+__global__ void __launch_bounds__(256, 2) k_bwd_level(const SolveTask* tasks, const SnDev* sn, const std::int32_t* rows,
+                                                       const F* W, const std::int32_t* pidx, double* x,
+                                                       std::int64_t n, int nrhs, double* work, int* cnts,
+                                                       int* arrive, int* err) {
+  extern __shared__ double dsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* wt = dsm + warp * kWarpSmem;     // wt[c * kTilePitch + i]: W[i0 + i, j0 + c]
+  double* tt = wt + 32 * kTilePitch;       // tt[i * kRowPitch + r]: the tile's rows, signed
+  double* xb = dsm + 8 * kWarpSmem;        // xb[r * kSB + i]: x of the super-block being applied
+  double* red = dsm;                       // [8][32][9] partial sums, over the tiles once they are used
+  const SolveTask tk = tasks[blockIdx.x];
+  const SnDev d = sn[tk.s];
+  const int m = d.m, k = d.k, rank = tk.rank, nr = tk.nr;
+  if (k == 0) return;
+  double* sv = work + tk.wofs;
+  double* ta = sv + static_cast<std::int64_t>(k) * 8;
+  int* cnt = cnts + tk.s;
   const F* Wf = W + d.w_off;
   const std::int32_t* pl = pidx + d.first;
   const std::int32_t* rw = rows + d.rows_off;
-  const int gt = rank * blockDim.x + threadIdx.x, gs = nr * blockDim.x;
-  const int sub = threadIdx.x & 7, gsub = (threadIdx.x >> 3) & 3;
-  const int wbase = rank * 32 + (threadIdx.x >> 5) * 4, ngrp = nr * 32;
-  const int nsb = (k + kSB - 1) / kSB;
-  for (int i = gt; i < m; i += gs)
-    for (int r = 0; r < nrhs; ++r)
-      t[r * m + i] = i < k ? x[d.first + pl[i] + static_cast<std::int64_t>(r) * n] : x[rw[i] + static_cast<std::int64_t>(r) * n];
-  grid.sync();
-  // sv_j = (W[A, A]^T t_A)_j - W[k:m, j]^T t[k:m] for j in super-block A, 128-row chunks of t
-  // staged in shared memory (W is zero above the diagonal of W[A, A]); the last super-block's x
-  // is final already. Rounds c0 are 32-column chunks, uniform over the CTA.
-  const int blast = (nsb - 1) * kSB;
-  for (int c0 = rank * 32; c0 < k; c0 += ngrp) {
-    const int j = c0 + (threadIdx.x >> 3);
-    const int bA = (c0 / kSB) * kSB;
+  const int nsb = (k + kSB - 1) / kSB, nch = (k + 31) / 32;
+  const int nown = owned_below(nch, rank, nr);
+  for (int idx = threadIdx.x; idx < nown * 32; idx += blockDim.x) {
+    const int i = (rank + (idx >> 5) * nr) * 32 + (idx & 31);
+    if (i >= k) continue;
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+      ta[static_cast<std::int64_t>(i) * 8 + r] = r < nrhs ? x[d.first + pl[i] + static_cast<std::int64_t>(r) * n] : 0.0;
+  }
+  if (nr > 1) {
+    publish(arrive + tk.s, 1, nr);
+    wait_count(arrive + tk.s, nr, err);
+  } else {
+    __syncthreads();
+  }
+  const int lastb = (nsb - 1) * kSB;
+  for (int u = 0; u < nown; ++u) {
+    const int j0 = (rank + u * nr) * 32;
+    const int bA = (j0 / kSB) * kSB, beA = min(bA + kSB, k);
+    const int t1 = (beA - bA + 31) / 32, t2 = (m - k + 31) / 32;
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int i0 = bA, chunk = 0; i0 < m; ++chunk) {
-      const int i1 = chunk == 0 ? min(bA + kSB, k) : min(i0 + kSB, m);
-      const double sg = chunk == 0 ? 1.0 : -1.0;
-      double wv[16];
-      const F* Wj = Wf + i0 + static_cast<std::int64_t>(j) * m;
+    for (int tau = warp; tau < t1 + t2; tau += 8) {
+      const bool own = tau < t1;
+      const int i = (own ? bA + 32 * tau : k + 32 * (tau - t1)) + lane;
+      const bool ok = i < (own ? beA : m);
+      const F* Wi = Wf + i + static_cast<std::int64_t>(j0) * m;
+      double wv[32];
 #pragma unroll
-      for (int u = 0; u < 16; ++u) wv[u] = (j < k && i0 + sub + 8 * u < i1) ? sg * Wj[sub + 8 * u] : 0.0;
-      __syncthreads();
-      for (int idx = threadIdx.x; idx < kSB * 8; idx += blockDim.x) {
-        const int r = idx / kSB, i = idx % kSB;
-        xb[idx] = (i0 + i < i1 && r < nrhs) ? __ldcg(&t[r * m + i0 + i]) : 0.0;
+      for (int cc = 0; cc < 32; ++cc)
+        wv[cc] = (ok && j0 + cc < k) ? static_cast<double>(Wi[static_cast<std::int64_t>(cc) * m]) : 0.0;
+      double rv[8];
+      if (ok && own) {
+        const double* ti = ta + static_cast<std::int64_t>(i) * 8;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) rv[r] = __ldcg(&ti[r]);
+      } else if (ok) {
+        const std::int64_t g = rw[i];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) rv[r] = r < nrhs ? -x[g + static_cast<std::int64_t>(r) * n] : 0.0;
+      } else {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) rv[r] = 0.0;
       }
-      __syncthreads();
 #pragma unroll
-      for (int u = 0; u < 16; ++u)
+      for (int cc = 0; cc < 32; ++cc) wt[cc * kTilePitch + lane] = wv[cc];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) acc[r] = fma(wv[u], xb[r * kSB + sub + 8 * u], acc[r]);
-      i0 = chunk == 0 ? k : i1;
+      for (int r = 0; r < 8; ++r) tt[lane * kRowPitch + r] = rv[r];
+      __syncwarp();
+#pragma unroll 8
+      for (int ii = 0; ii < 32; ++ii) {
+        const double w = wt[lane * kTilePitch + ii];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) acc[r] = fma(w, tt[ii * kRowPitch + r], acc[r]);
+      }
+      __syncwarp();
     }
+    __syncthreads();  // every warp is done with its tiles: red overlays them
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 4);
-      acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 2);
-      acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 1);
-    }
-    if (j < k && sub < nrhs) {
-      double a = acc[0];
+    for (int r = 0; r < 8; ++r) red[(warp * 32 + lane) * 9 + r] = acc[r];
+    __syncthreads();
+    const bool fin = bA == lastb;  // the last super-block: s is x
+    {
+      const int cc = threadIdx.x >> 3, r = threadIdx.x & 7, j = j0 + cc;
+      double s = 0.0;
 #pragma unroll
-      for (int r = 1; r < 8; ++r)
-        if (sub == r) a = acc[r];
-      sv[sub * k + j] = a;
-      if (j >= blast) x[d.first + pl[j] + static_cast<std::int64_t>(sub) * n] = a;
+      for (int w = 0; w < 8; ++w) s += red[(w * 32 + cc) * 9 + r];
+      if (j < k) {
+        sv[static_cast<std::int64_t>(j) * 8 + r] = s;
+        if (fin && r < nrhs) x[d.first + pl[j] + static_cast<std::int64_t>(r) * n] = s;
+      }
     }
-    if (c0 >= blast) publish(cnt);  // this CTA's 32 columns of the last super-block are final
-    else __syncthreads();
+    publish(cnt, fin ? 1 : 0, nr);
   }
   int target = 0;
-  for (int step = 0; step < nsb; ++step) {
-    const int q = nsb - 1 - step;
-    const int b = q * kSB, be = min(b + kSB, k), bs = be - b;
+  const int sub = threadIdx.x & 7, col = threadIdx.x >> 3;  // 8 lanes per column, 32 columns per chunk
+  for (int q = nsb - 1; q >= 1; --q) {
+    const int b = q * kSB, bs = min(kSB, k - b);
     target += sb_groups(q, k);
-    if (wbase >= b) break;  // no columns left for this CTA (uniform: b is a multiple of 32)
-    const int bprev = b - kSB;  // columns of the next super-block: [bprev, b)
-    // the CTA's column chunks below b are updated from the highest down: the next super-block's
-    // columns (the highest ones) are finished and published first, so the next step can start
-    // while the rest of the update runs (every column has one owner, so nothing else reads it)
-    const int top = wbase + ((b - 1 - wbase) / ngrp) * ngrp;  // uniform over the CTA
-    // prefetch the first column's W entries and old value
-    int j = top + gsub;
+    const int nlow = owned_below(b / 32, rank, nr);
+    if (nlow == 0) break;  // uniform over the CTA
+    // the first chunk's W entries and old values do not depend on the wait
+    int u = nlow - 1;
+    int j = (rank + u * nr) * 32 + col;
     double wv[16];
     {
       const F* Wj = Wf + b + static_cast<std::int64_t>(j) * m;
 #pragma unroll
-      for (int u = 0; u < 16; ++u) wv[u] = (j < b && sub + 8 * u < bs) ? Wj[sub + 8 * u] : 0.0;
+      for (int e = 0; e < 16; ++e) wv[e] = sub + 8 * e < bs ? static_cast<double>(Wj[sub + 8 * e]) : 0.0;
     }
-    double sold = (j < b && sub < nrhs) ? __ldcg(&sv[sub * k + j]) : 0.0;
-    int plj = (j < b && j >= bprev) ? pl[j] : 0;
-    wait_published(cnt, target, err);
+    if (nr > 1) wait_count(cnt, target, err);
     for (int idx = threadIdx.x; idx < kSB * 8; idx += blockDim.x) {
-      const int r = idx / kSB, i = idx % kSB;  // xb[r * kSB + i]: conflict-free reads below
-      xb[idx] = (i < bs && r < nrhs) ? __ldcg(&sv[r * k + b + i]) : 0.0;
+      const int r = idx / kSB, i = idx % kSB;
+      xb[idx] = i < bs ? __ldcg(&sv[static_cast<std::int64_t>(b + i) * 8 + r]) : 0.0;
     }
     __syncthreads();
-    for (int base = top; base >= wbase; base -= ngrp) {
-      j = base + gsub;
-      if (base != top) {
-        const F* Wj = Wf + b + static_cast<std::int64_t>(j) * m;
-#pragma unroll
-        for (int u = 0; u < 16; ++u) wv[u] = (j < b && sub + 8 * u < bs) ? Wj[sub + 8 * u] : 0.0;
-        sold = (j < b && sub < nrhs) ? __ldcg(&sv[sub * k + j]) : 0.0;
-        plj = (j < b && j >= bprev) ? pl[j] : 0;
-      }
+    for (;;) {
       double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
-      for (int u = 0; u < 16; ++u)
+      for (int e = 0; e < 16; ++e)
 #pragma unroll
-        for (int r = 0; r < 8; ++r) acc[r] = fma(wv[u], xb[r * kSB + sub + 8 * u], acc[r]);
+        for (int r = 0; r < 8; ++r) acc[r] = fma(wv[e], xb[r * kSB + sub + 8 * e], acc[r]);
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
         acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 4);
         acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 2);
         acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], 1);
       }
-      if (j < b && sub < nrhs) {
-        double a = acc[0];
+      double a = acc[0];
 #pragma unroll
-        for (int r = 1; r < 8; ++r)
-          if (sub == r) a = acc[r];
-        const double nv = sold - a;
-        sv[sub * k + j] = nv;
-        if (j >= bprev) x[d.first + plj + static_cast<std::int64_t>(sub) * n] = nv;
+      for (int r = 1; r < 8; ++r)
+        if (sub == r) a = acc[r];
+      double* sj = sv + static_cast<std::int64_t>(j) * 8 + sub;
+      const double nv = __ldcg(sj) - a;
+      *sj = nv;
+      const bool next = j - col >= b - kSB;  // the chunk lies in super-block q - 1: final now
+      if (next) {
+        if (sub < nrhs) x[d.first + pl[j] + static_cast<std::int64_t>(sub) * n] = nv;
+        publish(cnt, 1, nr);
       }
-      if (base >= bprev) publish(cnt);  // this CTA's 32 columns of the next super-block are final
-      else __syncthreads();
+      if (--u < 0) break;
+      j = (rank + u * nr) * 32 + col;
+      const F* Wj = Wf + b + static_cast<std::int64_t>(j) * m;
+#pragma unroll
+      for (int e = 0; e < 16; ++e) wv[e] = sub + 8 * e < bs ? static_cast<double>(Wj[sub + 8 * e]) : 0.0;
     }
+    __syncthreads();  // xb is rewritten by the next step
   }
 }
+
 
 void launch_gather_scale(std::int64_t n, int nrhs, const double* b, std::int64_t ldb, const double* d,
                          const std::int32_t* iperm, double* x, cudaStream_t s) {
@@ -761,42 +548,6 @@ void launch_scatter_scale(std::int64_t n, int nrhs, double* b, std::int64_t ldb,
   k_scatter_scale<<<blocks, 256, 0, s>>>(n, nrhs, b, ldb, d, iperm, x);
 }
 
-static std::size_t solve_smem(int maxm, int R) {
-  return static_cast<std::size_t>(maxm) * R * sizeof(double) + static_cast<std::size_t>(maxm) * sizeof(int);
-}
-
-int solve_rhs_chunk(int maxm, int nrhs) {
-  int R = nrhs < 8 ? nrhs : 8;  // the kernels carry at most 8 right-hand sides
-  while (R > 1 && solve_smem(maxm, R) > kSolveSmemMax) --R;
-  return R < 1 ? 1 : R;
-}
-
-template <class F>
-void launch_inv_blocks(int ns, const SnDev* sn, const F* panels, const signed char* piv, std::int32_t* blk,
-                       std::int32_t* nblk, F* inv, cudaStream_t s) {
-  if (ns <= 0) return;
-  note_launches(1);
-  k_inv_blocks<F><<<ns, 256, 0, s>>>(sn, panels, piv, blk, nblk, inv);
-}
-
-template <class F>
-void launch_solve_fwd(const std::int32_t* list, int nlist, int maxm, const SnDev* sn, const std::int32_t* child_ptr,
-                      const std::int32_t* children, const std::int32_t* rmap, const F* panels,
-                      const signed char* piv, const std::int32_t* pidx, const std::int32_t* blk,
-                      const std::int32_t* nblk, const F* inv, double* x, std::int64_t n, double* vec, int nrhs,
-                      cudaStream_t s) {
-  if (nlist <= 0) return;
-  const int R = solve_rhs_chunk(maxm, nrhs);
-  const std::size_t smem = solve_smem(maxm, R);
-  static std::once_flag configured;
-  std::call_once(configured, [&] {
-    cudaFuncSetAttribute(k_solve_fwd<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSolveSmemMax));
-  });
-  note_launches(1);
-  k_solve_fwd<F><<<nlist, 256, smem, s>>>(list, sn, child_ptr, children, rmap, panels, piv, pidx, blk, nblk, inv, x, n,
-                                          vec, nrhs, R);
-}
-
 template <class F>
 void launch_solve_diag_flat(std::int64_t npiv, const std::int64_t* dpos, const std::int32_t* pfirst, const F* panels,
                             const signed char* piv, const std::int32_t* pidx, double* x, std::int64_t n, int nrhs,
@@ -807,41 +558,27 @@ void launch_solve_diag_flat(std::int64_t npiv, const std::int64_t* dpos, const s
                                                                                 x, n, nrhs);
 }
 
-template <class F>
-void launch_solve_diag(int ns, const SnDev* sn, const F* panels, const signed char* piv, const std::int32_t* pidx,
-                       double* x, std::int64_t n, int nrhs, cudaStream_t s) {
-  if (ns <= 0) return;
-  note_launches(1);
-  k_solve_diag<F><<<ns, 128, 0, s>>>(sn, panels, piv, pidx, x, n, nrhs);
-}
-
-template <class F>
-void launch_solve_bwd(const std::int32_t* list, int nlist, int maxm, const SnDev* sn, const std::int32_t* rows,
-                      const F* panels, const std::int32_t* pidx, const std::int32_t* blk, const std::int32_t* nblk,
-                      const F* inv, double* x, std::int64_t n, int nrhs, cudaStream_t s) {
-  if (nlist <= 0) return;
-  const int R = solve_rhs_chunk(maxm, nrhs);
-  const std::size_t smem = solve_smem(maxm, R);
-  static std::once_flag configured;
-  std::call_once(configured, [&] {
-    cudaFuncSetAttribute(k_solve_bwd<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSolveSmemMax));
-  });
-  note_launches(1);
-  k_solve_bwd<F><<<nlist, 256, smem, s>>>(list, sn, rows, panels, pidx, blk, nblk, inv, x, n, nrhs, R);
-}
-
 namespace {
 template <class F>
+void configure_bwd() {
+  static std::once_flag configured;
+  std::call_once(configured, [] {
+    cudaFuncSetAttribute(k_bwd_level<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kBwdSmemBytes));
+  });
+}
+
+template <class F>
 int solve_coop_max_of(int device) {
+  configure_bwd<F>();
   int a = 0, b = 0, sms = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_solve_fwd_coop<F>, 256, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_solve_bwd_coop<F>, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_fwd_level<F>, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_bwd_level<F>, 256, kBwdSmemBytes);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   return (a < b ? a : b) * sms;
 }
 }  // namespace
 
-// co-resident CTAs of the cooperative sweeps, valid for both factor types
+// co-resident CTAs of the sweep kernels, valid for both factor types
 int solve_coop_max_ctas(int device) {
   const int a = solve_coop_max_of<double>(device), b = solve_coop_max_of<float>(device);
   return a < b ? a : b;
@@ -865,51 +602,47 @@ void launch_sb_build(const int2* sbl, int nsb, const int4* tiles, int ntiles, co
 }
 
 template <class F>
-cudaError_t launch_solve_fwd_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
-                                  const SnDev* sn, const std::int32_t* cptr, const ContribEntry* cent, const F* W,
-                                  const std::int32_t* pidx, double* x, std::int64_t n, double* vec, int nrhs,
-                                  double* work, const std::int64_t* work_off, int* cnts, int* err, cudaStream_t s) {
-  void* args[] = {&list, &cta_start, &nfronts, &sn, &cptr, &cent, &W, &pidx, &x, &n, &vec, &nrhs, &work, &work_off,
-                  &cnts, &err};
+cudaError_t launch_fwd_level(const SolveTask* tasks, int nctas, bool coop, const SnDev* sn, const std::int32_t* cptr,
+                             const ContribEntry* cent, const F* W, const std::int32_t* pidx, double* x, std::int64_t n,
+                             double* vec, int nrhs, double* work, int* cnts, int* err, cudaStream_t s) {
+  if (nctas <= 0) return cudaSuccess;
   note_launches(1);
-  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_solve_fwd_coop<F>), dim3(nctas), dim3(256), args, 0, s);
+  if (!coop) {
+    k_fwd_level<F><<<nctas, 256, 0, s>>>(tasks, sn, cptr, cent, W, pidx, x, n, vec, nrhs, work, cnts, err);
+    return cudaGetLastError();
+  }
+  void* args[] = {&tasks, &sn, &cptr, &cent, &W, &pidx, &x, &n, &vec, &nrhs, &work, &cnts, &err};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_fwd_level<F>), dim3(nctas), dim3(256), args, 0, s);
 }
 
 template <class F>
-cudaError_t launch_solve_bwd_coop(const std::int32_t* list, const std::int32_t* cta_start, int nfronts, int nctas,
-                                  const SnDev* sn, const std::int32_t* rows, const F* W, const std::int32_t* pidx,
-                                  double* x, std::int64_t n, int nrhs, double* work, const std::int64_t* work_off,
-                                  int* cnts, int* err, cudaStream_t s) {
-  void* args[] = {&list, &cta_start, &nfronts, &sn, &rows, &W, &pidx, &x, &n, &nrhs, &work, &work_off, &cnts, &err};
+cudaError_t launch_bwd_level(const SolveTask* tasks, int nctas, bool coop, const SnDev* sn, const std::int32_t* rows,
+                             const F* W, const std::int32_t* pidx, double* x, std::int64_t n, int nrhs, double* work,
+                             int* cnts, int* arrive, int* err, cudaStream_t s) {
+  if (nctas <= 0) return cudaSuccess;
+  configure_bwd<F>();
   note_launches(1);
-  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_solve_bwd_coop<F>), dim3(nctas), dim3(256), args, 0, s);
+  if (!coop) {
+    k_bwd_level<F><<<nctas, 256, kBwdSmemBytes, s>>>(tasks, sn, rows, W, pidx, x, n, nrhs, work, cnts, arrive, err);
+    return cudaGetLastError();
+  }
+  void* args[] = {&tasks, &sn, &rows, &W, &pidx, &x, &n, &nrhs, &work, &cnts, &arrive, &err};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_bwd_level<F>), dim3(nctas), dim3(256), args,
+                                     kBwdSmemBytes, s);
 }
 
 #define HSG_SOLVE_INSTANTIATE(F)                                                                                       \
-  template void launch_inv_blocks<F>(int, const SnDev*, const F*, const signed char*, std::int32_t*, std::int32_t*,   \
-                                     F*, cudaStream_t);                                                                \
-  template void launch_solve_fwd<F>(const std::int32_t*, int, int, const SnDev*, const std::int32_t*,                 \
-                                    const std::int32_t*, const std::int32_t*, const F*, const signed char*,            \
-                                    const std::int32_t*, const std::int32_t*, const std::int32_t*, const F*, double*,  \
-                                    std::int64_t, double*, int, cudaStream_t);                                         \
   template void launch_solve_diag_flat<F>(std::int64_t, const std::int64_t*, const std::int32_t*, const F*,          \
                                           const signed char*, const std::int32_t*, double*, std::int64_t, int,        \
                                           cudaStream_t);                                                               \
-  template void launch_solve_diag<F>(int, const SnDev*, const F*, const signed char*, const std::int32_t*, double*,   \
-                                     std::int64_t, int, cudaStream_t);                                                 \
-  template void launch_solve_bwd<F>(const std::int32_t*, int, int, const SnDev*, const std::int32_t*, const F*,      \
-                                    const std::int32_t*, const std::int32_t*, const std::int32_t*, const F*, double*,  \
-                                    std::int64_t, int, cudaStream_t);                                                  \
   template void launch_sb_build<F>(const int2*, int, const int4*, int, const SnDev*, const F*, const signed char*,    \
                                    F*, cudaStream_t);                                                                  \
-  template cudaError_t launch_solve_fwd_coop<F>(const std::int32_t*, const std::int32_t*, int, int, const SnDev*,    \
-                                                const std::int32_t*, const ContribEntry*, const F*,                    \
-                                                const std::int32_t*, double*, std::int64_t, double*, int, double*,      \
-                                                const std::int64_t*, int*, int*, cudaStream_t);                        \
-  template cudaError_t launch_solve_bwd_coop<F>(const std::int32_t*, const std::int32_t*, int, int, const SnDev*,    \
-                                                const std::int32_t*, const F*, const std::int32_t*, double*,            \
-                                                std::int64_t, int, double*, const std::int64_t*, int*, int*,            \
-                                                cudaStream_t);
+  template cudaError_t launch_fwd_level<F>(const SolveTask*, int, bool, const SnDev*, const std::int32_t*,           \
+                                           const ContribEntry*, const F*, const std::int32_t*, double*, std::int64_t,  \
+                                           double*, int, double*, int*, int*, cudaStream_t);                           \
+  template cudaError_t launch_bwd_level<F>(const SolveTask*, int, bool, const SnDev*, const std::int32_t*, const F*, \
+                                           const std::int32_t*, double*, std::int64_t, int, double*, int*, int*, int*, \
+                                           cudaStream_t);
 HSG_SOLVE_INSTANTIATE(double)
 HSG_SOLVE_INSTANTIATE(float)
 #undef HSG_SOLVE_INSTANTIATE
