@@ -37,7 +37,7 @@ struct AnalysisEntry {
 
 constexpr std::size_t kAnalysisCacheEntries = 8;
 // panel entries per CTA of a solve sweep
-constexpr double kSolveEntriesPerCta = 32768.0;
+constexpr double kSolveEntriesPerCta = 8192.0;
 std::mutex g_analysis_mu;
 std::list<AnalysisEntry> g_analysis_cache;  // most recently used first
 
@@ -206,6 +206,7 @@ GpuFactor::~GpuFactor() {
   DeviceGuard g(opt_.device);
   if (stream_) {
     cudaStreamSynchronize(stream_);
+    clear_sweep_graphs();
     cudaStreamDestroy(stream_);
   }
   if (ev0_) cudaEventDestroy(ev0_);
@@ -294,7 +295,10 @@ void GpuFactor::analyze_like(const GpuFactor& src) {
   sym_origin_ = src.sym_origin_;
   plan_ = src.plan_;  // shared: the plan is immutable
   cached_analysis_ = src.cached_analysis_;
-  cuda_check(cudaStreamSynchronize(src.stream_), "analyze_like: source");
+  {
+    std::lock_guard<std::mutex> lk(src.capture_mu_);
+    cuda_check(cudaStreamSynchronize(src.stream_), "analyze_like: source");
+  }
   d_a_.alloc(src.d_a_.n);
   d_b_.alloc(std::max<std::size_t>(1, src.d_b_.n));
   cuda_check(cudaMemcpyAsync(d_a_.p, src.d_a_.p, src.d_a_.n * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy");
@@ -598,6 +602,7 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
 }
 
 void GpuFactor::alloc_work() {
+  clear_sweep_graphs();  // captured launches name the buffers and the plan being replaced
   const FrontPlan& P = *plan_;
   const std::size_t fe = static_cast<std::size_t>(std::max<std::int64_t>(1, sym_.factor_entries));
   const std::size_t cbe = static_cast<std::size_t>(std::max<std::int64_t>(1, sym_.cb_arena));
@@ -791,7 +796,7 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
   cuda_check(cudaEventRecord(ev0_, s), "event");
   build_solve_operator();
   launch_gather_scale(n_, nr, db, ld, d_scale_.p, plan_->iperm.p, d_xwork_.p, s);
-  run_sweeps(d_xwork_.p, d_vec_.p, nr);
+  run_sweeps(d_xwork_.p, d_vec_.p, nr, true);
   launch_scatter_scale(n_, nr, db, ld, d_scale_.p, plan_->iperm.p, d_xwork_.p, s);
   cuda_check(cudaEventRecord(ev1_, s), "event");
   cuda_check(cudaGetLastError(), "solve launch");
@@ -836,7 +841,7 @@ void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ld
   cuda_check(cudaMemsetAsync(d_err_.p, 0, sizeof(int), s), "reset solve status");
   build_solve_operator();
   launch_gather_scale(n_, nr, b, ldb, d_scale_.p, plan_->iperm.p, xwork, s);
-  run_sweeps(xwork, vec, nr);
+  run_sweeps(xwork, vec, nr, false);  // no graph: instantiating one may allocate
   launch_scatter_scale(n_, nr, b, ldb, d_scale_.p, plan_->iperm.p, xwork, s);
   cuda_check(cudaGetLastError(), "solve launch");
   int err = 0;
@@ -845,9 +850,51 @@ void GpuFactor::solve_with_scratch(double* b, std::int64_t nrhs, std::int64_t ld
   HSG_REQUIRE(err == 0, HSG_INTERNAL, "solve: a wait between the CTAs of a front timed out");
 }
 
-void GpuFactor::run_sweeps(double* xwork, double* vec, int nr) {
-  if (single()) run_sweeps_t<float>(xwork, vec, nr);
-  else run_sweeps_t<double>(xwork, vec, nr);
+void GpuFactor::clear_sweep_graphs() {
+  for (SweepGraph& g : graphs_) cudaGraphExecDestroy(g.exec);
+  graphs_.clear();
+}
+
+void GpuFactor::run_sweeps(double* xwork, double* vec, int nr, bool graph) {
+  auto direct = [&] {
+    if (single()) run_sweeps_t<float>(xwork, vec, nr);
+    else run_sweeps_t<double>(xwork, vec, nr);
+  };
+  if (!graph || !graphs_ok_) return direct();
+  for (const SweepGraph& g : graphs_)
+    if (g.xwork == xwork && g.vec == vec && g.nr == nr) {
+      note_launches(g.launches);
+      cuda_check(cudaGraphLaunch(g.exec, stream_), "solve sweeps (graph)");
+      return;
+    }
+  // capture the sequence once; where capturing is refused (e.g. a cooperative launch), launch
+  // directly from now on
+  const long long l0 = hsg_kernel_launches();
+  cudaGraph_t cg = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::unique_lock<std::mutex> lk(capture_mu_);
+  bool ok = cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    try {
+      direct();
+    } catch (const Error&) {
+      ok = false;
+    }
+    ok = cudaStreamEndCapture(stream_, &cg) == cudaSuccess && ok && cg;
+    ok = ok && cudaGraphInstantiate(&exec, cg, 0) == cudaSuccess;
+    if (cg) cudaGraphDestroy(cg);
+  }
+  lk.unlock();
+  const long long captured = hsg_kernel_launches() - l0;
+  note_launches(-captured);  // counted when the graph runs
+  if (!ok) {
+    cudaGetLastError();  // the failed capture's error is not sticky
+    graphs_ok_ = false;
+    return direct();
+  }
+  graphs_.push_back(SweepGraph{xwork, vec, nr, captured, exec});
+  note_launches(captured);
+  cuda_check(cudaGraphLaunch(exec, stream_), "solve sweeps (graph)");
 }
 
 template <class F>

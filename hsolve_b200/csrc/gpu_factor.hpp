@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -195,8 +196,10 @@ class GpuFactor {
   void run_numeric(double alpha, double beta, bool detection, bool count_only);
   template <class R>
   void run_numeric_t(double alpha, double beta, bool detection, bool count_only);
-  // forward, diagonal and backward sweeps of nr right-hand sides gathered in xwork (n x nr)
-  void run_sweeps(double* xwork, double* vec, int nr);
+  // forward, diagonal and backward sweeps of nr right-hand sides gathered in xwork (n x nr); with
+  // graph, the launches are captured once per (xwork, vec, nr) in a CUDA graph and replayed
+  void run_sweeps(double* xwork, double* vec, int nr, bool graph);
+  void clear_sweep_graphs();
   template <class F>
   void run_sweeps_t(double* xwork, double* vec, int nr);
   template <class F>
@@ -250,6 +253,19 @@ class GpuFactor {
   DevBuf<int> d_sweep_cnt_;       // per front: forward and backward publication counters, backward arrivals
   bool w_ready_ = false;
   void build_solve_operator();
+  // captured sweep sequences (valid until the plan or the work buffers change)
+  struct SweepGraph {
+    double* xwork;
+    double* vec;
+    int nr;
+    long long launches;
+    cudaGraphExec_t exec;
+  };
+  std::vector<SweepGraph> graphs_;
+  bool graphs_ok_ = true;  // false once a capture failed: launch directly
+  // held while stream_ is capturing: another object's analyze_like synchronizes stream_, which is
+  // not permitted during a capture
+  mutable std::mutex capture_mu_;
   int solve_coop_max_ = 0;
   int coop_max_ = 0;
   bool shared_ = false;

@@ -307,15 +307,21 @@ __global__ void __launch_bounds__(256, 2) k_fwd_level(const SolveTask* tasks, co
         if (i >= m) continue;
         double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         const F* Wi = Wf + i + static_cast<std::int64_t>(b) * m;
-        for (int j0 = 0; j0 < bs; j0 += 8) {
-          double wv[8];
+        // 16-column batches; the next batch's loads are issued before this one is summed
+        double wv[16];
 #pragma unroll
-          for (int u = 0; u < 8; ++u)
-            wv[u] = j0 + u < bs ? static_cast<double>(Wi[static_cast<std::int64_t>(j0 + u) * m]) : 0.0;
+        for (int u = 0; u < 16; ++u) wv[u] = u < bs ? static_cast<double>(Wi[static_cast<std::int64_t>(u) * m]) : 0.0;
+        for (int j0 = 0; j0 < bs; j0 += 16) {
+          double wn[16];
 #pragma unroll
-          for (int u = 0; u < 8; ++u)
+          for (int u = 0; u < 16; ++u)
+            wn[u] = j0 + 16 + u < bs ? static_cast<double>(Wi[static_cast<std::int64_t>(j0 + 16 + u) * m]) : 0.0;
+#pragma unroll
+          for (int u = 0; u < 16; ++u)
 #pragma unroll
             for (int r = 0; r < 8; ++r) acc[r] = fma(wv[u], tb[(j0 + u) * 8 + r], acc[r]);
+#pragma unroll
+          for (int u = 0; u < 16; ++u) wv[u] = wn[u];
         }
         double* ti = t + static_cast<std::int64_t>(i) * 8;
         if (i < be) {
