@@ -40,6 +40,17 @@ struct SolveTask {
   std::int64_t wofs;
 };
 
+// Column chunks of one solve sweep launch: chunk c (blockIdx.y) carries columns [8c, 8c + 8) of the
+// launch's ncols right-hand sides, with its own contribution vectors, work array and counters at
+// c times the strides.
+struct SweepChunks {
+  int ncols;
+  int cnt_stride;
+  std::int64_t x_stride;
+  std::int64_t vec_stride;
+  std::int64_t work_stride;
+};
+
 // Counters written by the factorization kernels (integers: sums are order independent).
 struct FactorCounters {
   unsigned long long neg;

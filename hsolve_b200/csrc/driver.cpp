@@ -990,7 +990,7 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
     // the block width: multi-column solves cost little more than single ones on the GPU, and a block
     // of p takes up to p copies of a multiple eigenvalue at once
     const int p = cfg.block_size > 0
-                      ? static_cast<int>(std::max<std::int64_t>(1, std::min<std::int64_t>({cfg.block_size, nev, kMaxBlock, n / 16})))
+                      ? static_cast<int>(std::max<std::int64_t>(1, std::min<std::int64_t>({cfg.block_size, nev, kMaxKrylovBlock, n / 16})))
                       : auto_block(nev);
     block_used = p;
     GhiepRun run;

@@ -222,7 +222,7 @@ std::vector<double> ortho_block(Basis& B, KrylovOperator& op, int j, int p, std:
 }  // namespace
 
 KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, cudaStream_t s) {
-  const int p = std::max(1, std::min(opt.block, kMaxBlock));
+  const int p = std::max(1, std::min(opt.block, kMaxKrylovBlock));
   const int nev = std::max(1, opt.nev);
   int mmax = opt.ncv > 0 ? opt.ncv : std::max(2 * nev + 1, nev + 16) + 4 * p;
   mmax = std::max(mmax, nev + 2 * p);
@@ -425,7 +425,7 @@ namespace hsg {
 
 GeneralKsResult krylov_schur_general(KrylovOperator& op, std::int64_t n, const KsOptions& opt, cudaStream_t s) {
   using cplx = std::complex<double>;
-  const int p = std::max(1, std::min(opt.block, kMaxBlock));
+  const int p = std::max(1, std::min(opt.block, kMaxKrylovBlock));
   const int nev = std::max(1, opt.nev);
   int mmax = opt.ncv > 0 ? opt.ncv : std::max(2 * nev + 1, nev + 16) + 4 * p;
   mmax = std::max(mmax, nev + 2 * p + 2);

@@ -17,6 +17,10 @@
 
 namespace hsg {
 
+// Widest Krylov block: two 8-column chunks of one solve launch (a 16-column solve costs about 1.45x an
+// 8-column one, whose sweeps are latency-bound).
+constexpr int kMaxKrylovBlock = 16;
+
 struct KrylovOperator {
   virtual ~KrylovOperator() = default;
   // y = OP x (device, n x p)

@@ -441,7 +441,7 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
         }
       }
       work_max = std::max(work_max, wofs);
-      auto plan_tasks = [&](bool bwd, std::int64_t& off, int& ctas, bool& coop) {
+      auto plan_tasks = [&](bool bwd, int budget, std::int64_t& off, int& ctas, bool& coop) {
         auto cap = [&](const SnDev& dd) { return std::max(1, ((bwd ? dd.k : dd.m) + 31) / 32); };
         std::vector<int> nr(all.size());
         double wsum = 0.0;
@@ -453,8 +453,8 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
           nr[q] = static_cast<int>(std::min<double>(cap(dd), std::max(1.0, std::ceil(w / kSolveEntriesPerCta))));
           total += nr[q];
         }
-        if (total > solve_coop_max_) {
-          const int spare = solve_coop_max_ - static_cast<int>(all.size());
+        if (total > budget) {
+          const int spare = budget - static_cast<int>(all.size());
           for (std::size_t q = 0; q < all.size(); ++q) {
             const SnDev& dd = sn[all[q]];
             const double w = static_cast<double>(dd.m) * dd.k;
@@ -470,8 +470,12 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
           }
         ctas = static_cast<int>(static_cast<std::int64_t>(tasks.size()) - off);
       };
-      plan_tasks(false, L.fwd_task_off, L.fwd_ctas, L.fwd_coop);
-      plan_tasks(true, L.bwd_task_off, L.bwd_ctas, L.bwd_coop);
+      for (int c = 0; c < kSweepChunks; ++c) {
+        // a launch of c + 1 chunks runs (c + 1) CTAs per task: the co-resident bound is shared
+        const int budget = solve_coop_max_ / (c + 1);
+        plan_tasks(false, budget, L.fwd_task_off[c], L.fwd_ctas[c], L.fwd_coop[c]);
+        plan_tasks(true, budget, L.bwd_task_off[c], L.bwd_ctas[c], L.bwd_coop[c]);
+      }
     }
     // cooperative launch when the level's panel fronts fit the co-resident grid; CTAs apportioned
     // by m^2, for the whole device and for the shared budget (a third of it, used while several
@@ -618,9 +622,9 @@ void GpuFactor::alloc_work() {
   }
   d_scratch_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, P.scratch_max)));
   d_level_done_.alloc(static_cast<std::size_t>(std::max(1, P.ncoop)));
-  d_work_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, P.work_max)));
+  d_work_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, P.work_max)) * kSweepChunks);
   d_err_.alloc(1);
-  d_sweep_cnt_.alloc(static_cast<std::size_t>(3 * std::max(1, sym_.ns)));
+  d_sweep_cnt_.alloc(static_cast<std::size_t>(3 * std::max(1, sym_.ns)) * kSweepChunks);
   w_ready_ = false;
 }
 
@@ -819,7 +823,8 @@ void GpuFactor::solve(double* b, std::int64_t nrhs, std::int64_t ldb, bool on_de
 }
 
 std::size_t GpuFactor::solve_scratch_doubles(std::int64_t nrhs) const {
-  const std::int64_t nc = std::min<std::int64_t>(8, nrhs);
+  // contribution vectors of one sweep launch: 8 columns per chunk
+  const std::int64_t nc = std::min<std::int64_t>(8 * kSweepChunks, nrhs);
   return static_cast<std::size_t>(n_ * nrhs + std::max<std::int64_t>(1, plan_->vec_total) * nc);
 }
 
@@ -907,19 +912,27 @@ void GpuFactor::run_sweeps_t(double* xwork, double* vec, int nr) {
   int* fcnt = d_sweep_cnt_.p;
   int* bcnt = fcnt + ns;
   int* arrive = bcnt + ns;
-  // chunks of at most 8 right-hand sides (the sweeps carry 8)
-  for (int c0 = 0; c0 < nr; c0 += 8) {
-    const int nc = std::min(8, nr - c0);
+  // launches carry up to kSweepChunks chunks of 8 right-hand sides, each with its own contribution
+  // vectors (vec_total x 8), work array and counters
+  const int span = 8 * kSweepChunks;
+  for (int c0 = 0; c0 < nr; c0 += span) {
+    SweepChunks ck;
+    ck.ncols = std::min(span, nr - c0);
+    ck.cnt_stride = 3 * ns;
+    ck.x_stride = 8 * n_;
+    ck.vec_stride = 8 * std::max<std::int64_t>(1, plan_->vec_total);
+    ck.work_stride = std::max<std::int64_t>(1, plan_->work_max);
+    const int c = (ck.ncols + 7) / 8 - 1;
     double* xw = xwork + static_cast<std::int64_t>(c0) * n_;
     cuda_check(cudaMemsetAsync(d_sweep_cnt_.p, 0, d_sweep_cnt_.n * sizeof(int), s), "reset sweep counters");
     for (const LevelPlan& L : plan_->levels)
-      cuda_check(launch_fwd_level<F>(tasks + L.fwd_task_off, L.fwd_ctas, L.fwd_coop, plan_->sn.p, plan_->cptr.p,
-                                     plan_->cent.p, W, d_pidx_.p, xw, n_, vec, nc, d_work_.p, fcnt, d_err_.p, s),
+      cuda_check(launch_fwd_level<F>(tasks + L.fwd_task_off[c], L.fwd_ctas[c], L.fwd_coop[c], plan_->sn.p, plan_->cptr.p,
+                                     plan_->cent.p, W, d_pidx_.p, xw, n_, vec, ck, d_work_.p, fcnt, d_err_.p, s),
                  "forward solve");
-    launch_solve_diag_flat<F>(n_, plan_->dpos.p, plan_->pfirst.p, panels, d_piv_.p, d_pidx_.p, xw, n_, nc, s);
+    launch_solve_diag_flat<F>(n_, plan_->dpos.p, plan_->pfirst.p, panels, d_piv_.p, d_pidx_.p, xw, n_, ck.ncols, s);
     for (auto it = plan_->levels.rbegin(); it != plan_->levels.rend(); ++it)
-      cuda_check(launch_bwd_level<F>(tasks + it->bwd_task_off, it->bwd_ctas, it->bwd_coop, plan_->sn.p, plan_->rows.p, W,
-                                     d_pidx_.p, xw, n_, nc, d_work_.p, bcnt, arrive, d_err_.p, s),
+      cuda_check(launch_bwd_level<F>(tasks + it->bwd_task_off[c], it->bwd_ctas[c], it->bwd_coop[c], plan_->sn.p,
+                                     plan_->rows.p, W, d_pidx_.p, xw, n_, ck, d_work_.p, bcnt, arrive, d_err_.p, s),
                  "backward solve");
   }
 }

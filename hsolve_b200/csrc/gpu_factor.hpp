@@ -92,10 +92,10 @@ struct LevelPlan {
   std::int64_t cta_off = 0; int coop_ctas = 0; int done_slot = 0;
   std::int64_t all_off = 0; int all_n = 0; int maxm = 0;
   std::vector<std::pair<std::int64_t, int>> ea;  // (offset into items, count) per child rank
-  // solve sweeps: the level's CTA tasks (FrontPlan::tasks) of the forward and the backward sweep;
-  // coop: some front has several CTAs (cooperative launch)
-  std::int64_t fwd_task_off = 0; int fwd_ctas = 0; bool fwd_coop = false;
-  std::int64_t bwd_task_off = 0; int bwd_ctas = 0; bool bwd_coop = false;
+  // solve sweeps: the level's CTA tasks (FrontPlan::tasks) of the forward and the backward sweep,
+  // planned for launches of c + 1 column chunks; coop: some front has several CTAs (cooperative)
+  std::int64_t fwd_task_off[2] = {0, 0}; int fwd_ctas[2] = {0, 0}; bool fwd_coop[2] = {false, false};
+  std::int64_t bwd_task_off[2] = {0, 0}; int bwd_ctas[2] = {0, 0}; bool bwd_coop[2] = {false, false};
   bool coop_shared = false;          // the level also fits the shared budget's co-resident grid
   std::int64_t cta_off_shared = 0; int coop_ctas_shared = 0;  // cooperative plan of the shared budget
   std::int64_t ent_off = 0, ent_n = 0;  // inertia-only counts: this level's entries in FrontPlan::ent_idx

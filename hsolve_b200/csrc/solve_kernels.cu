@@ -244,9 +244,14 @@ template <class F>
 __global__ void __launch_bounds__(256, 2) k_fwd_level(const SolveTask* tasks, const SnDev* sn, const std::int32_t* cptr,
                                                        const ContribEntry* cent, const F* W,
                                                        const std::int32_t* pidx, double* x, std::int64_t n,
-                                                       double* vec, int nrhs, double* work, int* cnts, int* err) {
+                                                       double* vec, SweepChunks ck, double* work, int* cnts, int* err) {
   __shared__ double tb[kSB * 8];
   __shared__ double red[8][32][9];
+  const int nrhs = min(8, ck.ncols - 8 * static_cast<int>(blockIdx.y));
+  x += blockIdx.y * ck.x_stride;
+  vec += blockIdx.y * ck.vec_stride;
+  work += blockIdx.y * ck.work_stride;
+  cnts += blockIdx.y * ck.cnt_stride;
   const SolveTask tk = tasks[blockIdx.x];
   const SnDev d = sn[tk.s];
   const int m = d.m, k = d.k, c = m - k, rank = tk.rank, nr = tk.nr;
@@ -390,7 +395,7 @@ __global__ void __launch_bounds__(256, 2) k_fwd_level(const SolveTask* tasks, co
 template <class F>
 __global__ void __launch_bounds__(256, 2) k_bwd_level(const SolveTask* tasks, const SnDev* sn, const std::int32_t* rows,
                                                        const F* W, const std::int32_t* pidx, double* x,
-                                                       std::int64_t n, int nrhs, double* work, int* cnts,
+                                                       std::int64_t n, SweepChunks ck, double* work, int* cnts,
                                                        int* arrive, int* err) {
   extern __shared__ double dsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -398,6 +403,11 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const SolveTask* tasks, co
   double* tt = wt + 32 * kTilePitch;       // tt[i * kRowPitch + r]: the tile's rows, signed
   double* xb = dsm + 8 * kWarpSmem;        // xb[r * kSB + i]: x of the super-block being applied
   double* red = dsm;                       // [8][32][9] partial sums, over the tiles once they are used
+  const int nrhs = min(8, ck.ncols - 8 * static_cast<int>(blockIdx.y));
+  x += blockIdx.y * ck.x_stride;
+  work += blockIdx.y * ck.work_stride;
+  cnts += blockIdx.y * ck.cnt_stride;
+  arrive += blockIdx.y * ck.cnt_stride;
   const SolveTask tk = tasks[blockIdx.x];
   const SnDev d = sn[tk.s];
   const int m = d.m, k = d.k, rank = tk.rank, nr = tk.nr;
@@ -610,31 +620,35 @@ void launch_sb_build(const int2* sbl, int nsb, const int4* tiles, int ntiles, co
 template <class F>
 cudaError_t launch_fwd_level(const SolveTask* tasks, int nctas, bool coop, const SnDev* sn, const std::int32_t* cptr,
                              const ContribEntry* cent, const F* W, const std::int32_t* pidx, double* x, std::int64_t n,
-                             double* vec, int nrhs, double* work, int* cnts, int* err, cudaStream_t s) {
-  if (nctas <= 0) return cudaSuccess;
+                             double* vec, const SweepChunks& ck, double* work, int* cnts, int* err, cudaStream_t s) {
+  if (nctas <= 0 || ck.ncols <= 0) return cudaSuccess;
+  const dim3 grid(nctas, (ck.ncols + 7) / 8);
+  SweepChunks c = ck;
   note_launches(1);
   if (!coop) {
-    k_fwd_level<F><<<nctas, 256, 0, s>>>(tasks, sn, cptr, cent, W, pidx, x, n, vec, nrhs, work, cnts, err);
+    k_fwd_level<F><<<grid, 256, 0, s>>>(tasks, sn, cptr, cent, W, pidx, x, n, vec, c, work, cnts, err);
     return cudaGetLastError();
   }
-  void* args[] = {&tasks, &sn, &cptr, &cent, &W, &pidx, &x, &n, &vec, &nrhs, &work, &cnts, &err};
-  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_fwd_level<F>), dim3(nctas), dim3(256), args, 0, s);
+  void* args[] = {&tasks, &sn, &cptr, &cent, &W, &pidx, &x, &n, &vec, &c, &work, &cnts, &err};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_fwd_level<F>), grid, dim3(256), args, 0, s);
 }
 
 template <class F>
 cudaError_t launch_bwd_level(const SolveTask* tasks, int nctas, bool coop, const SnDev* sn, const std::int32_t* rows,
-                             const F* W, const std::int32_t* pidx, double* x, std::int64_t n, int nrhs, double* work,
-                             int* cnts, int* arrive, int* err, cudaStream_t s) {
-  if (nctas <= 0) return cudaSuccess;
+                             const F* W, const std::int32_t* pidx, double* x, std::int64_t n, const SweepChunks& ck,
+                             double* work, int* cnts, int* arrive, int* err, cudaStream_t s) {
+  if (nctas <= 0 || ck.ncols <= 0) return cudaSuccess;
   configure_bwd<F>();
+  const dim3 grid(nctas, (ck.ncols + 7) / 8);
+  SweepChunks c = ck;
   note_launches(1);
   if (!coop) {
-    k_bwd_level<F><<<nctas, 256, kBwdSmemBytes, s>>>(tasks, sn, rows, W, pidx, x, n, nrhs, work, cnts, arrive, err);
+    k_bwd_level<F><<<grid, 256, kBwdSmemBytes, s>>>(tasks, sn, rows, W, pidx, x, n, c, work, cnts, arrive, err);
     return cudaGetLastError();
   }
-  void* args[] = {&tasks, &sn, &rows, &W, &pidx, &x, &n, &nrhs, &work, &cnts, &arrive, &err};
-  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_bwd_level<F>), dim3(nctas), dim3(256), args,
-                                     kBwdSmemBytes, s);
+  void* args[] = {&tasks, &sn, &rows, &W, &pidx, &x, &n, &c, &work, &cnts, &arrive, &err};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_bwd_level<F>), grid, dim3(256), args, kBwdSmemBytes,
+                                     s);
 }
 
 #define HSG_SOLVE_INSTANTIATE(F)                                                                                       \
@@ -645,10 +659,10 @@ cudaError_t launch_bwd_level(const SolveTask* tasks, int nctas, bool coop, const
                                    F*, cudaStream_t);                                                                  \
   template cudaError_t launch_fwd_level<F>(const SolveTask*, int, bool, const SnDev*, const std::int32_t*,           \
                                            const ContribEntry*, const F*, const std::int32_t*, double*, std::int64_t,  \
-                                           double*, int, double*, int*, int*, cudaStream_t);                           \
+                                           double*, const SweepChunks&, double*, int*, int*, cudaStream_t);            \
   template cudaError_t launch_bwd_level<F>(const SolveTask*, int, bool, const SnDev*, const std::int32_t*, const F*, \
-                                           const std::int32_t*, double*, std::int64_t, int, double*, int*, int*, int*, \
-                                           cudaStream_t);
+                                           const std::int32_t*, double*, std::int64_t, const SweepChunks&, double*,    \
+                                           int*, int*, int*, cudaStream_t);
 HSG_SOLVE_INSTANTIATE(double)
 HSG_SOLVE_INSTANTIATE(float)
 #undef HSG_SOLVE_INSTANTIATE

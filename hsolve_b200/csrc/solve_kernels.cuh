@@ -32,18 +32,20 @@ void launch_sb_build(const int2* sbl, int nsb, const int4* tiles, int ntiles, co
                      const signed char* piv, F* W, cudaStream_t s);
 // co-resident CTAs of the sweep kernels (the bound of a cooperative level launch)
 int solve_coop_max_ctas(int device);
-// One level of the forward / backward sweep over at most 8 right-hand sides: one CTA per task
-// (front, rank, nr, work offset); coop: the level has fronts of several CTAs (cooperative launch,
-// nctas <= solve_coop_max_ctas). cnts / arrive: one counter per front, zero at the first launch of
-// a sweep; err: set to 1 when a wait between the CTAs of a front ran out (the solve is then invalid).
-// Work per front: 8 m doubles forward, 16 k backward.
+// One level of the forward / backward sweep: one CTA per task (front, rank, nr, work offset) and
+// 8-column chunk of the ck.ncols right-hand sides (grid nctas x chunks); coop: the level has fronts
+// of several CTAs (cooperative launch, nctas x chunks <= solve_coop_max_ctas). cnts / arrive: one
+// counter per front and chunk, zero at the first launch of a sweep; err: set to 1 when a wait
+// between the CTAs of a front ran out (the solve is then invalid). Work per front and chunk: 8 m
+// doubles forward, 16 k backward.
+constexpr int kSweepChunks = 2;  // 8-column chunks carried by one sweep launch
 template <class F>
 cudaError_t launch_fwd_level(const SolveTask* tasks, int nctas, bool coop, const SnDev* sn, const std::int32_t* cptr,
                              const ContribEntry* cent, const F* W, const std::int32_t* pidx, double* x, std::int64_t n,
-                             double* vec, int nrhs, double* work, int* cnts, int* err, cudaStream_t s);
+                             double* vec, const SweepChunks& ck, double* work, int* cnts, int* err, cudaStream_t s);
 template <class F>
 cudaError_t launch_bwd_level(const SolveTask* tasks, int nctas, bool coop, const SnDev* sn, const std::int32_t* rows,
-                             const F* W, const std::int32_t* pidx, double* x, std::int64_t n, int nrhs, double* work,
-                             int* cnts, int* arrive, int* err, cudaStream_t s);
+                             const F* W, const std::int32_t* pidx, double* x, std::int64_t n, const SweepChunks& ck,
+                             double* work, int* cnts, int* arrive, int* err, cudaStream_t s);
 
 }  // namespace hsg

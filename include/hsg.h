@@ -131,7 +131,7 @@ HSG_API int hsg_solve(hsg_factor* f, double* b, int64_t nrhs, int64_t ldb, int32
  * cudaMalloc would fail), or a serving loop that cannot afford the device-wide synchronisation
  * that cudaFree implies. This call allocates nothing: its work space is one fixed array compiled
  * into the library, HSG_SOLVE_STATIC_SCRATCH_BYTES (16 MiB) on every device that loads the library,
- * held until the process exits. It needs 8 * (n * nrhs + c * min(nrhs, 8)) bytes, where c is the
+ * held until the process exits. It needs 8 * (n * nrhs + c * min(nrhs, 16)) bytes, where c is the
  * total contribution-block row count of the factorization; a larger request returns
  * HSG_INVALID_INPUT with the sizes in hsg_last_error(), and the caller should split its right-hand
  * sides or use hsg_solve. The first call on a device looks up the array's device address (make
