@@ -471,6 +471,8 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
           }
         ctas = static_cast<int>(static_cast<std::int64_t>(tasks.size()) - off);
       };
+      L.tiny = !all.empty();
+      for (std::int32_t sq : all) L.tiny = L.tiny && sn[sq].m <= kTinyRows && sn[sq].k <= 32;
       for (int c = 0; c < kSweepChunks; ++c) {
         // a launch of c + 1 chunks runs (c + 1) CTAs per task: the co-resident bound is shared
         const int budget = solve_coop_max_ / (c + 1);
@@ -928,15 +930,28 @@ void GpuFactor::run_sweeps_t(double* xwork, double* vec, int nr) {
     const int c = (ck.ncols + 7) / 8 - 1;
     double* xw = xwork + static_cast<std::int64_t>(c0) * n_;
     cuda_check(cudaMemsetAsync(d_sweep_cnt_.p, 0, d_sweep_cnt_.n * sizeof(int), s), "reset sweep counters");
-    for (const LevelPlan& L : plan_->levels)
-      cuda_check(launch_fwd_level<F>(tasks + L.fwd_task_off[c], L.fwd_ctas[c], L.fwd_coop[c], plan_->sn.p, plan_->cptr.p,
-                                     plan_->cent.p, W, d_pidx_.p, xw, n_, vec, ck, d_work_.p, fcnt, d_err_.p, s),
-                 "forward solve");
+    for (const LevelPlan& L : plan_->levels) {
+      if (L.tiny)  // one CTA per task in the plan (nr = 1): one warp per front here
+        cuda_check(launch_fwd_tiny<F>(tasks + L.fwd_task_off[c], L.fwd_ctas[c], plan_->sn.p, plan_->cptr.p, plan_->cent.p,
+                                      W, d_pidx_.p, xw, n_, vec, ck, s),
+                   "forward solve");
+      else
+        cuda_check(launch_fwd_level<F>(tasks + L.fwd_task_off[c], L.fwd_ctas[c], L.fwd_coop[c], plan_->sn.p,
+                                       plan_->cptr.p, plan_->cent.p, W, d_pidx_.p, xw, n_, vec, ck, d_work_.p, fcnt,
+                                       d_err_.p, s),
+                   "forward solve");
+    }
     launch_solve_diag_flat<F>(n_, plan_->dpos.p, plan_->pfirst.p, panels, d_piv_.p, d_pidx_.p, xw, n_, ck.ncols, s);
-    for (auto it = plan_->levels.rbegin(); it != plan_->levels.rend(); ++it)
-      cuda_check(launch_bwd_level<F>(tasks + it->bwd_task_off[c], it->bwd_ctas[c], it->bwd_coop[c], plan_->sn.p,
-                                     plan_->rows.p, W, d_pidx_.p, xw, n_, ck, d_work_.p, bcnt, arrive, d_err_.p, s),
-                 "backward solve");
+    for (auto it = plan_->levels.rbegin(); it != plan_->levels.rend(); ++it) {
+      if (it->tiny)
+        cuda_check(launch_bwd_tiny<F>(tasks + it->bwd_task_off[c], it->bwd_ctas[c], plan_->sn.p, plan_->rows.p, W,
+                                      d_pidx_.p, xw, n_, ck, s),
+                   "backward solve");
+      else
+        cuda_check(launch_bwd_level<F>(tasks + it->bwd_task_off[c], it->bwd_ctas[c], it->bwd_coop[c], plan_->sn.p,
+                                       plan_->rows.p, W, d_pidx_.p, xw, n_, ck, d_work_.p, bcnt, arrive, d_err_.p, s),
+                   "backward solve");
+    }
   }
 }
 

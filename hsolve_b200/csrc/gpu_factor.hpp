@@ -96,6 +96,7 @@ struct LevelPlan {
   // planned for launches of c + 1 column chunks; coop: some front has several CTAs (cooperative)
   std::int64_t fwd_task_off[2] = {0, 0}; int fwd_ctas[2] = {0, 0}; bool fwd_coop[2] = {false, false};
   std::int64_t bwd_task_off[2] = {0, 0}; int bwd_ctas[2] = {0, 0}; bool bwd_coop[2] = {false, false};
+  bool tiny = false;                 // every front has m <= kTinyRows, k <= 32: one warp per front
   bool coop_shared = false;          // the level also fits the shared budget's co-resident grid
   std::int64_t cta_off_shared = 0; int coop_ctas_shared = 0;  // cooperative plan of the shared budget
   std::int64_t ent_off = 0, ent_n = 0;  // inertia-only counts: this level's entries in FrontPlan::ent_idx

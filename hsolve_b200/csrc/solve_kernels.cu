@@ -548,6 +548,118 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const SolveTask* tasks, co
 }
 
 
+// Levels of tiny fronts (m <= kTinyRows, k <= 32: one super-block, no chain): one warp per front,
+// eight fronts per CTA, no block barrier. Forward: lane owns rows lane, lane + 32, lane + 64; the pivot
+// rows' assembled values go to shared memory for z = W[B, B] t_B and the contribution rows' updates.
+// Backward: the front's rows of x (pivot rows' entry values, minus the contribution rows) are staged in
+// shared memory and lane j < k forms x_j = W[:, j]^T of them, reading its own column of W.
+template <class F>
+__global__ void __launch_bounds__(256) k_fwd_tiny(const SolveTask* tasks, int ntasks, const SnDev* sn,
+                                                   const std::int32_t* cptr, const ContribEntry* cent, const F* W,
+                                                   const std::int32_t* pidx, double* x, std::int64_t n, double* vec,
+                                                   SweepChunks ck) {
+  __shared__ double tbs[8][32][8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ti = blockIdx.x * 8 + warp;
+  if (ti >= ntasks) return;  // the whole warp: no block barrier follows
+  const int nrhs = min(8, ck.ncols - 8 * static_cast<int>(blockIdx.y));
+  x += blockIdx.y * ck.x_stride;
+  vec += blockIdx.y * ck.vec_stride;
+  const SnDev d = sn[tasks[ti].s];
+  const int m = d.m, k = d.k, c = m - k;
+  const F* Wf = W + d.w_off;
+  const std::int32_t* pl = pidx + d.first;
+  const std::int32_t* cp = cptr + d.cptr_off;
+  double* v = vec + d.vec_off * nrhs;
+  double t[kTinyRows / 32][8];
+#pragma unroll
+  for (int u = 0; u < kTinyRows / 32; ++u) {
+    const int i = lane + 32 * u;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) t[u][r] = 0.0;
+    if (i >= m) continue;
+    const int pos = i < k ? pl[i] : i;
+    if (i < k) {
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+        if (r < nrhs) t[u][r] = x[d.first + pos + static_cast<std::int64_t>(r) * n];
+    }
+    const int e1 = cp[pos + 1];
+    for (int e = cp[pos]; e < e1; ++e) {
+      const ContribEntry ce = cent[e];
+      const double* src = vec + ce.vec_off * nrhs + ce.a;
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+        if (r < nrhs) t[u][r] += src[static_cast<std::int64_t>(r) * ce.mc];
+    }
+  }
+  if (lane < k) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) tbs[warp][lane][r] = t[0][r];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int u = 0; u < kTinyRows / 32; ++u) {
+    const int i = lane + 32 * u;
+    if (i >= m) continue;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int j = 0; j < k; ++j) {
+      const double w = static_cast<double>(Wf[i + static_cast<std::int64_t>(j) * m]);
+#pragma unroll
+      for (int r = 0; r < 8; ++r) acc[r] = fma(w, tbs[warp][j][r], acc[r]);
+    }
+    if (i < k) {
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+        if (r < nrhs) x[d.first + pl[i] + static_cast<std::int64_t>(r) * n] = acc[r];
+    } else {
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+        if (r < nrhs) v[(i - k) + static_cast<std::int64_t>(r) * c] = t[u][r] - acc[r];
+    }
+  }
+}
+
+template <class F>
+__global__ void __launch_bounds__(256) k_bwd_tiny(const SolveTask* tasks, int ntasks, const SnDev* sn,
+                                                   const std::int32_t* rows, const F* W, const std::int32_t* pidx,
+                                                   double* x, std::int64_t n, SweepChunks ck) {
+  __shared__ double xs[8][kTinyRows][8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ti = blockIdx.x * 8 + warp;
+  if (ti >= ntasks) return;  // the whole warp: no block barrier follows
+  const int nrhs = min(8, ck.ncols - 8 * static_cast<int>(blockIdx.y));
+  x += blockIdx.y * ck.x_stride;
+  const SnDev d = sn[tasks[ti].s];
+  const int m = d.m, k = d.k;
+  if (k == 0) return;
+  const F* Wf = W + d.w_off;
+  const std::int32_t* pl = pidx + d.first;
+  const std::int32_t* rw = rows + d.rows_off;
+#pragma unroll
+  for (int u = 0; u < kTinyRows / 32; ++u) {
+    const int i = lane + 32 * u;
+    if (i >= m) continue;
+    const std::int64_t g = i < k ? d.first + pl[i] : rw[i];
+    const double sg = i < k ? 1.0 : -1.0;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) xs[warp][i][r] = r < nrhs ? sg * x[g + static_cast<std::int64_t>(r) * n] : 0.0;
+  }
+  __syncwarp();
+  if (lane < k) {
+    const F* Wj = Wf + static_cast<std::int64_t>(lane) * m;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = lane; i < m; ++i) {  // W[i, j] = 0 above the diagonal
+      const double w = static_cast<double>(Wj[i]);
+#pragma unroll
+      for (int r = 0; r < 8; ++r) acc[r] = fma(w, xs[warp][i][r], acc[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+      if (r < nrhs) x[d.first + pl[lane] + static_cast<std::int64_t>(r) * n] = acc[r];
+  }
+}
+
 void launch_gather_scale(std::int64_t n, int nrhs, const double* b, std::int64_t ldb, const double* d,
                          const std::int32_t* iperm, double* x, cudaStream_t s) {
   const std::int64_t total = n * nrhs;
@@ -651,6 +763,26 @@ cudaError_t launch_bwd_level(const SolveTask* tasks, int nctas, bool coop, const
                                      s);
 }
 
+template <class F>
+cudaError_t launch_fwd_tiny(const SolveTask* tasks, int ntasks, const SnDev* sn, const std::int32_t* cptr,
+                            const ContribEntry* cent, const F* W, const std::int32_t* pidx, double* x, std::int64_t n,
+                            double* vec, const SweepChunks& ck, cudaStream_t s) {
+  if (ntasks <= 0 || ck.ncols <= 0) return cudaSuccess;
+  note_launches(1);
+  k_fwd_tiny<F><<<dim3((ntasks + 7) / 8, (ck.ncols + 7) / 8), 256, 0, s>>>(tasks, ntasks, sn, cptr, cent, W, pidx, x,
+                                                                          n, vec, ck);
+  return cudaGetLastError();
+}
+
+template <class F>
+cudaError_t launch_bwd_tiny(const SolveTask* tasks, int ntasks, const SnDev* sn, const std::int32_t* rows, const F* W,
+                            const std::int32_t* pidx, double* x, std::int64_t n, const SweepChunks& ck, cudaStream_t s) {
+  if (ntasks <= 0 || ck.ncols <= 0) return cudaSuccess;
+  note_launches(1);
+  k_bwd_tiny<F><<<dim3((ntasks + 7) / 8, (ck.ncols + 7) / 8), 256, 0, s>>>(tasks, ntasks, sn, rows, W, pidx, x, n, ck);
+  return cudaGetLastError();
+}
+
 #define HSG_SOLVE_INSTANTIATE(F)                                                                                       \
   template void launch_solve_diag_flat<F>(std::int64_t, const std::int64_t*, const std::int32_t*, const F*,          \
                                           const signed char*, const std::int32_t*, double*, std::int64_t, int,        \
@@ -662,7 +794,12 @@ cudaError_t launch_bwd_level(const SolveTask* tasks, int nctas, bool coop, const
                                            double*, const SweepChunks&, double*, int*, int*, cudaStream_t);            \
   template cudaError_t launch_bwd_level<F>(const SolveTask*, int, bool, const SnDev*, const std::int32_t*, const F*, \
                                            const std::int32_t*, double*, std::int64_t, const SweepChunks&, double*,    \
-                                           int*, int*, int*, cudaStream_t);
+                                           int*, int*, int*, cudaStream_t);                                            \
+  template cudaError_t launch_fwd_tiny<F>(const SolveTask*, int, const SnDev*, const std::int32_t*,                  \
+                                          const ContribEntry*, const F*, const std::int32_t*, double*, std::int64_t,   \
+                                          double*, const SweepChunks&, cudaStream_t);                                  \
+  template cudaError_t launch_bwd_tiny<F>(const SolveTask*, int, const SnDev*, const std::int32_t*, const F*,        \
+                                          const std::int32_t*, double*, std::int64_t, const SweepChunks&, cudaStream_t);
 HSG_SOLVE_INSTANTIATE(double)
 HSG_SOLVE_INSTANTIATE(float)
 #undef HSG_SOLVE_INSTANTIATE

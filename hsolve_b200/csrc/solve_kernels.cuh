@@ -39,6 +39,16 @@ int solve_coop_max_ctas(int device);
 // between the CTAs of a front ran out (the solve is then invalid). Work per front and chunk: 8 m
 // doubles forward, 16 k backward.
 constexpr int kSweepChunks = 2;  // 8-column chunks carried by one sweep launch
+// levels whose fronts all have m <= kTinyRows and k <= 32 are solved one warp per front (tasks with
+// nr = 1, eight per CTA; ordinary launch)
+constexpr int kTinyRows = 96;
+template <class F>
+cudaError_t launch_fwd_tiny(const SolveTask* tasks, int ntasks, const SnDev* sn, const std::int32_t* cptr,
+                            const ContribEntry* cent, const F* W, const std::int32_t* pidx, double* x, std::int64_t n,
+                            double* vec, const SweepChunks& ck, cudaStream_t s);
+template <class F>
+cudaError_t launch_bwd_tiny(const SolveTask* tasks, int ntasks, const SnDev* sn, const std::int32_t* rows, const F* W,
+                            const std::int32_t* pidx, double* x, std::int64_t n, const SweepChunks& ck, cudaStream_t s);
 template <class F>
 cudaError_t launch_fwd_level(const SolveTask* tasks, int nctas, bool coop, const SnDev* sn, const std::int32_t* cptr,
                              const ContribEntry* cent, const F* W, const std::int32_t* pidx, double* x, std::int64_t n,
