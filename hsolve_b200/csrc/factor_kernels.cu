@@ -376,13 +376,16 @@ __device__ __forceinline__ float warp_maxf(float v) {
 // One warp: threshold Bunch-Kaufman on the panel's diagonal block (order w <= 32, shared memory,
 // ld kNB, all rows candidates). Same acceptance rules as dense_bk; column maxima are reduced in
 // single precision (a threshold test needs no more), the argmax for a 2 x 2 partner only when the
-// 1 x 1 test fails, one reciprocal per pivot, broadcast shared-memory reads in the update.
+// 1 x 1 test fails, one reciprocal per pivot. The update of a step reads the pivot column(s) into
+// registers first, so its column read-modify-writes are independent and pipeline (and the routine
+// stays a compact loop: it runs once per panel, from a cold instruction cache).
 // Warp-synchronous: no block barriers. Returns the eliminated count; [e, w) could not be pivoted.
 template <class R>
 __device__ int warp_block_bk(R* F, int w, bool root, double u, double thr, int* lab, signed char* pv,
                              StepShared& st, int j0 = 0, int prog0 = 0) {
   const int lane = threadIdx.x & 31;
   constexpr int ld = kNB;
+  __shared__ R s_c0[kNB], s_c1[kNB];
   int j = j0, lim = w, prog = prog0, force = 0;
   int neg = 0, pos = 0, zero = 0, two = 0, forced = 0;
   while (j < w) {
@@ -458,11 +461,17 @@ __device__ int warp_block_bk(R* F, int w, bool root, double u, double thr, int* 
       const R x0 = (i >= j + 2 && i < w) ? F[i + j * ld] : R(0);
       const R x1 = (i >= j + 2 && i < w) ? F[i + (j + 1) * ld] : R(0);
       const R l0 = ia * x0 + ib * x1, l1 = ib * x0 + ic * x1;
+      // the pivot columns go through shared memory into registers first, so that the column
+      // updates below are independent of each other (no store can alias a later load)
+      s_c0[i] = x0;
+      s_c1[i] = x1;
       __syncwarp();
-      for (int c2 = j + 2; c2 < w; ++c2) {
-        const R y0 = F[c2 + j * ld], y1 = F[c2 + (j + 1) * ld];
-        if (i >= c2 && i < w) F[i + c2 * ld] -= l0 * y0 + l1 * y1;
-      }
+      R y0[kNB], y1[kNB];
+#pragma unroll
+      for (int c2 = 0; c2 < kNB; ++c2) { y0[c2] = s_c0[c2]; y1[c2] = s_c1[c2]; }
+#pragma unroll
+      for (int c2 = 0; c2 < kNB; ++c2)
+        if (c2 >= j + 2 && i >= c2 && i < w) F[i + c2 * ld] -= l0 * y0[c2] + l1 * y1[c2];
       __syncwarp();
       if (i >= j + 2 && i < w) { F[i + j * ld] = l0; F[i + (j + 1) * ld] = l1; }
       if (lane == 0) { pv[j] = 2; pv[j + 1] = 3; }
@@ -476,12 +485,15 @@ __device__ int warp_block_bk(R* F, int w, bool root, double u, double thr, int* 
       const R inv = nul ? R(0) : R(1) / d;
       const R x = (i > j && i < w) ? F[i + j * ld] : R(0);
       const R xs = x * inv;
+      s_c0[i] = x;
       __syncwarp();
       if (!nul) {
-        for (int c2 = j + 1; c2 < w; ++c2) {
-          const R y = F[c2 + j * ld];
-          if (i >= c2 && i < w) F[i + c2 * ld] -= xs * y;
-        }
+        R y[kNB];
+#pragma unroll
+        for (int c2 = 0; c2 < kNB; ++c2) y[c2] = s_c0[c2];
+#pragma unroll
+        for (int c2 = 0; c2 < kNB; ++c2)
+          if (c2 > j && i >= c2 && i < w) F[i + c2 * ld] -= xs * y[c2];
       }
       __syncwarp();
       if (i > j && i < w) F[i + j * ld] = xs;
@@ -501,66 +513,6 @@ __device__ int warp_block_bk(R* F, int w, bool root, double u, double thr, int* 
   return j;
 }
 
-// Register fast path of warp_block_bk for full blocks (w == 32): lane i keeps row i in registers,
-// the positions are processed in order with compile-time indices and 1 x 1 pivots on their own
-// column. The first position whose 1 x 1 test fails (or that is a null pivot) hands the partially
-// factorized block to the shared-memory routine, which continues from there with the same rules.
-template <class R>
-__device__ int warp_block_bk_fast(R* F, int w, bool root, double u, double thr, int* lab, signed char* pv,
-                                  StepShared& st) {
-  const int lane = threadIdx.x & 31;
-  constexpr int ld = kNB;
-  if (w != kNB || root) return warp_block_bk(F, w, root, u, thr, lab, pv, st);
-  __shared__ __align__(16) R s_col[kNB];
-  R r[kNB];
-#pragma unroll
-  for (int c = 0; c < kNB; ++c) r[c] = c <= lane ? F[lane + c * ld] : R(0);
-  int pos = 0, neg = 0;
-  int stop = kNB;  // first position that needs the general routine
-#pragma unroll
-  for (int j = 0; j < kNB; ++j) {
-    if (stop == kNB) {
-      const R x = lane > j ? r[j] : R(0);
-      const float gcf = warp_maxf(static_cast<float>(fabs(x)));
-      const R d = __shfl_sync(0xffffffffu, r[j], j);
-      const double dcc = fabs(d);
-      const double gc = gcf;
-      const bool ok = dcc > 0.0 && dcc >= u * gc && !(thr >= 0.0 && fmax(dcc, gc) <= thr);
-      if (!ok) {
-        stop = j;
-      } else {
-        const R inv = R(1) / d;
-        const R xs = x * inv;
-        // column j to shared memory once, then broadcast 16-byte reads of F(c, j), c > j
-        s_col[lane] = r[j];
-        __syncwarp();
-        int c0 = j + 1;
-        if (c0 & 1) {
-          if (lane >= c0) r[c0] = fma(-xs, s_col[c0], r[c0]);
-          ++c0;
-        }
-#pragma unroll
-        for (int c = 0; c < kNB; c += 2) {
-          if (c < c0) continue;
-          const auto y2 = load_pair(&s_col[c]);
-          if (lane >= c) r[c] = fma(-xs, y2.x, r[c]);
-          if (lane >= c + 1) r[c + 1] = fma(-xs, y2.y, r[c + 1]);
-        }
-        __syncwarp();
-        if (lane > j) r[j] = xs;
-        if (d < 0) ++neg; else ++pos;
-      }
-    }
-  }
-#pragma unroll
-  for (int c = 0; c < kNB; ++c)
-    if (c <= lane) F[lane + c * ld] = r[c];
-  for (int t = lane; t < stop; t += 32) pv[t] = 1;
-  __syncwarp();
-  if (lane == 0) { st.neg += neg; st.pos += pos; }
-  if (stop == kNB) return kNB;
-  return warp_block_bk(F, w, root, u, thr, lab, pv, st, stop, stop > 0 ? 1 : 0);
-}
 }  // namespace
 
 // ---------------------------------------------------------------------- small fronts (smem)
@@ -835,7 +787,7 @@ __device__ void app_control_and_block(AppFront<R>& F, const FactorParams& prm, d
   if (threadIdx.x == 0) { bst.neg = bst.pos = bst.zero = bst.two = bst.forced = 0; bst.eb = 0; }
   __syncthreads();
   if (threadIdx.x < 32) {
-    const int e = warp_block_bk_fast(Bs, w, force, prm.u, thr, slab, spv, bst);
+    const int e = warp_block_bk(Bs, w, force, prm.u, thr, slab, spv, bst);
     if (threadIdx.x == 0) bst.eb = e;
   }
   __syncthreads();
