@@ -39,9 +39,10 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-# concurrent certified solves of the served form (measured: 3 to 6 workers reach the same throughput
-# on the n = 1e5 pencil, and fewer would leave the GPU idle between the latency-bound phases)
-SERVE_WORKERS = 4
+# concurrent certified solves of the served form (measured on the n = 1e5 pencil: 6 workers 14.7,
+# 4 workers 14.1, 8 workers 14.3 certified solves/s; fewer leave the GPU idle between the
+# latency-bound phases, more only queue on the same SMs)
+SERVE_WORKERS = 6
 
 WORKLOADS = {
     "interval_box1e5": dict(cells=(44, 34, 26), lengths=(1.0, 0.75, 0.55), form="generalized",
