@@ -433,6 +433,69 @@ def run_ours(args, w, rank, world, local):
     return line
 
 
+def scale_record(local):
+    """The path at the size of the reference's 1e6 configuration: the PEC cube 70^3 (Yee/FIT, standard
+    form, n = 999,810), 21 eigenvalues nearest sigma = 1071.43 (midway between two exact levels).
+    One factorization and 8-column solves on their own (roofline at this size: RINFOG flops against the
+    FP64 FMA probe, B_solve bytes against the measured copy bandwidth), then the certified solve through
+    a session (the analysis cached by the first call, as in the served form)."""
+    import torch
+
+    import hsolve_b200 as hsolve
+    from hsolve_b200._native import Factorization
+    from hsolve_b200.api import Session
+    from hsolve_b200.gen import yee
+
+    sigma, k = 1071.4257927949998, 21
+    a, _ = yee.pencil(yee.Box((70, 70, 70)), "standard")
+    n = a.shape[0]
+    f = Factorization(device=local)
+    t0 = time.perf_counter()
+    f.analyze(a, None, 1.0, -sigma)
+    t_an = time.perf_counter() - t0
+    assert f.factorize(1.0, -sigma)  # warm: the kernels' first use
+    est = f.estimate()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    assert f.factorize(1.0, -sigma)
+    torch.cuda.synchronize()
+    t_f = time.perf_counter() - t0
+    rhs = torch.randn((8, n), dtype=torch.float64, device=f"cuda:{local}")
+    x = rhs.clone()
+    f.solve_device(x.data_ptr(), 8, n)  # builds the solve operators, captures the sweeps
+    ts = []
+    for _ in range(5):
+        x.copy_(rhs)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        f.solve_device(x.data_ptr(), 8, n)
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1) / 1e3)
+    t_s = float(np.median(ts))
+    f.close()
+    del x, rhs
+    sess = Session(a, None, device=local)
+    sess.solve(sigma=sigma, k=k)  # warm
+    t0 = time.perf_counter()
+    r = sess.solve(sigma=sigma, k=k)
+    t_c = time.perf_counter() - t0
+    sess.close()
+    peaks, peak_src = measured_peaks()
+    fp64 = hsolve._native.fp64_peak_tflops(local)
+    b_solve = 2 * 8 * est["nnz_l"] + 4 * 8 * n * 8
+    return {"workload": "PEC cube 70^3 (n = 999,810), 21 nearest sigma = 1071.43, standard form, FP64",
+            "certified_solve_s": t_c, "certified": bool(certified(r)), "analysis_s": t_an,
+            "report_times": {kk: r.report[kk] for kk in ("time_factor_s", "time_iterate_s",
+                                                         "time_certificate_s", "time_verify_s")},
+            "factorization": {"ms": 1e3 * t_f, "flops": est["flops"], "achieved": est["flops"] / t_f / 1e12,
+                              "unit": "TFLOP/s", "peak": fp64, "frac": est["flops"] / t_f / 1e12 / fp64},
+            "solve_8_columns": {"ms": 1e3 * t_s, "bytes": b_solve, "achieved": b_solve / t_s / 1e9, "unit": "GB/s",
+                                "peak": peaks["hbm_gbs"], "frac": b_solve / t_s / 1e9 / peaks["hbm_gbs"],
+                                "peak_source": peak_src}}
+
+
 def cpu_certified_step(w, a, b):
     """One certified solve of the workload by the CPU port of the whole path (oracle/cpu_path.py:
     ordering by the reference's own nested dissection where built, analysis, the oracle's
@@ -453,6 +516,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="interval_box1e5", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-scale", action="store_true", help="skip the n = 1e6 record (scale_c3)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     w = WORKLOADS[args.workload]
@@ -475,6 +539,8 @@ def main():
     line = run_ours(args, w, rank, world, local)
     if line is None:
         return 0
+    if world == 1 and not args.no_scale:
+        line["scale_c3"] = scale_record(local)
     if args.no_cpu_baseline or world > 1:
         line.pop("_counts", None)
     else:
