@@ -9,8 +9,9 @@ the oracle and the reference's own sparse kernels.
   interval [40, 200] solve returns the 37 exact eigenvalues within 1e-10 relative, and every pair's
   backward error, recomputed on the host from (A, B, lambda, x) with the reference's residual
   kernel (or scipy where that kernel was not built), is <= 1e-10 and agrees with the report.
-* nearest_cube20 (PEC cube 20^3, standard form, n = 21,660, 10 nearest to sigma = 25, Krylov seed 0):
-  eigenvalues equal the exact spectrum's 10 nearest; certificate counts are exact.
+* nearest_cube20 (PEC cube 20^3, standard form, n = 21,660, 10 nearest to sigma = 25, Krylov seed 0)
+  and, at the size of the reference's 1e6 configuration, the PEC cube 70^3 (n = 999,810, 21 nearest):
+  eigenvalues equal the exact spectrum's k nearest; certificate counts are exact.
 * Nedelec tetrahedra (PEC box 2 x 1 x 0.5, consistent SPD mass): GPU inertia equals the oracle's.
 * hsg_spmm / hsg_shifted_residual against the reference's spmm / shifted_residual
   (src/sparse/kernels.cpp:797,850), p in {1, 8, 16}.
@@ -119,6 +120,29 @@ def test_cube20_nearest_matches_exact_spectrum():
     assert cert["passed"]
     assert cert["count_inertia"] == yee_exact.count_below(w, cert["upper"]) - yee_exact.count_below(w, cert["lower"])
     norm_a = float(abs(spla.eigsh(a, k=1, which="LM", tol=1e-8, return_eigenvectors=False)[0]))
+    eye = sp.identity(a.shape[0], format="csr")
+    for j, lam in enumerate(res.eigenvalues):
+        assert _host_eta(a, eye, lam, res.eigenvectors[:, j], norm_a, 1.0) <= 1e-10
+
+
+def test_cube70_nearest_at_the_1e6_scale_matches_exact_spectrum():
+    """The size of the reference's 1e6 configuration: PEC cube 70^3 (n = 999,810, standard form), the
+    21 eigenvalues nearest a shift midway between two exact levels (fronts up to 16,144, 1.05e9
+    nonzeros in L): eigenvalues within 1e-10 of the exact spectrum, exact certificate counts, every
+    backward error recomputed on the host <= 1e-10."""
+    box = yee.Box((70, 70, 70))
+    a, _ = yee.pencil(box, "standard")
+    assert a.shape[0] == 999810
+    w = yee_exact.exact_spectrum(box.cells, box.lengths)
+    sigma, k = 1071.4257927949998, 21
+    res = hsolve.solve(a, sigma=sigma, k=k)
+    assert res.success, res.report
+    order = np.argsort(np.abs(w - sigma), kind="stable")
+    np.testing.assert_allclose(np.sort(res.eigenvalues), np.sort(w[order[:k]]), rtol=EIG_RTOL)
+    cert = res.report["certificate"]
+    assert cert["passed"]
+    assert cert["count_inertia"] == yee_exact.count_below(w, cert["upper"]) - yee_exact.count_below(w, cert["lower"])
+    norm_a = float(abs(spla.eigsh(a, k=1, which="LM", tol=1e-6, return_eigenvectors=False)[0]))
     eye = sp.identity(a.shape[0], format="csr")
     for j, lam in enumerate(res.eigenvalues):
         assert _host_eta(a, eye, lam, res.eigenvectors[:, j], norm_a, 1.0) <= 1e-10
