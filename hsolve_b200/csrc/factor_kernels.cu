@@ -792,7 +792,8 @@ __device__ void app_control_and_block(AppFront<R>& F, const FactorParams& prm, d
   }
   __syncthreads();
   const int eb = bst.eb;
-  {
+  if (__syncthreads_or(threadIdx.x < w && slab[threadIdx.x] != static_cast<int>(threadIdx.x))) {
+    // the block's rows were swapped: its pivot labels follow
     int old = 0;
     if (threadIdx.x < w) old = F.plab[p + slab[threadIdx.x]];
     __syncthreads();
@@ -834,11 +835,12 @@ __device__ void app_rows(AppFront<R>& F, const StepView& v, int rank, int nr, R*
     if (t < w && s < t && s < eb && !(spv[s] == 2 && s + 1 == t)) x = Bs[t + s * kNB];
     Lm[e] = x;
   }
-  __syncthreads();
+  // did the block factorization swap any of its rows? (rarely: then the permutation below moves data)
+  const bool permuted = __syncthreads_or(threadIdx.x < w && slab[threadIdx.x] != static_cast<int>(threadIdx.x)) != 0;
   // permute the L rows p..p+w-1 of the eliminated columns c < p (a thread owns a column; the
   // columns are split into contiguous chunks over the ranks)
   const int cchunk = (p + nr - 1) / nr;
-  const int cend = min(p, (rank + 1) * cchunk);
+  const int cend = permuted ? min(p, (rank + 1) * cchunk) : 0;
   for (int cc = rank * cchunk + threadIdx.x; cc < cend; cc += blockDim.x) {
     R x[kNB];
     R* colp = F.f.col(cc) + p;
