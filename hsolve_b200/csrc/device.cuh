@@ -30,12 +30,16 @@ struct ContribEntry {
   std::int32_t mc;
 };
 
-// One CTA of a solve sweep level: front s, the CTA's rank among the front's nr CTAs, and the offset
-// of the front's work vectors.
+// One CTA of a solve sweep level: front s, the CTA's rank among the front's CTAs, and the offset of
+// the front's work vectors. Backward, the contribution-row tiles of every 32-column chunk may be cut
+// into `parts` parts: part 0 is the chunk owner's, parts 1.. belong to helper CTAs (ranks nr + h,
+// h = chunk + nch (part - 1)) that publish partial sums through the chunk's counter.
 struct SolveTask {
   std::int32_t s;
-  std::int32_t rank;
-  std::int32_t nr;
+  std::int32_t rank;   // < nr: a chunk owner; nr + h: backward helper h
+  std::int32_t nr;     // owner CTAs of the front
+  std::int32_t parts;  // backward: parts of each chunk's contribution-row tiles (1: no helpers)
+  std::int32_t hcnt;   // backward: first of the front's per-chunk helper counters
   std::int32_t pad;
   std::int64_t wofs;
 };

@@ -39,6 +39,8 @@ constexpr std::size_t kAnalysisCacheEntries = 8;
 // panel entries per CTA of a solve sweep (fewer, busier CTAs: their waits hold fewer SMs from
 // concurrent requests)
 constexpr double kSolveEntriesPerCta = 32768.0;
+// most parts a backward chunk's contribution-row tiles are cut into (owner + helpers)
+constexpr int kSolveParts = 4;
 std::mutex g_analysis_mu;
 std::list<AnalysisEntry> g_analysis_cache;  // most recently used first
 
@@ -358,6 +360,7 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
   if (coop_max_ == 0) coop_max_ = coop_max_ctas(opt_.device);
   if (solve_coop_max_ == 0) solve_coop_max_ = solve_coop_max_ctas(opt_.device);
   std::vector<SolveTask> tasks;
+  std::int32_t hcnt_total = 0;  // backward helper counters: one per 32-column chunk of every front
   std::int64_t work_max = 0;
   std::vector<int2> sbl;
   std::vector<int4> tiles;
@@ -405,11 +408,17 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
     {
       std::int64_t wofs = 0;
       std::vector<std::int64_t> fwofs(all.size());
+      std::vector<std::int32_t> hoff(all.size());
       for (std::size_t q = 0; q < all.size(); ++q) {
         const std::int32_t sq = all[q];
         SnDev& dw = sn[sq];
         fwofs[q] = wofs;
-        wofs += std::max<std::int64_t>(8 * static_cast<std::int64_t>(dw.m), 16 * static_cast<std::int64_t>(dw.k));
+        // forward t (8 m); backward s and the entry values (16 k) and the helpers' partial sums
+        wofs += std::max<std::int64_t>(8 * static_cast<std::int64_t>(dw.m),
+                                       16 * static_cast<std::int64_t>(dw.k) +
+                                           256 * static_cast<std::int64_t>((dw.k + 31) / 32) * (kSolveParts - 1));
+        hoff[q] = hcnt_total;
+        hcnt_total += (dw.k + 31) / 32;
         dw.cptr_off = static_cast<std::int64_t>(cptr.size());
         std::vector<std::int32_t> num(dw.m + 1, 0);
         for (std::int32_t e = S.child_ptr[sq]; e < S.child_ptr[sq + 1]; ++e) {
@@ -462,13 +471,38 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
             nr[q] = spare > 0 && wsum > 0.0 ? std::min(cap(dd), 1 + static_cast<int>(std::floor(spare * w / wsum))) : 1;
           }
         }
+        // backward helpers: where the level's CTAs fit the co-resident bound with room to spare, the
+        // contribution-row tiles of each chunk of the widest fronts are cut into up to kSolveParts
+        // parts (about 16 tiles per CTA), parts 1.. on helper CTAs
+        std::vector<int> parts(all.size(), 1);
+        int used = 0;
+        for (int v : nr) used += v;
+        if (bwd && used <= budget) {
+          int spare = budget - used;
+          std::vector<std::size_t> by(all.size());
+          std::iota(by.begin(), by.end(), std::size_t{0});
+          std::stable_sort(by.begin(), by.end(), [&](std::size_t x, std::size_t y) {
+            return sn[all[x]].m - sn[all[x]].k > sn[all[y]].m - sn[all[y]].k;
+          });
+          for (std::size_t q : by) {
+            const SnDev& dd = sn[all[q]];
+            const int nch = (dd.k + 31) / 32, t2 = (dd.m - dd.k + 31) / 32;
+            if (nch == 0 || spare < nch) continue;
+            int want = std::min({kSolveParts, std::max(1, (t2 + 4 + 15) / 16), std::max(1, t2)});
+            want = std::min(want, 1 + spare / nch);
+            parts[q] = want;
+            spare -= nch * (want - 1);
+          }
+        }
         off = static_cast<std::int64_t>(tasks.size());
         coop = false;
-        for (std::size_t q = 0; q < all.size(); ++q)
-          for (int r = 0; r < nr[q]; ++r) {
-            tasks.push_back(SolveTask{all[q], r, nr[q], 0, fwofs[q]});
-            coop = coop || nr[q] > 1;
-          }
+        for (std::size_t q = 0; q < all.size(); ++q) {
+          const int nch = (sn[all[q]].k + 31) / 32;
+          const int helpers = bwd ? nch * (parts[q] - 1) : 0;
+          for (int r = 0; r < nr[q] + helpers; ++r)
+            tasks.push_back(SolveTask{all[q], r, nr[q], bwd ? parts[q] : 1, bwd ? hoff[q] : 0, 0, fwofs[q]});
+          coop = coop || nr[q] > 1 || helpers > 0;
+        }
         ctas = static_cast<int>(static_cast<std::int64_t>(tasks.size()) - off);
       };
       L.tiny = !all.empty();
@@ -598,6 +632,7 @@ std::shared_ptr<FrontPlan> GpuFactor::make_plan() {
   P.iperm.upload(S.iperm, stream_);
   P.dest.upload(S.dest, stream_);
   P.tasks.upload(tasks, stream_);
+  P.hcnt_total = hcnt_total;
   P.cptr.upload(cptr, stream_);
   P.cent.upload(cent, stream_);
   P.sbl.upload(sbl, stream_);
@@ -629,7 +664,7 @@ void GpuFactor::alloc_work() {
   d_level_done_.alloc(static_cast<std::size_t>(std::max(1, P.ncoop)));
   d_work_.alloc(static_cast<std::size_t>(std::max<std::int64_t>(1, P.work_max)) * kSweepChunks);
   d_err_.alloc(1);
-  d_sweep_cnt_.alloc(static_cast<std::size_t>(3 * std::max(1, sym_.ns)) * kSweepChunks);
+  d_sweep_cnt_.alloc(static_cast<std::size_t>(3 * std::max(1, sym_.ns) + P.hcnt_total) * kSweepChunks);
   w_ready_ = false;
 }
 
@@ -917,13 +952,14 @@ void GpuFactor::run_sweeps_t(double* xwork, double* vec, int nr) {
   int* fcnt = d_sweep_cnt_.p;
   int* bcnt = fcnt + ns;
   int* arrive = bcnt + ns;
+  int* hcnt = arrive + ns;
   // launches carry up to kSweepChunks chunks of 8 right-hand sides, each with its own contribution
   // vectors (vec_total x 8), work array and counters
   const int span = 8 * kSweepChunks;
   for (int c0 = 0; c0 < nr; c0 += span) {
     SweepChunks ck;
     ck.ncols = std::min(span, nr - c0);
-    ck.cnt_stride = 3 * ns;
+    ck.cnt_stride = 3 * ns + plan_->hcnt_total;
     ck.x_stride = 8 * n_;
     ck.vec_stride = 8 * std::max<std::int64_t>(1, plan_->vec_total);
     ck.work_stride = std::max<std::int64_t>(1, plan_->work_max);
@@ -949,7 +985,7 @@ void GpuFactor::run_sweeps_t(double* xwork, double* vec, int nr) {
                    "backward solve");
       else
         cuda_check(launch_bwd_level<F>(tasks + it->bwd_task_off[c], it->bwd_ctas[c], it->bwd_coop[c], plan_->sn.p,
-                                       plan_->rows.p, W, d_pidx_.p, xw, n_, ck, d_work_.p, bcnt, arrive, d_err_.p, s),
+                                       plan_->rows.p, W, d_pidx_.p, xw, n_, ck, d_work_.p, bcnt, arrive, hcnt, d_err_.p, s),
                    "backward solve");
     }
   }

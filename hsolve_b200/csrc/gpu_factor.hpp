@@ -115,6 +115,7 @@ struct FrontPlan {
   std::int64_t arena_entries = 1;  // inertia-only counts: the largest level's panels
   std::int64_t scratch_max = 0, work_max = 0, w_total = 0;
   int ncoop = 0, nsbl = 0, ntiles = 0;
+  std::int32_t hcnt_total = 0;     // backward helper counters (one per 32-column chunk of every front)
   DevBuf<std::int32_t> row, col;   // the union pattern's entries (row, column)
   DevBuf<std::int64_t> dest;       // their positions in the factor storage
   DevBuf<SnDev> sn;

@@ -396,7 +396,7 @@ template <class F>
 __global__ void __launch_bounds__(256, 2) k_bwd_level(const SolveTask* tasks, const SnDev* sn, const std::int32_t* rows,
                                                        const F* W, const std::int32_t* pidx, double* x,
                                                        std::int64_t n, SweepChunks ck, double* work, int* cnts,
-                                                       int* arrive, int* err) {
+                                                       int* arrive, int* hcnts, int* err) {
   extern __shared__ double dsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* wt = dsm + warp * kWarpSmem;     // wt[c * kTilePitch + i]: W[i0 + i, j0 + c]
@@ -410,38 +410,25 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const SolveTask* tasks, co
   arrive += blockIdx.y * ck.cnt_stride;
   const SolveTask tk = tasks[blockIdx.x];
   const SnDev d = sn[tk.s];
-  const int m = d.m, k = d.k, rank = tk.rank, nr = tk.nr;
+  const int m = d.m, k = d.k, rank = tk.rank, nr = tk.nr, P = tk.parts;
   if (k == 0) return;
   double* sv = work + tk.wofs;
   double* ta = sv + static_cast<std::int64_t>(k) * 8;
+  double* partial = ta + static_cast<std::int64_t>(k) * 8;  // [chunk][part - 1][32 columns][8]
   int* cnt = cnts + tk.s;
+  int* hc = hcnts + blockIdx.y * ck.cnt_stride + tk.hcnt;  // per chunk: helper parts published
   const F* Wf = W + d.w_off;
   const std::int32_t* pl = pidx + d.first;
   const std::int32_t* rw = rows + d.rows_off;
   const int nsb = (k + kSB - 1) / kSB, nch = (k + 31) / 32;
-  const int nown = owned_below(nch, rank, nr);
-  for (int idx = threadIdx.x; idx < nown * 32; idx += blockDim.x) {
-    const int i = (rank + (idx >> 5) * nr) * 32 + (idx & 31);
-    if (i >= k) continue;
-#pragma unroll
-    for (int r = 0; r < 8; ++r)
-      ta[static_cast<std::int64_t>(i) * 8 + r] = r < nrhs ? x[d.first + pl[i] + static_cast<std::int64_t>(r) * n] : 0.0;
-  }
-  if (nr > 1) {
-    publish(arrive + tk.s, 1, nr);
-    wait_count(arrive + tk.s, nr, err);
-  } else {
-    __syncthreads();
-  }
-  const int lastb = (nsb - 1) * kSB;
-  for (int u = 0; u < nown; ++u) {
-    const int j0 = (rank + u * nr) * 32;
-    const int bA = (j0 / kSB) * kSB, beA = min(bA + kSB, k);
-    const int t1 = (beA - bA + 31) / 32, t2 = (m - k + 31) / 32;
-    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int tau = warp; tau < t1 + t2; tau += 8) {
-      const bool own = tau < t1;
-      const int i = (own ? bA + 32 * tau : k + 32 * (tau - t1)) + lane;
+  const int t2 = (m - k + 31) / 32;  // contribution-row tiles of a chunk
+  // the warp's share of ntl tiles of chunk j0: tiles tau < t1o are rows [bA, beA) of the chunk's
+  // super-block (entry values from ta, sign +), the others contribution-row tiles cb0 + (tau - t1o)
+  // (x of the ancestors, sign -); every tile is staged in shared memory so that lane c sums column c
+  auto sum_tiles = [&](int j0, int t1o, int bA, int beA, int cb0, int ntl, double* acc) {
+    for (int tau = warp; tau < ntl; tau += 8) {
+      const bool own = tau < t1o;
+      const int i = (own ? bA + 32 * tau : k + 32 * (cb0 + tau - t1o)) + lane;
       const bool ok = i < (own ? beA : m);
       const F* Wi = Wf + i + static_cast<std::int64_t>(j0) * m;
       double wv[32];
@@ -474,16 +461,63 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const SolveTask* tasks, co
       }
       __syncwarp();
     }
+  };
+  if (rank >= nr) {
+    // helper: part q of chunk ch's contribution-row tiles; its sum goes to the chunk's partials
+    // (it reads only W and the ancestors' final x, so it waits for nothing)
+    const int h = rank - nr, ch = h % nch, q = 1 + h / nch;
+    const int lo = (q * t2) / P, hi = ((q + 1) * t2) / P;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    sum_tiles(ch * 32, 0, 0, 0, lo, hi - lo, acc);
+    __syncthreads();  // red overlays the tiles
+#pragma unroll
+    for (int r = 0; r < 8; ++r) red[(warp * 32 + lane) * 9 + r] = acc[r];
+    __syncthreads();
+    {
+      const int cc = threadIdx.x >> 3, r = threadIdx.x & 7;
+      double sum = 0.0;
+#pragma unroll
+      for (int w = 0; w < 8; ++w) sum += red[(w * 32 + cc) * 9 + r];
+      partial[(static_cast<std::int64_t>(ch) * (P - 1) + (q - 1)) * 256 + cc * 8 + r] = sum;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(hc + ch, 1);
+    return;
+  }
+  const int nown = owned_below(nch, rank, nr);
+  for (int idx = threadIdx.x; idx < nown * 32; idx += blockDim.x) {
+    const int i = (rank + (idx >> 5) * nr) * 32 + (idx & 31);
+    if (i >= k) continue;
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+      ta[static_cast<std::int64_t>(i) * 8 + r] = r < nrhs ? x[d.first + pl[i] + static_cast<std::int64_t>(r) * n] : 0.0;
+  }
+  if (nr > 1) {
+    publish(arrive + tk.s, 1, nr);
+    wait_count(arrive + tk.s, nr, err);
+  } else {
+    __syncthreads();
+  }
+  const int lastb = (nsb - 1) * kSB;
+  for (int u = 0; u < nown; ++u) {
+    const int ch = rank + u * nr, j0 = ch * 32;
+    const int bA = (j0 / kSB) * kSB, beA = min(bA + kSB, k);
+    const int t1 = (beA - bA + 31) / 32;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    sum_tiles(j0, t1, bA, beA, 0, t1 + t2 / P, acc);  // the super-block's rows and part 0
     __syncthreads();  // every warp is done with its tiles: red overlays them
 #pragma unroll
     for (int r = 0; r < 8; ++r) red[(warp * 32 + lane) * 9 + r] = acc[r];
     __syncthreads();
+    if (P > 1) wait_count(hc + ch, P - 1, err);  // the helpers' parts of this chunk
     const bool fin = bA == lastb;  // the last super-block: s is x
     {
       const int cc = threadIdx.x >> 3, r = threadIdx.x & 7, j = j0 + cc;
       double s = 0.0;
 #pragma unroll
       for (int w = 0; w < 8; ++w) s += red[(w * 32 + cc) * 9 + r];
+      for (int q = 1; q < P; ++q) s += __ldcg(&partial[(static_cast<std::int64_t>(ch) * (P - 1) + (q - 1)) * 256 + cc * 8 + r]);
       if (j < k) {
         sv[static_cast<std::int64_t>(j) * 8 + r] = s;
         if (fin && r < nrhs) x[d.first + pl[j] + static_cast<std::int64_t>(r) * n] = s;
@@ -748,17 +782,17 @@ cudaError_t launch_fwd_level(const SolveTask* tasks, int nctas, bool coop, const
 template <class F>
 cudaError_t launch_bwd_level(const SolveTask* tasks, int nctas, bool coop, const SnDev* sn, const std::int32_t* rows,
                              const F* W, const std::int32_t* pidx, double* x, std::int64_t n, const SweepChunks& ck,
-                             double* work, int* cnts, int* arrive, int* err, cudaStream_t s) {
+                             double* work, int* cnts, int* arrive, int* hcnts, int* err, cudaStream_t s) {
   if (nctas <= 0 || ck.ncols <= 0) return cudaSuccess;
   configure_bwd<F>();
   const dim3 grid(nctas, (ck.ncols + 7) / 8);
   SweepChunks c = ck;
   note_launches(1);
   if (!coop) {
-    k_bwd_level<F><<<grid, 256, kBwdSmemBytes, s>>>(tasks, sn, rows, W, pidx, x, n, c, work, cnts, arrive, err);
+    k_bwd_level<F><<<grid, 256, kBwdSmemBytes, s>>>(tasks, sn, rows, W, pidx, x, n, c, work, cnts, arrive, hcnts, err);
     return cudaGetLastError();
   }
-  void* args[] = {&tasks, &sn, &rows, &W, &pidx, &x, &n, &c, &work, &cnts, &arrive, &err};
+  void* args[] = {&tasks, &sn, &rows, &W, &pidx, &x, &n, &c, &work, &cnts, &arrive, &hcnts, &err};
   return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_bwd_level<F>), grid, dim3(256), args, kBwdSmemBytes,
                                      s);
 }
@@ -794,7 +828,7 @@ cudaError_t launch_bwd_tiny(const SolveTask* tasks, int ntasks, const SnDev* sn,
                                            double*, const SweepChunks&, double*, int*, int*, cudaStream_t);            \
   template cudaError_t launch_bwd_level<F>(const SolveTask*, int, bool, const SnDev*, const std::int32_t*, const F*, \
                                            const std::int32_t*, double*, std::int64_t, const SweepChunks&, double*,    \
-                                           int*, int*, int*, cudaStream_t);                                            \
+                                           int*, int*, int*, int*, cudaStream_t);                                      \
   template cudaError_t launch_fwd_tiny<F>(const SolveTask*, int, const SnDev*, const std::int32_t*,                  \
                                           const ContribEntry*, const F*, const std::int32_t*, double*, std::int64_t,   \
                                           double*, const SweepChunks&, cudaStream_t);                                  \

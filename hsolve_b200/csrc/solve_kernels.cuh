@@ -36,8 +36,9 @@ int solve_coop_max_ctas(int device);
 // 8-column chunk of the ck.ncols right-hand sides (grid nctas x chunks); coop: the level has fronts
 // of several CTAs (cooperative launch, nctas x chunks <= solve_coop_max_ctas). cnts / arrive: one
 // counter per front and chunk, zero at the first launch of a sweep; err: set to 1 when a wait
-// between the CTAs of a front ran out (the solve is then invalid). Work per front and chunk: 8 m
-// doubles forward, 16 k backward.
+// between the CTAs of a front ran out (the solve is then invalid); hcnts: backward, one counter per
+// 32-column chunk of every front (at SolveTask::hcnt), zero at the first launch. Work per front and
+// chunk: 8 m doubles forward, 16 k + 256 nch (parts - 1) backward.
 constexpr int kSweepChunks = 2;  // 8-column chunks carried by one sweep launch
 // levels whose fronts all have m <= kTinyRows and k <= 32 are solved one warp per front (tasks with
 // nr = 1, eight per CTA; ordinary launch)
@@ -56,6 +57,6 @@ cudaError_t launch_fwd_level(const SolveTask* tasks, int nctas, bool coop, const
 template <class F>
 cudaError_t launch_bwd_level(const SolveTask* tasks, int nctas, bool coop, const SnDev* sn, const std::int32_t* rows,
                              const F* W, const std::int32_t* pidx, double* x, std::int64_t n, const SweepChunks& ck,
-                             double* work, int* cnts, int* arrive, int* err, cudaStream_t s);
+                             double* work, int* cnts, int* arrive, int* hcnts, int* err, cudaStream_t s);
 
 }  // namespace hsg
