@@ -423,6 +423,38 @@ void copy_cols(std::int64_t n, int p, const double* x, std::int64_t ldx, double*
   k_copy_cols<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, x, ldx, y, ldy);
 }
 
+namespace {
+// Lanczos recurrence with device-resident coefficients (ab[j]: alpha_j = v_j^T A v_j; ab[kLanczosMax + j]:
+// beta_j^2 = ||w_j||^2): w -= alpha_j v_j + beta_{j-1} v_{j-1}
+__global__ void k_lanczos_orth(std::int64_t n, double* w, const double* v, const double* vp, const double* ab, int j,
+                               int stride) {
+  const double alpha = ab[j];
+  const double beta = j > 0 ? sqrt(fmax(ab[stride + j - 1], 0.0)) : 0.0;
+  for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<std::int64_t>(gridDim.x) * blockDim.x)
+    w[i] -= alpha * v[i] + (j > 0 ? beta * vp[i] : 0.0);
+}
+// v = w / sqrt(nrm2[0]) (zero when the norm is zero: the Krylov space is invariant)
+__global__ void k_scale_by_norm(std::int64_t n, const double* w, double* v, const double* nrm2) {
+  const double q = nrm2[0];
+  const double f = q > 0.0 ? 1.0 / sqrt(q) : 0.0;
+  for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<std::int64_t>(gridDim.x) * blockDim.x)
+    v[i] = w[i] * f;
+}
+}  // namespace
+
+void lanczos_orth(std::int64_t n, double* w, const double* v, const double* vp, const double* ab, int j, int stride,
+                  cudaStream_t s) {
+  note_launches(1);
+  k_lanczos_orth<<<grid_for(n, 256), 256, 0, s>>>(n, w, v, vp, ab, j, stride);
+}
+
+void scale_by_norm(std::int64_t n, const double* w, double* v, const double* nrm2, cudaStream_t s) {
+  note_launches(1);
+  k_scale_by_norm<<<grid_for(n, 256), 256, 0, s>>>(n, w, v, nrm2);
+}
+
 void fill_normal(std::int64_t n, int p, double* y, std::int64_t ldy, std::uint64_t seed, cudaStream_t s) {
   note_launches(1);
   k_fill_normal<<<grid_for(n * p, 256), 256, 0, s>>>(n, p, y, ldy, seed);

@@ -35,6 +35,11 @@ void diag_scale(std::int64_t n, int p, const double* d, const double* x, std::in
 void copy_cols(std::int64_t n, int p, const double* x, std::int64_t ldx, double* y, std::int64_t ldy, cudaStream_t s);
 // standard normal entries from a counter-based stream (deterministic in seed)
 void fill_normal(std::int64_t n, int p, double* y, std::int64_t ldy, std::uint64_t seed, cudaStream_t s);
+// Lanczos with coefficients on the device: w -= ab[j] v + sqrt(ab[stride + j - 1]) vp (no second
+// term for j = 0); v = w / sqrt(nrm2[0]) (zero for a zero norm)
+void lanczos_orth(std::int64_t n, double* w, const double* v, const double* vp, const double* ab, int j, int stride,
+                  cudaStream_t s);
+void scale_by_norm(std::int64_t n, const double* w, double* v, const double* nrm2, cudaStream_t s);
 // R = B (X + sigma Y) - A Y (B == null: B = I) for p columns in one sweep over the rows of A and B,
 // and omega[c] = max_i |R(i, c)| / (|B| |X + sigma Y| + |A| |Y|)(i, c), the componentwise backward
 // error of every column (device array of p doubles, or null). r may be null (omega only).
