@@ -71,6 +71,7 @@ SIGNATURES = {
                                             _P]),
     "hsg_compute_ordering": (ctypes.c_int, [_I64, _P, _P, ctypes.c_uint64, _P]),
     "hsg_symbolic_stats": (ctypes.c_int, [_I64, _P, _P, _P, _I32, _P]),
+    "hsg_csr_inspect": (ctypes.c_int, [_I64, _P, _P, _P, _P, _P, _P, _P]),
 }
 
 
@@ -227,6 +228,27 @@ class Factorization:
 
     def order(self) -> int:
         return int(lib().hsg_order(self._h))
+
+
+def csr_inspect(m):
+    """hsg_csr_inspect on a real CSR matrix (host threads; the interpreter lock is released meanwhile):
+    (sorted without duplicates, explicit zero stored, structurally symmetric, entries above / below
+    the diagonal, ||M - M^T||_F / ||M||_F, (M + M^T) / 2 on M's pattern or None when M is symmetric)."""
+    n = m.shape[0]
+    rp = np.ascontiguousarray(m.indptr, dtype=np.int64)
+    ci = np.ascontiguousarray(m.indices, dtype=np.int32)
+    v = np.ascontiguousarray(m.data, dtype=np.float64)
+    flags = np.zeros(3, dtype=np.int32)
+    counts = np.zeros(2, dtype=np.int64)
+    defect = ctypes.c_double()
+    check(lib().hsg_csr_inspect(n, _ptr(rp), _ptr(ci), _ptr(v), _ptr(flags), _ptr(counts), ctypes.byref(defect),
+                                None))
+    sym = None
+    if flags[0] and flags[2] and defect.value > 0:  # a second pass forms (M + M^T) / 2
+        sym = np.empty(v.size)
+        check(lib().hsg_csr_inspect(n, _ptr(rp), _ptr(ci), _ptr(v), _ptr(flags), _ptr(counts),
+                                    ctypes.byref(defect), _ptr(sym)))
+    return bool(flags[0]), bool(flags[1]), bool(flags[2]), int(counts[0]), int(counts[1]), defect.value, sym
 
 
 def compute_ordering(A, seed: int = 2026) -> np.ndarray:

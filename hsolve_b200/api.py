@@ -217,6 +217,12 @@ def _struct_from(cfg: dict, verbose: int) -> _SolveConfig:
     return c
 
 
+def _is_csr(m) -> bool:
+    import scipy.sparse as sp
+
+    return sp.issparse(m) and m.format == "csr"
+
+
 def _as_csr(m, name, storage):
     import scipy.sparse as sp
 
@@ -297,6 +303,27 @@ def _complex_dtype(m) -> bool:
     if sp.issparse(m):
         return np.iscomplexobj(m.data)
     return np.iscomplexobj(np.asarray(m))
+
+
+def _prepare(m, name, storage, tol):
+    """The input as a canonical CSR matrix holding both triangles, symmetrized, with its Hermitian
+    defect: _as_csr + _hermitian_check. A real CSR matrix that is already canonical (sorted, no
+    duplicates, no stored zeros), holds both triangles and is structurally symmetric is checked by
+    the native hsg_csr_inspect on host threads, outside the interpreter lock; every other input takes
+    the general path."""
+    import scipy.sparse as sp
+
+    if (storage == "auto" and sp.issparse(m) and m.format == "csr" and m.dtype == np.float64 and m.ndim == 2
+            and m.shape[0] == m.shape[1] and m.nnz > 0 and m.indices.dtype in (np.int32, np.int64)
+            and m.shape[0] < 2**31):
+        canonical, zero, symmetric, up, lo, defect, sym = _native.csr_inspect(m)
+        if canonical and not zero and symmetric and (up == 0) == (lo == 0):
+            if defect > tol:
+                raise NotHermitianError(f"{name}: ||M - M^H||_F / ||M||_F = {defect:.3e} > hermitian_tol = {tol:g}")
+            if defect > 0:
+                m = sp.csr_matrix((sym, m.indices.copy(), m.indptr.copy()), shape=m.shape)
+            return m, defect
+    return _hermitian_check(_as_csr(m, name, storage), name, tol)
 
 
 def _hermitian_check(m, name, tol):
@@ -440,16 +467,15 @@ def solve(A, B=None, *, sigma=None, k=_Default(6), mode=_Default("nearest"), low
     cfg = merge_config(config, sigma, k, mode, lower, upper, tol, threads)
     verbose = _integer(verbose, "verbose")
     cdtype = _complex_dtype(A) or (B is not None and _complex_dtype(B))
-    a = _as_csr(A, "A", storage)
     htol = float(cfg.get("hermitian_tol", 1e-10))
-    a, da = _hermitian_check(a, "A", htol)
+    a, da = _prepare(A, "A", storage, htol)
     b = None
     db = 0.0
     if B is not None:
-        b = _as_csr(B, "B", storage)
+        b = _as_csr(B, "B", storage) if not _is_csr(B) else B
         if b.shape != a.shape:
             raise InvalidInputError(f"A is {a.shape} but B is {b.shape}")
-        b, db = _hermitian_check(b, "B", htol)
+        b, db = _prepare(b, "B", storage, htol)
     if np.iscomplexobj(a.data) or (b is not None and np.iscomplexobj(b.data)):
         ae, be = _embed(a), (_embed(b) if b is not None else None)
         w, v, report, _ = _eigsolve(ae, be, _struct_from(_embedded_config(cfg), verbose))
@@ -545,15 +571,14 @@ class Session:
     def __init__(self, A, B=None, *, device: int = 0, seed: int = 2026, storage: str = "auto",
                  hermitian_tol: float = 1e-10):
         self._cdtype = _complex_dtype(A) or (B is not None and _complex_dtype(B))
-        a = _as_csr(A, "A", storage)
-        a, self._da = _hermitian_check(a, "A", hermitian_tol)
+        a, self._da = _prepare(A, "A", storage, hermitian_tol)
         self._db = 0.0
         b = None
         if B is not None:
-            b = _as_csr(B, "B", storage)
+            b = _as_csr(B, "B", storage) if not _is_csr(B) else B
             if b.shape != a.shape:
                 raise InvalidInputError(f"A is {a.shape} but B is {b.shape}")
-            b, self._db = _hermitian_check(b, "B", hermitian_tol)
+            b, self._db = _prepare(b, "B", storage, hermitian_tol)
         self._complex = None
         if np.iscomplexobj(a.data) or (b is not None and np.iscomplexobj(b.data)):
             self._complex = (a, b)  # kept for the eigenvectors; the session holds the embedding

@@ -1,7 +1,9 @@
 // Host-only C ABI entry points (no GPU needed): status strings, ordering, symbolic statistics.
 #include <atomic>
 #include <cmath>
+#include <algorithm>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "common.hpp"
@@ -88,6 +90,76 @@ int hsg_symbolic_stats(int64_t n, const int64_t* rowptr, const int32_t* col, con
     out->max_front = s.max_front;
     out->ordering_s = s.ordering_seconds;
     out->analyze_s = s.ordering_seconds + s.symbolic_seconds;
+  });
+}
+
+int hsg_csr_inspect(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val, int32_t* flags,
+                    int64_t* counts, double* defect, double* sym) {
+  return guarded([&] {
+    HSG_REQUIRE(n >= 0 && rowptr && flags && counts && defect, HSG_INVALID_INPUT, "hsg_csr_inspect: null argument");
+    const int64_t nnz = rowptr[n];
+    HSG_REQUIRE(nnz == 0 || (col && val), HSG_INVALID_INPUT, "hsg_csr_inspect: null arrays");
+    // rows split over threads; every partial result is combined in thread order
+    const int nt = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>({8, std::thread::hardware_concurrency() ? static_cast<int64_t>(std::thread::hardware_concurrency()) : 1, n / 4096 + 1})));
+    struct Part {
+      bool sorted = true, zero = false, symmetric = true;
+      int64_t up = 0, lo = 0;
+      double d2 = 0.0, m2 = 0.0;
+    };
+    std::vector<Part> parts(nt);
+    // pass 1: order, zeros, triangle counts
+    auto pass1 = [&](int t) {
+      Part& q = parts[t];
+      for (int64_t i = n * t / nt; i < n * (t + 1) / nt; ++i)
+        for (int64_t e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+          const int64_t j = col[e];
+          if (j < 0 || j >= n) { q.sorted = false; continue; }
+          if (e > rowptr[i] && col[e - 1] >= j) q.sorted = false;
+          if (val[e] == 0.0) q.zero = true;
+          if (j > i) ++q.up;
+          else if (j < i) ++q.lo;
+        }
+    };
+    auto run = [&](auto&& f) {
+      std::vector<std::thread> th;
+      for (int t = 1; t < nt; ++t) th.emplace_back(f, t);
+      f(0);
+      for (auto& x : th) x.join();
+    };
+    run(pass1);
+    bool sorted = true, zero = false;
+    int64_t up = 0, lo = 0;
+    for (const Part& q : parts) { sorted = sorted && q.sorted; zero = zero || q.zero; up += q.up; lo += q.lo; }
+    flags[0] = sorted ? 1 : 0;
+    flags[1] = zero ? 1 : 0;
+    counts[0] = up;
+    counts[1] = lo;
+    flags[2] = 0;
+    *defect = 0.0;
+    if (!sorted) return;
+    // pass 2 (sorted rows): the transposed entry of every (i, j) by binary search in row j
+    auto pass2 = [&](int t) {
+      Part& q = parts[t];
+      for (int64_t i = n * t / nt; i < n * (t + 1) / nt; ++i)
+        for (int64_t e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+          const int64_t j = col[e];
+          const int32_t* b = col + rowptr[j];
+          const int32_t* en = col + rowptr[j + 1];
+          const int32_t* f = std::lower_bound(b, en, static_cast<int32_t>(i));
+          const double v = val[e];
+          q.m2 += v * v;
+          if (f == en || *f != i) { q.symmetric = false; continue; }
+          const double vt = val[rowptr[j] + (f - b)];
+          q.d2 += (v - vt) * (v - vt);
+          if (sym) sym[e] = 0.5 * (v + vt);
+        }
+    };
+    run(pass2);
+    bool symmetric = true;
+    double d2 = 0.0, m2 = 0.0;
+    for (const Part& q : parts) { symmetric = symmetric && q.symmetric; d2 += q.d2; m2 += q.m2; }
+    flags[2] = symmetric ? 1 : 0;
+    *defect = m2 > 0.0 ? std::sqrt(d2) / std::sqrt(m2) : 0.0;
   });
 }
 

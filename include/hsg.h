@@ -201,6 +201,15 @@ HSG_API int hsg_compute_ordering(int64_t n, const int64_t* rowptr, const int32_t
 HSG_API int hsg_symbolic_stats(int64_t n, const int64_t* rowptr, const int32_t* col, const int32_t* pivot_order,
                        int32_t amalgamate, hsg_estimate_t* out);
 
+/* Input checks of hsolve.solve on a real CSR matrix (python/hsolve/__init__.py:347-419 validates the
+ * same properties), on host threads: flags[0] = 1 when every row's columns are strictly increasing
+ * (sorted, no duplicates), flags[1] = 1 when an explicit zero is stored, flags[2] = 1 when the
+ * pattern is structurally symmetric; counts[0] / counts[1] = entries strictly above / below the
+ * diagonal; *defect = ||M - M^T||_F / ||M||_F (valid when flags[0] and flags[2]); sym (nullable, nnz
+ * entries) receives (M + M^T) / 2 on M's pattern when the defect is positive. */
+HSG_API int hsg_csr_inspect(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val, int32_t* flags,
+                            int64_t* counts, double* defect, double* sym);
+
 #ifdef __cplusplus
 }
 #endif

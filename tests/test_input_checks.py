@@ -144,3 +144,45 @@ def test_not_hermitian_raises():
     m[2, 7] = m[2, 7] + 1.0
     with pytest.raises(NotHermitianError):
         api._hermitian_check(api._as_csr(m.tocsr(), "A", "full"), "A", 1e-10)
+
+
+@pytest.mark.parametrize("case", ["symmetric", "near", "upper_only", "zeros", "unsorted", "unsymmetric_pattern", "far"])
+def test_native_fast_path_agrees_with_the_general_path(case):
+    """api._prepare checks a canonical real CSR matrix with the native hsg_csr_inspect (host threads);
+    every input must come out as the general path (_as_csr + _hermitian_check) makes it: the same
+    matrix, the same defect, the same error."""
+    m = _sym(300, 0.02, 11)
+    if case == "near":
+        noise = m.copy()
+        noise.data = noise.data * (1e-13 * np.random.default_rng(12).standard_normal(noise.nnz))
+        m = (m + noise).tocsr()
+    elif case == "upper_only":
+        m = sp.triu(m, format="csr")
+    elif case == "zeros":
+        m = m.copy()
+        m.data[3] = 0.0
+    elif case == "unsorted":
+        m = m.copy()
+        m.indices[:2] = m.indices[:2][::-1].copy()
+        m.has_sorted_indices = False
+    elif case == "unsymmetric_pattern":
+        m = m.tolil()
+        m[0, 7] = 1e-14
+        m[7, 0] = 0.0
+        m = m.tocsr()
+        m.eliminate_zeros()
+    elif case == "far":
+        m = m.tolil()
+        m[2, 9] = m[2, 9] + 1.0
+        m = m.tocsr()
+    original = m.copy()
+    try:
+        want, want_d = api._hermitian_check(api._as_csr(m.copy(), "A", "auto"), "A", 1e-10)
+    except NotHermitianError:
+        with pytest.raises(NotHermitianError):
+            api._prepare(m, "A", "auto", 1e-10)
+        return
+    got, got_d = api._prepare(m, "A", "auto", 1e-10)
+    _same(got, want)
+    assert abs(got_d - want_d) <= 1e-12 * max(want_d, 1e-300)
+    _same(m, original)  # the caller's matrix is not modified
