@@ -40,16 +40,19 @@ void to_dev(double* d, const std::vector<double>& h, cudaStream_t s) {
 }
 
 // Orthogonalize columns [j, j+p) of the basis against columns [0, j) (CGS2, B inner product),
-// returning the accumulated coefficients H (j x p) on the host.
+// returning the accumulated coefficients H (j x p) on the host. Both passes' coefficients stay on the
+// device (pass q's at q j p in B.g) and are read in one transfer at the end.
 std::vector<double> orthogonalize(Basis& B, int j, int p, cudaStream_t s) {
   std::vector<double> Htot(static_cast<std::size_t>(j) * p, 0.0), H;
   if (j == 0) return Htot;
+  const std::size_t jp = static_cast<std::size_t>(j) * p;
   for (int pass = 0; pass < 2; ++pass) {
-    gram(B.n, j, p, B.bid ? B.v(0) : B.bv(0), B.n, B.v(j), B.n, B.g.p, B.part.p, B.part_cap, s);
-    gemm_tall(B.n, j, p, B.v(0), B.n, B.g.p, j, B.v(j), B.n, -1.0, 1.0, s);
-    to_host(H, B.g.p, static_cast<std::size_t>(j) * p, s);
-    for (std::size_t t = 0; t < H.size(); ++t) Htot[t] += H[t];
+    double* G = B.g.p + pass * jp;
+    gram(B.n, j, p, B.bid ? B.v(0) : B.bv(0), B.n, B.v(j), B.n, G, B.part.p, B.part_cap, s);
+    gemm_tall(B.n, j, p, B.v(0), B.n, G, j, B.v(j), B.n, -1.0, 1.0, s);
   }
+  to_host(H, B.g.p, 2 * jp, s);
+  for (std::size_t t = 0; t < jp; ++t) Htot[t] = H[t] + H[jp + t];
   return Htot;
 }
 
