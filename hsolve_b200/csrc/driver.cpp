@@ -1336,6 +1336,9 @@ SolveOutput Session::solve_once(const hsg_solve_config_t& cfg, bool include_setu
       std::atomic<std::size_t> next{0};
       std::vector<std::exception_ptr> errs(lanes);
       std::vector<std::future<void>> futs;
+      // every lane's object exists before any lane runs: a new object copies F's analysis
+      // (analyze_like), which a running factorization of F re-plans when pivots are delayed
+      for (int lane = 0; lane < lanes; ++lane) S.slice_object(lane, single);
       for (int lane = 0; lane < lanes; ++lane) {
         GpuFactor& G = S.slice_object(lane, single);
         futs.push_back(std::async(std::launch::async, [&, lane] {
