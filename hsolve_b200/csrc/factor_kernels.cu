@@ -815,7 +815,11 @@ __device__ void app_control_and_block(AppFront<R>& F, const FactorParams& prm, d
 
 // All ranks: rows [p+w, m) solved against the block (L21 = F21 P L11^-T D^-1), backup, column maxima.
 // The block's strict lower part with the 2x2 couplings masked (they belong to D) is staged in Ls
-// (shared), the substitution runs fully unrolled in registers, one row per thread.
+// (shared). The rows of a rank go through shared memory in chunks of kRowChunk: all threads load
+// the chunk (coalesced, batches of loads in flight at once) and write the backup; one thread per row
+// runs the substitution fully unrolled in registers and applies D^-1 through per-column coefficients
+// (no branch on the pivot type, every store after the last load); a warp per four columns then
+// writes the L values back (coalesced) and reduces the column maxima.
 template <class R>
 __device__ void app_rows(AppFront<R>& F, const StepView& v, int rank, int nr, R* Bs, int* slab, signed char* spv,
                          unsigned long long* scm, unsigned long long* srm, R* Lm) {
@@ -854,89 +858,128 @@ __device__ void app_rows(AppFront<R>& F, const StepView& v, int rank, int nr, R*
   const int rchunk = (rtotal + nr - 1) / nr;
   const int rbeg = p + w + rank * rchunk, rend = min(m, rbeg + rchunk);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float* wl = reinterpret_cast<float*>(Lm + kNB * kNB);   // per-warp column maxima (8 x kNB floats)
-  R* Di = Lm + kNB * kNB + 8 * kNB;                         // D^-1 entries: a, b, c per pivot (3 x kNB)
-  for (int t = threadIdx.x; t < 8 * kNB; t += blockDim.x) wl[t] = 0.0f;
+  // D^-1 as three coefficients per column: out(t) = k0 y(t-1) + k1 y(t) + k2 y(t+1); ksel says
+  // which value the column maximum takes: 0 |out|, 1 |y| (null pivot, l = 0), 2 none (t >= eb)
+  R* k0 = Lm + kNB * kNB;
+  R* k1 = k0 + kNB;
+  R* k2 = k1 + kNB;
+  int* ksel = reinterpret_cast<int*>(k2 + kNB);
+  R* Y = Lm + kRowStage;  // kNB columns of kRowChunk rows
   for (int t = threadIdx.x; t < kNB; t += blockDim.x) {
-    R ia = R(0), ib = R(0), ic = R(0);
+    R a0 = R(0), a1 = R(1), a2 = R(0);
+    int sel = 2;
     if (t < eb) {
       const signed char ty = spv[t];
-      if (ty == 1) ia = R(1) / Bs[t + t * kNB];
-      else if (ty == 2 || ty == 3) {
+      sel = 0;
+      if (ty == 0) { a1 = R(0); sel = 1; }
+      else if (ty == 1) a1 = R(1) / Bs[t + t * kNB];
+      else {
         const int f0 = ty == 2 ? t : t - 1;
         const R a = Bs[f0 + f0 * kNB], b = Bs[f0 + 1 + f0 * kNB], cc = Bs[f0 + 1 + (f0 + 1) * kNB];
         const R idet = R(1) / (a * cc - b * b);
-        // first of the pair: l = ia y_t + ib y_{t+1}; second: l = ib y_{t-1} + ic y_t
-        if (ty == 2) { ia = cc * idet; ib = -b * idet; }
-        else { ib = -b * idet; ic = a * idet; }
+        // first of the pair: l = (c y_t - b y_{t+1}) / det; second: l = (a y_t - b y_{t-1}) / det
+        if (ty == 2) { a1 = cc * idet; a2 = -b * idet; }
+        else { a0 = -b * idet; a1 = a * idet; }
       }
     }
-    Di[t] = ia;
-    Di[kNB + t] = ib;
-    Di[2 * kNB + t] = ic;
+    k0[t] = a0;
+    k1[t] = a1;
+    k2[t] = a2;
+    ksel[t] = sel;
   }
-  __syncthreads();
-  float cm[kNB];
+  // warp `warp` writes back and reduces the maxima of columns 4 warp .. 4 warp + 3 (eight warps)
+  static_assert(kAppThreads / 32 * 4 == kNB, "the write-back pass takes four columns per warp");
+  constexpr int kStageBatch = 8;
+  double cm[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int c0 = rbeg; c0 < rend; c0 += kRowChunk) {
+    const int nrow = min(kRowChunk, rend - c0);
+    const int total = w * nrow;
+    __syncthreads();
+    // stage: element e = (column t, row r), column-major, consecutive threads on consecutive rows;
+    // a batch of loads is issued before any store (the stores could alias later loads)
+    for (int e0 = threadIdx.x; e0 < total; e0 += kStageBatch * kAppThreads) {
+      R x[kStageBatch];
 #pragma unroll
-  for (int t = 0; t < kNB; ++t) cm[t] = 0.0f;
-  for (int i = rbeg + threadIdx.x; i < rend; i += blockDim.x) {
-    // all loads first (no store in between: they overlap), block order = the pivot permutation;
-    // the backup is stored, then the substitution runs in place
-    R y[kNB];
-#pragma unroll
-    for (int t = 0; t < kNB; ++t) y[t] = t < w ? F.f.at(i, p + slab[t]) : R(0);
-#pragma unroll
-    for (int t = 0; t < kNB; ++t)
-      if (t < w) F.backup[static_cast<std::int64_t>(t) * m + i] = y[t];
-#pragma unroll
-    for (int t = 1; t < kNB; ++t) {
-      R acc = y[t];
-#pragma unroll
-      for (int s = 0; s < t; ++s) acc = fma(-y[s], Lm[t * kNB + s], acc);
-      y[t] = acc;
-    }
-#pragma unroll
-    for (int t = 0; t < kNB; ++t) {
-      if (t >= w) continue;
-      R out;
-      if (t < eb) {
-        const signed char ty = spv[t];
-        const R yp = t > 0 ? y[(t - 1) & (kNB - 1)] : R(0);
-        const R yn = t + 1 < kNB ? y[(t + 1) & (kNB - 1)] : R(0);
-        if (ty == 0) out = R(0);
-        else if (ty == 1) out = y[t] * Di[t];
-        else if (ty == 2) out = Di[t] * y[t] + Di[kNB + t] * yn;
-        else out = Di[kNB + t] * yp + Di[2 * kNB + t] * y[t];
-        cm[t] = fmaxf(cm[t], static_cast<float>(fabs(ty == 0 ? y[t] : out)));
-      } else {
-        out = y[t];
+      for (int u = 0; u < kStageBatch; ++u) {
+        const int e = e0 + u * kAppThreads;
+        const int t = e / nrow, r = e - t * nrow;
+        x[u] = e < total ? F.f.at(c0 + r, p + slab[t]) : R(0);
       }
-      F.f.at(i, p + t) = out;
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const int e = e0 + u * kAppThreads;
+        if (e < total) {
+          const int t = e / nrow, r = e - t * nrow;
+          F.backup[static_cast<std::int64_t>(t) * m + c0 + r] = x[u];
+          Y[t * kRowChunk + r] = x[u];
+        }
+      }
+    }
+    __syncthreads();
+    // one thread per row: substitution and D^-1 in registers, then the row back to shared memory
+    // (the l values; |y| of a null pivot column, whose l is zero, for its maximum)
+    for (int r = threadIdx.x; r < nrow; r += kAppThreads) {
+      R y[kNB];
+#pragma unroll
+      for (int t = 0; t < kNB; ++t) y[t] = t < w ? Y[t * kRowChunk + r] : R(0);
+#pragma unroll
+      for (int t = 1; t < kNB; ++t) {
+        R acc = y[t];
+#pragma unroll
+        for (int s2 = 0; s2 < t; ++s2) acc = fma(-y[s2], Lm[t * kNB + s2], acc);
+        y[t] = acc;
+      }
+      R prev = R(0);
+#pragma unroll
+      for (int t = 0; t < kNB; ++t) {
+        const R yn = t + 1 < kNB ? y[t + 1 < kNB ? t + 1 : t] : R(0);
+        const R out = fma(k0[t], prev, fma(k2[t], yn, k1[t] * y[t]));
+        prev = y[t];
+        y[t] = ksel[t] == 1 ? y[t] : out;
+        // the coefficients are read eight columns at a time (hoisting all of them would spill)
+        if ((t & 7) == 7) asm volatile("" ::: "memory");
+      }
+#pragma unroll
+      for (int t = 0; t < kNB; ++t)
+        if (t < w) Y[t * kRowChunk + r] = y[t];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int t = 4 * warp + c;
+      if (t < w) {
+        const int sel = ksel[t];
+        R* colp = F.f.col(p + t) + c0;
+        for (int r = lane; r < nrow; r += 32) {
+          const R x = Y[t * kRowChunk + r];
+          colp[r] = sel == 1 ? R(0) : x;
+          if (sel != 2) cm[c] = fmax(cm[c], static_cast<double>(fabs(x)));
+        }
+      }
     }
   }
 #pragma unroll
-  for (int t = 0; t < kNB; ++t) {
-    const float a = warp_maxf(cm[t]);
-    if (lane == 0) wl[warp * kNB + t] = a;
+  for (int c = 0; c < 4; ++c) {
+    double x = cm[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    const int t = 4 * warp + c;
+    // the column maximum of |l| (|y| for a null pivot), rounded to FP32 and up by 1e-7 to stay
+    // conservative (rounding is monotone: the same as the maximum of the rounded values); the accept
+    // step reads the maxima of all ranks
+    if (lane == 0 && t < w && x > 0.0) {
+      const double ad = static_cast<double>(static_cast<float>(x)) * (1.0 + 1e-7);
+      const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(ad));
+      atomicMax(&F.cmax[t], bits);
+      atomicMax(&F.rmax[t], bits);
+    }
   }
-  __syncthreads();
-  for (int t = threadIdx.x; t < w; t += blockDim.x) {
-    float a = 0.0f;
-    for (int v = 0; v < (int)(blockDim.x >> 5); ++v) a = fmaxf(a, wl[v * kNB + t]);
-    // column maximum of |l| (|y| for a null pivot, which has l = 0), rounded up to stay conservative
-    const double ad = static_cast<double>(a) * (1.0 + 1e-7);
-    scm[t] = static_cast<unsigned long long>(__double_as_longlong(ad));
-    srm[t] = scm[t];
-  }
-  __syncthreads();
-  for (int t = threadIdx.x; t < w; t += blockDim.x) {
-    if (scm[t]) atomicMax(&F.cmax[t], scm[t]);
-    if (srm[t]) atomicMax(&F.rmax[t], srm[t]);
-  }
+  (void)scm;
+  (void)srm;
 }
 
 // All ranks: the accepted prefix q (identical in every CTA); rank 0 books the inertia. The small
-// per-panel arrays are staged in shared memory first (one parallel load) so that the serial scans
+// per-panel arrays are staged in shared memory first (one parallel load) so that warp 0's tests
 // below touch no global memory. Bs / spv already hold the panel's block and pivot types (app_rows).
 template <class R>
 __device__ int app_accept(AppFront<R>& F, const StepView& v, int rank, double thr, double inv_u, int* sq,
@@ -950,54 +993,60 @@ __device__ int app_accept(AppFront<R>& F, const StepView& v, int rank, double th
     srm[t] = __ldcg(&F.rmax[t]);
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    // a forced step accepts its first pivot without the threshold; the block's later pivots were
-    // chosen from the block alone and pass the a-posteriori tests like any other
-    int q = 0;
-    while (q < eb) {
-      const bool checked = !(force && q == 0);
-      const signed char ty = spv[q];
-      const double cm = __longlong_as_double(static_cast<long long>(scm[q]));
-      if (ty == 0) {
-        if (checked && __longlong_as_double(static_cast<long long>(srm[q])) > thr) break;
-        q += 1;
-      } else if (ty == 1) {
-        if (checked && cm > inv_u) break;
-        q += 1;
-      } else {
-        const double cm2 = __longlong_as_double(static_cast<long long>(scm[q + 1]));
-        if (checked && fmax(cm, cm2) > inv_u) break;
-        q += 2;
+  if (threadIdx.x < 32) {
+    // warp 0: lane t tests the pivot that starts at t (the second of a 2x2 pair starts none); the
+    // accepted prefix ends at the first failing start. A forced step accepts its first pivot
+    // without the threshold; the block's later pivots were chosen from the block alone and pass the
+    // a-posteriori tests like any other.
+    const int t = threadIdx.x;
+    const signed char ty = t < eb ? spv[t] : static_cast<signed char>(3);
+    const bool start = t < eb && ty != 3;
+    bool fail = false;
+    if (start && !(force && t == 0)) {
+      const double cm = __longlong_as_double(static_cast<long long>(scm[t]));
+      if (ty == 0) fail = __longlong_as_double(static_cast<long long>(srm[t])) > thr;
+      else if (ty == 1) fail = cm > inv_u;
+      else {
+        const double cm2 = t + 1 < kNB ? __longlong_as_double(static_cast<long long>(scm[t + 1])) : 0.0;
+        fail = fmax(cm, cm2) > inv_u;
       }
     }
-    *sq = q;
-  }
-  __syncthreads();
-  const int q = *sq;
-  if (rank == 0) {
-    for (int t = threadIdx.x; t < q; t += blockDim.x) F.ppv[p + t] = spv[t];
-    if (threadIdx.x == 0) {
+    const unsigned fails = __ballot_sync(0xffffffffu, fail);
+    const unsigned over = __ballot_sync(0xffffffffu, start && ty != 0 && ty != 1 && t + 1 >= eb);
+    const int q = fails ? __ffs(fails) - 1 : (over ? eb + 1 : eb);
+    if (t == 0) *sq = q;
+    if (rank == 0) {
+      // inertia of the accepted pivots: lane t books the pivot that starts at t
       int neg = 0, pos = 0, zero = 0, two = 0;
-      for (int t = 0; t < q; ++t) {
-        const signed char ty = spv[t];
-        if (ty == 0) zero++;
-        else if (ty == 1) { if (Bs[t + t * kNB] < 0) neg++; else pos++; }
+      if (start && t < q) {
+        if (ty == 0) zero = 1;
+        else if (ty == 1) { if (Bs[t + t * kNB] < 0) neg = 1; else pos = 1; }
         else if (ty == 2) {
           const R a = Bs[t + t * kNB], b = Bs[t + 1 + t * kNB], cc = Bs[t + 1 + (t + 1) * kNB];
           const R det = a * cc - b * b;
-          if (det < 0) { neg++; pos++; } else if (a + cc < 0) neg += 2; else pos += 2;
-          two++;
+          if (det < 0) { neg = 1; pos = 1; } else if (a + cc < 0) neg = 2; else pos = 2;
+          two = 1;
         }
       }
-      AppCtrl* cw = F.ctrl;
-      cw->q = q;
-      cw->neg += neg;
-      cw->pos += pos;
-      cw->zero += zero;
-      cw->two += two;
-      if (force && q > 0) cw->forced += spv[0] == 2 ? 2 : 1;
+      neg = __reduce_add_sync(0xffffffffu, neg);
+      pos = __reduce_add_sync(0xffffffffu, pos);
+      zero = __reduce_add_sync(0xffffffffu, zero);
+      two = __reduce_add_sync(0xffffffffu, two);
+      if (t == 0) {
+        AppCtrl* cw = F.ctrl;
+        cw->q = q;
+        cw->neg += neg;
+        cw->pos += pos;
+        cw->zero += zero;
+        cw->two += two;
+        if (force && q > 0) cw->forced += spv[0] == 2 ? 2 : 1;
+      }
     }
   }
+  __syncthreads();
+  const int q = *sq;
+  if (rank == 0)
+    for (int t = threadIdx.x; t < q; t += blockDim.x) F.ppv[p + t] = spv[t];
   return q;
 }
 

@@ -14,6 +14,8 @@ constexpr int kTile = 64;              // trailing-update tile (rows = cols)
 constexpr int kKB = 128;               // pending pivots whose trailing update is applied at once (blocked step)
 constexpr int kUpdLd = kTile + 4;      // column stride of the staged update operands (conflict-free fragment reads)
 constexpr int kAppDynDoubles = 2 * kKB * kUpdLd;  // dynamic shared memory of the panel kernels
+constexpr int kRowStage = kNB * kNB + 4 * kNB;   // panel row step: the block's L and the D^-1 coefficients
+constexpr int kRowChunk = (kAppDynDoubles - kRowStage) / kNB;  // rows staged at once by the panel row step
 constexpr int kAppThreads = 256;
 constexpr int kCoopMinFront = 192;     // levels whose largest panel front is at least this use the cooperative kernel
 constexpr int kColsPerThread = kTile * kTile / kAppThreads;  // 16
