@@ -839,25 +839,6 @@ __device__ void app_rows(AppFront<R>& F, const StepView& v, int rank, int nr, R*
     if (t < w && s < t && s < eb && !(spv[s] == 2 && s + 1 == t)) x = Bs[t + s * kNB];
     Lm[e] = x;
   }
-  // did the block factorization swap any of its rows? (rarely: then the permutation below moves data)
-  const bool permuted = __syncthreads_or(threadIdx.x < w && slab[threadIdx.x] != static_cast<int>(threadIdx.x)) != 0;
-  // permute the L rows p..p+w-1 of the eliminated columns c < p (a thread owns a column; the
-  // columns are split into contiguous chunks over the ranks)
-  const int cchunk = (p + nr - 1) / nr;
-  const int cend = permuted ? min(p, (rank + 1) * cchunk) : 0;
-  for (int cc = rank * cchunk + threadIdx.x; cc < cend; cc += blockDim.x) {
-    R x[kNB];
-    R* colp = F.f.col(cc) + p;
-#pragma unroll
-    for (int a = 0; a < kNB; ++a) x[a] = a < w ? colp[slab[a]] : R(0);
-#pragma unroll
-    for (int a = 0; a < kNB; ++a)
-      if (a < w) colp[a] = x[a];
-  }
-  const int rtotal = m - (p + w);
-  const int rchunk = (rtotal + nr - 1) / nr;
-  const int rbeg = p + w + rank * rchunk, rend = min(m, rbeg + rchunk);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // D^-1 as three coefficients per column: out(t) = k0 y(t-1) + k1 y(t) + k2 y(t+1); ksel says
   // which value the column maximum takes: 0 |out|, 1 |y| (null pivot, l = 0), 2 none (t >= eb)
   R* k0 = Lm + kNB * kNB;
@@ -887,10 +868,31 @@ __device__ void app_rows(AppFront<R>& F, const StepView& v, int rank, int nr, R*
     k2[t] = a2;
     ksel[t] = sel;
   }
+  // did the block factorization swap any of its rows? (rarely: then the permutation below moves data)
+  const bool permuted = __syncthreads_or(threadIdx.x < w && slab[threadIdx.x] != static_cast<int>(threadIdx.x)) != 0;
+  // permute the L rows p..p+w-1 of the eliminated columns c < p (a thread owns a column; the
+  // columns are split into contiguous chunks over the ranks)
+  const int cchunk = (p + nr - 1) / nr;
+  const int cend = permuted ? min(p, (rank + 1) * cchunk) : 0;
+  for (int cc = rank * cchunk + threadIdx.x; cc < cend; cc += blockDim.x) {
+    R x[kNB];
+    R* colp = F.f.col(cc) + p;
+#pragma unroll
+    for (int a = 0; a < kNB; ++a) x[a] = a < w ? colp[slab[a]] : R(0);
+#pragma unroll
+    for (int a = 0; a < kNB; ++a)
+      if (a < w) colp[a] = x[a];
+  }
+  const int rtotal = m - (p + w);
+  const int rchunk = (rtotal + nr - 1) / nr;
+  const int rbeg = p + w + rank * rchunk, rend = min(m, rbeg + rchunk);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // warp `warp` writes back and reduces the maxima of columns 4 warp .. 4 warp + 3 (eight warps)
   static_assert(kAppThreads / 32 * 4 == kNB, "the write-back pass takes four columns per warp");
   constexpr int kStageBatch = 8;
-  double cm[4] = {0.0, 0.0, 0.0, 0.0};
+  // column maxima in FP32 (rounding is monotone: the maximum of the rounded values is the rounded
+  // maximum), reduced over the warp with one integer max on the bit patterns of the non-negative floats
+  float cm[4] = {0.0f, 0.0f, 0.0f, 0.0f};
   for (int c0 = rbeg; c0 < rend; c0 += kRowChunk) {
     const int nrow = min(kRowChunk, rend - c0);
     const int total = w * nrow;
@@ -950,25 +952,32 @@ __device__ void app_rows(AppFront<R>& F, const StepView& v, int rank, int nr, R*
       if (t < w) {
         const int sel = ksel[t];
         R* colp = F.f.col(p + t) + c0;
-        for (int r = lane; r < nrow; r += 32) {
-          const R x = Y[t * kRowChunk + r];
-          colp[r] = sel == 1 ? R(0) : x;
-          if (sel != 2) cm[c] = fmax(cm[c], static_cast<double>(fabs(x)));
+        // a batch of shared-memory reads before the global stores (which could alias them)
+        for (int r0 = lane; r0 < nrow; r0 += 32 * kStageBatch) {
+          R x[kStageBatch];
+#pragma unroll
+          for (int u = 0; u < kStageBatch; ++u) {
+            const int r = r0 + 32 * u;
+            x[u] = r < nrow ? Y[t * kRowChunk + r] : R(0);
+          }
+#pragma unroll
+          for (int u = 0; u < kStageBatch; ++u) {
+            const int r = r0 + 32 * u;
+            if (r < nrow) colp[r] = sel == 1 ? R(0) : x[u];
+            if (sel != 2) cm[c] = fmaxf(cm[c], static_cast<float>(fabs(x[u])));
+          }
         }
       }
     }
   }
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
-    double x = cm[c];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    const float x = warp_maxf(cm[c]);
     const int t = 4 * warp + c;
-    // the column maximum of |l| (|y| for a null pivot), rounded to FP32 and up by 1e-7 to stay
-    // conservative (rounding is monotone: the same as the maximum of the rounded values); the accept
-    // step reads the maxima of all ranks
-    if (lane == 0 && t < w && x > 0.0) {
-      const double ad = static_cast<double>(static_cast<float>(x)) * (1.0 + 1e-7);
+    // the column maximum of |l| (|y| for a null pivot), rounded up by 1e-7 to stay conservative;
+    // the accept step reads the maxima of all ranks
+    if (lane == 0 && t < w && x > 0.0f) {
+      const double ad = static_cast<double>(x) * (1.0 + 1e-7);
       const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(ad));
       atomicMax(&F.cmax[t], bits);
       atomicMax(&F.rmax[t], bits);
