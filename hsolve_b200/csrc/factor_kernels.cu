@@ -1335,8 +1335,10 @@ __device__ bool front_barrier(int* bar, int nr, unsigned long long* timeouts, in
   if (threadIdx.x == 0) {
     int ok = 1;
     if (nr > 1) {
-      __threadfence();
-      const int old = atomicAdd(bar, 1);
+      // arrival with release semantics (the CTA's writes, ordered before it by the block barrier,
+      // become visible to every rank that acquires the count) and acquire for the later reads
+      int old;
+      asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(bar) : "memory");
       const int target = (old / nr + 1) * nr;
       unsigned long long t0 = 0;
       for (unsigned it = 0;; ++it) {
@@ -1351,7 +1353,6 @@ __device__ bool front_barrier(int* bar, int nr, unsigned long long* timeouts, in
           __nanosleep(64);
         }
       }
-      __threadfence();
     }
     *s_ok = ok;
   }
