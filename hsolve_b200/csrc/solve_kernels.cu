@@ -210,16 +210,18 @@ __device__ __forceinline__ void wait_count(const int* cnt, int target, int* err)
   __syncthreads();
 }
 
+// thread 0, after a block barrier that orders the CTA's writes before it: add `count` to a counter
+// with release semantics (an acq_rel fence at device scope, then a relaxed reduction), so that a CTA
+// whose acquire load sees the new count also sees those writes
+__device__ __forceinline__ void add_release(int* cnt, int count) {
+  asm volatile("fence.acq_rel.gpu;\n\tred.relaxed.gpu.global.add.s32 [%0], %1;" :: "l"(cnt), "r"(count) : "memory");
+}
+
 // all threads, after their writes: make them visible to the front's other CTAs and add `count` to
 // the front's counter. A front solved by one CTA only synchronizes its threads.
 __device__ __forceinline__ void publish(int* cnt, int count, int nr) {
-  if (nr > 1) {
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0 && count > 0) atomicAdd(cnt, count);
-  } else {
-    __syncthreads();
-  }
+  __syncthreads();
+  if (nr > 1 && threadIdx.x == 0 && count > 0) add_release(cnt, count);
 }
 
 // groups / chunks g belong to CTA g mod nr: how many of `rank`'s lie below `hi`
@@ -480,9 +482,8 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const SolveTask* tasks, co
       for (int w = 0; w < 8; ++w) sum += red[(w * 32 + cc) * 9 + r];
       partial[(static_cast<std::int64_t>(ch) * (P - 1) + (q - 1)) * 256 + cc * 8 + r] = sum;
     }
-    __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) atomicAdd(hc + ch, 1);
+    if (threadIdx.x == 0) add_release(hc + ch, 1);
     return;
   }
   const int nown = owned_below(nch, rank, nr);
