@@ -153,15 +153,38 @@ __global__ void k_extend_add(const int2* items, const SnDev* sn, const std::int3
   const std::int32_t* rm = rmap + c.rmap_off;
   const R* src = cb + c.cb_off;
   const std::int32_t pc = p.m - p.k;
-  const std::int32_t bend = min(it.y + kExtendAddCols, mc);
-  for (std::int32_t bb = it.y; bb < bend; ++bb) {
-    const std::int32_t pb = rm[bb];
-    R* dst;
-    std::int64_t ld_off;
-    if (pb < p.k) { dst = panels + p.panel_off + static_cast<std::int64_t>(pb) * p.m; ld_off = 0; }
-    else { dst = cb + p.cb_off + static_cast<std::int64_t>(pb - p.k) * pc; ld_off = p.k; }
-    const R* col = src + static_cast<std::int64_t>(bb) * mc;
-    for (std::int32_t a = bb + threadIdx.x; a < mc; a += blockDim.x) dst[rm[a] - ld_off] += col[a];
+  const std::int32_t b0 = it.y;
+  const std::int32_t bend = min(b0 + kExtendAddCols, mc);
+  // the chunk's columns: destination column in the parent (its panel or its contribution block)
+  // (rows of a contribution-block column are numbered from p.k: off = p.k there, 0 in the panel)
+  R* dst[kExtendAddCols];
+  std::int32_t off[kExtendAddCols];
+#pragma unroll
+  for (int u = 0; u < kExtendAddCols; ++u) {
+    const std::int32_t bb = b0 + u;
+    dst[u] = nullptr;
+    off[u] = 0;
+    if (bb < bend) {
+      const std::int32_t pb = rm[bb];
+      if (pb < p.k) dst[u] = panels + p.panel_off + static_cast<std::int64_t>(pb) * p.m;
+      else { dst[u] = cb + p.cb_off + static_cast<std::int64_t>(pb - p.k) * pc; off[u] = p.k; }
+    }
+  }
+  // a thread takes row a of every column of the chunk (lower triangle: a >= the column): all
+  // sources and destinations are loaded before the stores, which could alias them for the compiler
+  // (they do not: each destination entry receives exactly one addition per launch)
+  for (std::int32_t a = b0 + threadIdx.x; a < mc; a += blockDim.x) {
+    const std::int32_t ra = rm[a];
+    R v[kExtendAddCols], d[kExtendAddCols];
+#pragma unroll
+    for (int u = 0; u < kExtendAddCols; ++u) {
+      const bool in = dst[u] != nullptr && a >= b0 + u;
+      v[u] = in ? src[static_cast<std::int64_t>(b0 + u) * mc + a] : R(0);
+      d[u] = in ? dst[u][ra - off[u]] : R(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kExtendAddCols; ++u)
+      if (dst[u] != nullptr && a >= b0 + u) dst[u][ra - off[u]] = d[u] + v[u];
   }
 }
 
