@@ -135,11 +135,15 @@ template <class R>
 __global__ void k_zero_cb(const std::int32_t* list, const SnDev* sn, R* cb) {
   const SnDev s = sn[list[blockIdx.x]];
   const std::int64_t c = s.m - s.k;
-  const std::int64_t total = c * c;
   R* base = cb + s.cb_off;
-  for (std::int64_t i = blockIdx.y * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < total;
-       i += static_cast<std::int64_t>(gridDim.y) * blockDim.x)
-    base[i] = R(0);
+  // the lower triangle only (column j: rows j .. c-1): no kernel reads a contribution block above
+  // its diagonal. A warp per column, columns dealt over the chunk's warps.
+  const int lane = threadIdx.x & 31;
+  const std::int64_t nw = static_cast<std::int64_t>(gridDim.y) * (blockDim.x >> 5);
+  for (std::int64_t j = static_cast<std::int64_t>(blockIdx.y) * (blockDim.x >> 5) + (threadIdx.x >> 5); j < c; j += nw) {
+    R* col = base + j * c;
+    for (std::int64_t i = j + lane; i < c; i += 32) col[i] = R(0);
+  }
 }
 
 // Extend-add: item = (child, first column of a column block). Adds the child's lower CB
