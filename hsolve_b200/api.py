@@ -43,8 +43,39 @@ _SOLVE_SIGS = {
     "hsg_session_solve": (ctypes.c_int, [_P, _P, _P]),
     "hsg_session_free": (None, [_P]),
     "hsg_session_estimate": (ctypes.c_int, [_P, _P]),
+    "hsg_default_exclusion_options": (None, [_P]),
+    "hsg_session_exclusion_check": (ctypes.c_int, [_P, _P, ctypes.c_int64, ctypes.c_int64, _P, _P]),
+    "hsg_exclusion_failure_bound": (ctypes.c_double, [ctypes.c_double, ctypes.c_int64, ctypes.c_int64,
+                                                      ctypes.c_int64, ctypes.c_double, ctypes.c_int32]),
+    "hsg_exclusion_block_steps": (ctypes.c_int64, [ctypes.c_double, ctypes.c_double, ctypes.c_int64,
+                                                   ctypes.c_int64, ctypes.c_double, ctypes.c_int32]),
 }
 _native.SIGNATURES.update(_SOLVE_SIGS)
+
+
+class _ExclusionOptions(ctypes.Structure):
+    """hsg_exclusion_options_t (include/hsg_solve.h)."""
+    _fields_ = [("sigma", ctypes.c_double), ("radius", ctypes.c_double), ("pass_radius", ctypes.c_double),
+                ("delta", ctypes.c_double), ("block_size", ctypes.c_int32), ("max_block_steps", ctypes.c_int32),
+                ("max_krylov_vectors", ctypes.c_int32), ("pad", ctypes.c_int32), ("seed", ctypes.c_uint64),
+                ("kappa", ctypes.c_double), ("rounding_margin", ctypes.c_double)]
+
+
+class _ExclusionResult(ctypes.Structure):
+    """hsg_exclusion_result_t (include/hsg_solve.h)."""
+    _fields_ = [("status", ctypes.c_int32), ("exact", ctypes.c_int32), ("over_budget", ctypes.c_int32),
+                ("rigorous", ctypes.c_int32), ("sigma", ctypes.c_double), ("claim_threshold", ctypes.c_double),
+                ("pass_threshold", ctypes.c_double), ("coupling", ctypes.c_double), ("epsilon", ctypes.c_double),
+                ("kappa", ctypes.c_double), ("deflated", ctypes.c_int64), ("dimension", ctypes.c_int64),
+                ("found_inside", ctypes.c_int64), ("certified_inside", ctypes.c_int64),
+                ("block_size", ctypes.c_int64), ("block_steps_planned", ctypes.c_int64),
+                ("block_steps", ctypes.c_int64), ("krylov_vectors_planned", ctypes.c_int64),
+                ("max_ritz", ctypes.c_double), ("failure_probability", ctypes.c_double),
+                ("new_count", ctypes.c_int64), ("new_inside", ctypes.c_int64), ("op_applications", ctypes.c_int64),
+                ("setup_s", ctypes.c_double), ("krylov_s", ctypes.c_double)]
+
+
+_EXCLUSION_STATUS = {0: "passed", 1: "detected", 2: "inconclusive"}
 
 _MODES = ("nearest", "interval", "smallest", "largest")
 _STORAGES = ("auto", "full", "upper", "lower")
@@ -609,6 +640,43 @@ class Session:
         if self._complex:
             return _complex_result(w, v, report, self._complex[0], self._complex[1], cfg, self._da, self._db)
         return _finish(w, v, report, cfg, self._da, self._db, self._cdtype, cplx)
+
+    def exclusion_check(self, X, *, sigma: float, radius: float, pass_radius: float, delta: float = 1e-12,
+                        block_size: int = 4, seed: int = 2026, kappa: float = 1.0, rounding_margin: float = 1e-6,
+                        max_block_steps: int = 0, max_krylov_vectors: int = 512) -> dict:
+        """Randomized exclusion certificate (hsolve's exclusion_check, include/hsolve/verify.hpp:18-80):
+        with X the found eigenvectors (n x m, any basis of their span), does the pencil have more
+        eigenvalues than the found ones within `radius` of `sigma`? The session factorizes at sigma, and
+        a block Lanczos run on the complement of span X, whose length is fixed beforehand from `delta`,
+        decides: status "passed" (no Ritz value with |theta| >= 1 / pass_radius; the statement fails with
+        probability <= failure_probability <= delta), "detected" or "inconclusive" (the gap between
+        radius and pass_radius is too small for the coupling of X, or the plan exceeds
+        max_krylov_vectors). B must be positive definite. For a complex pencil X is complex and the
+        check runs on the real 2n embedding (every count doubles)."""
+        x = np.asarray(X)
+        if x.ndim == 1:
+            x = x[:, None]
+        if self._complex:
+            xc = x.astype(np.complex128)
+            x = np.block([[xc.real, -xc.imag], [xc.imag, xc.real]])
+        x = np.asfortranarray(x, dtype=np.float64)
+        if x.shape[0] != self.n:
+            raise InvalidInputError(f"X has {x.shape[0]} rows, the pencil has {self.n}")
+        o = _ExclusionOptions()
+        _native.lib().hsg_default_exclusion_options(ctypes.byref(o))
+        o.sigma, o.radius, o.pass_radius, o.delta = float(sigma), float(radius), float(pass_radius), float(delta)
+        o.block_size, o.seed, o.kappa = int(block_size), int(seed), float(kappa)
+        o.rounding_margin, o.max_block_steps, o.max_krylov_vectors = float(rounding_margin), int(max_block_steps), \
+            int(max_krylov_vectors)
+        r = _ExclusionResult()
+        _native.check(_native.lib().hsg_session_exclusion_check(self._h, x.ctypes.data_as(ctypes.c_void_p),
+                                                                x.shape[1], x.shape[0], ctypes.byref(o),
+                                                                ctypes.byref(r)))
+        out = {f: getattr(r, f) for f, _ in _ExclusionResult._fields_}
+        out["status"] = _EXCLUSION_STATUS.get(r.status, "inconclusive")
+        for key in ("exact", "over_budget", "rigorous"):
+            out[key] = bool(out[key])
+        return out
 
     def estimate(self) -> dict:
         """Analysis of the session's pencil (for a complex pencil, of its real 2n embedding): factor

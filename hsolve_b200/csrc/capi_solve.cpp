@@ -5,6 +5,7 @@
 
 #include "common.hpp"
 #include "driver.hpp"
+#include "eigen.hpp"
 #include "hsg_solve.h"
 
 struct hsg_solution {
@@ -119,6 +120,43 @@ int hsg_session_solve(hsg_session* s, const hsg_solve_config_t* cfg, hsg_solutio
 }
 
 void hsg_session_free(hsg_session* s) { delete s; }
+
+void hsg_default_exclusion_options(hsg_exclusion_options_t* opt) {
+  if (!opt) return;
+  *opt = hsg_exclusion_options_t{};
+  opt->delta = 1e-12;
+  opt->block_size = 4;
+  opt->max_krylov_vectors = 512;
+  opt->seed = 2026;
+  opt->kappa = 1.0;
+  opt->rounding_margin = 1e-6;
+}
+
+int hsg_session_exclusion_check(hsg_session* s, const double* x, int64_t m, int64_t ldx,
+                                const hsg_exclusion_options_t* opt, hsg_exclusion_result_t* out) {
+  return guarded([&] {
+    HSG_REQUIRE(s && s->impl && x && opt && out, HSG_INVALID_INPUT, "hsg_session_exclusion_check: null argument");
+    *out = s->impl->exclusion_check(x, m, ldx, *opt);
+  });
+}
+
+double hsg_exclusion_failure_bound(double epsilon, int64_t block_steps, int64_t dimension, int64_t block_size,
+                                   double kappa, int32_t complex_scalars) {
+  double v = std::nan("");
+  const int st = guarded([&] {
+    v = hsg::exclusion_failure_bound(epsilon, block_steps, dimension, block_size, kappa, complex_scalars != 0);
+  });
+  return st == 0 ? v : std::nan("");
+}
+
+int64_t hsg_exclusion_block_steps(double epsilon, double delta, int64_t dimension, int64_t block_size, double kappa,
+                                  int32_t complex_scalars) {
+  int64_t v = -1;
+  const int st = guarded([&] {
+    v = hsg::exclusion_block_steps(epsilon, delta, dimension, block_size, kappa, complex_scalars != 0);
+  });
+  return st == 0 ? v : -1;
+}
 
 int hsg_solution_sizes(const hsg_solution* s, int64_t* n, int64_t* m) {
   return guarded([&] {

@@ -875,6 +875,89 @@ std::int64_t Session::order() const { return d_->a.n; }
 
 hsg_estimate_t Session::estimate() const { return d_->F->estimate(); }
 
+// Exclusion certificate on the session's factorization object, factorized at opt.sigma (hsolve's
+// exclusion_check, include/hsolve/verify.hpp:110-175). The start block is B^-1/2 G for a diagonal B
+// (kappa = 1 exactly), G for B = I; a general B takes the caller's kappa and the result is flagged
+// as not rigorous.
+hsg_exclusion_result_t Session::exclusion_check(const double* x, std::int64_t m, std::int64_t ldx,
+                                                const hsg_exclusion_options_t& o) {
+  Impl& S = *d_;
+  HSG_REQUIRE(S.problem != "GHIEP", HSG_UNSUPPORTED, "exclusion check: B must be positive definite");
+  const std::int64_t n = S.P.n;
+  HSG_REQUIRE(x && m >= 1 && m < n && ldx >= n, HSG_INVALID_INPUT,
+              "exclusion check: X must be n x m (1 <= m < n) with ld >= n");
+  HSG_REQUIRE(std::isfinite(o.sigma), HSG_INVALID_INPUT, "exclusion check: sigma must be finite");
+  cuda_check(cudaSetDevice(S.device), "cudaSetDevice");
+  Problem& P = S.P;
+  PoolStreamScope scope(P.s);
+  GpuFactor& F = *S.F;
+  double sigma = o.sigma;
+  Timers tm;
+  int used = 0;
+  HSG_REQUIRE(factorize_at(F, sigma, S.scale, 4, used, tm), HSG_FACTORIZATION_FAILED,
+              "exclusion check: A - sigma B could not be factorized near sigma");
+  ShiftInvertOp op(P, F);
+  DevBuf<double> X;
+  X.alloc(static_cast<std::size_t>(n) * m);
+  cuda_check(cudaMemcpy2DAsync(X.p, n * sizeof(double), x, ldx * sizeof(double), n * sizeof(double), m,
+                               cudaMemcpyHostToDevice, P.s), "exclusion check: X");
+  ExclusionOptions eo;
+  eo.radius = o.radius;
+  eo.pass_radius = o.pass_radius;
+  eo.delta = o.delta;
+  eo.block = o.block_size;
+  eo.seed = o.seed;
+  eo.rounding_margin = o.rounding_margin;
+  eo.max_block_steps = o.max_block_steps;
+  eo.max_krylov_vectors = o.max_krylov_vectors;
+  DevBuf<double> sc;
+  const double* start_scale = nullptr;
+  bool rigorous = true;
+  if (P.b_identity) {
+    eo.kappa = 1.0;
+  } else if (P.b_diagonal) {
+    std::vector<double> d(static_cast<std::size_t>(n));
+    cuda_check(cudaMemcpyAsync(d.data(), P.bdiag->p, n * sizeof(double), cudaMemcpyDeviceToHost, P.s), "B diagonal");
+    cuda_check(cudaStreamSynchronize(P.s), "B diagonal");
+    for (double& v : d) v = 1.0 / std::sqrt(v);
+    sc.upload(d, P.s);
+    start_scale = sc.p;
+    eo.kappa = 1.0;
+  } else {
+    eo.kappa = std::max(1.0, o.kappa);
+    rigorous = false;
+  }
+  const ExclusionResult r = hsg::exclusion_check(op, n, X.p, static_cast<int>(m), eo, start_scale, P.s);
+  cuda_check(cudaStreamSynchronize(P.s), "exclusion check");
+  hsg_exclusion_result_t out{};
+  out.status = static_cast<int32_t>(r.status);
+  out.exact = r.exact ? 1 : 0;
+  out.over_budget = r.over_budget ? 1 : 0;
+  out.rigorous = (rigorous || r.exact) ? 1 : 0;
+  out.sigma = sigma;
+  out.claim_threshold = r.claim_threshold;
+  out.pass_threshold = r.pass_threshold;
+  out.coupling = r.coupling;
+  out.epsilon = r.epsilon;
+  out.kappa = r.kappa;
+  out.deflated = r.deflated;
+  out.dimension = r.dimension;
+  out.found_inside = r.found_inside;
+  out.certified_inside = r.certified_inside;
+  out.block_size = r.block;
+  out.block_steps_planned = r.block_steps_planned;
+  out.block_steps = r.block_steps;
+  out.krylov_vectors_planned = r.krylov_vectors_planned;
+  out.max_ritz = r.max_ritz;
+  out.failure_probability = r.failure_probability;
+  out.new_count = r.new_count;
+  out.new_inside = r.new_inside;
+  out.op_applications = r.op_applications;
+  out.setup_s = r.setup_s;
+  out.krylov_s = r.krylov_s;
+  return out;
+}
+
 // factor_precision = single: the shift factorizations that serve the operator are FP32 with FP64
 // refinement of every application; the inertia counts stay FP64. As in hsolve (solver.hpp:116-126),
 // the attempt is abandoned for FP64 factors when an application's refinement does not converge or

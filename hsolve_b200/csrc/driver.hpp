@@ -38,6 +38,9 @@ class Session {
   Session(const Session&) = delete;
   Session& operator=(const Session&) = delete;
   SolveOutput solve(const hsg_solve_config_t& cfg, bool include_setup = false);
+  // randomized exclusion certificate on the factorization at opt.sigma (x: host, n x m, ld ldx)
+  hsg_exclusion_result_t exclusion_check(const double* x, std::int64_t m, std::int64_t ldx,
+                                         const hsg_exclusion_options_t& opt);
   std::int64_t order() const;
   hsg_estimate_t estimate() const;
 

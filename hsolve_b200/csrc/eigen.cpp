@@ -422,6 +422,199 @@ KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, 
   }
 }
 
+double exclusion_failure_bound(double eps, std::int64_t s, std::int64_t N, std::int64_t p, double kappa,
+                               bool complex_scalars) {
+  HSG_REQUIRE(s >= 1, HSG_INVALID_INPUT, "exclusion bound: block steps must be >= 1");
+  HSG_REQUIRE(p >= 1, HSG_INVALID_INPUT, "exclusion bound: block size must be >= 1");
+  HSG_REQUIRE(kappa >= 1.0, HSG_INVALID_INPUT, "exclusion bound: kappa must be >= 1");
+  if (N <= 0) return 0.0;
+  if (!(eps > 0.0)) return 1.0;
+  const double e = std::min(eps, 1.0);
+  const double inf = std::numeric_limits<double>::infinity();
+  auto cheb = [&](double steps, double x) {  // T_k(x) = cosh(k acosh x), x >= 1
+    const double a = steps * std::acosh(x);
+    return a < 700.0 ? std::cosh(a) : inf;
+  };
+  // direct bound: T_{s-1} mapped from [-Theta, (1 - eps) Theta] to [-1, 1]
+  const double c1 = cheb(static_cast<double>(s - 1), (2.0 + e) / (2.0 - e));
+  double t = (2.0 - e) / (e * c1 * c1 + 2.0 - e);
+  if (s >= 2) {
+    // squared bound: T_k in theta^2 on [0, (1 - eps)^2 Theta^2], k = floor((s - 2) / 2)
+    const double q = (1.0 - e) * (1.0 - e), e2 = 1.0 - q;
+    const std::int64_t k = (s - 2) / 2;
+    const double c2 = k == 0 ? 1.0 : (q > 0.0 ? cheb(static_cast<double>(k), (1.0 + e2) / (1.0 - e2)) : inf);
+    t = std::min(t, q / (e2 * c2 * c2 + q));
+  }
+  // the first coordinate of a uniform unit vector: real P(z^2 < x) <= sqrt(N x), complex <= (N-1) x
+  const double f = complex_scalars ? static_cast<double>(N - 1) * kappa * t
+                                   : std::sqrt(static_cast<double>(N) * kappa * t);
+  return std::pow(std::min(f, 1.0), static_cast<double>(p));
+}
+
+std::int64_t exclusion_block_steps(double eps, double delta, std::int64_t N, std::int64_t p, double kappa,
+                                   bool complex_scalars) {
+  if (!(eps > 0.0) || !(delta > 0.0 && delta < 1.0)) return -1;
+  HSG_REQUIRE(p >= 1, HSG_INVALID_INPUT, "exclusion steps: block size must be >= 1");
+  if (N <= 0) return 1;
+  const std::int64_t cover = (N + p - 1) / p + 1;
+  auto ok = [&](std::int64_t st) { return exclusion_failure_bound(eps, st, N, p, kappa, complex_scalars) <= delta; };
+  if (ok(1)) return 1;
+  std::int64_t hi = 1;
+  while (!ok(hi)) {  // doubling, then bisection on the monotone bound
+    if (hi >= cover) return cover;
+    hi *= 2;
+  }
+  std::int64_t lo = hi / 2;
+  while (hi - lo > 1) {
+    const std::int64_t mid = lo + (hi - lo) / 2;
+    if (ok(mid)) hi = mid;
+    else lo = mid;
+  }
+  return std::min(hi, cover);
+}
+
+namespace {
+
+void alloc_basis(Basis& B, std::int64_t n, bool bid, int cols, int pmax) {
+  B.n = n;
+  B.bid = bid;
+  B.cols = cols;
+  B.V.alloc(static_cast<std::size_t>(n) * cols);
+  if (!bid) B.BV.alloc(static_cast<std::size_t>(n) * cols);
+  B.tmp.alloc(static_cast<std::size_t>(n) * pmax);
+  B.g.alloc(static_cast<std::size_t>(2) * cols * pmax);
+  B.part_cap = gram_part_size(n, cols, pmax);
+  B.part.alloc(static_cast<std::size_t>(B.part_cap));
+  B.small.alloc(static_cast<std::size_t>(pmax) * pmax);
+}
+
+// largest eigenvalue of the symmetric part of a k x k matrix (host)
+double sym_max_eig(int k, std::vector<double> G) {
+  for (int a = 0; a < k; ++a)
+    for (int b = 0; b < a; ++b) { const double v = 0.5 * (G[a + b * k] + G[b + a * k]); G[a + b * k] = v; G[b + a * k] = v; }
+  std::vector<double> w;
+  sym_eig(k, G, w);
+  return w.empty() ? 0.0 : w.back();
+}
+
+}  // namespace
+
+ExclusionResult exclusion_check(KrylovOperator& op, std::int64_t n, const double* x, int m,
+                                const ExclusionOptions& opt, const double* start_scale, cudaStream_t s) {
+  HSG_REQUIRE(m >= 1 && m < n, HSG_INVALID_INPUT, "exclusion check: need 1 <= found vectors < n");
+  HSG_REQUIRE(opt.radius > 0.0 && opt.pass_radius > opt.radius, HSG_INVALID_INPUT,
+              "exclusion check: need 0 < radius < pass_radius");
+  HSG_REQUIRE(opt.delta > 0.0 && opt.delta < 1.0, HSG_INVALID_INPUT, "exclusion check: delta must lie in (0, 1)");
+  HSG_REQUIRE(opt.kappa >= 1.0, HSG_INVALID_INPUT, "exclusion check: kappa must be >= 1");
+  HSG_REQUIRE(opt.rounding_margin >= 0.0 && opt.rounding_margin < 0.5, HSG_INVALID_INPUT,
+              "exclusion check: rounding margin must lie in [0, 0.5)");
+  ExclusionResult res;
+  const int p = std::max(1, std::min(opt.block, kMaxKrylovBlock));
+  res.block = p;
+  res.kappa = opt.kappa;
+  res.deflated = m;
+  res.dimension = n - m;
+  const std::int64_t N = n - m;
+  const bool bid = op.b_identity();
+  std::mt19937_64 rng(opt.seed);
+  auto t0 = std::chrono::steady_clock::now();
+  // ---- X made B-orthonormal, and the coupling e = ||OP X - X H11||_B with H11 = X^T B OP X
+  Basis X1;
+  alloc_basis(X1, n, bid, 2 * m, m);
+  copy_cols(n, m, x, n, X1.v(0), n, s);
+  {
+    std::vector<double> H;
+    ortho_block(X1, op, 0, m, H, rng, s);
+  }
+  op.apply(X1.v(0), n, X1.v(m), n, m);
+  res.op_applications += m;
+  std::vector<double> H11, G;
+  gram(n, m, m, bid ? X1.v(0) : X1.bv(0), n, X1.v(m), n, X1.g.p, X1.part.p, X1.part_cap, s);
+  to_host(H11, X1.g.p, static_cast<std::size_t>(m) * m, s);
+  gemm_tall(n, m, m, X1.v(0), n, X1.g.p, m, X1.v(m), n, -1.0, 1.0, s);
+  if (!bid) op.bprod(X1.v(m), n, X1.bv(m), n, m);
+  gram(n, m, m, X1.v(m), n, bid ? X1.v(m) : X1.bv(m), n, X1.g.p, X1.part.p, X1.part_cap, s);
+  to_host(G, X1.g.p, static_cast<std::size_t>(m) * m, s);
+  {
+    std::vector<double> Hs(H11), mu;
+    for (int a = 0; a < m; ++a)
+      for (int b = 0; b < a; ++b) { const double v = 0.5 * (Hs[a + b * m] + Hs[b + a * m]); Hs[a + b * m] = v; Hs[b + a * m] = v; }
+    sym_eig(m, Hs, mu);
+    std::sort(mu.begin(), mu.end(), [](double a, double b) { return std::fabs(a) > std::fabs(b); });
+    res.deflated_theta = mu;
+  }
+  const double mu_max = res.deflated_theta.empty() ? 0.0 : std::fabs(res.deflated_theta.front());
+  // the B-norm of the residual block, with a guard for the rounding of H11 and of the Gram matrix
+  res.coupling = std::sqrt(std::max(0.0, sym_max_eig(m, G))) + 64.0 * std::numeric_limits<double>::epsilon() * mu_max;
+  const double e = res.coupling;
+  const double theta_c = 1.0 / opt.radius - e;
+  res.claim_threshold = theta_c * (1.0 - opt.rounding_margin);
+  res.pass_threshold = 1.0 / opt.pass_radius;
+  res.epsilon = res.claim_threshold > 0.0 ? 1.0 - res.pass_threshold / res.claim_threshold : 0.0;
+  for (double mv : res.deflated_theta) {
+    if (std::fabs(mv) >= theta_c) ++res.found_inside;
+    if (std::fabs(mv) >= 1.0 / opt.radius + e) ++res.certified_inside;
+  }
+  res.setup_s = seconds_since(t0);
+  if (!(res.epsilon > 0.0)) return res;  // no statement: the gap is too small for the coupling
+  // ---- the plan: s block steps fixed before the run
+  std::int64_t steps = exclusion_block_steps(res.epsilon, opt.delta, N, p, opt.kappa, false);
+  if (steps < 1) return res;
+  res.block_steps_planned = static_cast<int>(std::min<std::int64_t>(steps, 1 << 30));
+  bool capped = false;
+  if (opt.max_block_steps > 0 && steps > opt.max_block_steps) { steps = opt.max_block_steps; capped = true; }
+  res.exact = steps * p >= N;
+  const std::int64_t vectors = res.exact ? N : steps * p;
+  res.krylov_vectors_planned = static_cast<int>(std::min<std::int64_t>(vectors, 1 << 30));
+  if (opt.max_krylov_vectors > 0 && vectors > opt.max_krylov_vectors) {
+    res.over_budget = true;
+    return res;
+  }
+  if (res.exact) steps = (N + p - 1) / p;
+  const int S = static_cast<int>(steps);
+  // ---- block Lanczos on the complement of span X, full CGS2 re-orthogonalization against [X V]
+  t0 = std::chrono::steady_clock::now();
+  Basis B;
+  alloc_basis(B, n, bid, m + (S + 1) * p, std::max(m, p));
+  copy_cols(n, m, X1.v(0), n, B.v(0), n, s);
+  if (!bid) copy_cols(n, m, X1.bv(0), n, B.bv(0), n, s);
+  random_block(B, m, p, rng, s);
+  if (start_scale) diag_scale(n, p, start_scale, B.v(m), n, B.v(m), n, s);
+  {
+    std::vector<double> H;
+    ortho_block(B, op, m, p, H, rng, s);
+  }
+  const int k = S * p;
+  std::vector<double> T(static_cast<std::size_t>(k) * k, 0.0);
+  for (int st = 0; st < S; ++st) {
+    const int j = m + (st + 1) * p;
+    op.apply(B.v(j - p), n, B.v(j), n, p);
+    res.op_applications += p;
+    std::vector<double> H;
+    std::vector<double> R = ortho_block(B, op, j, p, H, rng, s);
+    const int rows = (st + 1) * p;  // the rows of H on V_0 .. V_st (below the m rows of X)
+    for (int c = 0; c < p; ++c) {
+      for (int t = 0; t < rows; ++t) T[t + static_cast<std::size_t>(st * p + c) * k] = H[(m + t) + static_cast<std::size_t>(c) * j];
+      if (st + 1 < S)
+        for (int a = 0; a < p; ++a) T[(rows + a) + static_cast<std::size_t>(st * p + c) * k] = R[a + static_cast<std::size_t>(c) * p];
+    }
+    res.block_steps = st + 1;
+  }
+  for (int a = 0; a < k; ++a)
+    for (int b = 0; b < a; ++b) { const double v = 0.5 * (T[a + static_cast<std::size_t>(b) * k] + T[b + static_cast<std::size_t>(a) * k]); T[a + static_cast<std::size_t>(b) * k] = v; T[b + static_cast<std::size_t>(a) * k] = v; }
+  sym_eig(k, T, res.ritz);
+  for (double th : res.ritz) {
+    res.max_ritz = std::max(res.max_ritz, std::fabs(th));
+    if (std::fabs(th) >= res.pass_threshold) ++res.new_count;
+    if (std::fabs(th) >= 1.0 / opt.radius) ++res.new_inside;
+  }
+  res.krylov_s = seconds_since(t0);
+  res.failure_probability = res.exact ? 0.0 : exclusion_failure_bound(res.epsilon, S, N, p, opt.kappa, false);
+  if (res.max_ritz >= res.pass_threshold) res.status = ExclusionStatus::Detected;
+  else if (!capped || res.failure_probability <= opt.delta) res.status = ExclusionStatus::Passed;
+  return res;
+}
+
 }  // namespace hsg
 
 namespace hsg {

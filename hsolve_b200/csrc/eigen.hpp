@@ -68,6 +68,64 @@ struct KsResult {
 
 KsResult krylov_schur(KrylovOperator& op, std::int64_t n, const KsOptions& opt, cudaStream_t stream);
 
+// Randomized exclusion check on the factorization already held at a shift sigma (hsolve's
+// exclusion_check, include/hsolve/verify.hpp:18-80; src/verify/exclusion.cpp): with X the found
+// eigenvectors of OP = (A - sigma B)^{-1} B (B positive definite), does the pencil have more
+// eigenvalues than the found ones within `radius` of sigma? Weyl reduction with the coupling
+// e = ||OP X - X H11||_B, then block Lanczos on the complement of span X from a Gaussian start
+// block, s block steps fixed before the run from the failure bound (exclusion_block_steps); the
+// check passes iff every Ritz value on the complement has |theta| < 1 / pass_radius.
+struct ExclusionOptions {
+  double radius = 0.0;           // r
+  double pass_radius = 0.0;      // r' > r
+  double delta = 1e-12;          // target failure probability
+  int block = 4;                 // p
+  std::uint64_t seed = 2026;
+  double kappa = 1.0;            // >= cond(S B S) of the start block's covariance (1 for B = I)
+  double rounding_margin = 1e-6;
+  double coupling_bound = -1.0;  // >= 0: the caller's bound on e (no application of OP to X)
+  int max_block_steps = 0;       // 0: no cap
+  int max_krylov_vectors = 512;  // the plan's basis size above which the check is Inconclusive
+};
+
+enum class ExclusionStatus { Passed = 0, Detected = 1, Inconclusive = 2 };
+
+struct ExclusionResult {
+  ExclusionStatus status = ExclusionStatus::Inconclusive;
+  double claim_threshold = 0.0;  // Theta_eff = (1/r - e)(1 - rounding_margin)
+  double pass_threshold = 0.0;   // tau = 1/r'
+  double coupling = 0.0;         // e
+  double epsilon = 0.0;          // 1 - tau / Theta_eff
+  double kappa = 1.0;
+  std::int64_t deflated = 0, dimension = 0;
+  std::int64_t found_inside = 0, certified_inside = 0;
+  int block = 0, block_steps_planned = 0, block_steps = 0, krylov_vectors_planned = 0;
+  bool exact = false, over_budget = false;
+  double max_ritz = 0.0;
+  double failure_probability = 1.0;
+  std::int64_t new_count = 0, new_inside = 0;
+  std::int64_t op_applications = 0;
+  bool rigorous = true;                // false: kappa is the caller's estimate, not a proven bound
+  std::vector<double> deflated_theta;  // eigenvalues of H11 by decreasing |mu|
+  std::vector<double> ritz;            // Ritz values of the run, ascending
+  double setup_s = 0.0, krylov_s = 0.0;
+};
+
+// P(pass and more than the found eigenvalues within r) for relative gap eps after s block steps of
+// p columns on a complement of dimension N (verify.hpp:177-180); 1 for eps <= 0, 0 for N = 0.
+double exclusion_failure_bound(double eps, std::int64_t s, std::int64_t N, std::int64_t p, double kappa,
+                               bool complex_scalars);
+// Smallest s >= 1 whose bound is <= delta, at most ceil(N / p) + 1 (a space covering the
+// complement); -1 for eps <= 0 or delta outside (0, 1) (verify.hpp:182-188).
+std::int64_t exclusion_block_steps(double eps, double delta, std::int64_t N, std::int64_t p, double kappa,
+                                   bool complex_scalars);
+
+// x: n x m device block (ld n), the found eigenvectors (any basis of their span). start_scale:
+// optional positive diagonal S (device, n) of the Gaussian start columns S g (B^-1/2 for a diagonal
+// B, which makes kappa = cond(S B S) = 1), or nullptr.
+ExclusionResult exclusion_check(KrylovOperator& op, std::int64_t n, const double* x, int m,
+                                const ExclusionOptions& opt, const double* start_scale, cudaStream_t stream);
+
 }  // namespace hsg
 
 namespace hsg {

@@ -84,6 +84,49 @@ HSG_API int hsg_solution_complex_copy(const hsg_solution* s, double* eigenvalues
 HSG_API const char* hsg_solution_report(const hsg_solution* s);
 HSG_API void hsg_solution_free(hsg_solution* s);
 
+/* Randomized exclusion certificate (hsolve's hs::exclusion_check, include/hsolve/verify.hpp:18-80,
+ * 110-175): on the factorization of K = A - sigma B (B positive definite) and the found eigenvectors
+ * X (host, n x m column-major, ld >= n), a block Lanczos run on the complement of span X from a
+ * Gaussian start decides, with failure probability at most `delta`, whether the pencil has more
+ * eigenvalues than the found ones within `radius` of sigma: status 0 passed (no Ritz value on the
+ * complement with |theta| >= 1 / pass_radius), 1 detected, 2 inconclusive (the gap between radius
+ * and pass_radius is too small for the coupling of X, or the plan exceeds max_krylov_vectors). The
+ * session factorizes at sigma (moved slightly, like the solver's shifts, when K is singular there;
+ * the shift used is returned). No counterpart in hsolve's C++ API beyond exclusion_check itself. */
+typedef struct {
+  double sigma, radius, pass_radius;
+  double delta;            /* target failure probability, in (0, 1); default 1e-12 */
+  int32_t block_size;      /* start columns p (1..16); default 4 */
+  int32_t max_block_steps; /* 0: no cap */
+  int32_t max_krylov_vectors; /* default 512 */
+  int32_t pad;
+  uint64_t seed;           /* default 2026 */
+  double kappa;            /* general B only: the caller's bound on cond(B); default 1 */
+  double rounding_margin;  /* default 1e-6 */
+} hsg_exclusion_options_t;
+
+typedef struct {
+  int32_t status;          /* 0 passed, 1 detected, 2 inconclusive */
+  int32_t exact;           /* the Krylov space covered the complement (failure probability 0) */
+  int32_t over_budget, rigorous;
+  double sigma;            /* the shift factorized */
+  double claim_threshold, pass_threshold, coupling, epsilon, kappa;
+  int64_t deflated, dimension, found_inside, certified_inside;
+  int64_t block_size, block_steps_planned, block_steps, krylov_vectors_planned;
+  double max_ritz, failure_probability;
+  int64_t new_count, new_inside, op_applications;
+  double setup_s, krylov_s;
+} hsg_exclusion_result_t;
+
+HSG_API void hsg_default_exclusion_options(hsg_exclusion_options_t* opt);
+HSG_API int hsg_session_exclusion_check(hsg_session* s, const double* x, int64_t m, int64_t ldx,
+                                        const hsg_exclusion_options_t* opt, hsg_exclusion_result_t* out);
+/* The failure bound delta(s) and the planned block steps (verify.hpp:177-188). */
+HSG_API double hsg_exclusion_failure_bound(double epsilon, int64_t block_steps, int64_t dimension,
+                                           int64_t block_size, double kappa, int32_t complex_scalars);
+HSG_API int64_t hsg_exclusion_block_steps(double epsilon, double delta, int64_t dimension, int64_t block_size,
+                                          double kappa, int32_t complex_scalars);
+
 #ifdef __cplusplus
 }
 #endif
