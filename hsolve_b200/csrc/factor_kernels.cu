@@ -405,11 +405,13 @@ __device__ __forceinline__ float warp_maxf(float v) {
 // single precision (a threshold test needs no more), the argmax for a 2 x 2 partner only when the
 // 1 x 1 test fails, one reciprocal per pivot. The update of a step reads the pivot column(s) into
 // registers first, so its column read-modify-writes are independent and pipeline (and the routine
-// stays a compact loop: it runs once per panel, from a cold instruction cache).
+// stays a compact loop: it runs once per panel, from a cold instruction cache). Not inlined: as a
+// function of its own it is register-allocated apart from the panel kernels' other phases (255
+// registers), which measured faster than the inlined loop; the call is once per panel.
 // Warp-synchronous: no block barriers. Returns the eliminated count; [e, w) could not be pivoted.
 template <class R>
-__device__ int warp_block_bk(R* F, int w, bool root, double u, double thr, int* lab, signed char* pv,
-                             StepShared& st, int j0 = 0, int prog0 = 0) {
+__device__ __noinline__ int warp_block_bk(R* F, int w, bool root, double u, double thr, int* lab, signed char* pv,
+                                          StepShared& st, int j0 = 0, int prog0 = 0) {
   const int lane = threadIdx.x & 31;
   constexpr int ld = kNB;
   __shared__ R s_c0[kNB], s_c1[kNB];
