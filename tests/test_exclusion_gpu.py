@@ -56,3 +56,29 @@ def test_exclusion_passes_detects_and_refuses():
     with pytest.raises(hsolve.InvalidInputError):
         sess.exclusion_check(x, sigma=sigma, radius=radius, pass_radius=radius)
     sess.close()
+
+
+def test_exclusion_complex_pencil_runs_on_the_embedding():
+    """A complex Hermitian (Bloch) pencil: the found complex eigenvectors are embedded into the real
+    2n problem the session holds, where every eigenvalue appears twice; the found set passes with
+    every count doubled."""
+    box = yee.Box((7, 6, 6), (1.0, 0.9, 0.8), "bloch", (0.9, 0.4, 0.2))
+    a, b = yee.pencil(box, "generalized")
+    w = yee_exact.exact_spectrum(box.cells, box.lengths, "bloch", box.phases)
+    wp = np.sort(w[w > 1.0])
+    sigma = 0.5 * (wp[8] + wp[9]) + 0.123
+    d = np.sort(np.abs(w - sigma))
+    k = next(k for k in range(4, 30) if d[k] > 1.2 * d[k - 1])
+    sess = hsolve.Session(a, b)
+    res = sess.solve(sigma=sigma, k=k)
+    assert res.report["success"]
+    x = res.eigenvectors
+    assert np.iscomplexobj(x) and x.shape[1] == k
+    radius = d[k - 1] * (1.0 + 1e-6)
+    pass_radius = d[k - 1] + 0.9 * (d[k] - d[k - 1])
+    r = sess.exclusion_check(x, sigma=sigma, radius=radius, pass_radius=pass_radius, delta=1e-12)
+    assert r["status"] == "passed", r
+    assert r["deflated"] == 2 * k and r["found_inside"] == 2 * k and r["certified_inside"] == 2 * k
+    assert r["dimension"] == 2 * a.shape[0] - 2 * k
+    assert r["failure_probability"] <= 1e-12 or r["exact"]
+    sess.close()
