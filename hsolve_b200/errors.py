@@ -4,7 +4,8 @@ from __future__ import annotations
 
 
 class HsolveError(Exception):
-    """Base class of every hsolve error. ``code`` is the hs::Error code name (snake_case)."""
+    """Root of the error classes this package raises; ``code`` holds the snake_case name of the C++
+    error code (hs::Error::Code) the error stands for."""
 
     code = "unknown"
 
@@ -51,7 +52,8 @@ class InternalError(HsolveError, RuntimeError):
 
 
 class HsolveWarning(UserWarning):
-    """Issued when a solve finishes without meeting the tolerance (report['success'] is False)."""
+    """Warning for a solve that returned pairs short of the requested tolerance; the report then
+    carries success = False."""
 
 
 ERROR_CLASSES = (InvalidInputError, HsolveIOError, NotHermitianError, UnsupportedError, FactorizationFailedError,
