@@ -656,6 +656,10 @@ class Session:
         x = np.asarray(X)
         if x.ndim == 1:
             x = x[:, None]
+        if x.ndim != 2:
+            raise InvalidInputError(f"X must be an n x m array, got {x.ndim} dimensions")
+        if np.iscomplexobj(x) and not self._complex:
+            raise InvalidInputError("X is complex but the pencil is real")
         if self._complex:
             xc = x.astype(np.complex128)
             x = np.block([[xc.real, -xc.imag], [xc.imag, xc.real]])
